@@ -1,0 +1,366 @@
+"""Benchmark of the UFEM Navier-Stokes hot path on B200.
+
+Workload (default): the 3D tetrahedral configuration -- unit cube, 64^3 cells x
+6 Kuhn tetrahedra (1,572,864 tets, 274,625 nodes, 64,300,048 CSR values),
+jitter 0.15h, 6 sine modes, nu = 1e-3, dt = 5e-3 -- with seeded synthetic data.
+A step is one full assembly of the linear system of a time step
+(LinearizeU + element assembly + scatter into the CSR + symmetric Dirichlet),
+inputs resident in HBM; the metric is elements assembled per second (Melem/s).
+
+`e2e` is the same metric through the public C ABI with host buffers: every step
+uploads the fields from pinned host memory (ufem_ns_upload_state), assembles,
+applies the boundary conditions and reads the RHS back (ufem_ns_download_system).
+
+Also reported (extra keys): the roofline of the assembly kernel, the FP64 CPU
+oracle timed on this host as the baseline, and full time steps per second
+(assembly + BCs + Krylov solve + update) for the plain FP64 path and the
+mixed-precision path with their relative difference.
+
+Multi-GPU: the path does not shard in this build (one GPU per mesh), so
+`--gpus N` (under torchrun) runs N independent replicas; value is the sum over
+ranks of the elements assembled divided by the max-over-ranks time.
+
+`--impl reference` times the reference algorithm's CPU restatement (the FP64
+oracle, all host threads) on the same workload and metric.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "Melem/s assembled"
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--n", type=int, default=64, help="cells per cube side (64 = the benchmark configuration)")
+    ap.add_argument("--precision", default="fp64", choices=["fp64", "fp32"])
+    ap.add_argument("--specialized", action="store_true", help="use the closed-form specialised kernels")
+    ap.add_argument("--no-extras", action="store_true", help="skip CPU baseline and time-step extras")
+    ap.add_argument("--time-steps", type=int, default=2, help="full time steps timed per solver variant")
+    return ap.parse_args()
+
+
+def dist_init(ngpus):
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+
+        import torch
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+    return rank, world, local
+
+
+def max_over_ranks(x: float, world: int) -> float:
+    if world <= 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def barrier(world):
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+class ClockSampler:
+    """nvidia-smi clock/throttle samples during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.gpu = gpu_index
+        self.proc = None
+        self.path = os.path.join("/tmp", f"ufem_clocks_{os.getpid()}.csv")
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+        return self
+
+    def __exit__(self, *exc):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self) -> dict:
+        try:
+            rows = [line.split(",") for line in open(self.path).read().strip().splitlines() if line.strip()]
+        except Exception:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unavailable"]}
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"]}
+        sm = [float(r[1]) for r in rows if r[1].strip().replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in rows if r[2].strip().replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[k] for r in rows for k in range(4) if len(r) > 5 + k and "Active" in r[5 + k]
+                          and "Not" not in r[5 + k]})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(rows)}
+
+
+def algorithmic_bytes(E, N, nnz, dim):
+    """Compulsory HBM bytes of one assembly: connectivity, node data read once
+    (coordinates, advection velocity, viscosity, state), each CSR value written
+    once, the RHS written once."""
+    neq = dim + 1
+    return E * (dim + 1) * 4 + N * (8 * dim + 8 * dim + 8 + 8 * neq) + nnz * 8 + N * neq * 8
+
+
+def measured_peak():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def profiled_traffic():
+    p = os.path.join(ROOT, "profiles", "assembly_traffic.json")
+    try:
+        with open(p) as f:
+            return json.load(f)
+    except Exception:
+        return None
+
+
+def cpu_baseline(pb, threads: int, reps: int = 1):
+    import oracle as O
+    o = O.Oracle(pb.coords, pb.conn, O.options(dt=pb.dt, use_specializations=False))
+    o.set_state(pb.up, pb.lin, pb.nu)
+    t = o.time_assembly(threads, reps) / reps
+    o.close()
+    return pb.nb_elems / t / 1e6, t
+
+
+def run_reference(args, rank, world):
+    """The reference algorithm on the host cores: the FP64 restatement of the
+    UFEM assembly (per-element Proto expression, BlockAccumulator reorder,
+    FEVbr column search), node-partitioned over all host threads like the
+    reference's MPI ranks."""
+    if rank != 0:
+        return
+    from coolfluid3_b200 import problems as P
+    import oracle as O
+    pb = P.make_problem(3, args.n, nu=1e-3, dt=5e-3, steps=10)
+    threads = os.cpu_count() or 1
+    o = O.Oracle(pb.coords, pb.conn, O.options(dt=pb.dt, use_specializations=False))
+    o.set_state(pb.up, pb.lin, pb.nu)
+    o.add_dirichlet(pb.bc_nodes, pb.bc_comps, pb.bc_values)
+    for _ in range(args.warmup):
+        o.time_assembly(threads, 1)
+    times = [o.time_assembly(threads, 1) for _ in range(args.steps)]
+    t = float(np.mean(times))
+    value = pb.nb_elems / t / 1e6
+    line = {
+        "impl": "reference", "metric": METRIC, "value": round(value, 3), "unit": "Melem/s", "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(t * 1e3, 3), "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": f"3D P1 tets {args.n}^3x6 ({pb.nb_elems} tets, {pb.nb_nodes} nodes) NS assembly",
+                   "parallelism": "replicas"},
+        "cpu_baseline": {"value": round(value, 3), "unit": "Melem/s", "cores": threads, "kind": "port",
+                         "sample": f"full assembly of the {pb.nb_elems}-tet mesh per step"},
+        "e2e": {"value": round(value, 3), "unit": "Melem/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def run_ours(args, rank, world, local):
+    import torch
+
+    from coolfluid3_b200 import NavierStokes
+    from coolfluid3_b200 import _native as Nat
+    from coolfluid3_b200 import problems as P
+
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    pb = P.make_problem(3, args.n, nu=1e-3, dt=5e-3, steps=10)
+    E, Nn, dim = pb.nb_elems, pb.nb_nodes, 3
+    ns = NavierStokes(pb.coords, pb.conn, dt=pb.dt, use_specializations=args.specialized, precision=args.precision)
+    ns.set_state(pb.up, pb.lin, pb.nu)
+    ns.add_dirichlet(pb.bc_nodes, pb.bc_comps, pb.bc_values)
+    stream = torch.cuda.Stream(device=dev)
+    sptr = stream.cuda_stream
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)  # 256 MiB > 126 MB L2
+
+    def assemble_step():
+        ns.assemble(sptr)
+        ns.apply_dirichlet(sptr)
+
+    ns.enable_timing(True)
+    with torch.cuda.stream(stream):
+        for _ in range(args.warmup):
+            flush.zero_()
+            assemble_step()
+    torch.cuda.synchronize()
+    barrier(world)
+    torch.cuda.synchronize()
+    starts = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    ends = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    kernel_ms = []
+    with ClockSampler(local) as clk:
+        with torch.cuda.stream(stream):
+            for k in range(args.steps):
+                flush.zero_()
+                starts[k].record(stream)
+                assemble_step()
+                ends[k].record(stream)
+                kernel_ms.append(ns.timings()["assembly_ms"])  # events on the launch stream, kernel alone
+        torch.cuda.synchronize()
+    barrier(world)
+    torch.cuda.synchronize()
+    step_ms = [s.elapsed_time(e) for s, e in zip(starts, ends)]
+    ms = max_over_ranks(float(np.mean(step_ms)), world)
+    value = E * world / (ms / 1e3) / 1e6
+    kern_ms = float(np.mean(kernel_ms))
+    B = algorithmic_bytes(E, Nn, ns.nnz, dim)
+    peak, peak_kind = measured_peak()
+    achieved = B / (kern_ms / 1e3) / 1e9
+    traffic = profiled_traffic()
+    traffic_bytes = None
+    if traffic and traffic.get("n") == args.n and traffic.get("precision") == args.precision \
+            and traffic.get("specialized", False) == args.specialized:
+        traffic_bytes = traffic.get("bytes_per_launch")
+
+    # ---- end to end through the C ABI with pinned host buffers ----------------
+    up_h = torch.from_numpy(pb.up).pin_memory()
+    lin_h = torch.from_numpy(pb.lin).pin_memory()
+    nu_h = torch.from_numpy(pb.nu).pin_memory()
+    rhs_h = torch.empty(ns.nb_rows, dtype=torch.float64).pin_memory()
+    lib = Nat.lib()
+
+    def e2e_step():
+        Nat.check(lib.ufem_ns_upload_state(ns.handle, Nat.raw_dptr(up_h.data_ptr()), Nat.raw_dptr(lin_h.data_ptr()),
+                                           Nat.raw_dptr(nu_h.data_ptr()), None, Nat.C.c_void_p(sptr)))
+        assemble_step()
+        Nat.check(lib.ufem_ns_download_system(ns.handle, None, Nat.raw_dptr(rhs_h.data_ptr()),
+                                              Nat.C.c_void_p(sptr)))
+        stream.synchronize()
+
+    for _ in range(args.warmup):
+        e2e_step()
+    barrier(world)
+    e2e_ms_list = []
+    for _ in range(args.steps):
+        s0 = torch.cuda.Event(enable_timing=True)
+        s1 = torch.cuda.Event(enable_timing=True)
+        s0.record(stream)
+        e2e_step()
+        s1.record(stream)
+        s1.synchronize()
+        e2e_ms_list.append(s0.elapsed_time(s1))
+    e2e_ms = max_over_ranks(float(np.mean(e2e_ms_list)), world)
+    h2d = pb.up.nbytes + pb.lin.nbytes + pb.nu.nbytes
+    d2h = ns.nb_rows * 8
+
+    line = {
+        "metric": METRIC, "value": round(value, 3), "unit": "Melem/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": round(ms, 4), "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64" if args.precision == "fp64" else "f32-element/f64-scatter",
+        "data": "synthetic",
+        "config": {"workload": f"3D P1 tets {args.n}^3x6 ({E} tets, {Nn} nodes, {ns.nnz} CSR values) "
+                               "PSPG/SUPG NS assembly + symmetric Dirichlet",
+                   "element_kernel": "specialized" if args.specialized else "generic (order-2 quadrature)",
+                   "precision": args.precision, "parallelism": "replicas" if world > 1 else "single GPU",
+                   "l2": "256 MiB buffer written between timed steps (flush)"},
+        "gpu_launches": 5 * args.steps,
+        "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
+                     "frac": round(achieved / peak, 4), "peak_kind": peak_kind,
+                     "traffic": traffic_bytes, "algorithmic_bytes": B, "kernel_ms": round(kern_ms, 4)},
+        "e2e": {"value": round(E * world / (e2e_ms / 1e3) / 1e6, 3), "unit": "Melem/s",
+                "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h), "ms_per_step": round(e2e_ms, 3)},
+        "clocks": clk.summary(),
+    }
+
+    if rank == 0 and world == 1 and not args.no_extras:
+        # ---- CPU baseline: the FP64 oracle on this host -------------------------
+        v1, t1 = cpu_baseline(pb, 1)
+        threads = os.cpu_count() or 1
+        vall, tall = cpu_baseline(pb, threads)
+        line["cpu_baseline"] = {"value": round(v1, 3), "unit": "Melem/s", "cores": 1, "kind": "port",
+                                "sample": f"one full FP64 assembly of the {E}-tet mesh ({t1:.2f} s)",
+                                "all_cores": {"value": round(vall, 3), "cores": threads, "seconds": round(tall, 3)}}
+        # ---- full time steps: plain FP64 vs mixed precision ---------------------
+        line["time_step"] = time_steps(ns, pb, args, stream, sptr)
+    ns.close()
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+
+
+def time_steps(ns, pb, args, stream, sptr):
+    """Full steps (assembly + BCs + Krylov + update), steps/s and per-step latency."""
+    import torch
+    out = {}
+    base_up = pb.up
+    results = {}
+    for label, kw in (("plain_fp64", dict(mixed=False)), ("mixed", dict(mixed=True, inner_tol=1e-4))):
+        ns.set_state(pb.up, pb.lin, pb.nu)
+        ns.set_solution(np.zeros(ns.nb_rows))
+        lat = []
+        iters = []
+        for k in range(args.time_steps):
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            st = ns.execute(sptr, tol=1e-10, max_iters=3000, **kw)
+            torch.cuda.synchronize()
+            lat.append((time.perf_counter() - t0) * 1e3)
+            iters.append(st["iterations"])
+        up, _ = ns.state()
+        results[label] = up
+        out[label] = {"steps_per_s": round(1e3 / float(np.mean(lat)), 3), "p50_ms": round(float(np.median(lat)), 2),
+                      "max_ms": round(float(np.max(lat)), 2), "krylov_iters": iters,
+                      "converged": int(st["converged"])}
+    ref = results["plain_fp64"]
+    out["mixed"]["rel_err_vs_plain"] = float(np.linalg.norm(results["mixed"] - ref) / np.linalg.norm(ref))
+    out["steps"] = args.time_steps
+    ns.set_state(base_up, pb.lin, pb.nu)
+    return out
+
+
+def main():
+    args = parse()
+    rank, world, local = dist_init(args.gpus)
+    try:
+        if args.impl == "reference":
+            run_reference(args, rank, world)
+        else:
+            run_ours(args, rank, world, local)
+    finally:
+        if world > 1:
+            import torch.distributed as dist
+            dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

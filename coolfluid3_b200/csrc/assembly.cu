@@ -1,0 +1,1010 @@
+// assembly.cu -- sm_100a kernels of the UFEM Navier-Stokes step, except the Krylov solve.
+//
+// Row-owner assembly.  The reference loops over elements and adds each element
+// matrix into the FEVbr block rows it touches (Proto/ElementLooper.hpp:173-179,
+// TrilinosFEVbrMatrix.cpp:271-357).  Here every CTA owns a contiguous range of
+// CSR block rows ("chunk").  Phase 1: one thread per incidence (row node i,
+// element e containing i at local position a) gathers the element's nodal data,
+// evaluates the element's row block a -- the neq x (n*neq) slice of
+// invdt*T + theta*A and the neq entries of -A*x + a -- and stages it in shared
+// memory.  Phase 2: one thread per (row, neighbour slot, equation) sums the
+// staged contributions of the row's incidences in ascending element order (the
+// order in which the reference adds them) and writes each CSR value exactly
+// once, coalesced.  No floating-point atomics, no element matrices in HBM.
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <cstdint>
+#include <type_traits>
+
+#include "internal.h"
+
+namespace ufem {
+namespace {
+
+template <int D>
+struct P1 {
+  static constexpr int n = D + 1;           // nodes per element
+  static constexpr int neq = D + 1;         // u, v, [w], p
+  static constexpr int nvals = n * neq * neq;  // one element row block
+};
+
+template <typename T>
+struct KParams {
+  T theta, dt, invdt, rho, c1, c2, a_ps, a_su, a_bu, u_ref;
+  int supg_type, has_force;
+};
+
+template <typename T>
+__device__ __forceinline__ KParams<T> make_kparams(const NSParams& p) {
+  KParams<T> k;
+  k.theta = T(p.theta); k.dt = T(p.dt); k.invdt = T(p.invdt); k.rho = T(p.rho);
+  k.c1 = T(p.c1); k.c2 = T(p.c2); k.a_ps = T(p.a_ps); k.a_su = T(p.a_su); k.a_bu = T(p.a_bu);
+  k.u_ref = T(p.u_ref); k.supg_type = p.supg_type; k.has_force = p.has_force;
+  return k;
+}
+
+__device__ __forceinline__ double tsqrt(double x) { return sqrt(x); }
+__device__ __forceinline__ float tsqrt(float x) { return sqrtf(x); }
+__device__ __forceinline__ double tabs(double x) { return fabs(x); }
+__device__ __forceinline__ float tabs(float x) { return fabsf(x); }
+__device__ __forceinline__ double tcbrt_pow(double x) { return pow(x, 1. / 3.); }
+__device__ __forceinline__ float tcbrt_pow(float x) { return powf(x, 1.f / 3.f); }
+
+// Runtime selection of a[i] for a compile-time-sized array without local memory.
+template <int M, typename T>
+__device__ __forceinline__ T sel(const T (&arr)[M], int i) {
+  T r = arr[0];
+#pragma unroll
+  for (int k = 1; k < M; ++k)
+    if (i == k) r = arr[k];
+  return r;
+}
+
+__device__ __forceinline__ void ld4(const double* __restrict__ p, double& a, double& b, double& c, double& d) {
+  const double2 x = __ldg(reinterpret_cast<const double2*>(p));
+  const double2 y = __ldg(reinterpret_cast<const double2*>(p) + 1);
+  a = x.x; b = x.y; c = y.x; d = y.y;
+}
+
+// Inverse and determinant in the cofactor form (Proto/ElementData.hpp:308-314).
+template <typename T>
+__device__ __forceinline__ void inverse_det(const T (&J)[2][2], T (&Ji)[2][2], T& det) {
+  det = J[0][0] * J[1][1] - J[1][0] * J[0][1];
+  const T inv = T(1) / det;
+  Ji[0][0] = J[1][1] * inv;
+  Ji[1][0] = -J[1][0] * inv;
+  Ji[0][1] = -J[0][1] * inv;
+  Ji[1][1] = J[0][0] * inv;
+}
+template <typename T>
+__device__ __forceinline__ void inverse_det(const T (&m)[3][3], T (&Ji)[3][3], T& det) {
+  T cof[3][3];
+#pragma unroll
+  for (int i = 0; i < 3; ++i)
+#pragma unroll
+    for (int j = 0; j < 3; ++j) {
+      const int i1 = (i + 1) % 3, i2 = (i + 2) % 3, j1 = (j + 1) % 3, j2 = (j + 2) % 3;
+      cof[i][j] = m[i1][j1] * m[i2][j2] - m[i1][j2] * m[i2][j1];
+    }
+  det = (cof[0][0] * m[0][0] + cof[1][0] * m[1][0]) + cof[2][0] * m[2][0];
+  const T inv = T(1) / det;
+#pragma unroll
+  for (int i = 0; i < 3; ++i)
+#pragma unroll
+    for (int j = 0; j < 3; ++j) Ji[j][i] = cof[i][j] * inv;
+}
+
+// Element data in the arithmetic type T.  Coordinates are made relative to the
+// element's node 0 in FP64 before any conversion, so the FP32 path keeps the
+// geometry at full relative accuracy.
+template <int D, typename T>
+struct Elem {
+  T Xr[D + 1][D];
+  T U[D + 1][D];   // u_adv
+  T NU[D + 1];     // nu_eff
+};
+
+template <int D, typename T>
+__device__ __forceinline__ void gather_geometry_uadv(const int (&ids)[4], const double* __restrict__ coords,
+                                                     const double* __restrict__ uadv, Elem<D, T>& el) {
+  double X0[4];
+  ld4(coords + 4ll * ids[0], X0[0], X0[1], X0[2], X0[3]);
+#pragma unroll
+  for (int b = 0; b <= D; ++b) {
+    double x[4];
+    ld4(coords + 4ll * ids[b], x[0], x[1], x[2], x[3]);
+#pragma unroll
+    for (int k = 0; k < D; ++k) el.Xr[b][k] = T(x[k] - X0[k]);
+    double u[4];
+    ld4(uadv + 4ll * ids[b], u[0], u[1], u[2], u[3]);
+#pragma unroll
+    for (int k = 0; k < D; ++k) el.U[b][k] = T(u[k]);
+    el.NU[b] = T(u[3]);
+  }
+}
+
+// ComputeTauImpl::compute_coefficients (SUPG.hpp:140-219).  Ji/det are the
+// element's (constant) Jacobian inverse and determinant.
+template <int D, typename T>
+__device__ __forceinline__ void compute_tau(int type, T c1, T c2, T u_ref, T a_ps, T a_su, T a_bu,
+                                            const Elem<D, T>& el, const T (&uc)[D], T element_nu, T dt,
+                                            const T (&Ji)[D][D], T det, T& tps, T& tsu, T& tbu) {
+  constexpr int n = D + 1;
+  if (type == 0) {  // TEZDUYAR
+    T h = T(1e10);
+#pragma unroll
+    for (int i = 0; i < n; ++i)
+#pragma unroll
+      for (int j = 0; j < n; ++j)
+        if (i != j) {
+          T s = 0;
+#pragma unroll
+          for (int k = 0; k < D; ++k) { const T d = el.Xr[i][k] - el.Xr[j][k]; s += d * d; }
+          h = s < h ? s : h;
+        }
+    h = tsqrt(h);
+    T um2 = 0;
+#pragma unroll
+    for (int k = 0; k < D; ++k) um2 += uc[k] * uc[k];
+    const T umag = tsqrt(um2);
+    tsu = T(1) / ((T(2) * umag) / h + T(2) / dt + (T(4) * element_nu) / (h * h));
+    tps = tsu;
+    tbu = tsu * umag * umag;
+  } else if (type == 1) {  // METRIC
+    T g[D][D];
+#pragma unroll
+    for (int a = 0; a < D; ++a)
+#pragma unroll
+      for (int b = 0; b < D; ++b) {
+        T s = 0;
+#pragma unroll
+        for (int k = 0; k < D; ++k) s += Ji[k][a] * Ji[k][b];
+        g[a][b] = s;
+      }
+    T adv = 0, sq = 0, tr = 0;
+#pragma unroll
+    for (int b = 0; b < D; ++b) {
+      T s = 0;
+#pragma unroll
+      for (int a = 0; a < D; ++a) s += uc[a] * g[a][b];
+      adv += s * uc[b];
+    }
+#pragma unroll
+    for (int a = 0; a < D; ++a) {
+      tr += g[a][a];
+#pragma unroll
+      for (int b = 0; b < D; ++b) sq += g[a][b] * g[a][b];
+    }
+    const T adv_sq = tabs(adv);
+    const T diff = element_nu * element_nu * sq;
+    tsu = T(1) / tsqrt((T(4) * c1 * c1 / (dt * dt)) + adv_sq + c2 * diff);
+    tps = tsu;
+    const T tsu_std = T(1) / tsqrt((T(4) / (dt * dt)) + adv_sq + T(16) * diff);
+    tbu = (T(1) / tsu_std) / tr;
+  } else {  // CF2
+    const T volume = (D == 2) ? det / T(2) : det / T(6);
+    const T pi = T(3.141592654);
+    const T he = (D == 2) ? tsqrt(T(4) / pi * volume) : tcbrt_pow(T(3) / T(4) / pi * volume);
+    const T ree = u_ref * he / (T(2) * element_nu);
+    const T xi = ree < T(3) ? ree / T(3) : T(1);
+    tps = he * xi / (T(2) * u_ref);
+    tbu = he * u_ref / xi;
+    tsu = 0;
+    T um2 = 0;
+#pragma unroll
+    for (int k = 0; k < D; ++k) um2 += uc[k] * uc[k];
+    const T umag = tsqrt(um2);
+    if (umag > T(1e-10)) {
+      // sum over nodes of u . grad N_b (a rounding-level number for P1)
+      T s = 0;
+#pragma unroll
+      for (int b = 0; b <= D; ++b) {
+        T t = 0;
+#pragma unroll
+        for (int k = 0; k < D; ++k) {
+          T gkb;
+          if (b == 0) {
+            T q = 0;
+#pragma unroll
+            for (int m = 0; m < D; ++m) q += Ji[k][m] * T(-1);
+            gkb = q;
+          } else {
+            gkb = Ji[k][b - 1];
+          }
+          t += uc[k] * gkb;
+        }
+        s += t;
+      }
+      const T h = T(2) * umag / s;
+      const T tau_adv = h / (T(2) * umag);
+      const T tau_time = T(0.5) * dt;
+      const T tau_diff = h * h / (T(4) * element_nu);
+      tsu = T(1) / (T(1) / tau_adv + T(1) / tau_time + T(1) / tau_diff);
+    }
+  }
+  tps *= a_ps;
+  tsu *= a_su;
+  tbu *= a_bu;
+}
+
+template <int D, typename T>
+__device__ __forceinline__ void centroid_N(T (&Nc)[D + 1]) {
+  const T mu = (D == 2) ? T(0.3333333333333333333333333) : T(0.25);
+  T s = 1;
+#pragma unroll
+  for (int k = 0; k < D; ++k) s -= mu;
+  Nc[0] = s;
+#pragma unroll
+  for (int k = 1; k <= D; ++k) Nc[k] = mu;
+}
+
+// Order-2 Gauss points (GaussImplementation.hpp:195-226 and :395-428).
+template <int D, typename T>
+__device__ __forceinline__ void gauss_N(int q, T (&N)[D + 1]) {
+  T xi[D];
+  if (D == 2) {
+    const T p[3][2] = {{T(0.5), T(0.0)}, {T(0.5), T(0.5)}, {T(0.0), T(0.5)}};
+#pragma unroll
+    for (int k = 0; k < D; ++k) xi[k] = p[q][k];
+  } else {
+    const T mu = T(0.13819660112501051517954131656);
+#pragma unroll
+    for (int k = 0; k < D; ++k) xi[k] = mu;
+    if (q > 0) xi[q - 1] = T(1) - T(3) * mu;
+  }
+  T s = 1;
+#pragma unroll
+  for (int k = 0; k < D; ++k) s -= xi[k];
+  N[0] = s;
+#pragma unroll
+  for (int k = 0; k < D; ++k) N[k + 1] = xi[k];
+}
+
+// Shared tail of both element forms: rhs row a, M = invdt*T + theta*A with the
+// p row of A divided by theta first (NavierStokesAssembly.hpp:69-71), staged.
+template <int D, typename T>
+__device__ __forceinline__ void stage_block(const T (&A)[D + 1][D + 1], const T (&Tm)[D + 1][D + 1],
+                                            const T (&xb)[D + 1], const KParams<T>& kp, T (&rhs)[D + 1],
+                                            T* __restrict__ st, int b, int CH) {
+  constexpr int neq = D + 1;
+#pragma unroll
+  for (int r = 0; r < neq; ++r) {
+    T s = 0;
+#pragma unroll
+    for (int c = 0; c < neq; ++c) s += -A[r][c] * xb[c];
+    rhs[r] += s;
+#pragma unroll
+    for (int c = 0; c < neq; ++c) {
+      const T a = (r == D) ? A[r][c] / kp.theta : A[r][c];
+      st[((b * neq + r) * neq + c) * CH] = kp.invdt * Tm[r][c] + kp.theta * a;
+    }
+  }
+}
+
+template <int D, typename T>
+__device__ __forceinline__ void load_state(const double* __restrict__ state, int node, T (&x)[D + 1]) {
+  double s[4];
+  ld4(state + 4ll * node, s[0], s[1], s[2], s[3]);
+#pragma unroll
+  for (int k = 0; k <= D; ++k) x[k] = T(s[k]);
+}
+
+// ---------------------------------------------------------------------------
+// Generic expression (NavierStokesAssembly.hpp:51-67) through the order-2
+// quadrature of Proto/ElementIntegration.hpp:236-258, for row node a.  Because
+// the P1 gradient G is constant, the q-sums are accumulated in factored form
+// (sum_q W f_q) * G, which is the same quadrature.
+// ---------------------------------------------------------------------------
+template <int D, typename T>
+__device__ __forceinline__ void generic_row(const int (&ids)[4], int a, const double* __restrict__ coords,
+                                            const double* __restrict__ uadv, const double* __restrict__ state,
+                                            const double* __restrict__ force, const KParams<T>& kp,
+                                            T* __restrict__ st, T* __restrict__ rst, int CH) {
+  constexpr int n = D + 1, neq = D + 1;
+  Elem<D, T> el;
+  gather_geometry_uadv<D, T>(ids, coords, uadv, el);
+  // tau from u_adv at the centroid, element_nu = |mean nodal nu| (SUPG.hpp:110-116)
+  T nsum = 0;
+#pragma unroll
+  for (int b = 0; b < n; ++b) nsum += el.NU[b];
+  const T element_nu = tabs(nsum / T(n));
+  T Nc[n];
+  centroid_N<D, T>(Nc);
+  T uc[D];
+#pragma unroll
+  for (int k = 0; k < D; ++k) {
+    T s = 0;
+#pragma unroll
+    for (int b = 0; b < n; ++b) s += Nc[b] * el.U[b][k];
+    uc[k] = s;
+  }
+  T J[D][D], Ji[D][D], det;
+#pragma unroll
+  for (int r = 0; r < D; ++r)
+#pragma unroll
+    for (int c = 0; c < D; ++c) J[r][c] = el.Xr[r + 1][c];
+  inverse_det<T>(J, Ji, det);
+  T tps, tsu, tbu;
+  compute_tau<D, T>(kp.supg_type, kp.c1, kp.c2, kp.u_ref, kp.a_ps, kp.a_su, kp.a_bu, el, uc, element_nu, kp.dt, Ji,
+                    det, tps, tsu, tbu);
+  T G[D][n];
+#pragma unroll
+  for (int r = 0; r < D; ++r) {
+    T s = 0;
+#pragma unroll
+    for (int k = 0; k < D; ++k) s += Ji[r][k] * T(-1);
+    G[r][0] = s;
+#pragma unroll
+    for (int b = 1; b <= D; ++b) G[r][b] = Ji[r][b - 1];
+  }
+  T Ga[D];
+#pragma unroll
+  for (int k = 0; k < D; ++k) Ga[k] = sel<n>(G[k], a);
+  T Da[n];
+#pragma unroll
+  for (int b = 0; b < n; ++b) {
+    T s = 0;
+#pragma unroll
+    for (int k = 0; k < D; ++k) s += Ga[k] * G[k][b];
+    Da[b] = s;
+  }
+  T F[n][D];
+  if (kp.has_force) {
+#pragma unroll
+    for (int b = 0; b < n; ++b) {
+      double f[4];
+      ld4(force + 4ll * ids[b], f[0], f[1], f[2], f[3]);
+#pragma unroll
+      for (int k = 0; k < D; ++k) F[b][k] = T(f[k]);
+    }
+  } else {
+#pragma unroll
+    for (int b = 0; b < n; ++b)
+#pragma unroll
+      for (int k = 0; k < D; ++k) F[b][k] = 0;
+  }
+  const T wq = (D == 2) ? T(1.0 / 6.0) : T(0.04166666666666666666666666666666666667);
+  const T W = wq * det;
+  T sW = 0, sWSp = 0, sWS = 0, gam[D], sWadv[n], sWN[n], Kd[n], Tuu[n], au[D];
+#pragma unroll
+  for (int k = 0; k < D; ++k) { gam[k] = 0; au[k] = 0; }
+#pragma unroll
+  for (int b = 0; b < n; ++b) { sWadv[b] = 0; sWN[b] = 0; Kd[b] = 0; Tuu[b] = 0; }
+#pragma unroll
+  for (int q = 0; q < n; ++q) {  // n Gauss points for both triangles (3) and tetrahedra (4)
+    T N[n];
+    gauss_N<D, T>(q, N);
+    T ua[D], gq[D], nuq = 0;
+#pragma unroll
+    for (int k = 0; k < D; ++k) {
+      T s = 0, f = 0;
+#pragma unroll
+      for (int b = 0; b < n; ++b) { s += N[b] * el.U[b][k]; f += N[b] * F[b][k]; }
+      ua[k] = s;
+      gq[k] = f;
+    }
+#pragma unroll
+    for (int b = 0; b < n; ++b) nuq += N[b] * el.NU[b];
+    T adv[n];
+#pragma unroll
+    for (int b = 0; b < n; ++b) {
+      T s = 0;
+#pragma unroll
+      for (int k = 0; k < D; ++k) s += ua[k] * G[k][b];
+      adv[b] = s;
+    }
+    const T Na = sel<n>(N, a), adva = sel<n>(adv, a);
+    const T Sa = Na + tsu * adva;
+    const T Spa = Na + tps * adva * T(0.5);
+    sW += W;
+    sWSp += W * Spa;
+    sWS += W * Sa;
+#pragma unroll
+    for (int k = 0; k < D; ++k) {
+      gam[k] += W * (tbu * Ga[k] + T(0.5) * ua[k] * Sa);
+      au[k] += W * (Sa * gq[k]);
+    }
+#pragma unroll
+    for (int b = 0; b < n; ++b) {
+      sWadv[b] += W * adv[b];
+      sWN[b] += W * N[b];
+      Kd[b] += W * (nuq * Da[b] + Sa * adv[b]);
+      Tuu[b] += W * (Sa * N[b]);
+    }
+  }
+  T rhs[neq];
+#pragma unroll
+  for (int k = 0; k < D; ++k) rhs[k] = au[k];
+  rhs[D] = 0;
+#pragma unroll
+  for (int b = 0; b < n; ++b) {
+    T A[neq][neq], Tm[neq][neq];
+#pragma unroll
+    for (int i = 0; i < D; ++i) {
+#pragma unroll
+      for (int j = 0; j < D; ++j) {
+        A[i][j] = (i == j ? Kd[b] : T(0)) + gam[i] * G[j][b];
+        Tm[i][j] = (i == j) ? Tuu[b] : T(0);
+      }
+      A[i][D] = G[i][b] * sWS / kp.rho;
+      Tm[i][D] = 0;
+      A[D][i] = G[i][b] * sWSp + tps * Ga[i] * sWadv[b];
+      Tm[D][i] = tps * Ga[i] * sWN[b];
+    }
+    A[D][D] = tps * Da[b] / kp.rho * sW;
+    Tm[D][D] = 0;
+    T xb[neq];
+    load_state<D, T>(state, ids[b], xb);
+    stage_block<D, T>(A, Tm, xb, kp, rhs, st, b, CH);
+  }
+#pragma unroll
+  for (int r = 0; r < neq; ++r) rst[r * CH] = rhs[r];
+}
+
+// ---------------------------------------------------------------------------
+// Specialised triangles, NavierStokesSpecializations.hpp:37-147, row i = a.
+// Each entry receives its terms in the reference's order.
+// ---------------------------------------------------------------------------
+template <int D, typename T>
+__device__ __forceinline__ void spec_tau_common(const Elem<D, T>& el, const double* __restrict__ state,
+                                                const int (&ids)[4], T nu, T dt, T& tps, T& tsu, T& tbu) {
+  // default ComputeTauImpl: METRIC, c1 = 1, c2 = 16, alphas 1, on the solution velocity u
+  constexpr int n = D + 1;
+  T Nc[n];
+  centroid_N<D, T>(Nc);
+  T uc[D];
+#pragma unroll
+  for (int k = 0; k < D; ++k) uc[k] = 0;
+#pragma unroll
+  for (int b = 0; b < n; ++b) {
+    T x[D + 1];
+    load_state<D, T>(state, ids[b], x);
+#pragma unroll
+    for (int k = 0; k < D; ++k) uc[k] += Nc[b] * x[k];
+  }
+  T J[D][D], Ji[D][D], det;
+#pragma unroll
+  for (int r = 0; r < D; ++r)
+#pragma unroll
+    for (int c = 0; c < D; ++c) J[r][c] = el.Xr[r + 1][c];
+  inverse_det<T>(J, Ji, det);
+  compute_tau<D, T>(1, T(1), T(16), T(1), T(1), T(1), T(1), el, uc, nu, dt, Ji, det, tps, tsu, tbu);
+}
+
+template <typename T>
+__device__ __forceinline__ void spec_tri_row(const int (&ids)[4], int ai, const double* __restrict__ coords,
+                                             const double* __restrict__ uadv, const double* __restrict__ state,
+                                             const KParams<T>& kp, T* __restrict__ st, T* __restrict__ rst, int CH) {
+  Elem<2, T> el;
+  gather_geometry_uadv<2, T>(ids, coords, uadv, el);
+  T u_avg[2];
+#pragma unroll
+  for (int k = 0; k < 2; ++k) {
+    T s = 0;
+#pragma unroll
+    for (int b = 0; b < 3; ++b) s += el.U[b][k];
+    u_avg[k] = s / T(3);
+  }
+  const auto& X = el.Xr;
+  const T volume = T(0.5) * ((X[1][0] - X[0][0]) * (X[2][1] - X[0][1]) - (X[2][0] - X[0][0]) * (X[1][1] - X[0][1]));
+  const T fc = T(0.5);
+  T nsum = 0;
+#pragma unroll
+  for (int b = 0; b < 3; ++b) nsum += el.NU[b];
+  const T nu = tabs(nsum / T(3));
+  T nx[3], ny[3];
+  nx[0] = X[1][1] - X[2][1]; ny[0] = X[2][0] - X[1][0];
+  nx[1] = X[2][1] - X[0][1]; ny[1] = X[0][0] - X[2][0];
+  nx[2] = X[0][1] - X[1][1]; ny[2] = X[1][0] - X[0][0];
+  T tau_ps, tau_su, tau_bulk;
+  spec_tau_common<2, T>(el, state, ids, nu, kp.dt, tau_ps, tau_su, tau_bulk);
+  const T nix = sel<3>(nx, ai), niy = sel<3>(ny, ai);
+  const T u_ni = u_avg[0] * nix + u_avg[1] * niy;
+  const T rho = kp.rho;
+  T rhs[3] = {0, 0, 0};
+#pragma unroll
+  for (int j = 0; j < 3; ++j) {
+    T A[3][3], Tm[3][3];
+#pragma unroll
+    for (int r = 0; r < 3; ++r)
+#pragma unroll
+      for (int c = 0; c < 3; ++c) { A[r][c] = 0; Tm[r][c] = 0; }
+    const T uk = u_avg[0], vk = u_avg[1];
+    const T uknj = uk * nx[j] + vk * ny[j];
+    T val = T(1. / 6.) * uknj;
+    val += tau_su / (T(4) * volume) * uknj * u_ni;
+    A[0][0] += val; A[1][1] += val;
+    val = tau_ps / (T(4) * volume) * uknj;
+    A[2][0] += val * nix; A[2][1] += val * niy;
+    val = fc / T(6);
+    val += fc * tau_su / (T(4) * volume) * u_ni;
+    A[0][0] += val * uk * nx[j]; A[0][1] += val * uk * ny[j];
+    A[1][0] += val * vk * nx[j]; A[1][1] += val * vk * ny[j];
+    val = fc * tau_ps / (T(4) * volume);
+    A[2][0] += val * nix * uk * nx[j]; A[2][1] += val * nix * uk * ny[j];
+    A[2][0] += val * niy * vk * nx[j]; A[2][1] += val * niy * vk * ny[j];
+    val = nu / (T(4) * volume);
+    A[0][0] += val * (T(4. / 3.) * nix * nx[j] + niy * ny[j]);
+    A[0][1] += val * nix * ny[j] / T(3);
+    A[1][0] += val * niy * nx[j] / T(3);
+    A[1][1] += val * (nix * nx[j] + T(4. / 3.) * niy * ny[j]);
+    val = T(1) / (T(6) * rho);
+    val += tau_su / (T(4) * rho * volume) * u_ni;
+    A[0][2] += nx[j] * val; A[1][2] += ny[j] * val;
+    const T laplacian = T(1) / (T(4) * rho * volume) * (nix * nx[j] + niy * ny[j]);
+    A[2][2] += tau_ps * laplacian;
+    val = T(1. / 6.);
+    A[2][0] += val * nx[j]; A[2][1] += val * ny[j];
+    val = tau_bulk / (T(4) * volume);
+    A[0][0] += val * nix * nx[j]; A[0][1] += val * nix * ny[j];
+    A[1][0] += val * niy * nx[j]; A[1][1] += val * niy * ny[j];
+    val = volume / T(12) * (T(1) + (ai == j ? T(1) : T(0)));
+    val += tau_su / T(6) * u_ni;
+    Tm[0][0] += val; Tm[1][1] += val;
+    val = tau_ps / T(6);
+    Tm[2][0] += val * nix; Tm[2][1] += val * niy;
+    T xb[3];
+    load_state<2, T>(state, ids[j], xb);
+    stage_block<2, T>(A, Tm, xb, kp, rhs, st, j, CH);
+  }
+#pragma unroll
+  for (int r = 0; r < 3; ++r) rst[r * CH] = rhs[r];
+}
+
+// Specialised tetrahedra, NavierStokesSpecializations.hpp:150-302, row i = a,
+// including the reference's use of vk in the W rows (:224-226, :236-238).
+template <typename T>
+__device__ __forceinline__ void spec_tet_row(const int (&ids)[4], int ai, const double* __restrict__ coords,
+                                             const double* __restrict__ uadv, const double* __restrict__ state,
+                                             const KParams<T>& kp, T* __restrict__ st, T* __restrict__ rst, int CH) {
+  Elem<3, T> el;
+  gather_geometry_uadv<3, T>(ids, coords, uadv, el);
+  T u_avg[3];
+#pragma unroll
+  for (int k = 0; k < 3; ++k) {
+    T s = 0;
+#pragma unroll
+    for (int b = 0; b < 4; ++b) s += el.U[b][k];
+    u_avg[k] = s / T(4);
+  }
+  const auto& X = el.Xr;
+  T J[3][3], Ji[3][3], det;
+#pragma unroll
+  for (int r = 0; r < 3; ++r)
+#pragma unroll
+    for (int c = 0; c < 3; ++c) J[r][c] = X[r + 1][c];
+  inverse_det<T>(J, Ji, det);
+  const T volume = det / T(6);
+  const T fc = T(0.5);
+  T nsum = 0;
+#pragma unroll
+  for (int b = 0; b < 4; ++b) nsum += el.NU[b];
+  const T nu = tabs(nsum / T(4));
+  T nr[4][3];
+  const int XX = 0, YY = 1, ZZ = 2;
+  nr[0][XX] = ((X[3][YY]-X[1][YY])*(X[2][ZZ]-X[1][ZZ]) - (X[2][YY]-X[1][YY])*(X[3][ZZ]-X[1][ZZ])) / T(2);
+  nr[0][YY] = ((X[3][ZZ]-X[1][ZZ])*(X[2][XX]-X[1][XX]) - (X[2][ZZ]-X[1][ZZ])*(X[3][XX]-X[1][XX])) / T(2);
+  nr[0][ZZ] = ((X[3][XX]-X[1][XX])*(X[2][YY]-X[1][YY]) - (X[2][XX]-X[1][XX])*(X[3][YY]-X[1][YY])) / T(2);
+  nr[1][XX] = ((X[2][YY]-X[0][YY])*(X[3][ZZ]-X[0][ZZ]) - (X[3][YY]-X[0][YY])*(X[2][ZZ]-X[0][ZZ])) / T(2);
+  nr[1][YY] = ((X[2][ZZ]-X[0][ZZ])*(X[3][XX]-X[0][XX]) - (X[3][ZZ]-X[0][ZZ])*(X[2][XX]-X[0][XX])) / T(2);
+  nr[1][ZZ] = ((X[2][XX]-X[0][XX])*(X[3][YY]-X[0][YY]) - (X[3][XX]-X[0][XX])*(X[2][YY]-X[0][YY])) / T(2);
+  nr[2][XX] = ((X[3][YY]-X[0][YY])*(X[1][ZZ]-X[0][ZZ]) - (X[1][YY]-X[0][YY])*(X[3][ZZ]-X[0][ZZ])) / T(2);
+  nr[2][YY] = ((X[3][ZZ]-X[0][ZZ])*(X[1][XX]-X[0][XX]) - (X[1][ZZ]-X[0][ZZ])*(X[3][XX]-X[0][XX])) / T(2);
+  nr[2][ZZ] = ((X[3][XX]-X[0][XX])*(X[1][YY]-X[0][YY]) - (X[1][XX]-X[0][XX])*(X[3][YY]-X[0][YY])) / T(2);
+  nr[3][XX] = ((X[1][YY]-X[0][YY])*(X[2][ZZ]-X[0][ZZ]) - (X[2][YY]-X[0][YY])*(X[1][ZZ]-X[0][ZZ])) / T(2);
+  nr[3][YY] = ((X[1][ZZ]-X[0][ZZ])*(X[2][XX]-X[0][XX]) - (X[2][ZZ]-X[0][ZZ])*(X[1][XX]-X[0][XX])) / T(2);
+  nr[3][ZZ] = ((X[1][XX]-X[0][XX])*(X[2][YY]-X[0][YY]) - (X[2][XX]-X[0][XX])*(X[1][YY]-X[0][YY])) / T(2);
+  T tau_ps, tau_su, tau_bulk;
+  spec_tau_common<3, T>(el, state, ids, nu, kp.dt, tau_ps, tau_su, tau_bulk);
+  T ni[3];
+#pragma unroll
+  for (int k = 0; k < 3; ++k) {
+    T col[4] = {nr[0][k], nr[1][k], nr[2][k], nr[3][k]};
+    ni[k] = sel<4>(col, ai);
+  }
+  const T u_ni = u_avg[XX] * ni[XX] + u_avg[YY] * ni[YY] + u_avg[ZZ] * ni[ZZ];
+  const T rho = kp.rho;
+  T rhs[4] = {0, 0, 0, 0};
+  // local rows/cols: 0 = U, 1 = V, 2 = W, 3 = P
+#pragma unroll
+  for (int j = 0; j < 4; ++j) {
+    T A[4][4], Tm[4][4];
+#pragma unroll
+    for (int r = 0; r < 4; ++r)
+#pragma unroll
+      for (int c = 0; c < 4; ++c) { A[r][c] = 0; Tm[r][c] = 0; }
+    const T uk = u_avg[XX], vk = u_avg[YY], wk = u_avg[ZZ];
+    const T* nj = nr[j];
+    const T uknj = uk * nj[XX] + vk * nj[YY] + wk * nj[ZZ];
+    T val = T(1. / 12.) * uknj;
+    val += tau_su / (T(9) * volume) * uknj * u_ni;
+    A[0][0] += val; A[1][1] += val; A[2][2] += val;
+    val = tau_ps / (T(9) * volume) * uknj;
+    A[3][0] += val * ni[XX]; A[3][1] += val * ni[YY]; A[3][2] += val * ni[ZZ];
+    val = fc / T(12);
+    val += fc * tau_su / (T(9) * volume) * u_ni;
+    A[0][0] += val * uk * nj[XX]; A[0][1] += val * uk * nj[YY]; A[0][2] += val * uk * nj[ZZ];
+    A[1][0] += val * vk * nj[XX]; A[1][1] += val * vk * nj[YY]; A[1][2] += val * vk * nj[ZZ];
+    A[2][0] += val * vk * nj[XX]; A[2][1] += val * vk * nj[YY]; A[2][2] += val * vk * nj[ZZ];
+    val = fc * tau_ps / (T(9) * volume);
+    A[3][0] += val * ni[XX] * uk * nj[XX]; A[3][1] += val * ni[XX] * uk * nj[YY];
+    A[3][2] += val * ni[XX] * uk * nj[ZZ]; A[3][0] += val * ni[YY] * vk * nj[XX];
+    A[3][1] += val * ni[YY] * vk * nj[YY]; A[3][2] += val * ni[YY] * vk * nj[ZZ];
+    A[3][0] += val * ni[ZZ] * vk * nj[XX]; A[3][1] += val * ni[ZZ] * vk * nj[YY];
+    A[3][2] += val * ni[ZZ] * vk * nj[ZZ];
+    val = nu / (T(9) * volume);
+    A[0][0] += val * (T(4. / 3.) * ni[XX] * nj[XX] + ni[YY] * nj[YY] + ni[ZZ] * nj[ZZ]);
+    A[0][1] += val * ni[XX] * nj[YY] / T(3);
+    A[0][2] += val * ni[XX] * nj[ZZ] / T(3);
+    A[1][0] += val * ni[YY] * nj[XX] / T(3);
+    A[1][1] += val * (ni[XX] * nj[XX] + T(4. / 3.) * ni[YY] * nj[YY] + ni[ZZ] * nj[ZZ]);
+    A[1][2] += val * ni[YY] * nj[ZZ] / T(3);
+    A[2][0] += val * ni[ZZ] * nj[XX] / T(3);
+    A[2][1] += val * ni[ZZ] * nj[YY] / T(3);
+    A[2][2] += val * (ni[XX] * nj[XX] + ni[YY] * nj[YY] + T(4. / 3.) * ni[ZZ] * nj[ZZ]);
+    val = T(1) / (T(12) * rho);
+    val += tau_su / (T(9) * rho * volume) * u_ni;
+    A[0][3] += nj[XX] * val; A[1][3] += nj[YY] * val; A[2][3] += nj[ZZ] * val;
+    val = tau_ps / (T(9) * rho * volume) * (ni[XX] * nj[XX] + ni[YY] * nj[YY] + ni[ZZ] * nj[ZZ]);
+    A[3][3] += val;
+    val = T(1. / 12.);
+    A[3][0] += val * nj[XX]; A[3][1] += val * nj[YY]; A[3][2] += val * nj[ZZ];
+    val = tau_bulk / (T(9) * volume);
+    A[0][0] += val * ni[XX] * nj[XX]; A[0][1] += val * ni[XX] * nj[YY];
+    A[0][2] += val * ni[XX] * nj[ZZ]; A[1][0] += val * ni[YY] * nj[XX];
+    A[1][1] += val * ni[YY] * nj[YY]; A[1][2] += val * ni[YY] * nj[ZZ];
+    A[2][0] += val * ni[ZZ] * nj[XX]; A[2][1] += val * ni[ZZ] * nj[YY];
+    A[2][2] += val * ni[ZZ] * nj[ZZ];
+    val = volume / T(20) * (T(1) + (ai == j ? T(1) : T(0)));
+    val += tau_su / T(12) * u_ni;
+    Tm[0][0] += val; Tm[1][1] += val; Tm[2][2] += val;
+    val = tau_ps / T(12);
+    Tm[3][0] += val * ni[XX]; Tm[3][1] += val * ni[YY]; Tm[3][2] += val * ni[ZZ];
+    T xb[4];
+    load_state<3, T>(state, ids[j], xb);
+    stage_block<3, T>(A, Tm, xb, kp, rhs, st, j, CH);
+  }
+#pragma unroll
+  for (int r = 0; r < 4; ++r) rst[r * CH] = rhs[r];
+}
+
+template <int D, typename T, int CH>
+constexpr size_t assembly_smem_bytes() {
+  return size_t(P1<D>::nvals + P1<D>::neq) * CH * sizeof(T) + size_t(CH) * 4 + size_t(3 * CH + 2) * 4;
+}
+
+// The row-owner assembly kernel.  One CTA per chunk of whole block rows.
+template <int D, typename T, int CH, bool SPEC>
+__global__ void __launch_bounds__(CH) ns_assembly_kernel(
+    const int32_t* __restrict__ chunk_row0, const int32_t* __restrict__ row_inc,
+    const int32_t* __restrict__ inc_elem, const uint32_t* __restrict__ inc_info, const int4* __restrict__ conn,
+    const double* __restrict__ coords, const double* __restrict__ uadv, const double* __restrict__ state,
+    const double* __restrict__ force, const int64_t* __restrict__ start, NSParams p, double* __restrict__ vals,
+    float* __restrict__ vals32, double* __restrict__ rhs) {
+  constexpr int neq = P1<D>::neq, nvals = P1<D>::nvals;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  T* st = reinterpret_cast<T*>(smem_raw);
+  T* rst = st + nvals * CH;
+  uint32_t* s_info = reinterpret_cast<uint32_t*>(rst + neq * CH);
+  int* s_rowinc = reinterpret_cast<int*>(s_info + CH);  // CH + 1
+  int* s_pref = s_rowinc + CH + 1;                      // CH + 1
+  int* s_slots = s_pref + CH + 1;                       // CH
+
+  const int chunk = blockIdx.x;
+  const int row0 = chunk_row0[chunk], row1 = chunk_row0[chunk + 1];
+  const int R = row1 - row0;
+  const int inc0 = row_inc[row0];
+  const int K = row_inc[row1] - inc0;
+  const int t = threadIdx.x;
+
+  // Phase 1: element row blocks
+  if (t < K) {
+    const int k = inc0 + t;
+    const int e = __ldg(inc_elem + k);
+    const uint32_t info = __ldg(inc_info + k);
+    s_info[t] = info;
+    const int a = int(info >> 24) & 3;
+    const int4 cn = __ldg(conn + e);
+    const int ids[4] = {cn.x, cn.y, cn.z, cn.w};
+    const KParams<T> kp = make_kparams<T>(p);
+    if constexpr (SPEC) {
+      if constexpr (D == 2) spec_tri_row<T>(ids, a, coords, uadv, state, kp, st + t, rst + t, CH);
+      else spec_tet_row<T>(ids, a, coords, uadv, state, kp, st + t, rst + t, CH);
+    } else {
+      generic_row<D, T>(ids, a, coords, uadv, state, force, kp, st + t, rst + t, CH);
+    }
+  }
+  for (int rl = t; rl <= R; rl += CH) s_rowinc[rl] = row_inc[row0 + rl] - inc0;
+  for (int rl = t; rl < R; rl += CH) s_slots[rl] = int(start[row0 + rl + 1] - start[row0 + rl]);
+  __syncthreads();
+  if (t == 0) {
+    int acc = 0;
+    s_pref[0] = 0;
+    for (int rl = 0; rl < R; ++rl) {
+      acc += s_slots[rl] * neq;
+      s_pref[rl + 1] = acc;
+    }
+  }
+  __syncthreads();
+
+  // Phase 2a: CSR values, one thread per (row, equation, neighbour slot)
+  const int nitems = s_pref[R];
+  for (int it = t; it < nitems; it += CH) {
+    int lo = 0, hi = R - 1;
+    while (lo < hi) {  // last rl with s_pref[rl] <= it
+      const int mid = (lo + hi + 1) >> 1;
+      if (s_pref[mid] <= it) lo = mid; else hi = mid - 1;
+    }
+    const int rl = lo;
+    const int S = s_slots[rl];
+    const int local = it - s_pref[rl];
+    const int r = local / S;
+    const int s = local - r * S;
+    const int kb = s_rowinc[rl], ke = s_rowinc[rl + 1];
+    double acc[neq];
+#pragma unroll
+    for (int c = 0; c < neq; ++c) acc[c] = 0.0;
+    for (int kk = kb; kk < ke; ++kk) {
+      const uint32_t info = s_info[kk];
+#pragma unroll
+      for (int b = 0; b < P1<D>::n; ++b) {
+        if (((info >> (6 * b)) & 63u) == uint32_t(s)) {
+#pragma unroll
+          for (int c = 0; c < neq; ++c) acc[c] += double(st[((b * neq + r) * neq + c) * CH + kk]);
+        }
+      }
+    }
+    const int64_t node = row0 + rl;
+    const int64_t base = int64_t(neq) * neq * start[node] + int64_t(r * S + s) * neq;
+#pragma unroll
+    for (int c = 0; c < neq; ++c) vals[base + c] = acc[c];
+    if (vals32 != nullptr) {
+#pragma unroll
+      for (int c = 0; c < neq; ++c) vals32[base + c] = float(acc[c]);
+    }
+  }
+  // Phase 2b: RHS, one thread per (row, equation)
+  for (int it = t; it < R * neq; it += CH) {
+    const int rl = it / neq, r = it - rl * neq;
+    const int kb = s_rowinc[rl], ke = s_rowinc[rl + 1];
+    double acc = 0.0;
+    for (int kk = kb; kk < ke; ++kk) acc += double(rst[r * CH + kk]);
+    rhs[int64_t(row0 + rl) * neq + r] = acc;
+  }
+}
+
+// LinearizeU (NavierStokes.cpp:105), evaluated left to right without FMA
+// contraction: u_adv = ((2.1875u - 2.1875u1) + 1.3125u2) - 0.3125u3.  Also
+// copies nu_eff into the node record read by the assembly.
+__global__ void linearize_kernel(int64_t N, int dim, const double* __restrict__ state,
+                                 const double* __restrict__ u1, const double* __restrict__ u2,
+                                 const double* __restrict__ u3, const double* __restrict__ nu,
+                                 double* __restrict__ uadv) {
+  const int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (i >= N) return;
+  double out[4] = {0, 0, 0, 0};
+  for (int k = 0; k < dim; ++k) {
+    const int64_t o = 4 * i + k;
+    double v = __dsub_rn(__dmul_rn(2.1875, state[o]), __dmul_rn(2.1875, u1[o]));
+    v = __dadd_rn(v, __dmul_rn(1.3125, u2[o]));
+    v = __dsub_rn(v, __dmul_rn(0.3125, u3[o]));
+    out[k] = v;
+  }
+  out[3] = nu[i];
+  reinterpret_cast<double2*>(uadv + 4 * i)[0] = make_double2(out[0], out[1]);
+  reinterpret_cast<double2*>(uadv + 4 * i)[1] = make_double2(out[2], out[3]);
+}
+
+// UpdateActions (NavierStokes.cpp:172-179): u3=u2, u2=u1, u1=u, u+=du, p+=dp.
+__global__ void update_kernel(int64_t N, int dim, double* __restrict__ state, double* __restrict__ u1,
+                              double* __restrict__ u2, double* __restrict__ u3, const double* __restrict__ sol) {
+  const int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (i >= N) return;
+  const int neq = dim + 1;
+  for (int k = 0; k < dim; ++k) {
+    const int64_t o = 4 * i + k;
+    u3[o] = u2[o];
+    u2[o] = u1[o];
+    const double u = state[o];
+    u1[o] = u;
+    state[o] = __dadd_rn(u, sol[i * neq + k]);
+  }
+  state[4 * i + dim] = __dadd_rn(state[4 * i + dim], sol[i * neq + dim]);
+}
+
+// Point CSR from the node graph: row node*neq + r, columns adj*neq + c.
+__global__ void build_csr_kernel(int64_t N, int neq, const int64_t* __restrict__ start,
+                                 const int32_t* __restrict__ adj, int64_t* __restrict__ rowptr,
+                                 int32_t* __restrict__ colidx, int64_t* __restrict__ diagpos) {
+  const int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (i >= N) return;
+  const int64_t s0 = start[i];
+  const int S = int(start[i + 1] - s0);
+  const int64_t base = int64_t(neq) * neq * s0;
+  int self = 0;
+  for (int s = 0; s < S; ++s)
+    if (adj[s0 + s] == i) self = s;
+  for (int r = 0; r < neq; ++r) {
+    const int64_t rb = base + int64_t(r) * S * neq;
+    rowptr[i * neq + r] = rb;
+    diagpos[i * neq + r] = rb + int64_t(self) * neq + r;
+    for (int s = 0; s < S; ++s) {
+      const int32_t cn = adj[s0 + s] * neq;
+      for (int c = 0; c < neq; ++c) colidx[rb + int64_t(s) * neq + c] = cn + c;
+    }
+  }
+  if (i == N - 1) rowptr[N * neq] = int64_t(neq) * neq * start[N];
+}
+
+// Symmetric Dirichlet, part 1: per-step values v = value - old for the first
+// and last application of every constrained dof.
+__global__ void dirichlet_values_kernel(int64_t nbc, int neq, const int64_t* __restrict__ bc_dof,
+                                        const double* __restrict__ first, const double* __restrict__ state,
+                                        double* __restrict__ vfirst) {
+  const int64_t u = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (u >= nbc) return;
+  const int64_t dof = bc_dof[u];
+  const int64_t node = dof / neq;
+  const int comp = int(dof - node * neq);
+  vfirst[u] = __dsub_rn(first[u], state[4 * node + comp]);
+}
+
+// Part 2: rows that are not constrained move their constrained columns to the
+// RHS in first-application order (the order of the sequential reference).
+__global__ void dirichlet_columns_kernel(int64_t nrows, const int64_t* __restrict__ fix_row,
+                                         const int64_t* __restrict__ fix_ptr, const int64_t* __restrict__ fix_pos,
+                                         const int32_t* __restrict__ fix_bc, const double* __restrict__ vfirst,
+                                         double* __restrict__ vals, float* __restrict__ vals32,
+                                         double* __restrict__ rhs) {
+  const int64_t q = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (q >= nrows) return;
+  const int64_t row = fix_row[q];
+  double r = rhs[row];
+  for (int64_t k = fix_ptr[q]; k < fix_ptr[q + 1]; ++k) {
+    const int64_t pos = fix_pos[k];
+    r = __dadd_rn(r, __dmul_rn(-vals[pos], vfirst[fix_bc[k]]));  // no FMA: same rounding as the sequential form
+    vals[pos] = 0.0;
+    if (vals32) vals32[pos] = 0.0f;
+  }
+  rhs[row] = r;
+}
+
+// Part 3: constrained rows become identity rows; rhs = sol = last value - old.
+__global__ void dirichlet_rows_kernel(int64_t nbc, int neq, const int64_t* __restrict__ bc_dof,
+                                      const double* __restrict__ last, const int64_t* __restrict__ bc_diag,
+                                      const int64_t* __restrict__ rowptr, const double* __restrict__ state,
+                                      double* __restrict__ vals, float* __restrict__ vals32,
+                                      double* __restrict__ rhs, double* __restrict__ sol) {
+  const int64_t u = blockIdx.x;
+  if (u >= nbc) return;
+  const int64_t dof = bc_dof[u];
+  for (int64_t p = rowptr[dof] + threadIdx.x; p < rowptr[dof + 1]; p += blockDim.x) {
+    vals[p] = 0.0;
+    if (vals32) vals32[p] = 0.0f;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    vals[bc_diag[u]] = 1.0;
+    if (vals32) vals32[bc_diag[u]] = 1.0f;
+    const int64_t node = dof / neq;
+    const int comp = int(dof - node * neq);
+    const double v = __dsub_rn(last[u], state[4 * node + comp]);
+    rhs[dof] = v;
+    sol[dof] = v;
+  }
+}
+
+template <int D, typename T, int CH, bool SPEC>
+int launch_assembly_t(ufem_ns_handle* h, cudaStream_t s, bool write32) {
+  NSParams p;
+  p.theta = h->opt.theta; p.dt = h->opt.dt; p.invdt = 1.0 / h->opt.dt; p.rho = h->opt.rho;
+  p.c1 = h->opt.c1; p.c2 = h->opt.c2; p.a_ps = h->opt.alpha_ps; p.a_su = h->opt.alpha_su;
+  p.a_bu = h->opt.alpha_bu; p.u_ref = h->opt.u_ref; p.supg_type = h->opt.supg_type;
+  p.has_force = h->d_force != nullptr;
+  constexpr size_t smem = assembly_smem_bytes<D, T, CH>();
+  const AssemblyPlan& plan = std::is_same<T, float>::value ? h->plan32 : h->plan64;
+  if (plan.cap != CH) return set_error(UFEM_ERR_STATE, "assembly plan does not match the kernel width");
+  ns_assembly_kernel<D, T, CH, SPEC><<<plan.nchunks, CH, smem, s>>>(
+      plan.chunk_row0, h->d_row_inc, h->d_inc_elem, h->d_inc_info, reinterpret_cast<const int4*>(h->d_conn),
+      h->d_coords, h->d_uadv, h->d_state, h->d_force, h->d_start, p, h->d_vals, write32 ? h->d_vals32 : nullptr,
+      h->d_rhs);
+  UFEM_CUDA_TRY(cudaGetLastError());
+  return UFEM_OK;
+}
+
+template <int D, typename T, int CH, bool SPEC>
+int set_smem_attr() {
+  constexpr size_t smem = assembly_smem_bytes<D, T, CH>();
+  UFEM_CUDA_TRY(cudaFuncSetAttribute(ns_assembly_kernel<D, T, CH, SPEC>,
+                                     cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
+  return UFEM_OK;
+}
+
+constexpr int kChunk2D = 256;
+constexpr int kChunk3D64 = 128;
+constexpr int kChunk3D32 = 256;
+
+}  // namespace
+
+int assembly_chunk_capacity(int dim, int precision) {
+  if (dim == 2) return kChunk2D;
+  return precision == 1 ? kChunk3D32 : kChunk3D64;
+}
+
+int configure_kernels() {
+  static bool done = false;
+  if (done) return UFEM_OK;
+  int rc;
+  if ((rc = set_smem_attr<2, double, kChunk2D, false>())) return rc;
+  if ((rc = set_smem_attr<2, double, kChunk2D, true>())) return rc;
+  if ((rc = set_smem_attr<2, float, kChunk2D, false>())) return rc;
+  if ((rc = set_smem_attr<2, float, kChunk2D, true>())) return rc;
+  if ((rc = set_smem_attr<3, double, kChunk3D64, false>())) return rc;
+  if ((rc = set_smem_attr<3, double, kChunk3D64, true>())) return rc;
+  if ((rc = set_smem_attr<3, float, kChunk3D32, false>())) return rc;
+  if ((rc = set_smem_attr<3, float, kChunk3D32, true>())) return rc;
+  done = true;
+  return UFEM_OK;
+}
+
+int launch_assembly(ufem_ns_handle* h, cudaStream_t s, bool write32) {
+  const bool spec = h->opt.use_specializations != 0;
+  const bool f32 = h->opt.precision == 1;
+  if (h->dim == 2) {
+    if (f32) return spec ? launch_assembly_t<2, float, kChunk2D, true>(h, s, write32)
+                         : launch_assembly_t<2, float, kChunk2D, false>(h, s, write32);
+    return spec ? launch_assembly_t<2, double, kChunk2D, true>(h, s, write32)
+                : launch_assembly_t<2, double, kChunk2D, false>(h, s, write32);
+  }
+  if (f32) return spec ? launch_assembly_t<3, float, kChunk3D32, true>(h, s, write32)
+                       : launch_assembly_t<3, float, kChunk3D32, false>(h, s, write32);
+  return spec ? launch_assembly_t<3, double, kChunk3D64, true>(h, s, write32)
+              : launch_assembly_t<3, double, kChunk3D64, false>(h, s, write32);
+}
+
+int launch_linearize(ufem_ns_handle* h, cudaStream_t s) {
+  const int64_t N = h->N;
+  const double* u1 = h->d_hist;
+  const double* u2 = h->d_hist + 4 * N;
+  const double* u3 = h->d_hist + 8 * N;
+  linearize_kernel<<<unsigned((N + 255) / 256), 256, 0, s>>>(N, h->dim, h->d_state, u1, u2, u3, h->d_nu, h->d_uadv);
+  UFEM_CUDA_TRY(cudaGetLastError());
+  return UFEM_OK;
+}
+
+int launch_update(ufem_ns_handle* h, cudaStream_t s) {
+  const int64_t N = h->N;
+  update_kernel<<<unsigned((N + 255) / 256), 256, 0, s>>>(N, h->dim, h->d_state, h->d_hist, h->d_hist + 4 * N,
+                                                        h->d_hist + 8 * N, h->d_sol);
+  UFEM_CUDA_TRY(cudaGetLastError());
+  return UFEM_OK;
+}
+
+int launch_build_csr(ufem_ns_handle* h, cudaStream_t s) {
+  const int64_t N = h->N;
+  build_csr_kernel<<<unsigned((N + 127) / 128), 128, 0, s>>>(N, h->neq, h->d_start, h->d_adj, h->d_rowptr,
+                                                           h->d_colidx, h->d_diagpos);
+  UFEM_CUDA_TRY(cudaGetLastError());
+  return UFEM_OK;
+}
+
+int launch_dirichlet(ufem_ns_handle* h, cudaStream_t s) {
+  const DirichletPlan& bp = h->bcp;
+  if (bp.nbc == 0) return UFEM_OK;
+  dirichlet_values_kernel<<<unsigned((bp.nbc + 255) / 256), 256, 0, s>>>(bp.nbc, h->neq, bp.bc_dof, bp.bc_first,
+                                                                         h->d_state, bp.vfirst);
+  UFEM_CUDA_TRY(cudaGetLastError());
+  if (bp.nfix_rows > 0) {
+    dirichlet_columns_kernel<<<unsigned((bp.nfix_rows + 127) / 128), 128, 0, s>>>(
+        bp.nfix_rows, bp.fix_row, bp.fix_ptr, bp.fix_pos, bp.fix_bc, bp.vfirst, h->d_vals, h->d_vals32, h->d_rhs);
+    UFEM_CUDA_TRY(cudaGetLastError());
+  }
+  dirichlet_rows_kernel<<<unsigned(bp.nbc), 64, 0, s>>>(bp.nbc, h->neq, bp.bc_dof, bp.bc_last, bp.bc_diag,
+                                                        h->d_rowptr, h->d_state, h->d_vals, h->d_vals32, h->d_rhs,
+                                                        h->d_sol);
+  UFEM_CUDA_TRY(cudaGetLastError());
+  return UFEM_OK;
+}
+
+}  // namespace ufem

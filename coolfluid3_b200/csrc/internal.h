@@ -1,0 +1,136 @@
+// internal.h -- shared declarations of the B200 UFEM library (not part of the ABI).
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <string>
+#include <vector>
+
+#include "../../include/ufem_b200.h"
+
+namespace ufem {
+
+// ---------------------------------------------------------------------------
+// Error reporting across the C ABI: a thread-local message plus a code.
+// ---------------------------------------------------------------------------
+int set_error(int code, const std::string& msg);
+
+#define UFEM_CUDA_TRY(expr)                                                              \
+  do {                                                                                   \
+    cudaError_t _e = (expr);                                                             \
+    if (_e != cudaSuccess)                                                               \
+      return ::ufem::set_error(UFEM_ERR_CUDA, std::string(#expr) + ": " + cudaGetErrorString(_e)); \
+  } while (0)
+
+// Scalar parameters of the element expression, passed to kernels by value.
+struct NSParams {
+  double theta, dt, invdt, rho;
+  double c1, c2, a_ps, a_su, a_bu, u_ref;
+  int supg_type;
+  int has_force;
+};
+
+// Row-owner assembly plan: CSR block rows are grouped into chunks of whole rows
+// whose incidences (row node, element) fit one CTA.  Incidences are sorted by
+// (row node, element id), so each CSR entry is summed in element order.
+struct AssemblyPlan {
+  int cap = 0;                 // incidences per chunk (== CTA threads)
+  int nchunks = 0;
+  int32_t* chunk_row0 = nullptr;  // nchunks + 1 (device)
+};
+
+// Symmetric-Dirichlet plan (sequential semantics of TrilinosFEVbrMatrix::
+// symmetric_dirichlet reduced to an order-preserving parallel form).
+struct DirichletPlan {
+  int64_t nbc = 0;             // unique (node, comp) dofs
+  int64_t nfix_rows = 0;       // non-BC rows holding BC columns
+  int64_t nfix = 0;            // entries moved to the RHS
+  int64_t* bc_dof = nullptr;   // nbc
+  double* bc_first = nullptr;  // value of the first application (moves columns)
+  double* bc_last = nullptr;   // value of the last application (sets row/rhs/sol)
+  int64_t* bc_diag = nullptr;  // CSR position of the diagonal of each BC row
+  int64_t* fix_row = nullptr;  // nfix_rows
+  int64_t* fix_ptr = nullptr;  // nfix_rows + 1
+  int64_t* fix_pos = nullptr;  // nfix CSR positions, per row in first-application order
+  int32_t* fix_bc = nullptr;   // nfix index into bc arrays
+  double* vfirst = nullptr;    // per step: bc_first - old
+  bool dirty = true;
+};
+
+struct KrylovWork;
+
+}  // namespace ufem
+
+struct ufem_ns_handle {
+  int dim = 0, nn = 0, neq = 0;
+  int64_t N = 0, E = 0;
+  int64_t nrows = 0, nnz = 0, bnnz = 0;
+  ufem_ns_options opt{};
+  bool state_set = false;
+
+  // host copies used by planning
+  std::vector<int64_t> start_h;   // N+1
+  std::vector<int32_t> adj_h;     // bnnz
+  struct BCEntry { uint32_t node; int comp; double value; };
+  std::vector<BCEntry> bcs;
+
+  // device mesh and fields (node records padded to 4 doubles)
+  double* d_coords = nullptr;   // N x 4 (x, y, [z], 0)
+  int32_t* d_conn = nullptr;    // E x 4 (triangles padded with node 0)
+  double* d_state = nullptr;    // N x 4 (u, v, [w], p) : p at index dim
+  double* d_hist = nullptr;     // 3 x N x 4 (u1, u2, u3)
+  double* d_uadv = nullptr;     // N x 4 (u_adv xyz, nu at index 3)
+  double* d_nu = nullptr;       // N
+  double* d_force = nullptr;    // N x 4 or null
+
+  // graph + CSR
+  int64_t* d_start = nullptr;   // N+1
+  int32_t* d_adj = nullptr;     // bnnz
+  int64_t* d_rowptr = nullptr;  // nrows+1
+  int32_t* d_colidx = nullptr;  // nnz
+  double* d_vals = nullptr;     // nnz
+  float* d_vals32 = nullptr;    // nnz (allocated when a mixed solve first runs)
+  double* d_rhs = nullptr;
+  double* d_sol = nullptr;
+  int64_t* d_diagpos = nullptr; // nrows
+
+  // row-owner incidences
+  int32_t* d_row_inc = nullptr;   // N+1
+  int32_t* d_inc_elem = nullptr;  // E*nn
+  uint32_t* d_inc_info = nullptr; // E*nn : 6-bit slots + local index << 24
+
+  ufem::AssemblyPlan plan64;       // chunks sized for the FP64-element kernel
+  ufem::AssemblyPlan plan32;       // chunks sized for the FP32-element kernel
+  ufem::DirichletPlan bcp;
+  ufem::KrylovWork* kw = nullptr;
+  bool vals32_valid = false;      // d_vals32 holds the current system (written by the assembly)
+
+  // transfer staging (reference field layouts <-> padded node records)
+  double* d_stage = nullptr;      // N x 4*dim doubles
+  double* d_x = nullptr;          // apply() operands
+  double* d_y = nullptr;
+
+  // timing: event pairs (start, stop) for linearize, assembly, dirichlet, solve, update
+  bool timing = false;
+  cudaEvent_t ev[10] = {};
+  bool ev_rec[5] = {};
+};
+
+namespace ufem {
+
+// kernels (assembly.cu)
+int launch_build_csr(ufem_ns_handle* h, cudaStream_t s);
+int launch_linearize(ufem_ns_handle* h, cudaStream_t s);
+int launch_assembly(ufem_ns_handle* h, cudaStream_t s, bool write32);
+int launch_dirichlet(ufem_ns_handle* h, cudaStream_t s);
+int launch_update(ufem_ns_handle* h, cudaStream_t s);
+int assembly_chunk_capacity(int dim, int precision);
+int configure_kernels();
+
+// Krylov (krylov.cu)
+int krylov_solve(ufem_ns_handle* h, const ufem_krylov_opts* ko, ufem_krylov_status* st, cudaStream_t s);
+int krylov_apply(ufem_ns_handle* h, const double* d_x, double* d_y, cudaStream_t s);
+void krylov_free(ufem_ns_handle* h);
+
+}  // namespace ufem

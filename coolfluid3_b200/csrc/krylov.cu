@@ -1,0 +1,861 @@
+// krylov.cu -- SolveLSS replacement: restarted GMRES and BiCGStab with a Jacobi
+// preconditioner on the assembled point CSR, plus FP64 iterative refinement
+// around an FP32 inner solve.
+//
+// The reference solves with Belos block GMRES + Ifpack ILU through Stratimikos
+// (TrilinosStratimikosStrategy.cpp:135-177, BelosGMRESParameters.cpp:28-41).
+// Here the SpMV walks the node graph (one warp per block row), dot products and
+// norms are reduced in FP64 in a fixed order (deterministic, no atomics), and the
+// Krylov scalars (Hessenberg, Givens rotations, BiCGStab alpha/omega, the
+// convergence test) live on the device, so whole stretches of iterations are
+// enqueued without a host round trip.  Kernels read a device "done" flag and
+// return at once after convergence.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdint>
+#include <type_traits>
+#include <vector>
+
+#include "internal.h"
+
+namespace ufem {
+
+struct KrylovWork {
+  int64_t n = 0;
+  int m = 0;
+  int nblk = 0;
+  // FP64 vectors
+  double *V = nullptr, *w = nullptr, *z = nullptr, *t = nullptr, *r = nullptr, *dinv = nullptr;
+  // FP32 vectors for the inner solve of the mixed path
+  float *V32 = nullptr, *w32 = nullptr, *z32 = nullptr, *t32 = nullptr, *r32 = nullptr, *x32 = nullptr,
+        *q32 = nullptr, *dinv32 = nullptr;
+  // BiCGStab vectors
+  double *bp = nullptr, *bv = nullptr, *bs = nullptr, *bt = nullptr, *brh = nullptr, *bph = nullptr, *bsh = nullptr;
+  float *bp32 = nullptr, *bv32 = nullptr, *bs32 = nullptr, *bt32 = nullptr, *brh32 = nullptr, *bph32 = nullptr,
+        *bsh32 = nullptr;
+  // reductions and solver scalars (device)
+  double* part = nullptr;  // (m+2) x nblk
+  double* hbuf = nullptr;  // 2 x (m+2)
+  double* H = nullptr;     // (m+1) x m
+  double *cs = nullptr, *sn = nullptr, *g = nullptr, *y = nullptr;
+  double* dctl = nullptr;  // scalars, see kD* below
+  int* ictl = nullptr;     // [0]=done [1]=jcount [2]=status [3]=iterations (BiCGStab)
+  double* h_dctl = nullptr;  // pinned mirrors
+  int* h_ictl = nullptr;
+};
+
+namespace {
+
+// dctl slots
+constexpr int kBnorm = 0, kBeta = 1, kEst = 2, kHnext = 3, kTrue = 4;
+constexpr int kRho = 5, kRhoOld = 6, kAlpha = 7, kOmega = 8, kRhV = 9, kTS = 10, kTT = 11, kR2 = 12, kScale = 13;
+constexpr int kRedThreads = 256;
+
+template <typename T>
+__device__ __forceinline__ T warp_sum(T v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+  return v;
+}
+
+// Deterministic block sum (fixed shuffle tree + fixed smem order); valid in thread 0.
+__device__ __forceinline__ double block_sum(double v, double* sm) {
+  v = warp_sum(v);
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  if (lane == 0) sm[wid] = v;
+  __syncthreads();
+  double s = 0.0;
+  if (threadIdx.x == 0)
+    for (int k = 0; k < int(blockDim.x >> 5); ++k) s += sm[k];
+  __syncthreads();
+  return s;
+}
+
+#define GRID_STRIDE(i, n) \
+  for (int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < (n); i += int64_t(gridDim.x) * blockDim.x)
+
+// y = A x on the node graph: one warp per block row (node), FEVbr point layout.
+template <typename VT, typename MT, typename AT>
+__global__ void spmv_kernel(int64_t N, int neq, const int64_t* __restrict__ start, const int32_t* __restrict__ adj,
+                            const MT* __restrict__ vals, const VT* __restrict__ x, VT* __restrict__ y,
+                            const int* __restrict__ done) {
+  if (done && *done) return;
+  const int64_t node = (int64_t(blockIdx.x) * blockDim.x + threadIdx.x) >> 5;
+  const int lane = threadIdx.x & 31;
+  if (node >= N) return;
+  const int64_t s0 = start[node];
+  const int S = int(start[node + 1] - s0);
+  const int64_t base = int64_t(neq) * neq * s0;
+  const int len = S * neq;
+  for (int r = 0; r < neq; ++r) {
+    AT acc = 0;
+    const MT* row = vals + base + int64_t(r) * len;
+    for (int idx = lane; idx < len; idx += 32) {
+      const int s = idx / neq;
+      const int c = idx - s * neq;
+      const int64_t col = int64_t(__ldg(adj + s0 + s)) * neq + c;
+      acc += AT(row[idx]) * AT(x[col]);
+    }
+    acc = warp_sum(acc);
+    if (lane == 0) y[node * neq + r] = VT(acc);
+  }
+}
+
+template <typename MT, typename VT>
+__global__ void jacobi_kernel(int64_t n, const int64_t* __restrict__ diagpos, const MT* __restrict__ vals,
+                              VT* __restrict__ dinv) {
+  GRID_STRIDE(i, n) {
+    const double d = double(vals[diagpos[i]]);
+    dinv[i] = VT(d != 0.0 ? 1.0 / d : 1.0);
+  }
+}
+
+// Node-block Jacobi: inverse of each neq x neq diagonal block (Gauss-Jordan with
+// partial pivoting), row-major per node.
+template <typename MT, typename VT>
+__global__ void block_jacobi_kernel(int64_t N, int neq, const int64_t* __restrict__ diagpos,
+                                    const MT* __restrict__ vals, VT* __restrict__ binv) {
+  GRID_STRIDE(i, N) {
+    double a[4][8];
+    for (int r = 0; r < neq; ++r) {
+      const int64_t d = diagpos[i * neq + r] - r;  // first column of the diagonal block in row r
+      for (int c = 0; c < neq; ++c) {
+        a[r][c] = double(vals[d + c]);
+        a[r][neq + c] = (r == c) ? 1.0 : 0.0;
+      }
+    }
+    for (int c = 0; c < neq; ++c) {
+      int piv = c;
+      for (int r = c + 1; r < neq; ++r)
+        if (fabs(a[r][c]) > fabs(a[piv][c])) piv = r;
+      if (piv != c)
+        for (int k = 0; k < 2 * neq; ++k) { const double tmp = a[c][k]; a[c][k] = a[piv][k]; a[piv][k] = tmp; }
+      const double p = a[c][c];
+      const double ip = (p != 0.0) ? 1.0 / p : 0.0;
+      for (int k = 0; k < 2 * neq; ++k) a[c][k] *= ip;
+      for (int r = 0; r < neq; ++r)
+        if (r != c) {
+          const double f = a[r][c];
+          for (int k = 0; k < 2 * neq; ++k) a[r][k] -= f * a[c][k];
+        }
+    }
+    for (int r = 0; r < neq; ++r)
+      for (int c = 0; c < neq; ++c) binv[(i * neq + r) * neq + c] = VT(a[r][neq + c]);
+  }
+}
+
+template <typename VT>
+__global__ void precond_kernel(int64_t n, int neq, int kind, const VT* __restrict__ dinv, const VT* __restrict__ v,
+                               VT* __restrict__ z, const int* __restrict__ done) {
+  if (done && *done) return;
+  GRID_STRIDE(i, n) {
+    if (kind == 0) {
+      z[i] = v[i];
+    } else if (kind == 1) {
+      z[i] = dinv[i] * v[i];
+    } else {
+      const int64_t node = i / neq;
+      const int r = int(i - node * neq);
+      double s = 0.0;
+      for (int c = 0; c < neq; ++c) s += double(dinv[(node * neq + r) * neq + c]) * double(v[node * neq + c]);
+      z[i] = VT(s);
+    }
+  }
+}
+
+// part[j * nblk + b] = block b's share of V_j . w, for j < k (grid.y = k).
+template <typename VT>
+__global__ void dot_partials_kernel(int64_t n, const VT* __restrict__ V, int64_t ldv, const VT* __restrict__ w,
+                                    double* __restrict__ part, const int* __restrict__ done) {
+  if (done && *done) return;
+  __shared__ double sm[32];
+  const int j = blockIdx.y;
+  const VT* v = V + int64_t(j) * ldv;
+  double s = 0.0;
+  GRID_STRIDE(i, n) s += double(v[i]) * double(w[i]);
+  s = block_sum(s, sm);
+  if (threadIdx.x == 0) part[int64_t(j) * gridDim.x + blockIdx.x] = s;
+}
+
+// out[j] = sum_b part[j * nblk + b] in a fixed order; one block per j.
+__global__ void reduce_partials_kernel(int nblk, const double* __restrict__ part, double* __restrict__ out,
+                                       const int* __restrict__ done) {
+  if (done && *done) return;
+  __shared__ double sm[32];
+  const int j = blockIdx.x;
+  double s = 0.0;
+  for (int b = threadIdx.x; b < nblk; b += blockDim.x) s += part[int64_t(j) * nblk + b];
+  s = block_sum(s, sm);
+  if (threadIdx.x == 0) out[j] = s;
+}
+
+// w -= sum_{j<k} h_j V_j ; optionally block partials of ||w||^2.
+template <typename VT>
+__global__ void multi_axpy_kernel(int64_t n, int k, const VT* __restrict__ V, int64_t ldv,
+                                  const double* __restrict__ h, VT* __restrict__ w, double* __restrict__ normpart,
+                                  const int* __restrict__ done) {
+  if (done && *done) return;
+  __shared__ double sm[32];
+  double s2 = 0.0;
+  GRID_STRIDE(i, n) {
+    double acc = double(w[i]);
+    for (int j = 0; j < k; ++j) acc -= h[j] * double(V[int64_t(j) * ldv + i]);
+    const VT wv = VT(acc);
+    w[i] = wv;
+    s2 += double(wv) * double(wv);
+  }
+  if (normpart) {
+    s2 = block_sum(s2, sm);
+    if (threadIdx.x == 0) normpart[blockIdx.x] = s2;
+  }
+}
+
+// t = V y (first k columns, k read from ictl[1]).
+template <typename VT>
+__global__ void combine_kernel(int64_t n, const VT* __restrict__ V, int64_t ldv, const double* __restrict__ y,
+                               const int* __restrict__ ictl, VT* __restrict__ t) {
+  const int k = ictl[1];
+  GRID_STRIDE(i, n) {
+    double acc = 0.0;
+    for (int j = 0; j < k; ++j) acc += y[j] * double(V[int64_t(j) * ldv + i]);
+    t[i] = VT(acc);
+  }
+}
+
+// Arnoldi step j: H(:,j) = h1 + h2, H(j+1,j) = ||w||, Givens update, convergence.
+__global__ void givens_kernel(int j, int m, const double* __restrict__ hbuf, const double* __restrict__ normpart,
+                              int nblk, double* __restrict__ H, double* __restrict__ cs, double* __restrict__ sn,
+                              double* __restrict__ g, double* __restrict__ dctl, int* __restrict__ ictl, double tol,
+                              int last) {
+  if (ictl[0]) return;
+  double nn = 0.0;
+  for (int b = 0; b < nblk; ++b) nn += normpart[b];
+  const double hnext = sqrt(nn);
+  for (int i = 0; i <= j; ++i) H[i * m + j] = hbuf[i] + hbuf[(m + 2) + i];
+  H[(j + 1) * m + j] = hnext;
+  for (int i = 0; i < j; ++i) {
+    const double a = H[i * m + j], b = H[(i + 1) * m + j];
+    H[i * m + j] = cs[i] * a + sn[i] * b;
+    H[(i + 1) * m + j] = -sn[i] * a + cs[i] * b;
+  }
+  const double a = H[j * m + j], b = H[(j + 1) * m + j];
+  const double den = sqrt(a * a + b * b);
+  const double c = den != 0.0 ? a / den : 1.0;
+  const double s = den != 0.0 ? b / den : 0.0;
+  cs[j] = c;
+  sn[j] = s;
+  H[j * m + j] = den;
+  H[(j + 1) * m + j] = 0.0;
+  g[j + 1] = -s * g[j];
+  g[j] = c * g[j];
+  const double res = fabs(g[j + 1]);
+  dctl[kEst] = res;
+  dctl[kHnext] = hnext;
+  ictl[1] = j + 1;
+  if (!isfinite(res) || !isfinite(hnext) || den == 0.0) {
+    ictl[0] = 1;
+    ictl[2] = 3;
+  } else if (res <= tol * dctl[kBnorm] || hnext <= 1e-300 * dctl[kBnorm] || last) {
+    ictl[0] = 1;
+  }
+}
+
+// dst = src * (1 / dctl[idx])
+template <typename VT>
+__global__ void scale_kernel(int64_t n, const VT* __restrict__ src, VT* __restrict__ dst,
+                             const double* __restrict__ dctl, int idx, const int* __restrict__ done) {
+  if (done && *done) return;
+  const double inv = 1.0 / dctl[idx];
+  GRID_STRIDE(i, n) dst[i] = VT(double(src[i]) * inv);
+}
+
+// r = b * bscale - w with block partials of ||r||^2 and (optionally) ||b||^2.
+template <typename VT, typename BT>
+__global__ void residual_kernel(int64_t n, const BT* __restrict__ b, const VT* __restrict__ w, VT* __restrict__ r,
+                                double* __restrict__ normpart, double* __restrict__ bpart) {
+  __shared__ double sm[32];
+  double s2 = 0.0, b2 = 0.0;
+  GRID_STRIDE(i, n) {
+    const double bi = double(b[i]);
+    const VT ri = VT(bi - double(w[i]));
+    r[i] = ri;
+    s2 += double(ri) * double(ri);
+    b2 += bi * bi;
+  }
+  s2 = block_sum(s2, sm);
+  if (threadIdx.x == 0) normpart[blockIdx.x] = s2;
+  if (bpart) {
+    b2 = block_sum(b2, sm);
+    if (threadIdx.x == 0) bpart[blockIdx.x] = b2;
+  }
+}
+
+// Restart: beta = ||r||, g = beta e1, done if converged.
+__global__ void restart_setup_kernel(int nblk, int m, const double* __restrict__ normpart,
+                                     const double* __restrict__ bpart, int first, double* __restrict__ g,
+                                     double* __restrict__ dctl, int* __restrict__ ictl, double tol) {
+  double nn = 0.0;
+  for (int b = 0; b < nblk; ++b) nn += normpart[b];
+  if (first) {
+    double bb = 0.0;
+    for (int b = 0; b < nblk; ++b) bb += bpart[b];
+    dctl[kBnorm] = sqrt(bb);
+  }
+  const double beta = sqrt(nn);
+  dctl[kBeta] = beta;
+  dctl[kEst] = beta;
+  for (int i = 0; i <= m; ++i) g[i] = 0.0;
+  g[0] = beta;
+  ictl[0] = 0;
+  ictl[1] = 0;
+  ictl[2] = 0;
+  if (!isfinite(beta)) {
+    ictl[0] = 1;
+    ictl[2] = 3;
+  } else if (beta <= tol * dctl[kBnorm] || beta == 0.0) {
+    ictl[0] = 1;
+  }
+}
+
+__global__ void backsolve_kernel(int m, const double* __restrict__ H, const double* __restrict__ g,
+                                 double* __restrict__ y, const int* __restrict__ ictl) {
+  const int k = ictl[1];
+  for (int i = k - 1; i >= 0; --i) {
+    double s = g[i];
+    for (int l = i + 1; l < k; ++l) s -= H[i * m + l] * y[l];
+    y[i] = s / H[i * m + i];
+  }
+}
+
+template <typename VT>
+__global__ void axpy_kernel(int64_t n, double alpha, const VT* __restrict__ x, VT* __restrict__ y) {
+  GRID_STRIDE(i, n) y[i] = VT(double(y[i]) + alpha * double(x[i]));
+}
+
+// x64 += dctl[idx] * d32
+template <typename VT>
+__global__ void add_scaled_kernel(int64_t n, const VT* __restrict__ d, double* __restrict__ x,
+                                  const double* __restrict__ dctl, int idx) {
+  const double sc = dctl[idx];
+  GRID_STRIDE(i, n) x[i] += sc * double(d[i]);
+}
+
+template <typename VT>
+__global__ void fill_kernel(int64_t n, VT v, VT* __restrict__ x) {
+  GRID_STRIDE(i, n) x[i] = v;
+}
+
+// dctl[idx] = (sqrt) sum of nblk partials
+__global__ void finalize_norm_kernel(int nblk, const double* __restrict__ part, double* __restrict__ dctl, int idx,
+                                     int take_sqrt) {
+  double s = 0.0;
+  for (int b = 0; b < nblk; ++b) s += part[b];
+  dctl[idx] = take_sqrt ? sqrt(s) : s;
+}
+
+// ---- BiCGStab scalar kernels ------------------------------------------------
+__global__ void bicg_init_kernel(double* dctl, int* ictl, double tol) {
+  dctl[kRhoOld] = 1.0;
+  dctl[kAlpha] = 1.0;
+  dctl[kOmega] = 1.0;
+  ictl[0] = (dctl[kBeta] <= tol * dctl[kBnorm] || dctl[kBnorm] == 0.0) ? 1 : 0;
+  ictl[2] = isfinite(dctl[kBeta]) ? 0 : 3;
+  if (ictl[2]) ictl[0] = 1;
+  ictl[3] = 0;
+}
+
+// p = r + beta (p - omega v), beta = (rho/rho_old)(alpha/omega)
+template <typename VT>
+__global__ void bicg_p_kernel(int64_t n, const VT* __restrict__ r, const VT* __restrict__ v, VT* __restrict__ p,
+                              const double* __restrict__ dctl, const int* __restrict__ ictl) {
+  if (ictl[0]) return;
+  const double beta = (dctl[kRho] / dctl[kRhoOld]) * (dctl[kAlpha] / dctl[kOmega]);
+  const double om = dctl[kOmega];
+  GRID_STRIDE(i, n) p[i] = VT(double(r[i]) + beta * (double(p[i]) - om * double(v[i])));
+}
+
+__global__ void bicg_check_rho_kernel(double* dctl, int* ictl) {
+  if (ictl[0]) return;
+  const double rho = dctl[kRho];
+  if (rho == 0.0 || !isfinite(rho)) {
+    ictl[0] = 1;
+    ictl[2] = isfinite(rho) ? 2 : 3;
+  }
+}
+
+__global__ void bicg_alpha_kernel(double* dctl, int* ictl) {
+  if (ictl[0]) return;
+  const double d = dctl[kRhV];
+  if (d == 0.0 || !isfinite(d)) {
+    ictl[0] = 1;
+    ictl[2] = isfinite(d) ? 2 : 3;
+    return;
+  }
+  dctl[kAlpha] = dctl[kRho] / d;
+}
+
+// s = r - alpha v
+template <typename VT>
+__global__ void bicg_s_kernel(int64_t n, const VT* __restrict__ r, const VT* __restrict__ v, VT* __restrict__ s,
+                              const double* __restrict__ dctl, const int* __restrict__ ictl) {
+  if (ictl[0]) return;
+  const double al = dctl[kAlpha];
+  GRID_STRIDE(i, n) s[i] = VT(double(r[i]) - al * double(v[i]));
+}
+
+__global__ void bicg_omega_kernel(double* dctl, int* ictl) {
+  if (ictl[0]) return;
+  const double tt = dctl[kTT];
+  dctl[kOmega] = (tt != 0.0) ? dctl[kTS] / tt : 0.0;
+  if (!isfinite(dctl[kOmega])) {
+    ictl[0] = 1;
+    ictl[2] = 3;
+  }
+}
+
+// x += alpha ph + omega sh ; r = s - omega t ; partials of ||r||^2
+template <typename VT>
+__global__ void bicg_xr_kernel(int64_t n, const VT* __restrict__ ph, const VT* __restrict__ sh,
+                               const VT* __restrict__ s, const VT* __restrict__ t, VT* __restrict__ x,
+                               VT* __restrict__ r, const double* __restrict__ dctl, const int* __restrict__ ictl,
+                               double* __restrict__ normpart) {
+  if (ictl[0]) return;
+  __shared__ double sm[32];
+  const double al = dctl[kAlpha], om = dctl[kOmega];
+  double s2 = 0.0;
+  GRID_STRIDE(i, n) {
+    x[i] = VT(double(x[i]) + al * double(ph[i]) + om * double(sh[i]));
+    const VT ri = VT(double(s[i]) - om * double(t[i]));
+    r[i] = ri;
+    s2 += double(ri) * double(ri);
+  }
+  s2 = block_sum(s2, sm);
+  if (threadIdx.x == 0) normpart[blockIdx.x] = s2;
+}
+
+__global__ void bicg_end_kernel(int nblk, const double* __restrict__ normpart, double* dctl, int* ictl, double tol,
+                                int maxit) {
+  if (ictl[0]) return;
+  double nn = 0.0;
+  for (int b = 0; b < nblk; ++b) nn += normpart[b];
+  const double rn = sqrt(nn);
+  dctl[kEst] = rn;
+  dctl[kRhoOld] = dctl[kRho];
+  ictl[3] += 1;
+  if (!isfinite(rn)) {
+    ictl[0] = 1;
+    ictl[2] = 3;
+  } else if (rn <= tol * dctl[kBnorm]) {
+    ictl[0] = 1;
+  } else if (ictl[3] >= maxit) {
+    ictl[0] = 1;
+    ictl[2] = 1;
+  }
+}
+
+// ---------------------------------------------------------------------------
+template <typename T>
+int dalloc(T** p, size_t count) {
+  if (*p) return UFEM_OK;
+  cudaError_t e = cudaMalloc(reinterpret_cast<void**>(p), std::max<size_t>(count, 1) * sizeof(T));
+  if (e != cudaSuccess)
+    return set_error(UFEM_ERR_NOMEM, std::string("cudaMalloc (Krylov workspace): ") + cudaGetErrorString(e));
+  return UFEM_OK;
+}
+
+template <typename T>
+void dfree(T*& p) {
+  if (p) cudaFree(p);
+  p = nullptr;
+}
+
+int ensure_work(ufem_ns_handle* h, int m, bool need32, bool bicg) {
+  if (!h->kw) h->kw = new KrylovWork();
+  KrylovWork& kw = *h->kw;
+  const int64_t n = h->nrows;
+  if (kw.m < m && (kw.V || kw.V32 || kw.part)) {  // a longer restart: reallocate the basis-sized buffers
+    dfree(kw.V); dfree(kw.V32); dfree(kw.part); dfree(kw.hbuf); dfree(kw.H);
+    dfree(kw.cs); dfree(kw.sn); dfree(kw.g); dfree(kw.y);
+  }
+  kw.m = std::max(kw.m, m);
+  kw.n = n;
+  kw.nblk = int(std::min<int64_t>(296, std::max<int64_t>(1, (n + 2047) / 2048)));
+  const int M = kw.m;
+  const size_t nd = size_t(n);
+  const size_t ndinv = size_t(h->N) * h->neq * h->neq;
+  int rc;
+  if ((rc = dalloc(&kw.w, nd)) || (rc = dalloc(&kw.z, nd)) || (rc = dalloc(&kw.t, nd)) || (rc = dalloc(&kw.r, nd)) ||
+      (rc = dalloc(&kw.dinv, ndinv)) || (rc = dalloc(&kw.part, size_t(M + 2) * kw.nblk)) ||
+      (rc = dalloc(&kw.hbuf, size_t(2) * (M + 2))) || (rc = dalloc(&kw.H, size_t(M + 1) * M)) ||
+      (rc = dalloc(&kw.cs, size_t(M))) || (rc = dalloc(&kw.sn, size_t(M))) || (rc = dalloc(&kw.g, size_t(M + 1))) ||
+      (rc = dalloc(&kw.y, size_t(M))) || (rc = dalloc(&kw.dctl, 16)) || (rc = dalloc(&kw.ictl, 8)))
+    return rc;
+  if (!kw.h_dctl) {
+    UFEM_CUDA_TRY(cudaMallocHost(reinterpret_cast<void**>(&kw.h_dctl), 16 * sizeof(double)));
+    UFEM_CUDA_TRY(cudaMallocHost(reinterpret_cast<void**>(&kw.h_ictl), 8 * sizeof(int)));
+  }
+  if (!bicg) {
+    if (need32) {
+      if ((rc = dalloc(&kw.V32, size_t(M + 1) * nd))) return rc;
+    } else {
+      if ((rc = dalloc(&kw.V, size_t(M + 1) * nd))) return rc;
+    }
+  }
+  if (need32) {
+    if ((rc = dalloc(&kw.w32, nd)) || (rc = dalloc(&kw.z32, nd)) || (rc = dalloc(&kw.t32, nd)) ||
+        (rc = dalloc(&kw.r32, nd)) || (rc = dalloc(&kw.x32, nd)) || (rc = dalloc(&kw.q32, nd)) ||
+        (rc = dalloc(&kw.dinv32, ndinv)) ||
+        (rc = dalloc(&h->d_vals32, size_t(h->nnz))))
+      return rc;
+  }
+  if (bicg) {
+    if (need32) {
+      if ((rc = dalloc(&kw.bp32, nd)) || (rc = dalloc(&kw.bv32, nd)) || (rc = dalloc(&kw.bs32, nd)) ||
+          (rc = dalloc(&kw.bt32, nd)) || (rc = dalloc(&kw.brh32, nd)) || (rc = dalloc(&kw.bph32, nd)) ||
+          (rc = dalloc(&kw.bsh32, nd)))
+        return rc;
+    } else {
+      if ((rc = dalloc(&kw.bp, nd)) || (rc = dalloc(&kw.bv, nd)) || (rc = dalloc(&kw.bs, nd)) ||
+          (rc = dalloc(&kw.bt, nd)) || (rc = dalloc(&kw.brh, nd)) || (rc = dalloc(&kw.bph, nd)) ||
+          (rc = dalloc(&kw.bsh, nd)))
+        return rc;
+    }
+  }
+  return UFEM_OK;
+}
+
+inline unsigned grid_for(int64_t n, int threads, int64_t cap = 8 * 148) {
+  return unsigned(std::max<int64_t>(1, std::min<int64_t>(cap, (n + threads - 1) / threads)));
+}
+
+template <typename VT, typename MT>
+int spmv(ufem_ns_handle* h, const MT* vals, const VT* x, VT* y, const int* done, cudaStream_t s) {
+  using AT = typename std::conditional<std::is_same<VT, double>::value, double, float>::type;
+  const int64_t threads = h->N * 32;
+  spmv_kernel<VT, MT, AT><<<unsigned((threads + 255) / 256), 256, 0, s>>>(h->N, h->neq, h->d_start, h->d_adj, vals, x,
+                                                                          y, done);
+  UFEM_CUDA_TRY(cudaGetLastError());
+  return UFEM_OK;
+}
+
+template <typename VT, typename MT>
+int setup_precond(ufem_ns_handle* h, int kind, const MT* vals, VT* dinv, cudaStream_t s) {
+  if (kind == 1)
+    jacobi_kernel<MT, VT><<<grid_for(h->nrows, 256), 256, 0, s>>>(h->nrows, h->d_diagpos, vals, dinv);
+  else if (kind == 2)
+    block_jacobi_kernel<MT, VT><<<grid_for(h->N, 128), 128, 0, s>>>(h->N, h->neq, h->d_diagpos, vals, dinv);
+  UFEM_CUDA_TRY(cudaGetLastError());
+  return UFEM_OK;
+}
+
+template <typename VT>
+int precond(ufem_ns_handle* h, int kind, const VT* dinv, const VT* v, VT* z, const int* done, cudaStream_t s) {
+  precond_kernel<VT><<<grid_for(h->nrows, 256), 256, 0, s>>>(h->nrows, h->neq, kind, dinv, v, z, done);
+  UFEM_CUDA_TRY(cudaGetLastError());
+  return UFEM_OK;
+}
+
+struct SolveResult {
+  int iters = 0;
+  int status = 0;  // 0 ok, 1 max iterations, 2 breakdown, 3 non-finite
+  double relres = 0.0;
+  bool converged = false;
+};
+
+// Final FP64-or-VT true residual ||b - A x|| / ||b|| into res.
+template <typename VT, typename MT, typename BT>
+int true_residual(ufem_ns_handle* h, const MT* vals, const BT* b, const VT* x, VT* w, VT* r, double bnorm,
+                  cudaStream_t s, double* out) {
+  KrylovWork& kw = *h->kw;
+  int rc;
+  if ((rc = spmv<VT, MT>(h, vals, x, w, nullptr, s))) return rc;
+  residual_kernel<VT, BT><<<unsigned(kw.nblk), kRedThreads, 0, s>>>(h->nrows, b, w, r, kw.part, nullptr);
+  finalize_norm_kernel<<<1, 1, 0, s>>>(kw.nblk, kw.part, kw.dctl, kTrue, 1);
+  UFEM_CUDA_TRY(cudaMemcpyAsync(kw.h_dctl, kw.dctl, 16 * sizeof(double), cudaMemcpyDeviceToHost, s));
+  UFEM_CUDA_TRY(cudaStreamSynchronize(s));
+  *out = bnorm > 0.0 ? kw.h_dctl[kTrue] / bnorm : 0.0;
+  return UFEM_OK;
+}
+
+// Right-preconditioned restarted GMRES(m) with CGS2 orthogonalisation:
+// A M^-1 u = b, x = x0 + M^-1 V y.  One host synchronisation per restart cycle.
+template <typename VT, typename MT, typename BT>
+int gmres(ufem_ns_handle* h, const MT* vals, const BT* b, VT* x, VT* V, VT* w, VT* z, VT* t, VT* r, VT* dinv,
+          int pkind, double tol, int maxit, int m, cudaStream_t s, SolveResult& res) {
+  KrylovWork& kw = *h->kw;
+  const int64_t n = h->nrows;
+  const int nblk = kw.nblk;
+  const unsigned g1 = unsigned(nblk);
+  int rc;
+  if ((rc = setup_precond<VT, MT>(h, pkind, vals, dinv, s))) return rc;
+  res = SolveResult();
+  bool first = true;
+  double bnorm = 0.0;
+  while (true) {
+    if ((rc = spmv<VT, MT>(h, vals, x, w, nullptr, s))) return rc;
+    residual_kernel<VT, BT><<<g1, kRedThreads, 0, s>>>(n, b, w, r, kw.part, first ? kw.part + nblk : nullptr);
+    restart_setup_kernel<<<1, 1, 0, s>>>(nblk, m, kw.part, kw.part + nblk, first ? 1 : 0, kw.g, kw.dctl, kw.ictl, tol);
+    scale_kernel<VT><<<g1, kRedThreads, 0, s>>>(n, r, V, kw.dctl, kBeta, kw.ictl);
+    UFEM_CUDA_TRY(cudaGetLastError());
+    first = false;
+    const int budget = std::max(1, std::min(m, maxit - res.iters));
+    for (int j = 0; j < budget; ++j) {
+      const VT* vj = V + int64_t(j) * n;
+      if ((rc = precond<VT>(h, pkind, dinv, vj, z, kw.ictl, s))) return rc;
+      if ((rc = spmv<VT, MT>(h, vals, z, w, kw.ictl, s))) return rc;
+      for (int pass = 0; pass < 2; ++pass) {  // classical Gram-Schmidt, twice
+        double* hb = kw.hbuf + pass * (kw.m + 2);
+        dot_partials_kernel<VT><<<dim3(g1, unsigned(j + 1)), kRedThreads, 0, s>>>(n, V, n, w, kw.part, kw.ictl);
+        reduce_partials_kernel<<<unsigned(j + 1), 256, 0, s>>>(nblk, kw.part, hb, kw.ictl);
+        multi_axpy_kernel<VT><<<g1, kRedThreads, 0, s>>>(n, j + 1, V, n, hb, w, pass == 1 ? kw.part : nullptr,
+                                                          kw.ictl);
+      }
+      givens_kernel<<<1, 1, 0, s>>>(j, kw.m, kw.hbuf, kw.part, nblk, kw.H, kw.cs, kw.sn, kw.g, kw.dctl, kw.ictl, tol,
+                                    j + 1 == budget ? 1 : 0);
+      scale_kernel<VT><<<g1, kRedThreads, 0, s>>>(n, w, V + int64_t(j + 1) * n, kw.dctl, kHnext, kw.ictl);
+      UFEM_CUDA_TRY(cudaGetLastError());
+    }
+    backsolve_kernel<<<1, 1, 0, s>>>(kw.m, kw.H, kw.g, kw.y, kw.ictl);
+    combine_kernel<VT><<<g1, kRedThreads, 0, s>>>(n, V, n, kw.y, kw.ictl, t);
+    if ((rc = precond<VT>(h, pkind, dinv, t, z, nullptr, s))) return rc;
+    UFEM_CUDA_TRY(cudaMemcpyAsync(kw.h_ictl, kw.ictl, 4 * sizeof(int), cudaMemcpyDeviceToHost, s));
+    UFEM_CUDA_TRY(cudaMemcpyAsync(kw.h_dctl, kw.dctl, 16 * sizeof(double), cudaMemcpyDeviceToHost, s));
+    UFEM_CUDA_TRY(cudaStreamSynchronize(s));
+    const int jc = kw.h_ictl[1];
+    bnorm = kw.h_dctl[kBnorm];
+    if (kw.h_ictl[2] == 3) {
+      res.status = 3;
+      res.relres = NAN;
+      return UFEM_OK;
+    }
+    if (bnorm == 0.0) {
+      fill_kernel<VT><<<g1, kRedThreads, 0, s>>>(n, VT(0), x);
+      UFEM_CUDA_TRY(cudaGetLastError());
+      res.converged = true;
+      return UFEM_OK;
+    }
+    if (jc > 0) {
+      axpy_kernel<VT><<<g1, kRedThreads, 0, s>>>(n, 1.0, z, x);
+      UFEM_CUDA_TRY(cudaGetLastError());
+    }
+    res.iters += jc;
+    if (jc == 0) {  // converged at the restart residual (exact)
+      res.converged = kw.h_dctl[kBeta] <= tol * bnorm;
+      res.relres = kw.h_dctl[kBeta] / bnorm;
+      res.status = res.converged ? 0 : 2;
+      return UFEM_OK;
+    }
+    if (res.iters >= maxit) {
+      double rr;
+      if ((rc = true_residual<VT, MT, BT>(h, vals, b, x, w, r, bnorm, s, &rr))) return rc;
+      res.relres = rr;
+      res.converged = rr <= tol;
+      res.status = res.converged ? 0 : 1;
+      return UFEM_OK;
+    }
+  }
+}
+
+// Right-preconditioned BiCGStab with device-side scalars; the host checks the
+// done flag every `check` iterations.
+template <typename VT, typename MT, typename BT>
+int bicgstab(ufem_ns_handle* h, const MT* vals, const BT* b, VT* x, VT* r, VT* rh, VT* p, VT* v, VT* sv, VT* tv,
+             VT* ph, VT* sh, VT* dinv, int pkind, double tol, int maxit, cudaStream_t st, SolveResult& res) {
+  KrylovWork& kw = *h->kw;
+  const int64_t n = h->nrows;
+  const int nblk = kw.nblk;
+  const unsigned g1 = unsigned(nblk);
+  int rc;
+  if ((rc = setup_precond<VT, MT>(h, pkind, vals, dinv, st))) return rc;
+  res = SolveResult();
+  if ((rc = spmv<VT, MT>(h, vals, x, v, nullptr, st))) return rc;
+  residual_kernel<VT, BT><<<g1, kRedThreads, 0, st>>>(n, b, v, r, kw.part, kw.part + nblk);
+  finalize_norm_kernel<<<1, 1, 0, st>>>(nblk, kw.part, kw.dctl, kBeta, 1);
+  finalize_norm_kernel<<<1, 1, 0, st>>>(nblk, kw.part + nblk, kw.dctl, kBnorm, 1);
+  UFEM_CUDA_TRY(cudaMemcpyAsync(rh, r, n * sizeof(VT), cudaMemcpyDeviceToDevice, st));
+  fill_kernel<VT><<<g1, kRedThreads, 0, st>>>(n, VT(0), p);
+  fill_kernel<VT><<<g1, kRedThreads, 0, st>>>(n, VT(0), v);
+  bicg_init_kernel<<<1, 1, 0, st>>>(kw.dctl, kw.ictl, tol);
+  UFEM_CUDA_TRY(cudaGetLastError());
+  auto dot = [&](const VT* a, const VT* c, int slot) -> int {
+    dot_partials_kernel<VT><<<dim3(g1, 1), kRedThreads, 0, st>>>(n, a, n, c, kw.part, kw.ictl);
+    reduce_partials_kernel<<<1, 256, 0, st>>>(nblk, kw.part, kw.dctl + slot, kw.ictl);
+    UFEM_CUDA_TRY(cudaGetLastError());
+    return UFEM_OK;
+  };
+  const int check = 8;
+  for (int it = 0; it < maxit; it += check) {
+    for (int k = 0; k < check; ++k) {
+      if ((rc = dot(rh, r, kRho))) return rc;
+      bicg_check_rho_kernel<<<1, 1, 0, st>>>(kw.dctl, kw.ictl);
+      bicg_p_kernel<VT><<<g1, kRedThreads, 0, st>>>(n, r, v, p, kw.dctl, kw.ictl);
+      if ((rc = precond<VT>(h, pkind, dinv, p, ph, kw.ictl, st))) return rc;
+      if ((rc = spmv<VT, MT>(h, vals, ph, v, kw.ictl, st))) return rc;
+      if ((rc = dot(rh, v, kRhV))) return rc;
+      bicg_alpha_kernel<<<1, 1, 0, st>>>(kw.dctl, kw.ictl);
+      bicg_s_kernel<VT><<<g1, kRedThreads, 0, st>>>(n, r, v, sv, kw.dctl, kw.ictl);
+      if ((rc = precond<VT>(h, pkind, dinv, sv, sh, kw.ictl, st))) return rc;
+      if ((rc = spmv<VT, MT>(h, vals, sh, tv, kw.ictl, st))) return rc;
+      if ((rc = dot(tv, sv, kTS))) return rc;
+      if ((rc = dot(tv, tv, kTT))) return rc;
+      bicg_omega_kernel<<<1, 1, 0, st>>>(kw.dctl, kw.ictl);
+      bicg_xr_kernel<VT><<<g1, kRedThreads, 0, st>>>(n, ph, sh, sv, tv, x, r, kw.dctl, kw.ictl, kw.part);
+      bicg_end_kernel<<<1, 1, 0, st>>>(nblk, kw.part, kw.dctl, kw.ictl, tol, maxit);
+      UFEM_CUDA_TRY(cudaGetLastError());
+    }
+    UFEM_CUDA_TRY(cudaMemcpyAsync(kw.h_ictl, kw.ictl, 4 * sizeof(int), cudaMemcpyDeviceToHost, st));
+    UFEM_CUDA_TRY(cudaStreamSynchronize(st));
+    if (kw.h_ictl[0]) break;
+  }
+  UFEM_CUDA_TRY(cudaMemcpyAsync(kw.h_ictl, kw.ictl, 4 * sizeof(int), cudaMemcpyDeviceToHost, st));
+  UFEM_CUDA_TRY(cudaMemcpyAsync(kw.h_dctl, kw.dctl, 16 * sizeof(double), cudaMemcpyDeviceToHost, st));
+  UFEM_CUDA_TRY(cudaStreamSynchronize(st));
+  res.iters = kw.h_ictl[3];
+  res.status = kw.h_ictl[2];
+  const double bnorm = kw.h_dctl[kBnorm];
+  if (bnorm == 0.0) {
+    fill_kernel<VT><<<g1, kRedThreads, 0, st>>>(n, VT(0), x);
+    UFEM_CUDA_TRY(cudaGetLastError());
+    res.converged = true;
+    return UFEM_OK;
+  }
+  double rr;
+  if ((rc = true_residual<VT, MT, BT>(h, vals, b, x, v, r, bnorm, st, &rr))) return rc;
+  res.relres = rr;
+  res.converged = rr <= tol;
+  if (res.converged) res.status = 0;
+  else if (res.status == 0) res.status = 1;
+  return UFEM_OK;
+}
+
+// dst32 = src64 * (1 / dctl[idx])
+__global__ void to32_scaled_kernel(int64_t n, const double* __restrict__ src, float* __restrict__ dst,
+                                   const double* __restrict__ dctl, int idx) {
+  const double inv = dctl[idx] > 0.0 ? 1.0 / dctl[idx] : 0.0;
+  GRID_STRIDE(i, n) dst[i] = float(src[i] * inv);
+}
+
+__global__ void vals_to32_kernel(int64_t n, const double* __restrict__ v, float* __restrict__ v32) {
+  GRID_STRIDE(i, n) v32[i] = float(v[i]);
+}
+
+}  // namespace
+
+int krylov_solve(ufem_ns_handle* h, const ufem_krylov_opts* ko, ufem_krylov_status* st, cudaStream_t s) {
+  ufem_krylov_opts o = *ko;
+  if (o.restart <= 0) o.restart = 30;
+  if (o.max_iters <= 0) o.max_iters = 1000;
+  if (o.tol <= 0) o.tol = 1e-10;
+  if (o.max_refine <= 0) o.max_refine = 20;
+  if (o.inner_tol <= 0) o.inner_tol = 1e-5;
+  if (o.precond < 0 || o.precond > 2) return set_error(UFEM_ERR_ARG, "precond must be 0, 1 or 2");
+  if (o.method < 0 || o.method > 1) return set_error(UFEM_ERR_ARG, "method must be 0 (GMRES) or 1 (BiCGStab)");
+  const bool mixed = o.mixed != 0;
+  const bool bicg = o.method == 1;
+  int rc;
+  if ((rc = ensure_work(h, o.restart, mixed, bicg))) return rc;
+  KrylovWork& kw = *h->kw;
+  const int64_t n = h->nrows;
+  const unsigned g1 = unsigned(kw.nblk);
+  ufem_krylov_status out{};
+  if (!mixed) {
+    SolveResult r;
+    if (bicg)
+      rc = bicgstab<double, double, double>(h, h->d_vals, h->d_rhs, h->d_sol, kw.r, kw.brh, kw.bp, kw.bv, kw.bs, kw.bt,
+                                            kw.bph, kw.bsh, kw.dinv, o.precond, o.tol, o.max_iters, s, r);
+    else
+      rc = gmres<double, double, double>(h, h->d_vals, h->d_rhs, h->d_sol, kw.V, kw.w, kw.z, kw.t, kw.r, kw.dinv,
+                                         o.precond, o.tol, o.max_iters, o.restart, s, r);
+    if (rc) return rc;
+    out.converged = r.converged;
+    out.status = r.status;
+    out.iterations = r.iters;
+    out.refinements = 0;
+    out.rel_residual = r.relres;
+  } else {
+    // FP64 iterative refinement around an FP32 inner Krylov solve.  The FP32
+    // matrix copy is written by the assembly kernel (or converted here).
+    if (!h->vals32_valid) {
+      vals_to32_kernel<<<grid_for(h->nnz, 256), 256, 0, s>>>(h->nnz, h->d_vals, h->d_vals32);
+      UFEM_CUDA_TRY(cudaGetLastError());
+      h->vals32_valid = true;
+    }
+    double bnorm = -1.0;
+    int total = 0;
+    int status = 0;
+    int ref = 0;
+    double relres = 0.0;
+    bool conv = false;
+    for (ref = 0; ref <= o.max_refine; ++ref) {
+      // r = b - A x in FP64
+      if ((rc = spmv<double, double>(h, h->d_vals, h->d_sol, kw.w, nullptr, s))) return rc;
+      residual_kernel<double, double><<<g1, kRedThreads, 0, s>>>(n, h->d_rhs, kw.w, kw.r, kw.part,
+                                                                 kw.part + kw.nblk);
+      finalize_norm_kernel<<<1, 1, 0, s>>>(kw.nblk, kw.part, kw.dctl, kScale, 1);
+      finalize_norm_kernel<<<1, 1, 0, s>>>(kw.nblk, kw.part + kw.nblk, kw.dctl, kR2, 1);
+      UFEM_CUDA_TRY(cudaMemcpyAsync(kw.h_dctl, kw.dctl, 16 * sizeof(double), cudaMemcpyDeviceToHost, s));
+      UFEM_CUDA_TRY(cudaStreamSynchronize(s));
+      if (bnorm < 0) bnorm = kw.h_dctl[kR2];
+      const double rn = kw.h_dctl[kScale];
+      if (!std::isfinite(rn)) { status = 3; relres = NAN; break; }
+      relres = bnorm > 0 ? rn / bnorm : 0.0;
+      if (bnorm == 0.0) {
+        fill_kernel<double><<<g1, kRedThreads, 0, s>>>(n, 0.0, h->d_sol);
+        UFEM_CUDA_TRY(cudaGetLastError());
+        conv = true;
+        break;
+      }
+      if (relres <= o.tol) { conv = true; break; }
+      if (ref == o.max_refine || total >= o.max_iters * (o.max_refine + 1)) { status = 1; break; }
+      // inner: A32 d = r / ||r||, d0 = 0
+      to32_scaled_kernel<<<g1, kRedThreads, 0, s>>>(n, kw.r, kw.r32, kw.dctl, kScale);
+      fill_kernel<float><<<g1, kRedThreads, 0, s>>>(n, 0.0f, kw.x32);
+      UFEM_CUDA_TRY(cudaGetLastError());
+      // keep ||r|| for the update: the inner solve reuses the scalar slots
+      UFEM_CUDA_TRY(cudaMemcpyAsync(kw.dctl + 14, kw.dctl + kScale, sizeof(double), cudaMemcpyDeviceToDevice, s));
+      SolveResult ir;
+      if (bicg)
+        rc = bicgstab<float, float, float>(h, h->d_vals32, kw.r32, kw.x32, kw.w32, kw.brh32, kw.bp32, kw.bv32,
+                                           kw.bs32, kw.bt32, kw.bph32, kw.bsh32, kw.dinv32, o.precond, o.inner_tol,
+                                           o.max_iters, s, ir);
+      else
+        rc = gmres<float, float, float>(h, h->d_vals32, kw.r32, kw.x32, kw.V32, kw.w32, kw.z32, kw.t32, kw.q32,
+                                        kw.dinv32, o.precond, o.inner_tol, o.max_iters, o.restart, s, ir);
+      if (rc) return rc;
+      total += ir.iters;
+      if (ir.status == 3) { status = 3; relres = NAN; break; }
+      add_scaled_kernel<float><<<g1, kRedThreads, 0, s>>>(n, kw.x32, h->d_sol, kw.dctl, 14);
+      UFEM_CUDA_TRY(cudaGetLastError());
+    }
+    out.converged = conv;
+    out.status = conv ? 0 : (status ? status : 1);
+    out.iterations = total;
+    out.refinements = ref;
+    out.rel_residual = relres;
+  }
+  if (st) *st = out;
+  return UFEM_OK;
+}
+
+int krylov_apply(ufem_ns_handle* h, const double* d_x, double* d_y, cudaStream_t s) {
+  return spmv<double, double>(h, h->d_vals, d_x, d_y, nullptr, s);
+}
+
+void krylov_free(ufem_ns_handle* h) {
+  if (!h->kw) return;
+  KrylovWork& k = *h->kw;
+  dfree(k.V); dfree(k.w); dfree(k.z); dfree(k.t); dfree(k.r); dfree(k.dinv);
+  dfree(k.V32); dfree(k.w32); dfree(k.z32); dfree(k.t32); dfree(k.r32); dfree(k.x32); dfree(k.q32); dfree(k.dinv32);
+  dfree(k.bp); dfree(k.bv); dfree(k.bs); dfree(k.bt); dfree(k.brh); dfree(k.bph); dfree(k.bsh);
+  dfree(k.bp32); dfree(k.bv32); dfree(k.bs32); dfree(k.bt32); dfree(k.brh32); dfree(k.bph32); dfree(k.bsh32);
+  dfree(k.part); dfree(k.hbuf); dfree(k.H); dfree(k.cs); dfree(k.sn); dfree(k.g); dfree(k.y);
+  dfree(k.dctl); dfree(k.ictl);
+  if (k.h_dctl) cudaFreeHost(k.h_dctl);
+  if (k.h_ictl) cudaFreeHost(k.h_ictl);
+  delete h->kw;
+  h->kw = nullptr;
+}
+
+}  // namespace ufem

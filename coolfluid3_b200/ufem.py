@@ -1,0 +1,249 @@
+"""Host-side mirror of UFEM's NavierStokes solver action on the B200 library.
+
+``NavierStokes`` follows the reference's ``cf3.UFEM.NavierStokes``
+(plugins/UFEM/src/UFEM/ns_implementation/NavierStokes.cpp:49-192), an
+``LSSActionUnsteady`` (LSSActionUnsteady.cpp:30-71) whose ``execute`` runs
+ZeroLSS -> LinearizeU -> Assembly -> BoundaryConditions -> SolveLSS -> Update.
+Option names and meanings are the reference's: ``use_specializations``,
+``supg_type`` ("metric" | "tezduyar" | "cf2"), ``theta``, the physics
+``density`` and ``dynamic_viscosity`` (the kinematic viscosity is derived as
+mu/rho, NavierStokesPhysics.cpp:86-105), and the time step.  Errors raise
+``UfemError`` carrying the library's status code.
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+
+from . import _native as N
+
+SUPG_TYPES = {"tezduyar": 0, "metric": 1, "cf2": 2}
+PRECISIONS = {"fp64": 0, "fp32": 1}
+
+
+def _stream(stream) -> C.c_void_p | None:
+    if stream is None:
+        return None
+    if isinstance(stream, int):
+        return C.c_void_p(stream)
+    return C.c_void_p(int(getattr(stream, "cuda_stream", stream)))
+
+
+def krylov_options(method: str = "gmres", restart: int = 30, max_iters: int = 1000, precond: str = "jacobi",
+                   tol: float = 1e-10, mixed: bool = False, max_refine: int = 20, inner_tol: float = 1e-5):
+    o = N.KrylovOpts()
+    o.method = {"gmres": 0, "bicgstab": 1}[method]
+    o.restart = restart
+    o.max_iters = max_iters
+    o.precond = {"none": 0, "jacobi": 1, "block_jacobi": 2}[precond]
+    o.tol = tol
+    o.mixed = 1 if mixed else 0
+    o.max_refine = max_refine
+    o.inner_tol = inner_tol
+    return o
+
+
+class NavierStokes:
+    """One UFEM NavierStokes action with its linear system on one GPU."""
+
+    def __init__(self, coords: np.ndarray, conn: np.ndarray, *, dt: float, density: float = 1.0,
+                 use_specializations: bool = True, supg_type: str = "metric", theta: float = 1.0,
+                 c1: float = 1.0, c2: float = 16.0, alpha_ps: float = 1.0, alpha_su: float = 1.0,
+                 alpha_bu: float = 1.0, u_ref: float = 1.0, precision: str = "fp64"):
+        self._lib = N.lib()
+        coords = np.ascontiguousarray(coords, np.float64)
+        conn = np.ascontiguousarray(conn, np.uint32)
+        self.dim = coords.shape[1]
+        self.neq = self.dim + 1
+        self.nb_nodes = coords.shape[0]
+        self.nb_elems = conn.shape[0]
+        if conn.shape[1] != self.dim + 1:
+            raise ValueError("connectivity must have dim+1 columns (P1 triangles or tetrahedra)")
+        self._opts = N.NSOptions()
+        self._lib.ufem_ns_default_options(C.byref(self._opts))
+        self._set_fields(dict(dt=dt, density=density, use_specializations=use_specializations,
+                              supg_type=supg_type, theta=theta, c1=c1, c2=c2, alpha_ps=alpha_ps,
+                              alpha_su=alpha_su, alpha_bu=alpha_bu, u_ref=u_ref, precision=precision))
+        mesh = N.Mesh(self.dim, 0, self.nb_nodes, self.nb_elems, N.dptr(coords), N.u32ptr(conn))
+        h = C.c_void_p()
+        N.check(self._lib.ufem_ns_create(C.byref(mesh), C.byref(self._opts), C.byref(h)))
+        self._h = h
+        nr, nnz, bnnz = C.c_int64(), C.c_int64(), C.c_int64()
+        N.check(self._lib.ufem_ns_sizes(self._h, C.byref(nr), C.byref(nnz), C.byref(bnnz)))
+        self.nb_rows, self.nnz, self.block_nnz = nr.value, nnz.value, bnnz.value
+
+    # -- options (NavierStokes.cpp:74-98 triggers) ---------------------------
+    def _set_fields(self, kw: dict) -> None:
+        o = self._opts
+        for k, v in kw.items():
+            if k == "dt":
+                o.dt = float(v)
+            elif k == "density":
+                o.rho = float(v)
+            elif k == "use_specializations":
+                o.use_specializations = 1 if v else 0
+            elif k == "supg_type":
+                if v not in SUPG_TYPES:
+                    raise ValueError(f"supg_type must be one of {sorted(SUPG_TYPES)}")
+                o.supg_type = SUPG_TYPES[v]
+            elif k == "precision":
+                o.precision = PRECISIONS[v]
+            elif k in ("theta", "c1", "c2", "alpha_ps", "alpha_su", "alpha_bu", "u_ref"):
+                setattr(o, k, float(v))
+            else:
+                raise KeyError(f"unknown option {k}")
+
+    def set_options(self, **kw) -> None:
+        self._set_fields(kw)
+        N.check(self._lib.ufem_ns_set_options(self._h, C.byref(self._opts)))
+
+    @property
+    def options(self) -> dict:
+        o = self._opts
+        inv = {v: k for k, v in SUPG_TYPES.items()}
+        return dict(dt=o.dt, density=o.rho, use_specializations=bool(o.use_specializations),
+                    supg_type=inv[o.supg_type], theta=o.theta, c1=o.c1, c2=o.c2, alpha_ps=o.alpha_ps,
+                    alpha_su=o.alpha_su, alpha_bu=o.alpha_bu, u_ref=o.u_ref,
+                    precision={v: k for k, v in PRECISIONS.items()}[o.precision])
+
+    # -- fields ----------------------------------------------------------------
+    def set_state(self, up: np.ndarray, lin: np.ndarray, nu: np.ndarray, force: np.ndarray | None = None) -> None:
+        up = np.ascontiguousarray(up, np.float64)
+        lin = np.ascontiguousarray(lin, np.float64)
+        nu = np.ascontiguousarray(nu, np.float64)
+        if up.shape != (self.nb_nodes, self.neq) or lin.shape != (self.nb_nodes, 4 * self.dim) or nu.shape != (self.nb_nodes,):
+            raise ValueError("field shapes must be (N, neq), (N, 4*dim), (N,)")
+        f = None if force is None else np.ascontiguousarray(force, np.float64)
+        N.check(self._lib.ufem_ns_set_state(self._h, N.dptr(up), N.dptr(lin), N.dptr(nu), N.dptr(f)))
+
+    def initial_conditions(self, u: np.ndarray, nu: float | np.ndarray, p: np.ndarray | None = None,
+                           force: np.ndarray | None = None) -> None:
+        """InitialConditions (NavierStokes.cpp:194-205): u_adv = u1 = u2 = u3 = u, nu_eff = nu."""
+        u = np.ascontiguousarray(u, np.float64)
+        up = np.zeros((self.nb_nodes, self.neq))
+        up[:, : self.dim] = u
+        if p is not None:
+            up[:, self.dim] = p
+        lin = np.tile(u, (1, 4))
+        nuv = np.broadcast_to(np.asarray(nu, np.float64), (self.nb_nodes,)).copy()
+        self.set_state(up, lin, nuv, force)
+
+    def state(self):
+        up = np.empty((self.nb_nodes, self.neq))
+        lin = np.empty((self.nb_nodes, 4 * self.dim))
+        N.check(self._lib.ufem_ns_get_state(self._h, N.dptr(up), N.dptr(lin)))
+        return up, lin
+
+    def solution(self) -> np.ndarray:
+        s = np.empty(self.nb_rows)
+        N.check(self._lib.ufem_ns_get_solution(self._h, N.dptr(s)))
+        return s
+
+    def set_solution(self, s: np.ndarray) -> None:
+        s = np.ascontiguousarray(s, np.float64)
+        N.check(self._lib.ufem_ns_set_solution(self._h, N.dptr(s)))
+
+    # -- boundary conditions -------------------------------------------------
+    def clear_dirichlet(self) -> None:
+        N.check(self._lib.ufem_ns_clear_dirichlet(self._h))
+
+    def add_dirichlet(self, nodes, comps, values) -> None:
+        """Ordered constant Dirichlet conditions; comps may be a scalar."""
+        nodes = np.ascontiguousarray(nodes, np.uint32)
+        values = np.ascontiguousarray(np.broadcast_to(np.asarray(values, np.float64), nodes.shape))
+        comps = np.ascontiguousarray(np.broadcast_to(np.asarray(comps, np.int32), nodes.shape))
+        N.check(self._lib.ufem_ns_add_dirichlet_dofs(self._h, N.u32ptr(nodes), N.i32ptr(comps), N.dptr(values),
+                                                      len(nodes)))
+
+    # -- actions -------------------------------------------------------------
+    def assemble(self, stream=None) -> None:
+        """ZeroLSS + LinearizeU + Assembly."""
+        N.check(self._lib.ufem_ns_assemble(self._h, _stream(stream)))
+
+    def apply_dirichlet(self, stream=None) -> None:
+        N.check(self._lib.ufem_ns_apply_dirichlet(self._h, _stream(stream)))
+
+    def solve(self, stream=None, raise_on_failure: bool = True, **krylov) -> dict:
+        st = N.KrylovStatus()
+        rc = self._lib.ufem_ns_solve(self._h, C.byref(krylov_options(**krylov)), C.byref(st), _stream(stream))
+        if rc != 0 and (raise_on_failure or rc != -7):
+            N.check(rc)
+        return st.as_dict()
+
+    def update(self, stream=None) -> None:
+        N.check(self._lib.ufem_ns_update(self._h, _stream(stream)))
+
+    def execute(self, stream=None, **krylov) -> dict:
+        """One time step (LSSAction::execute, LSSAction.cpp:122-135)."""
+        self.assemble(stream)
+        self.apply_dirichlet(stream)
+        st = self.solve(stream, **krylov)
+        self.update(stream)
+        return st
+
+    def step(self, nsteps: int, stream=None, **krylov) -> dict:
+        st = N.KrylovStatus()
+        N.check(self._lib.ufem_ns_step(self._h, nsteps, C.byref(krylov_options(**krylov)), C.byref(st),
+                                       _stream(stream)))
+        return st.as_dict()
+
+    # -- linear system access (LSS::System / Matrix) -------------------------
+    def csr(self):
+        rowptr = np.empty(self.nb_rows + 1, np.int64)
+        colidx = np.empty(self.nnz, np.int32)
+        N.check(self._lib.ufem_ns_csr(self._h, N.i64ptr(rowptr), N.i32ptr(colidx)))
+        return rowptr, colidx
+
+    def graph(self):
+        start = np.empty(self.nb_nodes + 1, np.int64)
+        adj = np.empty(self.block_nnz, np.uint32)
+        N.check(self._lib.ufem_ns_graph(self._h, N.i64ptr(start), N.u32ptr(adj)))
+        return start, adj
+
+    def system(self):
+        vals = np.empty(self.nnz)
+        rhs = np.empty(self.nb_rows)
+        N.check(self._lib.ufem_ns_get_system(self._h, N.dptr(vals), N.dptr(rhs)))
+        return vals, rhs
+
+    def apply(self, x: np.ndarray) -> np.ndarray:
+        x = np.ascontiguousarray(x, np.float64)
+        y = np.empty(self.nb_rows)
+        N.check(self._lib.ufem_ns_apply(self._h, N.dptr(x), N.dptr(y)))
+        return y
+
+    def device_view(self) -> dict:
+        v = N.DeviceView()
+        N.check(self._lib.ufem_ns_device_view_get(self._h, C.byref(v)))
+        return {k: getattr(v, k) for k, _ in v._fields_}
+
+    # -- timers (component timing of the reference) ----------------------------
+    def enable_timing(self, on: bool = True) -> None:
+        N.check(self._lib.ufem_ns_enable_timing(self._h, 1 if on else 0))
+
+    def timings(self) -> dict:
+        t = N.Timings()
+        N.check(self._lib.ufem_ns_get_timings(self._h, C.byref(t)))
+        return t.as_dict()
+
+    @property
+    def handle(self) -> C.c_void_p:
+        return self._h
+
+    def close(self) -> None:
+        if getattr(self, "_h", None):
+            self._lib.ufem_ns_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()

@@ -1,0 +1,197 @@
+/* ufem_b200.h -- C ABI of the B200-native UFEM Navier-Stokes hot path.
+ *
+ * Replaces, for P1 triangles and tetrahedra, the per-time-step pipeline of the
+ * reference's UFEM NavierStokes solver action and its Trilinos LSS fill:
+ *
+ *   ZeroLSS -> LinearizeU -> Assembly -> BoundaryConditions -> SolveLSS -> Update
+ *   (plugins/UFEM/src/UFEM/ns_implementation/NavierStokes.cpp:100-122,172-179)
+ *
+ * Conventions (identical to the reference):
+ *   - navier_stokes_solution field: N x neq doubles per node (u, v, [w], p),
+ *     neq = dim + 1 (Solver.cpp:358-464 creates it by tag; u before p).
+ *   - linearized_velocity field: N x 4*dim doubles per node (u_adv, u1, u2, u3).
+ *   - global dof = node*neq + comp; CSR row r = node*neq + eq holds the columns
+ *     adj(node)*neq + c for the sorted node neighbourhood adj(node) (self
+ *     included): the point form of the default FEVbr block matrix
+ *     (SparsityBuilder.cpp:157-189, TrilinosDetail.cpp:251-311).
+ *   - every function returns 0 on success and a negative UFEM_ERR_* code on
+ *     failure; ufem_last_error() gives a message (thread-local).  No C++
+ *     exception crosses this boundary.  There is no CPU fallback: if no
+ *     sm_100 device is present, ufem_ns_create fails with UFEM_ERR_CUDA.
+ *   - a handle owns all of its device memory; the caller owns host buffers.
+ *     One handle may be driven by one host thread at a time; distinct handles
+ *     are independent.  `stream` arguments are cudaStream_t values (NULL = the
+ *     legacy default stream).
+ */
+#ifndef UFEM_B200_H
+#define UFEM_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define UFEM_OK 0
+#define UFEM_ERR_ARG (-1)     /* invalid argument (cf3 BadValue / SetupError)   */
+#define UFEM_ERR_CUDA (-2)    /* CUDA runtime error or no usable device          */
+#define UFEM_ERR_MESH (-3)    /* invalid mesh: node id out of range, det J == 0  */
+#define UFEM_ERR_STATE (-4)   /* call out of order (e.g. assemble before state)  */
+#define UFEM_ERR_NOMEM (-5)   /* device allocation failed                         */
+#define UFEM_ERR_LIMIT (-6)   /* a node has more than 63 neighbours               */
+#define UFEM_ERR_SOLVE (-7)   /* Krylov solve failed (see ufem_krylov_status)     */
+
+/* Mesh: coords N x dim (row-major), conn E x (dim+1), host memory. */
+typedef struct ufem_mesh {
+  int32_t dim;          /* 2: Triag2D (LagrangeP1), 3: Tetra3D (LagrangeP1) */
+  int32_t reserved;
+  int64_t nb_nodes;
+  int64_t nb_elems;
+  const double* coords;
+  const uint32_t* conn;
+} ufem_mesh;
+
+/* Options of the NavierStokes action and its ComputeTauImpl
+ * (NavierStokes.cpp:74-98, SUPG.hpp:94-104, NavierStokesPhysics.cpp:24-91). */
+typedef struct ufem_ns_options {
+  double theta;                 /* theta-method coefficient, default 1      */
+  double dt;                    /* time step (LSSActionUnsteady::dt)       */
+  double rho;                   /* density; nu_eff is given per node        */
+  int32_t supg_type;            /* 0 tezduyar, 1 metric (default), 2 cf2    */
+  int32_t use_specializations;  /* 1 (reference default): closed-form P1    */
+  double c1, c2;                /* metric constants, default 1 and 16       */
+  double alpha_ps, alpha_su, alpha_bu;  /* tau scaling, default 1          */
+  double u_ref;                 /* cf2 reference velocity, default 1        */
+  int32_t precision;            /* 0: FP64 element arithmetic (plain drop-in)
+                                   1: FP32 element arithmetic, FP64 scatter */
+  int32_t reserved;
+} ufem_ns_options;
+
+/* Krylov options (SolveLSS / Belos GMRES replacement). */
+typedef struct ufem_krylov_opts {
+  int32_t method;      /* 0: GMRES(restart)  1: BiCGStab                          */
+  int32_t restart;     /* GMRES restart length, default 30                         */
+  int32_t max_iters;   /* total Krylov iterations (per refinement pass), 1000    */
+  int32_t precond;     /* 0 none, 1 point Jacobi (default), 2 node-block Jacobi   */
+  double tol;          /* ||b - A x|| / ||b|| target, default 1e-10                */
+  int32_t mixed;       /* 0: all FP64; 1: FP32 inner Krylov + FP64 refinement     */
+  int32_t max_refine;  /* outer refinement passes when mixed, default 20          */
+  double inner_tol;    /* relative tolerance of each inner FP32 solve, 1e-5       */
+} ufem_krylov_opts;
+
+typedef struct ufem_krylov_status {
+  int32_t converged;   /* 1 if ||b - A x|| / ||b|| <= tol (checked in FP64)       */
+  int32_t status;      /* 0 ok, 1 max iterations, 2 breakdown, 3 non-finite      */
+  int32_t iterations;  /* total Krylov iterations                                 */
+  int32_t refinements; /* outer FP64 refinement passes (mixed only)               */
+  double rel_residual; /* final FP64 ||b - A x|| / ||b||                          */
+} ufem_krylov_status;
+
+typedef struct ufem_ns_handle ufem_ns_handle;
+
+/* Phase timings of the last calls, milliseconds, from CUDA events recorded on
+ * the call's stream when timing is enabled (component timers of the
+ * reference, common/AllocatedComponent.cpp:24-80). */
+typedef struct ufem_ns_timings {
+  double linearize_ms;
+  double assembly_ms;     /* the row-owner assembly kernel alone */
+  double dirichlet_ms;
+  double solve_ms;
+  double update_ms;
+} ufem_ns_timings;
+
+/* Device pointers of the assembled system, for in-process consumers. */
+typedef struct ufem_ns_device_view {
+  const int64_t* rowptr;   /* nb_rows + 1 */
+  const int32_t* colidx;   /* nnz          */
+  const double* vals;      /* nnz          */
+  const double* rhs;       /* nb_rows      */
+  const double* solution;  /* nb_rows      */
+  int64_t nb_rows;
+  int64_t nnz;
+} ufem_ns_device_view;
+
+const char* ufem_last_error(void);
+const char* ufem_version(void);
+
+/* Fixture mesh generators (cf3/Tools/MeshGeneration/MeshGeneration.cpp:209-253
+ * for triangles; Kuhn 6-tet split for the cube).  Interior nodes are jittered by
+ * U(-jitter*h, +jitter*h) per coordinate from a counter-based hash of `seed`.
+ * coords: (nx+1)(ny+1) x 2 / (n+1)^3 x 3; conn: 2*nx*ny x 3 / 6n^3 x 4. */
+int ufem_mesh_rectangle_tris(int32_t nx, int32_t ny, double jitter, uint64_t seed, double* coords,
+                             uint32_t* conn);
+int ufem_mesh_cube_tets(int32_t n, double jitter, uint64_t seed, double* coords, uint32_t* conn);
+
+void ufem_ns_default_options(ufem_ns_options* opts);
+void ufem_krylov_default_opts(ufem_krylov_opts* opts);
+
+/* LSSAction::create_lss (LSSAction.cpp:137-153) + LSS::System::create
+ * (System.cpp:82-110): copies the mesh to the device, builds the node graph,
+ * the point CSR pattern and the row-owner assembly plan. */
+int ufem_ns_create(const ufem_mesh* mesh, const ufem_ns_options* opts, ufem_ns_handle** out);
+/* NavierStokes option triggers (trigger_assembly, NavierStokes.cpp:130-192). */
+int ufem_ns_set_options(ufem_ns_handle* h, const ufem_ns_options* opts);
+int ufem_ns_sizes(const ufem_ns_handle* h, int64_t* nb_rows, int64_t* nnz, int64_t* block_nnz);
+/* Host copies of the CSR pattern (rowptr nb_rows+1, colidx nnz). */
+int ufem_ns_csr(ufem_ns_handle* h, int64_t* rowptr, int32_t* colidx);
+/* Node graph (starting indices N+1, node connectivity block_nnz). */
+int ufem_ns_graph(ufem_ns_handle* h, int64_t* start, uint32_t* adj);
+
+/* Fields: up N x neq, lin N x 4*dim (u_adv, u1, u2, u3), nu N, force N x dim
+ * (NULL: zero body force).  Copies host -> device. */
+int ufem_ns_set_state(ufem_ns_handle* h, const double* up, const double* lin, const double* nu,
+                      const double* force);
+int ufem_ns_get_state(ufem_ns_handle* h, double* up, double* lin);
+/* Stream-ordered forms of the two calls above: the host buffers must stay valid
+ * (and, for an overlapping copy, be pinned) until `stream` reaches the copy. */
+int ufem_ns_upload_state(ufem_ns_handle* h, const double* up, const double* lin, const double* nu,
+                         const double* force, void* stream);
+int ufem_ns_download_state(ufem_ns_handle* h, double* up, double* lin, void* stream);
+/* The LSS solution vector (the increment; kept across steps like ZeroLSS
+ * with reset_solution=false). */
+int ufem_ns_set_solution(ufem_ns_handle* h, const double* sol);
+int ufem_ns_get_solution(ufem_ns_handle* h, double* sol);
+
+/* Constant Dirichlet conditions, applied in call order (BoundaryConditions
+ * node loops -> System::dirichlet(node, comp, new - old, symmetric),
+ * Proto/DirichletBC.hpp:34-51, TrilinosFEVbrMatrix.cpp:482-553). */
+int ufem_ns_clear_dirichlet(ufem_ns_handle* h);
+int ufem_ns_add_dirichlet(ufem_ns_handle* h, const uint32_t* nodes, int64_t n, int32_t comp,
+                          const double* values);
+/* Same, with a component per entry: lets a vector condition be listed node by
+ * node (u, v, [w] of each node in turn), the order DirichletBCSetter uses
+ * (Proto/DirichletBC.hpp:42-48). */
+int ufem_ns_add_dirichlet_dofs(ufem_ns_handle* h, const uint32_t* nodes, const int32_t* comps,
+                               const double* values, int64_t n);
+
+/* ZeroLSS + LinearizeU + Assembly (NavierStokesAssembly.hpp:27-75 or
+ * NavierStokesSpecializations.hpp:26-303).  Asynchronous on `stream`. */
+int ufem_ns_assemble(ufem_ns_handle* h, void* stream);
+/* BoundaryConditions: symmetric Dirichlet on the assembled system. */
+int ufem_ns_apply_dirichlet(ufem_ns_handle* h, void* stream);
+/* SolveLSS (SolveLSS.cpp:44-55): Krylov solve for the increment. */
+int ufem_ns_solve(ufem_ns_handle* h, const ufem_krylov_opts* kopts, ufem_krylov_status* status,
+                  void* stream);
+/* UpdateActions (NavierStokes.cpp:172-179). */
+int ufem_ns_update(ufem_ns_handle* h, void* stream);
+/* nsteps full time steps; status of the last solve. */
+int ufem_ns_step(ufem_ns_handle* h, int32_t nsteps, const ufem_krylov_opts* kopts,
+                 ufem_krylov_status* status, void* stream);
+
+/* Host copies of the assembled system (vals nnz, rhs nb_rows); either may be NULL. */
+int ufem_ns_get_system(ufem_ns_handle* h, double* vals, double* rhs);
+int ufem_ns_download_system(ufem_ns_handle* h, double* vals, double* rhs, void* stream);
+int ufem_ns_device_view_get(const ufem_ns_handle* h, ufem_ns_device_view* view);
+/* y = A x (FP64, host buffers) -- LSS::Matrix::apply with alpha=1, beta=0. */
+int ufem_ns_apply(ufem_ns_handle* h, const double* x, double* y);
+
+int ufem_ns_enable_timing(ufem_ns_handle* h, int32_t enable);
+int ufem_ns_get_timings(ufem_ns_handle* h, ufem_ns_timings* t);
+
+void ufem_ns_destroy(ufem_ns_handle* h);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* UFEM_B200_H */

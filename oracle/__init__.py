@@ -1,0 +1,288 @@
+"""FP64 CPU oracle of the UFEM Navier-Stokes step -- TEST INFRASTRUCTURE ONLY.
+
+Python binding of ``liboracle_ufem.so`` (``ufem_oracle.cpp``), the serial FP64
+restatement of the reference's assembly, symmetric Dirichlet, solve and update.
+Only ``tests/``, ``__graft_entry__.smoke()`` and ``bench.py``'s CPU-baseline
+leg may use it, and only as the checker or the timed CPU baseline; the product
+package never imports it.  Parity status: see the header of ufem_oracle.cpp.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "liboracle_ufem.so")
+
+_D = C.POINTER(C.c_double)
+_U32 = C.POINTER(C.c_uint32)
+_I32 = C.POINTER(C.c_int32)
+_I64 = C.POINTER(C.c_int64)
+
+
+class OrcOptions(C.Structure):
+    _fields_ = [("theta", C.c_double), ("dt", C.c_double), ("rho", C.c_double), ("supg_type", C.c_int32),
+                ("use_specializations", C.c_int32), ("c1", C.c_double), ("c2", C.c_double),
+                ("alpha_ps", C.c_double), ("alpha_su", C.c_double), ("alpha_bu", C.c_double),
+                ("u_ref", C.c_double), ("precision", C.c_int32), ("reserved", C.c_int32)]
+
+
+_SIG = {
+    "orc_mesh_rectangle_tris": (None, [C.c_int, C.c_int, C.c_double, C.c_uint64, _D, _U32]),
+    "orc_mesh_cube_tets": (None, [C.c_int, C.c_double, C.c_uint64, _D, _U32]),
+    "orc_create": (C.c_void_p, [C.c_int, C.c_int64, C.c_int64, _D, _U32, C.POINTER(OrcOptions)]),
+    "orc_destroy": (None, [C.c_void_p]),
+    "orc_create_lss": (C.c_void_p, [C.c_int64, C.c_int, _I64, _U32]),
+    "orc_set_row": (None, [C.c_void_p, C.c_int64, C.c_int, C.c_double, C.c_double]),
+    "orc_nrows": (C.c_int64, [C.c_void_p]),
+    "orc_set_options": (None, [C.c_void_p, C.POINTER(OrcOptions)]),
+    "orc_nnz": (C.c_int64, [C.c_void_p]),
+    "orc_block_nnz": (C.c_int64, [C.c_void_p]),
+    "orc_csr": (None, [C.c_void_p, _I64, _I32]),
+    "orc_graph": (None, [C.c_void_p, _I64, _U32]),
+    "orc_set_state": (None, [C.c_void_p, _D, _D, _D, _D]),
+    "orc_get_state": (None, [C.c_void_p, _D, _D]),
+    "orc_set_solution": (None, [C.c_void_p, _D]),
+    "orc_get_solution": (None, [C.c_void_p, _D]),
+    "orc_clear_dirichlet": (None, [C.c_void_p]),
+    "orc_add_dirichlet": (None, [C.c_void_p, _U32, C.c_int64, C.c_int, _D]),
+    "orc_add_dirichlet_dofs": (None, [C.c_void_p, _U32, _I32, _D, C.c_int64]),
+    "orc_assemble": (None, [C.c_void_p, C.c_int]),
+    "orc_apply_bcs": (None, [C.c_void_p]),
+    "orc_set_system": (None, [C.c_void_p, _D, _D]),
+    "orc_dirichlet": (None, [C.c_void_p, C.c_int64, C.c_int, C.c_double]),
+    "orc_get_system": (None, [C.c_void_p, _D, _D]),
+    "orc_solve": (C.c_int, [C.c_void_p, C.c_double, C.c_int, C.c_int, _I32, _D]),
+    "orc_update": (None, [C.c_void_p]),
+    "orc_step": (C.c_int, [C.c_void_p, C.c_int, C.c_double, C.c_int, C.c_int, C.c_int]),
+    "orc_time_assembly": (C.c_double, [C.c_void_p, C.c_int, C.c_int]),
+    "orc_element": (None, [C.c_void_p, C.c_int64, _D, _D, _D]),
+    "orc_tau": (None, [C.c_int, C.c_int, _D, _D, C.c_double, C.c_double, C.c_double, C.c_double, _D]),
+}
+
+_lib = None
+
+
+def lib() -> C.CDLL:
+    global _lib
+    if _lib is None:
+        src = os.path.join(HERE, "ufem_oracle.cpp")
+        if not os.path.exists(LIB_PATH) or os.path.getmtime(LIB_PATH) < os.path.getmtime(src):
+            subprocess.run(["make", "-s", "-C", HERE], check=True)
+        L = C.CDLL(LIB_PATH)
+        for name, (res, args) in _SIG.items():
+            fn = getattr(L, name)
+            fn.restype = res
+            fn.argtypes = args
+        _lib = L
+    return _lib
+
+
+def _d(a):
+    if a is None:
+        return None
+    assert a.dtype == np.float64 and a.flags.c_contiguous
+    return a.ctypes.data_as(_D)
+
+
+def options(dt=0.01, rho=1.0, theta=1.0, supg_type=1, use_specializations=True, c1=1.0, c2=16.0,
+            alpha_ps=1.0, alpha_su=1.0, alpha_bu=1.0, u_ref=1.0) -> OrcOptions:
+    o = OrcOptions()
+    o.theta, o.dt, o.rho = theta, dt, rho
+    o.supg_type = {"tezduyar": 0, "metric": 1, "cf2": 2}.get(supg_type, supg_type)
+    o.use_specializations = 1 if use_specializations else 0
+    o.c1, o.c2, o.alpha_ps, o.alpha_su, o.alpha_bu, o.u_ref = c1, c2, alpha_ps, alpha_su, alpha_bu, u_ref
+    return o
+
+
+def mesh_rectangle_tris(nx, ny, jitter, seed):
+    coords = np.empty(((nx + 1) * (ny + 1), 2))
+    conn = np.empty((2 * nx * ny, 3), np.uint32)
+    lib().orc_mesh_rectangle_tris(nx, ny, jitter, seed, _d(coords), conn.ctypes.data_as(_U32))
+    return coords, conn
+
+
+def mesh_cube_tets(n, jitter, seed):
+    coords = np.empty(((n + 1) ** 3, 3))
+    conn = np.empty((6 * n ** 3, 4), np.uint32)
+    lib().orc_mesh_cube_tets(n, jitter, seed, _d(coords), conn.ctypes.data_as(_U32))
+    return coords, conn
+
+
+def tau(dim, supg_type, X, uc, nu, dt, c1=1.0, c2=16.0):
+    X = np.ascontiguousarray(X, np.float64)
+    uc = np.ascontiguousarray(uc, np.float64)
+    out = np.empty(3)
+    lib().orc_tau(dim, supg_type, _d(X), _d(uc), nu, dt, c1, c2, _d(out))
+    return out  # tau_ps, tau_su, tau_bulk
+
+
+class LSS:
+    """A bare oracle linear system on a node graph (for LSS-level known answers)."""
+
+    def __init__(self, start, adj, neq):
+        start = np.ascontiguousarray(start, np.int64)
+        adj = np.ascontiguousarray(adj, np.uint32)
+        self.N = len(start) - 1
+        self.neq = neq
+        self._h = lib().orc_create_lss(self.N, neq, start.ctypes.data_as(_I64), adj.ctypes.data_as(_U32))
+        self.nnz = lib().orc_nnz(self._h)
+        self.nrows = lib().orc_nrows(self._h)
+
+    def set_row(self, blockrow, ieq, diag, offdiag):
+        lib().orc_set_row(self._h, blockrow, ieq, diag, offdiag)
+
+    def symmetric_dirichlet(self, blockrow, ieq, value):
+        lib().orc_dirichlet(self._h, blockrow, ieq, value)
+
+    def csr(self):
+        rp = np.empty(self.nrows + 1, np.int64)
+        ci = np.empty(self.nnz, np.int32)
+        lib().orc_csr(self._h, rp.ctypes.data_as(_I64), ci.ctypes.data_as(_I32))
+        return rp, ci
+
+    def system(self):
+        vals = np.empty(self.nnz)
+        rhs = np.empty(self.nrows)
+        lib().orc_get_system(self._h, _d(vals), _d(rhs))
+        return vals, rhs
+
+    def solution(self):
+        s = np.empty(self.nrows)
+        lib().orc_get_solution(self._h, _d(s))
+        return s
+
+    def dense(self):
+        rp, ci = self.csr()
+        vals, _ = self.system()
+        A = np.zeros((self.nrows, self.nrows))
+        for r in range(self.nrows):
+            A[r, ci[rp[r]:rp[r + 1]]] = vals[rp[r]:rp[r + 1]]
+        return A
+
+    def __del__(self):
+        if getattr(self, "_h", None):
+            lib().orc_destroy(self._h)
+            self._h = None
+
+
+class Oracle:
+    """Serial FP64 restatement of one NavierStokes action + its LSS."""
+
+    def __init__(self, coords, conn, opts: OrcOptions):
+        coords = np.ascontiguousarray(coords, np.float64)
+        conn = np.ascontiguousarray(conn, np.uint32)
+        self.dim = coords.shape[1]
+        self.neq = self.dim + 1
+        self.N = coords.shape[0]
+        self.E = conn.shape[0]
+        self.opts = opts
+        self._h = lib().orc_create(self.dim, self.N, self.E, _d(coords), conn.ctypes.data_as(_U32), C.byref(opts))
+        if not self._h:
+            raise ValueError("oracle: invalid mesh")
+        self.nnz = lib().orc_nnz(self._h)
+        self.block_nnz = lib().orc_block_nnz(self._h)
+        self.nrows = self.N * self.neq
+
+    def set_options(self, opts: OrcOptions):
+        self.opts = opts
+        lib().orc_set_options(self._h, C.byref(opts))
+
+    def csr(self):
+        rp = np.empty(self.nrows + 1, np.int64)
+        ci = np.empty(self.nnz, np.int32)
+        lib().orc_csr(self._h, rp.ctypes.data_as(_I64), ci.ctypes.data_as(_I32))
+        return rp, ci
+
+    def graph(self):
+        st = np.empty(self.N + 1, np.int64)
+        adj = np.empty(self.block_nnz, np.uint32)
+        lib().orc_graph(self._h, st.ctypes.data_as(_I64), adj.ctypes.data_as(_U32))
+        return st, adj
+
+    def set_state(self, up, lin, nu, force=None):
+        up = np.ascontiguousarray(up, np.float64)
+        lin = np.ascontiguousarray(lin, np.float64)
+        nu = np.ascontiguousarray(nu, np.float64)
+        f = None if force is None else np.ascontiguousarray(force, np.float64)
+        lib().orc_set_state(self._h, _d(up), _d(lin), _d(nu), _d(f))
+
+    def state(self):
+        up = np.empty((self.N, self.neq))
+        lin = np.empty((self.N, 4 * self.dim))
+        lib().orc_get_state(self._h, _d(up), _d(lin))
+        return up, lin
+
+    def set_solution(self, s):
+        lib().orc_set_solution(self._h, _d(np.ascontiguousarray(s, np.float64)))
+
+    def solution(self):
+        s = np.empty(self.nrows)
+        lib().orc_get_solution(self._h, _d(s))
+        return s
+
+    def add_dirichlet(self, nodes, comps, values):
+        nodes = np.ascontiguousarray(nodes, np.uint32)
+        comps = np.ascontiguousarray(np.broadcast_to(np.asarray(comps, np.int32), nodes.shape))
+        values = np.ascontiguousarray(np.broadcast_to(np.asarray(values, np.float64), nodes.shape))
+        lib().orc_add_dirichlet_dofs(self._h, nodes.ctypes.data_as(_U32), comps.ctypes.data_as(_I32), _d(values),
+                                     len(nodes))
+
+    def clear_dirichlet(self):
+        lib().orc_clear_dirichlet(self._h)
+
+    def assemble(self, nthreads: int = 1):
+        lib().orc_assemble(self._h, nthreads)
+
+    def apply_dirichlet(self):
+        lib().orc_apply_bcs(self._h)
+
+    def set_system(self, vals, rhs):
+        lib().orc_set_system(self._h, _d(np.ascontiguousarray(vals, np.float64)),
+                             _d(np.ascontiguousarray(rhs, np.float64)))
+
+    def dirichlet(self, node, comp, value):
+        lib().orc_dirichlet(self._h, node, comp, value)
+
+    def system(self):
+        vals = np.empty(self.nnz)
+        rhs = np.empty(self.nrows)
+        lib().orc_get_system(self._h, _d(vals), _d(rhs))
+        return vals, rhs
+
+    def solve(self, tol=1e-13, maxit=5000, restart=60):
+        it = C.c_int32()
+        rr = C.c_double()
+        rc = lib().orc_solve(self._h, tol, maxit, restart, C.byref(it), C.byref(rr))
+        return {"rc": rc, "iterations": it.value, "rel_residual": rr.value}
+
+    def update(self):
+        lib().orc_update(self._h)
+
+    def step(self, nsteps=1, tol=1e-13, maxit=5000, restart=60, nthreads=1):
+        return lib().orc_step(self._h, nsteps, tol, maxit, restart, nthreads)
+
+    def time_assembly(self, nthreads=1, reps=1) -> float:
+        return lib().orc_time_assembly(self._h, nthreads, reps)
+
+    def element(self, e):
+        nd = (self.dim + 1) ** 2
+        A = np.empty((nd, nd))
+        T = np.empty((nd, nd))
+        a = np.empty(nd)
+        lib().orc_element(self._h, e, _d(A), _d(T), _d(a))
+        return A, T, a
+
+    def close(self):
+        if self._h:
+            lib().orc_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
