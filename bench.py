@@ -329,20 +329,31 @@ def time_steps(ns, pb, args, stream, sptr):
         ns.set_solution(np.zeros(ns.nb_rows))
         lat = []
         iters = []
-        for k in range(args.time_steps):
-            torch.cuda.synchronize()
-            t0 = time.perf_counter()
-            st = ns.execute(sptr, tol=1e-10, max_iters=3000, **kw)
-            torch.cuda.synchronize()
-            lat.append((time.perf_counter() - t0) * 1e3)
-            iters.append(st["iterations"])
+        st = {"converged": 0}
+        try:
+            for k in range(args.time_steps):
+                torch.cuda.synchronize()
+                t0 = time.perf_counter()
+                ns.assemble(sptr)
+                ns.apply_dirichlet(sptr)
+                st = ns.solve(sptr, raise_on_failure=False, tol=1e-10, max_iters=3000, **kw)
+                ns.update(sptr)
+                torch.cuda.synchronize()
+                lat.append((time.perf_counter() - t0) * 1e3)
+                iters.append(st["iterations"])
+                if not st["converged"]:
+                    break
+        except Exception as exc:  # reported, not fatal: the assembly metric above stands
+            out[label] = {"error": str(exc)}
+            continue
         up, _ = ns.state()
         results[label] = up
         out[label] = {"steps_per_s": round(1e3 / float(np.mean(lat)), 3), "p50_ms": round(float(np.median(lat)), 2),
                       "max_ms": round(float(np.max(lat)), 2), "krylov_iters": iters,
-                      "converged": int(st["converged"])}
-    ref = results["plain_fp64"]
-    out["mixed"]["rel_err_vs_plain"] = float(np.linalg.norm(results["mixed"] - ref) / np.linalg.norm(ref))
+                      "converged": int(st["converged"]), "status": int(st.get("status", -1))}
+    if "plain_fp64" in results and "mixed" in results:
+        ref = results["plain_fp64"]
+        out["mixed"]["rel_err_vs_plain"] = float(np.linalg.norm(results["mixed"] - ref) / np.linalg.norm(ref))
     out["steps"] = args.time_steps
     ns.set_state(base_up, pb.lin, pb.nu)
     return out

@@ -31,15 +31,17 @@ struct P1 {
 
 template <typename T>
 struct KParams {
-  T theta, dt, invdt, rho, c1, c2, a_ps, a_su, a_bu, u_ref;
+  T theta, inv_theta, dt, invdt, rho, inv_rho, c2, a_ps, a_su, a_bu, u_ref;
+  T tau_c1, tau_std, two_dt;  // 4 c1^2 / dt^2, 4 / dt^2, 2 / dt (computed on the host in FP64)
   int supg_type, has_force;
 };
 
 template <typename T>
 __device__ __forceinline__ KParams<T> make_kparams(const NSParams& p) {
   KParams<T> k;
-  k.theta = T(p.theta); k.dt = T(p.dt); k.invdt = T(p.invdt); k.rho = T(p.rho);
-  k.c1 = T(p.c1); k.c2 = T(p.c2); k.a_ps = T(p.a_ps); k.a_su = T(p.a_su); k.a_bu = T(p.a_bu);
+  k.theta = T(p.theta); k.inv_theta = T(p.inv_theta); k.dt = T(p.dt); k.invdt = T(p.invdt); k.rho = T(p.rho);
+  k.inv_rho = T(p.inv_rho); k.tau_c1 = T(p.tau_c1); k.tau_std = T(p.tau_std); k.two_dt = T(p.two_dt);
+  k.c2 = T(p.c2); k.a_ps = T(p.a_ps); k.a_su = T(p.a_su); k.a_bu = T(p.a_bu);
   k.u_ref = T(p.u_ref); k.supg_type = p.supg_type; k.has_force = p.has_force;
   return k;
 }
@@ -124,13 +126,42 @@ __device__ __forceinline__ void gather_geometry_uadv(const int (&ids)[4], const 
   }
 }
 
-// ComputeTauImpl::compute_coefficients (SUPG.hpp:140-219).  Ji/det are the
-// element's (constant) Jacobian inverse and determinant.
+// Metric tensor of the METRIC tau, g = J^-T J^-1 = [grad xi_m . grad xi_n], in
+// the reference frame of the element's OWN node order (xi_m is the shape
+// function of original local node m+1).  The caller has relabelled the nodes
+// (row node first): original local node k sits at position k ^ a (tetrahedra)
+// or (k - a) mod 3 (triangles), and G holds the gradients in the relabelled
+// order.  g depends on the node order, so it is rebuilt from the original one.
 template <int D, typename T>
-__device__ __forceinline__ void compute_tau(int type, T c1, T c2, T u_ref, T a_ps, T a_su, T a_bu,
-                                            const Elem<D, T>& el, const T (&uc)[D], T element_nu, T dt,
-                                            const T (&Ji)[D][D], T det, T& tps, T& tsu, T& tbu) {
+__device__ __forceinline__ void metric_tensor(const T (&G)[D][D + 1], int a, T (&g)[D][D]) {
+  T col[D][D];
+#pragma unroll
+  for (int m = 0; m < D; ++m) {
+    const int k = m + 1;
+    const int pos = (D == 3) ? (k ^ a) : ((k - a + 3) % 3);
+#pragma unroll
+    for (int r = 0; r < D; ++r) col[m][r] = sel<D + 1>(G[r], pos);
+  }
+#pragma unroll
+  for (int m = 0; m < D; ++m)
+#pragma unroll
+    for (int q = 0; q < D; ++q) {
+      T s = 0;
+#pragma unroll
+      for (int r = 0; r < D; ++r) s += col[m][r] * col[q][r];
+      g[m][q] = s;
+    }
+}
+
+// ComputeTauImpl::compute_coefficients (SUPG.hpp:140-219).  G: node gradients
+// (any order), g: metric tensor in the element's own frame, det: det J.
+template <int D, typename T>
+__device__ __forceinline__ void compute_tau(const KParams<T>& kp, const Elem<D, T>& el, const T (&uc)[D],
+                                            T element_nu, const T (&G)[D][D + 1], const T (&g)[D][D], T det,
+                                            T& tps, T& tsu, T& tbu) {
   constexpr int n = D + 1;
+  const int type = kp.supg_type;
+  const T c2 = kp.c2, u_ref = kp.u_ref, dt = kp.dt;
   if (type == 0) {  // TEZDUYAR
     T h = T(1e10);
 #pragma unroll
@@ -148,20 +179,10 @@ __device__ __forceinline__ void compute_tau(int type, T c1, T c2, T u_ref, T a_p
 #pragma unroll
     for (int k = 0; k < D; ++k) um2 += uc[k] * uc[k];
     const T umag = tsqrt(um2);
-    tsu = T(1) / ((T(2) * umag) / h + T(2) / dt + (T(4) * element_nu) / (h * h));
+    tsu = T(1) / ((T(2) * umag) / h + kp.two_dt + (T(4) * element_nu) / (h * h));
     tps = tsu;
     tbu = tsu * umag * umag;
   } else if (type == 1) {  // METRIC
-    T g[D][D];
-#pragma unroll
-    for (int a = 0; a < D; ++a)
-#pragma unroll
-      for (int b = 0; b < D; ++b) {
-        T s = 0;
-#pragma unroll
-        for (int k = 0; k < D; ++k) s += Ji[k][a] * Ji[k][b];
-        g[a][b] = s;
-      }
     T adv = 0, sq = 0, tr = 0;
 #pragma unroll
     for (int b = 0; b < D; ++b) {
@@ -178,9 +199,9 @@ __device__ __forceinline__ void compute_tau(int type, T c1, T c2, T u_ref, T a_p
     }
     const T adv_sq = tabs(adv);
     const T diff = element_nu * element_nu * sq;
-    tsu = T(1) / tsqrt((T(4) * c1 * c1 / (dt * dt)) + adv_sq + c2 * diff);
+    tsu = T(1) / tsqrt(kp.tau_c1 + adv_sq + c2 * diff);  // tau_c1 = 4 c1^2 / dt^2
     tps = tsu;
-    const T tsu_std = T(1) / tsqrt((T(4) / (dt * dt)) + adv_sq + T(16) * diff);
+    const T tsu_std = T(1) / tsqrt(kp.tau_std + adv_sq + T(16) * diff);  // tau_std = 4 / dt^2
     tbu = (T(1) / tsu_std) / tr;
   } else {  // CF2
     const T volume = (D == 2) ? det / T(2) : det / T(6);
@@ -202,18 +223,7 @@ __device__ __forceinline__ void compute_tau(int type, T c1, T c2, T u_ref, T a_p
       for (int b = 0; b <= D; ++b) {
         T t = 0;
 #pragma unroll
-        for (int k = 0; k < D; ++k) {
-          T gkb;
-          if (b == 0) {
-            T q = 0;
-#pragma unroll
-            for (int m = 0; m < D; ++m) q += Ji[k][m] * T(-1);
-            gkb = q;
-          } else {
-            gkb = Ji[k][b - 1];
-          }
-          t += uc[k] * gkb;
-        }
+        for (int k = 0; k < D; ++k) t += uc[k] * G[k][b];
         s += t;
       }
       const T h = T(2) * umag / s;
@@ -223,9 +233,9 @@ __device__ __forceinline__ void compute_tau(int type, T c1, T c2, T u_ref, T a_p
       tsu = T(1) / (T(1) / tau_adv + T(1) / tau_time + T(1) / tau_diff);
     }
   }
-  tps *= a_ps;
-  tsu *= a_su;
-  tbu *= a_bu;
+  tps *= kp.a_ps;
+  tsu *= kp.a_su;
+  tbu *= kp.a_bu;
 }
 
 template <int D, typename T>
@@ -276,7 +286,7 @@ __device__ __forceinline__ void stage_block(const T (&A)[D + 1][D + 1], const T 
     rhs[r] += s;
 #pragma unroll
     for (int c = 0; c < neq; ++c) {
-      const T a = (r == D) ? A[r][c] / kp.theta : A[r][c];
+      const T a = (r == D) ? A[r][c] * kp.inv_theta : A[r][c];  // _A(p) / theta
       st[((b * neq + r) * neq + c) * CH] = kp.invdt * Tm[r][c] + kp.theta * a;
     }
   }
@@ -291,10 +301,23 @@ __device__ __forceinline__ void load_state(const double* __restrict__ state, int
 }
 
 // ---------------------------------------------------------------------------
-// Generic expression (NavierStokesAssembly.hpp:51-67) through the order-2
-// quadrature of Proto/ElementIntegration.hpp:236-258, for row node a.  Because
-// the P1 gradient G is constant, the q-sums are accumulated in factored form
-// (sum_q W f_q) * G, which is the same quadrature.
+// Generic expression (NavierStokesAssembly.hpp:51-67) for the row node, which
+// the caller has placed at local position 0.  The reference integrates it with
+// the order-2 Gauss rule (Proto/ElementIntegration.hpp:236-258, weight
+// w_q det J).  For P1 elements the gradients G are constant and every integrand
+// is a polynomial of degree <= 2 in the barycentric coordinates, which that
+// rule integrates exactly, so the sums are evaluated here in closed form with
+//   int N_k = m1 = V/n,   int N_k N_l = m2 (1 + d_kl),   m2 = V/(n(n+1)),
+// c_kb = U_k . G_b (U: nodal u_adv), ubar = mean U, alpha_b = ubar . G_b,
+// w_k = c_k0 and q = sum_k w_k U_k:
+//   int adv_b          = V alpha_b
+//   int N_0 adv_b      = m2 (n alpha_b + c_0b)
+//   int adv_0 adv_b    = m2 (n^2 alpha_0 alpha_b + q . G_b)
+//   int adv_0 N_b      = m2 (n alpha_0 + w_b)
+//   int ua_i S_0       = m2 (n ubar_i + U_0i) + tau_su m2 (n^2 ubar_i alpha_0 + q_i)
+//   int S_0 g_i        = m2 (n gbar_i + g_0i) + tau_su m2 (n^2 gbar_i alpha_0 + sum_k w_k g_ki)
+// (tests/test_gpu_parity.py checks the result against the oracle's literal
+// quadrature).
 // ---------------------------------------------------------------------------
 template <int D, typename T>
 __device__ __forceinline__ void generic_row(const int (&ids)[4], int a, const double* __restrict__ coords,
@@ -302,22 +325,28 @@ __device__ __forceinline__ void generic_row(const int (&ids)[4], int a, const do
                                             const double* __restrict__ force, const KParams<T>& kp,
                                             T* __restrict__ st, T* __restrict__ rst, int CH) {
   constexpr int n = D + 1, neq = D + 1;
+  const T inv_n = T(1.0 / n);
+  const T nT = T(n), n2 = T(n * n);
   Elem<D, T> el;
   gather_geometry_uadv<D, T>(ids, coords, uadv, el);
-  // tau from u_adv at the centroid, element_nu = |mean nodal nu| (SUPG.hpp:110-116)
+  // tau inputs: |mean nodal nu| and u_adv at the centroid (SUPG.hpp:110-116, 145-147)
   T nsum = 0;
 #pragma unroll
   for (int b = 0; b < n; ++b) nsum += el.NU[b];
-  const T element_nu = tabs(nsum / T(n));
+  const T nu_bar = nsum * inv_n;
   T Nc[n];
   centroid_N<D, T>(Nc);
-  T uc[D];
+  T uc[D], ub[D];
 #pragma unroll
   for (int k = 0; k < D; ++k) {
-    T s = 0;
+    T s = 0, m = 0;
 #pragma unroll
-    for (int b = 0; b < n; ++b) s += Nc[b] * el.U[b][k];
+    for (int b = 0; b < n; ++b) {
+      s += Nc[b] * el.U[b][k];
+      m += el.U[b][k];
+    }
     uc[k] = s;
+    ub[k] = m * inv_n;
   }
   T J[D][D], Ji[D][D], det;
 #pragma unroll
@@ -325,9 +354,6 @@ __device__ __forceinline__ void generic_row(const int (&ids)[4], int a, const do
 #pragma unroll
     for (int c = 0; c < D; ++c) J[r][c] = el.Xr[r + 1][c];
   inverse_det<T>(J, Ji, det);
-  T tps, tsu, tbu;
-  compute_tau<D, T>(kp.supg_type, kp.c1, kp.c2, kp.u_ref, kp.a_ps, kp.a_su, kp.a_bu, el, uc, element_nu, kp.dt, Ji,
-                    det, tps, tsu, tbu);
   T G[D][n];
 #pragma unroll
   for (int r = 0; r < D; ++r) {
@@ -338,19 +364,48 @@ __device__ __forceinline__ void generic_row(const int (&ids)[4], int a, const do
 #pragma unroll
     for (int b = 1; b <= D; ++b) G[r][b] = Ji[r][b - 1];
   }
-  T Ga[D];
-#pragma unroll
-  for (int k = 0; k < D; ++k) Ga[k] = sel<n>(G[k], a);
-  T Da[n];
+  T g[D][D];
+  metric_tensor<D, T>(G, a, g);
+  T tps, tsu, tbu;
+  compute_tau<D, T>(kp, el, uc, tabs(nu_bar), G, g, det, tps, tsu, tbu);
+  const T V = det * T(D == 2 ? 0.5 : 1.0 / 6.0);
+  const T m1 = V * inv_n;
+  const T m2 = V * T(1.0 / (n * (n + 1)));
+  T alpha[n], w[n], c0[n], D0[n];
 #pragma unroll
   for (int b = 0; b < n; ++b) {
+    T a = 0, ww = 0, cc = 0, dd = 0;
+#pragma unroll
+    for (int k = 0; k < D; ++k) {
+      a += ub[k] * G[k][b];
+      ww += el.U[b][k] * G[k][0];
+      cc += el.U[0][k] * G[k][b];
+      dd += G[k][0] * G[k][b];
+    }
+    alpha[b] = a;
+    w[b] = ww;
+    c0[b] = cc;
+    D0[b] = dd;
+  }
+  T q[D];
+#pragma unroll
+  for (int i = 0; i < D; ++i) {
     T s = 0;
 #pragma unroll
-    for (int k = 0; k < D; ++k) s += Ga[k] * G[k][b];
-    Da[b] = s;
+    for (int k = 0; k < n; ++k) s += w[k] * el.U[k][i];
+    q[i] = s;
   }
-  T F[n][D];
+  const T tsum2 = tsu * m2;
+  const T sWS = m1 + tsu * V * alpha[0];
+  const T sWSp = m1 + T(0.5) * tps * V * alpha[0];
+  T gam[D], au[D];
+#pragma unroll
+  for (int i = 0; i < D; ++i) {
+    gam[i] = tbu * V * G[i][0] + T(0.5) * (m2 * (nT * ub[i] + el.U[0][i]) + tsum2 * (n2 * ub[i] * alpha[0] + q[i]));
+    au[i] = 0;
+  }
   if (kp.has_force) {
+    T F[n][D];
 #pragma unroll
     for (int b = 0; b < n; ++b) {
       double f[4];
@@ -358,98 +413,85 @@ __device__ __forceinline__ void generic_row(const int (&ids)[4], int a, const do
 #pragma unroll
       for (int k = 0; k < D; ++k) F[b][k] = T(f[k]);
     }
-  } else {
-#pragma unroll
-    for (int b = 0; b < n; ++b)
-#pragma unroll
-      for (int k = 0; k < D; ++k) F[b][k] = 0;
-  }
-  const T wq = (D == 2) ? T(1.0 / 6.0) : T(0.04166666666666666666666666666666666667);
-  const T W = wq * det;
-  T sW = 0, sWSp = 0, sWS = 0, gam[D], sWadv[n], sWN[n], Kd[n], Tuu[n], au[D];
-#pragma unroll
-  for (int k = 0; k < D; ++k) { gam[k] = 0; au[k] = 0; }
-#pragma unroll
-  for (int b = 0; b < n; ++b) { sWadv[b] = 0; sWN[b] = 0; Kd[b] = 0; Tuu[b] = 0; }
-#pragma unroll
-  for (int q = 0; q < n; ++q) {  // n Gauss points for both triangles (3) and tetrahedra (4)
-    T N[n];
-    gauss_N<D, T>(q, N);
-    T ua[D], gq[D], nuq = 0;
-#pragma unroll
-    for (int k = 0; k < D; ++k) {
-      T s = 0, f = 0;
-#pragma unroll
-      for (int b = 0; b < n; ++b) { s += N[b] * el.U[b][k]; f += N[b] * F[b][k]; }
-      ua[k] = s;
-      gq[k] = f;
-    }
-#pragma unroll
-    for (int b = 0; b < n; ++b) nuq += N[b] * el.NU[b];
-    T adv[n];
-#pragma unroll
-    for (int b = 0; b < n; ++b) {
-      T s = 0;
-#pragma unroll
-      for (int k = 0; k < D; ++k) s += ua[k] * G[k][b];
-      adv[b] = s;
-    }
-    const T Na = sel<n>(N, a), adva = sel<n>(adv, a);
-    const T Sa = Na + tsu * adva;
-    const T Spa = Na + tps * adva * T(0.5);
-    sW += W;
-    sWSp += W * Spa;
-    sWS += W * Sa;
-#pragma unroll
-    for (int k = 0; k < D; ++k) {
-      gam[k] += W * (tbu * Ga[k] + T(0.5) * ua[k] * Sa);
-      au[k] += W * (Sa * gq[k]);
-    }
-#pragma unroll
-    for (int b = 0; b < n; ++b) {
-      sWadv[b] += W * adv[b];
-      sWN[b] += W * N[b];
-      Kd[b] += W * (nuq * Da[b] + Sa * adv[b]);
-      Tuu[b] += W * (Sa * N[b]);
-    }
-  }
-  T rhs[neq];
-#pragma unroll
-  for (int k = 0; k < D; ++k) rhs[k] = au[k];
-  rhs[D] = 0;
-#pragma unroll
-  for (int b = 0; b < n; ++b) {
-    T A[neq][neq], Tm[neq][neq];
 #pragma unroll
     for (int i = 0; i < D; ++i) {
+      T gs = 0, gw = 0;
 #pragma unroll
-      for (int j = 0; j < D; ++j) {
-        A[i][j] = (i == j ? Kd[b] : T(0)) + gam[i] * G[j][b];
-        Tm[i][j] = (i == j) ? Tuu[b] : T(0);
+      for (int k = 0; k < n; ++k) {
+        gs += F[k][i];
+        gw += w[k] * F[k][i];
       }
-      A[i][D] = G[i][b] * sWS / kp.rho;
-      Tm[i][D] = 0;
-      A[D][i] = G[i][b] * sWSp + tps * Ga[i] * sWadv[b];
-      Tm[D][i] = tps * Ga[i] * sWN[b];
+      const T gbar = gs * inv_n;
+      au[i] = m2 * (nT * gbar + F[0][i]) + tsum2 * (n2 * gbar * alpha[0] + gw);
     }
-    A[D][D] = tps * Da[b] / kp.rho * sW;
-    Tm[D][D] = 0;
-    T xb[neq];
-    load_state<D, T>(state, ids[b], xb);
-    stage_block<D, T>(A, Tm, xb, kp, rhs, st, b, CH);
   }
+  // nodal state (u, p) of the element: A x for the RHS
+  T xs[n][neq];
 #pragma unroll
-  for (int r = 0; r < neq; ++r) rst[r * CH] = rhs[r];
+  for (int b = 0; b < n; ++b) load_state<D, T>(state, ids[b], xs[b]);
+  T div = 0, gradp[D], kx[D], ax[D];
+#pragma unroll
+  for (int i = 0; i < D; ++i) {
+    gradp[i] = 0;
+    kx[i] = 0;
+    ax[i] = 0;
+  }
+  const T theta = kp.theta, invdt = kp.invdt, inv_rho = kp.inv_rho;
+#pragma unroll
+  for (int b = 0; b < n; ++b) {
+    const T Kd = nu_bar * V * D0[b] + m2 * (nT * alpha[b] + c0[b]);
+    T qg = 0;
+#pragma unroll
+    for (int k = 0; k < D; ++k) qg += q[k] * G[k][b];
+    const T Kdb = Kd + tsum2 * (n2 * alpha[0] * alpha[b] + qg);
+    const T Tuu = m2 * (b == 0 ? T(2) : T(1)) + tsum2 * (nT * alpha[0] + w[b]);
+    const T Vab = V * alpha[b];
+    // rows u_i: M = invdt*T + theta*A
+    const T diag = theta * Kdb + invdt * Tuu;
+#pragma unroll
+    for (int i = 0; i < D; ++i) {
+      const T tg = theta * gam[i];
+#pragma unroll
+      for (int j = 0; j < D; ++j)
+        st[((b * neq + i) * neq + j) * CH] = tg * G[j][b] + (i == j ? diag : T(0));
+      st[((b * neq + i) * neq + D) * CH] = theta * (G[i][b] * sWS * inv_rho);
+    }
+    // row p: theta * (A / theta) + invdt * T = A + invdt * T
+#pragma unroll
+    for (int j = 0; j < D; ++j)
+      st[((b * neq + D) * neq + j) * CH] = G[j][b] * sWSp + tps * G[j][0] * Vab + invdt * (tps * G[j][0] * m1);
+    st[((b * neq + D) * neq + D) * CH] = tps * D0[b] * inv_rho * V;
+    // pieces of A x
+#pragma unroll
+    for (int k = 0; k < D; ++k) {
+      div += G[k][b] * xs[b][k];
+      gradp[k] += G[k][b] * xs[b][D];
+      kx[k] += Kdb * xs[b][k];
+      ax[k] += Vab * xs[b][k];
+    }
+  }
+  // rhs row 0 = a - A x  (A before the theta combination)
+#pragma unroll
+  for (int i = 0; i < D; ++i) rst[i * CH] = au[i] - (kx[i] + gam[i] * div + sWS * inv_rho * gradp[i]);
+  T g0ax = 0, g0gp = 0;
+#pragma unroll
+  for (int k = 0; k < D; ++k) {
+    g0ax += G[k][0] * ax[k];
+    g0gp += G[k][0] * gradp[k];
+  }
+  rst[D * CH] = -(sWSp * div + tps * g0ax + tps * V * inv_rho * g0gp);
 }
 
 // ---------------------------------------------------------------------------
-// Specialised triangles, NavierStokesSpecializations.hpp:37-147, row i = a.
+// Specialised triangles, NavierStokesSpecializations.hpp:37-147, for the row
+// node at local position 0 (ai: the relabel key, used by the metric tau only).
 // Each entry receives its terms in the reference's order.
 // ---------------------------------------------------------------------------
 template <int D, typename T>
-__device__ __forceinline__ void spec_tau_common(const Elem<D, T>& el, const double* __restrict__ state,
-                                                const int (&ids)[4], T nu, T dt, T& tps, T& tsu, T& tbu) {
-  // default ComputeTauImpl: METRIC, c1 = 1, c2 = 16, alphas 1, on the solution velocity u
+__device__ __forceinline__ void spec_tau_common(const KParams<T>& kp, const Elem<D, T>& el, int a,
+                                                const double* __restrict__ state, const int (&ids)[4], T nu,
+                                                T& tps, T& tsu, T& tbu) {
+  // tau of the solution velocity u
   constexpr int n = D + 1;
   T Nc[n];
   centroid_N<D, T>(Nc);
@@ -469,7 +511,25 @@ __device__ __forceinline__ void spec_tau_common(const Elem<D, T>& el, const doub
 #pragma unroll
     for (int c = 0; c < D; ++c) J[r][c] = el.Xr[r + 1][c];
   inverse_det<T>(J, Ji, det);
-  compute_tau<D, T>(1, T(1), T(16), T(1), T(1), T(1), T(1), el, uc, nu, dt, Ji, det, tps, tsu, tbu);
+  T G[D][D + 1];
+#pragma unroll
+  for (int r = 0; r < D; ++r) {
+    T s = 0;
+#pragma unroll
+    for (int k = 0; k < D; ++k) s += Ji[r][k] * T(-1);
+    G[r][0] = s;
+#pragma unroll
+    for (int b = 1; b <= D; ++b) G[r][b] = Ji[r][b - 1];
+  }
+  T g[D][D];
+  metric_tensor<D, T>(G, a, g);
+  // a default ComputeTauImpl: METRIC, c1 = 1 (4 c1^2 / dt^2 = 4 / dt^2), c2 = 16, alphas 1
+  KParams<T> dk = kp;
+  dk.supg_type = 1;
+  dk.c2 = T(16);
+  dk.tau_c1 = kp.tau_std;
+  dk.a_ps = dk.a_su = dk.a_bu = T(1);
+  compute_tau<D, T>(dk, el, uc, nu, G, g, det, tps, tsu, tbu);
 }
 
 template <typename T>
@@ -498,8 +558,8 @@ __device__ __forceinline__ void spec_tri_row(const int (&ids)[4], int ai, const 
   nx[1] = X[2][1] - X[0][1]; ny[1] = X[0][0] - X[2][0];
   nx[2] = X[0][1] - X[1][1]; ny[2] = X[1][0] - X[0][0];
   T tau_ps, tau_su, tau_bulk;
-  spec_tau_common<2, T>(el, state, ids, nu, kp.dt, tau_ps, tau_su, tau_bulk);
-  const T nix = sel<3>(nx, ai), niy = sel<3>(ny, ai);
+  spec_tau_common<2, T>(kp, el, ai, state, ids, nu, tau_ps, tau_su, tau_bulk);
+  const T nix = nx[0], niy = ny[0];  // row node at local position 0
   const T u_ni = u_avg[0] * nix + u_avg[1] * niy;
   const T rho = kp.rho;
   T rhs[3] = {0, 0, 0};
@@ -539,7 +599,7 @@ __device__ __forceinline__ void spec_tri_row(const int (&ids)[4], int ai, const 
     val = tau_bulk / (T(4) * volume);
     A[0][0] += val * nix * nx[j]; A[0][1] += val * nix * ny[j];
     A[1][0] += val * niy * nx[j]; A[1][1] += val * niy * ny[j];
-    val = volume / T(12) * (T(1) + (ai == j ? T(1) : T(0)));
+    val = volume / T(12) * (T(1) + (j == 0 ? T(1) : T(0)));
     val += tau_su / T(6) * u_ni;
     Tm[0][0] += val; Tm[1][1] += val;
     val = tau_ps / T(6);
@@ -596,12 +656,12 @@ __device__ __forceinline__ void spec_tet_row(const int (&ids)[4], int ai, const 
   nr[3][YY] = ((X[1][ZZ]-X[0][ZZ])*(X[2][XX]-X[0][XX]) - (X[2][ZZ]-X[0][ZZ])*(X[1][XX]-X[0][XX])) / T(2);
   nr[3][ZZ] = ((X[1][XX]-X[0][XX])*(X[2][YY]-X[0][YY]) - (X[2][XX]-X[0][XX])*(X[1][YY]-X[0][YY])) / T(2);
   T tau_ps, tau_su, tau_bulk;
-  spec_tau_common<3, T>(el, state, ids, nu, kp.dt, tau_ps, tau_su, tau_bulk);
+  spec_tau_common<3, T>(kp, el, ai, state, ids, nu, tau_ps, tau_su, tau_bulk);
   T ni[3];
 #pragma unroll
   for (int k = 0; k < 3; ++k) {
     T col[4] = {nr[0][k], nr[1][k], nr[2][k], nr[3][k]};
-    ni[k] = sel<4>(col, ai);
+    ni[k] = col[0];  // row node at local position 0
   }
   const T u_ni = u_avg[XX] * ni[XX] + u_avg[YY] * ni[YY] + u_avg[ZZ] * ni[ZZ];
   const T rho = kp.rho;
@@ -656,7 +716,7 @@ __device__ __forceinline__ void spec_tet_row(const int (&ids)[4], int ai, const 
     A[1][1] += val * ni[YY] * nj[YY]; A[1][2] += val * ni[YY] * nj[ZZ];
     A[2][0] += val * ni[ZZ] * nj[XX]; A[2][1] += val * ni[ZZ] * nj[YY];
     A[2][2] += val * ni[ZZ] * nj[ZZ];
-    val = volume / T(20) * (T(1) + (ai == j ? T(1) : T(0)));
+    val = volume / T(20) * (T(1) + (j == 0 ? T(1) : T(0)));
     val += tau_su / T(12) * u_ni;
     Tm[0][0] += val; Tm[1][1] += val; Tm[2][2] += val;
     val = tau_ps / T(12);
@@ -669,9 +729,15 @@ __device__ __forceinline__ void spec_tet_row(const int (&ids)[4], int ai, const 
   for (int r = 0; r < 4; ++r) rst[r * CH] = rhs[r];
 }
 
+// Shared memory of one chunk: staged row blocks [value][incidence] (T), staged
+// RHS rows, the permuted slot word of every incidence, per-row offsets, and one
+// 64-bit contributor mask per (row, neighbour slot).
 template <int D, typename T, int CH>
 constexpr size_t assembly_smem_bytes() {
-  return size_t(P1<D>::nvals + P1<D>::neq) * CH * sizeof(T) + size_t(CH) * 4 + size_t(3 * CH + 2) * 4;
+  return size_t(P1<D>::nvals + P1<D>::neq) * CH * sizeof(T) +  // st, rst
+         size_t(P1<D>::n) * CH * 8 +                          // s_mask
+         size_t(CH) * 4 +                                     // s_info
+         size_t(4 * CH + 3) * 4;                              // s_rowinc, s_pref, s_spref, s_slots
 }
 
 // The row-owner assembly kernel.  One CTA per chunk of whole block rows.
@@ -682,31 +748,64 @@ __global__ void __launch_bounds__(CH) ns_assembly_kernel(
     const double* __restrict__ coords, const double* __restrict__ uadv, const double* __restrict__ state,
     const double* __restrict__ force, const int64_t* __restrict__ start, NSParams p, double* __restrict__ vals,
     float* __restrict__ vals32, double* __restrict__ rhs) {
-  constexpr int neq = P1<D>::neq, nvals = P1<D>::nvals;
+  constexpr int n = P1<D>::n, neq = P1<D>::neq, nvals = P1<D>::nvals;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   T* st = reinterpret_cast<T*>(smem_raw);
   T* rst = st + nvals * CH;
-  uint32_t* s_info = reinterpret_cast<uint32_t*>(rst + neq * CH);
-  int* s_rowinc = reinterpret_cast<int*>(s_info + CH);  // CH + 1
-  int* s_pref = s_rowinc + CH + 1;                      // CH + 1
-  int* s_slots = s_pref + CH + 1;                       // CH
+  unsigned long long* s_mask = reinterpret_cast<unsigned long long*>(rst + neq * CH);  // n * CH
+  uint32_t* s_info = reinterpret_cast<uint32_t*>(s_mask + n * CH);                     // CH
+  int* s_rowinc = reinterpret_cast<int*>(s_info + CH);                                 // CH + 1
+  int* s_pref = s_rowinc + CH + 1;                                                     // CH + 1
+  int* s_spref = s_pref + CH + 1;                                                      // CH + 1
+  int* s_slots = s_spref + CH + 1;                                                     // CH
 
   const int chunk = blockIdx.x;
   const int row0 = chunk_row0[chunk], row1 = chunk_row0[chunk + 1];
-  const int R = row1 - row0;
+  const int R = row1 - row0;  // 1 <= R <= K <= CH (every node has an incidence)
   const int inc0 = row_inc[row0];
   const int K = row_inc[row1] - inc0;
   const int t = threadIdx.x;
 
-  // Phase 1: element row blocks
+  // Row metadata and zeroed contributor masks
+  for (int rl = t; rl <= R; rl += CH) s_rowinc[rl] = row_inc[row0 + rl] - inc0;
+  for (int rl = t; rl < R; rl += CH) s_slots[rl] = int(start[row0 + rl + 1] - start[row0 + rl]);
+  for (int k = t; k < n * CH; k += CH) s_mask[k] = 0ull;
+  __syncthreads();
+  if (t == 0) {
+    int items = 0, slots = 0;
+    s_pref[0] = 0;
+    s_spref[0] = 0;
+    for (int rl = 0; rl < R; ++rl) {
+      items += s_slots[rl] * neq;
+      slots += s_slots[rl];
+      s_pref[rl + 1] = items;
+      s_spref[rl + 1] = slots;
+    }
+  }
+  __syncthreads();
+
+  // Phase 1: element row blocks, one thread per incidence.  The element's
+  // nodes are relabelled by the even permutation k -> k ^ a (tetrahedra) or the
+  // rotation k -> (k + a) mod 3 (triangles), which brings the row node to local
+  // position 0 and leaves det J, the orientation and the symmetric order-2 Gauss
+  // rules unchanged; the element routines then see a compile-time row index.
   if (t < K) {
     const int k = inc0 + t;
     const int e = __ldg(inc_elem + k);
     const uint32_t info = __ldg(inc_info + k);
-    s_info[t] = info;
     const int a = int(info >> 24) & 3;
     const int4 cn = __ldg(conn + e);
-    const int ids[4] = {cn.x, cn.y, cn.z, cn.w};
+    const int ids0[4] = {cn.x, cn.y, cn.z, cn.w};
+    int ids[4];
+    uint32_t pslots = 0;
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      const int src = (D == 3) ? (q ^ a) : (q < 3 ? (q + a) % 3 : 3);
+      ids[q] = ids0[src];
+      const uint32_t sl = (q < n) ? ((info >> (6 * src)) & 63u) : 0xFFu;
+      pslots |= sl << (8 * q);
+    }
+    s_info[t] = pslots;
     const KParams<T> kp = make_kparams<T>(p);
     if constexpr (SPEC) {
       if constexpr (D == 2) spec_tri_row<T>(ids, a, coords, uadv, state, kp, st + t, rst + t, CH);
@@ -714,21 +813,23 @@ __global__ void __launch_bounds__(CH) ns_assembly_kernel(
     } else {
       generic_row<D, T>(ids, a, coords, uadv, state, force, kp, st + t, rst + t, CH);
     }
-  }
-  for (int rl = t; rl <= R; rl += CH) s_rowinc[rl] = row_inc[row0 + rl] - inc0;
-  for (int rl = t; rl < R; rl += CH) s_slots[rl] = int(start[row0 + rl + 1] - start[row0 + rl]);
-  __syncthreads();
-  if (t == 0) {
-    int acc = 0;
-    s_pref[0] = 0;
-    for (int rl = 0; rl < R; ++rl) {
-      acc += s_slots[rl] * neq;
-      s_pref[rl + 1] = acc;
+    // contributor masks: bit = position of this incidence within its row
+    int lo = 0, hi = R - 1;
+    while (lo < hi) {  // last rl with s_rowinc[rl] <= t
+      const int mid = (lo + hi + 1) >> 1;
+      if (s_rowinc[mid] <= t) lo = mid; else hi = mid - 1;
+    }
+    const int bit = t - s_rowinc[lo];
+    if (bit < 64) {
+      const int sb = s_spref[lo];
+#pragma unroll
+      for (int q = 0; q < n; ++q) atomicOr(s_mask + sb + int((pslots >> (8 * q)) & 0xFFu), 1ull << bit);
     }
   }
   __syncthreads();
 
-  // Phase 2a: CSR values, one thread per (row, equation, neighbour slot)
+  // Phase 2a: CSR values, one thread per (row, equation, neighbour slot); the
+  // contributors of a slot are visited in ascending element order.
   const int nitems = s_pref[R];
   for (int it = t; it < nitems; it += CH) {
     int lo = 0, hi = R - 1;
@@ -742,16 +843,28 @@ __global__ void __launch_bounds__(CH) ns_assembly_kernel(
     const int r = local / S;
     const int s = local - r * S;
     const int kb = s_rowinc[rl], ke = s_rowinc[rl + 1];
+    const uint32_t key = uint32_t(s) * 0x01010101u;
     double acc[neq];
 #pragma unroll
     for (int c = 0; c < neq; ++c) acc[c] = 0.0;
-    for (int kk = kb; kk < ke; ++kk) {
-      const uint32_t info = s_info[kk];
+    if (ke - kb <= 64) {
+      unsigned long long m = s_mask[s_spref[rl] + s];
+      while (m) {
+        const int kk = kb + __ffsll(static_cast<long long>(m)) - 1;
+        m &= m - 1;
+        const int b = (__ffs(__vcmpeq4(s_info[kk], key)) - 1) >> 3;
+        const T* src = st + ((b * neq + r) * neq) * CH + kk;
 #pragma unroll
-      for (int b = 0; b < P1<D>::n; ++b) {
-        if (((info >> (6 * b)) & 63u) == uint32_t(s)) {
+        for (int c = 0; c < neq; ++c) acc[c] += double(src[c * CH]);
+      }
+    } else {  // rows with more than 64 incident elements: scan
+      for (int kk = kb; kk < ke; ++kk) {
+        const uint32_t eq = __vcmpeq4(s_info[kk], key);
+        if (eq) {
+          const int b = (__ffs(eq) - 1) >> 3;
+          const T* src = st + ((b * neq + r) * neq) * CH + kk;
 #pragma unroll
-          for (int c = 0; c < neq; ++c) acc[c] += double(st[((b * neq + r) * neq + c) * CH + kk]);
+          for (int c = 0; c < neq; ++c) acc[c] += double(src[c * CH]);
         }
       }
     }
@@ -860,10 +973,13 @@ __global__ void dirichlet_columns_kernel(int64_t nrows, const int64_t* __restric
   const int64_t q = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
   if (q >= nrows) return;
   const int64_t row = fix_row[q];
+  const int64_t k0 = fix_ptr[q], k1 = fix_ptr[q + 1];
   double r = rhs[row];
-  for (int64_t k = fix_ptr[q]; k < fix_ptr[q + 1]; ++k) {
+  // all loads first (they pipeline), then the zeroing stores
+  for (int64_t k = k0; k < k1; ++k)
+    r = __dadd_rn(r, __dmul_rn(-vals[fix_pos[k]], vfirst[fix_bc[k]]));  // no FMA: rounding of the sequential form
+  for (int64_t k = k0; k < k1; ++k) {
     const int64_t pos = fix_pos[k];
-    r = __dadd_rn(r, __dmul_rn(-vals[pos], vfirst[fix_bc[k]]));  // no FMA: same rounding as the sequential form
     vals[pos] = 0.0;
     if (vals32) vals32[pos] = 0.0f;
   }
@@ -898,8 +1014,13 @@ __global__ void dirichlet_rows_kernel(int64_t nbc, int neq, const int64_t* __res
 template <int D, typename T, int CH, bool SPEC>
 int launch_assembly_t(ufem_ns_handle* h, cudaStream_t s, bool write32) {
   NSParams p;
-  p.theta = h->opt.theta; p.dt = h->opt.dt; p.invdt = 1.0 / h->opt.dt; p.rho = h->opt.rho;
-  p.c1 = h->opt.c1; p.c2 = h->opt.c2; p.a_ps = h->opt.alpha_ps; p.a_su = h->opt.alpha_su;
+  const double dt = h->opt.dt, c1 = h->opt.c1;
+  p.theta = h->opt.theta; p.inv_theta = 1.0 / h->opt.theta; p.dt = dt; p.invdt = 1.0 / dt;
+  p.rho = h->opt.rho; p.inv_rho = 1.0 / h->opt.rho;
+  p.tau_c1 = 4. * c1 * c1 / (dt * dt);  // SUPG.hpp:184
+  p.tau_std = 4. / (dt * dt);           // SUPG.hpp:188
+  p.two_dt = 2. / dt;                   // SUPG.hpp:169
+  p.c2 = h->opt.c2; p.a_ps = h->opt.alpha_ps; p.a_su = h->opt.alpha_su;
   p.a_bu = h->opt.alpha_bu; p.u_ref = h->opt.u_ref; p.supg_type = h->opt.supg_type;
   p.has_force = h->d_force != nullptr;
   constexpr size_t smem = assembly_smem_bytes<D, T, CH>();

@@ -258,9 +258,9 @@ void ufem_ns_default_options(ufem_ns_options* o) {
 void ufem_krylov_default_opts(ufem_krylov_opts* o) {
   if (!o) return;
   std::memset(o, 0, sizeof(*o));
-  o->method = 0;
+  o->method = 1;  // BiCGStab: on the PSPG/SUPG systems it needs ~2-8x fewer SpMVs than GMRES(30..200) with Jacobi
   o->restart = 30;
-  o->max_iters = 1000;
+  o->max_iters = 3000;
   o->precond = 1;
   o->tol = 1e-10;
   o->mixed = 0;

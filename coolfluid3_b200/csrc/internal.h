@@ -25,8 +25,9 @@ int set_error(int code, const std::string& msg);
 
 // Scalar parameters of the element expression, passed to kernels by value.
 struct NSParams {
-  double theta, dt, invdt, rho;
-  double c1, c2, a_ps, a_su, a_bu, u_ref;
+  double theta, inv_theta, dt, invdt, rho, inv_rho;
+  double tau_c1, tau_std, two_dt;
+  double c2, a_ps, a_su, a_bu, u_ref;
   int supg_type;
   int has_force;
 };

@@ -76,30 +76,47 @@ __device__ __forceinline__ double block_sum(double v, double* sm) {
 #define GRID_STRIDE(i, n) \
   for (int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < (n); i += int64_t(gridDim.x) * blockDim.x)
 
-// y = A x on the node graph: one warp per block row (node), FEVbr point layout.
-template <typename VT, typename MT, typename AT>
-__global__ void spmv_kernel(int64_t N, int neq, const int64_t* __restrict__ start, const int32_t* __restrict__ adj,
-                            const MT* __restrict__ vals, const VT* __restrict__ x, VT* __restrict__ y,
-                            const int* __restrict__ done) {
+// y = A x on the node graph, FEVbr point layout: the NEQ rows of a node are
+// contiguous (row r, neighbour slot s, component c at r*S*NEQ + s*NEQ + c).
+// One warp per node; a lane owns columns j = lane, lane+32, ... of the block
+// row, gathers x once per column and multiplies it into all NEQ rows (row
+// values are read coalesced across the warp).  FP64 accumulation.
+template <int NEQ, typename VT, typename MT>
+__global__ void __launch_bounds__(256) spmv_kernel(int64_t N, const int64_t* __restrict__ start,
+                                                   const int32_t* __restrict__ adj, const MT* __restrict__ vals,
+                                                   const VT* __restrict__ x, VT* __restrict__ y,
+                                                   const int* __restrict__ done) {
   if (done && *done) return;
   const int64_t node = (int64_t(blockIdx.x) * blockDim.x + threadIdx.x) >> 5;
   const int lane = threadIdx.x & 31;
   if (node >= N) return;
-  const int64_t s0 = start[node];
-  const int S = int(start[node + 1] - s0);
-  const int64_t base = int64_t(neq) * neq * s0;
-  const int len = S * neq;
-  for (int r = 0; r < neq; ++r) {
-    AT acc = 0;
-    const MT* row = vals + base + int64_t(r) * len;
-    for (int idx = lane; idx < len; idx += 32) {
-      const int s = idx / neq;
-      const int c = idx - s * neq;
-      const int64_t col = int64_t(__ldg(adj + s0 + s)) * neq + c;
-      acc += AT(row[idx]) * AT(x[col]);
-    }
-    acc = warp_sum(acc);
-    if (lane == 0) y[node * neq + r] = VT(acc);
+  const int64_t s0 = __ldg(start + node);
+  const int len = int(__ldg(start + node + 1) - s0) * NEQ;
+  const MT* row = vals + int64_t(NEQ) * NEQ * s0;
+  double acc[NEQ];
+#pragma unroll
+  for (int r = 0; r < NEQ; ++r) acc[r] = 0.0;
+  for (int j = lane; j < len; j += 32) {
+    const int s = j / NEQ;
+    const int c = j - s * NEQ;
+    const double xj = double(x[int64_t(__ldg(adj + s0 + s)) * NEQ + c]);
+    MT v[NEQ];
+#pragma unroll
+    for (int r = 0; r < NEQ; ++r) v[r] = __ldcs(row + r * len + j);  // streamed once per SpMV
+#pragma unroll
+    for (int r = 0; r < NEQ; ++r) acc[r] += double(v[r]) * xj;
+  }
+#pragma unroll
+  for (int r = 0; r < NEQ; ++r) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) acc[r] += __shfl_xor_sync(0xffffffffu, acc[r], o);  // every lane: full sum
+  }
+  if (lane < NEQ) {
+    double out = acc[0];
+#pragma unroll
+    for (int r = 1; r < NEQ; ++r)
+      if (lane == r) out = acc[r];
+    y[node * NEQ + lane] = VT(out);
   }
 }
 
@@ -355,8 +372,173 @@ __global__ void finalize_norm_kernel(int nblk, const double* __restrict__ part, 
   dctl[idx] = take_sqrt ? sqrt(s) : s;
 }
 
-// ---- BiCGStab scalar kernels ------------------------------------------------
+// ---- BiCGStab kernels ---------------------------------------------------------
+// Scalars in dctl: rho (= rh.r of the current residual), rho_old, alpha, omega.
+// Each single-block "reduce" kernel folds the block partials in a fixed order
+// and computes the next scalar, so an iteration is ten launches.
+
+// p = r + beta (p - omega v), beta = (rho/rho_old)(alpha/omega); ph = M^-1 p
+// (point Jacobi or identity inline; block Jacobi applied by precond_kernel).
+template <typename VT>
+__global__ void bicg_p_kernel(int64_t n, int pkind, const VT* __restrict__ dinv, const VT* __restrict__ r,
+                              const VT* __restrict__ v, VT* __restrict__ p, VT* __restrict__ ph,
+                              const double* __restrict__ dctl, const int* __restrict__ ictl) {
+  if (ictl[0]) return;
+  const double beta = (dctl[kRho] / dctl[kRhoOld]) * (dctl[kAlpha] / dctl[kOmega]);
+  const double om = dctl[kOmega];
+  GRID_STRIDE(i, n) {
+    const VT pi = VT(double(r[i]) + beta * (double(p[i]) - om * double(v[i])));
+    p[i] = pi;
+    if (pkind != 2) ph[i] = (pkind == 1) ? VT(dinv[i] * pi) : pi;
+  }
+}
+
+// alpha = rho / (rh . v) from the block partials of rh . v.
+__global__ void bicg_alpha_kernel(int nblk, const double* __restrict__ part, double* __restrict__ dctl,
+                                  int* __restrict__ ictl, double alpha_max) {
+  if (ictl[0]) return;
+  __shared__ double sm[32];
+  double sv = 0.0;
+  for (int b = threadIdx.x; b < nblk; b += blockDim.x) sv += part[b];
+  const double d = block_sum(sv, sm);
+  if (threadIdx.x != 0) return;
+  dctl[kRhV] = d;
+  if (d == 0.0 || !isfinite(d)) {
+    ictl[0] = 1;
+    ictl[2] = isfinite(d) ? 2 : 3;
+    return;
+  }
+  const double a = dctl[kRho] / d;
+  if (!(fabs(a) < alpha_max)) {  // (rh, v) ~ 0: the step would overflow the vector type
+    ictl[0] = 1;
+    ictl[2] = 2;
+    return;
+  }
+  dctl[kAlpha] = a;
+}
+
+// s = r - alpha v ; sh = M^-1 s
+template <typename VT>
+__global__ void bicg_s_kernel(int64_t n, int pkind, const VT* __restrict__ dinv, const VT* __restrict__ r,
+                              const VT* __restrict__ v, VT* __restrict__ s, VT* __restrict__ sh,
+                              const double* __restrict__ dctl, const int* __restrict__ ictl) {
+  if (ictl[0]) return;
+  const double al = dctl[kAlpha];
+  GRID_STRIDE(i, n) {
+    const VT si = VT(double(r[i]) - al * double(v[i]));
+    s[i] = si;
+    if (pkind != 2) sh[i] = (pkind == 1) ? VT(dinv[i] * si) : si;
+  }
+}
+
+// block partials of t.s (part[0..nblk)) and t.t (part[nblk..2nblk))
+template <typename VT>
+__global__ void dot2_partials_kernel(int64_t n, const VT* __restrict__ t, const VT* __restrict__ s,
+                                     double* __restrict__ part, const int* __restrict__ ictl) {
+  if (ictl[0]) return;
+  __shared__ double sm[32];
+  double ts = 0.0, tt = 0.0;
+  GRID_STRIDE(i, n) {
+    const double ti = double(t[i]);
+    ts += ti * double(s[i]);
+    tt += ti * ti;
+  }
+  ts = block_sum(ts, sm);
+  tt = block_sum(tt, sm);
+  if (threadIdx.x == 0) {
+    part[blockIdx.x] = ts;
+    part[gridDim.x + blockIdx.x] = tt;
+  }
+}
+
+__global__ void bicg_omega_kernel(int nblk, const double* __restrict__ part, double* __restrict__ dctl,
+                                  int* __restrict__ ictl) {
+  if (ictl[0]) return;
+  __shared__ double sm[32];
+  double a = 0.0, b = 0.0;
+  for (int k = threadIdx.x; k < nblk; k += blockDim.x) {
+    a += part[k];
+    b += part[nblk + k];
+  }
+  const double ts = block_sum(a, sm);
+  const double tt = block_sum(b, sm);
+  if (threadIdx.x != 0) return;
+  const double om = (tt != 0.0) ? ts / tt : 0.0;
+  dctl[kTS] = ts;
+  dctl[kTT] = tt;
+  dctl[kOmega] = om;
+  if (!isfinite(om)) {
+    ictl[0] = 1;
+    ictl[2] = 3;
+  } else if (om == 0.0 && tt != 0.0) {
+    // t.s = 0 with t != 0: the next beta would divide by omega (breakdown);
+    // x is still advanced by alpha*ph in bicg_xr_kernel before stopping
+    ictl[2] = 2;
+  }
+}
+
+// x += alpha ph + omega sh ; r = s - omega t ; partials of r.r and rh.r
+template <typename VT>
+__global__ void bicg_xr_kernel(int64_t n, const VT* __restrict__ ph, const VT* __restrict__ sh,
+                               const VT* __restrict__ s, const VT* __restrict__ t, const VT* __restrict__ rh,
+                               VT* __restrict__ x, VT* __restrict__ r, const double* __restrict__ dctl,
+                               const int* __restrict__ ictl, double* __restrict__ part) {
+  if (ictl[0]) return;
+  __shared__ double sm[32];
+  const double al = dctl[kAlpha], om = dctl[kOmega];
+  double rr = 0.0, hr = 0.0;
+  GRID_STRIDE(i, n) {
+    x[i] = VT(double(x[i]) + al * double(ph[i]) + om * double(sh[i]));
+    const VT ri = VT(double(s[i]) - om * double(t[i]));
+    r[i] = ri;
+    rr += double(ri) * double(ri);
+    hr += double(rh[i]) * double(ri);
+  }
+  rr = block_sum(rr, sm);
+  hr = block_sum(hr, sm);
+  if (threadIdx.x == 0) {
+    part[blockIdx.x] = rr;
+    part[gridDim.x + blockIdx.x] = hr;
+  }
+}
+
+// ||r|| and the next rho = rh . r; convergence and iteration count.
+__global__ void bicg_end_kernel(int nblk, const double* __restrict__ part, double* __restrict__ dctl,
+                                int* __restrict__ ictl, double tol, int maxit) {
+  if (ictl[0]) return;
+  __shared__ double sm[32];
+  double a = 0.0, b = 0.0;
+  for (int k = threadIdx.x; k < nblk; k += blockDim.x) {
+    a += part[k];
+    b += part[nblk + k];
+  }
+  const double nn = block_sum(a, sm);
+  const double rho_new = block_sum(b, sm);
+  if (threadIdx.x != 0) return;
+  const double rn = sqrt(nn);
+  dctl[kEst] = rn;
+  dctl[kRhoOld] = dctl[kRho];
+  dctl[kRho] = rho_new;
+  ictl[3] += 1;
+  if (ictl[2] == 2) {  // omega breakdown flagged this iteration
+    ictl[0] = 1;
+  } else if (!isfinite(rn) || !isfinite(rho_new)) {
+    ictl[0] = 1;
+    ictl[2] = 3;
+  } else if (rn <= tol * dctl[kBnorm]) {
+    ictl[0] = 1;
+  } else if (rho_new == 0.0) {
+    ictl[0] = 1;
+    ictl[2] = 2;
+  } else if (ictl[3] >= maxit) {
+    ictl[0] = 1;
+    ictl[2] = 1;
+  }
+}
+
+// rho = ||r0||^2 (rh = r0), rho_old = alpha = omega = 1, converged test.
 __global__ void bicg_init_kernel(double* dctl, int* ictl, double tol) {
+  dctl[kRho] = dctl[kBeta] * dctl[kBeta];
   dctl[kRhoOld] = 1.0;
   dctl[kAlpha] = 1.0;
   dctl[kOmega] = 1.0;
@@ -364,95 +546,6 @@ __global__ void bicg_init_kernel(double* dctl, int* ictl, double tol) {
   ictl[2] = isfinite(dctl[kBeta]) ? 0 : 3;
   if (ictl[2]) ictl[0] = 1;
   ictl[3] = 0;
-}
-
-// p = r + beta (p - omega v), beta = (rho/rho_old)(alpha/omega)
-template <typename VT>
-__global__ void bicg_p_kernel(int64_t n, const VT* __restrict__ r, const VT* __restrict__ v, VT* __restrict__ p,
-                              const double* __restrict__ dctl, const int* __restrict__ ictl) {
-  if (ictl[0]) return;
-  const double beta = (dctl[kRho] / dctl[kRhoOld]) * (dctl[kAlpha] / dctl[kOmega]);
-  const double om = dctl[kOmega];
-  GRID_STRIDE(i, n) p[i] = VT(double(r[i]) + beta * (double(p[i]) - om * double(v[i])));
-}
-
-__global__ void bicg_check_rho_kernel(double* dctl, int* ictl) {
-  if (ictl[0]) return;
-  const double rho = dctl[kRho];
-  if (rho == 0.0 || !isfinite(rho)) {
-    ictl[0] = 1;
-    ictl[2] = isfinite(rho) ? 2 : 3;
-  }
-}
-
-__global__ void bicg_alpha_kernel(double* dctl, int* ictl) {
-  if (ictl[0]) return;
-  const double d = dctl[kRhV];
-  if (d == 0.0 || !isfinite(d)) {
-    ictl[0] = 1;
-    ictl[2] = isfinite(d) ? 2 : 3;
-    return;
-  }
-  dctl[kAlpha] = dctl[kRho] / d;
-}
-
-// s = r - alpha v
-template <typename VT>
-__global__ void bicg_s_kernel(int64_t n, const VT* __restrict__ r, const VT* __restrict__ v, VT* __restrict__ s,
-                              const double* __restrict__ dctl, const int* __restrict__ ictl) {
-  if (ictl[0]) return;
-  const double al = dctl[kAlpha];
-  GRID_STRIDE(i, n) s[i] = VT(double(r[i]) - al * double(v[i]));
-}
-
-__global__ void bicg_omega_kernel(double* dctl, int* ictl) {
-  if (ictl[0]) return;
-  const double tt = dctl[kTT];
-  dctl[kOmega] = (tt != 0.0) ? dctl[kTS] / tt : 0.0;
-  if (!isfinite(dctl[kOmega])) {
-    ictl[0] = 1;
-    ictl[2] = 3;
-  }
-}
-
-// x += alpha ph + omega sh ; r = s - omega t ; partials of ||r||^2
-template <typename VT>
-__global__ void bicg_xr_kernel(int64_t n, const VT* __restrict__ ph, const VT* __restrict__ sh,
-                               const VT* __restrict__ s, const VT* __restrict__ t, VT* __restrict__ x,
-                               VT* __restrict__ r, const double* __restrict__ dctl, const int* __restrict__ ictl,
-                               double* __restrict__ normpart) {
-  if (ictl[0]) return;
-  __shared__ double sm[32];
-  const double al = dctl[kAlpha], om = dctl[kOmega];
-  double s2 = 0.0;
-  GRID_STRIDE(i, n) {
-    x[i] = VT(double(x[i]) + al * double(ph[i]) + om * double(sh[i]));
-    const VT ri = VT(double(s[i]) - om * double(t[i]));
-    r[i] = ri;
-    s2 += double(ri) * double(ri);
-  }
-  s2 = block_sum(s2, sm);
-  if (threadIdx.x == 0) normpart[blockIdx.x] = s2;
-}
-
-__global__ void bicg_end_kernel(int nblk, const double* __restrict__ normpart, double* dctl, int* ictl, double tol,
-                                int maxit) {
-  if (ictl[0]) return;
-  double nn = 0.0;
-  for (int b = 0; b < nblk; ++b) nn += normpart[b];
-  const double rn = sqrt(nn);
-  dctl[kEst] = rn;
-  dctl[kRhoOld] = dctl[kRho];
-  ictl[3] += 1;
-  if (!isfinite(rn)) {
-    ictl[0] = 1;
-    ictl[2] = 3;
-  } else if (rn <= tol * dctl[kBnorm]) {
-    ictl[0] = 1;
-  } else if (ictl[3] >= maxit) {
-    ictl[0] = 1;
-    ictl[2] = 1;
-  }
 }
 
 // ---------------------------------------------------------------------------
@@ -532,10 +625,12 @@ inline unsigned grid_for(int64_t n, int threads, int64_t cap = 8 * 148) {
 
 template <typename VT, typename MT>
 int spmv(ufem_ns_handle* h, const MT* vals, const VT* x, VT* y, const int* done, cudaStream_t s) {
-  using AT = typename std::conditional<std::is_same<VT, double>::value, double, float>::type;
   const int64_t threads = h->N * 32;
-  spmv_kernel<VT, MT, AT><<<unsigned((threads + 255) / 256), 256, 0, s>>>(h->N, h->neq, h->d_start, h->d_adj, vals, x,
-                                                                          y, done);
+  const unsigned grid = unsigned((threads + 255) / 256);
+  if (h->neq == 4)
+    spmv_kernel<4, VT, MT><<<grid, 256, 0, s>>>(h->N, h->d_start, h->d_adj, vals, x, y, done);
+  else
+    spmv_kernel<3, VT, MT><<<grid, 256, 0, s>>>(h->N, h->d_start, h->d_adj, vals, x, y, done);
   UFEM_CUDA_TRY(cudaGetLastError());
   return UFEM_OK;
 }
@@ -575,7 +670,8 @@ int true_residual(ufem_ns_handle* h, const MT* vals, const BT* b, const VT* x, V
   finalize_norm_kernel<<<1, 1, 0, s>>>(kw.nblk, kw.part, kw.dctl, kTrue, 1);
   UFEM_CUDA_TRY(cudaMemcpyAsync(kw.h_dctl, kw.dctl, 16 * sizeof(double), cudaMemcpyDeviceToHost, s));
   UFEM_CUDA_TRY(cudaStreamSynchronize(s));
-  *out = bnorm > 0.0 ? kw.h_dctl[kTrue] / bnorm : 0.0;
+  // a zero RHS has the zero solution; a non-finite ||b|| never counts as converged
+  *out = bnorm > 0.0 ? kw.h_dctl[kTrue] / bnorm : (bnorm == 0.0 ? 0.0 : NAN);
   return UFEM_OK;
 }
 
@@ -679,30 +775,22 @@ int bicgstab(ufem_ns_handle* h, const MT* vals, const BT* b, VT* x, VT* r, VT* r
   fill_kernel<VT><<<g1, kRedThreads, 0, st>>>(n, VT(0), v);
   bicg_init_kernel<<<1, 1, 0, st>>>(kw.dctl, kw.ictl, tol);
   UFEM_CUDA_TRY(cudaGetLastError());
-  auto dot = [&](const VT* a, const VT* c, int slot) -> int {
-    dot_partials_kernel<VT><<<dim3(g1, 1), kRedThreads, 0, st>>>(n, a, n, c, kw.part, kw.ictl);
-    reduce_partials_kernel<<<1, 256, 0, st>>>(nblk, kw.part, kw.dctl + slot, kw.ictl);
-    UFEM_CUDA_TRY(cudaGetLastError());
-    return UFEM_OK;
-  };
+  const double alpha_max = std::is_same<VT, float>::value ? 1e20 : 1e150;
   const int check = 8;
   for (int it = 0; it < maxit; it += check) {
     for (int k = 0; k < check; ++k) {
-      if ((rc = dot(rh, r, kRho))) return rc;
-      bicg_check_rho_kernel<<<1, 1, 0, st>>>(kw.dctl, kw.ictl);
-      bicg_p_kernel<VT><<<g1, kRedThreads, 0, st>>>(n, r, v, p, kw.dctl, kw.ictl);
-      if ((rc = precond<VT>(h, pkind, dinv, p, ph, kw.ictl, st))) return rc;
+      bicg_p_kernel<VT><<<g1, kRedThreads, 0, st>>>(n, pkind, dinv, r, v, p, ph, kw.dctl, kw.ictl);
+      if (pkind == 2 && (rc = precond<VT>(h, pkind, dinv, p, ph, kw.ictl, st))) return rc;
       if ((rc = spmv<VT, MT>(h, vals, ph, v, kw.ictl, st))) return rc;
-      if ((rc = dot(rh, v, kRhV))) return rc;
-      bicg_alpha_kernel<<<1, 1, 0, st>>>(kw.dctl, kw.ictl);
-      bicg_s_kernel<VT><<<g1, kRedThreads, 0, st>>>(n, r, v, sv, kw.dctl, kw.ictl);
-      if ((rc = precond<VT>(h, pkind, dinv, sv, sh, kw.ictl, st))) return rc;
+      dot_partials_kernel<VT><<<dim3(g1, 1), kRedThreads, 0, st>>>(n, rh, n, v, kw.part, kw.ictl);
+      bicg_alpha_kernel<<<1, 256, 0, st>>>(nblk, kw.part, kw.dctl, kw.ictl, alpha_max);
+      bicg_s_kernel<VT><<<g1, kRedThreads, 0, st>>>(n, pkind, dinv, r, v, sv, sh, kw.dctl, kw.ictl);
+      if (pkind == 2 && (rc = precond<VT>(h, pkind, dinv, sv, sh, kw.ictl, st))) return rc;
       if ((rc = spmv<VT, MT>(h, vals, sh, tv, kw.ictl, st))) return rc;
-      if ((rc = dot(tv, sv, kTS))) return rc;
-      if ((rc = dot(tv, tv, kTT))) return rc;
-      bicg_omega_kernel<<<1, 1, 0, st>>>(kw.dctl, kw.ictl);
-      bicg_xr_kernel<VT><<<g1, kRedThreads, 0, st>>>(n, ph, sh, sv, tv, x, r, kw.dctl, kw.ictl, kw.part);
-      bicg_end_kernel<<<1, 1, 0, st>>>(nblk, kw.part, kw.dctl, kw.ictl, tol, maxit);
+      dot2_partials_kernel<VT><<<g1, kRedThreads, 0, st>>>(n, tv, sv, kw.part, kw.ictl);
+      bicg_omega_kernel<<<1, 256, 0, st>>>(nblk, kw.part, kw.dctl, kw.ictl);
+      bicg_xr_kernel<VT><<<g1, kRedThreads, 0, st>>>(n, ph, sh, sv, tv, rh, x, r, kw.dctl, kw.ictl, kw.part);
+      bicg_end_kernel<<<1, 256, 0, st>>>(nblk, kw.part, kw.dctl, kw.ictl, tol, maxit);
       UFEM_CUDA_TRY(cudaGetLastError());
     }
     UFEM_CUDA_TRY(cudaMemcpyAsync(kw.h_ictl, kw.ictl, 4 * sizeof(int), cudaMemcpyDeviceToHost, st));
@@ -719,6 +807,7 @@ int bicgstab(ufem_ns_handle* h, const MT* vals, const BT* b, VT* x, VT* r, VT* r
     fill_kernel<VT><<<g1, kRedThreads, 0, st>>>(n, VT(0), x);
     UFEM_CUDA_TRY(cudaGetLastError());
     res.converged = true;
+    res.status = 0;
     return UFEM_OK;
   }
   double rr;
@@ -746,7 +835,7 @@ __global__ void vals_to32_kernel(int64_t n, const double* __restrict__ v, float*
 int krylov_solve(ufem_ns_handle* h, const ufem_krylov_opts* ko, ufem_krylov_status* st, cudaStream_t s) {
   ufem_krylov_opts o = *ko;
   if (o.restart <= 0) o.restart = 30;
-  if (o.max_iters <= 0) o.max_iters = 1000;
+  if (o.max_iters <= 0) o.max_iters = 3000;
   if (o.tol <= 0) o.tol = 1e-10;
   if (o.max_refine <= 0) o.max_refine = 20;
   if (o.inner_tol <= 0) o.inner_tol = 1e-5;
@@ -825,7 +914,10 @@ int krylov_solve(ufem_ns_handle* h, const ufem_krylov_opts* ko, ufem_krylov_stat
                                         kw.dinv32, o.precond, o.inner_tol, o.max_iters, o.restart, s, ir);
       if (rc) return rc;
       total += ir.iters;
-      if (ir.status == 3) { status = 3; relres = NAN; break; }
+      // A breakdown (status 2) leaves a finite, partially converged correction:
+      // apply it and let the next FP64 residual restart the inner solve.  A
+      // non-finite inner iterate is never applied.
+      if (ir.status == 3 || !std::isfinite(ir.relres)) { status = 3; relres = NAN; break; }
       add_scaled_kernel<float><<<g1, kRedThreads, 0, s>>>(n, kw.x32, h->d_sol, kw.dctl, 14);
       UFEM_CUDA_TRY(cudaGetLastError());
     }

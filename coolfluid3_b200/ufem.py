@@ -30,7 +30,7 @@ def _stream(stream) -> C.c_void_p | None:
     return C.c_void_p(int(getattr(stream, "cuda_stream", stream)))
 
 
-def krylov_options(method: str = "gmres", restart: int = 30, max_iters: int = 1000, precond: str = "jacobi",
+def krylov_options(method: str = "bicgstab", restart: int = 30, max_iters: int = 3000, precond: str = "jacobi",
                    tol: float = 1e-10, mixed: bool = False, max_refine: int = 20, inner_tol: float = 1e-5):
     o = N.KrylovOpts()
     o.method = {"gmres": 0, "bicgstab": 1}[method]

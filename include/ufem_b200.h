@@ -69,9 +69,9 @@ typedef struct ufem_ns_options {
 
 /* Krylov options (SolveLSS / Belos GMRES replacement). */
 typedef struct ufem_krylov_opts {
-  int32_t method;      /* 0: GMRES(restart)  1: BiCGStab                          */
+  int32_t method;      /* 0: GMRES(restart)  1: BiCGStab (default)                */
   int32_t restart;     /* GMRES restart length, default 30                         */
-  int32_t max_iters;   /* total Krylov iterations (per refinement pass), 1000    */
+  int32_t max_iters;   /* total Krylov iterations (per refinement pass), 3000    */
   int32_t precond;     /* 0 none, 1 point Jacobi (default), 2 node-block Jacobi   */
   double tol;          /* ||b - A x|| / ||b|| target, default 1e-10                */
   int32_t mixed;       /* 0: all FP64; 1: FP32 inner Krylov + FP64 refinement     */

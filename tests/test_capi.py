@@ -45,7 +45,7 @@ def test_version_and_defaults():
     assert (o.alpha_ps, o.alpha_su, o.alpha_bu, o.precision) == (1.0, 1.0, 1.0, 0)
     k = N.KrylovOpts()
     lib.ufem_krylov_default_opts(C.byref(k))
-    assert (k.method, k.restart, k.precond, k.tol) == (0, 30, 1, 1e-10)
+    assert (k.method, k.restart, k.max_iters, k.precond, k.tol) == (1, 30, 3000, 1, 1e-10)
 
 
 def _create(coords, conn, **over):

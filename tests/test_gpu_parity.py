@@ -138,33 +138,37 @@ def test_apply_matches_scipy():
     assert vec_rel_error(y, ref) <= 1e-13
 
 
-@pytest.mark.parametrize("method,precond", [("gmres", "jacobi"), ("gmres", "block_jacobi"), ("bicgstab", "jacobi")])
-def test_solve_matches_oracle(method, precond):
-    pb = small_problem(2, 16)
+def fp64_residual(ns) -> float:
+    """||b - A x|| / ||b|| of the GPU's solution, evaluated on the host in FP64."""
+    rp, ci = ns.csr()
+    v, b = ns.system()
+    x = ns.solution()
+    return vec_rel_error(csr_matrix(rp, ci, v, ns.nb_rows) @ x, b)
+
+
+@pytest.mark.parametrize("dim,n", [(2, 16), (3, 6)])
+@pytest.mark.parametrize("method,precond,mixed", [("gmres", "jacobi", False), ("gmres", "block_jacobi", False),
+                                                  ("bicgstab", "jacobi", False), ("bicgstab", "block_jacobi", False),
+                                                  ("bicgstab", "jacobi", True), ("gmres", "jacobi", True)])
+def test_solve_matches_oracle(dim, n, method, precond, mixed):
+    """Solver tolerance 1e-12 on the FP64 residual (also for the FP32 inner
+    solve with FP64 refinement).  The solution is compared with the oracle's
+    (ILU-GMRES to 1e-13) within 1e-6: these pinned-pressure cavity systems
+    have condition numbers near 1e5."""
+    pb = small_problem(dim, n)
     ns = gpu_for(pb, use_specializations=False)
     o = oracle_for(pb, use_specializations=False)
     ns.assemble()
     ns.apply_dirichlet()
     o.assemble()
     o.apply_dirichlet()
-    st = ns.solve(method=method, precond=precond, tol=1e-12, max_iters=4000)
+    st = ns.solve(method=method, precond=precond, mixed=mixed, tol=1e-12, inner_tol=1e-4, max_iters=6000)
     assert st["converged"] == 1, st
+    if mixed:
+        assert st["refinements"] >= 1
+    assert fp64_residual(ns) <= 2e-12
     assert o.solve(tol=1e-13)["rc"] == 0
-    assert vec_rel_error(ns.solution(), o.solution()) <= 1e-8
-
-
-def test_mixed_precision_solve_reaches_fp64_accuracy():
-    pb = small_problem(3, 6)
-    ns = gpu_for(pb, use_specializations=False)
-    o = oracle_for(pb, use_specializations=False)
-    ns.assemble()
-    ns.apply_dirichlet()
-    o.assemble()
-    o.apply_dirichlet()
-    st = ns.solve(mixed=True, tol=1e-10, inner_tol=1e-4)
-    assert st["converged"] == 1 and st["refinements"] >= 1, st
-    o.solve(tol=1e-13)
-    assert vec_rel_error(ns.solution(), o.solution()) <= 1e-8
+    assert vec_rel_error(ns.solution(), o.solution()) <= 1e-6
 
 
 @pytest.mark.parametrize("dim,n,spec", [(2, 16, False), (2, 16, True), (3, 4, False)])
@@ -182,8 +186,8 @@ def test_time_steps_match_oracle(dim, n, spec):
         o.update()
     gup, glin = ns.state()
     oup, olin = o.state()
-    assert vec_rel_error(gup, oup) <= 1e-7
-    assert vec_rel_error(glin, olin) <= 1e-7
+    assert vec_rel_error(gup, oup) <= 1e-6
+    assert vec_rel_error(glin, olin) <= 1e-6
 
 
 def test_cfg1_one_step_plain_and_mixed():
@@ -195,7 +199,7 @@ def test_cfg1_one_step_plain_and_mixed():
     oup, _ = o.state()
     for mixed in (False, True):
         ns = gpu_for(pb, use_specializations=False)
-        st = ns.execute(tol=1e-10, mixed=mixed)
+        st = ns.execute(tol=1e-12, mixed=mixed, inner_tol=1e-4)
         assert st["converged"] == 1
         gup, _ = ns.state()
         assert vec_rel_error(gup, oup) <= 1e-6
