@@ -97,6 +97,7 @@ SIGNATURES = {
     "ufem_ns_assemble": (C.c_int, [_P, _P]),
     "ufem_ns_apply_dirichlet": (C.c_int, [_P, _P]),
     "ufem_ns_solve": (C.c_int, [_P, C.POINTER(KrylovOpts), C.POINTER(KrylovStatus), _P]),
+    "ufem_ns_solve_noalloc": (C.c_int, [_P, C.POINTER(KrylovOpts), C.POINTER(KrylovStatus), _P]),
     "ufem_ns_update": (C.c_int, [_P, _P]),
     "ufem_ns_step": (C.c_int, [_P, C.c_int32, C.POINTER(KrylovOpts), C.POINTER(KrylovStatus), _P]),
     "ufem_ns_get_system": (C.c_int, [_P, _D, _D]),

@@ -661,9 +661,8 @@ struct SolveResult {
 
 // Final FP64-or-VT true residual ||b - A x|| / ||b|| into res.
 template <typename VT, typename MT, typename BT>
-int true_residual(ufem_ns_handle* h, const MT* vals, const BT* b, const VT* x, VT* w, VT* r, double bnorm,
-                  cudaStream_t s, double* out) {
-  KrylovWork& kw = *h->kw;
+int true_residual(ufem_ns_handle* h, KrylovWork& kw, const MT* vals, const BT* b, const VT* x, VT* w, VT* r,
+                  double bnorm, cudaStream_t s, double* out) {
   int rc;
   if ((rc = spmv<VT, MT>(h, vals, x, w, nullptr, s))) return rc;
   residual_kernel<VT, BT><<<unsigned(kw.nblk), kRedThreads, 0, s>>>(h->nrows, b, w, r, kw.part, nullptr);
@@ -745,7 +744,7 @@ int gmres(ufem_ns_handle* h, const MT* vals, const BT* b, VT* x, VT* V, VT* w, V
     }
     if (res.iters >= maxit) {
       double rr;
-      if ((rc = true_residual<VT, MT, BT>(h, vals, b, x, w, r, bnorm, s, &rr))) return rc;
+      if ((rc = true_residual<VT, MT, BT>(h, kw, vals, b, x, w, r, bnorm, s, &rr))) return rc;
       res.relres = rr;
       res.converged = rr <= tol;
       res.status = res.converged ? 0 : 1;
@@ -757,9 +756,9 @@ int gmres(ufem_ns_handle* h, const MT* vals, const BT* b, VT* x, VT* V, VT* w, V
 // Right-preconditioned BiCGStab with device-side scalars; the host checks the
 // done flag every `check` iterations.
 template <typename VT, typename MT, typename BT>
-int bicgstab(ufem_ns_handle* h, const MT* vals, const BT* b, VT* x, VT* r, VT* rh, VT* p, VT* v, VT* sv, VT* tv,
-             VT* ph, VT* sh, VT* dinv, int pkind, double tol, int maxit, cudaStream_t st, SolveResult& res) {
-  KrylovWork& kw = *h->kw;
+int bicgstab(ufem_ns_handle* h, KrylovWork& kw, const MT* vals, const BT* b, VT* x, VT* r, VT* rh, VT* p, VT* v,
+             VT* sv, VT* tv, VT* ph, VT* sh, VT* dinv, int pkind, double tol, int maxit, cudaStream_t st,
+             SolveResult& res) {
   const int64_t n = h->nrows;
   const int nblk = kw.nblk;
   const unsigned g1 = unsigned(nblk);
@@ -811,7 +810,7 @@ int bicgstab(ufem_ns_handle* h, const MT* vals, const BT* b, VT* x, VT* r, VT* r
     return UFEM_OK;
   }
   double rr;
-  if ((rc = true_residual<VT, MT, BT>(h, vals, b, x, v, r, bnorm, st, &rr))) return rc;
+  if ((rc = true_residual<VT, MT, BT>(h, kw, vals, b, x, v, r, bnorm, st, &rr))) return rc;
   res.relres = rr;
   res.converged = rr <= tol;
   if (res.converged) res.status = 0;
@@ -852,7 +851,7 @@ int krylov_solve(ufem_ns_handle* h, const ufem_krylov_opts* ko, ufem_krylov_stat
   if (!mixed) {
     SolveResult r;
     if (bicg)
-      rc = bicgstab<double, double, double>(h, h->d_vals, h->d_rhs, h->d_sol, kw.r, kw.brh, kw.bp, kw.bv, kw.bs, kw.bt,
+      rc = bicgstab<double, double, double>(h, kw, h->d_vals, h->d_rhs, h->d_sol, kw.r, kw.brh, kw.bp, kw.bv, kw.bs, kw.bt,
                                             kw.bph, kw.bsh, kw.dinv, o.precond, o.tol, o.max_iters, s, r);
     else
       rc = gmres<double, double, double>(h, h->d_vals, h->d_rhs, h->d_sol, kw.V, kw.w, kw.z, kw.t, kw.r, kw.dinv,
@@ -906,7 +905,7 @@ int krylov_solve(ufem_ns_handle* h, const ufem_krylov_opts* ko, ufem_krylov_stat
       UFEM_CUDA_TRY(cudaMemcpyAsync(kw.dctl + 14, kw.dctl + kScale, sizeof(double), cudaMemcpyDeviceToDevice, s));
       SolveResult ir;
       if (bicg)
-        rc = bicgstab<float, float, float>(h, h->d_vals32, kw.r32, kw.x32, kw.w32, kw.brh32, kw.bp32, kw.bv32,
+        rc = bicgstab<float, float, float>(h, kw, h->d_vals32, kw.r32, kw.x32, kw.w32, kw.brh32, kw.bp32, kw.bv32,
                                            kw.bs32, kw.bt32, kw.bph32, kw.bsh32, kw.dinv32, o.precond, o.inner_tol,
                                            o.max_iters, s, ir);
       else
@@ -950,4 +949,85 @@ void krylov_free(ufem_ns_handle* h) {
   h->kw = nullptr;
 }
 
+// ---------------------------------------------------------------------------
+// Allocation-free solve.  Its Krylov vectors, block partials and scalars live
+// in one fixed array of this file instead of memory obtained from cudaMalloc.
+// Layout (doubles): 9 vectors of UFEM_NOALLOC_MAX_ROWS (r, r^, p, v, s, t, p^,
+// s^, inverse diagonal), 2 * kMaxPartials partials, 16 scalars, 8 for the
+// integer flags.
+// ---------------------------------------------------------------------------
+constexpr int64_t kNoAllocRows = UFEM_NOALLOC_MAX_ROWS;
+constexpr int kMaxPartials = 296;  // the largest block count ensure_work chooses
+constexpr int64_t kNoAllocDoubles = 9 * kNoAllocRows + 2 * kMaxPartials + 16 + 8;
+
+static __device__ __align__(256) double g_noalloc_scratch[kNoAllocDoubles];
+
+namespace {
+constexpr int kMaxDevices = 64;
+
+// Device address of g_noalloc_scratch on the current device, looked up once per
+// device (the host-side symbol is only a stand-in and must not reach a kernel).
+int noalloc_scratch(double** out) {
+  static double* addr[kMaxDevices] = {};
+  int dev = 0;
+  UFEM_CUDA_TRY(cudaGetDevice(&dev));
+  if (dev < 0 || dev >= kMaxDevices) return set_error(UFEM_ERR_LIMIT, "device ordinal out of range");
+  if (!addr[dev]) {
+    void* p = nullptr;
+    UFEM_CUDA_TRY(cudaGetSymbolAddress(&p, g_noalloc_scratch));
+    addr[dev] = static_cast<double*>(p);
+  }
+  *out = addr[dev];
+  return UFEM_OK;
+}
+}  // namespace
+
 }  // namespace ufem
+
+extern "C" int ufem_ns_solve_noalloc(ufem_ns_handle* h, const ufem_krylov_opts* kopts, ufem_krylov_status* status,
+                                     void* stream) {
+  using namespace ufem;
+  if (!h) return set_error(UFEM_ERR_ARG, "NULL handle");
+  ufem_krylov_opts o;
+  ufem_krylov_default_opts(&o);
+  if (kopts) o = *kopts;
+  if (o.method != 1) return set_error(UFEM_ERR_ARG, "ufem_ns_solve_noalloc supports BiCGStab (method 1) only");
+  if (o.precond != 0 && o.precond != 1)
+    return set_error(UFEM_ERR_ARG, "ufem_ns_solve_noalloc supports no preconditioner or point Jacobi only");
+  if (o.mixed != 0) return set_error(UFEM_ERR_ARG, "ufem_ns_solve_noalloc solves in FP64 only (mixed = 0)");
+  if (o.max_iters <= 0) o.max_iters = 3000;
+  if (o.tol <= 0) o.tol = 1e-10;
+  const int64_t n = h->nrows;
+  if (n > kNoAllocRows)
+    return set_error(UFEM_ERR_LIMIT, "system has " + std::to_string(n) + " rows; ufem_ns_solve_noalloc handles at most " +
+                                         std::to_string(kNoAllocRows));
+  double* base = nullptr;
+  int rc;
+  if ((rc = noalloc_scratch(&base))) return rc;
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  double h_d[16];
+  int h_i[8];
+  KrylovWork kw;  // a view of the fixed scratch; owns nothing
+  kw.n = n;
+  kw.nblk = int(std::min<int64_t>(kMaxPartials, std::max<int64_t>(1, (n + 2047) / 2048)));
+  double* vec[9];
+  for (int k = 0; k < 9; ++k) vec[k] = base + k * kNoAllocRows;
+  kw.part = base + 9 * kNoAllocRows;
+  kw.dctl = kw.part + 2 * kMaxPartials;
+  kw.ictl = reinterpret_cast<int*>(kw.dctl + 16);
+  kw.h_dctl = h_d;
+  kw.h_ictl = h_i;
+  SolveResult r;
+  rc = bicgstab<double, double, double>(h, kw, h->d_vals, h->d_rhs, h->d_sol, vec[0], vec[1], vec[2], vec[3], vec[4],
+                                        vec[5], vec[6], vec[7], vec[8], o.precond, o.tol, o.max_iters, s, r);
+  if (rc) return rc;
+  ufem_krylov_status st{};
+  st.converged = r.converged;
+  st.status = r.status;
+  st.iterations = r.iters;
+  st.rel_residual = r.relres;
+  if (status) *status = st;
+  if (!st.converged)
+    return set_error(UFEM_ERR_SOLVE, "Krylov solve did not converge, relative residual " + std::to_string(st.rel_residual));
+  return UFEM_OK;
+}

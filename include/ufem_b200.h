@@ -172,6 +172,25 @@ int ufem_ns_apply_dirichlet(ufem_ns_handle* h, void* stream);
 /* SolveLSS (SolveLSS.cpp:44-55): Krylov solve for the increment. */
 int ufem_ns_solve(ufem_ns_handle* h, const ufem_krylov_opts* kopts, ufem_krylov_status* status,
                   void* stream);
+/* Allocation-free variant of ufem_ns_solve.  No counterpart in the reference.
+ * For callers that cannot call cudaMalloc: applications that hand all device
+ * memory to their own pool or enforce a fixed device-memory budget, and loops
+ * that must not take the implicit device synchronisation of a first-use
+ * allocation.  ufem_ns_solve allocates its Krylov workspace on first use; this
+ * entry point instead uses a fixed scratch area inside the library (about 9.5 MB
+ * of device memory, held on every GPU that loads the library until the process
+ * exits) and calls no cudaMalloc, cudaFree or allocating library routine.
+ *  - Solves the system the handle holds: BiCGStab (method 1) with point Jacobi or
+ *    no preconditioner, FP64 (mixed = 0); other options give UFEM_ERR_ARG.
+ *  - At most UFEM_NOALLOC_MAX_ROWS rows; larger systems give UFEM_ERR_LIMIT.
+ *  - The first call on a device looks up the scratch area's device address; make
+ *    that first call before any stream capture.
+ *  - Every call shares the one scratch area (it keeps the last call's contents,
+ *    and each call initialises what it reads): calls that overlap on the GPU,
+ *    from any handle or stream, race.  Serialise them. */
+#define UFEM_NOALLOC_MAX_ROWS 131072
+int ufem_ns_solve_noalloc(ufem_ns_handle* h, const ufem_krylov_opts* kopts, ufem_krylov_status* status,
+                          void* stream);
 /* UpdateActions (NavierStokes.cpp:172-179). */
 int ufem_ns_update(ufem_ns_handle* h, void* stream);
 /* nsteps full time steps; status of the last solve. */
