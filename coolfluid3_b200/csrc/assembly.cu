@@ -735,9 +735,9 @@ __device__ __forceinline__ void spec_tet_row(const int (&ids)[4], int ai, const 
 template <int D, typename T, int CH>
 constexpr size_t assembly_smem_bytes() {
   return size_t(P1<D>::nvals + P1<D>::neq) * CH * sizeof(T) +  // st, rst
-         size_t(P1<D>::n) * CH * 8 +                          // s_mask
+         size_t(CH) * 8 +                                     // s_mask (sum of row slots <= CH)
          size_t(CH) * 4 +                                     // s_info
-         size_t(4 * CH + 3) * 4;                              // s_rowinc, s_pref, s_spref, s_slots
+         size_t(5 * CH + 3) * 4;                              // s_rowinc, s_pref, s_spref, s_slots, s_self
 }
 
 // The row-owner assembly kernel.  One CTA per chunk of whole block rows.
@@ -752,12 +752,13 @@ __global__ void __launch_bounds__(CH) ns_assembly_kernel(
   extern __shared__ __align__(16) unsigned char smem_raw[];
   T* st = reinterpret_cast<T*>(smem_raw);
   T* rst = st + nvals * CH;
-  unsigned long long* s_mask = reinterpret_cast<unsigned long long*>(rst + neq * CH);  // n * CH
-  uint32_t* s_info = reinterpret_cast<uint32_t*>(s_mask + n * CH);                     // CH
+  unsigned long long* s_mask = reinterpret_cast<unsigned long long*>(rst + neq * CH);  // CH
+  uint32_t* s_info = reinterpret_cast<uint32_t*>(s_mask + CH);                         // CH
   int* s_rowinc = reinterpret_cast<int*>(s_info + CH);                                 // CH + 1
   int* s_pref = s_rowinc + CH + 1;                                                     // CH + 1
   int* s_spref = s_pref + CH + 1;                                                      // CH + 1
   int* s_slots = s_spref + CH + 1;                                                     // CH
+  int* s_self = s_slots + CH;                                                          // CH: slot of the row node
 
   const int chunk = blockIdx.x;
   const int row0 = chunk_row0[chunk], row1 = chunk_row0[chunk + 1];
@@ -769,14 +770,14 @@ __global__ void __launch_bounds__(CH) ns_assembly_kernel(
   // Row metadata and zeroed contributor masks
   for (int rl = t; rl <= R; rl += CH) s_rowinc[rl] = row_inc[row0 + rl] - inc0;
   for (int rl = t; rl < R; rl += CH) s_slots[rl] = int(start[row0 + rl + 1] - start[row0 + rl]);
-  for (int k = t; k < n * CH; k += CH) s_mask[k] = 0ull;
+  for (int k = t; k < CH; k += CH) s_mask[k] = 0ull;
   __syncthreads();
   if (t == 0) {
     int items = 0, slots = 0;
     s_pref[0] = 0;
     s_spref[0] = 0;
     for (int rl = 0; rl < R; ++rl) {
-      items += s_slots[rl] * neq;
+      items += (s_slots[rl] - 1) * neq;  // off-diagonal blocks
       slots += s_slots[rl];
       s_pref[rl + 1] = items;
       s_spref[rl + 1] = slots;
@@ -820,16 +821,23 @@ __global__ void __launch_bounds__(CH) ns_assembly_kernel(
       if (s_rowinc[mid] <= t) lo = mid; else hi = mid - 1;
     }
     const int bit = t - s_rowinc[lo];
+    if (bit == 0) s_self[lo] = int(pslots & 0xFFu);  // relabelled node 0 is the row node
     if (bit < 64) {
       const int sb = s_spref[lo];
 #pragma unroll
-      for (int q = 0; q < n; ++q) atomicOr(s_mask + sb + int((pslots >> (8 * q)) & 0xFFu), 1ull << bit);
+      for (int q = 1; q < n; ++q) {  // off-diagonal slots; the diagonal block takes every incidence
+        unsigned* word = reinterpret_cast<unsigned*>(s_mask + sb + int((pslots >> (8 * q)) & 0xFFu)) + (bit >> 5);
+        atomicOr(word, 1u << (bit & 31));
+      }
     }
   }
   __syncthreads();
 
-  // Phase 2a: CSR values, one thread per (row, equation, neighbour slot); the
-  // contributors of a slot are visited in ascending element order.
+  // Phase 2a: off-diagonal CSR blocks, one thread per (row, equation,
+  // neighbour slot != self); the slot's contributors are visited in ascending
+  // element order.  Off-diagonal slots have a few contributors each, so the
+  // warps stay converged; the diagonal blocks (every incidence of the row)
+  // follow in phase 2b.
   const int nitems = s_pref[R];
   for (int it = t; it < nitems; it += CH) {
     int lo = 0, hi = R - 1;
@@ -840,8 +848,9 @@ __global__ void __launch_bounds__(CH) ns_assembly_kernel(
     const int rl = lo;
     const int S = s_slots[rl];
     const int local = it - s_pref[rl];
-    const int r = local / S;
-    const int s = local - r * S;
+    const int r = local / (S - 1);
+    const int s1 = local - r * (S - 1);
+    const int s = s1 + (s1 >= s_self[rl] ? 1 : 0);
     const int kb = s_rowinc[rl], ke = s_rowinc[rl + 1];
     const uint32_t key = uint32_t(s) * 0x01010101u;
     double acc[neq];
@@ -868,8 +877,7 @@ __global__ void __launch_bounds__(CH) ns_assembly_kernel(
         }
       }
     }
-    const int64_t node = row0 + rl;
-    const int64_t base = int64_t(neq) * neq * start[node] + int64_t(r * S + s) * neq;
+    const int64_t base = int64_t(neq) * neq * start[row0 + rl] + int64_t(r * S + s) * neq;
 #pragma unroll
     for (int c = 0; c < neq; ++c) vals[base + c] = acc[c];
     if (vals32 != nullptr) {
@@ -877,13 +885,30 @@ __global__ void __launch_bounds__(CH) ns_assembly_kernel(
       for (int c = 0; c < neq; ++c) vals32[base + c] = float(acc[c]);
     }
   }
-  // Phase 2b: RHS, one thread per (row, equation)
+  // Phase 2b: diagonal blocks and RHS, one thread per (row, equation): every
+  // incidence of the row contributes, with the row node at local position 0.
   for (int it = t; it < R * neq; it += CH) {
     const int rl = it / neq, r = it - rl * neq;
     const int kb = s_rowinc[rl], ke = s_rowinc[rl + 1];
-    double acc = 0.0;
-    for (int kk = kb; kk < ke; ++kk) acc += double(rst[r * CH + kk]);
-    rhs[int64_t(row0 + rl) * neq + r] = acc;
+    double acc[neq];
+#pragma unroll
+    for (int c = 0; c < neq; ++c) acc[c] = 0.0;
+    double racc = 0.0;
+    const T* src = st + (r * neq) * CH;  // b = 0
+    for (int kk = kb; kk < ke; ++kk) {
+#pragma unroll
+      for (int c = 0; c < neq; ++c) acc[c] += double(src[c * CH + kk]);
+      racc += double(rst[r * CH + kk]);
+    }
+    const int S = s_slots[rl];
+    const int64_t base = int64_t(neq) * neq * start[row0 + rl] + int64_t(r * S + s_self[rl]) * neq;
+#pragma unroll
+    for (int c = 0; c < neq; ++c) vals[base + c] = acc[c];
+    if (vals32 != nullptr) {
+#pragma unroll
+      for (int c = 0; c < neq; ++c) vals32[base + c] = float(acc[c]);
+    }
+    rhs[int64_t(row0 + rl) * neq + r] = racc;
   }
 }
 
@@ -1011,9 +1036,7 @@ __global__ void dirichlet_rows_kernel(int64_t nbc, int neq, const int64_t* __res
   }
 }
 
-template <int D, typename T, int CH, bool SPEC>
-int launch_assembly_t(ufem_ns_handle* h, cudaStream_t s, bool write32) {
-  NSParams p;
+void fill_params(const ufem_ns_handle* h, NSParams& p) {
   const double dt = h->opt.dt, c1 = h->opt.c1;
   p.theta = h->opt.theta; p.inv_theta = 1.0 / h->opt.theta; p.dt = dt; p.invdt = 1.0 / dt;
   p.rho = h->opt.rho; p.inv_rho = 1.0 / h->opt.rho;
@@ -1023,6 +1046,12 @@ int launch_assembly_t(ufem_ns_handle* h, cudaStream_t s, bool write32) {
   p.c2 = h->opt.c2; p.a_ps = h->opt.alpha_ps; p.a_su = h->opt.alpha_su;
   p.a_bu = h->opt.alpha_bu; p.u_ref = h->opt.u_ref; p.supg_type = h->opt.supg_type;
   p.has_force = h->d_force != nullptr;
+}
+
+template <int D, typename T, int CH, bool SPEC>
+int launch_assembly_t(ufem_ns_handle* h, cudaStream_t s, bool write32) {
+  NSParams p;
+  fill_params(h, p);
   constexpr size_t smem = assembly_smem_bytes<D, T, CH>();
   const AssemblyPlan& plan = std::is_same<T, float>::value ? h->plan32 : h->plan64;
   if (plan.cap != CH) return set_error(UFEM_ERR_STATE, "assembly plan does not match the kernel width");

@@ -466,9 +466,11 @@ int ufem_ns_create(const ufem_mesh* mesh, const ufem_ns_options* opts, ufem_ns_h
     int64_t i = 0;
     while (i < N) {
       chunk_row0.push_back(int32_t(i));
-      int64_t k = 0;
-      while (i < N && k + (row_inc[i + 1] - row_inc[i]) <= cap) {
+      int64_t k = 0, sl = 0;  // incidences and neighbourhood slots of the chunk, each <= cap
+      while (i < N && k + (row_inc[i + 1] - row_inc[i]) <= cap &&
+             sl + (h->start_h[i + 1] - h->start_h[i]) <= cap) {
         k += row_inc[i + 1] - row_inc[i];
+        sl += h->start_h[i + 1] - h->start_h[i];
         ++i;
       }
       if (k == 0) return false;

@@ -105,7 +105,7 @@ struct ufem_ns_handle {
   ufem::AssemblyPlan plan32;       // chunks sized for the FP32-element kernel
   ufem::DirichletPlan bcp;
   ufem::KrylovWork* kw = nullptr;
-  bool vals32_valid = false;      // d_vals32 holds the current system (written by the assembly)
+  bool vals32_valid = false;            // d_vals32 holds the current system (written by the assembly)
 
   // transfer staging (reference field layouts <-> padded node records)
   double* d_stage = nullptr;      // N x 4*dim doubles
