@@ -265,7 +265,7 @@ void ufem_krylov_default_opts(ufem_krylov_opts* o) {
   o->tol = 1e-10;
   o->mixed = 0;
   o->max_refine = 20;
-  o->inner_tol = 1e-5;
+  o->inner_tol = 1e-3;
 }
 
 int ufem_mesh_rectangle_tris(int32_t nx, int32_t ny, double jitter, uint64_t seed, double* coords, uint32_t* conn) {

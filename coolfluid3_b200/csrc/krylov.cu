@@ -28,13 +28,11 @@ struct KrylovWork {
   int nblk = 0;
   // FP64 vectors
   double *V = nullptr, *w = nullptr, *z = nullptr, *t = nullptr, *r = nullptr, *dinv = nullptr;
-  // FP32 vectors for the inner solve of the mixed path
+  // FP32 vectors for the inner GMRES solve of the mixed path
   float *V32 = nullptr, *w32 = nullptr, *z32 = nullptr, *t32 = nullptr, *r32 = nullptr, *x32 = nullptr,
         *q32 = nullptr, *dinv32 = nullptr;
   // BiCGStab vectors
   double *bp = nullptr, *bv = nullptr, *bs = nullptr, *bt = nullptr, *brh = nullptr, *bph = nullptr, *bsh = nullptr;
-  float *bp32 = nullptr, *bv32 = nullptr, *bs32 = nullptr, *bt32 = nullptr, *brh32 = nullptr, *bph32 = nullptr,
-        *bsh32 = nullptr;
   // reductions and solver scalars (device)
   double* part = nullptr;  // (m+2) x nblk
   double* hbuf = nullptr;  // 2 x (m+2)
@@ -52,6 +50,7 @@ namespace {
 constexpr int kBnorm = 0, kBeta = 1, kEst = 2, kHnext = 3, kTrue = 4;
 constexpr int kRho = 5, kRhoOld = 6, kAlpha = 7, kOmega = 8, kRhV = 9, kTS = 10, kTT = 11, kR2 = 12, kScale = 13;
 constexpr int kRedThreads = 256;
+constexpr int kInnerIterCap = 400;  // iterations of one FP32 inner solve of the mixed path
 
 template <typename T>
 __device__ __forceinline__ T warp_sum(T v) {
@@ -596,25 +595,18 @@ int ensure_work(ufem_ns_handle* h, int m, bool need32, bool bicg) {
       if ((rc = dalloc(&kw.V, size_t(M + 1) * nd))) return rc;
     }
   }
-  if (need32) {
+  if (need32 && (rc = dalloc(&h->d_vals32, size_t(h->nnz)))) return rc;
+  if (need32 && !bicg) {  // mixed GMRES runs its inner solve on FP32 vectors
     if ((rc = dalloc(&kw.w32, nd)) || (rc = dalloc(&kw.z32, nd)) || (rc = dalloc(&kw.t32, nd)) ||
         (rc = dalloc(&kw.r32, nd)) || (rc = dalloc(&kw.x32, nd)) || (rc = dalloc(&kw.q32, nd)) ||
-        (rc = dalloc(&kw.dinv32, ndinv)) ||
-        (rc = dalloc(&h->d_vals32, size_t(h->nnz))))
+        (rc = dalloc(&kw.dinv32, ndinv)))
       return rc;
   }
-  if (bicg) {
-    if (need32) {
-      if ((rc = dalloc(&kw.bp32, nd)) || (rc = dalloc(&kw.bv32, nd)) || (rc = dalloc(&kw.bs32, nd)) ||
-          (rc = dalloc(&kw.bt32, nd)) || (rc = dalloc(&kw.brh32, nd)) || (rc = dalloc(&kw.bph32, nd)) ||
-          (rc = dalloc(&kw.bsh32, nd)))
-        return rc;
-    } else {
-      if ((rc = dalloc(&kw.bp, nd)) || (rc = dalloc(&kw.bv, nd)) || (rc = dalloc(&kw.bs, nd)) ||
-          (rc = dalloc(&kw.bt, nd)) || (rc = dalloc(&kw.brh, nd)) || (rc = dalloc(&kw.bph, nd)) ||
-          (rc = dalloc(&kw.bsh, nd)))
-        return rc;
-    }
+  if (bicg) {  // FP64 vectors, also for the mixed path (FP32 operator only)
+    if ((rc = dalloc(&kw.bp, nd)) || (rc = dalloc(&kw.bv, nd)) || (rc = dalloc(&kw.bs, nd)) ||
+        (rc = dalloc(&kw.bt, nd)) || (rc = dalloc(&kw.brh, nd)) || (rc = dalloc(&kw.bph, nd)) ||
+        (rc = dalloc(&kw.bsh, nd)))
+      return rc;
   }
   return UFEM_OK;
 }
@@ -837,7 +829,7 @@ int krylov_solve(ufem_ns_handle* h, const ufem_krylov_opts* ko, ufem_krylov_stat
   if (o.max_iters <= 0) o.max_iters = 3000;
   if (o.tol <= 0) o.tol = 1e-10;
   if (o.max_refine <= 0) o.max_refine = 20;
-  if (o.inner_tol <= 0) o.inner_tol = 1e-5;
+  if (o.inner_tol <= 0) o.inner_tol = 1e-3;
   if (o.precond < 0 || o.precond > 2) return set_error(UFEM_ERR_ARG, "precond must be 0, 1 or 2");
   if (o.method < 0 || o.method > 1) return set_error(UFEM_ERR_ARG, "method must be 0 (GMRES) or 1 (BiCGStab)");
   const bool mixed = o.mixed != 0;
@@ -898,26 +890,39 @@ int krylov_solve(ufem_ns_handle* h, const ufem_krylov_opts* ko, ufem_krylov_stat
       if (relres <= o.tol) { conv = true; break; }
       if (ref == o.max_refine || total >= o.max_iters * (o.max_refine + 1)) { status = 1; break; }
       // inner: A32 d = r / ||r||, d0 = 0
-      to32_scaled_kernel<<<g1, kRedThreads, 0, s>>>(n, kw.r, kw.r32, kw.dctl, kScale);
-      fill_kernel<float><<<g1, kRedThreads, 0, s>>>(n, 0.0f, kw.x32);
-      UFEM_CUDA_TRY(cudaGetLastError());
       // keep ||r|| for the update: the inner solve reuses the scalar slots
       UFEM_CUDA_TRY(cudaMemcpyAsync(kw.dctl + 14, kw.dctl + kScale, sizeof(double), cudaMemcpyDeviceToDevice, s));
       SolveResult ir;
-      if (bicg)
-        rc = bicgstab<float, float, float>(h, kw, h->d_vals32, kw.r32, kw.x32, kw.w32, kw.brh32, kw.bp32, kw.bv32,
-                                           kw.bs32, kw.bt32, kw.bph32, kw.bsh32, kw.dinv32, o.precond, o.inner_tol,
-                                           o.max_iters, s, ir);
-      else
+      // Each inner solve is short: FP32 Krylov recurrences stagnate near the
+      // FP32-attainable accuracy, so a capped inner solve followed by a fresh
+      // FP64 residual makes steadier progress than one long FP32 run.
+      const int inner_iters = std::min(o.max_iters, kInnerIterCap);
+      if (bicg) {
+        // FP32 operator (half the SpMV traffic), FP64 vectors and scalars: the
+        // recurrences keep FP64 accuracy, only the operator is rounded, so the
+        // refinement contracts by about cond(A) * 2^-24 per pass.
+        scale_kernel<double><<<g1, kRedThreads, 0, s>>>(n, kw.r, kw.t, kw.dctl, kScale, nullptr);
+        fill_kernel<double><<<g1, kRedThreads, 0, s>>>(n, 0.0, kw.z);
+        UFEM_CUDA_TRY(cudaGetLastError());
+        rc = bicgstab<double, float, double>(h, kw, h->d_vals32, kw.t, kw.z, kw.w, kw.brh, kw.bp, kw.bv, kw.bs, kw.bt,
+                                             kw.bph, kw.bsh, kw.dinv, o.precond, o.inner_tol, inner_iters, s, ir);
+      } else {
+        to32_scaled_kernel<<<g1, kRedThreads, 0, s>>>(n, kw.r, kw.r32, kw.dctl, kScale);
+        fill_kernel<float><<<g1, kRedThreads, 0, s>>>(n, 0.0f, kw.x32);
+        UFEM_CUDA_TRY(cudaGetLastError());
         rc = gmres<float, float, float>(h, h->d_vals32, kw.r32, kw.x32, kw.V32, kw.w32, kw.z32, kw.t32, kw.q32,
-                                        kw.dinv32, o.precond, o.inner_tol, o.max_iters, o.restart, s, ir);
+                                        kw.dinv32, o.precond, o.inner_tol, inner_iters, o.restart, s, ir);
+      }
       if (rc) return rc;
       total += ir.iters;
       // A breakdown (status 2) leaves a finite, partially converged correction:
       // apply it and let the next FP64 residual restart the inner solve.  A
       // non-finite inner iterate is never applied.
       if (ir.status == 3 || !std::isfinite(ir.relres)) { status = 3; relres = NAN; break; }
-      add_scaled_kernel<float><<<g1, kRedThreads, 0, s>>>(n, kw.x32, h->d_sol, kw.dctl, 14);
+      if (bicg)
+        add_scaled_kernel<double><<<g1, kRedThreads, 0, s>>>(n, kw.z, h->d_sol, kw.dctl, 14);
+      else
+        add_scaled_kernel<float><<<g1, kRedThreads, 0, s>>>(n, kw.x32, h->d_sol, kw.dctl, 14);
       UFEM_CUDA_TRY(cudaGetLastError());
     }
     out.converged = conv;
@@ -940,7 +945,6 @@ void krylov_free(ufem_ns_handle* h) {
   dfree(k.V); dfree(k.w); dfree(k.z); dfree(k.t); dfree(k.r); dfree(k.dinv);
   dfree(k.V32); dfree(k.w32); dfree(k.z32); dfree(k.t32); dfree(k.r32); dfree(k.x32); dfree(k.q32); dfree(k.dinv32);
   dfree(k.bp); dfree(k.bv); dfree(k.bs); dfree(k.bt); dfree(k.brh); dfree(k.bph); dfree(k.bsh);
-  dfree(k.bp32); dfree(k.bv32); dfree(k.bs32); dfree(k.bt32); dfree(k.brh32); dfree(k.bph32); dfree(k.bsh32);
   dfree(k.part); dfree(k.hbuf); dfree(k.H); dfree(k.cs); dfree(k.sn); dfree(k.g); dfree(k.y);
   dfree(k.dctl); dfree(k.ictl);
   if (k.h_dctl) cudaFreeHost(k.h_dctl);

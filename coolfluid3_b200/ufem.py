@@ -31,7 +31,7 @@ def _stream(stream) -> C.c_void_p | None:
 
 
 def krylov_options(method: str = "bicgstab", restart: int = 30, max_iters: int = 3000, precond: str = "jacobi",
-                   tol: float = 1e-10, mixed: bool = False, max_refine: int = 20, inner_tol: float = 1e-5):
+                   tol: float = 1e-10, mixed: bool = False, max_refine: int = 20, inner_tol: float = 1e-3):
     o = N.KrylovOpts()
     o.method = {"gmres": 0, "bicgstab": 1}[method]
     o.restart = restart

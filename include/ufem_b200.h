@@ -76,7 +76,7 @@ typedef struct ufem_krylov_opts {
   double tol;          /* ||b - A x|| / ||b|| target, default 1e-10                */
   int32_t mixed;       /* 0: all FP64; 1: FP32 inner Krylov + FP64 refinement     */
   int32_t max_refine;  /* outer refinement passes when mixed, default 20          */
-  double inner_tol;    /* relative tolerance of each inner FP32 solve, 1e-5       */
+  double inner_tol;    /* relative tolerance of each inner FP32 solve, 1e-3       */
 } ufem_krylov_opts;
 
 typedef struct ufem_krylov_status {
