@@ -104,6 +104,10 @@ SIGNATURES = {
     "ufem_ns_download_system": (C.c_int, [_P, _D, _D, _P]),
     "ufem_ns_device_view_get": (C.c_int, [_P, C.POINTER(DeviceView)]),
     "ufem_ns_apply": (C.c_int, [_P, _D, _D]),
+    "ufem_ns_set_assembly_kernel": (C.c_int, [_P, C.c_int32, C.c_int32]),
+    "ufem_ns_get_assembly_kernel": (C.c_int, [_P, C.POINTER(C.c_int32), C.POINTER(C.c_int32)]),
+    "ufem_ns_tune_assembly": (C.c_int, [_P, C.c_void_p, C.c_int32, C.POINTER(C.c_int32), C.POINTER(C.c_int32),
+                                        C.POINTER(C.c_float)]),
     "ufem_ns_enable_timing": (C.c_int, [_P, C.c_int32]),
     "ufem_ns_get_timings": (C.c_int, [_P, C.POINTER(Timings)]),
     "ufem_ns_destroy": (None, [_P]),

@@ -271,6 +271,24 @@ __device__ __forceinline__ void gauss_N(int q, T (&N)[D + 1]) {
   for (int k = 0; k < D; ++k) N[k + 1] = xi[k];
 }
 
+// Stores one row (neq values) of a staged element block: contiguous and
+// vectorised when the staging pitch CH is 1 (warp kernel, 16-byte aligned
+// rows), strided otherwise (chunk kernel, value-major staging).
+template <int NEQ, typename T>
+__device__ __forceinline__ void put_row(T* __restrict__ st, int idx, int CH, const T (&v)[NEQ]) {
+  if (NEQ == 4 && CH == 1) {
+    if constexpr (std::is_same<T, float>::value) {
+      *reinterpret_cast<float4*>(st + idx) = make_float4(v[0], v[1], v[2], v[3]);
+    } else {
+      reinterpret_cast<double2*>(st + idx)[0] = make_double2(v[0], v[1]);
+      reinterpret_cast<double2*>(st + idx)[1] = make_double2(v[2], v[3]);
+    }
+  } else {
+#pragma unroll
+    for (int c = 0; c < NEQ; ++c) st[(idx + c) * CH] = v[c];
+  }
+}
+
 // Shared tail of both element forms: rhs row a, M = invdt*T + theta*A with the
 // p row of A divided by theta first (NavierStokesAssembly.hpp:69-71), staged.
 template <int D, typename T>
@@ -284,11 +302,13 @@ __device__ __forceinline__ void stage_block(const T (&A)[D + 1][D + 1], const T 
 #pragma unroll
     for (int c = 0; c < neq; ++c) s += -A[r][c] * xb[c];
     rhs[r] += s;
+    T row[neq];
 #pragma unroll
     for (int c = 0; c < neq; ++c) {
       const T a = (r == D) ? A[r][c] * kp.inv_theta : A[r][c];  // _A(p) / theta
-      st[((b * neq + r) * neq + c) * CH] = kp.invdt * Tm[r][c] + kp.theta * a;
+      row[c] = kp.invdt * Tm[r][c] + kp.theta * a;
     }
+    put_row<neq, T>(st, (b * neq + r) * neq, CH, row);
   }
 }
 
@@ -451,16 +471,20 @@ __device__ __forceinline__ void generic_row(const int (&ids)[4], int a, const do
 #pragma unroll
     for (int i = 0; i < D; ++i) {
       const T tg = theta * gam[i];
+      T row[neq];
 #pragma unroll
-      for (int j = 0; j < D; ++j)
-        st[((b * neq + i) * neq + j) * CH] = tg * G[j][b] + (i == j ? diag : T(0));
-      st[((b * neq + i) * neq + D) * CH] = theta * (G[i][b] * sWS * inv_rho);
+      for (int j = 0; j < D; ++j) row[j] = tg * G[j][b] + (i == j ? diag : T(0));
+      row[D] = theta * (G[i][b] * sWS * inv_rho);
+      put_row<neq, T>(st, (b * neq + i) * neq, CH, row);
     }
     // row p: theta * (A / theta) + invdt * T = A + invdt * T
+    {
+      T row[neq];
 #pragma unroll
-    for (int j = 0; j < D; ++j)
-      st[((b * neq + D) * neq + j) * CH] = G[j][b] * sWSp + tps * G[j][0] * Vab + invdt * (tps * G[j][0] * m1);
-    st[((b * neq + D) * neq + D) * CH] = tps * D0[b] * inv_rho * V;
+      for (int j = 0; j < D; ++j) row[j] = G[j][b] * sWSp + tps * G[j][0] * Vab + invdt * (tps * G[j][0] * m1);
+      row[D] = tps * D0[b] * inv_rho * V;
+      put_row<neq, T>(st, (b * neq + D) * neq, CH, row);
+    }
     // pieces of A x
 #pragma unroll
     for (int k = 0; k < D; ++k) {
@@ -471,15 +495,17 @@ __device__ __forceinline__ void generic_row(const int (&ids)[4], int a, const do
     }
   }
   // rhs row 0 = a - A x  (A before the theta combination)
+  T rrow[neq];
 #pragma unroll
-  for (int i = 0; i < D; ++i) rst[i * CH] = au[i] - (kx[i] + gam[i] * div + sWS * inv_rho * gradp[i]);
+  for (int i = 0; i < D; ++i) rrow[i] = au[i] - (kx[i] + gam[i] * div + sWS * inv_rho * gradp[i]);
   T g0ax = 0, g0gp = 0;
 #pragma unroll
   for (int k = 0; k < D; ++k) {
     g0ax += G[k][0] * ax[k];
     g0gp += G[k][0] * gradp[k];
   }
-  rst[D * CH] = -(sWSp * div + tps * g0ax + tps * V * inv_rho * g0gp);
+  rrow[D] = -(sWSp * div + tps * g0ax + tps * V * inv_rho * g0gp);
+  put_row<neq, T>(rst, 0, CH, rrow);
 }
 
 // ---------------------------------------------------------------------------
@@ -608,8 +634,7 @@ __device__ __forceinline__ void spec_tri_row(const int (&ids)[4], int ai, const 
     load_state<2, T>(state, ids[j], xb);
     stage_block<2, T>(A, Tm, xb, kp, rhs, st, j, CH);
   }
-#pragma unroll
-  for (int r = 0; r < 3; ++r) rst[r * CH] = rhs[r];
+  put_row<3, T>(rst, 0, CH, rhs);
 }
 
 // Specialised tetrahedra, NavierStokesSpecializations.hpp:150-302, row i = a,
@@ -725,8 +750,7 @@ __device__ __forceinline__ void spec_tet_row(const int (&ids)[4], int ai, const 
     load_state<3, T>(state, ids[j], xb);
     stage_block<3, T>(A, Tm, xb, kp, rhs, st, j, CH);
   }
-#pragma unroll
-  for (int r = 0; r < 4; ++r) rst[r * CH] = rhs[r];
+  put_row<4, T>(rst, 0, CH, rhs);
 }
 
 // Shared memory of one chunk: staged row blocks [value][incidence] (T), staged
@@ -743,7 +767,7 @@ constexpr size_t assembly_smem_bytes() {
 // The row-owner assembly kernel.  One CTA per chunk of whole block rows.
 template <int D, typename T, int CH, bool SPEC>
 __global__ void __launch_bounds__(CH) ns_assembly_kernel(
-    const int32_t* __restrict__ chunk_row0, const int32_t* __restrict__ row_inc,
+    const int2* __restrict__ chunk_rows, const int32_t* __restrict__ row_inc,
     const int32_t* __restrict__ inc_elem, const uint32_t* __restrict__ inc_info, const int4* __restrict__ conn,
     const double* __restrict__ coords, const double* __restrict__ uadv, const double* __restrict__ state,
     const double* __restrict__ force, const int64_t* __restrict__ start, NSParams p, double* __restrict__ vals,
@@ -760,8 +784,8 @@ __global__ void __launch_bounds__(CH) ns_assembly_kernel(
   int* s_slots = s_spref + CH + 1;                                                     // CH
   int* s_self = s_slots + CH;                                                          // CH: slot of the row node
 
-  const int chunk = blockIdx.x;
-  const int row0 = chunk_row0[chunk], row1 = chunk_row0[chunk + 1];
+  const int2 cr = chunk_rows[blockIdx.x];
+  const int row0 = cr.x, row1 = cr.y;
   const int R = row1 - row0;  // 1 <= R <= K <= CH (every node has an incidence)
   const int inc0 = row_inc[row0];
   const int K = row_inc[row1] - inc0;
@@ -912,6 +936,224 @@ __global__ void __launch_bounds__(CH) ns_assembly_kernel(
   }
 }
 
+// ---------------------------------------------------------------------------
+// Warp-per-row-group assembly.  A warp owns a range of consecutive block rows
+// with at most 32 incidences in total; lane l evaluates incidence l of the
+// range (incidences are sorted by row, then element id) and stages its element
+// row block in the warp's shared-memory slice, value-major with a 33-element
+// pitch (conflict-free for both the per-lane writes and the per-value reads).
+// Contributor masks (bit = lane) are built with shared atomicOr, one word per
+// neighbour slot.  The lanes then own CSR items: a diagonal entry or an RHS
+// entry (sum over all lanes of the row) or an off-diagonal (row, equation,
+// slot) quad (sum over the mask bits).  Lanes are visited in ascending order,
+// i.e. every CSR value is the element-ordered sum of its contributions, as in
+// the chunk kernel, and each value is written once.
+// ---------------------------------------------------------------------------
+// Lane pitch of the staging slice, in elements of T: 16-byte aligned rows
+// whose quarter-warp 16-byte accesses hit distinct banks (3D), odd for the
+// scalar accesses of the 2D layout.
+template <int D, typename T>
+constexpr int warp_lane_pitch() {
+  return D == 3 ? (sizeof(T) == 4 ? 68 : 70) : 31;
+}
+
+template <int D, typename T>
+constexpr size_t warp_stage_bytes() {
+  return size_t(32) * warp_lane_pitch<D, T>() * sizeof(T) +  // staged row blocks + RHS rows, one slice per lane
+         size_t(D * 64 + 32 + 36 + 36) * 4;                   // slot masks per local position, pslots, prefix, offsets
+}
+static_assert(warp_stage_bytes<2, float>() % 16 == 0 && warp_stage_bytes<2, double>() % 16 == 0 &&
+                  warp_stage_bytes<3, float>() % 16 == 0 && warp_stage_bytes<3, double>() % 16 == 0,
+              "per-warp staging slices must stay 16-byte aligned");
+
+// Loads NV consecutive staged values (16-byte aligned when NV is a multiple of 4).
+template <int NV, typename T>
+__device__ __forceinline__ void load_run(const T* __restrict__ src, T (&v)[NV]) {
+  if constexpr (NV % 4 == 0 && std::is_same<T, float>::value) {
+#pragma unroll
+    for (int q = 0; q < NV / 4; ++q) {
+      const float4 x = reinterpret_cast<const float4*>(src)[q];
+      v[4 * q] = x.x; v[4 * q + 1] = x.y; v[4 * q + 2] = x.z; v[4 * q + 3] = x.w;
+    }
+  } else if constexpr (NV % 2 == 0 && std::is_same<T, double>::value && NV % 4 == 0) {
+#pragma unroll
+    for (int q = 0; q < NV / 2; ++q) {
+      const double2 x = reinterpret_cast<const double2*>(src)[q];
+      v[2 * q] = x.x; v[2 * q + 1] = x.y;
+    }
+  } else {
+#pragma unroll
+    for (int q = 0; q < NV; ++q) v[q] = src[q];
+  }
+}
+
+template <int D, typename T, bool SPEC, int WPB>
+__global__ void __launch_bounds__(32 * WPB) ns_assembly_warp_kernel(
+    int ngroups, const int2* __restrict__ groups, const int32_t* __restrict__ row_inc,
+    const int32_t* __restrict__ inc_elem, const uint32_t* __restrict__ inc_info, const int4* __restrict__ conn,
+    const double* __restrict__ coords, const double* __restrict__ uadv, const double* __restrict__ state,
+    const double* __restrict__ force, const int64_t* __restrict__ start, NSParams p, double* __restrict__ vals,
+    float* __restrict__ vals32, double* __restrict__ rhs) {
+  constexpr int n = P1<D>::n, neq = P1<D>::neq, nvals = P1<D>::nvals;
+  constexpr int LS = warp_lane_pitch<D, T>();
+  constexpr int RPI = (D == 3) ? 2 : 3;      // equations (CSR rows) per off-diagonal item
+  constexpr int RG = neq / RPI;              // items per (row, slot)
+  constexpr int NV = RPI * neq;              // values per off-diagonal item
+  constexpr unsigned FULL = 0xffffffffu;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  T* stage = reinterpret_cast<T*>(smem_raw + size_t(warp) * warp_stage_bytes<D, T>());
+  uint32_t* s_mask = reinterpret_cast<uint32_t*>(stage + 32 * LS);  // D x 64: local position 1..n-1, slot
+  uint32_t* s_pslots = s_mask + D * 64;                              // 32
+  int* s_pref = reinterpret_cast<int*>(s_pslots + 32);               // 33 (+3 pad)
+  int* s_off = s_pref + 36;                                          // 33 (+3 pad): lane offset of each row
+
+  const int g = blockIdx.x * WPB + warp;
+  if (g >= ngroups) return;  // whole warp; no CTA-wide barrier below
+  const int2 gr = groups[g];
+  const int row0 = gr.x, R = gr.y - gr.x;  // 1 <= R <= K <= 32
+  const int i0 = __ldg(row_inc + row0);
+  const int K = __ldg(row_inc + row0 + R) - i0;
+  int my_off = 0, my_items = 0;
+  if (lane < R) {
+    my_off = __ldg(row_inc + row0 + lane) - i0;
+    my_items = int(__ldg(start + row0 + lane + 1) - __ldg(start + row0 + lane) - 1) * RG;
+  }
+  int pref = my_items;  // inclusive scan of the off-diagonal item counts
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const int v = __shfl_up_sync(FULL, pref, o);
+    if (lane >= o) pref += v;
+  }
+  const int nitems = __shfl_sync(FULL, pref, R - 1);
+  if (lane < R) {
+    s_pref[lane + 1] = pref;
+    s_off[lane] = my_off;
+  }
+  if (lane == 0) {
+    s_pref[0] = 0;
+    s_off[R] = K;
+  }
+#pragma unroll
+  for (int q = 0; q < D * 2; ++q) s_mask[q * 32 + lane] = 0u;
+  __syncwarp();
+
+  // Phase 1: one lane per incidence; the row node is relabelled to local
+  // position 0 exactly as in the chunk kernel.  Lane k stages its block
+  // (local column node b, equation r, component c) at k*LS + (b*neq + r)*neq + c
+  // and its RHS row at k*LS + nvals + r.
+  uint32_t pslots = 0xFFFFFFFFu;
+  if (lane < K) {
+    const int k = i0 + lane;
+    const int e = __ldg(inc_elem + k);
+    const uint32_t info = __ldg(inc_info + k);
+    const int a = int(info >> 24) & 3;
+    const int4 cn = __ldg(conn + e);
+    const int ids0[4] = {cn.x, cn.y, cn.z, cn.w};
+    int ids[4];
+    pslots = 0;
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      const int src = (D == 3) ? (q ^ a) : (q < 3 ? (q + a) % 3 : 3);
+      ids[q] = ids0[src];
+      const uint32_t sl = (q < n) ? ((info >> (6 * src)) & 63u) : 0xFFu;
+      pslots |= sl << (8 * q);
+    }
+    T* st = stage + lane * LS;
+    const KParams<T> kp = make_kparams<T>(p);
+    if constexpr (SPEC) {
+      if constexpr (D == 2) spec_tri_row<T>(ids, a, coords, uadv, state, kp, st, st + nvals, 1);
+      else spec_tet_row<T>(ids, a, coords, uadv, state, kp, st, st + nvals, 1);
+    } else {
+      generic_row<D, T>(ids, a, coords, uadv, state, force, kp, st, st + nvals, 1);
+    }
+#pragma unroll
+    for (int q = 1; q < n; ++q) atomicOr(s_mask + (q - 1) * 64 + ((pslots >> (8 * q)) & 0xFFu), 1u << lane);
+  }
+  s_pslots[lane] = pslots;
+  __syncwarp();
+
+  // Phase 2a: diagonal entries and RHS entries, neq * (neq + 1) items per row,
+  // each the sum over the row's lanes in element order.
+  constexpr int ND = neq * (neq + 1);
+  for (int it = lane; it < R * ND; it += 32) {
+    const int rl = it / ND, j = it - rl * ND;
+    const int kb = s_off[rl], ke = s_off[rl + 1];  // lanes of row rl
+    const int row = row0 + rl;
+    const T* src = stage + (j < neq * neq ? j : nvals + (j - neq * neq));  // b = 0 block, or the RHS row
+    double acc = 0.0;
+    for (int k = kb; k < ke; ++k) acc += double(src[k * LS]);
+    if (j < neq * neq) {
+      const int r = j / neq, c = j - r * neq;
+      const int64_t s0 = __ldg(start + row);
+      const int S = int(__ldg(start + row + 1) - s0);
+      const int self = int(s_pslots[kb] & 0xFFu);
+      const int64_t pos = int64_t(neq) * neq * s0 + int64_t(r * S + self) * neq + c;
+      vals[pos] = acc;
+      if (vals32 != nullptr) vals32[pos] = float(acc);
+    } else {
+      rhs[int64_t(row) * neq + (j - neq * neq)] = acc;
+    }
+  }
+
+  // Phase 2b: off-diagonal items (row, slot != self, group of RPI equations):
+  // the contributors of slot s are the row's lanes holding s at local position
+  // b = 1..n-1, visited in ascending lane (= element) order.
+  for (int it = lane; it < nitems; it += 32) {
+    int lo = 0, hi = R - 1;
+    while (lo < hi) {  // last rl with s_pref[rl] <= it
+      const int mid = (lo + hi + 1) >> 1;
+      if (s_pref[mid] <= it) lo = mid; else hi = mid - 1;
+    }
+    const int rl = lo;
+    const int row = row0 + rl;
+    const int64_t s0 = __ldg(start + row);
+    const int S = int(__ldg(start + row + 1) - s0);
+    const int local = it - s_pref[rl];
+    const int s1 = local / RG;
+    const int rg = local - s1 * RG;
+    const int kb = s_off[rl], ke = s_off[rl + 1];
+    const int self = int(s_pslots[kb] & 0xFFu);
+    const int s = s1 + (s1 >= self ? 1 : 0);
+    const unsigned rowmask = unsigned((1ull << ke) - (1ull << kb));
+    const unsigned m1 = s_mask[s] & rowmask;
+    const unsigned m2 = s_mask[64 + s] & rowmask;
+    const unsigned m3 = (D == 3) ? (s_mask[128 + s] & rowmask) : 0u;
+    unsigned m = m1 | m2 | m3;
+    double acc[NV];
+#pragma unroll
+    for (int q = 0; q < NV; ++q) acc[q] = 0.0;
+    while (m) {
+      const int k = __ffs(m) - 1;
+      m &= m - 1;
+      const int b = 1 + int((m2 >> k) & 1u) + 2 * int((m3 >> k) & 1u);
+      T v[NV];
+      load_run<NV, T>(stage + k * LS + (b * neq + rg * RPI) * neq, v);
+#pragma unroll
+      for (int q = 0; q < NV; ++q) acc[q] += double(v[q]);
+    }
+#pragma unroll
+    for (int rr = 0; rr < RPI; ++rr) {
+      const int r = rg * RPI + rr;
+      const int64_t pos = int64_t(neq) * neq * s0 + int64_t(r * S + s) * neq;
+      if constexpr (neq == 4) {
+        reinterpret_cast<double2*>(vals + pos)[0] = make_double2(acc[4 * rr], acc[4 * rr + 1]);
+        reinterpret_cast<double2*>(vals + pos)[1] = make_double2(acc[4 * rr + 2], acc[4 * rr + 3]);
+        if (vals32 != nullptr)
+          *reinterpret_cast<float4*>(vals32 + pos) =
+              make_float4(float(acc[4 * rr]), float(acc[4 * rr + 1]), float(acc[4 * rr + 2]), float(acc[4 * rr + 3]));
+      } else {
+#pragma unroll
+        for (int c = 0; c < neq; ++c) vals[pos + c] = acc[rr * neq + c];
+        if (vals32 != nullptr) {
+#pragma unroll
+          for (int c = 0; c < neq; ++c) vals32[pos + c] = float(acc[rr * neq + c]);
+        }
+      }
+    }
+  }
+}
+
 // LinearizeU (NavierStokes.cpp:105), evaluated left to right without FMA
 // contraction: u_adv = ((2.1875u - 2.1875u1) + 1.3125u2) - 0.3125u3.  Also
 // copies nu_eff into the node record read by the assembly.
@@ -1049,14 +1291,27 @@ void fill_params(const ufem_ns_handle* h, NSParams& p) {
 }
 
 template <int D, typename T, int CH, bool SPEC>
-int launch_assembly_t(ufem_ns_handle* h, cudaStream_t s, bool write32) {
-  NSParams p;
-  fill_params(h, p);
+int launch_chunk_t(const ufem_ns_handle* h, const AssemblyPlan& plan, const NSParams& p, cudaStream_t s,
+                   bool write32) {
+  if (plan.nchunks == 0) return UFEM_OK;
   constexpr size_t smem = assembly_smem_bytes<D, T, CH>();
-  const AssemblyPlan& plan = std::is_same<T, float>::value ? h->plan32 : h->plan64;
   if (plan.cap != CH) return set_error(UFEM_ERR_STATE, "assembly plan does not match the kernel width");
   ns_assembly_kernel<D, T, CH, SPEC><<<plan.nchunks, CH, smem, s>>>(
-      plan.chunk_row0, h->d_row_inc, h->d_inc_elem, h->d_inc_info, reinterpret_cast<const int4*>(h->d_conn),
+      plan.chunks, h->d_row_inc, h->d_inc_elem, h->d_inc_info, reinterpret_cast<const int4*>(h->d_conn),
+      h->d_coords, h->d_uadv, h->d_state, h->d_force, h->d_start, p, h->d_vals, write32 ? h->d_vals32 : nullptr,
+      h->d_rhs);
+  UFEM_CUDA_TRY(cudaGetLastError());
+  return UFEM_OK;
+}
+
+template <int D, typename T, bool SPEC, int WPB>
+int launch_warp_t(const ufem_ns_handle* h, const NSParams& p, cudaStream_t s, bool write32) {
+  const WarpPlan& wp = h->wplan;
+  if (wp.ngroups == 0) return UFEM_OK;
+  constexpr size_t smem = warp_stage_bytes<D, T>() * WPB;
+  const unsigned grid = unsigned((wp.ngroups + WPB - 1) / WPB);
+  ns_assembly_warp_kernel<D, T, SPEC, WPB><<<grid, 32 * WPB, smem, s>>>(
+      wp.ngroups, wp.groups, h->d_row_inc, h->d_inc_elem, h->d_inc_info, reinterpret_cast<const int4*>(h->d_conn),
       h->d_coords, h->d_uadv, h->d_state, h->d_force, h->d_start, p, h->d_vals, write32 ? h->d_vals32 : nullptr,
       h->d_rhs);
   UFEM_CUDA_TRY(cudaGetLastError());
@@ -1064,10 +1319,32 @@ int launch_assembly_t(ufem_ns_handle* h, cudaStream_t s, bool write32) {
 }
 
 template <int D, typename T, int CH, bool SPEC>
+int launch_assembly_t(ufem_ns_handle* h, cudaStream_t s, bool write32) {
+  NSParams p;
+  fill_params(h, p);
+  constexpr bool f32 = std::is_same<T, float>::value;
+  if (h->asm_variant == kAsmChunk) return launch_chunk_t<D, T, CH, SPEC>(h, f32 ? h->plan32 : h->plan64, p, s, write32);
+  int rc;
+  switch (h->asm_warps) {
+    case 2: rc = launch_warp_t<D, T, SPEC, 2>(h, p, s, write32); break;
+    case 8: rc = launch_warp_t<D, T, SPEC, 8>(h, p, s, write32); break;
+    default: rc = launch_warp_t<D, T, SPEC, 4>(h, p, s, write32); break;
+  }
+  if (rc) return rc;
+  return launch_chunk_t<D, T, CH, SPEC>(h, f32 ? h->wplan.big32 : h->wplan.big64, p, s, write32);
+}
+
+template <int D, typename T, int CH, bool SPEC>
 int set_smem_attr() {
   constexpr size_t smem = assembly_smem_bytes<D, T, CH>();
   UFEM_CUDA_TRY(cudaFuncSetAttribute(ns_assembly_kernel<D, T, CH, SPEC>,
                                      cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
+  UFEM_CUDA_TRY(cudaFuncSetAttribute(ns_assembly_warp_kernel<D, T, SPEC, 2>,
+                                     cudaFuncAttributeMaxDynamicSharedMemorySize, int(2 * warp_stage_bytes<D, T>())));
+  UFEM_CUDA_TRY(cudaFuncSetAttribute(ns_assembly_warp_kernel<D, T, SPEC, 4>,
+                                     cudaFuncAttributeMaxDynamicSharedMemorySize, int(4 * warp_stage_bytes<D, T>())));
+  UFEM_CUDA_TRY(cudaFuncSetAttribute(ns_assembly_warp_kernel<D, T, SPEC, 8>,
+                                     cudaFuncAttributeMaxDynamicSharedMemorySize, int(8 * warp_stage_bytes<D, T>())));
   return UFEM_OK;
 }
 

@@ -224,7 +224,8 @@ void destroy_impl(ufem_ns_handle* h) {
   dfree(h->d_nu); dfree(h->d_force); dfree(h->d_start); dfree(h->d_adj); dfree(h->d_rowptr);
   dfree(h->d_colidx); dfree(h->d_vals); dfree(h->d_vals32); dfree(h->d_rhs); dfree(h->d_sol);
   dfree(h->d_diagpos); dfree(h->d_row_inc); dfree(h->d_inc_elem); dfree(h->d_inc_info);
-  dfree(h->plan64.chunk_row0); dfree(h->plan32.chunk_row0); dfree(h->d_stage); dfree(h->d_x); dfree(h->d_y);
+  dfree(h->plan64.chunks); dfree(h->plan32.chunks); dfree(h->wplan.groups);
+  dfree(h->wplan.big64.chunks); dfree(h->wplan.big32.chunks); dfree(h->d_stage); dfree(h->d_x); dfree(h->d_y);
   for (auto& e : h->ev)
     if (e) cudaEventDestroy(e);
   delete h;
@@ -461,30 +462,50 @@ int ufem_ns_create(const ufem_mesh* mesh, const ufem_ns_options* opts, ufem_ns_h
         inc_info[p] = info;
       }
   });
-  // --- chunks of whole rows with at most `cap` incidences, one plan per kernel width
-  auto make_chunks = [&](int cap, std::vector<int32_t>& chunk_row0) -> bool {
+  // --- chunks of whole rows with at most `cap` incidences (and slots), one plan
+  // per kernel width; `only_big` restricts a plan to the rows the warp kernel
+  // leaves out (more than 32 incidences).
+  auto inc_of = [&](int64_t i) { return int64_t(row_inc[i + 1] - row_inc[i]); };
+  auto slots_of = [&](int64_t i) { return h->start_h[i + 1] - h->start_h[i]; };
+  auto make_chunks = [&](int cap, bool only_big, std::vector<int2>& chunks) -> bool {
     int64_t i = 0;
     while (i < N) {
-      chunk_row0.push_back(int32_t(i));
+      if (only_big && inc_of(i) <= 32) { ++i; continue; }
+      const int64_t first = i;
       int64_t k = 0, sl = 0;  // incidences and neighbourhood slots of the chunk, each <= cap
-      while (i < N && k + (row_inc[i + 1] - row_inc[i]) <= cap &&
-             sl + (h->start_h[i + 1] - h->start_h[i]) <= cap) {
-        k += row_inc[i + 1] - row_inc[i];
-        sl += h->start_h[i + 1] - h->start_h[i];
+      while (i < N && (!only_big || inc_of(i) > 32) && k + inc_of(i) <= cap && sl + slots_of(i) <= cap) {
+        k += inc_of(i);
+        sl += slots_of(i);
         ++i;
       }
-      if (k == 0) return false;
+      if (i == first) return false;
+      chunks.push_back(make_int2(int(first), int(i)));
     }
-    chunk_row0.push_back(int32_t(N));
     return true;
   };
-  std::vector<int32_t> chunks64, chunks32;
-  if (!make_chunks(assembly_chunk_capacity(dim, 0), chunks64) || !make_chunks(assembly_chunk_capacity(dim, 1), chunks32))
+  std::vector<int2> chunks64, chunks32, big64, big32, groups;
+  if (!make_chunks(assembly_chunk_capacity(dim, 0), false, chunks64) ||
+      !make_chunks(assembly_chunk_capacity(dim, 1), false, chunks32) ||
+      !make_chunks(assembly_chunk_capacity(dim, 0), true, big64) ||
+      !make_chunks(assembly_chunk_capacity(dim, 1), true, big32))
     return fail(set_error(UFEM_ERR_LIMIT, "a node has more incident elements than one assembly chunk holds"));
+  // --- warp groups: consecutive rows with at most 32 incidences in total
+  for (int64_t i = 0; i < N;) {
+    if (inc_of(i) > 32) { ++i; continue; }
+    const int64_t first = i;
+    int64_t k = 0;
+    while (i < N && inc_of(i) <= 32 && k + inc_of(i) <= 32) k += inc_of(i++);
+    groups.push_back(make_int2(int(first), int(i)));
+  }
   h->plan64.cap = assembly_chunk_capacity(dim, 0);
-  h->plan64.nchunks = int(chunks64.size()) - 1;
+  h->plan64.nchunks = int(chunks64.size());
   h->plan32.cap = assembly_chunk_capacity(dim, 1);
-  h->plan32.nchunks = int(chunks32.size()) - 1;
+  h->plan32.nchunks = int(chunks32.size());
+  h->wplan.ngroups = int(groups.size());
+  h->wplan.big64.cap = h->plan64.cap;
+  h->wplan.big64.nchunks = int(big64.size());
+  h->wplan.big32.cap = h->plan32.cap;
+  h->wplan.big32.nchunks = int(big32.size());
 
   // --- device allocations and uploads
   std::vector<double> c4(size_t(N) * 4, 0.0);
@@ -504,8 +525,11 @@ int ufem_ns_create(const ufem_mesh* mesh, const ufem_ns_options* opts, ufem_ns_h
       (rc = dmalloc(&h->d_row_inc, size_t(N) + 1, "row_inc")) ||
       (rc = dmalloc(&h->d_inc_elem, inc_elem.size(), "inc_elem")) ||
       (rc = dmalloc(&h->d_inc_info, inc_info.size(), "inc_info")) ||
-      (rc = dmalloc(&h->plan64.chunk_row0, chunks64.size(), "chunks64")) ||
-      (rc = dmalloc(&h->plan32.chunk_row0, chunks32.size(), "chunks32")) ||
+      (rc = dmalloc(&h->plan64.chunks, chunks64.size(), "chunks64")) ||
+      (rc = dmalloc(&h->plan32.chunks, chunks32.size(), "chunks32")) ||
+      (rc = dmalloc(&h->wplan.groups, std::max<size_t>(groups.size(), 1), "groups")) ||
+      (rc = dmalloc(&h->wplan.big64.chunks, std::max<size_t>(big64.size(), 1), "big64")) ||
+      (rc = dmalloc(&h->wplan.big32.chunks, std::max<size_t>(big32.size(), 1), "big32")) ||
       (rc = dmalloc(&h->d_stage, size_t(N) * 4 * dim, "stage")))
     return fail(rc);
   if (opts->precision == 1 && (rc = dmalloc(&h->d_vals32, size_t(h->nnz), "vals32"))) return fail(rc);
@@ -519,8 +543,11 @@ int ufem_ns_create(const ufem_mesh* mesh, const ufem_ns_options* opts, ufem_ns_h
       (ce = up(h->d_row_inc, row_inc.data(), row_inc.size() * 4)) ||
       (ce = up(h->d_inc_elem, inc_elem.data(), inc_elem.size() * 4)) ||
       (ce = up(h->d_inc_info, inc_info.data(), inc_info.size() * 4)) ||
-      (ce = up(h->plan64.chunk_row0, chunks64.data(), chunks64.size() * 4)) ||
-      (ce = up(h->plan32.chunk_row0, chunks32.data(), chunks32.size() * 4)))
+      (ce = up(h->plan64.chunks, chunks64.data(), chunks64.size() * sizeof(int2))) ||
+      (ce = up(h->plan32.chunks, chunks32.data(), chunks32.size() * sizeof(int2))) ||
+      (ce = up(h->wplan.groups, groups.data(), groups.size() * sizeof(int2))) ||
+      (ce = up(h->wplan.big64.chunks, big64.data(), big64.size() * sizeof(int2))) ||
+      (ce = up(h->wplan.big32.chunks, big32.data(), big32.size() * sizeof(int2))))
     return fail(set_error(UFEM_ERR_CUDA, std::string("upload: ") + cudaGetErrorString(ce)));
   if ((ce = cudaMemset(h->d_sol, 0, size_t(h->nrows) * 8)) || (ce = cudaMemset(h->d_state, 0, size_t(N) * 32)) ||
       (ce = cudaMemset(h->d_hist, 0, size_t(N) * 96)) || (ce = cudaMemset(h->d_uadv, 0, size_t(N) * 32)) ||
@@ -697,6 +724,81 @@ int ufem_ns_assemble(ufem_ns_handle* h, void* stream) {
   if ((rc = launch_assembly(h, s, w32))) return rc;
   record(h, 1, true, s);
   h->vals32_valid = w32;
+  return UFEM_OK;
+}
+
+int ufem_ns_set_assembly_kernel(ufem_ns_handle* h, int32_t variant, int32_t warps_per_cta) {
+  if (!h) return set_error(UFEM_ERR_ARG, "NULL handle");
+  if (variant != kAsmWarp && variant != kAsmChunk) return set_error(UFEM_ERR_ARG, "assembly variant must be 0 or 1");
+  if (warps_per_cta != 2 && warps_per_cta != 4 && warps_per_cta != 8)
+    return set_error(UFEM_ERR_ARG, "warps_per_cta must be 2, 4 or 8");
+  h->asm_variant = variant;
+  h->asm_warps = warps_per_cta;
+  return UFEM_OK;
+}
+
+int ufem_ns_get_assembly_kernel(ufem_ns_handle* h, int32_t* variant, int32_t* warps_per_cta) {
+  if (!h) return set_error(UFEM_ERR_ARG, "NULL handle");
+  if (variant) *variant = h->asm_variant;
+  if (warps_per_cta) *warps_per_cta = h->asm_warps;
+  return UFEM_OK;
+}
+
+int ufem_ns_tune_assembly(ufem_ns_handle* h, void* stream, int32_t reps, int32_t* variant, int32_t* warps_per_cta,
+                          float* ms_per_launch) {
+  if (!h) return set_error(UFEM_ERR_ARG, "NULL handle");
+  if (!h->state_set) return set_error(UFEM_ERR_STATE, "ufem_ns_set_state must be called before tuning");
+  if (reps < 1) reps = 5;
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  const bool w32 = h->d_vals32 != nullptr;
+  struct Cand { int variant, warps; };
+  const Cand cands[] = {{kAsmWarp, 2}, {kAsmWarp, 4}, {kAsmWarp, 8}, {kAsmChunk, 4}};
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  UFEM_CUDA_TRY(cudaEventCreate(&e0));
+  if (cudaEventCreate(&e1) != cudaSuccess) {
+    cudaEventDestroy(e0);
+    return set_error(UFEM_ERR_CUDA, "cudaEventCreate failed");
+  }
+  int rc = UFEM_OK;
+  float best = -1.0f;
+  Cand pick = cands[0];
+  const int saved_v = h->asm_variant, saved_w = h->asm_warps;
+  if ((rc = launch_linearize(h, s)) == UFEM_OK) {
+    for (const Cand& c : cands) {
+      h->asm_variant = c.variant;
+      h->asm_warps = c.warps;
+      if ((rc = launch_assembly(h, s, w32))) break;  // warm-up
+      cudaEventRecord(e0, s);
+      for (int r = 0; r < reps && rc == UFEM_OK; ++r) rc = launch_assembly(h, s, w32);
+      if (rc) break;
+      cudaEventRecord(e1, s);
+      cudaError_t ce = cudaEventSynchronize(e1);
+      float ms = 0.0f;
+      if (ce == cudaSuccess) ce = cudaEventElapsedTime(&ms, e0, e1);
+      if (ce != cudaSuccess) {
+        rc = set_error(UFEM_ERR_CUDA, std::string("assembly tuning: ") + cudaGetErrorString(ce));
+        break;
+      }
+      ms /= float(reps);
+      if (best < 0.0f || ms < best) {
+        best = ms;
+        pick = c;
+      }
+    }
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  if (rc) {
+    h->asm_variant = saved_v;
+    h->asm_warps = saved_w;
+    return rc;
+  }
+  h->asm_variant = pick.variant;
+  h->asm_warps = pick.warps;
+  h->vals32_valid = w32;
+  if (variant) *variant = pick.variant;
+  if (warps_per_cta) *warps_per_cta = pick.warps;
+  if (ms_per_launch) *ms_per_launch = best;
   return UFEM_OK;
 }
 

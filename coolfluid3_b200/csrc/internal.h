@@ -32,14 +32,26 @@ struct NSParams {
   int has_force;
 };
 
-// Row-owner assembly plan: CSR block rows are grouped into chunks of whole rows
-// whose incidences (row node, element) fit one CTA.  Incidences are sorted by
+// Row-owner assembly plans.  Incidences (row node, element) are sorted by
 // (row node, element id), so each CSR entry is summed in element order.
+//  - chunk plan: ranges of whole rows whose incidences fit one CTA of `cap`
+//    threads (one thread per incidence);
+//  - warp plan: ranges of consecutive rows with at most 32 incidences in total,
+//    one warp each (one lane per incidence).  Rows with more than 32 incidences
+//    are left to a chunk plan that lists only those rows.
 struct AssemblyPlan {
   int cap = 0;                 // incidences per chunk (== CTA threads)
   int nchunks = 0;
-  int32_t* chunk_row0 = nullptr;  // nchunks + 1 (device)
+  int2* chunks = nullptr;      // [first row, end row) per chunk (device)
 };
+struct WarpPlan {
+  int ngroups = 0;
+  int2* groups = nullptr;      // [first row, end row) per warp (device)
+  AssemblyPlan big64, big32;   // rows with more than 32 incidences
+};
+
+// Assembly kernel variants (selected per handle, see ufem_ns_set_assembly_kernel).
+enum AssemblyVariant { kAsmWarp = 0, kAsmChunk = 1 };
 
 // Symmetric-Dirichlet plan (sequential semantics of TrilinosFEVbrMatrix::
 // symmetric_dirichlet reduced to an order-preserving parallel form).
@@ -101,8 +113,11 @@ struct ufem_ns_handle {
   int32_t* d_inc_elem = nullptr;  // E*nn
   uint32_t* d_inc_info = nullptr; // E*nn : 6-bit slots + local index << 24
 
-  ufem::AssemblyPlan plan64;       // chunks sized for the FP64-element kernel
-  ufem::AssemblyPlan plan32;       // chunks sized for the FP32-element kernel
+  ufem::AssemblyPlan plan64;       // chunks sized for the FP64-element chunk kernel (all rows)
+  ufem::AssemblyPlan plan32;       // chunks sized for the FP32-element chunk kernel (all rows)
+  ufem::WarpPlan wplan;            // warp-per-row-group kernel
+  int asm_variant = ufem::kAsmWarp;
+  int asm_warps = 4;               // warps per CTA of the warp kernel
   ufem::DirichletPlan bcp;
   ufem::KrylovWork* kw = nullptr;
   bool vals32_valid = false;            // d_vals32 holds the current system (written by the assembly)

@@ -218,6 +218,27 @@ class NavierStokes:
         N.check(self._lib.ufem_ns_device_view_get(self._h, C.byref(v)))
         return {k: getattr(v, k) for k, _ in v._fields_}
 
+    # -- assembly kernel selection and autotuning -----------------------------
+    ASSEMBLY_VARIANTS = {"warp": 0, "chunk": 1}
+
+    def set_assembly_kernel(self, variant: str = "warp", warps_per_cta: int = 4) -> None:
+        """Pick the assembly kernel: "warp" (warp per row group) or "chunk" (CTA per row range)."""
+        N.check(self._lib.ufem_ns_set_assembly_kernel(self._h, self.ASSEMBLY_VARIANTS[variant], int(warps_per_cta)))
+
+    def assembly_kernel(self) -> tuple[str, int]:
+        v, w = C.c_int32(), C.c_int32()
+        N.check(self._lib.ufem_ns_get_assembly_kernel(self._h, C.byref(v), C.byref(w)))
+        names = {i: k for k, i in self.ASSEMBLY_VARIANTS.items()}
+        return names[v.value], w.value
+
+    def tune_assembly(self, reps: int = 5, stream: int = 0) -> dict:
+        """Time every assembly kernel candidate on this mesh and keep the fastest."""
+        v, w, ms = C.c_int32(), C.c_int32(), C.c_float()
+        N.check(self._lib.ufem_ns_tune_assembly(self._h, C.c_void_p(stream), int(reps), C.byref(v), C.byref(w),
+                                                C.byref(ms)))
+        names = {i: k for k, i in self.ASSEMBLY_VARIANTS.items()}
+        return {"variant": names[v.value], "warps_per_cta": w.value, "ms": ms.value}
+
     # -- timers (component timing of the reference) ----------------------------
     def enable_timing(self, on: bool = True) -> None:
         N.check(self._lib.ufem_ns_enable_timing(self._h, 1 if on else 0))

@@ -204,6 +204,23 @@ int ufem_ns_device_view_get(const ufem_ns_handle* h, ufem_ns_device_view* view);
 /* y = A x (FP64, host buffers) -- LSS::Matrix::apply with alpha=1, beta=0. */
 int ufem_ns_apply(ufem_ns_handle* h, const double* x, double* y);
 
+/* Assembly kernel selection.  No counterpart in the reference (one code path
+ * there).  variant 0: warp per group of consecutive rows holding at most 32
+ * incident elements (rows with more use the chunk kernel); variant 1: chunk
+ * kernel (one CTA per range of whole rows) for every row.  warps_per_cta:
+ * 2, 4 or 8 (variant 0 only).  All variants sum every CSR value in element
+ * order; they agree to rounding level (the compiler may contract multiply-adds
+ * of the element expression differently in each kernel), and each one is
+ * deterministic. */
+int ufem_ns_set_assembly_kernel(ufem_ns_handle* h, int32_t variant, int32_t warps_per_cta);
+int ufem_ns_get_assembly_kernel(ufem_ns_handle* h, int32_t* variant, int32_t* warps_per_cta);
+/* Autotuner: times every (variant, warps_per_cta) candidate on this handle's
+ * mesh and state (`reps` launches each after one warm-up, CUDA events on
+ * `stream`), keeps the fastest and reports it.  Requires ufem_ns_set_state.
+ * Overwrites the assembled system (assemble again afterwards). */
+int ufem_ns_tune_assembly(ufem_ns_handle* h, void* stream, int32_t reps, int32_t* variant,
+                          int32_t* warps_per_cta, float* ms_per_launch);
+
 int ufem_ns_enable_timing(ufem_ns_handle* h, int32_t enable);
 int ufem_ns_get_timings(ufem_ns_handle* h, ufem_ns_timings* t);
 
