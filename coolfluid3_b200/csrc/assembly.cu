@@ -13,6 +13,7 @@
 // once, coalesced.  No floating-point atomics, no element matrices in HBM.
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cmath>
 #include <cstdint>
 #include <type_traits>
@@ -989,7 +990,7 @@ __device__ __forceinline__ void load_run(const T* __restrict__ src, T (&v)[NV]) 
 
 template <int D, typename T, bool SPEC, int WPB>
 __global__ void __launch_bounds__(32 * WPB) ns_assembly_warp_kernel(
-    int ngroups, const int2* __restrict__ groups, const int32_t* __restrict__ row_inc,
+    int ngroups, const int4* __restrict__ groups, const int32_t* __restrict__ row_inc,
     const int32_t* __restrict__ inc_elem, const uint32_t* __restrict__ inc_info, const int4* __restrict__ conn,
     const double* __restrict__ coords, const double* __restrict__ uadv, const double* __restrict__ state,
     const double* __restrict__ force, const int64_t* __restrict__ start, NSParams p, double* __restrict__ vals,
@@ -1008,149 +1009,170 @@ __global__ void __launch_bounds__(32 * WPB) ns_assembly_warp_kernel(
   int* s_pref = reinterpret_cast<int*>(s_pslots + 32);               // 33 (+3 pad)
   int* s_off = s_pref + 36;                                          // 33 (+3 pad): lane offset of each row
 
-  const int g = blockIdx.x * WPB + warp;
+  // Persistent warps: a warp walks the groups g, g + stride, ...  While it
+  // reduces one group it already loads the incidence records (element id, slot
+  // word) and the connectivity of the next, so the next element phase starts
+  // with only the node gathers outstanding.
+  int g = blockIdx.x * WPB + warp;
   if (g >= ngroups) return;  // whole warp; no CTA-wide barrier below
-  const int2 gr = groups[g];
-  const int row0 = gr.x, R = gr.y - gr.x;  // 1 <= R <= K <= 32
-  const int i0 = __ldg(row_inc + row0);
-  const int K = __ldg(row_inc + row0 + R) - i0;
-  int my_off = 0, my_items = 0;
-  if (lane < R) {
-    my_off = __ldg(row_inc + row0 + lane) - i0;
-    my_items = int(__ldg(start + row0 + lane + 1) - __ldg(start + row0 + lane) - 1) * RG;
-  }
-  int pref = my_items;  // inclusive scan of the off-diagonal item counts
-#pragma unroll
-  for (int o = 1; o < 32; o <<= 1) {
-    const int v = __shfl_up_sync(FULL, pref, o);
-    if (lane >= o) pref += v;
-  }
-  const int nitems = __shfl_sync(FULL, pref, R - 1);
-  if (lane < R) {
-    s_pref[lane + 1] = pref;
-    s_off[lane] = my_off;
-  }
-  if (lane == 0) {
-    s_pref[0] = 0;
-    s_off[R] = K;
-  }
-#pragma unroll
-  for (int q = 0; q < D * 2; ++q) s_mask[q * 32 + lane] = 0u;
-  __syncwarp();
-
-  // Phase 1: one lane per incidence; the row node is relabelled to local
-  // position 0 exactly as in the chunk kernel.  Lane k stages its block
-  // (local column node b, equation r, component c) at k*LS + (b*neq + r)*neq + c
-  // and its RHS row at k*LS + nvals + r.
-  uint32_t pslots = 0xFFFFFFFFu;
-  if (lane < K) {
-    const int k = i0 + lane;
-    const int e = __ldg(inc_elem + k);
-    const uint32_t info = __ldg(inc_info + k);
-    const int a = int(info >> 24) & 3;
-    const int4 cn = __ldg(conn + e);
-    const int ids0[4] = {cn.x, cn.y, cn.z, cn.w};
-    int ids[4];
-    pslots = 0;
-#pragma unroll
-    for (int q = 0; q < 4; ++q) {
-      const int src = (D == 3) ? (q ^ a) : (q < 3 ? (q + a) % 3 : 3);
-      ids[q] = ids0[src];
-      const uint32_t sl = (q < n) ? ((info >> (6 * src)) & 63u) : 0xFFu;
-      pslots |= sl << (8 * q);
+  const int gstride = gridDim.x * WPB;
+  int4 G = groups[g];  // first row, end row, first incidence, incidences
+  int pe = 0, poff = 0, pitems = 0;
+  uint32_t pinfo = 0;
+  int4 pcn = make_int4(0, 0, 0, 0);
+  auto fetch_records = [&](const int4& q) {
+    if (lane < q.w) {
+      pe = __ldg(inc_elem + q.z + lane);
+      pinfo = __ldg(inc_info + q.z + lane);
     }
-    T* st = stage + lane * LS;
-    const KParams<T> kp = make_kparams<T>(p);
-    if constexpr (SPEC) {
-      if constexpr (D == 2) spec_tri_row<T>(ids, a, coords, uadv, state, kp, st, st + nvals, 1);
-      else spec_tet_row<T>(ids, a, coords, uadv, state, kp, st, st + nvals, 1);
-    } else {
-      generic_row<D, T>(ids, a, coords, uadv, state, force, kp, st, st + nvals, 1);
+    if (lane < q.y - q.x) {
+      poff = __ldg(row_inc + q.x + lane) - q.z;
+      pitems = int(__ldg(start + q.x + lane + 1) - __ldg(start + q.x + lane) - 1) * RG;
+    }
+  };
+  fetch_records(G);
+  if (lane < G.w) pcn = __ldg(conn + pe);
+  for (;;) {
+    const int row0 = G.x, R = G.y - G.x, K = G.w;  // 1 <= R <= K <= 32
+    const int gn = g + gstride;
+    const int4 Gn = gn < ngroups ? groups[gn] : make_int4(0, 0, 0, 0);
+    __syncwarp();  // the previous group's reads of the shared slice are complete
+    int pref = lane < R ? pitems : 0;  // inclusive scan of the off-diagonal item counts
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const int v = __shfl_up_sync(FULL, pref, o);
+      if (lane >= o) pref += v;
+    }
+    const int nitems = __shfl_sync(FULL, pref, R - 1);
+    if (lane < R) {
+      s_pref[lane + 1] = pref;
+      s_off[lane] = poff;
+    }
+    if (lane == 0) {
+      s_pref[0] = 0;
+      s_off[R] = K;
     }
 #pragma unroll
-    for (int q = 1; q < n; ++q) atomicOr(s_mask + (q - 1) * 64 + ((pslots >> (8 * q)) & 0xFFu), 1u << lane);
-  }
-  s_pslots[lane] = pslots;
-  __syncwarp();
+    for (int q = 0; q < D * 2; ++q) s_mask[q * 32 + lane] = 0u;
+    __syncwarp();
 
-  // Phase 2a: diagonal entries and RHS entries, neq * (neq + 1) items per row,
-  // each the sum over the row's lanes in element order.
-  constexpr int ND = neq * (neq + 1);
-  for (int it = lane; it < R * ND; it += 32) {
-    const int rl = it / ND, j = it - rl * ND;
-    const int kb = s_off[rl], ke = s_off[rl + 1];  // lanes of row rl
-    const int row = row0 + rl;
-    const T* src = stage + (j < neq * neq ? j : nvals + (j - neq * neq));  // b = 0 block, or the RHS row
-    double acc = 0.0;
-    for (int k = kb; k < ke; ++k) acc += double(src[k * LS]);
-    if (j < neq * neq) {
-      const int r = j / neq, c = j - r * neq;
+    // Phase 1: one lane per incidence; the row node is relabelled to local
+    // position 0 exactly as in the chunk kernel.  Lane k stages its block
+    // (local column node b, equation r, component c) at k*LS + (b*neq + r)*neq + c
+    // and its RHS row at k*LS + nvals + r.
+    uint32_t pslots = 0xFFFFFFFFu;
+    if (lane < K) {
+      const uint32_t info = pinfo;
+      const int a = int(info >> 24) & 3;
+      const int ids0[4] = {pcn.x, pcn.y, pcn.z, pcn.w};
+      int ids[4];
+      pslots = 0;
+#pragma unroll
+      for (int q = 0; q < 4; ++q) {
+        const int src = (D == 3) ? (q ^ a) : (q < 3 ? (q + a) % 3 : 3);
+        ids[q] = ids0[src];
+        const uint32_t sl = (q < n) ? ((info >> (6 * src)) & 63u) : 0xFFu;
+        pslots |= sl << (8 * q);
+      }
+      T* st = stage + lane * LS;
+      const KParams<T> kp = make_kparams<T>(p);
+      if constexpr (SPEC) {
+        if constexpr (D == 2) spec_tri_row<T>(ids, a, coords, uadv, state, kp, st, st + nvals, 1);
+        else spec_tet_row<T>(ids, a, coords, uadv, state, kp, st, st + nvals, 1);
+      } else {
+        generic_row<D, T>(ids, a, coords, uadv, state, force, kp, st, st + nvals, 1);
+      }
+#pragma unroll
+      for (int q = 1; q < n; ++q) atomicOr(s_mask + (q - 1) * 64 + ((pslots >> (8 * q)) & 0xFFu), 1u << lane);
+    }
+    s_pslots[lane] = pslots;
+    __syncwarp();
+    fetch_records(Gn);  // next group's records load while this group is reduced
+
+    // Phase 2a: diagonal entries and RHS entries, neq * (neq + 1) items per row,
+    // each the sum over the row's lanes in element order.
+    constexpr int ND = neq * (neq + 1);
+    for (int it = lane; it < R * ND; it += 32) {
+      const int rl = it / ND, j = it - rl * ND;
+      const int kb = s_off[rl], ke = s_off[rl + 1];  // lanes of row rl
+      const int row = row0 + rl;
+      const T* src = stage + (j < neq * neq ? j : nvals + (j - neq * neq));  // b = 0 block, or the RHS row
+      double acc = 0.0;
+      for (int k = kb; k < ke; ++k) acc += double(src[k * LS]);
+      if (j < neq * neq) {
+        const int r = j / neq, c = j - r * neq;
+        const int64_t s0 = __ldg(start + row);
+        const int S = int(__ldg(start + row + 1) - s0);
+        const int self = int(s_pslots[kb] & 0xFFu);
+        const int64_t pos = int64_t(neq) * neq * s0 + int64_t(r * S + self) * neq + c;
+        vals[pos] = acc;
+        if (vals32 != nullptr) vals32[pos] = float(acc);
+      } else {
+        rhs[int64_t(row) * neq + (j - neq * neq)] = acc;
+      }
+    }
+
+    if (lane < Gn.w) pcn = __ldg(conn + pe);
+
+    // Phase 2b: off-diagonal items (row, slot != self, group of RPI equations):
+    // the contributors of slot s are the row's lanes holding s at local position
+    // b = 1..n-1, visited in ascending lane (= element) order.
+    for (int it = lane; it < nitems; it += 32) {
+      int lo = 0, hi = R - 1;
+      while (lo < hi) {  // last rl with s_pref[rl] <= it
+        const int mid = (lo + hi + 1) >> 1;
+        if (s_pref[mid] <= it) lo = mid; else hi = mid - 1;
+      }
+      const int rl = lo;
+      const int row = row0 + rl;
       const int64_t s0 = __ldg(start + row);
       const int S = int(__ldg(start + row + 1) - s0);
+      const int local = it - s_pref[rl];
+      const int s1 = local / RG;
+      const int rg = local - s1 * RG;
+      const int kb = s_off[rl], ke = s_off[rl + 1];
       const int self = int(s_pslots[kb] & 0xFFu);
-      const int64_t pos = int64_t(neq) * neq * s0 + int64_t(r * S + self) * neq + c;
-      vals[pos] = acc;
-      if (vals32 != nullptr) vals32[pos] = float(acc);
-    } else {
-      rhs[int64_t(row) * neq + (j - neq * neq)] = acc;
-    }
-  }
-
-  // Phase 2b: off-diagonal items (row, slot != self, group of RPI equations):
-  // the contributors of slot s are the row's lanes holding s at local position
-  // b = 1..n-1, visited in ascending lane (= element) order.
-  for (int it = lane; it < nitems; it += 32) {
-    int lo = 0, hi = R - 1;
-    while (lo < hi) {  // last rl with s_pref[rl] <= it
-      const int mid = (lo + hi + 1) >> 1;
-      if (s_pref[mid] <= it) lo = mid; else hi = mid - 1;
-    }
-    const int rl = lo;
-    const int row = row0 + rl;
-    const int64_t s0 = __ldg(start + row);
-    const int S = int(__ldg(start + row + 1) - s0);
-    const int local = it - s_pref[rl];
-    const int s1 = local / RG;
-    const int rg = local - s1 * RG;
-    const int kb = s_off[rl], ke = s_off[rl + 1];
-    const int self = int(s_pslots[kb] & 0xFFu);
-    const int s = s1 + (s1 >= self ? 1 : 0);
-    const unsigned rowmask = unsigned((1ull << ke) - (1ull << kb));
-    const unsigned m1 = s_mask[s] & rowmask;
-    const unsigned m2 = s_mask[64 + s] & rowmask;
-    const unsigned m3 = (D == 3) ? (s_mask[128 + s] & rowmask) : 0u;
-    unsigned m = m1 | m2 | m3;
-    double acc[NV];
+      const int s = s1 + (s1 >= self ? 1 : 0);
+      const unsigned rowmask = unsigned((1ull << ke) - (1ull << kb));
+      const unsigned m1 = s_mask[s] & rowmask;
+      const unsigned m2 = s_mask[64 + s] & rowmask;
+      const unsigned m3 = (D == 3) ? (s_mask[128 + s] & rowmask) : 0u;
+      unsigned m = m1 | m2 | m3;
+      double acc[NV];
 #pragma unroll
-    for (int q = 0; q < NV; ++q) acc[q] = 0.0;
-    while (m) {
-      const int k = __ffs(m) - 1;
-      m &= m - 1;
-      const int b = 1 + int((m2 >> k) & 1u) + 2 * int((m3 >> k) & 1u);
-      T v[NV];
-      load_run<NV, T>(stage + k * LS + (b * neq + rg * RPI) * neq, v);
+      for (int q = 0; q < NV; ++q) acc[q] = 0.0;
+      while (m) {
+        const int k = __ffs(m) - 1;
+        m &= m - 1;
+        const int b = 1 + int((m2 >> k) & 1u) + 2 * int((m3 >> k) & 1u);
+        T v[NV];
+        load_run<NV, T>(stage + k * LS + (b * neq + rg * RPI) * neq, v);
 #pragma unroll
-      for (int q = 0; q < NV; ++q) acc[q] += double(v[q]);
-    }
+        for (int q = 0; q < NV; ++q) acc[q] += double(v[q]);
+      }
 #pragma unroll
-    for (int rr = 0; rr < RPI; ++rr) {
-      const int r = rg * RPI + rr;
-      const int64_t pos = int64_t(neq) * neq * s0 + int64_t(r * S + s) * neq;
-      if constexpr (neq == 4) {
-        reinterpret_cast<double2*>(vals + pos)[0] = make_double2(acc[4 * rr], acc[4 * rr + 1]);
-        reinterpret_cast<double2*>(vals + pos)[1] = make_double2(acc[4 * rr + 2], acc[4 * rr + 3]);
-        if (vals32 != nullptr)
-          *reinterpret_cast<float4*>(vals32 + pos) =
-              make_float4(float(acc[4 * rr]), float(acc[4 * rr + 1]), float(acc[4 * rr + 2]), float(acc[4 * rr + 3]));
-      } else {
+      for (int rr = 0; rr < RPI; ++rr) {
+        const int r = rg * RPI + rr;
+        const int64_t pos = int64_t(neq) * neq * s0 + int64_t(r * S + s) * neq;
+        if constexpr (neq == 4) {
+          reinterpret_cast<double2*>(vals + pos)[0] = make_double2(acc[4 * rr], acc[4 * rr + 1]);
+          reinterpret_cast<double2*>(vals + pos)[1] = make_double2(acc[4 * rr + 2], acc[4 * rr + 3]);
+          if (vals32 != nullptr)
+            *reinterpret_cast<float4*>(vals32 + pos) =
+                make_float4(float(acc[4 * rr]), float(acc[4 * rr + 1]), float(acc[4 * rr + 2]), float(acc[4 * rr + 3]));
+        } else {
 #pragma unroll
-        for (int c = 0; c < neq; ++c) vals[pos + c] = acc[rr * neq + c];
-        if (vals32 != nullptr) {
+          for (int c = 0; c < neq; ++c) vals[pos + c] = acc[rr * neq + c];
+          if (vals32 != nullptr) {
 #pragma unroll
-          for (int c = 0; c < neq; ++c) vals32[pos + c] = float(acc[rr * neq + c]);
+            for (int c = 0; c < neq; ++c) vals32[pos + c] = float(acc[rr * neq + c]);
+          }
         }
       }
     }
+    if (gn >= ngroups) break;
+    g = gn;
+    G = Gn;
   }
 }
 
@@ -1304,12 +1326,25 @@ int launch_chunk_t(const ufem_ns_handle* h, const AssemblyPlan& plan, const NSPa
   return UFEM_OK;
 }
 
+// Resident CTAs of a kernel on the current device (persistent-warp grids).
+template <typename K>
+int resident_ctas(K kernel, int threads, size_t smem) {
+  int dev = 0, sms = 0, per_sm = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess ||
+      cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess ||
+      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, threads, smem) != cudaSuccess || per_sm < 1)
+    return 0;
+  return sms * per_sm;
+}
+
 template <int D, typename T, bool SPEC, int WPB>
 int launch_warp_t(const ufem_ns_handle* h, const NSParams& p, cudaStream_t s, bool write32) {
   const WarpPlan& wp = h->wplan;
   if (wp.ngroups == 0) return UFEM_OK;
   constexpr size_t smem = warp_stage_bytes<D, T>() * WPB;
-  const unsigned grid = unsigned((wp.ngroups + WPB - 1) / WPB);
+  static const int resident = resident_ctas(ns_assembly_warp_kernel<D, T, SPEC, WPB>, 32 * WPB, smem);
+  if (resident <= 0) return set_error(UFEM_ERR_CUDA, "occupancy query of the warp assembly kernel failed");
+  const unsigned grid = unsigned(std::min<int64_t>((wp.ngroups + WPB - 1) / WPB, resident));
   ns_assembly_warp_kernel<D, T, SPEC, WPB><<<grid, 32 * WPB, smem, s>>>(
       wp.ngroups, wp.groups, h->d_row_inc, h->d_inc_elem, h->d_inc_info, reinterpret_cast<const int4*>(h->d_conn),
       h->d_coords, h->d_uadv, h->d_state, h->d_force, h->d_start, p, h->d_vals, write32 ? h->d_vals32 : nullptr,

@@ -483,7 +483,8 @@ int ufem_ns_create(const ufem_mesh* mesh, const ufem_ns_options* opts, ufem_ns_h
     }
     return true;
   };
-  std::vector<int2> chunks64, chunks32, big64, big32, groups;
+  std::vector<int2> chunks64, chunks32, big64, big32;
+  std::vector<int4> groups;
   if (!make_chunks(assembly_chunk_capacity(dim, 0), false, chunks64) ||
       !make_chunks(assembly_chunk_capacity(dim, 1), false, chunks32) ||
       !make_chunks(assembly_chunk_capacity(dim, 0), true, big64) ||
@@ -495,7 +496,7 @@ int ufem_ns_create(const ufem_mesh* mesh, const ufem_ns_options* opts, ufem_ns_h
     const int64_t first = i;
     int64_t k = 0;
     while (i < N && inc_of(i) <= 32 && k + inc_of(i) <= 32) k += inc_of(i++);
-    groups.push_back(make_int2(int(first), int(i)));
+    groups.push_back(make_int4(int(first), int(i), row_inc[first], int(k)));
   }
   h->plan64.cap = assembly_chunk_capacity(dim, 0);
   h->plan64.nchunks = int(chunks64.size());
@@ -545,7 +546,7 @@ int ufem_ns_create(const ufem_mesh* mesh, const ufem_ns_options* opts, ufem_ns_h
       (ce = up(h->d_inc_info, inc_info.data(), inc_info.size() * 4)) ||
       (ce = up(h->plan64.chunks, chunks64.data(), chunks64.size() * sizeof(int2))) ||
       (ce = up(h->plan32.chunks, chunks32.data(), chunks32.size() * sizeof(int2))) ||
-      (ce = up(h->wplan.groups, groups.data(), groups.size() * sizeof(int2))) ||
+      (ce = up(h->wplan.groups, groups.data(), groups.size() * sizeof(int4))) ||
       (ce = up(h->wplan.big64.chunks, big64.data(), big64.size() * sizeof(int2))) ||
       (ce = up(h->wplan.big32.chunks, big32.data(), big32.size() * sizeof(int2))))
     return fail(set_error(UFEM_ERR_CUDA, std::string("upload: ") + cudaGetErrorString(ce)));

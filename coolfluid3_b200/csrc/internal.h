@@ -46,7 +46,7 @@ struct AssemblyPlan {
 };
 struct WarpPlan {
   int ngroups = 0;
-  int2* groups = nullptr;      // [first row, end row) per warp (device)
+  int4* groups = nullptr;      // first row, end row, first incidence, incidences (device)
   AssemblyPlan big64, big32;   // rows with more than 32 incidences
 };
 
