@@ -108,22 +108,41 @@ struct Elem {
   T NU[D + 1];     // nu_eff
 };
 
+// Nodal inputs of the element routines.  FP64 element arithmetic reads the
+// FP64 node records; the FP32 path reads node32, an FP32 copy of
+// (u_adv, nu_eff, u, p) per node written by the linearisation kernel (the same
+// round-to-nearest values a conversion here would give), and keeps only the
+// coordinates in FP64 so that differences are formed before rounding.
+struct NodeData {
+  const double* coords;  // N x 4
+  const double* uadv;    // N x 4 (u_adv, nu_eff)
+  const double* state;   // N x 4 (u, p)
+  const float* node32;   // N x 8 (u_adv, nu_eff, u, p), FP32 path only
+};
+
 template <int D, typename T>
-__device__ __forceinline__ void gather_geometry_uadv(const int (&ids)[4], const double* __restrict__ coords,
-                                                     const double* __restrict__ uadv, Elem<D, T>& el) {
+__device__ __forceinline__ void gather_geometry_uadv(const int (&ids)[4], const NodeData& nd, Elem<D, T>& el) {
   double X0[4];
-  ld4(coords + 4ll * ids[0], X0[0], X0[1], X0[2], X0[3]);
+  ld4(nd.coords + 4ll * ids[0], X0[0], X0[1], X0[2], X0[3]);
 #pragma unroll
   for (int b = 0; b <= D; ++b) {
     double x[4];
-    ld4(coords + 4ll * ids[b], x[0], x[1], x[2], x[3]);
+    ld4(nd.coords + 4ll * ids[b], x[0], x[1], x[2], x[3]);
 #pragma unroll
     for (int k = 0; k < D; ++k) el.Xr[b][k] = T(x[k] - X0[k]);
-    double u[4];
-    ld4(uadv + 4ll * ids[b], u[0], u[1], u[2], u[3]);
+    if constexpr (std::is_same<T, float>::value) {
+      const float4 u = __ldg(reinterpret_cast<const float4*>(nd.node32) + 2ll * ids[b]);
+      const float uu[4] = {u.x, u.y, u.z, u.w};
 #pragma unroll
-    for (int k = 0; k < D; ++k) el.U[b][k] = T(u[k]);
-    el.NU[b] = T(u[3]);
+      for (int k = 0; k < D; ++k) el.U[b][k] = uu[k];
+      el.NU[b] = u.w;
+    } else {
+      double u[4];
+      ld4(nd.uadv + 4ll * ids[b], u[0], u[1], u[2], u[3]);
+#pragma unroll
+      for (int k = 0; k < D; ++k) el.U[b][k] = T(u[k]);
+      el.NU[b] = T(u[3]);
+    }
   }
 }
 
@@ -314,11 +333,20 @@ __device__ __forceinline__ void stage_block(const T (&A)[D + 1][D + 1], const T 
 }
 
 template <int D, typename T>
-__device__ __forceinline__ void load_state(const double* __restrict__ state, int node, T (&x)[D + 1]) {
-  double s[4];
-  ld4(state + 4ll * node, s[0], s[1], s[2], s[3]);
+__device__ __forceinline__ void load_state(const NodeData& nd, int node, T (&x)[D + 1]) {
+  if constexpr (std::is_same<T, float>::value) {
+    const float4 v = __ldg(reinterpret_cast<const float4*>(nd.node32) + 2ll * node + 1);
+    const float vv[4] = {v.x, v.y, v.z, v.w};
+    // (u, v, [w], p): p sits at index D of the padded record
 #pragma unroll
-  for (int k = 0; k <= D; ++k) x[k] = T(s[k]);
+    for (int k = 0; k < D; ++k) x[k] = vv[k];
+    x[D] = vv[3];
+  } else {
+    double s[4];
+    ld4(nd.state + 4ll * node, s[0], s[1], s[2], s[3]);
+#pragma unroll
+    for (int k = 0; k <= D; ++k) x[k] = T(s[k]);
+  }
 }
 
 // ---------------------------------------------------------------------------
@@ -341,15 +369,14 @@ __device__ __forceinline__ void load_state(const double* __restrict__ state, int
 // quadrature).
 // ---------------------------------------------------------------------------
 template <int D, typename T>
-__device__ __forceinline__ void generic_row(const int (&ids)[4], int a, const double* __restrict__ coords,
-                                            const double* __restrict__ uadv, const double* __restrict__ state,
+__device__ __forceinline__ void generic_row(const int (&ids)[4], int a, const NodeData& nd,
                                             const double* __restrict__ force, const KParams<T>& kp,
                                             T* __restrict__ st, T* __restrict__ rst, int CH) {
   constexpr int n = D + 1, neq = D + 1;
   const T inv_n = T(1.0 / n);
   const T nT = T(n), n2 = T(n * n);
   Elem<D, T> el;
-  gather_geometry_uadv<D, T>(ids, coords, uadv, el);
+  gather_geometry_uadv<D, T>(ids, nd, el);
   // tau inputs: |mean nodal nu| and u_adv at the centroid (SUPG.hpp:110-116, 145-147)
   T nsum = 0;
 #pragma unroll
@@ -449,7 +476,7 @@ __device__ __forceinline__ void generic_row(const int (&ids)[4], int a, const do
   // nodal state (u, p) of the element: A x for the RHS
   T xs[n][neq];
 #pragma unroll
-  for (int b = 0; b < n; ++b) load_state<D, T>(state, ids[b], xs[b]);
+  for (int b = 0; b < n; ++b) load_state<D, T>(nd, ids[b], xs[b]);
   T div = 0, gradp[D], kx[D], ax[D];
 #pragma unroll
   for (int i = 0; i < D; ++i) {
@@ -516,7 +543,7 @@ __device__ __forceinline__ void generic_row(const int (&ids)[4], int a, const do
 // ---------------------------------------------------------------------------
 template <int D, typename T>
 __device__ __forceinline__ void spec_tau_common(const KParams<T>& kp, const Elem<D, T>& el, int a,
-                                                const double* __restrict__ state, const int (&ids)[4], T nu,
+                                                const NodeData& nd, const int (&ids)[4], T nu,
                                                 T& tps, T& tsu, T& tbu) {
   // tau of the solution velocity u
   constexpr int n = D + 1;
@@ -528,7 +555,7 @@ __device__ __forceinline__ void spec_tau_common(const KParams<T>& kp, const Elem
 #pragma unroll
   for (int b = 0; b < n; ++b) {
     T x[D + 1];
-    load_state<D, T>(state, ids[b], x);
+    load_state<D, T>(nd, ids[b], x);
 #pragma unroll
     for (int k = 0; k < D; ++k) uc[k] += Nc[b] * x[k];
   }
@@ -560,11 +587,9 @@ __device__ __forceinline__ void spec_tau_common(const KParams<T>& kp, const Elem
 }
 
 template <typename T>
-__device__ __forceinline__ void spec_tri_row(const int (&ids)[4], int ai, const double* __restrict__ coords,
-                                             const double* __restrict__ uadv, const double* __restrict__ state,
-                                             const KParams<T>& kp, T* __restrict__ st, T* __restrict__ rst, int CH) {
+__device__ __forceinline__ void spec_tri_row(const int (&ids)[4], int ai, const NodeData& nd, const KParams<T>& kp, T* __restrict__ st, T* __restrict__ rst, int CH) {
   Elem<2, T> el;
-  gather_geometry_uadv<2, T>(ids, coords, uadv, el);
+  gather_geometry_uadv<2, T>(ids, nd, el);
   T u_avg[2];
 #pragma unroll
   for (int k = 0; k < 2; ++k) {
@@ -585,7 +610,7 @@ __device__ __forceinline__ void spec_tri_row(const int (&ids)[4], int ai, const 
   nx[1] = X[2][1] - X[0][1]; ny[1] = X[0][0] - X[2][0];
   nx[2] = X[0][1] - X[1][1]; ny[2] = X[1][0] - X[0][0];
   T tau_ps, tau_su, tau_bulk;
-  spec_tau_common<2, T>(kp, el, ai, state, ids, nu, tau_ps, tau_su, tau_bulk);
+  spec_tau_common<2, T>(kp, el, ai, nd, ids, nu, tau_ps, tau_su, tau_bulk);
   const T nix = nx[0], niy = ny[0];  // row node at local position 0
   const T u_ni = u_avg[0] * nix + u_avg[1] * niy;
   const T rho = kp.rho;
@@ -632,7 +657,7 @@ __device__ __forceinline__ void spec_tri_row(const int (&ids)[4], int ai, const 
     val = tau_ps / T(6);
     Tm[2][0] += val * nix; Tm[2][1] += val * niy;
     T xb[3];
-    load_state<2, T>(state, ids[j], xb);
+    load_state<2, T>(nd, ids[j], xb);
     stage_block<2, T>(A, Tm, xb, kp, rhs, st, j, CH);
   }
   put_row<3, T>(rst, 0, CH, rhs);
@@ -641,11 +666,9 @@ __device__ __forceinline__ void spec_tri_row(const int (&ids)[4], int ai, const 
 // Specialised tetrahedra, NavierStokesSpecializations.hpp:150-302, row i = a,
 // including the reference's use of vk in the W rows (:224-226, :236-238).
 template <typename T>
-__device__ __forceinline__ void spec_tet_row(const int (&ids)[4], int ai, const double* __restrict__ coords,
-                                             const double* __restrict__ uadv, const double* __restrict__ state,
-                                             const KParams<T>& kp, T* __restrict__ st, T* __restrict__ rst, int CH) {
+__device__ __forceinline__ void spec_tet_row(const int (&ids)[4], int ai, const NodeData& nd, const KParams<T>& kp, T* __restrict__ st, T* __restrict__ rst, int CH) {
   Elem<3, T> el;
-  gather_geometry_uadv<3, T>(ids, coords, uadv, el);
+  gather_geometry_uadv<3, T>(ids, nd, el);
   T u_avg[3];
 #pragma unroll
   for (int k = 0; k < 3; ++k) {
@@ -682,7 +705,7 @@ __device__ __forceinline__ void spec_tet_row(const int (&ids)[4], int ai, const 
   nr[3][YY] = ((X[1][ZZ]-X[0][ZZ])*(X[2][XX]-X[0][XX]) - (X[2][ZZ]-X[0][ZZ])*(X[1][XX]-X[0][XX])) / T(2);
   nr[3][ZZ] = ((X[1][XX]-X[0][XX])*(X[2][YY]-X[0][YY]) - (X[2][XX]-X[0][XX])*(X[1][YY]-X[0][YY])) / T(2);
   T tau_ps, tau_su, tau_bulk;
-  spec_tau_common<3, T>(kp, el, ai, state, ids, nu, tau_ps, tau_su, tau_bulk);
+  spec_tau_common<3, T>(kp, el, ai, nd, ids, nu, tau_ps, tau_su, tau_bulk);
   T ni[3];
 #pragma unroll
   for (int k = 0; k < 3; ++k) {
@@ -748,7 +771,7 @@ __device__ __forceinline__ void spec_tet_row(const int (&ids)[4], int ai, const 
     val = tau_ps / T(12);
     Tm[3][0] += val * ni[XX]; Tm[3][1] += val * ni[YY]; Tm[3][2] += val * ni[ZZ];
     T xb[4];
-    load_state<3, T>(state, ids[j], xb);
+    load_state<3, T>(nd, ids[j], xb);
     stage_block<3, T>(A, Tm, xb, kp, rhs, st, j, CH);
   }
   put_row<4, T>(rst, 0, CH, rhs);
@@ -771,7 +794,8 @@ __global__ void __launch_bounds__(CH) ns_assembly_kernel(
     const int2* __restrict__ chunk_rows, const int32_t* __restrict__ row_inc,
     const int32_t* __restrict__ inc_elem, const uint32_t* __restrict__ inc_info, const int4* __restrict__ conn,
     const double* __restrict__ coords, const double* __restrict__ uadv, const double* __restrict__ state,
-    const double* __restrict__ force, const int64_t* __restrict__ start, NSParams p, double* __restrict__ vals,
+    const float* __restrict__ node32, const double* __restrict__ force, const int64_t* __restrict__ start,
+    NSParams p, double* __restrict__ vals,
     float* __restrict__ vals32, double* __restrict__ rhs) {
   constexpr int n = P1<D>::n, neq = P1<D>::neq, nvals = P1<D>::nvals;
   extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -833,11 +857,12 @@ __global__ void __launch_bounds__(CH) ns_assembly_kernel(
     }
     s_info[t] = pslots;
     const KParams<T> kp = make_kparams<T>(p);
+    const NodeData nd{coords, uadv, state, node32};
     if constexpr (SPEC) {
-      if constexpr (D == 2) spec_tri_row<T>(ids, a, coords, uadv, state, kp, st + t, rst + t, CH);
-      else spec_tet_row<T>(ids, a, coords, uadv, state, kp, st + t, rst + t, CH);
+      if constexpr (D == 2) spec_tri_row<T>(ids, a, nd, kp, st + t, rst + t, CH);
+      else spec_tet_row<T>(ids, a, nd, kp, st + t, rst + t, CH);
     } else {
-      generic_row<D, T>(ids, a, coords, uadv, state, force, kp, st + t, rst + t, CH);
+      generic_row<D, T>(ids, a, nd, force, kp, st + t, rst + t, CH);
     }
     // contributor masks: bit = position of this incidence within its row
     int lo = 0, hi = R - 1;
@@ -993,7 +1018,8 @@ __global__ void __launch_bounds__(32 * WPB) ns_assembly_warp_kernel(
     int ngroups, const int4* __restrict__ groups, const int32_t* __restrict__ row_inc,
     const int32_t* __restrict__ inc_elem, const uint32_t* __restrict__ inc_info, const int4* __restrict__ conn,
     const double* __restrict__ coords, const double* __restrict__ uadv, const double* __restrict__ state,
-    const double* __restrict__ force, const int64_t* __restrict__ start, NSParams p, double* __restrict__ vals,
+    const float* __restrict__ node32, const double* __restrict__ force, const int64_t* __restrict__ start,
+    NSParams p, double* __restrict__ vals,
     float* __restrict__ vals32, double* __restrict__ rhs) {
   constexpr int n = P1<D>::n, neq = P1<D>::neq, nvals = P1<D>::nvals;
   constexpr int LS = warp_lane_pitch<D, T>();
@@ -1076,11 +1102,12 @@ __global__ void __launch_bounds__(32 * WPB) ns_assembly_warp_kernel(
       }
       T* st = stage + lane * LS;
       const KParams<T> kp = make_kparams<T>(p);
+      const NodeData nd{coords, uadv, state, node32};
       if constexpr (SPEC) {
-        if constexpr (D == 2) spec_tri_row<T>(ids, a, coords, uadv, state, kp, st, st + nvals, 1);
-        else spec_tet_row<T>(ids, a, coords, uadv, state, kp, st, st + nvals, 1);
+        if constexpr (D == 2) spec_tri_row<T>(ids, a, nd, kp, st, st + nvals, 1);
+        else spec_tet_row<T>(ids, a, nd, kp, st, st + nvals, 1);
       } else {
-        generic_row<D, T>(ids, a, coords, uadv, state, force, kp, st, st + nvals, 1);
+        generic_row<D, T>(ids, a, nd, force, kp, st, st + nvals, 1);
       }
 #pragma unroll
       for (int q = 1; q < n; ++q) atomicOr(s_mask + (q - 1) * 64 + ((pslots >> (8 * q)) & 0xFFu), 1u << lane);
@@ -1182,7 +1209,7 @@ __global__ void __launch_bounds__(32 * WPB) ns_assembly_warp_kernel(
 __global__ void linearize_kernel(int64_t N, int dim, const double* __restrict__ state,
                                  const double* __restrict__ u1, const double* __restrict__ u2,
                                  const double* __restrict__ u3, const double* __restrict__ nu,
-                                 double* __restrict__ uadv) {
+                                 double* __restrict__ uadv, float* __restrict__ node32) {
   const int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
   if (i >= N) return;
   double out[4] = {0, 0, 0, 0};
@@ -1196,6 +1223,12 @@ __global__ void linearize_kernel(int64_t N, int dim, const double* __restrict__ 
   out[3] = nu[i];
   reinterpret_cast<double2*>(uadv + 4 * i)[0] = make_double2(out[0], out[1]);
   reinterpret_cast<double2*>(uadv + 4 * i)[1] = make_double2(out[2], out[3]);
+  if (node32 != nullptr) {  // FP32 copy for the FP32 element path: (u_adv, nu), (u, p)
+    float4* q = reinterpret_cast<float4*>(node32) + 2 * i;
+    q[0] = make_float4(float(out[0]), float(out[1]), float(out[2]), float(out[3]));
+    const double* x = state + 4 * i;
+    q[1] = make_float4(float(x[0]), float(x[1]), dim == 3 ? float(x[2]) : 0.0f, float(x[dim]));
+  }
 }
 
 // UpdateActions (NavierStokes.cpp:172-179): u3=u2, u2=u1, u1=u, u+=du, p+=dp.
@@ -1320,7 +1353,8 @@ int launch_chunk_t(const ufem_ns_handle* h, const AssemblyPlan& plan, const NSPa
   if (plan.cap != CH) return set_error(UFEM_ERR_STATE, "assembly plan does not match the kernel width");
   ns_assembly_kernel<D, T, CH, SPEC><<<plan.nchunks, CH, smem, s>>>(
       plan.chunks, h->d_row_inc, h->d_inc_elem, h->d_inc_info, reinterpret_cast<const int4*>(h->d_conn),
-      h->d_coords, h->d_uadv, h->d_state, h->d_force, h->d_start, p, h->d_vals, write32 ? h->d_vals32 : nullptr,
+      h->d_coords, h->d_uadv, h->d_state, h->d_node32, h->d_force, h->d_start, p, h->d_vals,
+      write32 ? h->d_vals32 : nullptr,
       h->d_rhs);
   UFEM_CUDA_TRY(cudaGetLastError());
   return UFEM_OK;
@@ -1347,7 +1381,8 @@ int launch_warp_t(const ufem_ns_handle* h, const NSParams& p, cudaStream_t s, bo
   const unsigned grid = unsigned(std::min<int64_t>((wp.ngroups + WPB - 1) / WPB, resident));
   ns_assembly_warp_kernel<D, T, SPEC, WPB><<<grid, 32 * WPB, smem, s>>>(
       wp.ngroups, wp.groups, h->d_row_inc, h->d_inc_elem, h->d_inc_info, reinterpret_cast<const int4*>(h->d_conn),
-      h->d_coords, h->d_uadv, h->d_state, h->d_force, h->d_start, p, h->d_vals, write32 ? h->d_vals32 : nullptr,
+      h->d_coords, h->d_uadv, h->d_state, h->d_node32, h->d_force, h->d_start, p, h->d_vals,
+      write32 ? h->d_vals32 : nullptr,
       h->d_rhs);
   UFEM_CUDA_TRY(cudaGetLastError());
   return UFEM_OK;
@@ -1430,7 +1465,8 @@ int launch_linearize(ufem_ns_handle* h, cudaStream_t s) {
   const double* u1 = h->d_hist;
   const double* u2 = h->d_hist + 4 * N;
   const double* u3 = h->d_hist + 8 * N;
-  linearize_kernel<<<unsigned((N + 255) / 256), 256, 0, s>>>(N, h->dim, h->d_state, u1, u2, u3, h->d_nu, h->d_uadv);
+  linearize_kernel<<<unsigned((N + 255) / 256), 256, 0, s>>>(N, h->dim, h->d_state, u1, u2, u3, h->d_nu, h->d_uadv,
+                                                            h->opt.precision == 1 ? h->d_node32 : nullptr);
   UFEM_CUDA_TRY(cudaGetLastError());
   return UFEM_OK;
 }

@@ -221,7 +221,7 @@ void destroy_impl(ufem_ns_handle* h) {
   krylov_free(h);
   free_bc_plan(h->bcp);
   dfree(h->d_coords); dfree(h->d_conn); dfree(h->d_state); dfree(h->d_hist); dfree(h->d_uadv);
-  dfree(h->d_nu); dfree(h->d_force); dfree(h->d_start); dfree(h->d_adj); dfree(h->d_rowptr);
+  dfree(h->d_nu); dfree(h->d_force); dfree(h->d_node32); dfree(h->d_start); dfree(h->d_adj); dfree(h->d_rowptr);
   dfree(h->d_colidx); dfree(h->d_vals); dfree(h->d_vals32); dfree(h->d_rhs); dfree(h->d_sol);
   dfree(h->d_diagpos); dfree(h->d_row_inc); dfree(h->d_inc_elem); dfree(h->d_inc_info);
   dfree(h->plan64.chunks); dfree(h->plan32.chunks); dfree(h->wplan.groups);
@@ -533,7 +533,9 @@ int ufem_ns_create(const ufem_mesh* mesh, const ufem_ns_options* opts, ufem_ns_h
       (rc = dmalloc(&h->wplan.big32.chunks, std::max<size_t>(big32.size(), 1), "big32")) ||
       (rc = dmalloc(&h->d_stage, size_t(N) * 4 * dim, "stage")))
     return fail(rc);
-  if (opts->precision == 1 && (rc = dmalloc(&h->d_vals32, size_t(h->nnz), "vals32"))) return fail(rc);
+  if (opts->precision == 1 && ((rc = dmalloc(&h->d_vals32, size_t(h->nnz), "vals32")) ||
+                               (rc = dmalloc(&h->d_node32, size_t(h->N) * 8, "node32"))))
+    return fail(rc);
   auto up = [&](void* dst, const void* src, size_t bytes) {
     return cudaMemcpy(dst, src, bytes, cudaMemcpyHostToDevice);
   };
@@ -569,6 +571,7 @@ int ufem_ns_set_options(ufem_ns_handle* h, const ufem_ns_options* opts) {
   if ((rc = validate_options(opts))) return rc;
   h->opt = *opts;
   if (opts->precision == 1 && !h->d_vals32 && (rc = dmalloc(&h->d_vals32, size_t(h->nnz), "vals32"))) return rc;
+  if (opts->precision == 1 && !h->d_node32 && (rc = dmalloc(&h->d_node32, size_t(h->N) * 8, "node32"))) return rc;
   h->vals32_valid = false;
   return UFEM_OK;
 }

@@ -96,6 +96,7 @@ struct ufem_ns_handle {
   double* d_uadv = nullptr;     // N x 4 (u_adv xyz, nu at index 3)
   double* d_nu = nullptr;       // N
   double* d_force = nullptr;    // N x 4 or null
+  float* d_node32 = nullptr;    // N x 8: FP32 (u_adv, nu, u, p) for the FP32 element path
 
   // graph + CSR
   int64_t* d_start = nullptr;   // N+1
