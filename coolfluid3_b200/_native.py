@@ -108,6 +108,15 @@ SIGNATURES = {
     "ufem_ns_get_assembly_kernel": (C.c_int, [_P, C.POINTER(C.c_int32), C.POINTER(C.c_int32)]),
     "ufem_ns_tune_assembly": (C.c_int, [_P, C.c_void_p, C.c_int32, C.POINTER(C.c_int32), C.POINTER(C.c_int32),
                                         C.POINTER(C.c_float)]),
+    "ufem_batch_create": (C.c_int, [C.POINTER(_P), C.c_int32, C.POINTER(_P)]),
+    "ufem_batch_size": (C.c_int, [_P, C.POINTER(C.c_int32), C.POINTER(C.c_int64)]),
+    "ufem_batch_set_graphs": (C.c_int, [_P, C.c_int32]),
+    "ufem_batch_set_assembly_warps": (C.c_int, [_P, C.c_int32]),
+    "ufem_batch_assemble": (C.c_int, [_P, C.c_void_p]),
+    "ufem_batch_solve": (C.c_int, [_P, C.POINTER(KrylovOpts), C.POINTER(KrylovStatus), C.c_void_p]),
+    "ufem_batch_update": (C.c_int, [_P, C.c_void_p]),
+    "ufem_batch_step": (C.c_int, [_P, C.POINTER(KrylovOpts), C.POINTER(KrylovStatus), C.c_void_p]),
+    "ufem_batch_destroy": (None, [_P]),
     "ufem_ns_enable_timing": (C.c_int, [_P, C.c_int32]),
     "ufem_ns_get_timings": (C.c_int, [_P, C.POINTER(Timings)]),
     "ufem_ns_destroy": (None, [_P]),

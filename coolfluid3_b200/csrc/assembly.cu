@@ -983,10 +983,13 @@ constexpr int warp_lane_pitch() {
   return D == 3 ? (sizeof(T) == 4 ? 68 : 70) : 31;
 }
 
+constexpr size_t kDescSlot = (sizeof(AsmDesc) + 15) / 16 * 16;
+
 template <int D, typename T>
 constexpr size_t warp_stage_bytes() {
   return size_t(32) * warp_lane_pitch<D, T>() * sizeof(T) +  // staged row blocks + RHS rows, one slice per lane
-         size_t(D * 64 + 32 + 36 + 36) * 4;                   // slot masks per local position, pslots, prefix, offsets
+         size_t(D * 64 + 32 + 36 + 36) * 4 +                  // slot masks per local position, pslots, prefix, offsets
+         2 * kDescSlot;                                       // descriptors of the current and the next mesh
 }
 static_assert(warp_stage_bytes<2, float>() % 16 == 0 && warp_stage_bytes<2, double>() % 16 == 0 &&
                   warp_stage_bytes<3, float>() % 16 == 0 && warp_stage_bytes<3, double>() % 16 == 0,
@@ -1013,14 +1016,11 @@ __device__ __forceinline__ void load_run(const T* __restrict__ src, T (&v)[NV]) 
   }
 }
 
-template <int D, typename T, bool SPEC, int WPB>
-__global__ void __launch_bounds__(32 * WPB) ns_assembly_warp_kernel(
-    int ngroups, const int4* __restrict__ groups, const int32_t* __restrict__ row_inc,
-    const int32_t* __restrict__ inc_elem, const uint32_t* __restrict__ inc_info, const int4* __restrict__ conn,
-    const double* __restrict__ coords, const double* __restrict__ uadv, const double* __restrict__ state,
-    const float* __restrict__ node32, const double* __restrict__ force, const int64_t* __restrict__ start,
-    NSParams p, double* __restrict__ vals,
-    float* __restrict__ vals32, double* __restrict__ rhs) {
+template <int D, typename T, bool SPEC, int WPB, bool BATCH>
+__global__ void __launch_bounds__(32 * WPB) ns_assembly_warp_kernel(int ngroups, int nmesh,
+                                                                     const AsmDesc* __restrict__ descs,
+                                                                     const int* __restrict__ gprefix,
+                                                                     const __grid_constant__ AsmDesc one) {
   constexpr int n = P1<D>::n, neq = P1<D>::neq, nvals = P1<D>::nvals;
   constexpr int LS = warp_lane_pitch<D, T>();
   constexpr int RPI = (D == 3) ? 2 : 3;      // equations (CSR rows) per off-diagonal item
@@ -1034,35 +1034,75 @@ __global__ void __launch_bounds__(32 * WPB) ns_assembly_warp_kernel(
   uint32_t* s_pslots = s_mask + D * 64;                              // 32
   int* s_pref = reinterpret_cast<int*>(s_pslots + 32);               // 33 (+3 pad)
   int* s_off = s_pref + 36;                                          // 33 (+3 pad): lane offset of each row
+  // Mesh descriptors: a one-mesh launch reads its descriptor from the kernel
+  // parameters; a batch keeps the descriptors of the current and the next
+  // group's mesh in the warp's slice (copied when the mesh changes).
+  AsmDesc* s_desc = reinterpret_cast<AsmDesc*>(reinterpret_cast<unsigned char*>(s_off + 36));
+  int mesh0 = -1, mesh1 = -1;  // mesh held by descriptor slot 0 / 1
+  auto load_desc = [&](int m, int slot) {
+    if constexpr (BATCH) {
+      const int held = slot ? mesh1 : mesh0;
+      if (held != m) {  // warp-uniform
+        constexpr int W = int(sizeof(AsmDesc) / 8);
+        const unsigned long long* src = reinterpret_cast<const unsigned long long*>(descs + m);
+        unsigned long long* dst = reinterpret_cast<unsigned long long*>(s_desc + slot);
+        for (int q = lane; q < W; q += 32) dst[q] = __ldg(src + q);
+        if (slot) mesh1 = m; else mesh0 = m;
+        __syncwarp();
+      }
+    }
+  };
+  auto desc = [&](int slot) -> const AsmDesc& {
+    if constexpr (BATCH) return s_desc[slot]; else return one;
+  };
 
-  // Persistent warps: a warp walks the groups g, g + stride, ...  While it
-  // reduces one group it already loads the incidence records (element id, slot
-  // word) and the connectivity of the next, so the next element phase starts
-  // with only the node gathers outstanding.
+  // Persistent warps: a warp walks the global groups g, g + stride, ... of all
+  // meshes of the launch (mesh m owns groups [gprefix[m], gprefix[m + 1])).
+  // While it reduces one group it already loads the incidence records
+  // (element id, slot word) and the connectivity of the next, so the next
+  // element phase starts with only the node gathers outstanding.
   int g = blockIdx.x * WPB + warp;
   if (g >= ngroups) return;  // whole warp; no CTA-wide barrier below
   const int gstride = gridDim.x * WPB;
-  int4 G = groups[g];  // first row, end row, first incidence, incidences
+  auto mesh_of = [&](int q) {  // last m with gprefix[m] <= q
+    int lo = 0, hi = nmesh - 1;
+    while (lo < hi) {
+      const int mid = (lo + hi + 1) >> 1;
+      if (__ldg(gprefix + mid) <= q) lo = mid; else hi = mid - 1;
+    }
+    return lo;
+  };
+  int cm = BATCH ? mesh_of(g) : 0;
+  int cs = 0;  // descriptor slot of the current mesh
+  load_desc(cm, cs);
+  // first row, end row, first incidence, incidences
+  int4 G = __ldg(desc(cs).groups + (g - (BATCH ? __ldg(gprefix + cm) : 0)));
   int pe = 0, poff = 0, pitems = 0;
   uint32_t pinfo = 0;
   int4 pcn = make_int4(0, 0, 0, 0);
-  auto fetch_records = [&](const int4& q) {
+  auto fetch_records = [&](const int4& q, const AsmDesc& d) {
     if (lane < q.w) {
-      pe = __ldg(inc_elem + q.z + lane);
-      pinfo = __ldg(inc_info + q.z + lane);
+      pe = __ldg(d.inc_elem + q.z + lane);
+      pinfo = __ldg(d.inc_info + q.z + lane);
     }
     if (lane < q.y - q.x) {
-      poff = __ldg(row_inc + q.x + lane) - q.z;
-      pitems = int(__ldg(start + q.x + lane + 1) - __ldg(start + q.x + lane) - 1) * RG;
+      poff = __ldg(d.row_inc + q.x + lane) - q.z;
+      pitems = int(__ldg(d.start + q.x + lane + 1) - __ldg(d.start + q.x + lane) - 1) * RG;
     }
   };
-  fetch_records(G);
-  if (lane < G.w) pcn = __ldg(conn + pe);
+  fetch_records(G, desc(cs));
+  if (lane < G.w) pcn = __ldg(desc(cs).conn + pe);
   for (;;) {
     const int row0 = G.x, R = G.y - G.x, K = G.w;  // 1 <= R <= K <= 32
     const int gn = g + gstride;
-    const int4 Gn = gn < ngroups ? groups[gn] : make_int4(0, 0, 0, 0);
+    const int mn = (BATCH && gn < ngroups) ? mesh_of(gn) : cm;
+    const int ns = (mn == cm) ? cs : 1 - cs;  // descriptor slot of the next group's mesh
     __syncwarp();  // the previous group's reads of the shared slice are complete
+    load_desc(mn, ns);
+    const int4 Gn = gn < ngroups ? __ldg(desc(ns).groups + (gn - (BATCH ? __ldg(gprefix + mn) : 0)))
+                                 : make_int4(0, 0, 0, 0);
+    const AsmDesc& dc = desc(cs);
+    const int64_t* __restrict__ start = dc.start;
     int pref = lane < R ? pitems : 0;  // inclusive scan of the off-diagonal item counts
 #pragma unroll
     for (int o = 1; o < 32; o <<= 1) {
@@ -1101,20 +1141,23 @@ __global__ void __launch_bounds__(32 * WPB) ns_assembly_warp_kernel(
         pslots |= sl << (8 * q);
       }
       T* st = stage + lane * LS;
-      const KParams<T> kp = make_kparams<T>(p);
-      const NodeData nd{coords, uadv, state, node32};
+      const KParams<T> kp = make_kparams<T>(dc.p);
+      const NodeData nd{dc.coords, dc.uadv, dc.state, dc.node32};
       if constexpr (SPEC) {
         if constexpr (D == 2) spec_tri_row<T>(ids, a, nd, kp, st, st + nvals, 1);
         else spec_tet_row<T>(ids, a, nd, kp, st, st + nvals, 1);
       } else {
-        generic_row<D, T>(ids, a, nd, force, kp, st, st + nvals, 1);
+        generic_row<D, T>(ids, a, nd, dc.force, kp, st, st + nvals, 1);
       }
 #pragma unroll
       for (int q = 1; q < n; ++q) atomicOr(s_mask + (q - 1) * 64 + ((pslots >> (8 * q)) & 0xFFu), 1u << lane);
     }
     s_pslots[lane] = pslots;
     __syncwarp();
-    fetch_records(Gn);  // next group's records load while this group is reduced
+    fetch_records(Gn, desc(ns));  // next group's records load while this group is reduced
+    double* __restrict__ vals = dc.vals;
+    float* __restrict__ vals32 = dc.vals32;
+    double* __restrict__ rhs = dc.rhs;
 
     // Phase 2a: diagonal entries and RHS entries, neq * (neq + 1) items per row,
     // each the sum over the row's lanes in element order.
@@ -1139,7 +1182,7 @@ __global__ void __launch_bounds__(32 * WPB) ns_assembly_warp_kernel(
       }
     }
 
-    if (lane < Gn.w) pcn = __ldg(conn + pe);
+    if (lane < Gn.w) pcn = __ldg(desc(ns).conn + pe);
 
     // Phase 2b: off-diagonal items (row, slot != self, group of RPI equations):
     // the contributors of slot s are the row's lanes holding s at local position
@@ -1200,6 +1243,8 @@ __global__ void __launch_bounds__(32 * WPB) ns_assembly_warp_kernel(
     if (gn >= ngroups) break;
     g = gn;
     G = Gn;
+    cm = mn;
+    cs = ns;
   }
 }
 
@@ -1333,6 +1378,8 @@ __global__ void dirichlet_rows_kernel(int64_t nbc, int neq, const int64_t* __res
   }
 }
 
+}  // namespace
+
 void fill_params(const ufem_ns_handle* h, NSParams& p) {
   const double dt = h->opt.dt, c1 = h->opt.c1;
   p.theta = h->opt.theta; p.inv_theta = 1.0 / h->opt.theta; p.dt = dt; p.invdt = 1.0 / dt;
@@ -1344,6 +1391,26 @@ void fill_params(const ufem_ns_handle* h, NSParams& p) {
   p.a_bu = h->opt.alpha_bu; p.u_ref = h->opt.u_ref; p.supg_type = h->opt.supg_type;
   p.has_force = h->d_force != nullptr;
 }
+
+void fill_desc(const ufem_ns_handle* h, bool write32, AsmDesc& d) {
+  d.coords = h->d_coords;
+  d.uadv = h->d_uadv;
+  d.state = h->d_state;
+  d.node32 = h->d_node32;
+  d.force = h->d_force;
+  d.start = h->d_start;
+  d.row_inc = h->d_row_inc;
+  d.inc_elem = h->d_inc_elem;
+  d.inc_info = h->d_inc_info;
+  d.conn = reinterpret_cast<const int4*>(h->d_conn);
+  d.groups = h->wplan.groups;
+  d.vals = h->d_vals;
+  d.vals32 = write32 ? h->d_vals32 : nullptr;
+  d.rhs = h->d_rhs;
+  fill_params(h, d.p);
+}
+
+namespace {
 
 template <int D, typename T, int CH, bool SPEC>
 int launch_chunk_t(const ufem_ns_handle* h, const AssemblyPlan& plan, const NSParams& p, cudaStream_t s,
@@ -1371,21 +1438,27 @@ int resident_ctas(K kernel, int threads, size_t smem) {
   return sms * per_sm;
 }
 
-template <int D, typename T, bool SPEC, int WPB>
-int launch_warp_t(const ufem_ns_handle* h, const NSParams& p, cudaStream_t s, bool write32) {
-  const WarpPlan& wp = h->wplan;
-  if (wp.ngroups == 0) return UFEM_OK;
+template <int D, typename T, bool SPEC, int WPB, bool BATCH>
+int launch_warp_t(int ngroups, int nmesh, const AsmDesc* descs, const int* gprefix, const AsmDesc& one,
+                  cudaStream_t s) {
+  if (ngroups == 0) return UFEM_OK;
   constexpr size_t smem = warp_stage_bytes<D, T>() * WPB;
-  static const int resident = resident_ctas(ns_assembly_warp_kernel<D, T, SPEC, WPB>, 32 * WPB, smem);
+  static const int resident = resident_ctas(ns_assembly_warp_kernel<D, T, SPEC, WPB, BATCH>, 32 * WPB, smem);
   if (resident <= 0) return set_error(UFEM_ERR_CUDA, "occupancy query of the warp assembly kernel failed");
-  const unsigned grid = unsigned(std::min<int64_t>((wp.ngroups + WPB - 1) / WPB, resident));
-  ns_assembly_warp_kernel<D, T, SPEC, WPB><<<grid, 32 * WPB, smem, s>>>(
-      wp.ngroups, wp.groups, h->d_row_inc, h->d_inc_elem, h->d_inc_info, reinterpret_cast<const int4*>(h->d_conn),
-      h->d_coords, h->d_uadv, h->d_state, h->d_node32, h->d_force, h->d_start, p, h->d_vals,
-      write32 ? h->d_vals32 : nullptr,
-      h->d_rhs);
+  const unsigned grid = unsigned(std::min<int64_t>((ngroups + WPB - 1) / WPB, resident));
+  ns_assembly_warp_kernel<D, T, SPEC, WPB, BATCH><<<grid, 32 * WPB, smem, s>>>(ngroups, nmesh, descs, gprefix, one);
   UFEM_CUDA_TRY(cudaGetLastError());
   return UFEM_OK;
+}
+
+template <int D, typename T, bool SPEC, bool BATCH>
+int launch_warp_w(int warps, int ngroups, int nmesh, const AsmDesc* descs, const int* gprefix, const AsmDesc& one,
+                  cudaStream_t s) {
+  switch (warps) {
+    case 2: return launch_warp_t<D, T, SPEC, 2, BATCH>(ngroups, nmesh, descs, gprefix, one, s);
+    case 8: return launch_warp_t<D, T, SPEC, 8, BATCH>(ngroups, nmesh, descs, gprefix, one, s);
+    default: return launch_warp_t<D, T, SPEC, 4, BATCH>(ngroups, nmesh, descs, gprefix, one, s);
+  }
 }
 
 template <int D, typename T, int CH, bool SPEC>
@@ -1395,12 +1468,10 @@ int launch_assembly_t(ufem_ns_handle* h, cudaStream_t s, bool write32) {
   constexpr bool f32 = std::is_same<T, float>::value;
   if (h->asm_variant == kAsmChunk) return launch_chunk_t<D, T, CH, SPEC>(h, f32 ? h->plan32 : h->plan64, p, s, write32);
   int rc;
-  switch (h->asm_warps) {
-    case 2: rc = launch_warp_t<D, T, SPEC, 2>(h, p, s, write32); break;
-    case 8: rc = launch_warp_t<D, T, SPEC, 8>(h, p, s, write32); break;
-    default: rc = launch_warp_t<D, T, SPEC, 4>(h, p, s, write32); break;
-  }
-  if (rc) return rc;
+  AsmDesc one;  // this handle's descriptor, passed as a kernel parameter
+  fill_desc(h, write32, one);
+  if ((rc = launch_warp_w<D, T, SPEC, false>(h->asm_warps, h->wplan.ngroups, 1, nullptr, nullptr, one, s)))
+    return rc;
   return launch_chunk_t<D, T, CH, SPEC>(h, f32 ? h->wplan.big32 : h->wplan.big64, p, s, write32);
 }
 
@@ -1409,11 +1480,17 @@ int set_smem_attr() {
   constexpr size_t smem = assembly_smem_bytes<D, T, CH>();
   UFEM_CUDA_TRY(cudaFuncSetAttribute(ns_assembly_kernel<D, T, CH, SPEC>,
                                      cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
-  UFEM_CUDA_TRY(cudaFuncSetAttribute(ns_assembly_warp_kernel<D, T, SPEC, 2>,
+  UFEM_CUDA_TRY(cudaFuncSetAttribute(ns_assembly_warp_kernel<D, T, SPEC, 2, false>,
                                      cudaFuncAttributeMaxDynamicSharedMemorySize, int(2 * warp_stage_bytes<D, T>())));
-  UFEM_CUDA_TRY(cudaFuncSetAttribute(ns_assembly_warp_kernel<D, T, SPEC, 4>,
+  UFEM_CUDA_TRY(cudaFuncSetAttribute(ns_assembly_warp_kernel<D, T, SPEC, 4, false>,
                                      cudaFuncAttributeMaxDynamicSharedMemorySize, int(4 * warp_stage_bytes<D, T>())));
-  UFEM_CUDA_TRY(cudaFuncSetAttribute(ns_assembly_warp_kernel<D, T, SPEC, 8>,
+  UFEM_CUDA_TRY(cudaFuncSetAttribute(ns_assembly_warp_kernel<D, T, SPEC, 8, false>,
+                                     cudaFuncAttributeMaxDynamicSharedMemorySize, int(8 * warp_stage_bytes<D, T>())));
+  UFEM_CUDA_TRY(cudaFuncSetAttribute(ns_assembly_warp_kernel<D, T, SPEC, 2, true>,
+                                     cudaFuncAttributeMaxDynamicSharedMemorySize, int(2 * warp_stage_bytes<D, T>())));
+  UFEM_CUDA_TRY(cudaFuncSetAttribute(ns_assembly_warp_kernel<D, T, SPEC, 4, true>,
+                                     cudaFuncAttributeMaxDynamicSharedMemorySize, int(4 * warp_stage_bytes<D, T>())));
+  UFEM_CUDA_TRY(cudaFuncSetAttribute(ns_assembly_warp_kernel<D, T, SPEC, 8, true>,
                                      cudaFuncAttributeMaxDynamicSharedMemorySize, int(8 * warp_stage_bytes<D, T>())));
   return UFEM_OK;
 }
@@ -1458,6 +1535,39 @@ int launch_assembly(ufem_ns_handle* h, cudaStream_t s, bool write32) {
                        : launch_assembly_t<3, float, kChunk3D32, false>(h, s, write32);
   return spec ? launch_assembly_t<3, double, kChunk3D64, true>(h, s, write32)
               : launch_assembly_t<3, double, kChunk3D64, false>(h, s, write32);
+}
+
+int launch_assembly_batch(int dim, int precision, bool spec, int warps, int ngroups, int nmesh,
+                          const AsmDesc* d_descs, const int* d_gprefix, cudaStream_t s) {
+  const bool f32 = precision == 1;
+  if (dim == 2) {
+    if (f32) return spec ? launch_warp_w<2, float, true, true>(warps, ngroups, nmesh, d_descs, d_gprefix, AsmDesc{}, s)
+                         : launch_warp_w<2, float, false, true>(warps, ngroups, nmesh, d_descs, d_gprefix, AsmDesc{}, s);
+    return spec ? launch_warp_w<2, double, true, true>(warps, ngroups, nmesh, d_descs, d_gprefix, AsmDesc{}, s)
+                : launch_warp_w<2, double, false, true>(warps, ngroups, nmesh, d_descs, d_gprefix, AsmDesc{}, s);
+  }
+  if (f32) return spec ? launch_warp_w<3, float, true, true>(warps, ngroups, nmesh, d_descs, d_gprefix, AsmDesc{}, s)
+                       : launch_warp_w<3, float, false, true>(warps, ngroups, nmesh, d_descs, d_gprefix, AsmDesc{}, s);
+  return spec ? launch_warp_w<3, double, true, true>(warps, ngroups, nmesh, d_descs, d_gprefix, AsmDesc{}, s)
+              : launch_warp_w<3, double, false, true>(warps, ngroups, nmesh, d_descs, d_gprefix, AsmDesc{}, s);
+}
+
+int launch_assembly_big_rows(ufem_ns_handle* h, cudaStream_t s, bool write32) {
+  NSParams p;
+  fill_params(h, p);
+  const bool spec = h->opt.use_specializations != 0;
+  const bool f32 = h->opt.precision == 1;
+  const WarpPlan& w = h->wplan;
+  if (h->dim == 2) {
+    if (f32) return spec ? launch_chunk_t<2, float, kChunk2D, true>(h, w.big32, p, s, write32)
+                         : launch_chunk_t<2, float, kChunk2D, false>(h, w.big32, p, s, write32);
+    return spec ? launch_chunk_t<2, double, kChunk2D, true>(h, w.big64, p, s, write32)
+                : launch_chunk_t<2, double, kChunk2D, false>(h, w.big64, p, s, write32);
+  }
+  if (f32) return spec ? launch_chunk_t<3, float, kChunk3D32, true>(h, w.big32, p, s, write32)
+                       : launch_chunk_t<3, float, kChunk3D32, false>(h, w.big32, p, s, write32);
+  return spec ? launch_chunk_t<3, double, kChunk3D64, true>(h, w.big64, p, s, write32)
+              : launch_chunk_t<3, double, kChunk3D64, false>(h, w.big64, p, s, write32);
 }
 
 int launch_linearize(ufem_ns_handle* h, cudaStream_t s) {

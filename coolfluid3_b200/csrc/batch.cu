@@ -1,0 +1,1058 @@
+// batch.cu -- many independent meshes stepped together (no counterpart in the
+// reference, which runs one UFEM solver per process).
+//
+// A batch holds handles of the same dimension, element precision and element
+// form.  Every phase of a time step is one launch over all members:
+//  - linearisation, the symmetric Dirichlet passes and the update run over the
+//    concatenated node / boundary-condition index spaces (a thread finds its
+//    mesh by binary search over a prefix of the member sizes);
+//  - the assembly is the persistent warp kernel over all members' row groups;
+//  - the solve is BiCGStab with point Jacobi and PER-MESH scalars: each member
+//    is split into fixed chunks of kChunkRows rows, vector kernels produce one
+//    partial per chunk, and one warp per mesh folds that mesh's partials in a
+//    fixed order.  A member's arithmetic therefore depends only on its own
+//    data: its results are bitwise the same alone (a batch of one) and in any
+//    mix.  Converged members drop out (their kernels return at once) while the
+//    others continue.
+// The iteration block (8 BiCGStab iterations) is captured once into a CUDA
+// graph and replayed; the host reads the members' done flags between blocks.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdint>
+#include <string>
+#include <vector>
+
+#include "internal.h"
+
+namespace ufem {
+namespace {
+
+constexpr int kChunkRows = 2048;  // rows per solver chunk (one CTA, one partial)
+constexpr int kThreads = 256;
+constexpr int kBlockIters = 8;    // BiCGStab iterations per host check / graph replay
+constexpr int kDc = 16;           // per-mesh double scalars
+constexpr int kIc = 8;            // per-mesh int flags
+
+// per-mesh scalar slots (dctl[m * kDc + ...])
+constexpr int sBnorm = 0, sBeta = 1, sEst = 2, sRho = 5, sRhoOld = 6, sAlpha = 7, sOmega = 8, sTrue = 9,
+              sTol = 10, sTS = 11, sTT = 12;
+// per-mesh flags (ictl[m * kIc + ...])
+constexpr int fDone = 0, fStatus = 2, fIters = 3, fMaxit = 4, fOuter = 5;
+
+struct BatchMesh {
+  int64_t N, nrows, row_off;  // row_off: first row in the concatenated solver vectors
+  int dim, neq;
+  double* state;
+  double* hist;  // u1, u2, u3 (3 x N x 4)
+  const double* nu;
+  double* uadv;
+  float* node32;
+  const int64_t* start;
+  const int32_t* adj;
+  const int64_t* diagpos;
+  const int64_t* rowptr;
+  double* vals;
+  float* vals32;
+  double* rhs;
+  double* sol;
+  int64_t nbc, nfix_rows;
+  const int64_t* bc_dof;
+  const double* bc_first;
+  const double* bc_last;
+  const int64_t* bc_diag;
+  double* vfirst;
+  const int64_t* fix_row;
+  const int64_t* fix_ptr;
+  const int64_t* fix_pos;
+  const int32_t* fix_bc;
+};
+
+struct Chunk {
+  int mesh, lo, hi, pad;  // local rows [lo, hi) of `mesh`
+};
+
+__device__ __forceinline__ int find_mesh(const int64_t* __restrict__ prefix, int nmesh, int64_t i) {
+  int lo = 0, hi = nmesh - 1;
+  while (lo < hi) {  // last m with prefix[m] <= i
+    const int mid = (lo + hi + 1) >> 1;
+    if (__ldg(prefix + mid) <= i) lo = mid; else hi = mid - 1;
+  }
+  return lo;
+}
+
+__device__ __forceinline__ double block_sum(double v, double* sm) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  if (lane == 0) sm[wid] = v;
+  __syncthreads();
+  double s = 0.0;
+  if (threadIdx.x == 0)
+    for (int k = 0; k < int(blockDim.x >> 5); ++k) s += sm[k];
+  __syncthreads();
+  return s;
+}
+
+// ---- node-parallel phases ------------------------------------------------------
+
+// LinearizeU + FP32 node copy, as linearize_kernel, over all members' nodes.
+__global__ void linearize_batch_kernel(int64_t total, int nmesh, const int64_t* __restrict__ node_prefix,
+                                       const BatchMesh* __restrict__ bm) {
+  const int64_t g = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (g >= total) return;
+  const int m = find_mesh(node_prefix, nmesh, g);
+  const BatchMesh& M = bm[m];
+  const int64_t i = g - node_prefix[m];
+  const int dim = M.dim;
+  const double* u1 = M.hist;
+  const double* u2 = M.hist + 4 * M.N;
+  const double* u3 = M.hist + 8 * M.N;
+  double out[4] = {0, 0, 0, 0};
+  for (int k = 0; k < dim; ++k) {
+    const int64_t o = 4 * i + k;
+    double v = __dsub_rn(__dmul_rn(2.1875, M.state[o]), __dmul_rn(2.1875, u1[o]));
+    v = __dadd_rn(v, __dmul_rn(1.3125, u2[o]));
+    v = __dsub_rn(v, __dmul_rn(0.3125, u3[o]));
+    out[k] = v;
+  }
+  out[3] = M.nu[i];
+  reinterpret_cast<double2*>(M.uadv + 4 * i)[0] = make_double2(out[0], out[1]);
+  reinterpret_cast<double2*>(M.uadv + 4 * i)[1] = make_double2(out[2], out[3]);
+  if (M.node32 != nullptr) {
+    float4* q = reinterpret_cast<float4*>(M.node32) + 2 * i;
+    q[0] = make_float4(float(out[0]), float(out[1]), float(out[2]), float(out[3]));
+    const double* x = M.state + 4 * i;
+    q[1] = make_float4(float(x[0]), float(x[1]), dim == 3 ? float(x[2]) : 0.0f, float(x[dim]));
+  }
+}
+
+// u3 = u2, u2 = u1, u1 = u, u += du, p += dp
+__global__ void update_batch_kernel(int64_t total, int nmesh, const int64_t* __restrict__ node_prefix,
+                                    const BatchMesh* __restrict__ bm) {
+  const int64_t g = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (g >= total) return;
+  const int m = find_mesh(node_prefix, nmesh, g);
+  const BatchMesh& M = bm[m];
+  const int64_t i = g - node_prefix[m];
+  const int dim = M.dim, neq = M.neq;
+  double* u1 = M.hist;
+  double* u2 = M.hist + 4 * M.N;
+  double* u3 = M.hist + 8 * M.N;
+  for (int k = 0; k < dim; ++k) {
+    const int64_t o = 4 * i + k;
+    u3[o] = u2[o];
+    u2[o] = u1[o];
+    const double u = M.state[o];
+    u1[o] = u;
+    M.state[o] = __dadd_rn(u, M.sol[i * neq + k]);
+  }
+  M.state[4 * i + dim] = __dadd_rn(M.state[4 * i + dim], M.sol[i * neq + dim]);
+}
+
+// Symmetric Dirichlet over all members, the three passes of the one-mesh form.
+__global__ void dirichlet_values_batch_kernel(int64_t total, int nmesh, const int64_t* __restrict__ bc_prefix,
+                                              const BatchMesh* __restrict__ bm) {
+  const int64_t g = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (g >= total) return;
+  const int m = find_mesh(bc_prefix, nmesh, g);
+  const BatchMesh& M = bm[m];
+  const int64_t u = g - bc_prefix[m];
+  const int64_t dof = M.bc_dof[u];
+  const int64_t node = dof / M.neq;
+  const int comp = int(dof - node * M.neq);
+  M.vfirst[u] = __dsub_rn(M.bc_first[u], M.state[4 * node + comp]);
+}
+
+__global__ void dirichlet_columns_batch_kernel(int64_t total, int nmesh, const int64_t* __restrict__ fix_prefix,
+                                               const BatchMesh* __restrict__ bm) {
+  const int64_t g = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (g >= total) return;
+  const int m = find_mesh(fix_prefix, nmesh, g);
+  const BatchMesh& M = bm[m];
+  const int64_t q = g - fix_prefix[m];
+  const int64_t row = M.fix_row[q];
+  const int64_t k0 = M.fix_ptr[q], k1 = M.fix_ptr[q + 1];
+  double r = M.rhs[row];
+  for (int64_t k = k0; k < k1; ++k) r = __dadd_rn(r, __dmul_rn(-M.vals[M.fix_pos[k]], M.vfirst[M.fix_bc[k]]));
+  for (int64_t k = k0; k < k1; ++k) {
+    const int64_t pos = M.fix_pos[k];
+    M.vals[pos] = 0.0;
+    if (M.vals32) M.vals32[pos] = 0.0f;
+  }
+  M.rhs[row] = r;
+}
+
+__global__ void dirichlet_rows_batch_kernel(int nmesh, const int64_t* __restrict__ bc_prefix,
+                                            const BatchMesh* __restrict__ bm) {
+  const int64_t g = blockIdx.x;
+  const int m = find_mesh(bc_prefix, nmesh, g);
+  const BatchMesh& M = bm[m];
+  const int64_t u = g - bc_prefix[m];
+  const int64_t dof = M.bc_dof[u];
+  for (int64_t p = M.rowptr[dof] + threadIdx.x; p < M.rowptr[dof + 1]; p += blockDim.x) {
+    M.vals[p] = 0.0;
+    if (M.vals32) M.vals32[p] = 0.0f;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    M.vals[M.bc_diag[u]] = 1.0;
+    if (M.vals32) M.vals32[M.bc_diag[u]] = 1.0f;
+    const int64_t node = dof / M.neq;
+    const int comp = int(dof - node * M.neq);
+    const double v = __dsub_rn(M.bc_last[u], M.state[4 * node + comp]);
+    M.rhs[dof] = v;
+    M.sol[dof] = v;
+  }
+}
+
+// ---- solver kernels --------------------------------------------------------------
+// Vector locations: a BiCGStab operand is either one of the batch's
+// concatenated work vectors (offset by the mesh's row_off) or a member's own
+// rhs / sol array.
+enum Loc { kWork = 0, kRhs = 1, kSol = 2 };
+
+template <int L>
+__device__ __forceinline__ double* vec(const BatchMesh& M, double* work) {
+  if constexpr (L == kRhs) return M.rhs;
+  else if constexpr (L == kSol) return M.sol;
+  else return work + M.row_off;
+}
+
+// y = A x, one warp per node over all members (FP64 accumulation, as spmv_kernel).
+template <int NEQ, typename MT, int XL>
+__global__ void __launch_bounds__(256) spmv_batch_kernel(int64_t total_nodes, int nmesh,
+                                                         const int64_t* __restrict__ node_prefix,
+                                                         const BatchMesh* __restrict__ bm, double* xwork,
+                                                         double* __restrict__ ywork, const int* __restrict__ ictl) {
+  const int64_t gnode = (int64_t(blockIdx.x) * blockDim.x + threadIdx.x) >> 5;
+  const int lane = threadIdx.x & 31;
+  if (gnode >= total_nodes) return;
+  const int m = find_mesh(node_prefix, nmesh, gnode);
+  if (ictl[m * kIc + fDone]) return;
+  const BatchMesh& M = bm[m];
+  const int64_t node = gnode - node_prefix[m];
+  const double* x = vec<XL>(M, xwork);
+  double* y = ywork + M.row_off;
+  const MT* vals;
+  if constexpr (std::is_same<MT, float>::value) vals = M.vals32; else vals = M.vals;
+  const int64_t s0 = __ldg(M.start + node);
+  const int len = int(__ldg(M.start + node + 1) - s0) * NEQ;
+  const MT* row = vals + int64_t(NEQ) * NEQ * s0;
+  double acc[NEQ];
+#pragma unroll
+  for (int r = 0; r < NEQ; ++r) acc[r] = 0.0;
+  for (int j = lane; j < len; j += 32) {
+    const int s = j / NEQ;
+    const int c = j - s * NEQ;
+    const double xj = x[int64_t(__ldg(M.adj + s0 + s)) * NEQ + c];
+    MT v[NEQ];
+#pragma unroll
+    for (int r = 0; r < NEQ; ++r) v[r] = __ldcs(row + r * len + j);
+#pragma unroll
+    for (int r = 0; r < NEQ; ++r) acc[r] += double(v[r]) * xj;
+  }
+#pragma unroll
+  for (int r = 0; r < NEQ; ++r) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) acc[r] += __shfl_xor_sync(0xffffffffu, acc[r], o);
+  }
+  if (lane < NEQ) {
+    double out = acc[0];
+#pragma unroll
+    for (int r = 1; r < NEQ; ++r)
+      if (lane == r) out = acc[r];
+    y[node * NEQ + lane] = out;
+  }
+}
+
+// dinv = 1 / diag (point Jacobi) of the operator the solve uses.
+template <typename MT>
+__global__ void jacobi_batch_kernel(const Chunk* __restrict__ chunks, const BatchMesh* __restrict__ bm,
+                                    double* __restrict__ dinv, const int* __restrict__ ictl) {
+  const Chunk c = chunks[blockIdx.x];
+  if (ictl[c.mesh * kIc + fDone]) return;
+  const BatchMesh& M = bm[c.mesh];
+  const MT* vals;
+  if constexpr (std::is_same<MT, float>::value) vals = M.vals32; else vals = M.vals;
+  for (int i = c.lo + threadIdx.x; i < c.hi; i += blockDim.x) {
+    const double d = double(vals[M.diagpos[i]]);
+    dinv[M.row_off + i] = d != 0.0 ? 1.0 / d : 1.0;
+  }
+}
+
+// r = b - w (w = A x), partials of r.r and b.b; rh = r when `init`.
+template <int BL>
+__global__ void residual_batch_kernel(const Chunk* __restrict__ chunks, const BatchMesh* __restrict__ bm,
+                                      double* bwork, const double* __restrict__ w, double* __restrict__ r,
+                                      double* __restrict__ rh, double* __restrict__ part, int nchunks,
+                                      const int* __restrict__ ictl, int skip_done) {
+  __shared__ double sm[32];
+  const Chunk c = chunks[blockIdx.x];
+  if (skip_done && ictl[c.mesh * kIc + fDone]) return;  // uniform per CTA
+  const BatchMesh& M = bm[c.mesh];
+  const double* b = vec<BL>(M, bwork);
+  const int64_t off = M.row_off;
+  double s2 = 0.0, b2 = 0.0;
+  for (int i = c.lo + threadIdx.x; i < c.hi; i += blockDim.x) {
+    const double bi = b[i];
+    const double ri = bi - w[off + i];
+    r[off + i] = ri;
+    if (rh) rh[off + i] = ri;
+    s2 += ri * ri;
+    b2 += bi * bi;
+  }
+  s2 = block_sum(s2, sm);
+  b2 = block_sum(b2, sm);
+  if (threadIdx.x == 0) {
+    part[blockIdx.x] = s2;
+    part[nchunks + blockIdx.x] = b2;
+  }
+}
+
+// Per-mesh fold of chunk partials: one warp per mesh, fixed order.
+__device__ __forceinline__ void fold2(const double* __restrict__ part, int nchunks, int c0, int c1, double& a,
+                                      double& b) {
+  const int lane = threadIdx.x & 31;
+  a = 0.0;
+  b = 0.0;
+  for (int k = c0 + lane; k < c1; k += 32) {
+    a += part[k];
+    b += part[nchunks + k];
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    a += __shfl_xor_sync(0xffffffffu, a, o);
+    b += __shfl_xor_sync(0xffffffffu, b, o);
+  }
+}
+
+// Start of a solve: ||r0||, ||b||, BiCGStab scalars, per-mesh tol / maxit.
+// `outer_done` meshes (already converged in the refinement loop) stay done.
+__global__ void bicg_init_batch_kernel(int nmesh, const int* __restrict__ cprefix, const double* __restrict__ part,
+                                       int nchunks, double* __restrict__ dctl, int* __restrict__ ictl, double tol,
+                                       int maxit, int use_outer) {
+  const int m = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  if (m >= nmesh) return;
+  double rr, bb;
+  fold2(part, nchunks, cprefix[m], cprefix[m + 1], rr, bb);
+  if ((threadIdx.x & 31) != 0) return;
+  double* d = dctl + m * kDc;
+  int* f = ictl + m * kIc;
+  const double beta = sqrt(rr), bnorm = sqrt(bb);
+  d[sBeta] = beta;
+  d[sBnorm] = bnorm;
+  d[sEst] = beta;
+  d[sRho] = rr;
+  d[sRhoOld] = 1.0;
+  d[sAlpha] = 1.0;
+  d[sOmega] = 1.0;
+  d[sTol] = tol;
+  f[fMaxit] = maxit;
+  f[fIters] = 0;
+  f[fStatus] = isfinite(beta) ? 0 : 3;
+  f[fDone] = (f[fStatus] != 0 || beta <= tol * bnorm || bnorm == 0.0 || (use_outer && f[fOuter])) ? 1 : 0;
+}
+
+// p = r + beta (p - omega v), ph = D^-1 p
+__global__ void bicg_p_batch_kernel(const Chunk* __restrict__ chunks, const BatchMesh* __restrict__ bm, int pkind,
+                                    const double* __restrict__ dinv, const double* __restrict__ r,
+                                    const double* __restrict__ v, double* __restrict__ p, double* __restrict__ ph,
+                                    const double* __restrict__ dctl, const int* __restrict__ ictl) {
+  const Chunk c = chunks[blockIdx.x];
+  if (ictl[c.mesh * kIc + fDone]) return;
+  const double* d = dctl + c.mesh * kDc;
+  const double beta = (d[sRho] / d[sRhoOld]) * (d[sAlpha] / d[sOmega]);
+  const double om = d[sOmega];
+  const int64_t off = bm[c.mesh].row_off;
+  for (int i = c.lo + threadIdx.x; i < c.hi; i += blockDim.x) {
+    const int64_t k = off + i;
+    const double pi = r[k] + beta * (p[k] - om * v[k]);
+    p[k] = pi;
+    ph[k] = pkind == 1 ? dinv[k] * pi : pi;
+  }
+}
+
+// partials of a.b (and, when `c2` is set, of c2.c2 into the second half)
+__global__ void dot_batch_kernel(const Chunk* __restrict__ chunks, const BatchMesh* __restrict__ bm,
+                                 const double* __restrict__ a, const double* __restrict__ b,
+                                 const double* __restrict__ c2, double* __restrict__ part, int nchunks,
+                                 const int* __restrict__ ictl) {
+  __shared__ double sm[32];
+  const Chunk c = chunks[blockIdx.x];
+  if (ictl[c.mesh * kIc + fDone]) return;
+  const int64_t off = bm[c.mesh].row_off;
+  double s = 0.0, t = 0.0;
+  for (int i = c.lo + threadIdx.x; i < c.hi; i += blockDim.x) {
+    const int64_t k = off + i;
+    s += a[k] * b[k];
+    if (c2) t += c2[k] * c2[k];
+  }
+  s = block_sum(s, sm);
+  if (c2) t = block_sum(t, sm);
+  if (threadIdx.x == 0) {
+    part[blockIdx.x] = s;
+    part[nchunks + blockIdx.x] = t;
+  }
+}
+
+__global__ void bicg_alpha_batch_kernel(int nmesh, const int* __restrict__ cprefix, const double* __restrict__ part,
+                                        int nchunks, double* __restrict__ dctl, int* __restrict__ ictl) {
+  const int m = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  if (m >= nmesh || ictl[m * kIc + fDone]) return;
+  double hv, unused;
+  fold2(part, nchunks, cprefix[m], cprefix[m + 1], hv, unused);
+  if ((threadIdx.x & 31) != 0) return;
+  double* d = dctl + m * kDc;
+  int* f = ictl + m * kIc;
+  if (hv == 0.0 || !isfinite(hv)) {
+    f[fDone] = 1;
+    f[fStatus] = isfinite(hv) ? 2 : 3;
+    return;
+  }
+  const double a = d[sRho] / hv;
+  if (!(fabs(a) < 1e150)) {
+    f[fDone] = 1;
+    f[fStatus] = 2;
+    return;
+  }
+  d[sAlpha] = a;
+}
+
+// s = r - alpha v, sh = D^-1 s
+__global__ void bicg_s_batch_kernel(const Chunk* __restrict__ chunks, const BatchMesh* __restrict__ bm, int pkind,
+                                    const double* __restrict__ dinv, const double* __restrict__ r,
+                                    const double* __restrict__ v, double* __restrict__ s, double* __restrict__ sh,
+                                    const double* __restrict__ dctl, const int* __restrict__ ictl) {
+  const Chunk c = chunks[blockIdx.x];
+  if (ictl[c.mesh * kIc + fDone]) return;
+  const double al = dctl[c.mesh * kDc + sAlpha];
+  const int64_t off = bm[c.mesh].row_off;
+  for (int i = c.lo + threadIdx.x; i < c.hi; i += blockDim.x) {
+    const int64_t k = off + i;
+    const double si = r[k] - al * v[k];
+    s[k] = si;
+    sh[k] = pkind == 1 ? dinv[k] * si : si;
+  }
+}
+
+__global__ void bicg_omega_batch_kernel(int nmesh, const int* __restrict__ cprefix, const double* __restrict__ part,
+                                        int nchunks, double* __restrict__ dctl, int* __restrict__ ictl) {
+  const int m = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  if (m >= nmesh || ictl[m * kIc + fDone]) return;
+  double ts, tt;
+  fold2(part, nchunks, cprefix[m], cprefix[m + 1], ts, tt);
+  if ((threadIdx.x & 31) != 0) return;
+  double* d = dctl + m * kDc;
+  int* f = ictl + m * kIc;
+  const double om = (tt != 0.0) ? ts / tt : 0.0;
+  d[sTS] = ts;
+  d[sTT] = tt;
+  d[sOmega] = om;
+  if (!isfinite(om)) {
+    f[fDone] = 1;
+    f[fStatus] = 3;
+  } else if (om == 0.0 && tt != 0.0) {
+    f[fStatus] = 2;  // breakdown: x still advances by alpha ph, then the solve stops
+  }
+}
+
+// x += alpha ph + omega sh ; r = s - omega t ; partials of r.r and rh.r
+template <int XL>
+__global__ void bicg_xr_batch_kernel(const Chunk* __restrict__ chunks, const BatchMesh* __restrict__ bm,
+                                     const double* __restrict__ ph, const double* __restrict__ sh,
+                                     const double* __restrict__ s, const double* __restrict__ t,
+                                     const double* __restrict__ rh, double* xwork, double* __restrict__ r,
+                                     const double* __restrict__ dctl, const int* __restrict__ ictl,
+                                     double* __restrict__ part, int nchunks) {
+  __shared__ double sm[32];
+  const Chunk c = chunks[blockIdx.x];
+  if (ictl[c.mesh * kIc + fDone]) return;
+  const BatchMesh& M = bm[c.mesh];
+  const double al = dctl[c.mesh * kDc + sAlpha], om = dctl[c.mesh * kDc + sOmega];
+  const int64_t off = M.row_off;
+  double* x = vec<XL>(M, xwork);
+  double rr = 0.0, hr = 0.0;
+  for (int i = c.lo + threadIdx.x; i < c.hi; i += blockDim.x) {
+    const int64_t k = off + i;
+    x[i] = x[i] + al * ph[k] + om * sh[k];
+    const double ri = s[k] - om * t[k];
+    r[k] = ri;
+    rr += ri * ri;
+    hr += rh[k] * ri;
+  }
+  rr = block_sum(rr, sm);
+  hr = block_sum(hr, sm);
+  if (threadIdx.x == 0) {
+    part[blockIdx.x] = rr;
+    part[nchunks + blockIdx.x] = hr;
+  }
+}
+
+__global__ void bicg_end_batch_kernel(int nmesh, const int* __restrict__ cprefix, const double* __restrict__ part,
+                                      int nchunks, double* __restrict__ dctl, int* __restrict__ ictl) {
+  const int m = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  if (m >= nmesh || ictl[m * kIc + fDone]) return;
+  double nn, rho_new;
+  fold2(part, nchunks, cprefix[m], cprefix[m + 1], nn, rho_new);
+  if ((threadIdx.x & 31) != 0) return;
+  double* d = dctl + m * kDc;
+  int* f = ictl + m * kIc;
+  const double rn = sqrt(nn);
+  d[sEst] = rn;
+  d[sRhoOld] = d[sRho];
+  d[sRho] = rho_new;
+  f[fIters] += 1;
+  if (f[fStatus] == 2) {
+    f[fDone] = 1;
+  } else if (!isfinite(rn) || !isfinite(rho_new)) {
+    f[fDone] = 1;
+    f[fStatus] = 3;
+  } else if (rn <= d[sTol] * d[sBnorm]) {
+    f[fDone] = 1;
+  } else if (rho_new == 0.0) {
+    f[fDone] = 1;
+    f[fStatus] = 2;
+  } else if (f[fIters] >= f[fMaxit]) {
+    f[fDone] = 1;
+    f[fStatus] = 1;
+  }
+}
+
+// True residual of the finished solve: relres = ||b - A x|| / ||b|| into dctl[sTrue].
+__global__ void true_res_batch_kernel(int nmesh, const int* __restrict__ cprefix, const double* __restrict__ part,
+                                      int nchunks, double* __restrict__ dctl) {
+  const int m = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  if (m >= nmesh) return;
+  double rr, bb;
+  fold2(part, nchunks, cprefix[m], cprefix[m + 1], rr, bb);
+  if ((threadIdx.x & 31) != 0) return;
+  const double bn = sqrt(bb);
+  dctl[m * kDc + sTrue] = bn > 0.0 ? sqrt(rr) / bn : (isfinite(rr) ? 0.0 : NAN);
+  dctl[m * kDc + sBnorm] = bn;
+}
+
+// Outer refinement bookkeeping: meshes whose FP64 residual meets `tol` (or is
+// not finite) are marked done for the rest of the refinement loop.
+__global__ void outer_mark_kernel(int nmesh, const double* __restrict__ dctl, int* __restrict__ ictl, double tol) {
+  const int m = blockIdx.x * blockDim.x + threadIdx.x;
+  if (m >= nmesh) return;
+  const double rr = dctl[m * kDc + sTrue];
+  if (!(rr > tol) || !isfinite(rr)) ictl[m * kIc + fOuter] = 1;
+}
+
+// sol += corr for meshes still refining; corr = 0, res = r for the next pass.
+__global__ void add_corr_batch_kernel(const Chunk* __restrict__ chunks, const BatchMesh* __restrict__ bm,
+                                      double* __restrict__ corr, const int* __restrict__ outer_flags) {
+  const Chunk c = chunks[blockIdx.x];
+  if (outer_flags[c.mesh * kIc + fOuter]) return;
+  const BatchMesh& M = bm[c.mesh];
+  for (int i = c.lo + threadIdx.x; i < c.hi; i += blockDim.x) {
+    M.sol[i] += corr[M.row_off + i];
+    corr[M.row_off + i] = 0.0;
+  }
+}
+
+// x = 0 where b = 0 (the solution of A x = 0), as the one-mesh solver does.
+template <int XL>
+__global__ void zero_x_if_b0_kernel(const Chunk* __restrict__ chunks, const BatchMesh* __restrict__ bm,
+                                    double* xwork, const double* __restrict__ dctl, const int* __restrict__ ictl,
+                                    int use_outer) {
+  const Chunk c = chunks[blockIdx.x];
+  if (dctl[c.mesh * kDc + sBnorm] != 0.0 || (use_outer && ictl[c.mesh * kIc + fOuter])) return;
+  double* x = vec<XL>(bm[c.mesh], xwork);
+  for (int i = c.lo + threadIdx.x; i < c.hi; i += blockDim.x) x[i] = 0.0;
+}
+
+__global__ void zero_batch_kernel(const Chunk* __restrict__ chunks, const BatchMesh* __restrict__ bm,
+                                  double* __restrict__ a, double* __restrict__ b) {
+  const Chunk c = chunks[blockIdx.x];
+  const int64_t off = bm[c.mesh].row_off;
+  for (int i = c.lo + threadIdx.x; i < c.hi; i += blockDim.x) {
+    a[off + i] = 0.0;
+    if (b) b[off + i] = 0.0;
+  }
+}
+
+template <typename T>
+int dmal(T** p, size_t n) {
+  const cudaError_t e = cudaMalloc(reinterpret_cast<void**>(p), std::max<size_t>(n, 1) * sizeof(T));
+  if (e != cudaSuccess) {
+    *p = nullptr;
+    return set_error(UFEM_ERR_NOMEM, std::string("batch cudaMalloc: ") + cudaGetErrorString(e));
+  }
+  return UFEM_OK;
+}
+template <typename T>
+void dfr(T*& p) {
+  if (p) cudaFree(p);
+  p = nullptr;
+}
+
+}  // namespace
+}  // namespace ufem
+
+using namespace ufem;
+
+struct ufem_batch {
+  std::vector<ufem_ns_handle*> members;
+  int dim = 0, neq = 0, precision = 0, spec = 0, warps = 4;
+  int nmesh = 0;
+  int64_t total_nodes = 0, total_rows = 0, total_bc = 0, total_fix = 0;
+  int ngroups = 0, nchunks = 0;
+  bool graphs = true;
+  // device
+  AsmDesc* d_asm = nullptr;
+  int* d_gprefix = nullptr;
+  BatchMesh* d_mesh = nullptr;
+  int64_t* d_node_prefix = nullptr;
+  int64_t* d_bc_prefix = nullptr;
+  int64_t* d_fix_prefix = nullptr;
+  Chunk* d_chunks = nullptr;
+  int* d_cprefix = nullptr;
+  double *r = nullptr, *rh = nullptr, *p = nullptr, *v = nullptr, *s = nullptr, *t = nullptr, *ph = nullptr,
+         *sh = nullptr, *dinv = nullptr, *w = nullptr, *res = nullptr, *corr = nullptr;
+  double* part = nullptr;
+  double* dctl = nullptr;
+  int* ictl = nullptr;
+  double* h_dctl = nullptr;
+  int* h_ictl = nullptr;
+  // captured iteration blocks: [mixed]
+  cudaGraphExec_t block_exec[2] = {nullptr, nullptr};
+  cudaStream_t capture_stream = nullptr;
+  int block_pkind[2] = {-1, -1};
+};
+
+namespace {
+
+void batch_free(ufem_batch* b) {
+  for (auto& g : b->block_exec)
+    if (g) cudaGraphExecDestroy(g);
+  if (b->capture_stream) cudaStreamDestroy(b->capture_stream);
+  dfr(b->d_asm); dfr(b->d_gprefix); dfr(b->d_mesh); dfr(b->d_node_prefix); dfr(b->d_bc_prefix);
+  dfr(b->d_fix_prefix); dfr(b->d_chunks); dfr(b->d_cprefix);
+  dfr(b->r); dfr(b->rh); dfr(b->p); dfr(b->v); dfr(b->s); dfr(b->t); dfr(b->ph); dfr(b->sh); dfr(b->dinv);
+  dfr(b->w); dfr(b->res); dfr(b->corr); dfr(b->part); dfr(b->dctl); dfr(b->ictl);
+  if (b->h_dctl) cudaFreeHost(b->h_dctl);
+  if (b->h_ictl) cudaFreeHost(b->h_ictl);
+  delete b;
+}
+
+// (Re)build the member descriptors: Dirichlet plans and pointers may change
+// between steps (new BC lists, FP32 buffers allocated on option changes).
+int batch_refresh(ufem_batch* b) {
+  int rc;
+  std::vector<AsmDesc> ad(b->nmesh);
+  std::vector<BatchMesh> bm(b->nmesh);
+  std::vector<int64_t> bcp(b->nmesh + 1, 0), fxp(b->nmesh + 1, 0);
+  for (int m = 0; m < b->nmesh; ++m) {
+    ufem_ns_handle* h = b->members[m];
+    if (h->bcp.dirty && (rc = build_bc_plan(h))) return rc;
+    fill_desc(h, h->d_vals32 != nullptr, ad[m]);
+    BatchMesh& M = bm[m];
+    M.N = h->N;
+    M.nrows = h->nrows;
+    M.dim = h->dim;
+    M.neq = h->neq;
+    M.state = h->d_state;
+    M.hist = h->d_hist;
+    M.nu = h->d_nu;
+    M.uadv = h->d_uadv;
+    M.node32 = h->opt.precision == 1 ? h->d_node32 : nullptr;
+    M.start = h->d_start;
+    M.adj = h->d_adj;
+    M.diagpos = h->d_diagpos;
+    M.rowptr = h->d_rowptr;
+    M.vals = h->d_vals;
+    M.vals32 = h->d_vals32;
+    M.rhs = h->d_rhs;
+    M.sol = h->d_sol;
+    const DirichletPlan& P = h->bcp;
+    M.nbc = P.nbc;
+    M.nfix_rows = P.nfix_rows;
+    M.bc_dof = P.bc_dof;
+    M.bc_first = P.bc_first;
+    M.bc_last = P.bc_last;
+    M.bc_diag = P.bc_diag;
+    M.vfirst = P.vfirst;
+    M.fix_row = P.fix_row;
+    M.fix_ptr = P.fix_ptr;
+    M.fix_pos = P.fix_pos;
+    M.fix_bc = P.fix_bc;
+    bcp[m + 1] = bcp[m] + P.nbc;
+    fxp[m + 1] = fxp[m] + P.nfix_rows;
+  }
+  int64_t off = 0;
+  for (int m = 0; m < b->nmesh; ++m) {
+    bm[m].row_off = off;
+    off += bm[m].nrows;
+  }
+  b->total_bc = bcp[b->nmesh];
+  b->total_fix = fxp[b->nmesh];
+  UFEM_CUDA_TRY(cudaMemcpy(b->d_asm, ad.data(), ad.size() * sizeof(AsmDesc), cudaMemcpyHostToDevice));
+  UFEM_CUDA_TRY(cudaMemcpy(b->d_mesh, bm.data(), bm.size() * sizeof(BatchMesh), cudaMemcpyHostToDevice));
+  UFEM_CUDA_TRY(cudaMemcpy(b->d_bc_prefix, bcp.data(), bcp.size() * 8, cudaMemcpyHostToDevice));
+  UFEM_CUDA_TRY(cudaMemcpy(b->d_fix_prefix, fxp.data(), fxp.size() * 8, cudaMemcpyHostToDevice));
+  return UFEM_OK;
+}
+
+bool batch_dirty(const ufem_batch* b) {
+  for (const ufem_ns_handle* h : b->members)
+    if (h->bcp.dirty) return true;
+  return false;
+}
+
+inline unsigned blocks_for(int64_t n, int threads) { return unsigned((n + threads - 1) / threads); }
+
+template <typename MT, int XL>
+int spmv_b(ufem_batch* b, double* x, double* y, cudaStream_t st) {
+  const unsigned grid = blocks_for(b->total_nodes * 32, 256);
+  if (b->neq == 4)
+    spmv_batch_kernel<4, MT, XL><<<grid, 256, 0, st>>>(b->total_nodes, b->nmesh, b->d_node_prefix, b->d_mesh, x, y,
+                                                       b->ictl);
+  else
+    spmv_batch_kernel<3, MT, XL><<<grid, 256, 0, st>>>(b->total_nodes, b->nmesh, b->d_node_prefix, b->d_mesh, x, y,
+                                                       b->ictl);
+  UFEM_CUDA_TRY(cudaGetLastError());
+  return UFEM_OK;
+}
+
+// One BiCGStab iteration for every member that is not done.
+template <typename MT, int XL>
+int bicg_iteration(ufem_batch* b, int pkind, double* xwork, cudaStream_t st) {
+  const unsigned nc = unsigned(b->nchunks);
+  const unsigned gm = blocks_for(int64_t(b->nmesh) * 32, 256);
+  int rc;
+  bicg_p_batch_kernel<<<nc, kThreads, 0, st>>>(b->d_chunks, b->d_mesh, pkind, b->dinv, b->r, b->v, b->p, b->ph,
+                                                b->dctl, b->ictl);
+  if ((rc = spmv_b<MT, kWork>(b, b->ph, b->v, st))) return rc;
+  dot_batch_kernel<<<nc, kThreads, 0, st>>>(b->d_chunks, b->d_mesh, b->rh, b->v, nullptr, b->part, b->nchunks,
+                                             b->ictl);
+  bicg_alpha_batch_kernel<<<gm, 256, 0, st>>>(b->nmesh, b->d_cprefix, b->part, b->nchunks, b->dctl, b->ictl);
+  bicg_s_batch_kernel<<<nc, kThreads, 0, st>>>(b->d_chunks, b->d_mesh, pkind, b->dinv, b->r, b->v, b->s, b->sh,
+                                                b->dctl, b->ictl);
+  if ((rc = spmv_b<MT, kWork>(b, b->sh, b->t, st))) return rc;
+  dot_batch_kernel<<<nc, kThreads, 0, st>>>(b->d_chunks, b->d_mesh, b->t, b->s, b->t, b->part, b->nchunks, b->ictl);
+  bicg_omega_batch_kernel<<<gm, 256, 0, st>>>(b->nmesh, b->d_cprefix, b->part, b->nchunks, b->dctl, b->ictl);
+  bicg_xr_batch_kernel<XL><<<nc, kThreads, 0, st>>>(b->d_chunks, b->d_mesh, b->ph, b->sh, b->s, b->t, b->rh, xwork,
+                                                     b->r, b->dctl, b->ictl, b->part, b->nchunks);
+  bicg_end_batch_kernel<<<gm, 256, 0, st>>>(b->nmesh, b->d_cprefix, b->part, b->nchunks, b->dctl, b->ictl);
+  UFEM_CUDA_TRY(cudaGetLastError());
+  return UFEM_OK;
+}
+
+// r = b - A x with partials; XL / BL: where x and b live.
+template <typename MT, int XL, int BL>
+int residual_b(ufem_batch* b, double* x, double* bw, bool init_rh, bool skip_done, cudaStream_t st) {
+  int rc;
+  if ((rc = spmv_b<MT, XL>(b, x, b->w, st))) return rc;
+  residual_batch_kernel<BL><<<unsigned(b->nchunks), kThreads, 0, st>>>(
+      b->d_chunks, b->d_mesh, bw, b->w, b->r, init_rh ? b->rh : nullptr, b->part, b->nchunks, b->ictl,
+      skip_done ? 1 : 0);
+  UFEM_CUDA_TRY(cudaGetLastError());
+  return UFEM_OK;
+}
+
+// BiCGStab over the batch.  MT: operator values; XL/BL: solution and RHS
+// locations; `use_outer`: skip meshes already converged in refinement.
+template <typename MT, int XL, int BL>
+int bicgstab_b(ufem_batch* b, int pkind, double tol, int maxit, bool use_outer, int slot, cudaStream_t st) {
+  const unsigned nc = unsigned(b->nchunks);
+  const unsigned gm = blocks_for(int64_t(b->nmesh) * 32, 256);
+  int rc;
+  double* xw = XL == kWork ? b->corr : nullptr;
+  double* bw = BL == kWork ? b->res : nullptr;
+  // every mesh takes part in the set-up (flags are reset by the init kernel)
+  if (use_outer)  // flags prepared by the caller in the host mirror: fOuter set, the rest zero
+    UFEM_CUDA_TRY(cudaMemcpyAsync(b->ictl, b->h_ictl, sizeof(int) * kIc * b->nmesh, cudaMemcpyHostToDevice, st));
+  else
+    UFEM_CUDA_TRY(cudaMemsetAsync(b->ictl, 0, sizeof(int) * kIc * b->nmesh, st));
+  if (pkind == 1) jacobi_batch_kernel<MT><<<nc, kThreads, 0, st>>>(b->d_chunks, b->d_mesh, b->dinv, b->ictl);
+  if ((rc = residual_b<MT, XL, BL>(b, xw, bw, true, false, st))) return rc;
+  zero_batch_kernel<<<nc, kThreads, 0, st>>>(b->d_chunks, b->d_mesh, b->p, b->v);
+  bicg_init_batch_kernel<<<gm, 256, 0, st>>>(b->nmesh, b->d_cprefix, b->part, b->nchunks, b->dctl, b->ictl, tol,
+                                             maxit, use_outer ? 1 : 0);
+  zero_x_if_b0_kernel<XL><<<nc, kThreads, 0, st>>>(b->d_chunks, b->d_mesh, xw, b->dctl, b->ictl, use_outer ? 1 : 0);
+  UFEM_CUDA_TRY(cudaGetLastError());
+  const bool use_graph = b->graphs;
+  if (use_graph && (b->block_exec[slot] == nullptr || b->block_pkind[slot] != pkind)) {
+    if (b->block_exec[slot]) {
+      cudaGraphExecDestroy(b->block_exec[slot]);
+      b->block_exec[slot] = nullptr;
+    }
+    cudaGraph_t g = nullptr;
+    UFEM_CUDA_TRY(cudaStreamBeginCapture(b->capture_stream, cudaStreamCaptureModeThreadLocal));
+    int crc = UFEM_OK;
+    for (int k = 0; k < kBlockIters && crc == UFEM_OK; ++k) crc = bicg_iteration<MT, XL>(b, pkind, xw, b->capture_stream);
+    const cudaError_t ce = cudaStreamEndCapture(b->capture_stream, &g);
+    if (crc) {
+      if (g) cudaGraphDestroy(g);
+      return crc;
+    }
+    if (ce != cudaSuccess) return set_error(UFEM_ERR_CUDA, std::string("graph capture: ") + cudaGetErrorString(ce));
+    const cudaError_t ie = cudaGraphInstantiate(&b->block_exec[slot], g, 0);
+    cudaGraphDestroy(g);
+    if (ie != cudaSuccess) return set_error(UFEM_ERR_CUDA, std::string("graph instantiate: ") + cudaGetErrorString(ie));
+    b->block_pkind[slot] = pkind;
+  }
+  for (int it = 0; it < maxit; it += kBlockIters) {
+    if (use_graph) {
+      UFEM_CUDA_TRY(cudaGraphLaunch(b->block_exec[slot], st));
+    } else {
+      for (int k = 0; k < kBlockIters; ++k)
+        if ((rc = bicg_iteration<MT, XL>(b, pkind, xw, st))) return rc;
+    }
+    UFEM_CUDA_TRY(cudaMemcpyAsync(b->h_ictl, b->ictl, sizeof(int) * kIc * b->nmesh, cudaMemcpyDeviceToHost, st));
+    UFEM_CUDA_TRY(cudaStreamSynchronize(st));
+    bool all = true;
+    for (int m = 0; m < b->nmesh && all; ++m) all = b->h_ictl[m * kIc + fDone] != 0;
+    if (all) break;
+  }
+  return UFEM_OK;
+}
+
+// FP64 true residual of every member's current solution into dctl[sTrue].
+int true_residual_b(ufem_batch* b, cudaStream_t st) {
+  int rc;
+  UFEM_CUDA_TRY(cudaMemsetAsync(b->ictl, 0, sizeof(int) * kIc * b->nmesh, st));
+  if ((rc = residual_b<double, kSol, kRhs>(b, nullptr, nullptr, false, false, st))) return rc;
+  true_res_batch_kernel<<<blocks_for(int64_t(b->nmesh) * 32, 256), 256, 0, st>>>(b->nmesh, b->d_cprefix, b->part,
+                                                                                 b->nchunks, b->dctl);
+  UFEM_CUDA_TRY(cudaGetLastError());
+  return UFEM_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int ufem_batch_create(ufem_ns_handle* const* members, int32_t n, ufem_batch** out) {
+  if (!members || !out || n < 1) return set_error(UFEM_ERR_ARG, "ufem_batch_create: members, n >= 1 and out required");
+  *out = nullptr;
+  for (int32_t m = 0; m < n; ++m) {
+    const ufem_ns_handle* h = members[m];
+    if (!h) return set_error(UFEM_ERR_ARG, "ufem_batch_create: NULL member");
+    if (!h->state_set) return set_error(UFEM_ERR_STATE, "ufem_batch_create: every member needs its state set");
+    if (h->dim != members[0]->dim || h->opt.precision != members[0]->opt.precision ||
+        h->opt.use_specializations != members[0]->opt.use_specializations)
+      return set_error(UFEM_ERR_ARG, "ufem_batch_create: members must share dim, precision and element form");
+    for (int32_t q = 0; q < m; ++q)
+      if (members[q] == h) return set_error(UFEM_ERR_ARG, "ufem_batch_create: a handle appears twice");
+  }
+  ufem_batch* b = new ufem_batch();
+  b->members.assign(members, members + n);
+  b->nmesh = n;
+  b->dim = members[0]->dim;
+  b->neq = members[0]->neq;
+  b->precision = members[0]->opt.precision;
+  b->spec = members[0]->opt.use_specializations;
+  b->warps = members[0]->asm_warps;
+  std::vector<int> gprefix(n + 1, 0);
+  std::vector<int64_t> nprefix(n + 1, 0);
+  std::vector<Chunk> chunks;
+  std::vector<int> cprefix(n + 1, 0);
+  for (int m = 0; m < n; ++m) {
+    const ufem_ns_handle* h = members[m];
+    gprefix[m + 1] = gprefix[m] + h->wplan.ngroups;
+    nprefix[m + 1] = nprefix[m] + h->N;
+    for (int64_t lo = 0; lo < h->nrows; lo += kChunkRows)
+      chunks.push_back(Chunk{m, int(lo), int(std::min<int64_t>(h->nrows, lo + kChunkRows)), 0});
+    cprefix[m + 1] = int(chunks.size());
+    b->total_rows += h->nrows;
+  }
+  b->total_nodes = nprefix[n];
+  b->ngroups = gprefix[n];
+  b->nchunks = int(chunks.size());
+  const size_t R = size_t(b->total_rows);
+  int rc;
+  if ((rc = dmal(&b->d_asm, n)) || (rc = dmal(&b->d_gprefix, n + 1)) || (rc = dmal(&b->d_mesh, n)) ||
+      (rc = dmal(&b->d_node_prefix, n + 1)) || (rc = dmal(&b->d_bc_prefix, n + 1)) ||
+      (rc = dmal(&b->d_fix_prefix, n + 1)) || (rc = dmal(&b->d_chunks, chunks.size())) ||
+      (rc = dmal(&b->d_cprefix, n + 1)) || (rc = dmal(&b->r, R)) || (rc = dmal(&b->rh, R)) ||
+      (rc = dmal(&b->p, R)) || (rc = dmal(&b->v, R)) || (rc = dmal(&b->s, R)) || (rc = dmal(&b->t, R)) ||
+      (rc = dmal(&b->ph, R)) || (rc = dmal(&b->sh, R)) || (rc = dmal(&b->dinv, R)) || (rc = dmal(&b->w, R)) ||
+      (rc = dmal(&b->part, 2 * chunks.size())) || (rc = dmal(&b->dctl, size_t(kDc) * n)) ||
+      (rc = dmal(&b->ictl, size_t(kIc) * n))) {
+    batch_free(b);
+    return rc;
+  }
+  if (b->precision == 1 && ((rc = dmal(&b->res, R)) || (rc = dmal(&b->corr, R)))) {
+    batch_free(b);
+    return rc;
+  }
+  cudaError_t ce;
+  if ((ce = cudaMallocHost(reinterpret_cast<void**>(&b->h_dctl), sizeof(double) * kDc * n)) != cudaSuccess ||
+      (ce = cudaMallocHost(reinterpret_cast<void**>(&b->h_ictl), sizeof(int) * kIc * n)) != cudaSuccess ||
+      (ce = cudaStreamCreateWithFlags(&b->capture_stream, cudaStreamNonBlocking)) != cudaSuccess ||
+      (ce = cudaMemcpy(b->d_gprefix, gprefix.data(), gprefix.size() * 4, cudaMemcpyHostToDevice)) != cudaSuccess ||
+      (ce = cudaMemcpy(b->d_node_prefix, nprefix.data(), nprefix.size() * 8, cudaMemcpyHostToDevice)) !=
+          cudaSuccess ||
+      (ce = cudaMemcpy(b->d_chunks, chunks.data(), chunks.size() * sizeof(Chunk), cudaMemcpyHostToDevice)) !=
+          cudaSuccess ||
+      (ce = cudaMemcpy(b->d_cprefix, cprefix.data(), cprefix.size() * 4, cudaMemcpyHostToDevice)) != cudaSuccess) {
+    batch_free(b);
+    return set_error(UFEM_ERR_CUDA, std::string("ufem_batch_create: ") + cudaGetErrorString(ce));
+  }
+  if ((rc = batch_refresh(b))) {
+    batch_free(b);
+    return rc;
+  }
+  *out = b;
+  return UFEM_OK;
+}
+
+int ufem_batch_size(const ufem_batch* b, int32_t* n, int64_t* rows) {
+  if (!b) return set_error(UFEM_ERR_ARG, "NULL batch");
+  if (n) *n = b->nmesh;
+  if (rows) *rows = b->total_rows;
+  return UFEM_OK;
+}
+
+int ufem_batch_set_graphs(ufem_batch* b, int32_t enable) {
+  if (!b) return set_error(UFEM_ERR_ARG, "NULL batch");
+  b->graphs = enable != 0;
+  return UFEM_OK;
+}
+
+int ufem_batch_set_assembly_warps(ufem_batch* b, int32_t warps_per_cta) {
+  if (!b) return set_error(UFEM_ERR_ARG, "NULL batch");
+  if (warps_per_cta != 2 && warps_per_cta != 4 && warps_per_cta != 8)
+    return set_error(UFEM_ERR_ARG, "warps_per_cta must be 2, 4 or 8");
+  b->warps = warps_per_cta;
+  return UFEM_OK;
+}
+
+int ufem_batch_assemble(ufem_batch* b, void* stream) {
+  if (!b) return set_error(UFEM_ERR_ARG, "NULL batch");
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  int rc;
+  if (batch_dirty(b)) {
+    UFEM_CUDA_TRY(cudaStreamSynchronize(st));
+    if ((rc = batch_refresh(b))) return rc;
+  }
+  linearize_batch_kernel<<<blocks_for(b->total_nodes, 256), 256, 0, st>>>(b->total_nodes, b->nmesh,
+                                                                          b->d_node_prefix, b->d_mesh);
+  UFEM_CUDA_TRY(cudaGetLastError());
+  if ((rc = launch_assembly_batch(b->dim, b->precision, b->spec != 0, b->warps, b->ngroups, b->nmesh, b->d_asm,
+                                  b->d_gprefix, st)))
+    return rc;
+  for (ufem_ns_handle* h : b->members) {  // rows with more than 32 elements (none on most meshes)
+    h->vals32_valid = h->d_vals32 != nullptr;
+    const AssemblyPlan& big = h->opt.precision == 1 ? h->wplan.big32 : h->wplan.big64;
+    if (big.nchunks > 0 && (rc = launch_assembly_big_rows(h, st, h->d_vals32 != nullptr))) return rc;
+  }
+  if (b->total_bc > 0) {
+    dirichlet_values_batch_kernel<<<blocks_for(b->total_bc, 256), 256, 0, st>>>(b->total_bc, b->nmesh,
+                                                                                 b->d_bc_prefix, b->d_mesh);
+    if (b->total_fix > 0)
+      dirichlet_columns_batch_kernel<<<blocks_for(b->total_fix, 128), 128, 0, st>>>(b->total_fix, b->nmesh,
+                                                                                    b->d_fix_prefix, b->d_mesh);
+    dirichlet_rows_batch_kernel<<<unsigned(b->total_bc), 64, 0, st>>>(b->nmesh, b->d_bc_prefix, b->d_mesh);
+    UFEM_CUDA_TRY(cudaGetLastError());
+  }
+  return UFEM_OK;
+}
+
+int ufem_batch_solve(ufem_batch* b, const ufem_krylov_opts* kopts, ufem_krylov_status* statuses, void* stream) {
+  if (!b) return set_error(UFEM_ERR_ARG, "NULL batch");
+  ufem_krylov_opts o;
+  ufem_krylov_default_opts(&o);
+  if (kopts) o = *kopts;
+  if (o.method != 1) return set_error(UFEM_ERR_ARG, "the batched solve is BiCGStab (method 1)");
+  if (o.precond != 0 && o.precond != 1) return set_error(UFEM_ERR_ARG, "the batched solve supports precond 0 or 1");
+  if (o.max_iters <= 0) o.max_iters = 3000;
+  if (o.tol <= 0) o.tol = 1e-10;
+  if (o.max_refine <= 0) o.max_refine = 20;
+  if (o.inner_tol <= 0) o.inner_tol = 1e-3;
+  const bool mixed = o.mixed != 0;
+  if (mixed && b->precision != 1)
+    return set_error(UFEM_ERR_ARG, "a mixed batched solve needs FP32-element members (precision 1)");
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  int rc;
+  std::vector<int> iters(b->nmesh, 0), status(b->nmesh, 0), refines(b->nmesh, 0);
+  if (!mixed) {
+    if ((rc = bicgstab_b<double, kSol, kRhs>(b, o.precond, o.tol, o.max_iters, false, 0, st))) return rc;
+    UFEM_CUDA_TRY(cudaMemcpyAsync(b->h_ictl, b->ictl, sizeof(int) * kIc * b->nmesh, cudaMemcpyDeviceToHost, st));
+    UFEM_CUDA_TRY(cudaStreamSynchronize(st));
+    for (int m = 0; m < b->nmesh; ++m) {
+      iters[m] = b->h_ictl[m * kIc + fIters];
+      status[m] = b->h_ictl[m * kIc + fStatus];
+    }
+  } else {
+    // FP64 refinement: r = b - A64 x; inner BiCGStab on A32 d = r (FP64
+    // vectors and scalars), x += d; meshes leave the loop once converged.
+    std::vector<int> outer(b->nmesh, 0);
+    const int inner_cap = std::min(o.max_iters, 400);
+    for (int ref = 0; ref <= o.max_refine; ++ref) {
+      if ((rc = true_residual_b(b, st))) return rc;
+      outer_mark_kernel<<<blocks_for(b->nmesh, 128), 128, 0, st>>>(b->nmesh, b->dctl, b->ictl, o.tol);
+      UFEM_CUDA_TRY(cudaGetLastError());
+      UFEM_CUDA_TRY(cudaMemcpyAsync(b->h_ictl, b->ictl, sizeof(int) * kIc * b->nmesh, cudaMemcpyDeviceToHost, st));
+      UFEM_CUDA_TRY(cudaStreamSynchronize(st));
+      bool all = true;
+      for (int m = 0; m < b->nmesh; ++m) {
+        outer[m] = outer[m] || b->h_ictl[m * kIc + fOuter];
+        all = all && outer[m];
+      }
+      if (all || ref == o.max_refine) break;
+      // res = r (the residual just formed), corr = 0; inner solve on the rest
+      UFEM_CUDA_TRY(cudaMemcpyAsync(b->res, b->r, sizeof(double) * b->total_rows, cudaMemcpyDeviceToDevice, st));
+      zero_batch_kernel<<<unsigned(b->nchunks), kThreads, 0, st>>>(b->d_chunks, b->d_mesh, b->corr, nullptr);
+      for (int m = 0; m < b->nmesh; ++m) {
+        for (int q = 0; q < kIc; ++q) b->h_ictl[m * kIc + q] = 0;
+        b->h_ictl[m * kIc + fOuter] = outer[m];
+      }
+      if ((rc = bicgstab_b<float, kWork, kWork>(b, o.precond, o.inner_tol, inner_cap, true, 1, st))) return rc;
+      UFEM_CUDA_TRY(cudaMemcpyAsync(b->h_ictl, b->ictl, sizeof(int) * kIc * b->nmesh, cudaMemcpyDeviceToHost, st));
+      UFEM_CUDA_TRY(cudaStreamSynchronize(st));
+      for (int m = 0; m < b->nmesh; ++m) {
+        if (outer[m]) continue;
+        iters[m] += b->h_ictl[m * kIc + fIters];
+        refines[m] = ref + 1;
+        if (b->h_ictl[m * kIc + fStatus] == 3) status[m] = 3;
+      }
+      // apply the corrections (outer flags on the device still hold `outer`)
+      add_corr_batch_kernel<<<unsigned(b->nchunks), kThreads, 0, st>>>(b->d_chunks, b->d_mesh, b->corr, b->ictl);
+      UFEM_CUDA_TRY(cudaGetLastError());
+    }
+  }
+  // final FP64 residuals
+  if ((rc = true_residual_b(b, st))) return rc;
+  UFEM_CUDA_TRY(cudaMemcpyAsync(b->h_dctl, b->dctl, sizeof(double) * kDc * b->nmesh, cudaMemcpyDeviceToHost, st));
+  UFEM_CUDA_TRY(cudaStreamSynchronize(st));
+  if (statuses) {
+    for (int m = 0; m < b->nmesh; ++m) {
+      const double rr = b->h_dctl[m * kDc + sTrue];
+      ufem_krylov_status& s = statuses[m];
+      s.iterations = iters[m];
+      s.refinements = refines[m];
+      s.rel_residual = rr;
+      s.converged = std::isfinite(rr) && rr <= o.tol;
+      s.status = s.converged ? 0 : (status[m] ? status[m] : (std::isfinite(rr) ? 1 : 3));
+    }
+  }
+  return UFEM_OK;
+}
+
+int ufem_batch_update(ufem_batch* b, void* stream) {
+  if (!b) return set_error(UFEM_ERR_ARG, "NULL batch");
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  update_batch_kernel<<<blocks_for(b->total_nodes, 256), 256, 0, st>>>(b->total_nodes, b->nmesh, b->d_node_prefix,
+                                                                       b->d_mesh);
+  UFEM_CUDA_TRY(cudaGetLastError());
+  return UFEM_OK;
+}
+
+int ufem_batch_step(ufem_batch* b, const ufem_krylov_opts* kopts, ufem_krylov_status* statuses, void* stream) {
+  int rc;
+  if ((rc = ufem_batch_assemble(b, stream))) return rc;
+  if ((rc = ufem_batch_solve(b, kopts, statuses, stream))) return rc;
+  return ufem_batch_update(b, stream);
+}
+
+void ufem_batch_destroy(ufem_batch* b) {
+  if (b) batch_free(b);
+}
+
+}  // extern "C"

@@ -128,6 +128,8 @@ inline int64_t row_start(const ufem_ns_handle* h, int64_t node, int r) {
   return int64_t(h->neq) * h->neq * h->start_h[node] + int64_t(r) * S * h->neq;
 }
 
+}  // namespace
+
 // Turn the ordered BC list into the parallel plan.  Final state of the
 // sequential reference (TrilinosFEVbrMatrix.cpp:482-553 applied in order):
 //  - a constrained row is an identity row with rhs = sol = value_last - old;
@@ -211,6 +213,8 @@ int build_bc_plan(ufem_ns_handle* h) {
   return UFEM_OK;
 }
 
+namespace {
+
 void record(ufem_ns_handle* h, int phase, bool stop, cudaStream_t s) {
   if (!h->timing) return;
   cudaEventRecord(h->ev[2 * phase + (stop ? 1 : 0)], s);
@@ -225,7 +229,8 @@ void destroy_impl(ufem_ns_handle* h) {
   dfree(h->d_colidx); dfree(h->d_vals); dfree(h->d_vals32); dfree(h->d_rhs); dfree(h->d_sol);
   dfree(h->d_diagpos); dfree(h->d_row_inc); dfree(h->d_inc_elem); dfree(h->d_inc_info);
   dfree(h->plan64.chunks); dfree(h->plan32.chunks); dfree(h->wplan.groups);
-  dfree(h->wplan.big64.chunks); dfree(h->wplan.big32.chunks); dfree(h->d_stage); dfree(h->d_x); dfree(h->d_y);
+  dfree(h->wplan.big64.chunks); dfree(h->wplan.big32.chunks); dfree(h->d_desc); dfree(h->d_gprefix);
+  if (h->h_desc) cudaFreeHost(h->h_desc); dfree(h->d_stage); dfree(h->d_x); dfree(h->d_y);
   for (auto& e : h->ev)
     if (e) cudaEventDestroy(e);
   delete h;
@@ -529,6 +534,7 @@ int ufem_ns_create(const ufem_mesh* mesh, const ufem_ns_options* opts, ufem_ns_h
       (rc = dmalloc(&h->plan64.chunks, chunks64.size(), "chunks64")) ||
       (rc = dmalloc(&h->plan32.chunks, chunks32.size(), "chunks32")) ||
       (rc = dmalloc(&h->wplan.groups, std::max<size_t>(groups.size(), 1), "groups")) ||
+      (rc = dmalloc(&h->d_desc, 1, "assembly descriptor")) || (rc = dmalloc(&h->d_gprefix, 2, "group prefix")) ||
       (rc = dmalloc(&h->wplan.big64.chunks, std::max<size_t>(big64.size(), 1), "big64")) ||
       (rc = dmalloc(&h->wplan.big32.chunks, std::max<size_t>(big32.size(), 1), "big32")) ||
       (rc = dmalloc(&h->d_stage, size_t(N) * 4 * dim, "stage")))
@@ -549,6 +555,7 @@ int ufem_ns_create(const ufem_mesh* mesh, const ufem_ns_options* opts, ufem_ns_h
       (ce = up(h->plan64.chunks, chunks64.data(), chunks64.size() * sizeof(int2))) ||
       (ce = up(h->plan32.chunks, chunks32.data(), chunks32.size() * sizeof(int2))) ||
       (ce = up(h->wplan.groups, groups.data(), groups.size() * sizeof(int4))) ||
+      (ce = up(h->d_gprefix, std::vector<int>{0, int(groups.size())}.data(), 2 * sizeof(int))) ||
       (ce = up(h->wplan.big64.chunks, big64.data(), big64.size() * sizeof(int2))) ||
       (ce = up(h->wplan.big32.chunks, big32.data(), big32.size() * sizeof(int2))))
     return fail(set_error(UFEM_ERR_CUDA, std::string("upload: ") + cudaGetErrorString(ce)));
@@ -556,6 +563,8 @@ int ufem_ns_create(const ufem_mesh* mesh, const ufem_ns_options* opts, ufem_ns_h
       (ce = cudaMemset(h->d_hist, 0, size_t(N) * 96)) || (ce = cudaMemset(h->d_uadv, 0, size_t(N) * 32)) ||
       (ce = cudaMemset(h->d_nu, 0, size_t(N) * 8)) || (ce = cudaMemset(h->d_rhs, 0, size_t(h->nrows) * 8)))
     return fail(set_error(UFEM_ERR_CUDA, std::string("memset: ") + cudaGetErrorString(ce)));
+  if ((ce = cudaMallocHost(reinterpret_cast<void**>(&h->h_desc), sizeof(AsmDesc))) != cudaSuccess)
+    return fail(set_error(UFEM_ERR_NOMEM, std::string("cudaMallocHost: ") + cudaGetErrorString(ce)));
   if ((rc = launch_build_csr(h, 0))) return fail(rc);
   if ((ce = cudaDeviceSynchronize()) != cudaSuccess)
     return fail(set_error(UFEM_ERR_CUDA, std::string("CSR build: ") + cudaGetErrorString(ce)));

@@ -50,6 +50,27 @@ struct WarpPlan {
   AssemblyPlan big64, big32;   // rows with more than 32 incidences
 };
 
+// Everything the warp assembly kernel reads or writes for one mesh.  A launch
+// takes an array of these plus a prefix of their group counts, so one
+// persistent launch assembles one mesh (a handle) or many (a batch).
+struct AsmDesc {
+  const double* coords;
+  const double* uadv;
+  const double* state;
+  const float* node32;
+  const double* force;
+  const int64_t* start;
+  const int32_t* row_inc;
+  const int32_t* inc_elem;
+  const uint32_t* inc_info;
+  const int4* conn;
+  const int4* groups;
+  double* vals;
+  float* vals32;  // null: no FP32 copy of the values
+  double* rhs;
+  NSParams p;
+};
+
 // Assembly kernel variants (selected per handle, see ufem_ns_set_assembly_kernel).
 enum AssemblyVariant { kAsmWarp = 0, kAsmChunk = 1 };
 
@@ -117,6 +138,9 @@ struct ufem_ns_handle {
   ufem::AssemblyPlan plan64;       // chunks sized for the FP64-element chunk kernel (all rows)
   ufem::AssemblyPlan plan32;       // chunks sized for the FP32-element chunk kernel (all rows)
   ufem::WarpPlan wplan;            // warp-per-row-group kernel
+  ufem::AsmDesc* d_desc = nullptr; // this handle as a one-mesh assembly batch (device)
+  int* d_gprefix = nullptr;        // {0, wplan.ngroups} (device)
+  ufem::AsmDesc* h_desc = nullptr; // pinned mirror of d_desc
   int asm_variant = ufem::kAsmWarp;
   int asm_warps = 4;               // warps per CTA of the warp kernel
   ufem::DirichletPlan bcp;
@@ -140,10 +164,21 @@ namespace ufem {
 int launch_build_csr(ufem_ns_handle* h, cudaStream_t s);
 int launch_linearize(ufem_ns_handle* h, cudaStream_t s);
 int launch_assembly(ufem_ns_handle* h, cudaStream_t s, bool write32);
+void fill_params(const ufem_ns_handle* h, NSParams& p);
+void fill_desc(const ufem_ns_handle* h, bool write32, AsmDesc& d);
+// Warp assembly of many meshes in one persistent launch (same dim and precision;
+// rows with more than 32 incidences go through each mesh's chunk plan).
+int launch_assembly_batch(int dim, int precision, bool spec, int warps, int ngroups, int nmesh,
+                          const AsmDesc* d_descs, const int* d_gprefix, cudaStream_t s);
 int launch_dirichlet(ufem_ns_handle* h, cudaStream_t s);
 int launch_update(ufem_ns_handle* h, cudaStream_t s);
 int assembly_chunk_capacity(int dim, int precision);
 int configure_kernels();
+
+int launch_assembly_big_rows(ufem_ns_handle* h, cudaStream_t s, bool write32);
+
+// host.cu
+int build_bc_plan(ufem_ns_handle* h);
 
 // Krylov (krylov.cu)
 int krylov_solve(ufem_ns_handle* h, const ufem_krylov_opts* ko, ufem_krylov_status* st, cudaStream_t s);

@@ -268,3 +268,59 @@ class NavierStokes:
 
     def __exit__(self, *exc):
         self.close()
+
+
+class Batch:
+    """Several NavierStokes handles stepped together: each phase of a time step
+    is one launch over all members, and the BiCGStab solve keeps per-member
+    scalars, so a member's results are the same alone and in any batch.
+
+    Members must share dim, precision and element form; they stay owned by the
+    caller (the batch keeps references) and must not be closed while it lives.
+    """
+
+    def __init__(self, members: list, graphs: bool = True, assembly_warps: int | None = None):
+        if not members:
+            raise ValueError("a batch needs at least one member")
+        self._lib = N.lib()
+        self.members = list(members)
+        arr = (C.c_void_p * len(self.members))(*[m.handle for m in self.members])
+        self._b = C.c_void_p()
+        N.check(self._lib.ufem_batch_create(arr, len(self.members), C.byref(self._b)))
+        self.set_graphs(graphs)
+        if assembly_warps is not None:
+            N.check(self._lib.ufem_batch_set_assembly_warps(self._b, int(assembly_warps)))
+
+    def __len__(self) -> int:
+        return len(self.members)
+
+    def set_graphs(self, on: bool) -> None:
+        N.check(self._lib.ufem_batch_set_graphs(self._b, 1 if on else 0))
+
+    def assemble(self, stream=None) -> None:
+        N.check(self._lib.ufem_batch_assemble(self._b, _stream(stream)))
+
+    def solve(self, stream=None, **krylov) -> list[dict]:
+        sts = (N.KrylovStatus * len(self.members))()
+        N.check(self._lib.ufem_batch_solve(self._b, C.byref(krylov_options(**krylov)), sts, _stream(stream)))
+        return [s.as_dict() for s in sts]
+
+    def update(self, stream=None) -> None:
+        N.check(self._lib.ufem_batch_update(self._b, _stream(stream)))
+
+    def step(self, stream=None, **krylov) -> list[dict]:
+        """One time step of every member: assemble, Dirichlet, solve, update."""
+        sts = (N.KrylovStatus * len(self.members))()
+        N.check(self._lib.ufem_batch_step(self._b, C.byref(krylov_options(**krylov)), sts, _stream(stream)))
+        return [s.as_dict() for s in sts]
+
+    def close(self) -> None:
+        if getattr(self, "_b", None):
+            self._lib.ufem_batch_destroy(self._b)
+            self._b = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

@@ -221,6 +221,28 @@ int ufem_ns_get_assembly_kernel(ufem_ns_handle* h, int32_t* variant, int32_t* wa
 int ufem_ns_tune_assembly(ufem_ns_handle* h, void* stream, int32_t reps, int32_t* variant,
                           int32_t* warps_per_cta, float* ms_per_launch);
 
+/* ---- batches: many meshes per launch (no counterpart in the reference) ----
+ * A batch steps several handles of the same dim, precision and element form
+ * together: every phase of a time step is one launch over all members (the
+ * assembly one persistent launch), and the solve is BiCGStab with point Jacobi
+ * (or none) and per-member scalars, so each member converges on its own and
+ * its results are bitwise the same alone and in any batch.  The iteration
+ * blocks are replayed from captured CUDA graphs.  Members stay owned by the
+ * caller and must outlive the batch; a member's BC list may change between
+ * steps, its mesh may not.  mixed = 1 needs precision-1 members. */
+typedef struct ufem_batch ufem_batch;
+int ufem_batch_create(ufem_ns_handle* const* members, int32_t n, ufem_batch** out);
+int ufem_batch_size(const ufem_batch* b, int32_t* n, int64_t* rows);
+int ufem_batch_set_graphs(ufem_batch* b, int32_t enable);
+int ufem_batch_set_assembly_warps(ufem_batch* b, int32_t warps_per_cta);
+/* LinearizeU + assembly + symmetric Dirichlet of every member. */
+int ufem_batch_assemble(ufem_batch* b, void* stream);
+/* statuses: one per member, or NULL. */
+int ufem_batch_solve(ufem_batch* b, const ufem_krylov_opts* kopts, ufem_krylov_status* statuses, void* stream);
+int ufem_batch_update(ufem_batch* b, void* stream);
+int ufem_batch_step(ufem_batch* b, const ufem_krylov_opts* kopts, ufem_krylov_status* statuses, void* stream);
+void ufem_batch_destroy(ufem_batch* b);
+
 int ufem_ns_enable_timing(ufem_ns_handle* h, int32_t enable);
 int ufem_ns_get_timings(ufem_ns_handle* h, ufem_ns_timings* t);
 

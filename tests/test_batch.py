@@ -1,0 +1,111 @@
+"""GPU tests of batches: several meshes stepped by one launch per phase.
+
+Stated tolerances: a member's state after batched steps is BITWISE equal to
+the same member stepped alone (a batch of one), whatever the other members
+are; the batched assembly agrees with the one-mesh kernel to 1e-14 of each
+CSR row's largest entry (the same element code compiled into two kernels);
+batched solves agree with the one-mesh solver within 1e-6 relative and reach
+the FP64 residual tolerance; the mixed batched solve (FP32 operator, FP64
+vectors, FP64 refinement) meets the same residual and agrees within 1e-6.
+"""
+import numpy as np
+import pytest
+
+from coolfluid3_b200 import Batch, NavierStokes
+from coolfluid3_b200 import problems as P
+
+from .util import row_scaled_error, vec_rel_error
+
+pytestmark = pytest.mark.gpu
+
+
+def member(dim, n, seed, precision="fp64", nu=1e-2, dt=0.01, spec=False):
+    pb = P.make_problem(dim, n, nu=nu, dt=dt, seed=seed)
+    ns = NavierStokes(pb.coords, pb.conn, dt=pb.dt, use_specializations=spec, precision=precision)
+    ns.set_state(pb.up, pb.lin, pb.nu)
+    ns.add_dirichlet(pb.bc_nodes, pb.bc_comps, pb.bc_values)
+    return ns
+
+
+SIZES_2D = [(2, 6, 11), (2, 13, 12), (2, 9, 13), (2, 20, 14)]
+SIZES_3D = [(3, 3, 21), (3, 5, 22), (3, 4, 23)]
+
+
+def run_batch(specs, steps, precision="fp64", graphs=True, **krylov):
+    ms = [member(*s, precision=precision) for s in specs]
+    b = Batch(ms, graphs=graphs)
+    sts = []
+    for _ in range(steps):
+        sts.append(b.step(**krylov))
+    states = [m.state()[0] for m in ms]
+    b.close()
+    return states, sts
+
+
+@pytest.mark.parametrize("specs", [SIZES_2D, SIZES_3D])
+def test_member_results_identical_alone_and_in_the_mix(specs):
+    mixed, _ = run_batch(specs, 2)
+    for k, s in enumerate(specs):
+        alone, _ = run_batch([s], 2)
+        assert np.array_equal(alone[0], mixed[k]), s
+    # a different mix (reversed order, one member left out)
+    sub = list(reversed(specs[1:]))
+    other, _ = run_batch(sub, 2)
+    for k, s in enumerate(sub):
+        assert np.array_equal(other[k], mixed[specs.index(s)]), s
+
+
+def test_graphs_do_not_change_results():
+    a, sa = run_batch(SIZES_2D[:3], 2, graphs=True)
+    b, sb = run_batch(SIZES_2D[:3], 2, graphs=False)
+    for x, y in zip(a, b):
+        assert np.array_equal(x, y)
+    assert [s["iterations"] for s in sa[-1]] == [s["iterations"] for s in sb[-1]]
+
+
+@pytest.mark.parametrize("specs", [SIZES_2D, SIZES_3D])
+def test_batched_assembly_matches_single_handle(specs):
+    ms = [member(*s) for s in specs]
+    singles = [member(*s) for s in specs]
+    b = Batch(ms)
+    b.assemble()
+    for m, s in zip(ms, singles):
+        s.assemble()
+        s.apply_dirichlet()
+        v, r = m.system()
+        vs, rs = s.system()
+        rp, _ = s.csr()
+        assert row_scaled_error(v, vs, rp) <= 1e-14
+        assert vec_rel_error(r, rs) <= 1e-14
+    b.close()
+
+
+@pytest.mark.parametrize("specs", [SIZES_2D, SIZES_3D])
+def test_batched_step_matches_single_handle(specs):
+    states, sts = run_batch(specs, 2, tol=1e-12)
+    for k, s in enumerate(specs):
+        ref = member(*s)
+        for _ in range(2):
+            ref.execute(tol=1e-12)
+        up, _ = ref.state()
+        assert vec_rel_error(states[k], up) <= 1e-6, s
+        assert sts[-1][k]["converged"] and sts[-1][k]["rel_residual"] <= 1e-12
+
+
+@pytest.mark.parametrize("specs", [SIZES_2D, SIZES_3D])
+def test_mixed_batched_solve(specs):
+    plain, _ = run_batch(specs, 1, precision="fp32", tol=1e-10)
+    mixed, sts = run_batch(specs, 1, precision="fp32", tol=1e-10, mixed=True)
+    for k in range(len(specs)):
+        assert sts[0][k]["converged"] and sts[0][k]["rel_residual"] <= 1e-10
+        assert vec_rel_error(mixed[k], plain[k]) <= 1e-6
+
+
+def test_batch_rejects_incompatible_members():
+    from coolfluid3_b200 import UfemError
+    a = member(2, 4, 1)
+    c = member(3, 2, 2)
+    with pytest.raises(UfemError):
+        Batch([a, c])
+    with pytest.raises(UfemError):
+        Batch([a, a])
