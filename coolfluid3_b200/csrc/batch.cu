@@ -34,6 +34,7 @@ constexpr int kThreads = 256;
 constexpr int kBlockIters = 8;    // BiCGStab iterations per host check / graph replay
 constexpr int kDc = 16;           // per-mesh double scalars
 constexpr int kIc = 8;            // per-mesh int flags
+constexpr int kMaxRestarts = 10;  // BiCGStab restarts after breakdowns in one solve
 
 // per-mesh scalar slots (dctl[m * kDc + ...])
 constexpr int sBnorm = 0, sBeta = 1, sEst = 2, sRho = 5, sRhoOld = 6, sAlpha = 7, sOmega = 8, sTrue = 9,
@@ -577,6 +578,7 @@ __global__ void zero_batch_kernel(const Chunk* __restrict__ chunks, const BatchM
 
 template <typename T>
 int dmal(T** p, size_t n) {
+  DeviceLock lk(device_mutex());
   const cudaError_t e = cudaMalloc(reinterpret_cast<void**>(p), std::max<size_t>(n, 1) * sizeof(T));
   if (e != cudaSuccess) {
     *p = nullptr;
@@ -586,6 +588,7 @@ int dmal(T** p, size_t n) {
 }
 template <typename T>
 void dfr(T*& p) {
+  DeviceLock lk(device_mutex());
   if (p) cudaFree(p);
   p = nullptr;
 }
@@ -627,6 +630,7 @@ struct ufem_batch {
 namespace {
 
 void batch_free(ufem_batch* b) {
+  DeviceLock lk(device_mutex());
   for (auto& g : b->block_exec)
     if (g) cudaGraphExecDestroy(g);
   if (b->capture_stream) cudaStreamDestroy(b->capture_stream);
@@ -777,6 +781,7 @@ int bicgstab_b(ufem_batch* b, int pkind, double tol, int maxit, bool use_outer, 
   UFEM_CUDA_TRY(cudaGetLastError());
   const bool use_graph = b->graphs;
   if (use_graph && (b->block_exec[slot] == nullptr || b->block_pkind[slot] != pkind)) {
+    DeviceLock lk(device_mutex());  // no implicit device synchronisation from other threads during capture
     if (b->block_exec[slot]) {
       cudaGraphExecDestroy(b->block_exec[slot]);
       b->block_exec[slot] = nullptr;
@@ -882,6 +887,7 @@ int ufem_batch_create(ufem_ns_handle* const* members, int32_t n, ufem_batch** ou
     return rc;
   }
   cudaError_t ce;
+  DeviceLock device_lock(device_mutex());
   if ((ce = cudaMallocHost(reinterpret_cast<void**>(&b->h_dctl), sizeof(double) * kDc * n)) != cudaSuccess ||
       (ce = cudaMallocHost(reinterpret_cast<void**>(&b->h_ictl), sizeof(int) * kIc * n)) != cudaSuccess ||
       (ce = cudaStreamCreateWithFlags(&b->capture_stream, cudaStreamNonBlocking)) != cudaSuccess ||
@@ -966,10 +972,24 @@ int ufem_batch_solve(ufem_batch* b, const ufem_krylov_opts* kopts, ufem_krylov_s
   if (o.max_refine <= 0) o.max_refine = 20;
   if (o.inner_tol <= 0) o.inner_tol = 1e-3;
   const bool mixed = o.mixed != 0;
-  if (mixed && b->precision != 1)
-    return set_error(UFEM_ERR_ARG, "a mixed batched solve needs FP32-element members (precision 1)");
   cudaStream_t st = static_cast<cudaStream_t>(stream);
   int rc;
+  if (mixed) {  // FP32 operator copies: allocated once, written by every later assembly
+    bool added = false;
+    for (ufem_ns_handle* h : b->members)
+      if (h->d_vals32 == nullptr) {
+        if ((rc = ensure_vals32(h, st))) return rc;
+        added = true;
+      }
+    if (added) {
+      if (b->res == nullptr && ((rc = dmal(&b->res, size_t(b->total_rows))) || (rc = dmal(&b->corr, size_t(b->total_rows)))))
+        return rc;
+      UFEM_CUDA_TRY(cudaStreamSynchronize(st));
+      if ((rc = batch_refresh(b))) return rc;
+    }
+    if (b->res == nullptr && ((rc = dmal(&b->res, size_t(b->total_rows))) || (rc = dmal(&b->corr, size_t(b->total_rows)))))
+      return rc;
+  }
   std::vector<int> iters(b->nmesh, 0), status(b->nmesh, 0), refines(b->nmesh, 0);
   if (!mixed) {
     if ((rc = bicgstab_b<double, kSol, kRhs>(b, o.precond, o.tol, o.max_iters, false, 0, st))) return rc;
@@ -978,6 +998,30 @@ int ufem_batch_solve(ufem_batch* b, const ufem_krylov_opts* kopts, ufem_krylov_s
     for (int m = 0; m < b->nmesh; ++m) {
       iters[m] = b->h_ictl[m * kIc + fIters];
       status[m] = b->h_ictl[m * kIc + fStatus];
+    }
+    // members that broke down (rho or omega ~ 0) restart from their iterate;
+    // the others are held by their outer flag
+    for (int restart = 0; restart < kMaxRestarts; ++restart) {
+      int used = 0;
+      bool any = false;
+      for (int m = 0; m < b->nmesh; ++m)
+        if (status[m] == 2 && iters[m] < o.max_iters) {
+          any = true;
+          used = std::max(used, iters[m]);
+        }
+      if (!any) break;
+      for (int m = 0; m < b->nmesh; ++m) {
+        for (int q = 0; q < kIc; ++q) b->h_ictl[m * kIc + q] = 0;
+        b->h_ictl[m * kIc + fOuter] = (status[m] == 2 && iters[m] < o.max_iters) ? 0 : 1;
+      }
+      if ((rc = bicgstab_b<double, kSol, kRhs>(b, o.precond, o.tol, o.max_iters - used, true, 0, st))) return rc;
+      UFEM_CUDA_TRY(cudaMemcpyAsync(b->h_ictl, b->ictl, sizeof(int) * kIc * b->nmesh, cudaMemcpyDeviceToHost, st));
+      UFEM_CUDA_TRY(cudaStreamSynchronize(st));
+      for (int m = 0; m < b->nmesh; ++m) {
+        if (b->h_ictl[m * kIc + fOuter]) continue;
+        iters[m] += b->h_ictl[m * kIc + fIters];
+        status[m] = b->h_ictl[m * kIc + fStatus];
+      }
     }
   } else {
     // FP64 refinement: r = b - A64 x; inner BiCGStab on A32 d = r (FP64

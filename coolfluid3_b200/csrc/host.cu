@@ -16,6 +16,11 @@
 
 namespace ufem {
 
+std::recursive_mutex& device_mutex() {
+  static std::recursive_mutex m;
+  return m;
+}
+
 static thread_local std::string g_err;
 
 int set_error(int code, const std::string& msg) {
@@ -53,6 +58,7 @@ inline double uniform01(uint64_t seed, uint64_t idx) {
 
 template <typename T>
 int dmalloc(T** p, size_t count, const char* what) {
+  DeviceLock lk(device_mutex());
   cudaError_t e = cudaMalloc(reinterpret_cast<void**>(p), std::max<size_t>(count, 1) * sizeof(T));
   if (e != cudaSuccess) {
     *p = nullptr;
@@ -63,6 +69,7 @@ int dmalloc(T** p, size_t count, const char* what) {
 
 template <typename T>
 void dfree(T*& p) {
+  DeviceLock lk(device_mutex());
   if (p) cudaFree(p);
   p = nullptr;
 }
@@ -222,6 +229,7 @@ void record(ufem_ns_handle* h, int phase, bool stop, cudaStream_t s) {
 }
 
 void destroy_impl(ufem_ns_handle* h) {
+  DeviceLock lk(device_mutex());
   krylov_free(h);
   free_bc_plan(h->bcp);
   dfree(h->d_coords); dfree(h->d_conn); dfree(h->d_state); dfree(h->d_hist); dfree(h->d_uadv);
@@ -514,6 +522,7 @@ int ufem_ns_create(const ufem_mesh* mesh, const ufem_ns_options* opts, ufem_ns_h
   h->wplan.big32.nchunks = int(big32.size());
 
   // --- device allocations and uploads
+  DeviceLock device_lock(device_mutex());
   std::vector<double> c4(size_t(N) * 4, 0.0);
   for (int64_t i = 0; i < N; ++i)
     for (int k = 0; k < dim; ++k) c4[i * 4 + k] = mesh->coords[i * dim + k];
@@ -582,6 +591,20 @@ int ufem_ns_set_options(ufem_ns_handle* h, const ufem_ns_options* opts) {
   if (opts->precision == 1 && !h->d_vals32 && (rc = dmalloc(&h->d_vals32, size_t(h->nnz), "vals32"))) return rc;
   if (opts->precision == 1 && !h->d_node32 && (rc = dmalloc(&h->d_node32, size_t(h->N) * 8, "node32"))) return rc;
   h->vals32_valid = false;
+  return UFEM_OK;
+}
+
+int ufem_ns_device_bytes(const ufem_ns_handle* h, int64_t* bytes) {
+  if (!h || !bytes) return set_error(UFEM_ERR_ARG, "NULL argument");
+  const int64_t N = h->N, E = h->E, R = h->nrows, Z = h->nnz;
+  int64_t b = N * (32 + 32 + 96 + 32 + 8) + E * 16 + (N + 1) * 12 + h->bnnz * 4 + (R + 1) * 8 + Z * 12 +
+              R * (8 + 8 + 8) + E * h->nn * 8 + N * 16 + N * 4 * h->dim * 8;
+  if (h->d_force) b += N * 32;
+  if (h->d_vals32) b += Z * 4;
+  if (h->d_node32) b += N * 32;
+  if (h->kw) b += R * 8 * 13;  // Krylov vectors once a solve has run
+  b += h->bcp.nbc * 40 + h->bcp.nfix_rows * 16 + h->bcp.nfix * 12;
+  *bytes = b;
   return UFEM_OK;
 }
 
@@ -883,7 +906,10 @@ int ufem_ns_download_system(ufem_ns_handle* h, double* vals, double* rhs, void* 
 int ufem_ns_get_system(ufem_ns_handle* h, double* vals, double* rhs) {
   int rc = ufem_ns_download_system(h, vals, rhs, nullptr);
   if (rc) return rc;
-  UFEM_CUDA_TRY(cudaDeviceSynchronize());
+  {
+    DeviceLock lk(device_mutex());
+    UFEM_CUDA_TRY(cudaDeviceSynchronize());
+  }
   return UFEM_OK;
 }
 
@@ -937,7 +963,10 @@ int ufem_ns_get_timings(ufem_ns_handle* h, ufem_ns_timings* t) {
 
 void ufem_ns_destroy(ufem_ns_handle* h) {
   if (!h) return;
-  cudaDeviceSynchronize();
+  {
+    DeviceLock lk(device_mutex());
+    cudaDeviceSynchronize();
+  }
   destroy_impl(h);
 }
 

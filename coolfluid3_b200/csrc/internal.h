@@ -4,6 +4,7 @@
 #include <cuda_runtime.h>
 
 #include <cstdint>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -15,6 +16,12 @@ namespace ufem {
 // Error reporting across the C ABI: a thread-local message plus a code.
 // ---------------------------------------------------------------------------
 int set_error(int code, const std::string& msg);
+
+// Serialises device-lifecycle calls (allocation, free, device-wide
+// synchronisation) with CUDA-graph capture: a capture in one host thread must
+// not overlap an implicit device synchronisation issued by another.
+std::recursive_mutex& device_mutex();
+using DeviceLock = std::lock_guard<std::recursive_mutex>;
 
 #define UFEM_CUDA_TRY(expr)                                                              \
   do {                                                                                   \
@@ -184,5 +191,8 @@ int build_bc_plan(ufem_ns_handle* h);
 int krylov_solve(ufem_ns_handle* h, const ufem_krylov_opts* ko, ufem_krylov_status* st, cudaStream_t s);
 int krylov_apply(ufem_ns_handle* h, const double* d_x, double* d_y, cudaStream_t s);
 void krylov_free(ufem_ns_handle* h);
+// Allocates the FP32 copy of the values (converted from the current FP64
+// values); later assemblies write both.
+int ensure_vals32(ufem_ns_handle* h, cudaStream_t s);
 
 }  // namespace ufem

@@ -51,6 +51,7 @@ constexpr int kBnorm = 0, kBeta = 1, kEst = 2, kHnext = 3, kTrue = 4;
 constexpr int kRho = 5, kRhoOld = 6, kAlpha = 7, kOmega = 8, kRhV = 9, kTS = 10, kTT = 11, kR2 = 12, kScale = 13;
 constexpr int kRedThreads = 256;
 constexpr int kInnerIterCap = 400;  // iterations of one FP32 inner solve of the mixed path
+constexpr int kMaxRestarts = 10;    // BiCGStab restarts after breakdowns in one solve
 
 template <typename T>
 __device__ __forceinline__ T warp_sum(T v) {
@@ -551,6 +552,7 @@ __global__ void bicg_init_kernel(double* dctl, int* ictl, double tol) {
 template <typename T>
 int dalloc(T** p, size_t count) {
   if (*p) return UFEM_OK;
+  DeviceLock lk(device_mutex());
   cudaError_t e = cudaMalloc(reinterpret_cast<void**>(p), std::max<size_t>(count, 1) * sizeof(T));
   if (e != cudaSuccess)
     return set_error(UFEM_ERR_NOMEM, std::string("cudaMalloc (Krylov workspace): ") + cudaGetErrorString(e));
@@ -559,6 +561,7 @@ int dalloc(T** p, size_t count) {
 
 template <typename T>
 void dfree(T*& p) {
+  DeviceLock lk(device_mutex());
   if (p) cudaFree(p);
   p = nullptr;
 }
@@ -585,6 +588,7 @@ int ensure_work(ufem_ns_handle* h, int m, bool need32, bool bicg) {
       (rc = dalloc(&kw.y, size_t(M))) || (rc = dalloc(&kw.dctl, 16)) || (rc = dalloc(&kw.ictl, 8)))
     return rc;
   if (!kw.h_dctl) {
+    DeviceLock lk(device_mutex());
     UFEM_CUDA_TRY(cudaMallocHost(reinterpret_cast<void**>(&kw.h_dctl), 16 * sizeof(double)));
     UFEM_CUDA_TRY(cudaMallocHost(reinterpret_cast<void**>(&kw.h_ictl), 8 * sizeof(int)));
   }
@@ -842,12 +846,25 @@ int krylov_solve(ufem_ns_handle* h, const ufem_krylov_opts* ko, ufem_krylov_stat
   ufem_krylov_status out{};
   if (!mixed) {
     SolveResult r;
-    if (bicg)
-      rc = bicgstab<double, double, double>(h, kw, h->d_vals, h->d_rhs, h->d_sol, kw.r, kw.brh, kw.bp, kw.bv, kw.bs, kw.bt,
-                                            kw.bph, kw.bsh, kw.dinv, o.precond, o.tol, o.max_iters, s, r);
-    else
+    if (bicg) {
+      // A breakdown (rho or omega ~ 0) leaves a finite iterate: restart from it
+      // while iterations remain.
+      int used = 0;
+      for (int restarts = 0;; ++restarts) {
+        rc = bicgstab<double, double, double>(h, kw, h->d_vals, h->d_rhs, h->d_sol, kw.r, kw.brh, kw.bp, kw.bv, kw.bs,
+                                              kw.bt, kw.bph, kw.bsh, kw.dinv, o.precond, o.tol, o.max_iters - used, s, r);
+        if (rc) return rc;
+        used += r.iters;
+        if (r.status == 2 && !r.converged && std::isfinite(r.relres) && used < o.max_iters &&
+            restarts < kMaxRestarts)
+          continue;
+        break;
+      }
+      r.iters = used;
+    } else {
       rc = gmres<double, double, double>(h, h->d_vals, h->d_rhs, h->d_sol, kw.V, kw.w, kw.z, kw.t, kw.r, kw.dinv,
                                          o.precond, o.tol, o.max_iters, o.restart, s, r);
+    }
     if (rc) return rc;
     out.converged = r.converged;
     out.status = r.status;
@@ -935,6 +952,17 @@ int krylov_solve(ufem_ns_handle* h, const ufem_krylov_opts* ko, ufem_krylov_stat
   return UFEM_OK;
 }
 
+int ensure_vals32(ufem_ns_handle* h, cudaStream_t s) {
+  if (h->d_vals32 == nullptr) {
+    int rc;
+    if ((rc = dalloc(&h->d_vals32, size_t(h->nnz)))) return rc;
+    vals_to32_kernel<<<grid_for(h->nnz, 256), 256, 0, s>>>(h->nnz, h->d_vals, h->d_vals32);
+    UFEM_CUDA_TRY(cudaGetLastError());
+    h->vals32_valid = true;
+  }
+  return UFEM_OK;
+}
+
 int krylov_apply(ufem_ns_handle* h, const double* d_x, double* d_y, cudaStream_t s) {
   return spmv<double, double>(h, h->d_vals, d_x, d_y, nullptr, s);
 }
@@ -947,6 +975,7 @@ void krylov_free(ufem_ns_handle* h) {
   dfree(k.bp); dfree(k.bv); dfree(k.bs); dfree(k.bt); dfree(k.brh); dfree(k.bph); dfree(k.bsh);
   dfree(k.part); dfree(k.hbuf); dfree(k.H); dfree(k.cs); dfree(k.sn); dfree(k.g); dfree(k.y);
   dfree(k.dctl); dfree(k.ictl);
+  DeviceLock lk(device_mutex());
   if (k.h_dctl) cudaFreeHost(k.h_dctl);
   if (k.h_ictl) cudaFreeHost(k.h_ictl);
   delete h->kw;

@@ -1,0 +1,372 @@
+"""Serving loop: time-stepping solves of different sizes on one GPU.
+
+Requests (a mesh, initial fields, Dirichlet list, time step and a number of
+steps) arrive over time.  The server
+
+  * admits them by HBM budget: a request is admitted when a slot is free and
+    its estimated device footprint fits the remaining budget (first fit in
+    arrival order); the estimate is replaced by the handle's actual footprint
+    once it exists, and released when the request completes;
+  * builds each admitted request's handle (mesh plan, CSR pattern, fields)
+    on a pool of host threads while the GPU keeps stepping the others, and
+    keeps mesh, pattern and state resident on the device until the request
+    completes;
+  * batches continuously: one worker per mesh dimension steps ALL its active
+    requests together every tick (one batched assembly launch, one batched
+    BiCGStab with per-request scalars, see ``ufem.Batch``) on its own CUDA
+    stream, so 2D and 3D work overlaps on the device; requests that arrive
+    while others run join at the next tick, finished ones leave;
+  * reports throughput (time steps per second) beside p50/p99 step latency
+    and request latency.
+
+Because a batch member's arithmetic does not depend on the other members, a
+request's results are bitwise the same whether it ran alone or in the mix.
+
+``run_plain`` is the reference point: the same requests, one at a time, each
+through the plain FP64 one-handle path (``NavierStokes.execute``).
+"""
+from __future__ import annotations
+
+import math
+import threading
+import time
+from collections import deque
+from concurrent.futures import ThreadPoolExecutor
+from dataclasses import dataclass, field
+
+import numpy as np
+
+from . import problems as P
+from .ufem import Batch, NavierStokes
+
+
+@dataclass
+class Request:
+    rid: int
+    coords: np.ndarray
+    conn: np.ndarray
+    up: np.ndarray
+    lin: np.ndarray
+    nu: np.ndarray
+    bc_nodes: np.ndarray
+    bc_comps: np.ndarray
+    bc_values: np.ndarray
+    dt: float
+    nsteps: int
+    arrival: float = 0.0  # seconds after the start of the run
+
+    @property
+    def dim(self) -> int:
+        return self.coords.shape[1]
+
+    @property
+    def nb_elems(self) -> int:
+        return self.conn.shape[0]
+
+
+@dataclass
+class Result:
+    rid: int
+    state: np.ndarray | None
+    step_ms: list = field(default_factory=list)
+    statuses: list = field(default_factory=list)
+    arrival: float = 0.0
+    admitted: float = 0.0
+    finished: float = 0.0
+    error: str | None = None  # a request rejected at set-up (bad mesh or fields)
+
+    @property
+    def ok(self) -> bool:
+        return self.error is None and all(s.get("converged", 0) for s in self.statuses)
+
+
+def estimate_bytes(req: Request, precision: str = "fp64") -> int:
+    """Device footprint of a request before its handle exists (P1 meshes:
+    about 7 (2D) or 15 (3D) graph neighbours per node, plus 30% margin)."""
+    n_nodes, n_elems, dim = len(req.coords), len(req.conn), req.dim
+    neq = dim + 1
+    bnnz = int(1.3 * n_nodes * (7 if dim == 2 else 15))
+    nnz = bnnz * neq * neq
+    rows = n_nodes * neq
+    per_value = 16  # FP64 values, column indices, FP32 operator copy
+    return n_nodes * 256 + n_elems * 40 + bnnz * 4 + nnz * per_value + rows * 8 * 16
+
+
+def make_request(rid: int, dim: int, n_elems: float, nu: float, seed: int, nsteps: int = 10,
+                 arrival: float = 0.0) -> Request:
+    """A lid-driven cavity request on the structured generators, sized to
+    about n_elems elements (2D: 2 s^2 triangles, 3D: 6 s^3 tetrahedra)."""
+    if dim == 2:
+        s = max(2, int(round(math.sqrt(n_elems / 2.0))))
+        dt = 0.01
+    else:
+        s = max(2, int(round((n_elems / 6.0) ** (1.0 / 3.0))))
+        dt = 5e-3
+    pb = P.make_problem(dim, s, nu=nu, dt=dt, seed=seed)
+    return Request(rid, pb.coords, pb.conn, pb.up, pb.lin, pb.nu, pb.bc_nodes, pb.bc_comps, pb.bc_values, dt,
+                   nsteps, arrival)
+
+
+def poisson_workload(n: int, rate: float, elems=(1e4, 2e6), nu=(1e-4, 1e-1), dims=(2, 3), nsteps: int = 10,
+                     seed: int = 20261203) -> list[Request]:
+    """Seeded synthetic serving workload: Poisson arrivals at `rate` per second,
+    element counts and viscosities log-uniform, dimensions drawn uniformly."""
+    rng = np.random.default_rng(seed)
+    t = 0.0
+    out = []
+    for k in range(n):
+        t += rng.exponential(1.0 / rate)
+        dim = int(rng.choice(dims))
+        e = math.exp(rng.uniform(math.log(elems[0]), math.log(elems[1])))
+        v = math.exp(rng.uniform(math.log(nu[0]), math.log(nu[1])))
+        out.append(make_request(k, dim, e, v, seed + 7 * k + 1, nsteps, t))
+    return out
+
+
+def _percentiles(xs) -> dict:
+    if not xs:
+        return {"p50": None, "p99": None, "mean": None}
+    a = np.asarray(xs, np.float64)
+    return {"p50": float(np.percentile(a, 50)), "p99": float(np.percentile(a, 99)), "mean": float(a.mean())}
+
+
+def summarize(results: list[Result], t_start: float, t_end: float) -> dict:
+    steps = sum(len(r.step_ms) for r in results if r.error is None)
+    span = max(t_end - t_start, 1e-9)
+    return {
+        "requests": len(results),
+        "steps": steps,
+        "seconds": span,
+        "steps_per_s": steps / span,
+        "step_ms": _percentiles([x for r in results for x in r.step_ms]),
+        "request_s": _percentiles([r.finished - r.arrival for r in results if r.error is None]),
+        "rejected": sum(1 for r in results if r.error is not None),
+    }
+
+
+def _new_handle(req: Request, precision: str, use_specializations: bool) -> NavierStokes:
+    ns = NavierStokes(req.coords, req.conn, dt=req.dt, use_specializations=use_specializations, precision=precision)
+    ns.set_state(req.up, req.lin, req.nu)
+    ns.add_dirichlet(req.bc_nodes, req.bc_comps, req.bc_values)
+    return ns
+
+
+class _Active:
+    def __init__(self, req: Request, ns: NavierStokes, admitted: float, reserved: int):
+        self.req = req
+        self.ns = ns
+        self.reserved = reserved
+        self.result = Result(req.rid, None, arrival=req.arrival, admitted=admitted)
+        self.done_steps = 0
+
+
+class Server:
+    """Continuous-batching server for one GPU (see the module docstring)."""
+
+    def __init__(self, hbm_budget_bytes: int, max_slots: int = 64, precision: str = "fp64", mixed: bool = True,
+                 krylov: dict | None = None, graphs: bool = True, creators: int = 2,
+                 use_specializations: bool = False, realtime: bool = True):
+        if precision not in ("fp32", "fp64"):
+            raise ValueError("precision must be fp32 or fp64")
+        self.budget = int(hbm_budget_bytes)
+        self.max_slots = int(max_slots)
+        self.precision = precision
+        self.graphs = graphs
+        self.creators = creators
+        self.spec = use_specializations
+        self.realtime = realtime
+        self.krylov = dict(method="bicgstab", precond="jacobi", tol=1e-10, max_iters=3000)
+        if mixed:
+            self.krylov.update(mixed=True, inner_tol=1e-6, max_refine=20)
+        self.krylov.update(krylov or {})
+        self._lock = threading.Condition()
+        self._used = 0
+        self._slots = 0
+        self.peak_bytes = 0
+        self.max_batch = 0
+        self.errors: list = []
+
+    # -- budget ---------------------------------------------------------------
+    def _try_reserve(self, nbytes: int) -> bool:
+        with self._lock:
+            if self._slots < self.max_slots and self._used + nbytes <= self.budget:
+                self._used += nbytes
+                self._slots += 1
+                self.peak_bytes = max(self.peak_bytes, self._used)
+                return True
+            return False
+
+    def _adjust(self, old: int, new: int) -> None:
+        with self._lock:
+            self._used += new - old
+            self.peak_bytes = max(self.peak_bytes, self._used)
+
+    def _release(self, nbytes: int) -> None:
+        with self._lock:
+            self._used -= nbytes
+            self._slots -= 1
+            self._lock.notify_all()
+
+    # -- run ------------------------------------------------------------------
+    def run(self, requests: list[Request]) -> tuple[list[Result], dict]:
+        import torch
+
+        reqs = sorted(requests, key=lambda r: r.arrival)
+        for r in reqs:
+            if estimate_bytes(r, self.precision) > self.budget:
+                raise ValueError(f"request {r.rid} alone exceeds the HBM budget")
+        inbox = {2: deque(), 3: deque()}
+        results: list[Result] = []
+        state = {"open": len(reqs)}
+        t0 = time.perf_counter()
+        now = lambda: time.perf_counter() - t0  # noqa: E731
+
+        def worker(dim: int):
+            stream = torch.cuda.Stream()
+            active: list[_Active] = []
+            batch = None
+            members = None
+            try:
+                while True:
+                    with self._lock:
+                        while not inbox[dim] and not active and state["open"] > 0:
+                            self._lock.wait(0.05)
+                        if not inbox[dim] and not active and state["open"] <= 0:
+                            break
+                        while inbox[dim]:
+                            active.append(inbox[dim].popleft())
+                    if not active:
+                        continue
+                    ids = tuple(id(a.ns) for a in active)
+                    if ids != members:
+                        if batch is not None:
+                            batch.close()
+                        batch = Batch([a.ns for a in active], graphs=self.graphs)
+                        members = ids
+                        self.max_batch = max(self.max_batch, len(active))
+                    ts = time.perf_counter()
+                    sts = batch.step(stream, **self.krylov)
+                    stream.synchronize()
+                    ms = (time.perf_counter() - ts) * 1e3
+                    finished = []
+                    for a, st in zip(active, sts):
+                        a.result.step_ms.append(ms)
+                        a.result.statuses.append(st)
+                        a.done_steps += 1
+                        if a.done_steps >= a.req.nsteps:
+                            finished.append(a)
+                    for a in finished:
+                        active.remove(a)
+                    if finished:
+                        batch.close()
+                        batch, members = None, None
+                    for a in finished:
+                        a.result.state = a.ns.state()[0]
+                        a.ns.close()
+                        a.result.finished = now()
+                        self._release(a.reserved)
+                        with self._lock:
+                            results.append(a.result)
+                            state["open"] -= 1
+                            self._lock.notify_all()
+            except Exception as e:  # surface worker failures to the caller
+                with self._lock:
+                    self.errors.append(e)
+                    state["open"] = -10 ** 9
+                    self._lock.notify_all()
+            finally:
+                if batch is not None:
+                    batch.close()
+
+        def create(req: Request, est: int, admitted: float):
+            try:
+                ns = _new_handle(req, self.precision, self.spec)
+            except Exception as e:  # the request is rejected; the others go on
+                self._release(est)
+                with self._lock:
+                    results.append(Result(req.rid, None, arrival=req.arrival, admitted=admitted, finished=now(),
+                                          error=str(e)))
+                    state["open"] -= 1
+                    self._lock.notify_all()
+                return
+            actual = ns.device_bytes() + req.coords.shape[0] * (req.dim + 1) * 8 * 14  # + batch vectors
+            self._adjust(est, actual)
+            a = _Active(req, ns, admitted, actual)
+            with self._lock:
+                inbox[req.dim].append(a)
+                self._lock.notify_all()
+
+        workers = [threading.Thread(target=worker, args=(d,), daemon=True) for d in (2, 3)]
+        for w in workers:
+            w.start()
+        pool = ThreadPoolExecutor(max_workers=self.creators)
+        waiting: deque = deque()
+        pending = deque(reqs)
+        try:
+            while pending or waiting:
+                if self.errors:
+                    break
+                t = now()
+                while pending and (pending[0].arrival <= t or not self.realtime):
+                    waiting.append(pending.popleft())
+                admitted_any = False
+                for req in list(waiting):  # first fit in arrival order
+                    est = estimate_bytes(req, self.precision)
+                    if self._try_reserve(est):
+                        waiting.remove(req)
+                        pool.submit(create, req, est, now())
+                        admitted_any = True
+                if not admitted_any:
+                    with self._lock:
+                        timeout = 0.01
+                        if pending and not waiting and self.realtime:
+                            timeout = max(0.0, min(0.05, pending[0].arrival - now()))
+                        self._lock.wait(timeout)
+            with self._lock:
+                while state["open"] > 0 and not self.errors:
+                    self._lock.wait(0.1)
+        finally:
+            pool.shutdown(wait=True)
+            with self._lock:
+                if state["open"] > 0:
+                    state["open"] = 0
+                self._lock.notify_all()
+            for w in workers:
+                w.join()
+        if self.errors:
+            raise self.errors[0]
+        t_end = max((r.finished for r in results), default=now())
+        t_start = min((r.arrival for r in results), default=0.0) if self.realtime else 0.0
+        stats = summarize(results, t_start, t_end)
+        stats.update(peak_reserved_bytes=self.peak_bytes, budget_bytes=self.budget, max_batch=self.max_batch)
+        return sorted(results, key=lambda r: r.rid), stats
+
+
+def run_plain(requests: list[Request], krylov: dict | None = None, realtime: bool = True,
+              use_specializations: bool = False) -> tuple[list[Result], dict]:
+    """The same requests one at a time in arrival order through the plain
+    FP64 one-handle path (assemble, Dirichlet, BiCGStab + Jacobi, update)."""
+    kr = dict(method="bicgstab", precond="jacobi", tol=1e-10, max_iters=3000)
+    kr.update(krylov or {})
+    reqs = sorted(requests, key=lambda r: r.arrival)
+    results = []
+    t0 = time.perf_counter()
+    for req in reqs:
+        if realtime:
+            wait = req.arrival - (time.perf_counter() - t0)
+            if wait > 0:
+                time.sleep(wait)
+        res = Result(req.rid, None, arrival=req.arrival, admitted=time.perf_counter() - t0)
+        ns = _new_handle(req, "fp64", use_specializations)
+        for _ in range(req.nsteps):
+            ts = time.perf_counter()
+            st = ns.execute(**kr)  # synchronises (the solve reads its status)
+            res.step_ms.append((time.perf_counter() - ts) * 1e3)
+            res.statuses.append(st)
+        res.state = ns.state()[0]
+        ns.close()
+        res.finished = time.perf_counter() - t0
+        results.append(res)
+    t_end = max(r.finished for r in results)
+    t_start = min(r.arrival for r in results) if realtime else 0.0
+    return sorted(results, key=lambda r: r.rid), summarize(results, t_start, t_end)

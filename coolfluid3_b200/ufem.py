@@ -218,6 +218,12 @@ class NavierStokes:
         N.check(self._lib.ufem_ns_device_view_get(self._h, C.byref(v)))
         return {k: getattr(v, k) for k, _ in v._fields_}
 
+    def device_bytes(self) -> int:
+        """Device memory held by this handle (bytes)."""
+        v = C.c_int64()
+        N.check(self._lib.ufem_ns_device_bytes(self._h, C.byref(v)))
+        return v.value
+
     # -- assembly kernel selection and autotuning -----------------------------
     ASSEMBLY_VARIANTS = {"warp": 0, "chunk": 1}
 

@@ -131,6 +131,8 @@ void ufem_krylov_default_opts(ufem_krylov_opts* opts);
 int ufem_ns_create(const ufem_mesh* mesh, const ufem_ns_options* opts, ufem_ns_handle** out);
 /* NavierStokes option triggers (trigger_assembly, NavierStokes.cpp:130-192). */
 int ufem_ns_set_options(ufem_ns_handle* h, const ufem_ns_options* opts);
+/* Device memory held by the handle (bytes, approximate to a few percent). */
+int ufem_ns_device_bytes(const ufem_ns_handle* h, int64_t* bytes);
 int ufem_ns_sizes(const ufem_ns_handle* h, int64_t* nb_rows, int64_t* nnz, int64_t* block_nnz);
 /* Host copies of the CSR pattern (rowptr nb_rows+1, colidx nnz). */
 int ufem_ns_csr(ufem_ns_handle* h, int64_t* rowptr, int32_t* colidx);
@@ -229,7 +231,10 @@ int ufem_ns_tune_assembly(ufem_ns_handle* h, void* stream, int32_t reps, int32_t
  * its results are bitwise the same alone and in any batch.  The iteration
  * blocks are replayed from captured CUDA graphs.  Members stay owned by the
  * caller and must outlive the batch; a member's BC list may change between
- * steps, its mesh may not.  mixed = 1 needs precision-1 members. */
+ * steps, its mesh may not.  mixed = 1 solves with an FP32 copy of each
+ * member's operator (allocated on first use, then written by every assembly),
+ * FP64 vectors and dot products, and FP64 refinement residuals of the
+ * assembled FP64 system. */
 typedef struct ufem_batch ufem_batch;
 int ufem_batch_create(ufem_ns_handle* const* members, int32_t n, ufem_batch** out);
 int ufem_batch_size(const ufem_batch* b, int32_t* n, int64_t* rows);

@@ -101,6 +101,18 @@ def test_mixed_batched_solve(specs):
         assert vec_rel_error(mixed[k], plain[k]) <= 1e-6
 
 
+@pytest.mark.parametrize("specs", [SIZES_2D, SIZES_3D])
+def test_mixed_batched_solve_fp64_elements(specs):
+    """FP64 element arithmetic, FP32 operator copy for the Krylov iterations,
+    FP64 refinement: the FP64 residual tolerance is met and the state agrees
+    with the plain FP64 batched solve to 1e-8 (both solved to 1e-12)."""
+    plain, _ = run_batch(specs, 2, tol=1e-12)
+    mixed, sts = run_batch(specs, 2, tol=1e-12, mixed=True, inner_tol=1e-6)
+    for k in range(len(specs)):
+        assert sts[-1][k]["converged"] and sts[-1][k]["rel_residual"] <= 1e-12
+        assert vec_rel_error(mixed[k], plain[k]) <= 1e-8
+
+
 def test_batch_rejects_incompatible_members():
     from coolfluid3_b200 import UfemError
     a = member(2, 4, 1)
