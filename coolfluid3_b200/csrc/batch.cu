@@ -13,7 +13,8 @@
 //    fixed order.  A member's arithmetic therefore depends only on its own
 //    data: its results are bitwise the same alone (a batch of one) and in any
 //    mix.  Converged members drop out (their kernels return at once) while the
-//    others continue.
+//    others continue.  The mixed-precision solve iterates with an FP32 copy of
+//    each operator and replaces the residual by the FP64 one every few blocks.
 // The iteration block (8 BiCGStab iterations) is captured once into a CUDA
 // graph and replayed; the host reads the members' done flags between blocks.
 #include <cuda_runtime.h>
@@ -38,9 +39,10 @@ constexpr int kMaxRestarts = 10;  // BiCGStab restarts after breakdowns in one s
 
 // per-mesh scalar slots (dctl[m * kDc + ...])
 constexpr int sBnorm = 0, sBeta = 1, sEst = 2, sRho = 5, sRhoOld = 6, sAlpha = 7, sOmega = 8, sTrue = 9,
-              sTol = 10, sTS = 11, sTT = 12;
+              sTol = 10, sTS = 11, sTT = 12, sLastTrue = 13;
 // per-mesh flags (ictl[m * kIc + ...])
-constexpr int fDone = 0, fStatus = 2, fIters = 3, fMaxit = 4, fOuter = 5;
+constexpr int fDone = 0, fStatus = 2, fIters = 3, fMaxit = 4, fOuter = 5, fFinal = 6, fRepl = 7;
+constexpr int kReplaceBlocks = 4;  // mixed solve: FP64 residual replacement every 4 blocks (32 iterations)
 
 struct BatchMesh {
   int64_t N, nrows, row_off;  // row_off: first row in the concatenated solver vectors
@@ -226,12 +228,13 @@ template <int NEQ, typename MT, int XL>
 __global__ void __launch_bounds__(256) spmv_batch_kernel(int64_t total_nodes, int nmesh,
                                                          const int64_t* __restrict__ node_prefix,
                                                          const BatchMesh* __restrict__ bm, double* xwork,
-                                                         double* __restrict__ ywork, const int* __restrict__ ictl) {
+                                                         double* __restrict__ ywork, const int* __restrict__ ictl,
+                                                         int skip_flag) {
   const int64_t gnode = (int64_t(blockIdx.x) * blockDim.x + threadIdx.x) >> 5;
   const int lane = threadIdx.x & 31;
   if (gnode >= total_nodes) return;
   const int m = find_mesh(node_prefix, nmesh, gnode);
-  if (ictl[m * kIc + fDone]) return;
+  if (ictl[m * kIc + skip_flag]) return;
   const BatchMesh& M = bm[m];
   const int64_t node = gnode - node_prefix[m];
   const double* x = vec<XL>(M, xwork);
@@ -350,10 +353,13 @@ __global__ void bicg_init_batch_kernel(int nmesh, const int* __restrict__ cprefi
   d[sAlpha] = 1.0;
   d[sOmega] = 1.0;
   d[sTol] = tol;
+  d[sLastTrue] = beta;
   f[fMaxit] = maxit;
   f[fIters] = 0;
   f[fStatus] = isfinite(beta) ? 0 : 3;
   f[fDone] = (f[fStatus] != 0 || beta <= tol * bnorm || bnorm == 0.0 || (use_outer && f[fOuter])) ? 1 : 0;
+  f[fFinal] = f[fDone];  // (residual replacement only visits meshes that are not final)
+  f[fRepl] = 0;
 }
 
 // p = r + beta (p - omega v), ph = D^-1 p
@@ -534,25 +540,72 @@ __global__ void true_res_batch_kernel(int nmesh, const int* __restrict__ cprefix
   dctl[m * kDc + sBnorm] = bn;
 }
 
-// Outer refinement bookkeeping: meshes whose FP64 residual meets `tol` (or is
-// not finite) are marked done for the rest of the refinement loop.
-__global__ void outer_mark_kernel(int nmesh, const double* __restrict__ dctl, int* __restrict__ ictl, double tol) {
-  const int m = blockIdx.x * blockDim.x + threadIdx.x;
-  if (m >= nmesh) return;
-  const double rr = dctl[m * kDc + sTrue];
-  if (!(rr > tol) || !isfinite(rr)) ictl[m * kIc + fOuter] = 1;
+// Mixed solve, FP64 residual replacement ("reliable update"): the iterations
+// apply the FP32 copy of the operator, whose rounding makes the recursive
+// residual drift from the true one; every few blocks r is replaced by the FP64
+// residual b - A x of the assembled FP64 system (x is kept in FP64), and rho =
+// rh . r is recomputed.  The Krylov directions are kept, so the iteration
+// count stays close to that of the FP64 solve while the answer is FP64's.
+template <int BL>
+__global__ void replace_batch_kernel(const Chunk* __restrict__ chunks, const BatchMesh* __restrict__ bm,
+                                     double* bwork, const double* __restrict__ w, double* __restrict__ r,
+                                     const double* __restrict__ rh, double* __restrict__ part, int nchunks,
+                                     const int* __restrict__ ictl) {
+  __shared__ double sm[32];
+  const Chunk c = chunks[blockIdx.x];
+  if (ictl[c.mesh * kIc + fFinal]) return;
+  const BatchMesh& M = bm[c.mesh];
+  const double* b = vec<BL>(M, bwork);
+  const int64_t off = M.row_off;
+  double rr = 0.0, hr = 0.0;
+  for (int i = c.lo + threadIdx.x; i < c.hi; i += blockDim.x) {
+    const double ri = b[i] - w[off + i];
+    r[off + i] = ri;
+    rr += ri * ri;
+    hr += rh[off + i] * ri;
+  }
+  rr = block_sum(rr, sm);
+  hr = block_sum(hr, sm);
+  if (threadIdx.x == 0) {
+    part[blockIdx.x] = rr;
+    part[nchunks + blockIdx.x] = hr;
+  }
 }
 
-// sol += corr for meshes still refining; corr = 0, res = r for the next pass.
-__global__ void add_corr_batch_kernel(const Chunk* __restrict__ chunks, const BatchMesh* __restrict__ bm,
-                                      double* __restrict__ corr, const int* __restrict__ outer_flags) {
-  const Chunk c = chunks[blockIdx.x];
-  if (outer_flags[c.mesh * kIc + fOuter]) return;
-  const BatchMesh& M = bm[c.mesh];
-  for (int i = c.lo + threadIdx.x; i < c.hi; i += blockDim.x) {
-    M.sol[i] += corr[M.row_off + i];
-    corr[M.row_off + i] = 0.0;
+// After a replacement: converged on the TRUE residual -> final; iteration
+// limit, breakdown or non-finite -> final with that status; otherwise go on
+// (also when the recursive residual had already claimed convergence).
+__global__ void replace_end_batch_kernel(int nmesh, const int* __restrict__ cprefix,
+                                         const double* __restrict__ part, int nchunks, double* __restrict__ dctl,
+                                         int* __restrict__ ictl) {
+  const int m = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  if (m >= nmesh || ictl[m * kIc + fFinal]) return;
+  double rr, hr;
+  fold2(part, nchunks, cprefix[m], cprefix[m + 1], rr, hr);
+  if ((threadIdx.x & 31) != 0) return;
+  double* d = dctl + m * kDc;
+  int* f = ictl + m * kIc;
+  const double rn = sqrt(rr);
+  d[sEst] = rn;
+  if (!isfinite(rn) || !isfinite(hr)) {
+    f[fStatus] = 3;
+    f[fDone] = f[fFinal] = 1;
+  } else if (rn <= d[sTol] * d[sBnorm]) {
+    f[fStatus] = 0;
+    f[fDone] = f[fFinal] = 1;
+  } else if (f[fDone] && f[fStatus] != 0) {  // iteration limit or breakdown
+    f[fFinal] = 1;
+  } else if (rn > 10.0 * d[sLastTrue]) {
+    // the true residual grew since the last replacement: treat as a breakdown,
+    // the solve restarts from this iterate
+    f[fStatus] = 2;
+    f[fDone] = f[fFinal] = 1;
+  } else {
+    d[sRho] = hr;
+    f[fDone] = 0;
   }
+  d[sLastTrue] = rn;
+  f[fRepl] += 1;
 }
 
 // x = 0 where b = 0 (the solution of A x = 0), as the one-mesh solver does.
@@ -615,7 +668,7 @@ struct ufem_batch {
   Chunk* d_chunks = nullptr;
   int* d_cprefix = nullptr;
   double *r = nullptr, *rh = nullptr, *p = nullptr, *v = nullptr, *s = nullptr, *t = nullptr, *ph = nullptr,
-         *sh = nullptr, *dinv = nullptr, *w = nullptr, *res = nullptr, *corr = nullptr;
+         *sh = nullptr, *dinv = nullptr, *w = nullptr;
   double* part = nullptr;
   double* dctl = nullptr;
   int* ictl = nullptr;
@@ -637,7 +690,7 @@ void batch_free(ufem_batch* b) {
   dfr(b->d_asm); dfr(b->d_gprefix); dfr(b->d_mesh); dfr(b->d_node_prefix); dfr(b->d_bc_prefix);
   dfr(b->d_fix_prefix); dfr(b->d_chunks); dfr(b->d_cprefix);
   dfr(b->r); dfr(b->rh); dfr(b->p); dfr(b->v); dfr(b->s); dfr(b->t); dfr(b->ph); dfr(b->sh); dfr(b->dinv);
-  dfr(b->w); dfr(b->res); dfr(b->corr); dfr(b->part); dfr(b->dctl); dfr(b->ictl);
+  dfr(b->w); dfr(b->part); dfr(b->dctl); dfr(b->ictl);
   if (b->h_dctl) cudaFreeHost(b->h_dctl);
   if (b->h_ictl) cudaFreeHost(b->h_ictl);
   delete b;
@@ -710,14 +763,14 @@ bool batch_dirty(const ufem_batch* b) {
 inline unsigned blocks_for(int64_t n, int threads) { return unsigned((n + threads - 1) / threads); }
 
 template <typename MT, int XL>
-int spmv_b(ufem_batch* b, double* x, double* y, cudaStream_t st) {
+int spmv_b(ufem_batch* b, double* x, double* y, cudaStream_t st, int skip_flag = fDone) {
   const unsigned grid = blocks_for(b->total_nodes * 32, 256);
   if (b->neq == 4)
     spmv_batch_kernel<4, MT, XL><<<grid, 256, 0, st>>>(b->total_nodes, b->nmesh, b->d_node_prefix, b->d_mesh, x, y,
-                                                       b->ictl);
+                                                       b->ictl, skip_flag);
   else
     spmv_batch_kernel<3, MT, XL><<<grid, 256, 0, st>>>(b->total_nodes, b->nmesh, b->d_node_prefix, b->d_mesh, x, y,
-                                                       b->ictl);
+                                                       b->ictl, skip_flag);
   UFEM_CUDA_TRY(cudaGetLastError());
   return UFEM_OK;
 }
@@ -761,19 +814,23 @@ int residual_b(ufem_batch* b, double* x, double* bw, bool init_rh, bool skip_don
 // BiCGStab over the batch.  MT: operator values; XL/BL: solution and RHS
 // locations; `use_outer`: skip meshes already converged in refinement.
 template <typename MT, int XL, int BL>
-int bicgstab_b(ufem_batch* b, int pkind, double tol, int maxit, bool use_outer, int slot, cudaStream_t st) {
+int bicgstab_b(ufem_batch* b, int pkind, double tol, int maxit, bool use_outer, int slot, cudaStream_t st,
+               bool reliable = false) {
   const unsigned nc = unsigned(b->nchunks);
   const unsigned gm = blocks_for(int64_t(b->nmesh) * 32, 256);
   int rc;
-  double* xw = XL == kWork ? b->corr : nullptr;
-  double* bw = BL == kWork ? b->res : nullptr;
+  double* xw = nullptr;  // solution and RHS are the members' own arrays (kSol, kRhs)
+  double* bw = nullptr;
   // every mesh takes part in the set-up (flags are reset by the init kernel)
   if (use_outer)  // flags prepared by the caller in the host mirror: fOuter set, the rest zero
     UFEM_CUDA_TRY(cudaMemcpyAsync(b->ictl, b->h_ictl, sizeof(int) * kIc * b->nmesh, cudaMemcpyHostToDevice, st));
   else
     UFEM_CUDA_TRY(cudaMemsetAsync(b->ictl, 0, sizeof(int) * kIc * b->nmesh, st));
   if (pkind == 1) jacobi_batch_kernel<MT><<<nc, kThreads, 0, st>>>(b->d_chunks, b->d_mesh, b->dinv, b->ictl);
-  if ((rc = residual_b<MT, XL, BL>(b, xw, bw, true, false, st))) return rc;
+  // the initial residual is FP64 in a mixed solve (residual replacement)
+  if ((rc = reliable ? residual_b<double, XL, BL>(b, xw, bw, true, false, st)
+                     : residual_b<MT, XL, BL>(b, xw, bw, true, false, st)))
+    return rc;
   zero_batch_kernel<<<nc, kThreads, 0, st>>>(b->d_chunks, b->d_mesh, b->p, b->v);
   bicg_init_batch_kernel<<<gm, 256, 0, st>>>(b->nmesh, b->d_cprefix, b->part, b->nchunks, b->dctl, b->ictl, tol,
                                              maxit, use_outer ? 1 : 0);
@@ -801,18 +858,35 @@ int bicgstab_b(ufem_batch* b, int pkind, double tol, int maxit, bool use_outer, 
     if (ie != cudaSuccess) return set_error(UFEM_ERR_CUDA, std::string("graph instantiate: ") + cudaGetErrorString(ie));
     b->block_pkind[slot] = pkind;
   }
-  for (int it = 0; it < maxit; it += kBlockIters) {
+  int blocks = 0;
+  for (int it = 0; it < maxit + kBlockIters; it += kBlockIters) {
     if (use_graph) {
       UFEM_CUDA_TRY(cudaGraphLaunch(b->block_exec[slot], st));
     } else {
       for (int k = 0; k < kBlockIters; ++k)
         if ((rc = bicg_iteration<MT, XL>(b, pkind, xw, st))) return rc;
     }
+    ++blocks;
     UFEM_CUDA_TRY(cudaMemcpyAsync(b->h_ictl, b->ictl, sizeof(int) * kIc * b->nmesh, cudaMemcpyDeviceToHost, st));
     UFEM_CUDA_TRY(cudaStreamSynchronize(st));
     bool all = true;
     for (int m = 0; m < b->nmesh && all; ++m) all = b->h_ictl[m * kIc + fDone] != 0;
-    if (all) break;
+    if (!reliable) {
+      if (all) break;
+      continue;
+    }
+    if (all || blocks % kReplaceBlocks == 0) {
+      if ((rc = spmv_b<double, XL>(b, xw, b->w, st, fFinal))) return rc;
+      replace_batch_kernel<BL><<<nc, kThreads, 0, st>>>(b->d_chunks, b->d_mesh, bw, b->w, b->r, b->rh, b->part,
+                                                       b->nchunks, b->ictl);
+      replace_end_batch_kernel<<<gm, 256, 0, st>>>(b->nmesh, b->d_cprefix, b->part, b->nchunks, b->dctl, b->ictl);
+      UFEM_CUDA_TRY(cudaGetLastError());
+      UFEM_CUDA_TRY(cudaMemcpyAsync(b->h_ictl, b->ictl, sizeof(int) * kIc * b->nmesh, cudaMemcpyDeviceToHost, st));
+      UFEM_CUDA_TRY(cudaStreamSynchronize(st));
+      bool fin = true;
+      for (int m = 0; m < b->nmesh && fin; ++m) fin = b->h_ictl[m * kIc + fFinal] != 0;
+      if (fin) break;
+    }
   }
   return UFEM_OK;
 }
@@ -879,10 +953,6 @@ int ufem_batch_create(ufem_ns_handle* const* members, int32_t n, ufem_batch** ou
       (rc = dmal(&b->ph, R)) || (rc = dmal(&b->sh, R)) || (rc = dmal(&b->dinv, R)) || (rc = dmal(&b->w, R)) ||
       (rc = dmal(&b->part, 2 * chunks.size())) || (rc = dmal(&b->dctl, size_t(kDc) * n)) ||
       (rc = dmal(&b->ictl, size_t(kIc) * n))) {
-    batch_free(b);
-    return rc;
-  }
-  if (b->precision == 1 && ((rc = dmal(&b->res, R)) || (rc = dmal(&b->corr, R)))) {
     batch_free(b);
     return rc;
   }
@@ -982,83 +1052,76 @@ int ufem_batch_solve(ufem_batch* b, const ufem_krylov_opts* kopts, ufem_krylov_s
         added = true;
       }
     if (added) {
-      if (b->res == nullptr && ((rc = dmal(&b->res, size_t(b->total_rows))) || (rc = dmal(&b->corr, size_t(b->total_rows)))))
-        return rc;
       UFEM_CUDA_TRY(cudaStreamSynchronize(st));
       if ((rc = batch_refresh(b))) return rc;
     }
-    if (b->res == nullptr && ((rc = dmal(&b->res, size_t(b->total_rows))) || (rc = dmal(&b->corr, size_t(b->total_rows)))))
-      return rc;
   }
-  std::vector<int> iters(b->nmesh, 0), status(b->nmesh, 0), refines(b->nmesh, 0);
-  if (!mixed) {
-    if ((rc = bicgstab_b<double, kSol, kRhs>(b, o.precond, o.tol, o.max_iters, false, 0, st))) return rc;
+  std::vector<int> iters(b->nmesh, 0), status(b->nmesh, 0), refines(b->nmesh, 0);  // refines: FP64 replacements
+  // Plain: FP64 operator.  Mixed: FP32 copy of the operator in the
+  // iterations, FP64 vectors, dot products and residual replacement.
+  auto run = [&](int maxit, bool outer) -> int {
+    return mixed ? bicgstab_b<float, kSol, kRhs>(b, o.precond, o.tol, maxit, outer, 1, st, true)
+                 : bicgstab_b<double, kSol, kRhs>(b, o.precond, o.tol, maxit, outer, 0, st, false);
+  };
+  if ((rc = run(o.max_iters, false))) return rc;
+  UFEM_CUDA_TRY(cudaMemcpyAsync(b->h_ictl, b->ictl, sizeof(int) * kIc * b->nmesh, cudaMemcpyDeviceToHost, st));
+  UFEM_CUDA_TRY(cudaStreamSynchronize(st));
+  for (int m = 0; m < b->nmesh; ++m) {
+    iters[m] = b->h_ictl[m * kIc + fIters];
+    status[m] = b->h_ictl[m * kIc + fStatus];
+    refines[m] = b->h_ictl[m * kIc + fRepl];
+  }
+  // members that broke down (rho or omega ~ 0) restart from their iterate;
+  // the others are held by their outer flag
+  for (int restart = 0; restart < kMaxRestarts; ++restart) {
+    int used = 0;
+    bool any = false;
+    for (int m = 0; m < b->nmesh; ++m)
+      if (status[m] == 2 && iters[m] < o.max_iters) {
+        any = true;
+        used = std::max(used, iters[m]);
+      }
+    if (!any) break;
+    for (int m = 0; m < b->nmesh; ++m) {
+      for (int q = 0; q < kIc; ++q) b->h_ictl[m * kIc + q] = 0;
+      b->h_ictl[m * kIc + fOuter] = (status[m] == 2 && iters[m] < o.max_iters) ? 0 : 1;
+    }
+    if ((rc = run(o.max_iters - used, true))) return rc;
     UFEM_CUDA_TRY(cudaMemcpyAsync(b->h_ictl, b->ictl, sizeof(int) * kIc * b->nmesh, cudaMemcpyDeviceToHost, st));
     UFEM_CUDA_TRY(cudaStreamSynchronize(st));
     for (int m = 0; m < b->nmesh; ++m) {
-      iters[m] = b->h_ictl[m * kIc + fIters];
+      if (b->h_ictl[m * kIc + fOuter]) continue;
+      iters[m] += b->h_ictl[m * kIc + fIters];
       status[m] = b->h_ictl[m * kIc + fStatus];
+      refines[m] += b->h_ictl[m * kIc + fRepl];
     }
-    // members that broke down (rho or omega ~ 0) restart from their iterate;
-    // the others are held by their outer flag
-    for (int restart = 0; restart < kMaxRestarts; ++restart) {
-      int used = 0;
-      bool any = false;
-      for (int m = 0; m < b->nmesh; ++m)
-        if (status[m] == 2 && iters[m] < o.max_iters) {
-          any = true;
-          used = std::max(used, iters[m]);
-        }
-      if (!any) break;
+  }
+  if (mixed) {
+    // members the FP32-operator iteration did not bring to the FP64 tolerance
+    // finish with the FP64 operator, from their current iterate
+    if ((rc = true_residual_b(b, st))) return rc;
+    UFEM_CUDA_TRY(cudaMemcpyAsync(b->h_dctl, b->dctl, sizeof(double) * kDc * b->nmesh, cudaMemcpyDeviceToHost, st));
+    UFEM_CUDA_TRY(cudaStreamSynchronize(st));
+    bool any = false;
+    std::vector<int> redo(b->nmesh, 0);
+    for (int m = 0; m < b->nmesh; ++m) {
+      const double rr = b->h_dctl[m * kDc + sTrue];
+      redo[m] = !(std::isfinite(rr) && rr <= o.tol) && std::isfinite(rr) ? 1 : 0;
+      any = any || redo[m];
+    }
+    if (any) {
       for (int m = 0; m < b->nmesh; ++m) {
         for (int q = 0; q < kIc; ++q) b->h_ictl[m * kIc + q] = 0;
-        b->h_ictl[m * kIc + fOuter] = (status[m] == 2 && iters[m] < o.max_iters) ? 0 : 1;
+        b->h_ictl[m * kIc + fOuter] = redo[m] ? 0 : 1;
       }
-      if ((rc = bicgstab_b<double, kSol, kRhs>(b, o.precond, o.tol, o.max_iters - used, true, 0, st))) return rc;
+      if ((rc = bicgstab_b<double, kSol, kRhs>(b, o.precond, o.tol, o.max_iters, true, 0, st, false))) return rc;
       UFEM_CUDA_TRY(cudaMemcpyAsync(b->h_ictl, b->ictl, sizeof(int) * kIc * b->nmesh, cudaMemcpyDeviceToHost, st));
       UFEM_CUDA_TRY(cudaStreamSynchronize(st));
       for (int m = 0; m < b->nmesh; ++m) {
-        if (b->h_ictl[m * kIc + fOuter]) continue;
+        if (!redo[m]) continue;
         iters[m] += b->h_ictl[m * kIc + fIters];
         status[m] = b->h_ictl[m * kIc + fStatus];
       }
-    }
-  } else {
-    // FP64 refinement: r = b - A64 x; inner BiCGStab on A32 d = r (FP64
-    // vectors and scalars), x += d; meshes leave the loop once converged.
-    std::vector<int> outer(b->nmesh, 0);
-    const int inner_cap = std::min(o.max_iters, 400);
-    for (int ref = 0; ref <= o.max_refine; ++ref) {
-      if ((rc = true_residual_b(b, st))) return rc;
-      outer_mark_kernel<<<blocks_for(b->nmesh, 128), 128, 0, st>>>(b->nmesh, b->dctl, b->ictl, o.tol);
-      UFEM_CUDA_TRY(cudaGetLastError());
-      UFEM_CUDA_TRY(cudaMemcpyAsync(b->h_ictl, b->ictl, sizeof(int) * kIc * b->nmesh, cudaMemcpyDeviceToHost, st));
-      UFEM_CUDA_TRY(cudaStreamSynchronize(st));
-      bool all = true;
-      for (int m = 0; m < b->nmesh; ++m) {
-        outer[m] = outer[m] || b->h_ictl[m * kIc + fOuter];
-        all = all && outer[m];
-      }
-      if (all || ref == o.max_refine) break;
-      // res = r (the residual just formed), corr = 0; inner solve on the rest
-      UFEM_CUDA_TRY(cudaMemcpyAsync(b->res, b->r, sizeof(double) * b->total_rows, cudaMemcpyDeviceToDevice, st));
-      zero_batch_kernel<<<unsigned(b->nchunks), kThreads, 0, st>>>(b->d_chunks, b->d_mesh, b->corr, nullptr);
-      for (int m = 0; m < b->nmesh; ++m) {
-        for (int q = 0; q < kIc; ++q) b->h_ictl[m * kIc + q] = 0;
-        b->h_ictl[m * kIc + fOuter] = outer[m];
-      }
-      if ((rc = bicgstab_b<float, kWork, kWork>(b, o.precond, o.inner_tol, inner_cap, true, 1, st))) return rc;
-      UFEM_CUDA_TRY(cudaMemcpyAsync(b->h_ictl, b->ictl, sizeof(int) * kIc * b->nmesh, cudaMemcpyDeviceToHost, st));
-      UFEM_CUDA_TRY(cudaStreamSynchronize(st));
-      for (int m = 0; m < b->nmesh; ++m) {
-        if (outer[m]) continue;
-        iters[m] += b->h_ictl[m * kIc + fIters];
-        refines[m] = ref + 1;
-        if (b->h_ictl[m * kIc + fStatus] == 3) status[m] = 3;
-      }
-      // apply the corrections (outer flags on the device still hold `outer`)
-      add_corr_batch_kernel<<<unsigned(b->nchunks), kThreads, 0, st>>>(b->d_chunks, b->d_mesh, b->corr, b->ictl);
-      UFEM_CUDA_TRY(cudaGetLastError());
     }
   }
   // final FP64 residuals

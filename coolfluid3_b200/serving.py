@@ -11,11 +11,14 @@ steps) arrive over time.  The server
     on a pool of host threads while the GPU keeps stepping the others, and
     keeps mesh, pattern and state resident on the device until the request
     completes;
-  * batches continuously: one worker per mesh dimension steps ALL its active
-    requests together every tick (one batched assembly launch, one batched
-    BiCGStab with per-request scalars, see ``ufem.Batch``) on its own CUDA
-    stream, so 2D and 3D work overlaps on the device; requests that arrive
-    while others run join at the next tick, finished ones leave;
+  * batches continuously: requests below `large_rows` rows are stepped
+    together by one worker per mesh dimension every tick (one batched
+    assembly launch, one batched BiCGStab with per-request scalars, see
+    ``ufem.Batch``); larger requests, whose solves already fill the GPU, run
+    one per worker on `large_workers` further workers so that they do not hold
+    back the small ones.  Every worker has its own CUDA stream, so the classes
+    overlap on the device; requests that arrive while others run join at the
+    next tick, finished ones leave;
   * reports throughput (time steps per second) beside p50/p99 step latency
     and request latency.
 
@@ -110,14 +113,16 @@ def make_request(rid: int, dim: int, n_elems: float, nu: float, seed: int, nstep
 def poisson_workload(n: int, rate: float, elems=(1e4, 2e6), nu=(1e-4, 1e-1), dims=(2, 3), nsteps: int = 10,
                      seed: int = 20261203) -> list[Request]:
     """Seeded synthetic serving workload: Poisson arrivals at `rate` per second,
-    element counts and viscosities log-uniform, dimensions drawn uniformly."""
+    element counts and viscosities log-uniform, dimensions drawn uniformly.
+    `elems` is one (low, high) range or a {dim: (low, high)} mapping."""
     rng = np.random.default_rng(seed)
     t = 0.0
     out = []
     for k in range(n):
         t += rng.exponential(1.0 / rate)
         dim = int(rng.choice(dims))
-        e = math.exp(rng.uniform(math.log(elems[0]), math.log(elems[1])))
+        lo, hi = elems[dim] if isinstance(elems, dict) else elems
+        e = math.exp(rng.uniform(math.log(lo), math.log(hi)))
         v = math.exp(rng.uniform(math.log(nu[0]), math.log(nu[1])))
         out.append(make_request(k, dim, e, v, seed + 7 * k + 1, nsteps, t))
     return out
@@ -165,7 +170,8 @@ class Server:
 
     def __init__(self, hbm_budget_bytes: int, max_slots: int = 64, precision: str = "fp64", mixed: bool = True,
                  krylov: dict | None = None, graphs: bool = True, creators: int = 2,
-                 use_specializations: bool = False, realtime: bool = True):
+                 use_specializations: bool = False, realtime: bool = True, large_rows: int = 200_000,
+                 large_workers: int = 2):
         if precision not in ("fp32", "fp64"):
             raise ValueError("precision must be fp32 or fp64")
         self.budget = int(hbm_budget_bytes)
@@ -175,6 +181,8 @@ class Server:
         self.creators = creators
         self.spec = use_specializations
         self.realtime = realtime
+        self.large_rows = int(large_rows)
+        self.large_workers = int(large_workers)
         self.krylov = dict(method="bicgstab", precond="jacobi", tol=1e-10, max_iters=3000)
         if mixed:
             self.krylov.update(mixed=True, inner_tol=1e-6, max_refine=20)
@@ -215,13 +223,15 @@ class Server:
         for r in reqs:
             if estimate_bytes(r, self.precision) > self.budget:
                 raise ValueError(f"request {r.rid} alone exceeds the HBM budget")
-        inbox = {2: deque(), 3: deque()}
+        # queues: (dim, "small") feeds one batching worker per dimension;
+        # (dim, "large") feeds `large_workers` workers that run one request each
+        inbox = {(d, c): deque() for d in (2, 3) for c in ("small", "large")}
         results: list[Result] = []
         state = {"open": len(reqs)}
         t0 = time.perf_counter()
         now = lambda: time.perf_counter() - t0  # noqa: E731
 
-        def worker(dim: int):
+        def worker(key: tuple, capacity: int):
             stream = torch.cuda.Stream()
             active: list[_Active] = []
             batch = None
@@ -229,12 +239,12 @@ class Server:
             try:
                 while True:
                     with self._lock:
-                        while not inbox[dim] and not active and state["open"] > 0:
+                        while not inbox[key] and not active and state["open"] > 0:
                             self._lock.wait(0.05)
-                        if not inbox[dim] and not active and state["open"] <= 0:
+                        if not inbox[key] and not active and state["open"] <= 0:
                             break
-                        while inbox[dim]:
-                            active.append(inbox[dim].popleft())
+                        while inbox[key] and len(active) < capacity:
+                            active.append(inbox[key].popleft())
                     if not active:
                         continue
                     ids = tuple(id(a.ns) for a in active)
@@ -293,10 +303,13 @@ class Server:
             self._adjust(est, actual)
             a = _Active(req, ns, admitted, actual)
             with self._lock:
-                inbox[req.dim].append(a)
+                cls = "large" if ns.nb_rows >= self.large_rows else "small"
+                inbox[(req.dim, cls)].append(a)
                 self._lock.notify_all()
 
-        workers = [threading.Thread(target=worker, args=(d,), daemon=True) for d in (2, 3)]
+        workers = [threading.Thread(target=worker, args=((d, "small"), self.max_slots), daemon=True) for d in (2, 3)]
+        workers += [threading.Thread(target=worker, args=((d, "large"), 1), daemon=True)
+                    for d in (2, 3) for _ in range(self.large_workers)]
         for w in workers:
             w.start()
         pool = ThreadPoolExecutor(max_workers=self.creators)
@@ -360,7 +373,10 @@ def run_plain(requests: list[Request], krylov: dict | None = None, realtime: boo
         ns = _new_handle(req, "fp64", use_specializations)
         for _ in range(req.nsteps):
             ts = time.perf_counter()
-            st = ns.execute(**kr)  # synchronises (the solve reads its status)
+            ns.assemble()
+            ns.apply_dirichlet()
+            st = ns.solve(raise_on_failure=False, **kr)  # synchronises (the solve reads its status)
+            ns.update()
             res.step_ms.append((time.perf_counter() - ts) * 1e3)
             res.statuses.append(st)
         res.state = ns.state()[0]

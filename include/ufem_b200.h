@@ -231,10 +231,11 @@ int ufem_ns_tune_assembly(ufem_ns_handle* h, void* stream, int32_t reps, int32_t
  * its results are bitwise the same alone and in any batch.  The iteration
  * blocks are replayed from captured CUDA graphs.  Members stay owned by the
  * caller and must outlive the batch; a member's BC list may change between
- * steps, its mesh may not.  mixed = 1 solves with an FP32 copy of each
+ * steps, its mesh may not.  mixed = 1 iterates with an FP32 copy of each
  * member's operator (allocated on first use, then written by every assembly),
- * FP64 vectors and dot products, and FP64 refinement residuals of the
- * assembled FP64 system. */
+ * FP64 vectors and dot products, and replaces the recursive residual by the
+ * FP64 residual of the assembled FP64 system every 32 iterations and before
+ * accepting convergence (status.refinements counts the replacements). */
 typedef struct ufem_batch ufem_batch;
 int ufem_batch_create(ufem_ns_handle* const* members, int32_t n, ufem_batch** out);
 int ufem_batch_size(const ufem_batch* b, int32_t* n, int64_t* rows);

@@ -6,7 +6,8 @@ are; the batched assembly agrees with the one-mesh kernel to 1e-14 of each
 CSR row's largest entry (the same element code compiled into two kernels);
 batched solves agree with the one-mesh solver within 1e-6 relative and reach
 the FP64 residual tolerance; the mixed batched solve (FP32 operator, FP64
-vectors, FP64 refinement) meets the same residual and agrees within 1e-6.
+vectors, FP64 residual replacement) meets the same residual and agrees within
+1e-6.
 """
 import numpy as np
 import pytest
@@ -94,23 +95,26 @@ def test_batched_step_matches_single_handle(specs):
 
 @pytest.mark.parametrize("specs", [SIZES_2D, SIZES_3D])
 def test_mixed_batched_solve(specs):
-    plain, _ = run_batch(specs, 1, precision="fp32", tol=1e-10)
-    mixed, sts = run_batch(specs, 1, precision="fp32", tol=1e-10, mixed=True)
+    """FP32 elements; the mixed solve (FP32 operator, FP64 residual
+    replacement) against the FP64-operator solve, both to 1e-12."""
+    plain, _ = run_batch(specs, 1, precision="fp32", tol=1e-12)
+    mixed, sts = run_batch(specs, 1, precision="fp32", tol=1e-12, mixed=True)
     for k in range(len(specs)):
-        assert sts[0][k]["converged"] and sts[0][k]["rel_residual"] <= 1e-10
+        assert sts[0][k]["converged"] and sts[0][k]["rel_residual"] <= 1e-12
+        assert sts[0][k]["refinements"] >= 1  # convergence is accepted on the FP64 residual
         assert vec_rel_error(mixed[k], plain[k]) <= 1e-6
 
 
 @pytest.mark.parametrize("specs", [SIZES_2D, SIZES_3D])
 def test_mixed_batched_solve_fp64_elements(specs):
     """FP64 element arithmetic, FP32 operator copy for the Krylov iterations,
-    FP64 refinement: the FP64 residual tolerance is met and the state agrees
-    with the plain FP64 batched solve to 1e-8 (both solved to 1e-12)."""
+    FP64 residual replacement: the FP64 residual tolerance is met and the
+    state agrees with the plain FP64 batched solve to 1e-7 (both to 1e-12)."""
     plain, _ = run_batch(specs, 2, tol=1e-12)
-    mixed, sts = run_batch(specs, 2, tol=1e-12, mixed=True, inner_tol=1e-6)
+    mixed, sts = run_batch(specs, 2, tol=1e-12, mixed=True)
     for k in range(len(specs)):
         assert sts[-1][k]["converged"] and sts[-1][k]["rel_residual"] <= 1e-12
-        assert vec_rel_error(mixed[k], plain[k]) <= 1e-8
+        assert vec_rel_error(mixed[k], plain[k]) <= 1e-7
 
 
 def test_batch_rejects_incompatible_members():
