@@ -54,6 +54,8 @@ def parse():
     ap.add_argument("--precision", default="fp64", choices=["fp64", "fp32"])
     ap.add_argument("--asm-kernel", default="auto", choices=["auto", "warp", "chunk"],
                     help="assembly kernel variant; auto = the library's autotuner picks it on this mesh")
+    ap.add_argument("--asm-warps", type=int, default=4, choices=[2, 4, 8],
+                    help="warps per CTA of the warp assembly kernel when --asm-kernel is given")
     ap.add_argument("--specialized", action="store_true", help="use the closed-form specialised kernels")
     ap.add_argument("--no-extras", action="store_true", help="skip CPU baseline and time-step extras")
     ap.add_argument("--time-steps", type=int, default=2, help="full time steps timed per solver variant")
@@ -229,7 +231,7 @@ def run_ours(args, rank, world, local):
     if args.asm_kernel == "auto":
         tuned = ns.tune_assembly(reps=3, stream=sptr)
     else:
-        ns.set_assembly_kernel(args.asm_kernel, 4)
+        ns.set_assembly_kernel(args.asm_kernel, args.asm_warps)
         tuned = None
     asm_variant, asm_warps = ns.assembly_kernel()
     big_rows = int((np.bincount(pb.conn.ravel(), minlength=Nn) > 32).sum())
