@@ -86,13 +86,21 @@ def dist_init(ngpus):
 
 
 def max_over_ranks(x: float, world: int) -> float:
+    """Max of a per-rank time over the job (NCCL on GPUs, gloo on CPU)."""
     if world <= 1:
         return x
     import torch
     import torch.distributed as dist
-    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dev = "cuda" if dist.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([x], dtype=torch.float64, device=dev)
     dist.all_reduce(t, op=dist.ReduceOp.MAX)
     return float(t.item())
+
+
+def replica_value(units_per_rank: float, ms_max: float, world: int) -> float:
+    """Whole-job throughput of N independent replicas: all ranks' units over
+    the max-over-ranks time (millions of units per second)."""
+    return units_per_rank * world / (ms_max / 1e3) / 1e6
 
 
 def barrier(world):
@@ -266,7 +274,7 @@ def run_ours(args, rank, world, local):
     torch.cuda.synchronize()
     step_ms = [s.elapsed_time(e) for s, e in zip(starts, ends)]
     ms = max_over_ranks(float(np.mean(step_ms)), world)
-    value = E * world / (ms / 1e3) / 1e6
+    value = replica_value(E, ms, world)
     kern_ms = float(np.mean(kernel_ms))
     B = algorithmic_bytes(E, Nn, ns.nnz, dim)
     peak, peak_kind = measured_peak()

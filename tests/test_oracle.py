@@ -114,6 +114,35 @@ def test_symmetric_dirichlet_reference_kat():
     assert s.solution()[1] == 10.0
 
 
+def test_symmetric_dirichlet_golden_fixture():
+    """The same known-answer test, every check taken from the committed
+    fixture that tests/golden/make_golden.py extracted from the reference's
+    test source (global node ids, the reference's get_value column-first order
+    already resolved)."""
+    import json
+    import os
+    kat = json.load(open(os.path.join(os.path.dirname(__file__), "golden", "lss_symmetric_dirichlet_kat.json")))
+    n = kat["nodes"]
+    start = [0]
+    adj = []
+    for i in range(n):
+        nb = [j for j in (i - 1, i, i + 1) if 0 <= j < n]
+        adj += nb
+        start.append(len(adj))
+    s = O.LSS(np.array(start), np.array(adj, np.uint32), kat["neq"])
+    for r in range(n):
+        s.set_row(r, 0, kat["set_row"]["diag"], kat["set_row"]["offdiag"])
+    d = kat["dirichlet"]
+    s.symmetric_dirichlet(d["node"], d["eq"], d["value"])
+    A = s.dense()
+    _, rhs = s.system()
+    assert len(kat["matrix_checks"]) == 10 and len(kat["rhs_checks"]) == 5
+    for c in kat["matrix_checks"]:
+        assert A[c["row"], c["col"]] == c["value"], c
+    for c in kat["rhs_checks"]:
+        assert rhs[c["row"]] == c["value"], c
+
+
 def _parallel_dirichlet(rowptr, colidx, vals, rhs, sol, state_flat, nodes, comps, values, neq):
     """The order-preserving parallel form the GPU applies (see csrc/host.cu)."""
     dof = nodes.astype(np.int64) * neq + comps
