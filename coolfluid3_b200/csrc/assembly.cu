@@ -985,15 +985,30 @@ constexpr int warp_lane_pitch() {
 
 constexpr size_t kDescSlot = (sizeof(AsmDesc) + 15) / 16 * 16;
 
-template <int D, typename T>
+// KC: lanes that evaluate incidences (group capacity); the staging holds KC lanes.
+template <int D, typename T, int KC = 32, bool BATCH = false>
 constexpr size_t warp_stage_bytes() {
-  return size_t(32) * warp_lane_pitch<D, T>() * sizeof(T) +  // staged row blocks + RHS rows, one slice per lane
+  return size_t(KC) * warp_lane_pitch<D, T>() * sizeof(T) +  // staged row blocks + RHS rows, one slice per lane
          size_t(D * 64 + 32 + 36 + 36) * 4 +                  // slot masks per local position, pslots, prefix, offsets
-         2 * kDescSlot;                                       // descriptors of the current and the next mesh
+         (BATCH ? 2 * kDescSlot : 0);                         // batch: descriptors of the current and next mesh
 }
 static_assert(warp_stage_bytes<2, float>() % 16 == 0 && warp_stage_bytes<2, double>() % 16 == 0 &&
-                  warp_stage_bytes<3, float>() % 16 == 0 && warp_stage_bytes<3, double>() % 16 == 0,
+                  warp_stage_bytes<3, float>() % 16 == 0 && warp_stage_bytes<3, double>() % 16 == 0 &&
+                  warp_stage_bytes<3, float, 24>() % 16 == 0 && warp_stage_bytes<3, double, 24>() % 16 == 0 &&
+                  warp_stage_bytes<2, float, 32, true>() % 16 == 0 && warp_stage_bytes<2, double, 32, true>() % 16 == 0 &&
+                  warp_stage_bytes<3, float, 32, true>() % 16 == 0 && warp_stage_bytes<3, double, 32, true>() % 16 == 0,
               "per-warp staging slices must stay 16-byte aligned");
+
+// Resident-CTA hints (register budgets) of the 24-lane tetrahedron variants,
+// matched to the warps their smaller staging lets an SM hold: FP64 16 warps
+// (<= 128 registers), FP32 20 warps (<= 102).  The 32-lane variants keep the
+// compiler's choice (their staging caps the warps anyway).
+template <int D, typename T, int KC, int WPB>
+constexpr int warp_min_blocks() {
+  if (D != 3 || KC == 32) return 0;  // 0: no hint
+  const int warps = sizeof(T) == 8 ? 16 : 20;
+  return warps / WPB > 0 ? warps / WPB : 1;
+}
 
 // Loads NV consecutive staged values (16-byte aligned when NV is a multiple of 4).
 template <int NV, typename T>
@@ -1016,11 +1031,15 @@ __device__ __forceinline__ void load_run(const T* __restrict__ src, T (&v)[NV]) 
   }
 }
 
-template <int D, typename T, bool SPEC, int WPB, bool BATCH>
-__global__ void __launch_bounds__(32 * WPB) ns_assembly_warp_kernel(int ngroups, int nmesh,
-                                                                     const AsmDesc* __restrict__ descs,
-                                                                     const int* __restrict__ gprefix,
-                                                                     const __grid_constant__ AsmDesc one) {
+template <int D, typename T, bool SPEC, int WPB, bool BATCH, int KC>
+__global__ void __launch_bounds__(32 * WPB, warp_min_blocks<D, T, KC, WPB>()) ns_assembly_warp_kernel(
+    int ngroups, int nmesh, const AsmDesc* __restrict__ descs, const int* __restrict__ gprefix,
+    // one-mesh launch (BATCH false): the mesh's arrays as separate parameters
+    const int4* __restrict__ groups_1, const int32_t* __restrict__ row_inc_1, const int32_t* __restrict__ inc_elem_1,
+    const uint32_t* __restrict__ inc_info_1, const int4* __restrict__ conn_1, const double* __restrict__ coords_1,
+    const double* __restrict__ uadv_1, const double* __restrict__ state_1, const float* __restrict__ node32_1,
+    const double* __restrict__ force_1, const int64_t* __restrict__ start_1, NSParams p_1,
+    double* __restrict__ vals_1, float* __restrict__ vals32_1, double* __restrict__ rhs_1) {
   constexpr int n = P1<D>::n, neq = P1<D>::neq, nvals = P1<D>::nvals;
   constexpr int LS = warp_lane_pitch<D, T>();
   constexpr int RPI = (D == 3) ? 2 : 3;      // equations (CSR rows) per off-diagonal item
@@ -1029,8 +1048,8 @@ __global__ void __launch_bounds__(32 * WPB) ns_assembly_warp_kernel(int ngroups,
   constexpr unsigned FULL = 0xffffffffu;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  T* stage = reinterpret_cast<T*>(smem_raw + size_t(warp) * warp_stage_bytes<D, T>());
-  uint32_t* s_mask = reinterpret_cast<uint32_t*>(stage + 32 * LS);  // D x 64: local position 1..n-1, slot
+  T* stage = reinterpret_cast<T*>(smem_raw + size_t(warp) * warp_stage_bytes<D, T, KC, BATCH>());
+  uint32_t* s_mask = reinterpret_cast<uint32_t*>(stage + KC * LS);  // D x 64: local position 1..n-1, slot
   uint32_t* s_pslots = s_mask + D * 64;                              // 32
   int* s_pref = reinterpret_cast<int*>(s_pslots + 32);               // 33 (+3 pad)
   int* s_off = s_pref + 36;                                          // 33 (+3 pad): lane offset of each row
@@ -1052,9 +1071,9 @@ __global__ void __launch_bounds__(32 * WPB) ns_assembly_warp_kernel(int ngroups,
       }
     }
   };
-  auto desc = [&](int slot) -> const AsmDesc& {
-    if constexpr (BATCH) return s_desc[slot]; else return one;
-  };
+  // Field f of the mesh in descriptor slot `slot`: a batch reads its shared
+  // descriptor copy, a one-mesh launch its own parameters.
+#define UFEM_F(slot, f) (BATCH ? s_desc[(slot)].f : f##_1)
 
   // Persistent warps: a warp walks the global groups g, g + stride, ... of all
   // meshes of the launch (mesh m owns groups [gprefix[m], gprefix[m + 1])).
@@ -1076,33 +1095,38 @@ __global__ void __launch_bounds__(32 * WPB) ns_assembly_warp_kernel(int ngroups,
   int cs = 0;  // descriptor slot of the current mesh
   load_desc(cm, cs);
   // first row, end row, first incidence, incidences
-  int4 G = __ldg(desc(cs).groups + (g - (BATCH ? __ldg(gprefix + cm) : 0)));
+  int4 G = BATCH ? __ldg(UFEM_F(cs, groups) + (g - __ldg(gprefix + cm))) : groups_1[g];
   int pe = 0, poff = 0, pitems = 0;
   uint32_t pinfo = 0;
   int4 pcn = make_int4(0, 0, 0, 0);
-  auto fetch_records = [&](const int4& q, const AsmDesc& d) {
+  auto fetch_records = [&](const int4& q, const int32_t* inc_elem, const uint32_t* inc_info,
+                           const int32_t* row_inc, const int64_t* start) {
     if (lane < q.w) {
-      pe = __ldg(d.inc_elem + q.z + lane);
-      pinfo = __ldg(d.inc_info + q.z + lane);
+      pe = __ldg(inc_elem + q.z + lane);
+      pinfo = __ldg(inc_info + q.z + lane);
     }
     if (lane < q.y - q.x) {
-      poff = __ldg(d.row_inc + q.x + lane) - q.z;
-      pitems = int(__ldg(d.start + q.x + lane + 1) - __ldg(d.start + q.x + lane) - 1) * RG;
+      poff = __ldg(row_inc + q.x + lane) - q.z;
+      pitems = int(__ldg(start + q.x + lane + 1) - __ldg(start + q.x + lane) - 1) * RG;
     }
   };
-  fetch_records(G, desc(cs));
-  if (lane < G.w) pcn = __ldg(desc(cs).conn + pe);
+  fetch_records(G, UFEM_F(cs, inc_elem), UFEM_F(cs, inc_info), UFEM_F(cs, row_inc), UFEM_F(cs, start));
+  if (lane < G.w) pcn = __ldg(UFEM_F(cs, conn) + pe);
   for (;;) {
-    const int row0 = G.x, R = G.y - G.x, K = G.w;  // 1 <= R <= K <= 32
+    const int row0 = G.x, R = G.y - G.x, K = G.w;  // 1 <= R <= K <= KC
     const int gn = g + gstride;
     const int mn = (BATCH && gn < ngroups) ? mesh_of(gn) : cm;
     const int ns = (mn == cm) ? cs : 1 - cs;  // descriptor slot of the next group's mesh
+    int4 Gn = make_int4(0, 0, 0, 0);
+    if constexpr (!BATCH) {
+      if (gn < ngroups) Gn = groups_1[gn];
+    }
     __syncwarp();  // the previous group's reads of the shared slice are complete
-    load_desc(mn, ns);
-    const int4 Gn = gn < ngroups ? __ldg(desc(ns).groups + (gn - (BATCH ? __ldg(gprefix + mn) : 0)))
-                                 : make_int4(0, 0, 0, 0);
-    const AsmDesc& dc = desc(cs);
-    const int64_t* __restrict__ start = dc.start;
+    if constexpr (BATCH) {
+      load_desc(mn, ns);
+      if (gn < ngroups) Gn = __ldg(s_desc[ns].groups + (gn - __ldg(gprefix + mn)));
+    }
+    const int64_t* __restrict__ start = UFEM_F(cs, start);
     int pref = lane < R ? pitems : 0;  // inclusive scan of the off-diagonal item counts
 #pragma unroll
     for (int o = 1; o < 32; o <<= 1) {
@@ -1141,23 +1165,24 @@ __global__ void __launch_bounds__(32 * WPB) ns_assembly_warp_kernel(int ngroups,
         pslots |= sl << (8 * q);
       }
       T* st = stage + lane * LS;
-      const KParams<T> kp = make_kparams<T>(dc.p);
-      const NodeData nd{dc.coords, dc.uadv, dc.state, dc.node32};
+      const KParams<T> kp = make_kparams<T>(UFEM_F(cs, p));
+      const NodeData nd{UFEM_F(cs, coords), UFEM_F(cs, uadv), UFEM_F(cs, state), UFEM_F(cs, node32)};
       if constexpr (SPEC) {
         if constexpr (D == 2) spec_tri_row<T>(ids, a, nd, kp, st, st + nvals, 1);
         else spec_tet_row<T>(ids, a, nd, kp, st, st + nvals, 1);
       } else {
-        generic_row<D, T>(ids, a, nd, dc.force, kp, st, st + nvals, 1);
+        generic_row<D, T>(ids, a, nd, UFEM_F(cs, force), kp, st, st + nvals, 1);
       }
 #pragma unroll
       for (int q = 1; q < n; ++q) atomicOr(s_mask + (q - 1) * 64 + ((pslots >> (8 * q)) & 0xFFu), 1u << lane);
     }
     s_pslots[lane] = pslots;
     __syncwarp();
-    fetch_records(Gn, desc(ns));  // next group's records load while this group is reduced
-    double* __restrict__ vals = dc.vals;
-    float* __restrict__ vals32 = dc.vals32;
-    double* __restrict__ rhs = dc.rhs;
+    fetch_records(Gn, UFEM_F(ns, inc_elem), UFEM_F(ns, inc_info), UFEM_F(ns, row_inc),
+                  UFEM_F(ns, start));  // next group's records load while this group is reduced
+    double* __restrict__ vals = UFEM_F(cs, vals);
+    float* __restrict__ vals32 = UFEM_F(cs, vals32);
+    double* __restrict__ rhs = UFEM_F(cs, rhs);
 
     // Phase 2a: diagonal entries and RHS entries, neq * (neq + 1) items per row,
     // each the sum over the row's lanes in element order.
@@ -1182,7 +1207,7 @@ __global__ void __launch_bounds__(32 * WPB) ns_assembly_warp_kernel(int ngroups,
       }
     }
 
-    if (lane < Gn.w) pcn = __ldg(desc(ns).conn + pe);
+    if (lane < Gn.w) pcn = __ldg(UFEM_F(ns, conn) + pe);
 
     // Phase 2b: off-diagonal items (row, slot != self, group of RPI equations):
     // the contributors of slot s are the row's lanes holding s at local position
@@ -1246,6 +1271,7 @@ __global__ void __launch_bounds__(32 * WPB) ns_assembly_warp_kernel(int ngroups,
     cm = mn;
     cs = ns;
   }
+#undef UFEM_F
 }
 
 // LinearizeU (NavierStokes.cpp:105), evaluated left to right without FMA
@@ -1392,7 +1418,7 @@ void fill_params(const ufem_ns_handle* h, NSParams& p) {
   p.has_force = h->d_force != nullptr;
 }
 
-void fill_desc(const ufem_ns_handle* h, bool write32, AsmDesc& d) {
+void fill_desc(const ufem_ns_handle* h, bool write32, AsmDesc& d, const WarpPlan* plan) {
   d.coords = h->d_coords;
   d.uadv = h->d_uadv;
   d.state = h->d_state;
@@ -1403,7 +1429,7 @@ void fill_desc(const ufem_ns_handle* h, bool write32, AsmDesc& d) {
   d.inc_elem = h->d_inc_elem;
   d.inc_info = h->d_inc_info;
   d.conn = reinterpret_cast<const int4*>(h->d_conn);
-  d.groups = h->wplan.groups;
+  d.groups = (plan ? plan : &h->wplan)->groups;
   d.vals = h->d_vals;
   d.vals32 = write32 ? h->d_vals32 : nullptr;
   d.rhs = h->d_rhs;
@@ -1438,26 +1464,28 @@ int resident_ctas(K kernel, int threads, size_t smem) {
   return sms * per_sm;
 }
 
-template <int D, typename T, bool SPEC, int WPB, bool BATCH>
+template <int D, typename T, bool SPEC, int WPB, bool BATCH, int KC>
 int launch_warp_t(int ngroups, int nmesh, const AsmDesc* descs, const int* gprefix, const AsmDesc& one,
                   cudaStream_t s) {
   if (ngroups == 0) return UFEM_OK;
-  constexpr size_t smem = warp_stage_bytes<D, T>() * WPB;
-  static const int resident = resident_ctas(ns_assembly_warp_kernel<D, T, SPEC, WPB, BATCH>, 32 * WPB, smem);
+  constexpr size_t smem = warp_stage_bytes<D, T, KC, BATCH>() * WPB;
+  static const int resident = resident_ctas(ns_assembly_warp_kernel<D, T, SPEC, WPB, BATCH, KC>, 32 * WPB, smem);
   if (resident <= 0) return set_error(UFEM_ERR_CUDA, "occupancy query of the warp assembly kernel failed");
   const unsigned grid = unsigned(std::min<int64_t>((ngroups + WPB - 1) / WPB, resident));
-  ns_assembly_warp_kernel<D, T, SPEC, WPB, BATCH><<<grid, 32 * WPB, smem, s>>>(ngroups, nmesh, descs, gprefix, one);
+  ns_assembly_warp_kernel<D, T, SPEC, WPB, BATCH, KC><<<grid, 32 * WPB, smem, s>>>(
+      ngroups, nmesh, descs, gprefix, one.groups, one.row_inc, one.inc_elem, one.inc_info, one.conn, one.coords,
+      one.uadv, one.state, one.node32, one.force, one.start, one.p, one.vals, one.vals32, one.rhs);
   UFEM_CUDA_TRY(cudaGetLastError());
   return UFEM_OK;
 }
 
-template <int D, typename T, bool SPEC, bool BATCH>
+template <int D, typename T, bool SPEC, bool BATCH, int KC = 32>
 int launch_warp_w(int warps, int ngroups, int nmesh, const AsmDesc* descs, const int* gprefix, const AsmDesc& one,
                   cudaStream_t s) {
   switch (warps) {
-    case 2: return launch_warp_t<D, T, SPEC, 2, BATCH>(ngroups, nmesh, descs, gprefix, one, s);
-    case 8: return launch_warp_t<D, T, SPEC, 8, BATCH>(ngroups, nmesh, descs, gprefix, one, s);
-    default: return launch_warp_t<D, T, SPEC, 4, BATCH>(ngroups, nmesh, descs, gprefix, one, s);
+    case 2: return launch_warp_t<D, T, SPEC, 2, BATCH, KC>(ngroups, nmesh, descs, gprefix, one, s);
+    case 8: return launch_warp_t<D, T, SPEC, 8, BATCH, KC>(ngroups, nmesh, descs, gprefix, one, s);
+    default: return launch_warp_t<D, T, SPEC, 4, BATCH, KC>(ngroups, nmesh, descs, gprefix, one, s);
   }
 }
 
@@ -1468,11 +1496,32 @@ int launch_assembly_t(ufem_ns_handle* h, cudaStream_t s, bool write32) {
   constexpr bool f32 = std::is_same<T, float>::value;
   if (h->asm_variant == kAsmChunk) return launch_chunk_t<D, T, CH, SPEC>(h, f32 ? h->plan32 : h->plan64, p, s, write32);
   int rc;
+  const bool w24 = D == 3 && h->asm_variant == kAsmWarp24;
+  const WarpPlan& wp = w24 ? h->wplan24 : h->wplan;
   AsmDesc one;  // this handle's descriptor, passed as a kernel parameter
-  fill_desc(h, write32, one);
-  if ((rc = launch_warp_w<D, T, SPEC, false>(h->asm_warps, h->wplan.ngroups, 1, nullptr, nullptr, one, s)))
-    return rc;
-  return launch_chunk_t<D, T, CH, SPEC>(h, f32 ? h->wplan.big32 : h->wplan.big64, p, s, write32);
+  fill_desc(h, write32, one, &wp);
+  if constexpr (D == 3) {
+    if (w24) rc = launch_warp_w<D, T, SPEC, false, 24>(h->asm_warps, wp.ngroups, 1, nullptr, nullptr, one, s);
+    else rc = launch_warp_w<D, T, SPEC, false, 32>(h->asm_warps, wp.ngroups, 1, nullptr, nullptr, one, s);
+  } else {
+    rc = launch_warp_w<D, T, SPEC, false, 32>(h->asm_warps, wp.ngroups, 1, nullptr, nullptr, one, s);
+  }
+  if (rc) return rc;
+  return launch_chunk_t<D, T, CH, SPEC>(h, f32 ? wp.big32 : wp.big64, p, s, write32);
+}
+
+template <int D, typename T, bool SPEC, bool BATCH, int KC>
+int set_warp_smem_attr() {
+  UFEM_CUDA_TRY(cudaFuncSetAttribute(ns_assembly_warp_kernel<D, T, SPEC, 2, BATCH, KC>,
+                                     cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     int(2 * warp_stage_bytes<D, T, KC, BATCH>())));
+  UFEM_CUDA_TRY(cudaFuncSetAttribute(ns_assembly_warp_kernel<D, T, SPEC, 4, BATCH, KC>,
+                                     cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     int(4 * warp_stage_bytes<D, T, KC, BATCH>())));
+  UFEM_CUDA_TRY(cudaFuncSetAttribute(ns_assembly_warp_kernel<D, T, SPEC, 8, BATCH, KC>,
+                                     cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     int(8 * warp_stage_bytes<D, T, KC, BATCH>())));
+  return UFEM_OK;
 }
 
 template <int D, typename T, int CH, bool SPEC>
@@ -1480,18 +1529,12 @@ int set_smem_attr() {
   constexpr size_t smem = assembly_smem_bytes<D, T, CH>();
   UFEM_CUDA_TRY(cudaFuncSetAttribute(ns_assembly_kernel<D, T, CH, SPEC>,
                                      cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
-  UFEM_CUDA_TRY(cudaFuncSetAttribute(ns_assembly_warp_kernel<D, T, SPEC, 2, false>,
-                                     cudaFuncAttributeMaxDynamicSharedMemorySize, int(2 * warp_stage_bytes<D, T>())));
-  UFEM_CUDA_TRY(cudaFuncSetAttribute(ns_assembly_warp_kernel<D, T, SPEC, 4, false>,
-                                     cudaFuncAttributeMaxDynamicSharedMemorySize, int(4 * warp_stage_bytes<D, T>())));
-  UFEM_CUDA_TRY(cudaFuncSetAttribute(ns_assembly_warp_kernel<D, T, SPEC, 8, false>,
-                                     cudaFuncAttributeMaxDynamicSharedMemorySize, int(8 * warp_stage_bytes<D, T>())));
-  UFEM_CUDA_TRY(cudaFuncSetAttribute(ns_assembly_warp_kernel<D, T, SPEC, 2, true>,
-                                     cudaFuncAttributeMaxDynamicSharedMemorySize, int(2 * warp_stage_bytes<D, T>())));
-  UFEM_CUDA_TRY(cudaFuncSetAttribute(ns_assembly_warp_kernel<D, T, SPEC, 4, true>,
-                                     cudaFuncAttributeMaxDynamicSharedMemorySize, int(4 * warp_stage_bytes<D, T>())));
-  UFEM_CUDA_TRY(cudaFuncSetAttribute(ns_assembly_warp_kernel<D, T, SPEC, 8, true>,
-                                     cudaFuncAttributeMaxDynamicSharedMemorySize, int(8 * warp_stage_bytes<D, T>())));
+  int rc;
+  if ((rc = set_warp_smem_attr<D, T, SPEC, false, 32>()) || (rc = set_warp_smem_attr<D, T, SPEC, true, 32>()))
+    return rc;
+  if constexpr (D == 3) {
+    if ((rc = set_warp_smem_attr<D, T, SPEC, false, 24>())) return rc;
+  }
   return UFEM_OK;
 }
 

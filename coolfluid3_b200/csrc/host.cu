@@ -236,9 +236,12 @@ void destroy_impl(ufem_ns_handle* h) {
   dfree(h->d_nu); dfree(h->d_force); dfree(h->d_node32); dfree(h->d_start); dfree(h->d_adj); dfree(h->d_rowptr);
   dfree(h->d_colidx); dfree(h->d_vals); dfree(h->d_vals32); dfree(h->d_rhs); dfree(h->d_sol);
   dfree(h->d_diagpos); dfree(h->d_row_inc); dfree(h->d_inc_elem); dfree(h->d_inc_info);
-  dfree(h->plan64.chunks); dfree(h->plan32.chunks); dfree(h->wplan.groups);
-  dfree(h->wplan.big64.chunks); dfree(h->wplan.big32.chunks); dfree(h->d_desc); dfree(h->d_gprefix);
-  if (h->h_desc) cudaFreeHost(h->h_desc); dfree(h->d_stage); dfree(h->d_x); dfree(h->d_y);
+  dfree(h->plan64.chunks); dfree(h->plan32.chunks);
+  for (WarpPlan* wp : {&h->wplan, &h->wplan24}) {
+    dfree(wp->groups);
+    dfree(wp->big64.chunks);
+    dfree(wp->big32.chunks);
+  } dfree(h->d_stage); dfree(h->d_x); dfree(h->d_y);
   for (auto& e : h->ev)
     if (e) cudaEventDestroy(e);
   delete h;
@@ -480,13 +483,14 @@ int ufem_ns_create(const ufem_mesh* mesh, const ufem_ns_options* opts, ufem_ns_h
   // leaves out (more than 32 incidences).
   auto inc_of = [&](int64_t i) { return int64_t(row_inc[i + 1] - row_inc[i]); };
   auto slots_of = [&](int64_t i) { return h->start_h[i + 1] - h->start_h[i]; };
-  auto make_chunks = [&](int cap, bool only_big, std::vector<int2>& chunks) -> bool {
+  auto make_chunks = [&](int cap, int big_above, std::vector<int2>& chunks) -> bool {
+    const bool only_big = big_above > 0;
     int64_t i = 0;
     while (i < N) {
-      if (only_big && inc_of(i) <= 32) { ++i; continue; }
+      if (only_big && inc_of(i) <= big_above) { ++i; continue; }
       const int64_t first = i;
       int64_t k = 0, sl = 0;  // incidences and neighbourhood slots of the chunk, each <= cap
-      while (i < N && (!only_big || inc_of(i) > 32) && k + inc_of(i) <= cap && sl + slots_of(i) <= cap) {
+      while (i < N && (!only_big || inc_of(i) > big_above) && k + inc_of(i) <= cap && sl + slots_of(i) <= cap) {
         k += inc_of(i);
         sl += slots_of(i);
         ++i;
@@ -496,30 +500,42 @@ int ufem_ns_create(const ufem_mesh* mesh, const ufem_ns_options* opts, ufem_ns_h
     }
     return true;
   };
-  std::vector<int2> chunks64, chunks32, big64, big32;
-  std::vector<int4> groups;
-  if (!make_chunks(assembly_chunk_capacity(dim, 0), false, chunks64) ||
-      !make_chunks(assembly_chunk_capacity(dim, 1), false, chunks32) ||
-      !make_chunks(assembly_chunk_capacity(dim, 0), true, big64) ||
-      !make_chunks(assembly_chunk_capacity(dim, 1), true, big32))
+  std::vector<int2> chunks64, chunks32;
+  if (!make_chunks(assembly_chunk_capacity(dim, 0), 0, chunks64) ||
+      !make_chunks(assembly_chunk_capacity(dim, 1), 0, chunks32))
     return fail(set_error(UFEM_ERR_LIMIT, "a node has more incident elements than one assembly chunk holds"));
-  // --- warp groups: consecutive rows with at most 32 incidences in total
-  for (int64_t i = 0; i < N;) {
-    if (inc_of(i) > 32) { ++i; continue; }
-    const int64_t first = i;
-    int64_t k = 0;
-    while (i < N && inc_of(i) <= 32 && k + inc_of(i) <= 32) k += inc_of(i++);
-    groups.push_back(make_int4(int(first), int(i), row_inc[first], int(k)));
-  }
   h->plan64.cap = assembly_chunk_capacity(dim, 0);
   h->plan64.nchunks = int(chunks64.size());
   h->plan32.cap = assembly_chunk_capacity(dim, 1);
   h->plan32.nchunks = int(chunks32.size());
-  h->wplan.ngroups = int(groups.size());
-  h->wplan.big64.cap = h->plan64.cap;
-  h->wplan.big64.nchunks = int(big64.size());
-  h->wplan.big32.cap = h->plan32.cap;
-  h->wplan.big32.nchunks = int(big32.size());
+  // --- warp groups: consecutive rows with at most `cap` incidences in total;
+  // rows with more go to a chunk plan that lists only them
+  struct WarpPlanHost {
+    std::vector<int4> groups;
+    std::vector<int2> big64, big32;
+  };
+  auto make_warp_plan = [&](int cap, WarpPlan& wp, WarpPlanHost& hp) -> bool {
+    for (int64_t i = 0; i < N;) {
+      if (inc_of(i) > cap) { ++i; continue; }
+      const int64_t first = i;
+      int64_t k = 0;
+      while (i < N && inc_of(i) <= cap && k + inc_of(i) <= cap) k += inc_of(i++);
+      hp.groups.push_back(make_int4(int(first), int(i), row_inc[first], int(k)));
+    }
+    if (!make_chunks(assembly_chunk_capacity(dim, 0), cap, hp.big64) ||
+        !make_chunks(assembly_chunk_capacity(dim, 1), cap, hp.big32))
+      return false;
+    wp.cap = cap;
+    wp.ngroups = int(hp.groups.size());
+    wp.big64.cap = h->plan64.cap;
+    wp.big64.nchunks = int(hp.big64.size());
+    wp.big32.cap = h->plan32.cap;
+    wp.big32.nchunks = int(hp.big32.size());
+    return true;
+  };
+  WarpPlanHost wh32, wh24;
+  if (!make_warp_plan(32, h->wplan, wh32) || (dim == 3 && !make_warp_plan(24, h->wplan24, wh24)))
+    return fail(set_error(UFEM_ERR_LIMIT, "a node has more incident elements than one assembly chunk holds"));
 
   // --- device allocations and uploads
   DeviceLock device_lock(device_mutex());
@@ -542,10 +558,6 @@ int ufem_ns_create(const ufem_mesh* mesh, const ufem_ns_options* opts, ufem_ns_h
       (rc = dmalloc(&h->d_inc_info, inc_info.size(), "inc_info")) ||
       (rc = dmalloc(&h->plan64.chunks, chunks64.size(), "chunks64")) ||
       (rc = dmalloc(&h->plan32.chunks, chunks32.size(), "chunks32")) ||
-      (rc = dmalloc(&h->wplan.groups, std::max<size_t>(groups.size(), 1), "groups")) ||
-      (rc = dmalloc(&h->d_desc, 1, "assembly descriptor")) || (rc = dmalloc(&h->d_gprefix, 2, "group prefix")) ||
-      (rc = dmalloc(&h->wplan.big64.chunks, std::max<size_t>(big64.size(), 1), "big64")) ||
-      (rc = dmalloc(&h->wplan.big32.chunks, std::max<size_t>(big32.size(), 1), "big32")) ||
       (rc = dmalloc(&h->d_stage, size_t(N) * 4 * dim, "stage")))
     return fail(rc);
   if (opts->precision == 1 && ((rc = dmalloc(&h->d_vals32, size_t(h->nnz), "vals32")) ||
@@ -562,18 +574,27 @@ int ufem_ns_create(const ufem_mesh* mesh, const ufem_ns_options* opts, ufem_ns_h
       (ce = up(h->d_inc_elem, inc_elem.data(), inc_elem.size() * 4)) ||
       (ce = up(h->d_inc_info, inc_info.data(), inc_info.size() * 4)) ||
       (ce = up(h->plan64.chunks, chunks64.data(), chunks64.size() * sizeof(int2))) ||
-      (ce = up(h->plan32.chunks, chunks32.data(), chunks32.size() * sizeof(int2))) ||
-      (ce = up(h->wplan.groups, groups.data(), groups.size() * sizeof(int4))) ||
-      (ce = up(h->d_gprefix, std::vector<int>{0, int(groups.size())}.data(), 2 * sizeof(int))) ||
-      (ce = up(h->wplan.big64.chunks, big64.data(), big64.size() * sizeof(int2))) ||
-      (ce = up(h->wplan.big32.chunks, big32.data(), big32.size() * sizeof(int2))))
+      (ce = up(h->plan32.chunks, chunks32.data(), chunks32.size() * sizeof(int2))))
     return fail(set_error(UFEM_ERR_CUDA, std::string("upload: ") + cudaGetErrorString(ce)));
+  auto upload_warp_plan = [&](WarpPlan& wp, const WarpPlanHost& hp) -> int {
+    int r;
+    if ((r = dmalloc(&wp.groups, std::max<size_t>(hp.groups.size(), 1), "groups")) ||
+        (r = dmalloc(&wp.big64.chunks, std::max<size_t>(hp.big64.size(), 1), "big rows")) ||
+        (r = dmalloc(&wp.big32.chunks, std::max<size_t>(hp.big32.size(), 1), "big rows")))
+      return r;
+    cudaError_t e;
+    if ((e = up(wp.groups, hp.groups.data(), hp.groups.size() * sizeof(int4))) ||
+        (e = up(wp.big64.chunks, hp.big64.data(), hp.big64.size() * sizeof(int2))) ||
+        (e = up(wp.big32.chunks, hp.big32.data(), hp.big32.size() * sizeof(int2))))
+      return set_error(UFEM_ERR_CUDA, std::string("upload: ") + cudaGetErrorString(e));
+    return UFEM_OK;
+  };
+  if ((rc = upload_warp_plan(h->wplan, wh32)) || (dim == 3 && (rc = upload_warp_plan(h->wplan24, wh24))))
+    return fail(rc);
   if ((ce = cudaMemset(h->d_sol, 0, size_t(h->nrows) * 8)) || (ce = cudaMemset(h->d_state, 0, size_t(N) * 32)) ||
       (ce = cudaMemset(h->d_hist, 0, size_t(N) * 96)) || (ce = cudaMemset(h->d_uadv, 0, size_t(N) * 32)) ||
       (ce = cudaMemset(h->d_nu, 0, size_t(N) * 8)) || (ce = cudaMemset(h->d_rhs, 0, size_t(h->nrows) * 8)))
     return fail(set_error(UFEM_ERR_CUDA, std::string("memset: ") + cudaGetErrorString(ce)));
-  if ((ce = cudaMallocHost(reinterpret_cast<void**>(&h->h_desc), sizeof(AsmDesc))) != cudaSuccess)
-    return fail(set_error(UFEM_ERR_NOMEM, std::string("cudaMallocHost: ") + cudaGetErrorString(ce)));
   if ((rc = launch_build_csr(h, 0))) return fail(rc);
   if ((ce = cudaDeviceSynchronize()) != cudaSuccess)
     return fail(set_error(UFEM_ERR_CUDA, std::string("CSR build: ") + cudaGetErrorString(ce)));
@@ -765,7 +786,10 @@ int ufem_ns_assemble(ufem_ns_handle* h, void* stream) {
 
 int ufem_ns_set_assembly_kernel(ufem_ns_handle* h, int32_t variant, int32_t warps_per_cta) {
   if (!h) return set_error(UFEM_ERR_ARG, "NULL handle");
-  if (variant != kAsmWarp && variant != kAsmChunk) return set_error(UFEM_ERR_ARG, "assembly variant must be 0 or 1");
+  if (variant != kAsmWarp && variant != kAsmChunk && variant != kAsmWarp24)
+    return set_error(UFEM_ERR_ARG, "assembly variant must be 0, 1 or 2");
+  if (variant == kAsmWarp24 && h->dim != 3)
+    return set_error(UFEM_ERR_ARG, "assembly variant 2 (24-incidence groups) is for tetrahedra");
   if (warps_per_cta != 2 && warps_per_cta != 4 && warps_per_cta != 8)
     return set_error(UFEM_ERR_ARG, "warps_per_cta must be 2, 4 or 8");
   h->asm_variant = variant;
@@ -788,7 +812,11 @@ int ufem_ns_tune_assembly(ufem_ns_handle* h, void* stream, int32_t reps, int32_t
   cudaStream_t s = static_cast<cudaStream_t>(stream);
   const bool w32 = h->d_vals32 != nullptr;
   struct Cand { int variant, warps; };
-  const Cand cands[] = {{kAsmWarp, 2}, {kAsmWarp, 4}, {kAsmWarp, 8}, {kAsmChunk, 4}};
+  std::vector<Cand> cands = {{kAsmWarp, 2}, {kAsmWarp, 4}, {kAsmWarp, 8}, {kAsmChunk, 4}};
+  if (h->dim == 3) {
+    cands.push_back({kAsmWarp24, 2});
+    cands.push_back({kAsmWarp24, 4});
+  }
   cudaEvent_t e0 = nullptr, e1 = nullptr;
   UFEM_CUDA_TRY(cudaEventCreate(&e0));
   if (cudaEventCreate(&e1) != cudaSuccess) {

@@ -52,6 +52,7 @@ struct AssemblyPlan {
   int2* chunks = nullptr;      // [first row, end row) per chunk (device)
 };
 struct WarpPlan {
+  int cap = 32;                // incidences per group (lanes per warp that evaluate elements)
   int ngroups = 0;
   int4* groups = nullptr;      // first row, end row, first incidence, incidences (device)
   AssemblyPlan big64, big32;   // rows with more than 32 incidences
@@ -79,7 +80,7 @@ struct AsmDesc {
 };
 
 // Assembly kernel variants (selected per handle, see ufem_ns_set_assembly_kernel).
-enum AssemblyVariant { kAsmWarp = 0, kAsmChunk = 1 };
+enum AssemblyVariant { kAsmWarp = 0, kAsmChunk = 1, kAsmWarp24 = 2 };
 
 // Symmetric-Dirichlet plan (sequential semantics of TrilinosFEVbrMatrix::
 // symmetric_dirichlet reduced to an order-preserving parallel form).
@@ -144,10 +145,8 @@ struct ufem_ns_handle {
 
   ufem::AssemblyPlan plan64;       // chunks sized for the FP64-element chunk kernel (all rows)
   ufem::AssemblyPlan plan32;       // chunks sized for the FP32-element chunk kernel (all rows)
-  ufem::WarpPlan wplan;            // warp-per-row-group kernel
-  ufem::AsmDesc* d_desc = nullptr; // this handle as a one-mesh assembly batch (device)
-  int* d_gprefix = nullptr;        // {0, wplan.ngroups} (device)
-  ufem::AsmDesc* h_desc = nullptr; // pinned mirror of d_desc
+  ufem::WarpPlan wplan;            // warp-per-row-group kernel, groups of <= 32 incidences
+  ufem::WarpPlan wplan24;          // tetrahedra: groups of <= 24 incidences (smaller staging, more warps)
   int asm_variant = ufem::kAsmWarp;
   int asm_warps = 4;               // warps per CTA of the warp kernel
   ufem::DirichletPlan bcp;
@@ -172,7 +171,7 @@ int launch_build_csr(ufem_ns_handle* h, cudaStream_t s);
 int launch_linearize(ufem_ns_handle* h, cudaStream_t s);
 int launch_assembly(ufem_ns_handle* h, cudaStream_t s, bool write32);
 void fill_params(const ufem_ns_handle* h, NSParams& p);
-void fill_desc(const ufem_ns_handle* h, bool write32, AsmDesc& d);
+void fill_desc(const ufem_ns_handle* h, bool write32, AsmDesc& d, const WarpPlan* plan = nullptr);
 // Warp assembly of many meshes in one persistent launch (same dim and precision;
 // rows with more than 32 incidences go through each mesh's chunk plan).
 int launch_assembly_batch(int dim, int precision, bool spec, int warps, int ngroups, int nmesh,

@@ -225,10 +225,12 @@ class NavierStokes:
         return v.value
 
     # -- assembly kernel selection and autotuning -----------------------------
-    ASSEMBLY_VARIANTS = {"warp": 0, "chunk": 1}
+    ASSEMBLY_VARIANTS = {"warp": 0, "chunk": 1, "warp24": 2}
 
     def set_assembly_kernel(self, variant: str = "warp", warps_per_cta: int = 4) -> None:
-        """Pick the assembly kernel: "warp" (warp per row group) or "chunk" (CTA per row range)."""
+        """Pick the assembly kernel: "warp" (warp per group of rows with <= 32 incident elements),
+        "warp24" (tetrahedra: groups of <= 24, smaller staging, more resident warps) or "chunk"
+        (CTA per row range)."""
         N.check(self._lib.ufem_ns_set_assembly_kernel(self._h, self.ASSEMBLY_VARIANTS[variant], int(warps_per_cta)))
 
     def assembly_kernel(self) -> tuple[str, int]:

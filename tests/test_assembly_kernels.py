@@ -23,6 +23,11 @@ from .util import row_scaled_error, small_problem, vec_rel_error
 pytestmark = pytest.mark.gpu
 
 VARIANTS = [("warp", 2), ("warp", 4), ("warp", 8), ("chunk", 4)]
+VARIANTS_3D = VARIANTS + [("warp24", 2), ("warp24", 4)]
+
+
+def variants(dim):
+    return VARIANTS_3D if dim == 3 else VARIANTS
 
 
 def fan_mesh(dim: int, m: int):
@@ -73,7 +78,7 @@ def test_variants_agree_and_are_deterministic(dim, n, precision, spec):
     rp, _ = ns.csr()
     tol = 1e-14 if precision == "fp64" else 1e-6
     ref_v, ref_r = assembled(ns, "warp", 4)
-    for variant, warps in VARIANTS:
+    for variant, warps in variants(dim):
         v, r = assembled(ns, variant, warps)
         assert row_scaled_error(v, ref_v, rp) <= tol, (variant, warps)
         assert vec_rel_error(r, ref_r) <= tol, (variant, warps)
@@ -93,7 +98,7 @@ def test_fan_mesh_rows_above_32_elements(dim, m, spec):
     o.assemble()
     ov, orr = o.system()
     rp, _ = o.csr()
-    for variant, warps in VARIANTS:
+    for variant, warps in variants(dim):
         v, r = assembled(ns, variant, warps)
         assert row_scaled_error(v, ov, rp) <= 1e-11, (variant, warps)
         assert vec_rel_error(r, orr) <= 1e-11, (variant, warps)
@@ -106,7 +111,7 @@ def test_autotuner_picks_a_candidate_and_keeps_results():
     ns.assemble()
     v0, r0 = ns.system()
     res = ns.tune_assembly(reps=3)
-    assert (res["variant"], res["warps_per_cta"]) in VARIANTS and res["ms"] > 0
+    assert (res["variant"], res["warps_per_cta"]) in VARIANTS_3D and res["ms"] > 0
     assert ns.assembly_kernel() == (res["variant"], res["warps_per_cta"])
     ns.assemble()
     v1, r1 = ns.system()
