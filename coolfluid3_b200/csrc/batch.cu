@@ -8,9 +8,10 @@
 //    mesh by binary search over a prefix of the member sizes);
 //  - the assembly is the persistent warp kernel over all members' row groups;
 //  - the solve is BiCGStab with point Jacobi and PER-MESH scalars: each member
-//    is split into fixed chunks of kChunkRows rows, vector kernels produce one
-//    partial per chunk, and one warp per mesh folds that mesh's partials in a
-//    fixed order.  A member's arithmetic therefore depends only on its own
+//    is split into fixed chunks of kChunkNodes nodes, vector kernels produce
+//    one partial per chunk, and the last CTA of each mesh to finish (an atomic
+//    counter per mesh) folds that mesh's partials in a fixed order and updates
+//    its scalars, so an iteration is seven launches.  A member's arithmetic therefore depends only on its own
 //    data: its results are bitwise the same alone (a batch of one) and in any
 //    mix.  Converged members drop out (their kernels return at once) while the
 //    others continue.  The mixed-precision solve iterates with an FP32 copy of
@@ -30,19 +31,23 @@
 namespace ufem {
 namespace {
 
-constexpr int kChunkRows = 2048;  // rows per solver chunk (one CTA, one partial)
+constexpr int kChunkNodes = 512;  // nodes per solver chunk (one CTA, one partial): 2048 rows for tets
 constexpr int kThreads = 256;
 constexpr int kBlockIters = 8;    // BiCGStab iterations per host check / graph replay
 constexpr int kDc = 16;           // per-mesh double scalars
-constexpr int kIc = 8;            // per-mesh int flags
+constexpr int kIc = 12;           // per-mesh int flags
 constexpr int kMaxRestarts = 10;  // BiCGStab restarts after breakdowns in one solve
 
 // per-mesh scalar slots (dctl[m * kDc + ...])
 constexpr int sBnorm = 0, sBeta = 1, sEst = 2, sRho = 5, sRhoOld = 6, sAlpha = 7, sOmega = 8, sTrue = 9,
               sTol = 10, sTS = 11, sTT = 12, sLastTrue = 13;
 // per-mesh flags (ictl[m * kIc + ...])
-constexpr int fDone = 0, fStatus = 2, fIters = 3, fMaxit = 4, fOuter = 5, fFinal = 6, fRepl = 7;
-constexpr int kReplaceBlocks = 4;  // mixed solve: FP64 residual replacement every 4 blocks (32 iterations)
+constexpr int fDone = 0, fStatus = 2, fIters = 3, fMaxit = 4, fOuter = 5, fFinal = 6, fRepl = 7, fLastRepl = 8,
+              fSkipRepl = 9;
+// Mixed solve: a member's residual is replaced by the FP64 one when it claims
+// convergence and every kReplaceIters of its own iterations (a per-member
+// schedule, so its arithmetic does not depend on the other members).
+constexpr int kReplaceIters = 32;
 
 struct BatchMesh {
   int64_t N, nrows, row_off;  // row_off: first row in the concatenated solver vectors
@@ -316,19 +321,160 @@ __global__ void residual_batch_kernel(const Chunk* __restrict__ chunks, const Ba
 }
 
 // Per-mesh fold of chunk partials: one warp per mesh, fixed order.
-__device__ __forceinline__ void fold2(const double* __restrict__ part, int nchunks, int c0, int c1, double& a,
+__device__ __forceinline__ void fold2(const double* part, int nchunks, int c0, int c1, double& a,
                                       double& b) {
   const int lane = threadIdx.x & 31;
   a = 0.0;
   b = 0.0;
-  for (int k = c0 + lane; k < c1; k += 32) {
-    a += part[k];
-    b += part[nchunks + k];
+  for (int k = c0 + lane; k < c1; k += 32) {  // L2 reads: partials written by other CTAs of this launch
+    a += __ldcg(part + k);
+    b += __ldcg(part + nchunks + k);
   }
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1) {
     a += __shfl_xor_sync(0xffffffffu, a, o);
     b += __shfl_xor_sync(0xffffffffu, b, o);
+  }
+}
+
+// ---- fused iteration kernels ------------------------------------------------
+// A chunk CTA writes its partial(s), and the last CTA of the mesh to finish
+// (per-mesh counter, reset by that CTA) folds all of the mesh's partials in
+// chunk order and applies the scalar update: deterministic, no waiting.
+__device__ __forceinline__ bool last_chunk_of_mesh(int* counter, int nchunks_mesh, int* s_flag) {
+  __threadfence();
+  __syncthreads();
+  if (threadIdx.x == 0) *s_flag = (atomicAdd(counter, 1) == nchunks_mesh - 1) ? 1 : 0;
+  __syncthreads();
+  if (*s_flag == 0) return false;
+  __threadfence();
+  if (threadIdx.x == 0) *counter = 0;  // ready for the next launch
+  return true;
+}
+
+// Dot partials over a vector chunk, MODE 1: rh.v (-> alpha), MODE 2: t.s and
+// t.t (-> omega); the mesh's last CTA folds the partials in chunk order and
+// updates the scalar.
+template <int MODE>
+__global__ void dot_fold_batch_kernel(const Chunk* __restrict__ chunks, const BatchMesh* __restrict__ bm,
+                                      const int* __restrict__ cprefix, const double* __restrict__ a,
+                                      const double* __restrict__ bv, double* __restrict__ part, int nchunks,
+                                      double* __restrict__ dctl, int* __restrict__ ictl,
+                                      int* __restrict__ counters) {
+  __shared__ double sm[32];
+  __shared__ int s_flag;
+  const Chunk c = chunks[blockIdx.x];
+  const int m = c.mesh;
+  if (ictl[m * kIc + fDone]) return;  // uniform per CTA
+  const int64_t off = bm[m].row_off;
+  double pa = 0.0, pb = 0.0;
+  for (int i = c.lo + threadIdx.x; i < c.hi; i += blockDim.x) {
+    const int64_t k = off + i;
+    const double ai = a[k];
+    pa += ai * bv[k];              // MODE 1: rh . v ; MODE 2: t . s
+    if (MODE == 2) pb += ai * ai;  // t . t
+  }
+  pa = block_sum(pa, sm);
+  if (MODE == 2) pb = block_sum(pb, sm);
+  if (threadIdx.x == 0) {
+    part[blockIdx.x] = pa;
+    part[nchunks + blockIdx.x] = pb;
+  }
+  const int c0 = cprefix[m], c1 = cprefix[m + 1];
+  if (!last_chunk_of_mesh(counters + m * 4 + MODE - 1, c1 - c0, &s_flag)) return;
+  if (threadIdx.x >= 32) return;
+  double fa, fb;
+  fold2(part, nchunks, c0, c1, fa, fb);
+  if (threadIdx.x != 0) return;
+  double* d = dctl + m * kDc;
+  int* f = ictl + m * kIc;
+  if (MODE == 1) {  // alpha = rho / (rh . v)
+    if (fa == 0.0 || !isfinite(fa)) {
+      f[fDone] = 1;
+      f[fStatus] = isfinite(fa) ? 2 : 3;
+      return;
+    }
+    const double al = d[sRho] / fa;
+    if (!(fabs(al) < 1e150)) {
+      f[fDone] = 1;
+      f[fStatus] = 2;
+      return;
+    }
+    d[sAlpha] = al;
+  } else {  // omega = (t . s) / (t . t)
+    const double om = (fb != 0.0) ? fa / fb : 0.0;
+    d[sTS] = fa;
+    d[sTT] = fb;
+    d[sOmega] = om;
+    if (!isfinite(om)) {
+      f[fDone] = 1;
+      f[fStatus] = 3;
+    } else if (om == 0.0 && fb != 0.0) {
+      f[fStatus] = 2;  // breakdown: x still advances by alpha ph, then the solve stops
+    }
+  }
+}
+
+// x += alpha ph + omega sh ; r = s - omega t ; partials of r.r and rh.r; the
+// mesh's last CTA computes rho_new, the residual estimate and convergence.
+template <int XL>
+__global__ void bicg_xr_end_batch_kernel(const Chunk* __restrict__ chunks, const BatchMesh* __restrict__ bm,
+                                         const int* __restrict__ cprefix, const double* __restrict__ ph,
+                                         const double* __restrict__ sh, const double* __restrict__ s,
+                                         const double* __restrict__ t, const double* __restrict__ rh,
+                                         double* xwork, double* __restrict__ r, double* __restrict__ dctl,
+                                         int* __restrict__ ictl, double* __restrict__ part, int nchunks,
+                                         int* __restrict__ counters) {
+  __shared__ double sm[32];
+  __shared__ int s_flag;
+  const Chunk c = chunks[blockIdx.x];
+  const int m = c.mesh;
+  if (ictl[m * kIc + fDone]) return;
+  const BatchMesh& M = bm[m];
+  const double al = dctl[m * kDc + sAlpha], om = dctl[m * kDc + sOmega];
+  const int64_t off = M.row_off;
+  double* x = vec<XL>(M, xwork);
+  double rr = 0.0, hr = 0.0;
+  for (int i = c.lo + threadIdx.x; i < c.hi; i += blockDim.x) {
+    const int64_t k = off + i;
+    x[i] = x[i] + al * ph[k] + om * sh[k];
+    const double ri = s[k] - om * t[k];
+    r[k] = ri;
+    rr += ri * ri;
+    hr += rh[k] * ri;
+  }
+  rr = block_sum(rr, sm);
+  hr = block_sum(hr, sm);
+  if (threadIdx.x == 0) {
+    part[blockIdx.x] = rr;
+    part[nchunks + blockIdx.x] = hr;
+  }
+  const int c0 = cprefix[m], c1 = cprefix[m + 1];
+  if (!last_chunk_of_mesh(counters + m * 4 + 2, c1 - c0, &s_flag)) return;
+  if (threadIdx.x >= 32) return;
+  double nn, rho_new;
+  fold2(part, nchunks, c0, c1, nn, rho_new);
+  if (threadIdx.x != 0) return;
+  double* d = dctl + m * kDc;
+  int* f = ictl + m * kIc;
+  const double rn = sqrt(nn);
+  d[sEst] = rn;
+  d[sRhoOld] = d[sRho];
+  d[sRho] = rho_new;
+  f[fIters] += 1;
+  if (f[fStatus] == 2) {
+    f[fDone] = 1;
+  } else if (!isfinite(rn) || !isfinite(rho_new)) {
+    f[fDone] = 1;
+    f[fStatus] = 3;
+  } else if (rn <= d[sTol] * d[sBnorm]) {
+    f[fDone] = 1;
+  } else if (rho_new == 0.0) {
+    f[fDone] = 1;
+    f[fStatus] = 2;
+  } else if (f[fIters] >= f[fMaxit]) {
+    f[fDone] = 1;
+    f[fStatus] = 1;
   }
 }
 
@@ -360,6 +506,7 @@ __global__ void bicg_init_batch_kernel(int nmesh, const int* __restrict__ cprefi
   f[fDone] = (f[fStatus] != 0 || beta <= tol * bnorm || bnorm == 0.0 || (use_outer && f[fOuter])) ? 1 : 0;
   f[fFinal] = f[fDone];  // (residual replacement only visits meshes that are not final)
   f[fRepl] = 0;
+  f[fLastRepl] = 0;
 }
 
 // p = r + beta (p - omega v), ph = D^-1 p
@@ -381,51 +528,7 @@ __global__ void bicg_p_batch_kernel(const Chunk* __restrict__ chunks, const Batc
   }
 }
 
-// partials of a.b (and, when `c2` is set, of c2.c2 into the second half)
-__global__ void dot_batch_kernel(const Chunk* __restrict__ chunks, const BatchMesh* __restrict__ bm,
-                                 const double* __restrict__ a, const double* __restrict__ b,
-                                 const double* __restrict__ c2, double* __restrict__ part, int nchunks,
-                                 const int* __restrict__ ictl) {
-  __shared__ double sm[32];
-  const Chunk c = chunks[blockIdx.x];
-  if (ictl[c.mesh * kIc + fDone]) return;
-  const int64_t off = bm[c.mesh].row_off;
-  double s = 0.0, t = 0.0;
-  for (int i = c.lo + threadIdx.x; i < c.hi; i += blockDim.x) {
-    const int64_t k = off + i;
-    s += a[k] * b[k];
-    if (c2) t += c2[k] * c2[k];
-  }
-  s = block_sum(s, sm);
-  if (c2) t = block_sum(t, sm);
-  if (threadIdx.x == 0) {
-    part[blockIdx.x] = s;
-    part[nchunks + blockIdx.x] = t;
-  }
-}
 
-__global__ void bicg_alpha_batch_kernel(int nmesh, const int* __restrict__ cprefix, const double* __restrict__ part,
-                                        int nchunks, double* __restrict__ dctl, int* __restrict__ ictl) {
-  const int m = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-  if (m >= nmesh || ictl[m * kIc + fDone]) return;
-  double hv, unused;
-  fold2(part, nchunks, cprefix[m], cprefix[m + 1], hv, unused);
-  if ((threadIdx.x & 31) != 0) return;
-  double* d = dctl + m * kDc;
-  int* f = ictl + m * kIc;
-  if (hv == 0.0 || !isfinite(hv)) {
-    f[fDone] = 1;
-    f[fStatus] = isfinite(hv) ? 2 : 3;
-    return;
-  }
-  const double a = d[sRho] / hv;
-  if (!(fabs(a) < 1e150)) {
-    f[fDone] = 1;
-    f[fStatus] = 2;
-    return;
-  }
-  d[sAlpha] = a;
-}
 
 // s = r - alpha v, sh = D^-1 s
 __global__ void bicg_s_batch_kernel(const Chunk* __restrict__ chunks, const BatchMesh* __restrict__ bm, int pkind,
@@ -444,88 +547,8 @@ __global__ void bicg_s_batch_kernel(const Chunk* __restrict__ chunks, const Batc
   }
 }
 
-__global__ void bicg_omega_batch_kernel(int nmesh, const int* __restrict__ cprefix, const double* __restrict__ part,
-                                        int nchunks, double* __restrict__ dctl, int* __restrict__ ictl) {
-  const int m = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-  if (m >= nmesh || ictl[m * kIc + fDone]) return;
-  double ts, tt;
-  fold2(part, nchunks, cprefix[m], cprefix[m + 1], ts, tt);
-  if ((threadIdx.x & 31) != 0) return;
-  double* d = dctl + m * kDc;
-  int* f = ictl + m * kIc;
-  const double om = (tt != 0.0) ? ts / tt : 0.0;
-  d[sTS] = ts;
-  d[sTT] = tt;
-  d[sOmega] = om;
-  if (!isfinite(om)) {
-    f[fDone] = 1;
-    f[fStatus] = 3;
-  } else if (om == 0.0 && tt != 0.0) {
-    f[fStatus] = 2;  // breakdown: x still advances by alpha ph, then the solve stops
-  }
-}
 
-// x += alpha ph + omega sh ; r = s - omega t ; partials of r.r and rh.r
-template <int XL>
-__global__ void bicg_xr_batch_kernel(const Chunk* __restrict__ chunks, const BatchMesh* __restrict__ bm,
-                                     const double* __restrict__ ph, const double* __restrict__ sh,
-                                     const double* __restrict__ s, const double* __restrict__ t,
-                                     const double* __restrict__ rh, double* xwork, double* __restrict__ r,
-                                     const double* __restrict__ dctl, const int* __restrict__ ictl,
-                                     double* __restrict__ part, int nchunks) {
-  __shared__ double sm[32];
-  const Chunk c = chunks[blockIdx.x];
-  if (ictl[c.mesh * kIc + fDone]) return;
-  const BatchMesh& M = bm[c.mesh];
-  const double al = dctl[c.mesh * kDc + sAlpha], om = dctl[c.mesh * kDc + sOmega];
-  const int64_t off = M.row_off;
-  double* x = vec<XL>(M, xwork);
-  double rr = 0.0, hr = 0.0;
-  for (int i = c.lo + threadIdx.x; i < c.hi; i += blockDim.x) {
-    const int64_t k = off + i;
-    x[i] = x[i] + al * ph[k] + om * sh[k];
-    const double ri = s[k] - om * t[k];
-    r[k] = ri;
-    rr += ri * ri;
-    hr += rh[k] * ri;
-  }
-  rr = block_sum(rr, sm);
-  hr = block_sum(hr, sm);
-  if (threadIdx.x == 0) {
-    part[blockIdx.x] = rr;
-    part[nchunks + blockIdx.x] = hr;
-  }
-}
 
-__global__ void bicg_end_batch_kernel(int nmesh, const int* __restrict__ cprefix, const double* __restrict__ part,
-                                      int nchunks, double* __restrict__ dctl, int* __restrict__ ictl) {
-  const int m = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-  if (m >= nmesh || ictl[m * kIc + fDone]) return;
-  double nn, rho_new;
-  fold2(part, nchunks, cprefix[m], cprefix[m + 1], nn, rho_new);
-  if ((threadIdx.x & 31) != 0) return;
-  double* d = dctl + m * kDc;
-  int* f = ictl + m * kIc;
-  const double rn = sqrt(nn);
-  d[sEst] = rn;
-  d[sRhoOld] = d[sRho];
-  d[sRho] = rho_new;
-  f[fIters] += 1;
-  if (f[fStatus] == 2) {
-    f[fDone] = 1;
-  } else if (!isfinite(rn) || !isfinite(rho_new)) {
-    f[fDone] = 1;
-    f[fStatus] = 3;
-  } else if (rn <= d[sTol] * d[sBnorm]) {
-    f[fDone] = 1;
-  } else if (rho_new == 0.0) {
-    f[fDone] = 1;
-    f[fStatus] = 2;
-  } else if (f[fIters] >= f[fMaxit]) {
-    f[fDone] = 1;
-    f[fStatus] = 1;
-  }
-}
 
 // True residual of the finished solve: relres = ||b - A x|| / ||b|| into dctl[sTrue].
 __global__ void true_res_batch_kernel(int nmesh, const int* __restrict__ cprefix, const double* __restrict__ part,
@@ -553,7 +576,7 @@ __global__ void replace_batch_kernel(const Chunk* __restrict__ chunks, const Bat
                                      const int* __restrict__ ictl) {
   __shared__ double sm[32];
   const Chunk c = chunks[blockIdx.x];
-  if (ictl[c.mesh * kIc + fFinal]) return;
+  if (ictl[c.mesh * kIc + fSkipRepl]) return;
   const BatchMesh& M = bm[c.mesh];
   const double* b = vec<BL>(M, bwork);
   const int64_t off = M.row_off;
@@ -579,7 +602,7 @@ __global__ void replace_end_batch_kernel(int nmesh, const int* __restrict__ cpre
                                          const double* __restrict__ part, int nchunks, double* __restrict__ dctl,
                                          int* __restrict__ ictl) {
   const int m = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-  if (m >= nmesh || ictl[m * kIc + fFinal]) return;
+  if (m >= nmesh || ictl[m * kIc + fSkipRepl]) return;
   double rr, hr;
   fold2(part, nchunks, cprefix[m], cprefix[m + 1], rr, hr);
   if ((threadIdx.x & 31) != 0) return;
@@ -606,6 +629,7 @@ __global__ void replace_end_batch_kernel(int nmesh, const int* __restrict__ cpre
   }
   d[sLastTrue] = rn;
   f[fRepl] += 1;
+  f[fLastRepl] = f[fIters];
 }
 
 // x = 0 where b = 0 (the solution of A x = 0), as the one-mesh solver does.
@@ -670,6 +694,7 @@ struct ufem_batch {
   double *r = nullptr, *rh = nullptr, *p = nullptr, *v = nullptr, *s = nullptr, *t = nullptr, *ph = nullptr,
          *sh = nullptr, *dinv = nullptr, *w = nullptr;
   double* part = nullptr;
+  int* counters = nullptr;  // per mesh: last-CTA counters of the fused kernels (4 ints)
   double* dctl = nullptr;
   int* ictl = nullptr;
   double* h_dctl = nullptr;
@@ -690,7 +715,7 @@ void batch_free(ufem_batch* b) {
   dfr(b->d_asm); dfr(b->d_gprefix); dfr(b->d_mesh); dfr(b->d_node_prefix); dfr(b->d_bc_prefix);
   dfr(b->d_fix_prefix); dfr(b->d_chunks); dfr(b->d_cprefix);
   dfr(b->r); dfr(b->rh); dfr(b->p); dfr(b->v); dfr(b->s); dfr(b->t); dfr(b->ph); dfr(b->sh); dfr(b->dinv);
-  dfr(b->w); dfr(b->part); dfr(b->dctl); dfr(b->ictl);
+  dfr(b->w); dfr(b->part); dfr(b->counters); dfr(b->dctl); dfr(b->ictl);
   if (b->h_dctl) cudaFreeHost(b->h_dctl);
   if (b->h_ictl) cudaFreeHost(b->h_ictl);
   delete b;
@@ -775,26 +800,26 @@ int spmv_b(ufem_batch* b, double* x, double* y, cudaStream_t st, int skip_flag =
   return UFEM_OK;
 }
 
-// One BiCGStab iteration for every member that is not done.
+// One BiCGStab iteration for every member that is not done: seven launches
+// (p update; SpMV; rh.v + alpha; s update; SpMV; t.s, t.t + omega; x, r update
+// + rho and convergence), the scalars computed by each mesh's last CTA.
 template <typename MT, int XL>
 int bicg_iteration(ufem_batch* b, int pkind, double* xwork, cudaStream_t st) {
   const unsigned nc = unsigned(b->nchunks);
-  const unsigned gm = blocks_for(int64_t(b->nmesh) * 32, 256);
   int rc;
   bicg_p_batch_kernel<<<nc, kThreads, 0, st>>>(b->d_chunks, b->d_mesh, pkind, b->dinv, b->r, b->v, b->p, b->ph,
                                                 b->dctl, b->ictl);
   if ((rc = spmv_b<MT, kWork>(b, b->ph, b->v, st))) return rc;
-  dot_batch_kernel<<<nc, kThreads, 0, st>>>(b->d_chunks, b->d_mesh, b->rh, b->v, nullptr, b->part, b->nchunks,
-                                             b->ictl);
-  bicg_alpha_batch_kernel<<<gm, 256, 0, st>>>(b->nmesh, b->d_cprefix, b->part, b->nchunks, b->dctl, b->ictl);
+  dot_fold_batch_kernel<1><<<nc, kThreads, 0, st>>>(b->d_chunks, b->d_mesh, b->d_cprefix, b->rh, b->v, b->part,
+                                                     b->nchunks, b->dctl, b->ictl, b->counters);
   bicg_s_batch_kernel<<<nc, kThreads, 0, st>>>(b->d_chunks, b->d_mesh, pkind, b->dinv, b->r, b->v, b->s, b->sh,
                                                 b->dctl, b->ictl);
   if ((rc = spmv_b<MT, kWork>(b, b->sh, b->t, st))) return rc;
-  dot_batch_kernel<<<nc, kThreads, 0, st>>>(b->d_chunks, b->d_mesh, b->t, b->s, b->t, b->part, b->nchunks, b->ictl);
-  bicg_omega_batch_kernel<<<gm, 256, 0, st>>>(b->nmesh, b->d_cprefix, b->part, b->nchunks, b->dctl, b->ictl);
-  bicg_xr_batch_kernel<XL><<<nc, kThreads, 0, st>>>(b->d_chunks, b->d_mesh, b->ph, b->sh, b->s, b->t, b->rh, xwork,
-                                                     b->r, b->dctl, b->ictl, b->part, b->nchunks);
-  bicg_end_batch_kernel<<<gm, 256, 0, st>>>(b->nmesh, b->d_cprefix, b->part, b->nchunks, b->dctl, b->ictl);
+  dot_fold_batch_kernel<2><<<nc, kThreads, 0, st>>>(b->d_chunks, b->d_mesh, b->d_cprefix, b->t, b->s, b->part,
+                                                     b->nchunks, b->dctl, b->ictl, b->counters);
+  bicg_xr_end_batch_kernel<XL><<<nc, kThreads, 0, st>>>(b->d_chunks, b->d_mesh, b->d_cprefix, b->ph, b->sh, b->s,
+                                                         b->t, b->rh, xwork, b->r, b->dctl, b->ictl, b->part,
+                                                         b->nchunks, b->counters);
   UFEM_CUDA_TRY(cudaGetLastError());
   return UFEM_OK;
 }
@@ -875,8 +900,19 @@ int bicgstab_b(ufem_batch* b, int pkind, double tol, int maxit, bool use_outer, 
       if (all) break;
       continue;
     }
-    if (all || blocks % kReplaceBlocks == 0) {
-      if ((rc = spmv_b<double, XL>(b, xw, b->w, st, fFinal))) return rc;
+    // members due for a replacement: not final, and either claiming
+    // convergence (or stopped) or kReplaceIters past their last replacement
+    bool any_due = false;
+    for (int m = 0; m < b->nmesh; ++m) {
+      int* f = b->h_ictl + m * kIc;
+      const bool due = !f[fFinal] && (f[fDone] || f[fIters] - f[fLastRepl] >= kReplaceIters);
+      f[fSkipRepl] = due ? 0 : 1;
+      any_due = any_due || due;
+    }
+    (void)blocks;
+    if (any_due) {
+      UFEM_CUDA_TRY(cudaMemcpyAsync(b->ictl, b->h_ictl, sizeof(int) * kIc * b->nmesh, cudaMemcpyHostToDevice, st));
+      if ((rc = spmv_b<double, XL>(b, xw, b->w, st, fSkipRepl))) return rc;
       replace_batch_kernel<BL><<<nc, kThreads, 0, st>>>(b->d_chunks, b->d_mesh, bw, b->w, b->r, b->rh, b->part,
                                                        b->nchunks, b->ictl);
       replace_end_batch_kernel<<<gm, 256, 0, st>>>(b->nmesh, b->d_cprefix, b->part, b->nchunks, b->dctl, b->ictl);
@@ -935,8 +971,8 @@ int ufem_batch_create(ufem_ns_handle* const* members, int32_t n, ufem_batch** ou
     const ufem_ns_handle* h = members[m];
     gprefix[m + 1] = gprefix[m] + h->wplan.ngroups;
     nprefix[m + 1] = nprefix[m] + h->N;
-    for (int64_t lo = 0; lo < h->nrows; lo += kChunkRows)
-      chunks.push_back(Chunk{m, int(lo), int(std::min<int64_t>(h->nrows, lo + kChunkRows)), 0});
+    for (int64_t n0 = 0; n0 < h->N; n0 += kChunkNodes)
+      chunks.push_back(Chunk{m, int(n0 * h->neq), int(std::min<int64_t>(h->N, n0 + kChunkNodes) * h->neq), 0});
     cprefix[m + 1] = int(chunks.size());
     b->total_rows += h->nrows;
   }
@@ -952,6 +988,7 @@ int ufem_batch_create(ufem_ns_handle* const* members, int32_t n, ufem_batch** ou
       (rc = dmal(&b->p, R)) || (rc = dmal(&b->v, R)) || (rc = dmal(&b->s, R)) || (rc = dmal(&b->t, R)) ||
       (rc = dmal(&b->ph, R)) || (rc = dmal(&b->sh, R)) || (rc = dmal(&b->dinv, R)) || (rc = dmal(&b->w, R)) ||
       (rc = dmal(&b->part, 2 * chunks.size())) || (rc = dmal(&b->dctl, size_t(kDc) * n)) ||
+      (rc = dmal(&b->counters, size_t(4) * n)) ||
       (rc = dmal(&b->ictl, size_t(kIc) * n))) {
     batch_free(b);
     return rc;
@@ -966,7 +1003,8 @@ int ufem_batch_create(ufem_ns_handle* const* members, int32_t n, ufem_batch** ou
           cudaSuccess ||
       (ce = cudaMemcpy(b->d_chunks, chunks.data(), chunks.size() * sizeof(Chunk), cudaMemcpyHostToDevice)) !=
           cudaSuccess ||
-      (ce = cudaMemcpy(b->d_cprefix, cprefix.data(), cprefix.size() * 4, cudaMemcpyHostToDevice)) != cudaSuccess) {
+      (ce = cudaMemcpy(b->d_cprefix, cprefix.data(), cprefix.size() * 4, cudaMemcpyHostToDevice)) != cudaSuccess ||
+      (ce = cudaMemset(b->counters, 0, sizeof(int) * 4 * n)) != cudaSuccess) {
     batch_free(b);
     return set_error(UFEM_ERR_CUDA, std::string("ufem_batch_create: ") + cudaGetErrorString(ce));
   }
