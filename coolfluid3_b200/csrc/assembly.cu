@@ -1358,44 +1358,60 @@ __global__ void dirichlet_values_kernel(int64_t nbc, int neq, const int64_t* __r
 
 // Part 2: rows that are not constrained move their constrained columns to the
 // RHS in first-application order (the order of the sequential reference).
+// One warp per row: the lanes load the row's constrained entries in parallel,
+// lane 0 adds them to the RHS one by one in first-application order (the
+// rounding of the sequential form: no FMA, no reassociation), then the lanes
+// zero the entries.
 __global__ void dirichlet_columns_kernel(int64_t nrows, const int64_t* __restrict__ fix_row,
                                          const int64_t* __restrict__ fix_ptr, const int64_t* __restrict__ fix_pos,
                                          const int32_t* __restrict__ fix_bc, const double* __restrict__ vfirst,
                                          double* __restrict__ vals, float* __restrict__ vals32,
                                          double* __restrict__ rhs) {
-  const int64_t q = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
-  if (q >= nrows) return;
+  const int64_t q = (int64_t(blockIdx.x) * blockDim.x + threadIdx.x) >> 5;
+  const int lane = threadIdx.x & 31;
+  if (q >= nrows) return;  // whole warp
   const int64_t row = fix_row[q];
   const int64_t k0 = fix_ptr[q], k1 = fix_ptr[q + 1];
   double r = rhs[row];
-  // all loads first (they pipeline), then the zeroing stores
-  for (int64_t k = k0; k < k1; ++k)
-    r = __dadd_rn(r, __dmul_rn(-vals[fix_pos[k]], vfirst[fix_bc[k]]));  // no FMA: rounding of the sequential form
-  for (int64_t k = k0; k < k1; ++k) {
-    const int64_t pos = fix_pos[k];
-    vals[pos] = 0.0;
-    if (vals32) vals32[pos] = 0.0f;
+  for (int64_t kb = k0; kb < k1; kb += 32) {
+    const int n = int(k1 - kb < 32 ? k1 - kb : 32);
+    double term = 0.0;
+    int64_t pos = -1;
+    if (lane < n) {
+      pos = fix_pos[kb + lane];
+      term = __dmul_rn(-vals[pos], vfirst[fix_bc[kb + lane]]);
+    }
+    for (int j = 0; j < n; ++j) {
+      const double tj = __shfl_sync(0xffffffffu, term, j);
+      r = __dadd_rn(r, tj);
+    }
+    if (lane < n) {
+      vals[pos] = 0.0;
+      if (vals32) vals32[pos] = 0.0f;
+    }
   }
-  rhs[row] = r;
+  if (lane == 0) rhs[row] = r;
 }
 
 // Part 3: constrained rows become identity rows; rhs = sol = last value - old.
+// One warp per constrained dof: the lanes zero the row (the diagonal entry is
+// written 1 in the same pass, so no ordering between lanes is needed).
 __global__ void dirichlet_rows_kernel(int64_t nbc, int neq, const int64_t* __restrict__ bc_dof,
                                       const double* __restrict__ last, const int64_t* __restrict__ bc_diag,
                                       const int64_t* __restrict__ rowptr, const double* __restrict__ state,
                                       double* __restrict__ vals, float* __restrict__ vals32,
                                       double* __restrict__ rhs, double* __restrict__ sol) {
-  const int64_t u = blockIdx.x;
+  const int64_t u = (int64_t(blockIdx.x) * blockDim.x + threadIdx.x) >> 5;
+  const int lane = threadIdx.x & 31;
   if (u >= nbc) return;
   const int64_t dof = bc_dof[u];
-  for (int64_t p = rowptr[dof] + threadIdx.x; p < rowptr[dof + 1]; p += blockDim.x) {
-    vals[p] = 0.0;
-    if (vals32) vals32[p] = 0.0f;
+  const int64_t diag = bc_diag[u];
+  for (int64_t p = rowptr[dof] + lane; p < rowptr[dof + 1]; p += 32) {
+    const double v = (p == diag) ? 1.0 : 0.0;
+    vals[p] = v;
+    if (vals32) vals32[p] = float(v);
   }
-  __syncthreads();
-  if (threadIdx.x == 0) {
-    vals[bc_diag[u]] = 1.0;
-    if (vals32) vals32[bc_diag[u]] = 1.0f;
+  if (lane == 0) {
     const int64_t node = dof / neq;
     const int comp = int(dof - node * neq);
     const double v = __dsub_rn(last[u], state[4 * node + comp]);
@@ -1647,11 +1663,12 @@ int launch_dirichlet(ufem_ns_handle* h, cudaStream_t s) {
                                                                          h->d_state, bp.vfirst);
   UFEM_CUDA_TRY(cudaGetLastError());
   if (bp.nfix_rows > 0) {
-    dirichlet_columns_kernel<<<unsigned((bp.nfix_rows + 127) / 128), 128, 0, s>>>(
+    dirichlet_columns_kernel<<<unsigned((bp.nfix_rows * 32 + 255) / 256), 256, 0, s>>>(
         bp.nfix_rows, bp.fix_row, bp.fix_ptr, bp.fix_pos, bp.fix_bc, bp.vfirst, h->d_vals, h->d_vals32, h->d_rhs);
     UFEM_CUDA_TRY(cudaGetLastError());
   }
-  dirichlet_rows_kernel<<<unsigned(bp.nbc), 64, 0, s>>>(bp.nbc, h->neq, bp.bc_dof, bp.bc_last, bp.bc_diag,
+  dirichlet_rows_kernel<<<unsigned((bp.nbc * 32 + 255) / 256), 256, 0, s>>>(bp.nbc, h->neq, bp.bc_dof, bp.bc_last,
+                                                                            bp.bc_diag,
                                                         h->d_rowptr, h->d_state, h->d_vals, h->d_vals32, h->d_rhs,
                                                         h->d_sol);
   UFEM_CUDA_TRY(cudaGetLastError());

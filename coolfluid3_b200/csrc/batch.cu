@@ -175,7 +175,8 @@ __global__ void dirichlet_values_batch_kernel(int64_t total, int nmesh, const in
 
 __global__ void dirichlet_columns_batch_kernel(int64_t total, int nmesh, const int64_t* __restrict__ fix_prefix,
                                                const BatchMesh* __restrict__ bm) {
-  const int64_t g = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+  const int64_t g = (int64_t(blockIdx.x) * blockDim.x + threadIdx.x) >> 5;  // one warp per row
+  const int lane = threadIdx.x & 31;
   if (g >= total) return;
   const int m = find_mesh(fix_prefix, nmesh, g);
   const BatchMesh& M = bm[m];
@@ -183,30 +184,39 @@ __global__ void dirichlet_columns_batch_kernel(int64_t total, int nmesh, const i
   const int64_t row = M.fix_row[q];
   const int64_t k0 = M.fix_ptr[q], k1 = M.fix_ptr[q + 1];
   double r = M.rhs[row];
-  for (int64_t k = k0; k < k1; ++k) r = __dadd_rn(r, __dmul_rn(-M.vals[M.fix_pos[k]], M.vfirst[M.fix_bc[k]]));
-  for (int64_t k = k0; k < k1; ++k) {
-    const int64_t pos = M.fix_pos[k];
-    M.vals[pos] = 0.0;
-    if (M.vals32) M.vals32[pos] = 0.0f;
+  for (int64_t kb = k0; kb < k1; kb += 32) {
+    const int n = int(k1 - kb < 32 ? k1 - kb : 32);
+    double term = 0.0;
+    int64_t pos = -1;
+    if (lane < n) {
+      pos = M.fix_pos[kb + lane];
+      term = __dmul_rn(-M.vals[pos], M.vfirst[M.fix_bc[kb + lane]]);
+    }
+    for (int j = 0; j < n; ++j) r = __dadd_rn(r, __shfl_sync(0xffffffffu, term, j));  // first-application order
+    if (lane < n) {
+      M.vals[pos] = 0.0;
+      if (M.vals32) M.vals32[pos] = 0.0f;
+    }
   }
-  M.rhs[row] = r;
+  if (lane == 0) M.rhs[row] = r;
 }
 
-__global__ void dirichlet_rows_batch_kernel(int nmesh, const int64_t* __restrict__ bc_prefix,
+__global__ void dirichlet_rows_batch_kernel(int64_t total, int nmesh, const int64_t* __restrict__ bc_prefix,
                                             const BatchMesh* __restrict__ bm) {
-  const int64_t g = blockIdx.x;
+  const int64_t g = (int64_t(blockIdx.x) * blockDim.x + threadIdx.x) >> 5;  // one warp per constrained dof
+  const int lane = threadIdx.x & 31;
+  if (g >= total) return;
   const int m = find_mesh(bc_prefix, nmesh, g);
   const BatchMesh& M = bm[m];
   const int64_t u = g - bc_prefix[m];
   const int64_t dof = M.bc_dof[u];
-  for (int64_t p = M.rowptr[dof] + threadIdx.x; p < M.rowptr[dof + 1]; p += blockDim.x) {
-    M.vals[p] = 0.0;
-    if (M.vals32) M.vals32[p] = 0.0f;
+  const int64_t diag = M.bc_diag[u];
+  for (int64_t p = M.rowptr[dof] + lane; p < M.rowptr[dof + 1]; p += 32) {
+    const double v = (p == diag) ? 1.0 : 0.0;
+    M.vals[p] = v;
+    if (M.vals32) M.vals32[p] = float(v);
   }
-  __syncthreads();
-  if (threadIdx.x == 0) {
-    M.vals[M.bc_diag[u]] = 1.0;
-    if (M.vals32) M.vals32[M.bc_diag[u]] = 1.0f;
+  if (lane == 0) {
     const int64_t node = dof / M.neq;
     const int comp = int(dof - node * M.neq);
     const double v = __dsub_rn(M.bc_last[u], M.state[4 * node + comp]);
@@ -1060,9 +1070,10 @@ int ufem_batch_assemble(ufem_batch* b, void* stream) {
     dirichlet_values_batch_kernel<<<blocks_for(b->total_bc, 256), 256, 0, st>>>(b->total_bc, b->nmesh,
                                                                                  b->d_bc_prefix, b->d_mesh);
     if (b->total_fix > 0)
-      dirichlet_columns_batch_kernel<<<blocks_for(b->total_fix, 128), 128, 0, st>>>(b->total_fix, b->nmesh,
-                                                                                    b->d_fix_prefix, b->d_mesh);
-    dirichlet_rows_batch_kernel<<<unsigned(b->total_bc), 64, 0, st>>>(b->nmesh, b->d_bc_prefix, b->d_mesh);
+      dirichlet_columns_batch_kernel<<<blocks_for(b->total_fix * 32, 256), 256, 0, st>>>(b->total_fix, b->nmesh,
+                                                                                         b->d_fix_prefix, b->d_mesh);
+    dirichlet_rows_batch_kernel<<<blocks_for(b->total_bc * 32, 256), 256, 0, st>>>(b->total_bc, b->nmesh,
+                                                                                   b->d_bc_prefix, b->d_mesh);
     UFEM_CUDA_TRY(cudaGetLastError());
   }
   return UFEM_OK;
