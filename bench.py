@@ -52,7 +52,7 @@ def parse():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--n", type=int, default=64, help="cells per cube side (64 = the benchmark configuration)")
     ap.add_argument("--precision", default="fp64", choices=["fp64", "fp32"])
-    ap.add_argument("--asm-kernel", default="auto", choices=["auto", "warp", "chunk"],
+    ap.add_argument("--asm-kernel", default="auto", choices=["auto", "warp", "warp24", "chunk"],
                     help="assembly kernel variant; auto = the library's autotuner picks it on this mesh")
     ap.add_argument("--asm-warps", type=int, default=4, choices=[2, 4, 8],
                     help="warps per CTA of the warp assembly kernel when --asm-kernel is given")
@@ -110,18 +110,63 @@ def barrier(world):
 
 
 class ClockSampler:
-    """nvidia-smi clock/throttle samples during the timed region."""
+    """SM clock and clock-event-reason samples taken DURING the timed region.
+
+    A timed region of K assembly steps lasts only tens of milliseconds, shorter
+    than nvidia-smi's 200 ms sampling period, so a thread polls NVML (the
+    library behind nvidia-smi) every `interval` seconds while the region runs;
+    without NVML it falls back to `nvidia-smi -lms 200`.  Read-only queries.
+    """
 
     FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
               "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
               "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+    NAMES = ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap")
 
-    def __init__(self, gpu_index: int):
+    def __init__(self, gpu_index: int, interval: float = 0.002):
         self.gpu = gpu_index
+        self.interval = interval
         self.proc = None
+        self.thread = None
+        self.samples: list[tuple[float, float, int]] = []  # (sm MHz, max sm MHz, reason bits)
         self.path = os.path.join("/tmp", f"ufem_clocks_{os.getpid()}.csv")
 
+    def _nvml_handle(self, nv):
+        try:
+            import torch
+            uuid = str(torch.cuda.get_device_properties(self.gpu).uuid)
+            return nv.nvmlDeviceGetHandleByUUID(uuid if uuid.startswith("GPU-") else "GPU-" + uuid)
+        except Exception:
+            return nv.nvmlDeviceGetHandleByIndex(self.gpu)
+
     def __enter__(self):
+        import threading
+        try:
+            import pynvml as nv
+            nv.nvmlInit()
+            h = self._nvml_handle(nv)
+            bits = (nv.nvmlClocksEventReasonHwSlowdown, nv.nvmlClocksEventReasonHwThermalSlowdown,
+                    nv.nvmlClocksEventReasonSwThermalSlowdown, nv.nvmlClocksEventReasonSwPowerCap)
+            mx = float(nv.nvmlDeviceGetMaxClockInfo(h, nv.NVML_CLOCK_SM))
+            self.stop = threading.Event()
+
+            def poll():
+                while True:
+                    try:
+                        sm = float(nv.nvmlDeviceGetClockInfo(h, nv.NVML_CLOCK_SM))
+                        r = int(nv.nvmlDeviceGetCurrentClocksEventReasons(h))
+                        self.samples.append((sm, mx, sum(1 << k for k, b in enumerate(bits) if r & b)))
+                    except Exception:
+                        return
+                    if self.stop.wait(self.interval):
+                        return
+
+            poll_once = threading.Thread(target=poll, daemon=True)
+            self.thread = poll_once
+            poll_once.start()
+            return self
+        except Exception:
+            self.thread = None
         try:
             self.proc = subprocess.Popen(
                 ["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
@@ -131,6 +176,9 @@ class ClockSampler:
         return self
 
     def __exit__(self, *exc):
+        if self.thread is not None:
+            self.stop.set()
+            self.thread.join(timeout=5)
         if self.proc is not None:
             self.proc.terminate()
             try:
@@ -139,6 +187,13 @@ class ClockSampler:
                 self.proc.kill()
 
     def summary(self) -> dict:
+        if self.thread is not None:
+            if not self.samples:
+                return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"], "source": "nvml"}
+            reasons = sorted({self.NAMES[k] for _, _, r in self.samples for k in range(4) if r >> k & 1})
+            return {"sm_mhz": statistics.median(s for s, _, _ in self.samples),
+                    "sm_max_mhz": max(m for _, m, _ in self.samples), "reasons": reasons,
+                    "samples": len(self.samples), "source": "nvml"}
         try:
             rows = [line.split(",") for line in open(self.path).read().strip().splitlines() if line.strip()]
         except Exception:
@@ -147,11 +202,10 @@ class ClockSampler:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"]}
         sm = [float(r[1]) for r in rows if r[1].strip().replace(".", "").isdigit()]
         mx = [float(r[2]) for r in rows if r[2].strip().replace(".", "").isdigit()]
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        reasons = sorted({names[k] for r in rows for k in range(4) if len(r) > 5 + k and "Active" in r[5 + k]
+        reasons = sorted({self.NAMES[k] for r in rows for k in range(4) if len(r) > 5 + k and "Active" in r[5 + k]
                           and "Not" not in r[5 + k]})
         return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
-                "reasons": reasons, "samples": len(rows)}
+                "reasons": reasons, "samples": len(rows), "source": "nvidia-smi"}
 
 
 def algorithmic_bytes(E, N, nnz, dim):
@@ -242,7 +296,8 @@ def run_ours(args, rank, world, local):
         ns.set_assembly_kernel(args.asm_kernel, args.asm_warps)
         tuned = None
     asm_variant, asm_warps = ns.assembly_kernel()
-    big_rows = int((np.bincount(pb.conn.ravel(), minlength=Nn) > 32).sum())
+    lanes = 24 if asm_variant == "warp24" else 32  # incidences a warp group holds; longer rows go to the chunk kernel
+    big_rows = int((np.bincount(pb.conn.ravel(), minlength=Nn) > lanes).sum())
     asm_launches = 1 if asm_variant == "chunk" else 1 + (1 if big_rows else 0)  # warp kernel + chunk kernel for big rows
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)  # 256 MiB > 126 MB L2
 
