@@ -27,6 +27,7 @@
 #include <vector>
 
 #include "internal.h"
+#include "spmv_node.cuh"
 
 namespace ufem {
 namespace {
@@ -238,9 +239,9 @@ __device__ __forceinline__ double* vec(const BatchMesh& M, double* work) {
   else return work + M.row_off;
 }
 
-// y = A x, one warp per node over all members (FP64 accumulation, as spmv_kernel).
+// y = A x, one warp per node over all members (spmv_node, as spmv_kernel).
 template <int NEQ, typename MT, int XL>
-__global__ void __launch_bounds__(256) spmv_batch_kernel(int64_t total_nodes, int nmesh,
+__global__ void __launch_bounds__(256, 6) spmv_batch_kernel(int64_t total_nodes, int nmesh,
                                                          const int64_t* __restrict__ node_prefix,
                                                          const BatchMesh* __restrict__ bm, double* xwork,
                                                          double* __restrict__ ywork, const int* __restrict__ ictl,
@@ -257,33 +258,8 @@ __global__ void __launch_bounds__(256) spmv_batch_kernel(int64_t total_nodes, in
   const MT* vals;
   if constexpr (std::is_same<MT, float>::value) vals = M.vals32; else vals = M.vals;
   const int64_t s0 = __ldg(M.start + node);
-  const int len = int(__ldg(M.start + node + 1) - s0) * NEQ;
-  const MT* row = vals + int64_t(NEQ) * NEQ * s0;
-  double acc[NEQ];
-#pragma unroll
-  for (int r = 0; r < NEQ; ++r) acc[r] = 0.0;
-  for (int j = lane; j < len; j += 32) {
-    const int s = j / NEQ;
-    const int c = j - s * NEQ;
-    const double xj = x[int64_t(__ldg(M.adj + s0 + s)) * NEQ + c];
-    MT v[NEQ];
-#pragma unroll
-    for (int r = 0; r < NEQ; ++r) v[r] = __ldcs(row + r * len + j);
-#pragma unroll
-    for (int r = 0; r < NEQ; ++r) acc[r] += double(v[r]) * xj;
-  }
-#pragma unroll
-  for (int r = 0; r < NEQ; ++r) {
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) acc[r] += __shfl_xor_sync(0xffffffffu, acc[r], o);
-  }
-  if (lane < NEQ) {
-    double out = acc[0];
-#pragma unroll
-    for (int r = 1; r < NEQ; ++r)
-      if (lane == r) out = acc[r];
-    y[node * NEQ + lane] = out;
-  }
+  const int S = int(__ldg(M.start + node + 1) - s0);
+  spmv_node<NEQ, MT, double, double>(vals + int64_t(NEQ) * NEQ * s0, S, M.adj + s0, x, lane, y + node * NEQ);
 }
 
 // dinv = 1 / diag (point Jacobi) of the operator the solve uses.
@@ -295,6 +271,7 @@ __global__ void jacobi_batch_kernel(const Chunk* __restrict__ chunks, const Batc
   const BatchMesh& M = bm[c.mesh];
   const MT* vals;
   if constexpr (std::is_same<MT, float>::value) vals = M.vals32; else vals = M.vals;
+#pragma unroll 4
   for (int i = c.lo + threadIdx.x; i < c.hi; i += blockDim.x) {
     const double d = double(vals[M.diagpos[i]]);
     dinv[M.row_off + i] = d != 0.0 ? 1.0 / d : 1.0;
@@ -314,6 +291,7 @@ __global__ void residual_batch_kernel(const Chunk* __restrict__ chunks, const Ba
   const double* b = vec<BL>(M, bwork);
   const int64_t off = M.row_off;
   double s2 = 0.0, b2 = 0.0;
+#pragma unroll 4
   for (int i = c.lo + threadIdx.x; i < c.hi; i += blockDim.x) {
     const double bi = b[i];
     const double ri = bi - w[off + i];
@@ -378,6 +356,7 @@ __global__ void dot_fold_batch_kernel(const Chunk* __restrict__ chunks, const Ba
   if (ictl[m * kIc + fDone]) return;  // uniform per CTA
   const int64_t off = bm[m].row_off;
   double pa = 0.0, pb = 0.0;
+#pragma unroll 4
   for (int i = c.lo + threadIdx.x; i < c.hi; i += blockDim.x) {
     const int64_t k = off + i;
     const double ai = a[k];
@@ -445,6 +424,7 @@ __global__ void bicg_xr_end_batch_kernel(const Chunk* __restrict__ chunks, const
   const int64_t off = M.row_off;
   double* x = vec<XL>(M, xwork);
   double rr = 0.0, hr = 0.0;
+#pragma unroll 4
   for (int i = c.lo + threadIdx.x; i < c.hi; i += blockDim.x) {
     const int64_t k = off + i;
     x[i] = x[i] + al * ph[k] + om * sh[k];
@@ -530,6 +510,7 @@ __global__ void bicg_p_batch_kernel(const Chunk* __restrict__ chunks, const Batc
   const double beta = (d[sRho] / d[sRhoOld]) * (d[sAlpha] / d[sOmega]);
   const double om = d[sOmega];
   const int64_t off = bm[c.mesh].row_off;
+#pragma unroll 4
   for (int i = c.lo + threadIdx.x; i < c.hi; i += blockDim.x) {
     const int64_t k = off + i;
     const double pi = r[k] + beta * (p[k] - om * v[k]);
@@ -549,6 +530,7 @@ __global__ void bicg_s_batch_kernel(const Chunk* __restrict__ chunks, const Batc
   if (ictl[c.mesh * kIc + fDone]) return;
   const double al = dctl[c.mesh * kDc + sAlpha];
   const int64_t off = bm[c.mesh].row_off;
+#pragma unroll 4
   for (int i = c.lo + threadIdx.x; i < c.hi; i += blockDim.x) {
     const int64_t k = off + i;
     const double si = r[k] - al * v[k];
@@ -591,6 +573,7 @@ __global__ void replace_batch_kernel(const Chunk* __restrict__ chunks, const Bat
   const double* b = vec<BL>(M, bwork);
   const int64_t off = M.row_off;
   double rr = 0.0, hr = 0.0;
+#pragma unroll 4
   for (int i = c.lo + threadIdx.x; i < c.hi; i += blockDim.x) {
     const double ri = b[i] - w[off + i];
     r[off + i] = ri;
@@ -657,6 +640,7 @@ __global__ void zero_batch_kernel(const Chunk* __restrict__ chunks, const BatchM
                                   double* __restrict__ a, double* __restrict__ b) {
   const Chunk c = chunks[blockIdx.x];
   const int64_t off = bm[c.mesh].row_off;
+#pragma unroll 4
   for (int i = c.lo + threadIdx.x; i < c.hi; i += blockDim.x) {
     a[off + i] = 0.0;
     if (b) b[off + i] = 0.0;

@@ -19,6 +19,7 @@
 #include <vector>
 
 #include "internal.h"
+#include "spmv_node.cuh"
 
 namespace ufem {
 
@@ -74,50 +75,27 @@ __device__ __forceinline__ double block_sum(double v, double* sm) {
 }
 
 #define GRID_STRIDE(i, n) \
-  for (int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < (n); i += int64_t(gridDim.x) * blockDim.x)
+  _Pragma("unroll 4") for (int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < (n); i += int64_t(gridDim.x) * blockDim.x)
 
 // y = A x on the node graph, FEVbr point layout: the NEQ rows of a node are
 // contiguous (row r, neighbour slot s, component c at r*S*NEQ + s*NEQ + c).
-// One warp per node; a lane owns columns j = lane, lane+32, ... of the block
-// row, gathers x once per column and multiplies it into all NEQ rows (row
-// values are read coalesced across the warp).  FP64 accumulation.
+// One warp per node (spmv_node: for NEQ = 4 a lane owns column pairs of one
+// neighbour, 16-byte value and x loads, coalesced across the warp), FP64
+// accumulation, fixed-order warp reduction; 48 resident warps per SM.
 template <int NEQ, typename VT, typename MT>
-__global__ void __launch_bounds__(256) spmv_kernel(int64_t N, const int64_t* __restrict__ start,
-                                                   const int32_t* __restrict__ adj, const MT* __restrict__ vals,
-                                                   const VT* __restrict__ x, VT* __restrict__ y,
-                                                   const int* __restrict__ done) {
-  if (done && *done) return;
+__global__ void __launch_bounds__(256, 6) spmv_kernel(int64_t N, const int64_t* __restrict__ start,
+                                                      const int32_t* __restrict__ adj, const MT* __restrict__ vals,
+                                                      const VT* __restrict__ x, VT* __restrict__ y,
+                                                      const int* __restrict__ done) {
   const int64_t node = (int64_t(blockIdx.x) * blockDim.x + threadIdx.x) >> 5;
   const int lane = threadIdx.x & 31;
   if (node >= N) return;
+  // the done flag and the row extent are loaded together (no dependent round trip)
+  const int stop = done ? *done : 0;
   const int64_t s0 = __ldg(start + node);
-  const int len = int(__ldg(start + node + 1) - s0) * NEQ;
-  const MT* row = vals + int64_t(NEQ) * NEQ * s0;
-  double acc[NEQ];
-#pragma unroll
-  for (int r = 0; r < NEQ; ++r) acc[r] = 0.0;
-  for (int j = lane; j < len; j += 32) {
-    const int s = j / NEQ;
-    const int c = j - s * NEQ;
-    const double xj = double(x[int64_t(__ldg(adj + s0 + s)) * NEQ + c]);
-    MT v[NEQ];
-#pragma unroll
-    for (int r = 0; r < NEQ; ++r) v[r] = __ldcs(row + r * len + j);  // streamed once per SpMV
-#pragma unroll
-    for (int r = 0; r < NEQ; ++r) acc[r] += double(v[r]) * xj;
-  }
-#pragma unroll
-  for (int r = 0; r < NEQ; ++r) {
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) acc[r] += __shfl_xor_sync(0xffffffffu, acc[r], o);  // every lane: full sum
-  }
-  if (lane < NEQ) {
-    double out = acc[0];
-#pragma unroll
-    for (int r = 1; r < NEQ; ++r)
-      if (lane == r) out = acc[r];
-    y[node * NEQ + lane] = VT(out);
-  }
+  const int S = int(__ldg(start + node + 1) - s0);
+  if (stop) return;
+  spmv_node<NEQ, MT, VT, VT>(vals + int64_t(NEQ) * NEQ * s0, S, adj + s0, x, lane, y + node * NEQ);
 }
 
 template <typename MT, typename VT>

@@ -1,0 +1,100 @@
+// spmv_node.cuh -- one node's block row times x, one warp per node (device code
+// shared by the one-mesh and the batched Krylov solvers).
+//
+// The point CSR keeps every node's NEQ rows contiguous over one sorted
+// neighbourhood of S nodes: row r of the node holds NEQ*S values starting at
+// row_base + r*NEQ*S, column (s, c) at offset s*NEQ + c (s = neighbour slot).
+// For NEQ = 4 a lane owns column PAIRS (s, 2h..2h+1): one 16-byte (FP64) or
+// 8-byte (FP32) load per row and one for the two x entries, which are
+// contiguous because both columns belong to the same neighbour.  NEQ = 3 keeps
+// one column per lane.  The NEQ row sums are reduced over the warp with a
+// butterfly that halves the number of values per lane in the first two steps
+// (6 shuffles instead of 5 per row), in a fixed order, so results are
+// deterministic.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <type_traits>
+
+namespace ufem {
+
+template <typename T>
+struct Pair;
+template <>
+struct Pair<double> { using type = double2; };
+template <>
+struct Pair<float> { using type = float2; };
+
+// Sums a[0..3] over the warp.  Afterwards the lanes 8r .. 8r+7 hold the total
+// of a[r] (all eight the same value).
+__device__ __forceinline__ double warp_sum4(const double (&a)[4], int lane) {
+  constexpr unsigned FULL = 0xffffffffu;
+  const bool up16 = (lane & 16) != 0;
+  const double b0 = (up16 ? a[2] : a[0]) + __shfl_xor_sync(FULL, up16 ? a[0] : a[2], 16);
+  const double b1 = (up16 ? a[3] : a[1]) + __shfl_xor_sync(FULL, up16 ? a[1] : a[3], 16);
+  const bool up8 = (lane & 8) != 0;
+  double c = (up8 ? b1 : b0) + __shfl_xor_sync(FULL, up8 ? b0 : b1, 8);
+  c += __shfl_xor_sync(FULL, c, 4);
+  c += __shfl_xor_sync(FULL, c, 2);
+  c += __shfl_xor_sync(FULL, c, 1);
+  return c;
+}
+
+// Partial row sums of one node's block row: acc[r] += sum over this lane's
+// columns of row r.  `row` points at the node's first value, S is the number
+// of neighbours (the node itself included), `adj` the node's neighbour list.
+template <int NEQ, typename MT, typename VT>
+__device__ __forceinline__ void spmv_node_partial(const MT* __restrict__ row, int S, const int32_t* __restrict__ adj,
+                                                  const VT* __restrict__ x, int lane, double (&acc)[4]) {
+  if constexpr (NEQ == 4) {
+    using MP = typename Pair<MT>::type;
+    using XP = typename Pair<VT>::type;
+    const MP* __restrict__ rp = reinterpret_cast<const MP*>(row);
+    const int stride = 2 * S;  // pairs per row
+#pragma unroll 1
+    for (int p = lane; p < 2 * S; p += 32) {
+      const int s = p >> 1;
+      const int c0 = (p & 1) * 2;
+      const int col = __ldg(adj + s);
+      const XP xv = __ldg(reinterpret_cast<const XP*>(x + int64_t(col) * 4 + c0));
+      MP v[4];
+#pragma unroll
+      for (int r = 0; r < 4; ++r) v[r] = __ldcs(rp + (r * stride + p));  // streamed once
+#pragma unroll
+      for (int r = 0; r < 4; ++r) {
+        acc[r] = fma(double(v[r].x), double(xv.x), acc[r]);
+        acc[r] = fma(double(v[r].y), double(xv.y), acc[r]);
+      }
+    }
+  } else {
+    const int len = NEQ * S;
+#pragma unroll 1
+    for (int j = lane; j < len; j += 32) {
+      const int s = j / NEQ;
+      const int c = j - s * NEQ;
+      const double xj = double(__ldg(x + int64_t(__ldg(adj + s)) * NEQ + c));
+      MT v[NEQ];
+#pragma unroll
+      for (int r = 0; r < NEQ; ++r) v[r] = __ldcs(row + r * len + j);
+#pragma unroll
+      for (int r = 0; r < NEQ; ++r) acc[r] = fma(double(v[r]), xj, acc[r]);
+    }
+  }
+}
+
+// y[0..NEQ) of one node = its block row times x (FP64 accumulation), written by
+// lanes 0, 8, 16 (, 24).
+template <int NEQ, typename MT, typename VT, typename YT>
+__device__ __forceinline__ void spmv_node(const MT* __restrict__ row, int S, const int32_t* __restrict__ adj,
+                                          const VT* __restrict__ x, int lane, YT* __restrict__ y) {
+  double acc[4] = {0.0, 0.0, 0.0, 0.0};
+  spmv_node_partial<NEQ, MT, VT>(row, S, adj, x, lane, acc);
+  const double sum = warp_sum4(acc, lane);
+  const int r = lane >> 3;
+  if ((lane & 7) == 0 && r < NEQ) y[r] = YT(sum);
+}
+
+
+}  // namespace ufem
