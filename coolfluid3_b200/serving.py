@@ -17,8 +17,10 @@ steps) arrive over time.  The server
     ``ufem.Batch``); larger requests, whose solves already fill the GPU, run
     one per worker on `large_workers` further workers so that they do not hold
     back the small ones.  Every worker has its own CUDA stream, so the classes
-    overlap on the device; requests that arrive while others run join at the
-    next tick, finished ones leave;
+    overlap on the device (the batching workers' streams have the higher
+    priority: their kernels are short and latency-bound, the large requests'
+    are bandwidth-bound and fill the gaps); requests that arrive while others
+    run join at the next tick, finished ones leave;
   * reports throughput (time steps per second) beside p50/p99 step latency
     and request latency.
 
@@ -171,7 +173,7 @@ class Server:
     def __init__(self, hbm_budget_bytes: int, max_slots: int = 64, precision: str = "fp64", mixed: bool = True,
                  krylov: dict | None = None, graphs: bool = True, creators: int = 2,
                  use_specializations: bool = False, realtime: bool = True, large_rows: int = 200_000,
-                 large_workers: int = 2):
+                 large_workers: int = 2, small_priority: bool = True):
         if precision not in ("fp32", "fp64"):
             raise ValueError("precision must be fp32 or fp64")
         self.budget = int(hbm_budget_bytes)
@@ -183,6 +185,7 @@ class Server:
         self.realtime = realtime
         self.large_rows = int(large_rows)
         self.large_workers = int(large_workers)
+        self.small_priority = bool(small_priority)
         self.krylov = dict(method="bicgstab", precond="jacobi", tol=1e-10, max_iters=3000)
         if mixed:
             self.krylov.update(mixed=True, inner_tol=1e-6, max_refine=20)
@@ -232,7 +235,9 @@ class Server:
         now = lambda: time.perf_counter() - t0  # noqa: E731
 
         def worker(key: tuple, capacity: int):
-            stream = torch.cuda.Stream()
+            # the batched small requests are latency-bound: a high-priority stream lets
+            # their short kernels start ahead of the large requests' queued work
+            stream = torch.cuda.Stream(priority=-1 if (self.small_priority and key[1] == "small") else 0)
             active: list[_Active] = []
             batch = None
             members = None
