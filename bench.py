@@ -68,6 +68,7 @@ def parse():
                          "converge on larger 2D lid-driven meshes at dt = 0.01)")
     ap.add_argument("--serve-steps", type=int, default=10, help="time steps per served request")
     ap.add_argument("--serve-budget-gb", type=float, default=60.0, help="HBM budget of the server (GB)")
+    ap.add_argument("--serve-reps", type=int, default=3, help="served runs per form (the median is reported)")
     return ap.parse_args()
 
 
@@ -479,13 +480,22 @@ def serving_compare(args):
         "plain": dict(pick(pst, plain), form="FP64 elements, FP64 BiCGStab + Jacobi, one request at a time"),
     }
     for label, mixed in (("served_fp64", False), ("served_mixed", True)):
-        srv = S.Server(int(args.serve_budget_gb * 1e9), precision="fp64", mixed=mixed, krylov=dict(tol=1e-10),
-                       realtime=True)
-        res, st = srv.run(reqs)
+        # the served makespan depends on how the threads and streams interleave on
+        # the device, so each form is served `serve_reps` times and the run with
+        # the median throughput is reported (with the range)
+        runs = []
+        for _ in range(max(1, args.serve_reps)):
+            srv = S.Server(int(args.serve_budget_gb * 1e9), precision="fp64", mixed=mixed, krylov=dict(tol=1e-10),
+                           realtime=True)
+            res, st = srv.run(reqs)
+            runs.append((st["steps_per_s"], st, res, srv))
+        runs.sort(key=lambda x: x[0])
+        _, st, res, srv = runs[len(runs) // 2]
         diffs = [float(np.linalg.norm(a.state - b.state) / np.linalg.norm(b.state))
                  for a, b in zip(res, plain) if a.ok and b.ok]
         out[label] = dict(pick(st, res), max_batch=srv.max_batch, peak_reserved_gb=round(srv.peak_bytes / 1e9, 3),
                           speedup_steps_per_s=round(st["steps_per_s"] / pst["steps_per_s"], 3),
+                          runs_steps_per_s=[round(r[0], 2) for r in runs],
                           max_rel_diff_vs_plain=max(diffs) if diffs else None,
                           form=("FP64 elements, " + ("FP32 operator copy + FP64 residual replacement"
                                                      if mixed else "FP64 BiCGStab + Jacobi")
