@@ -165,11 +165,12 @@ __device__ __forceinline__ void metric_tensor(const T (&G)[D][D + 1], int a, T (
 #pragma unroll
   for (int m = 0; m < D; ++m)
 #pragma unroll
-    for (int q = 0; q < D; ++q) {
+    for (int q = m; q < D; ++q) {  // symmetric: the same products in the same order
       T s = 0;
 #pragma unroll
       for (int r = 0; r < D; ++r) s += col[m][r] * col[q][r];
       g[m][q] = s;
+      g[q][m] = s;
     }
 }
 
@@ -221,8 +222,8 @@ __device__ __forceinline__ void compute_tau(const KParams<T>& kp, const Elem<D, 
     const T diff = element_nu * element_nu * sq;
     tsu = T(1) / tsqrt(kp.tau_c1 + adv_sq + c2 * diff);  // tau_c1 = 4 c1^2 / dt^2
     tps = tsu;
-    const T tsu_std = T(1) / tsqrt(kp.tau_std + adv_sq + T(16) * diff);  // tau_std = 4 / dt^2
-    tbu = (T(1) / tsu_std) / tr;
+    // 1 / tau_su of the standard constants (tau_std = 4 / dt^2)
+    tbu = tsqrt(kp.tau_std + adv_sq + T(16) * diff) / tr;
   } else {  // CF2
     const T volume = (D == 2) ? det / T(2) : det / T(6);
     const T pi = T(3.141592654);
@@ -390,11 +391,12 @@ __device__ __forceinline__ void generic_row(const int (&ids)[4], int a, const No
     T s = 0, m = 0;
 #pragma unroll
     for (int b = 0; b < n; ++b) {
-      s += Nc[b] * el.U[b][k];
+      if constexpr (D == 2) s += Nc[b] * el.U[b][k];
       m += el.U[b][k];
     }
-    uc[k] = s;
     ub[k] = m * inv_n;
+    // tetrahedra: N_b(centroid) = 1/4 exactly, so the centroid value is the mean
+    uc[k] = (D == 3) ? ub[k] : s;
   }
   T J[D][D], Ji[D][D], det;
 #pragma unroll
@@ -405,9 +407,9 @@ __device__ __forceinline__ void generic_row(const int (&ids)[4], int a, const No
   T G[D][n];
 #pragma unroll
   for (int r = 0; r < D; ++r) {
-    T s = 0;
+    T s = -Ji[r][0];
 #pragma unroll
-    for (int k = 0; k < D; ++k) s += Ji[r][k] * T(-1);
+    for (int k = 1; k < D; ++k) s -= Ji[r][k];
     G[r][0] = s;
 #pragma unroll
     for (int b = 1; b <= D; ++b) G[r][b] = Ji[r][b - 1];
@@ -485,6 +487,14 @@ __device__ __forceinline__ void generic_row(const int (&ids)[4], int a, const No
     ax[i] = 0;
   }
   const T theta = kp.theta, invdt = kp.invdt, inv_rho = kp.inv_rho;
+  const T thS = theta * sWS * inv_rho;  // u rows, p column: theta * G_ib * sWS / rho
+  const T tpv = tps * inv_rho * V;      // p row, p column: tps * D0_b * V / rho
+  T cj[D], ej[D];                        // p row, u_j columns: G_jb sWSp + cj Vab + ej
+#pragma unroll
+  for (int j = 0; j < D; ++j) {
+    cj[j] = tps * G[j][0];
+    ej[j] = invdt * (cj[j] * m1);
+  }
 #pragma unroll
   for (int b = 0; b < n; ++b) {
     const T Kd = nu_bar * V * D0[b] + m2 * (nT * alpha[b] + c0[b]);
@@ -502,15 +512,15 @@ __device__ __forceinline__ void generic_row(const int (&ids)[4], int a, const No
       T row[neq];
 #pragma unroll
       for (int j = 0; j < D; ++j) row[j] = tg * G[j][b] + (i == j ? diag : T(0));
-      row[D] = theta * (G[i][b] * sWS * inv_rho);
+      row[D] = G[i][b] * thS;
       put_row<neq, T>(st, (b * neq + i) * neq, CH, row);
     }
     // row p: theta * (A / theta) + invdt * T = A + invdt * T
     {
       T row[neq];
 #pragma unroll
-      for (int j = 0; j < D; ++j) row[j] = G[j][b] * sWSp + tps * G[j][0] * Vab + invdt * (tps * G[j][0] * m1);
-      row[D] = tps * D0[b] * inv_rho * V;
+      for (int j = 0; j < D; ++j) row[j] = G[j][b] * sWSp + (cj[j] * Vab + ej[j]);
+      row[D] = D0[b] * tpv;
       put_row<neq, T>(st, (b * neq + D) * neq, CH, row);
     }
     // pieces of A x
@@ -1193,6 +1203,7 @@ __global__ void __launch_bounds__(32 * WPB, warp_min_blocks<D, T, KC, WPB>()) ns
       const int row = row0 + rl;
       const T* src = stage + (j < neq * neq ? j : nvals + (j - neq * neq));  // b = 0 block, or the RHS row
       double acc = 0.0;
+#pragma unroll 8
       for (int k = kb; k < ke; ++k) acc += double(src[k * LS]);
       if (j < neq * neq) {
         const int r = j / neq, c = j - r * neq;
