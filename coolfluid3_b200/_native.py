@@ -16,7 +16,7 @@ LIB_PATH = os.path.join(_HERE, "libufem_b200.so")
 UFEM_OK = 0
 ERRORS = {
     -1: "UFEM_ERR_ARG", -2: "UFEM_ERR_CUDA", -3: "UFEM_ERR_MESH", -4: "UFEM_ERR_STATE",
-    -5: "UFEM_ERR_NOMEM", -6: "UFEM_ERR_LIMIT", -7: "UFEM_ERR_SOLVE",
+    -5: "UFEM_ERR_NOMEM", -6: "UFEM_ERR_LIMIT", -7: "UFEM_ERR_SOLVE", -8: "UFEM_ERR_IO",
 }
 
 
@@ -100,6 +100,9 @@ SIGNATURES = {
     "ufem_ns_solve_noalloc": (C.c_int, [_P, C.POINTER(KrylovOpts), C.POINTER(KrylovStatus), _P]),
     "ufem_ns_update": (C.c_int, [_P, _P]),
     "ufem_ns_step": (C.c_int, [_P, C.c_int32, C.POINTER(KrylovOpts), C.POINTER(KrylovStatus), _P]),
+    "ufem_ns_write_restart": (C.c_int, [_P, C.c_char_p, C.c_double, C.c_double, C.c_int64]),
+    "ufem_ns_read_restart": (C.c_int, [_P, C.c_char_p, C.POINTER(C.c_double), C.POINTER(C.c_double),
+                                       C.POINTER(C.c_int64)]),
     "ufem_ns_get_system": (C.c_int, [_P, _D, _D]),
     "ufem_ns_download_system": (C.c_int, [_P, _D, _D, _P]),
     "ufem_ns_device_view_get": (C.c_int, [_P, C.POINTER(DeviceView)]),

@@ -129,6 +129,21 @@ class NavierStokes:
         nuv = np.broadcast_to(np.asarray(nu, np.float64), (self.nb_nodes,)).copy()
         self.set_state(up, lin, nuv, force)
 
+    def write_restart(self, path: str, current_time: float = 0.0, time_step: float | None = None,
+                      iteration: int = 0) -> None:
+        """WriteRestartFile (solver/actions/WriteRestartFile.cpp:62-90): the
+        device-resident state to `path` (XML) and `path`.bin (tables)."""
+        dt = self._opts.dt if time_step is None else time_step
+        N.check(self._lib.ufem_ns_write_restart(self._h, str(path).encode(), float(current_time), float(dt),
+                                                int(iteration)))
+
+    def read_restart(self, path: str) -> tuple[float, float, int]:
+        """ReadRestartFile (ReadRestartFile.cpp:67-110): restores the state;
+        returns (current_time, time_step, iteration)."""
+        t, dt, it = C.c_double(), C.c_double(), C.c_int64()
+        N.check(self._lib.ufem_ns_read_restart(self._h, str(path).encode(), C.byref(t), C.byref(dt), C.byref(it)))
+        return t.value, dt.value, it.value
+
     def state(self):
         up = np.empty((self.nb_nodes, self.neq))
         lin = np.empty((self.nb_nodes, 4 * self.dim))

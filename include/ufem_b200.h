@@ -40,6 +40,7 @@ extern "C" {
 #define UFEM_ERR_NOMEM (-5)   /* device allocation failed                         */
 #define UFEM_ERR_LIMIT (-6)   /* a node has more than 63 neighbours               */
 #define UFEM_ERR_SOLVE (-7)   /* Krylov solve failed (see ufem_krylov_status)     */
+#define UFEM_ERR_IO (-8)      /* restart file unreadable or malformed (cf3 FileFormatError) */
 
 /* Mesh: coords N x dim (row-major), conn E x (dim+1), host memory. */
 typedef struct ufem_mesh {
@@ -198,6 +199,25 @@ int ufem_ns_update(ufem_ns_handle* h, void* stream);
 /* nsteps full time steps; status of the last solve. */
 int ufem_ns_step(ufem_ns_handle* h, int32_t nsteps, const ufem_krylov_opts* kopts,
                  ufem_krylov_status* status, void* stream);
+
+/* Restart files of the device-resident state.
+ * ufem_ns_write_restart replaces WriteRestartFile::execute
+ * (solver/actions/WriteRestartFile.cpp:62-90): `path` receives the XML restart
+ * node (version 1, nb_procs 1, current_time, time_step, iteration, one <field>
+ * node per table) and `path`.bin the tables as raw FP64 rows with a checksum
+ * each -- navier_stokes_solution, linearized_velocity, navier_stokes_viscosity
+ * and body_force when set, in the layouts of ufem_ns_set_state, and the linear
+ * system's solution vector (the next solve's initial guess).
+ * ufem_ns_read_restart replaces ReadRestartFile::execute (ReadRestartFile.cpp:67-110):
+ * it checks version, process count, node count and dimension and every table's
+ * shape and checksum (UFEM_ERR_IO otherwise), restores the state and returns the
+ * time, time step and iteration (each output may be NULL).  Stepping a handle
+ * read from a restart gives bitwise the same states as stepping the handle that
+ * wrote it. */
+int ufem_ns_write_restart(ufem_ns_handle* h, const char* path, double current_time, double time_step,
+                          int64_t iteration);
+int ufem_ns_read_restart(ufem_ns_handle* h, const char* path, double* current_time, double* time_step,
+                         int64_t* iteration);
 
 /* Host copies of the assembled system (vals nnz, rhs nb_rows); either may be NULL. */
 int ufem_ns_get_system(ufem_ns_handle* h, double* vals, double* rhs);
