@@ -1667,6 +1667,25 @@ int launch_build_csr(ufem_ns_handle* h, cudaStream_t s) {
   return UFEM_OK;
 }
 
+// rhs[dof] += contributions of the constant Neumann faces, in face order.
+__global__ void neumann_kernel(int64_t n, const int64_t* __restrict__ dof, const int64_t* __restrict__ ptr,
+                               const double* __restrict__ val, double* __restrict__ rhs) {
+  const int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  double r = rhs[dof[i]];
+  for (int64_t k = ptr[i]; k < ptr[i + 1]; ++k) r = __dadd_rn(r, val[k]);
+  rhs[dof[i]] = r;
+}
+
+int launch_neumann(ufem_ns_handle* h, cudaStream_t s) {
+  const DirichletPlan& bp = h->bcp;
+  if (bp.nneu == 0) return UFEM_OK;
+  neumann_kernel<<<unsigned((bp.nneu + 255) / 256), 256, 0, s>>>(bp.nneu, bp.neu_dof, bp.neu_ptr, bp.neu_val,
+                                                                  h->d_rhs);
+  UFEM_CUDA_TRY(cudaGetLastError());
+  return UFEM_OK;
+}
+
 int launch_dirichlet(ufem_ns_handle* h, cudaStream_t s) {
   const DirichletPlan& bp = h->bcp;
   if (bp.nbc == 0) return UFEM_OK;

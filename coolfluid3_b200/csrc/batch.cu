@@ -1052,6 +1052,8 @@ int ufem_batch_assemble(ufem_batch* b, void* stream) {
     const AssemblyPlan& big = h->opt.precision == 1 ? h->wplan.big32 : h->wplan.big64;
     if (big.nchunks > 0 && (rc = launch_assembly_big_rows(h, st, h->d_vals32 != nullptr))) return rc;
   }
+  for (ufem_ns_handle* h : b->members)  // constant Neumann faces, before the Dirichlet passes
+    if (h->bcp.nneu > 0 && (rc = launch_neumann(h, st))) return rc;
   if (b->total_bc > 0) {
     dirichlet_values_batch_kernel<<<blocks_for(b->total_bc, 256), 256, 0, st>>>(b->total_bc, b->nmesh,
                                                                                  b->d_bc_prefix, b->d_mesh);

@@ -119,7 +119,8 @@ int check_device() {
 void free_bc_plan(DirichletPlan& b) {
   dfree(b.bc_dof); dfree(b.bc_first); dfree(b.bc_last); dfree(b.bc_diag);
   dfree(b.fix_row); dfree(b.fix_ptr); dfree(b.fix_pos); dfree(b.fix_bc); dfree(b.vfirst);
-  b.nbc = b.nfix_rows = b.nfix = 0;
+  dfree(b.neu_dof); dfree(b.neu_ptr); dfree(b.neu_val);
+  b.nbc = b.nfix_rows = b.nfix = b.nneu = 0;
 }
 
 // Slot of node `b` in the sorted neighbourhood of node `a`, or -1.
@@ -143,10 +144,59 @@ inline int64_t row_start(const ufem_ns_handle* h, int64_t node, int r) {
 //  - in every other row, each constrained column is moved to the RHS with the
 //    value of that dof's FIRST application (later applications find a zero),
 //    in first-application order, then zeroed.
+// Constant Neumann faces (BCNeumannConstant.cpp:54-60 on Line2D): each face
+// adds (weight * detJ) * ((N_i * flux) * |normal|) to the RHS dof of both of
+// its nodes -- one Gauss point (weight 2), detJ = |x1 - x0| / 2
+// (Line2D.cpp:109-114), N_i = 1/2, normal = (dy, -dx) / 2 (Line2D.cpp:83-87).
+// The contributions are static (fixed mesh and flux): they are evaluated here
+// once, in FP64, and kept per dof in face order so that the device adds them
+// in the reference's order.
+int build_neumann_plan(ufem_ns_handle* h) {
+  DirichletPlan& bp = h->bcp;
+  if (h->neumann.empty()) return UFEM_OK;
+  const int neq = h->neq;
+  std::vector<std::pair<int64_t, double>> c;  // (dof, contribution) in face order
+  c.reserve(h->neumann.size() * 2);
+  for (const auto& f : h->neumann) {
+    const double* xa = &h->coords_h[size_t(f.a) * 2];
+    const double* xb = &h->coords_h[size_t(f.b) * 2];
+    const double dxdxi = 0.5 * (xb[0] - xa[0]), dydxi = 0.5 * (xb[1] - xa[1]);
+    const double detj = std::sqrt(dxdxi * dxdxi + dydxi * dydxi);
+    const double nx = 0.5 * (xb[1] - xa[1]), ny = 0.5 * (-xb[0] + xa[0]);
+    const double nrm = std::sqrt(nx * nx + ny * ny);
+    const double w = 2.0 * detj;
+    const double v = w * ((0.5 * f.flux) * nrm);
+    c.push_back({int64_t(f.a) * neq + f.comp, v});
+    c.push_back({int64_t(f.b) * neq + f.comp, v});
+  }
+  std::stable_sort(c.begin(), c.end(), [](const auto& x, const auto& y) { return x.first < y.first; });
+  std::vector<int64_t> dof, ptr(1, 0);
+  std::vector<double> val;
+  for (size_t i = 0; i < c.size(); ++i) {
+    if (dof.empty() || dof.back() != c[i].first) {
+      if (!dof.empty()) ptr.push_back(int64_t(val.size()));
+      dof.push_back(c[i].first);
+    }
+    val.push_back(c[i].second);
+  }
+  ptr.push_back(int64_t(val.size()));
+  int rc;
+  if ((rc = dmalloc(&bp.neu_dof, dof.size(), "neumann dofs")) || (rc = dmalloc(&bp.neu_ptr, ptr.size(), "neumann")) ||
+      (rc = dmalloc(&bp.neu_val, val.size(), "neumann values")))
+    return rc;
+  UFEM_CUDA_TRY(cudaMemcpy(bp.neu_dof, dof.data(), dof.size() * 8, cudaMemcpyHostToDevice));
+  UFEM_CUDA_TRY(cudaMemcpy(bp.neu_ptr, ptr.data(), ptr.size() * 8, cudaMemcpyHostToDevice));
+  UFEM_CUDA_TRY(cudaMemcpy(bp.neu_val, val.data(), val.size() * 8, cudaMemcpyHostToDevice));
+  bp.nneu = int64_t(dof.size());
+  return UFEM_OK;
+}
+
 int build_bc_plan(ufem_ns_handle* h) {
   DirichletPlan& bp = h->bcp;
   free_bc_plan(bp);
   bp.dirty = false;
+  int rc;
+  if ((rc = build_neumann_plan(h))) return rc;
   if (h->bcs.empty()) return UFEM_OK;
   const int neq = h->neq;
   std::vector<int32_t> uid(size_t(h->nrows), -1);
@@ -200,7 +250,6 @@ int build_bc_plan(ufem_ns_handle* h) {
   bp.nbc = int64_t(dofs.size());
   bp.nfix_rows = int64_t(frow.size());
   bp.nfix = int64_t(fixes.size());
-  int rc;
   if ((rc = dmalloc(&bp.bc_dof, dofs.size(), "bc_dof")) || (rc = dmalloc(&bp.bc_first, dofs.size(), "bc_first")) ||
       (rc = dmalloc(&bp.bc_last, dofs.size(), "bc_last")) || (rc = dmalloc(&bp.bc_diag, dofs.size(), "bc_diag")) ||
       (rc = dmalloc(&bp.vfirst, dofs.size(), "vfirst")) || (rc = dmalloc(&bp.fix_row, frow.size(), "fix_row")) ||
@@ -539,6 +588,7 @@ int ufem_ns_create(const ufem_mesh* mesh, const ufem_ns_options* opts, ufem_ns_h
 
   // --- device allocations and uploads
   DeviceLock device_lock(device_mutex());
+  if (dim == 2) h->coords_h.assign(mesh->coords, mesh->coords + size_t(N) * 2);
   std::vector<double> c4(size_t(N) * 4, 0.0);
   for (int64_t i = 0; i < N; ++i)
     for (int k = 0; k < dim; ++k) c4[i * 4 + k] = mesh->coords[i * dim + k];
@@ -737,6 +787,27 @@ int ufem_ns_get_solution(ufem_ns_handle* h, double* sol) {
   return UFEM_OK;
 }
 
+int ufem_ns_add_neumann(ufem_ns_handle* h, const uint32_t* faces, int64_t nfaces, int32_t comp, double flux) {
+  if (!h) return set_error(UFEM_ERR_ARG, "NULL handle");
+  if (h->dim != 2)
+    return set_error(UFEM_ERR_ARG, "constant Neumann conditions are defined on Line2D faces (2D meshes)");
+  if (nfaces < 0 || (nfaces > 0 && !faces)) return set_error(UFEM_ERR_ARG, "invalid face array");
+  if (comp < 0 || comp >= h->neq) return set_error(UFEM_ERR_ARG, "component out of range");
+  if (!std::isfinite(flux)) return set_error(UFEM_ERR_ARG, "flux must be finite");
+  for (int64_t i = 0; i < 2 * nfaces; ++i)
+    if (int64_t(faces[i]) >= h->N) return set_error(UFEM_ERR_ARG, "Neumann face node id out of range");
+  for (int64_t i = 0; i < nfaces; ++i) h->neumann.push_back({faces[2 * i], faces[2 * i + 1], comp, flux});
+  h->bcp.dirty = true;
+  return UFEM_OK;
+}
+
+int ufem_ns_clear_neumann(ufem_ns_handle* h) {
+  if (!h) return set_error(UFEM_ERR_ARG, "NULL handle");
+  h->neumann.clear();
+  h->bcp.dirty = true;
+  return UFEM_OK;
+}
+
 int ufem_ns_clear_dirichlet(ufem_ns_handle* h) {
   if (!h) return set_error(UFEM_ERR_ARG, "NULL handle");
   h->bcs.clear();
@@ -875,6 +946,7 @@ int ufem_ns_apply_dirichlet(ufem_ns_handle* h, void* stream) {
     if ((rc = build_bc_plan(h))) return rc;
   }
   record(h, 2, false, s);
+  if ((rc = launch_neumann(h, s))) return rc;
   if ((rc = launch_dirichlet(h, s))) return rc;
   record(h, 2, true, s);
   return UFEM_OK;

@@ -97,6 +97,12 @@ struct DirichletPlan {
   int64_t* fix_pos = nullptr;  // nfix CSR positions, per row in first-application order
   int32_t* fix_bc = nullptr;   // nfix index into bc arrays
   double* vfirst = nullptr;    // per step: bc_first - old
+  // constant Neumann faces: per RHS dof (neu_dof), its face contributions in
+  // face order (neu_val[neu_ptr[i] .. neu_ptr[i+1]))
+  int64_t nneu = 0;
+  int64_t* neu_dof = nullptr;
+  int64_t* neu_ptr = nullptr;
+  double* neu_val = nullptr;
   bool dirty = true;
 };
 
@@ -114,8 +120,11 @@ struct ufem_ns_handle {
   // host copies used by planning
   std::vector<int64_t> start_h;   // N+1
   std::vector<int32_t> adj_h;     // bnnz
+  std::vector<double> coords_h;   // N x 2, 2D meshes only (constant Neumann faces)
   struct BCEntry { uint32_t node; int comp; double value; };
   std::vector<BCEntry> bcs;
+  struct NeumannFace { uint32_t a, b; int comp; double flux; };
+  std::vector<NeumannFace> neumann;  // constant Neumann conditions on Line2D faces
 
   // device mesh and fields (node records padded to 4 doubles)
   double* d_coords = nullptr;   // N x 4 (x, y, [z], 0)
@@ -177,6 +186,8 @@ void fill_desc(const ufem_ns_handle* h, bool write32, AsmDesc& d, const WarpPlan
 int launch_assembly_batch(int dim, int precision, bool spec, int warps, int ngroups, int nmesh,
                           const AsmDesc* d_descs, const int* d_gprefix, cudaStream_t s);
 int launch_dirichlet(ufem_ns_handle* h, cudaStream_t s);
+// Adds the constant Neumann contributions to the RHS (before the Dirichlet passes).
+int launch_neumann(ufem_ns_handle* h, cudaStream_t s);
 int launch_update(ufem_ns_handle* h, cudaStream_t s);
 int assembly_chunk_capacity(int dim, int precision);
 int configure_kernels();

@@ -172,6 +172,17 @@ class NavierStokes:
                                                       len(nodes)))
 
     # -- actions -------------------------------------------------------------
+    def add_neumann(self, faces: np.ndarray, comp: int, flux: float) -> None:
+        """BCNeumannConstant (BCNeumannConstant.cpp:54-60) on Line2D faces
+        (nfaces x 2 node ids) of a 2D mesh; added before the Dirichlet conditions."""
+        faces = np.ascontiguousarray(faces, np.uint32)
+        if faces.ndim != 2 or faces.shape[1] != 2:
+            raise ValueError("faces must be (nfaces, 2) node ids")
+        N.check(self._lib.ufem_ns_add_neumann(self._h, N.u32ptr(faces), len(faces), int(comp), float(flux)))
+
+    def clear_neumann(self) -> None:
+        N.check(self._lib.ufem_ns_clear_neumann(self._h))
+
     def assemble(self, stream=None) -> None:
         """ZeroLSS + LinearizeU + Assembly."""
         N.check(self._lib.ufem_ns_assemble(self._h, _stream(stream)))

@@ -167,6 +167,17 @@ int ufem_ns_add_dirichlet(ufem_ns_handle* h, const uint32_t* nodes, int64_t n, i
 int ufem_ns_add_dirichlet_dofs(ufem_ns_handle* h, const uint32_t* nodes, const int32_t* comps,
                                const double* values, int64_t n);
 
+/* Constant Neumann condition: BCNeumannConstant
+ * (plugins/UFEM/src/UFEM/BCNeumannConstant.cpp:54-60), defined there on Line2D
+ * faces only, so 2D meshes only here (UFEM_ERR_ARG otherwise).  faces: nfaces
+ * x 2 node ids; each face adds integral<1>(N^T flux |normal|) to the RHS rows of
+ * component `comp` of its two nodes, evaluated as the reference does
+ * (one Gauss point of weight 2 times the face's jacobian determinant |dx|/2,
+ * N = 1/2, |normal| = |dx|/2: flux |dx|^2 / 4 per node).  The contributions are
+ * added before the Dirichlet conditions, face by face in the order given. */
+int ufem_ns_add_neumann(ufem_ns_handle* h, const uint32_t* faces, int64_t nfaces, int32_t comp, double flux);
+int ufem_ns_clear_neumann(ufem_ns_handle* h);
+
 /* ZeroLSS + LinearizeU + Assembly (NavierStokesAssembly.hpp:27-75 or
  * NavierStokesSpecializations.hpp:26-303).  Asynchronous on `stream`. */
 int ufem_ns_assemble(ufem_ns_handle* h, void* stream);

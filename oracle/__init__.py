@@ -48,6 +48,8 @@ _SIG = {
     "orc_set_solution": (None, [C.c_void_p, _D]),
     "orc_get_solution": (None, [C.c_void_p, _D]),
     "orc_clear_dirichlet": (None, [C.c_void_p]),
+    "orc_clear_neumann": (None, [C.c_void_p]),
+    "orc_add_neumann": (None, [C.c_void_p, _U32, C.c_int64, C.c_int, C.c_double]),
     "orc_add_dirichlet": (None, [C.c_void_p, _U32, C.c_int64, C.c_int, _D]),
     "orc_add_dirichlet_dofs": (None, [C.c_void_p, _U32, _I32, _D, C.c_int64]),
     "orc_assemble": (None, [C.c_void_p, C.c_int]),
@@ -233,6 +235,14 @@ class Oracle:
 
     def clear_dirichlet(self):
         lib().orc_clear_dirichlet(self._h)
+
+    def add_neumann(self, faces, comp: int, flux: float):
+        """Constant Neumann condition on Line2D faces (nfaces x 2 node ids)."""
+        faces = np.ascontiguousarray(faces, np.uint32)
+        lib().orc_add_neumann(self._h, faces.ctypes.data_as(_U32), len(faces), int(comp), float(flux))
+
+    def clear_neumann(self):
+        lib().orc_clear_neumann(self._h)
 
     def assemble(self, nthreads: int = 1):
         lib().orc_assemble(self._h, nthreads)

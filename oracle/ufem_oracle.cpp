@@ -53,6 +53,13 @@ typedef struct orc_options {
 
 namespace {
 
+// One Line2D face of a constant Neumann condition (BCNeumannConstant).
+struct NeumannFace {
+  uint32_t a, b;
+  int comp;
+  double flux;
+};
+
 struct BC {
   uint32_t node;
   int comp;
@@ -78,6 +85,7 @@ struct Oracle {
   std::vector<double> nu;        // navier_stokes_viscosity N
   std::vector<double> force;     // body_force N x dim (empty = zero)
   std::vector<BC> bcs;
+  std::vector<NeumannFace> neumann;
   // node -> incident elements (for the node-partitioned multi-thread baseline)
   std::vector<int64_t> inc_start;
   std::vector<uint32_t> inc_elem;
@@ -793,7 +801,33 @@ void symmetric_dirichlet(Oracle& S, int64_t b, int c, double v) {
   S.sol[b * neq + c] = v;
 }
 
+// BCNeumannConstant (plugins/UFEM/src/UFEM/BCNeumannConstant.cpp:54-60):
+// rhs(var) += integral<1>(transpose(N(var)) * flux * _norm(normal)) over each
+// Line2D face.  integral<1> is one Gauss point (xi = 0, weight 2) with the
+// weight multiplied by the face's jacobian determinant
+// (Proto/ElementIntegration.hpp:200, Line2D.cpp:109-114: |x1 - x0| / 2);
+// N = (1/2, 1/2); normal is Line2D::normal (Line2D.cpp:83-87), the unnormalised
+// (dy, -dx) / 2.  Evaluated as the reference's expression tree:
+// (weight * detJ) * ((N_i * flux) * |normal|), added face by face.
+void apply_neumann(Oracle& S) {
+  for (const NeumannFace& f : S.neumann) {
+    const double* xa = &S.coords[(size_t)f.a * 2];
+    const double* xb = &S.coords[(size_t)f.b * 2];
+    const double dxdxi = 0.5 * (xb[0] - xa[0]), dydxi = 0.5 * (xb[1] - xa[1]);
+    const double detj = std::sqrt(dxdxi * dxdxi + dydxi * dydxi);
+    const double nx = 0.5 * (xb[1] - xa[1]), ny = 0.5 * (-xb[0] + xa[0]);
+    const double nrm = std::sqrt(nx * nx + ny * ny);
+    const double w = 2.0 * detj;
+    const double c = w * ((0.5 * f.flux) * nrm);
+    S.rhs[(size_t)f.a * S.neq + f.comp] += c;
+    S.rhs[(size_t)f.b * S.neq + f.comp] += c;
+  }
+}
+
+// BoundaryConditions in list order: the constant Neumann faces first, then the
+// Dirichlet conditions in the order they were added.
 void apply_bcs(Oracle& S) {
+  apply_neumann(S);
   for (const BC& bc : S.bcs) {
     const double old = S.up[(int64_t)bc.node * S.neq + bc.comp];
     symmetric_dirichlet(S, bc.node, bc.comp, bc.value - old);
@@ -1114,6 +1148,12 @@ void orc_get_solution(void* h, double* sol) {
 }
 
 void orc_clear_dirichlet(void* h) { static_cast<Oracle*>(h)->bcs.clear(); }
+void orc_clear_neumann(void* h) { static_cast<Oracle*>(h)->neumann.clear(); }
+// faces: nfaces x 2 node ids (Line2D)
+void orc_add_neumann(void* h, const uint32_t* faces, int64_t nfaces, int comp, double flux) {
+  Oracle* S = static_cast<Oracle*>(h);
+  for (int64_t i = 0; i < nfaces; ++i) S->neumann.push_back({faces[2 * i], faces[2 * i + 1], comp, flux});
+}
 
 void orc_add_dirichlet(void* h, const uint32_t* nodes, int64_t n, int comp, const double* values) {
   Oracle* S = static_cast<Oracle*>(h);
