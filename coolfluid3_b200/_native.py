@@ -94,6 +94,9 @@ SIGNATURES = {
     "ufem_ns_clear_dirichlet": (C.c_int, [_P]),
     "ufem_ns_add_dirichlet": (C.c_int, [_P, _U32, C.c_int64, C.c_int32, _D]),
     "ufem_ns_add_dirichlet_dofs": (C.c_int, [_P, _U32, _I32, _D, C.c_int64]),
+    "ufem_ns_add_dirichlet_function": (C.c_int, [_P, _U32, C.c_int64, C.c_int32, C.c_char_p]),
+    "ufem_ns_set_time": (C.c_int, [_P, C.c_double]),
+    "ufem_ns_get_time": (C.c_int, [_P, C.POINTER(C.c_double)]),
     "ufem_ns_add_neumann": (C.c_int, [_P, _U32, C.c_int64, C.c_int32, C.c_double]),
     "ufem_ns_clear_neumann": (C.c_int, [_P]),
     "ufem_ns_assemble": (C.c_int, [_P, _P]),

@@ -1052,8 +1052,10 @@ int ufem_batch_assemble(ufem_batch* b, void* stream) {
     const AssemblyPlan& big = h->opt.precision == 1 ? h->wplan.big32 : h->wplan.big64;
     if (big.nchunks > 0 && (rc = launch_assembly_big_rows(h, st, h->d_vals32 != nullptr))) return rc;
   }
-  for (ufem_ns_handle* h : b->members)  // constant Neumann faces, before the Dirichlet passes
+  for (ufem_ns_handle* h : b->members) {  // function values and constant Neumann faces, before the Dirichlet passes
+    if ((rc = launch_dirichlet_functions(h, st))) return rc;
     if (h->bcp.nneu > 0 && (rc = launch_neumann(h, st))) return rc;
+  }
   if (b->total_bc > 0) {
     dirichlet_values_batch_kernel<<<blocks_for(b->total_bc, 256), 256, 0, st>>>(b->total_bc, b->nmesh,
                                                                                  b->d_bc_prefix, b->d_mesh);
@@ -1185,6 +1187,7 @@ int ufem_batch_update(ufem_batch* b, void* stream) {
   update_batch_kernel<<<blocks_for(b->total_nodes, 256), 256, 0, st>>>(b->total_nodes, b->nmesh, b->d_node_prefix,
                                                                        b->d_mesh);
   UFEM_CUDA_TRY(cudaGetLastError());
+  for (ufem_ns_handle* h : b->members) h->time += h->opt.dt;  // as ufem_ns_update
   return UFEM_OK;
 }
 

@@ -120,6 +120,7 @@ void free_bc_plan(DirichletPlan& b) {
   dfree(b.bc_dof); dfree(b.bc_first); dfree(b.bc_last); dfree(b.bc_diag);
   dfree(b.fix_row); dfree(b.fix_ptr); dfree(b.fix_pos); dfree(b.fix_bc); dfree(b.vfirst);
   dfree(b.neu_dof); dfree(b.neu_ptr); dfree(b.neu_val);
+  dfree(b.fn_first); dfree(b.fn_last); dfree(b.fn_code); dfree(b.fn_off); dfree(b.fn_const);
   b.nbc = b.nfix_rows = b.nfix = b.nneu = 0;
 }
 
@@ -202,6 +203,7 @@ int build_bc_plan(ufem_ns_handle* h) {
   std::vector<int32_t> uid(size_t(h->nrows), -1);
   std::vector<int64_t> dofs;
   std::vector<double> first, last;
+  std::vector<int32_t> ffirst, flast;  // expression of the first / last application, -1: constant
   for (const auto& e : h->bcs) {
     const int64_t dof = int64_t(e.node) * neq + e.comp;
     int32_t& u = uid[dof];
@@ -210,8 +212,11 @@ int build_bc_plan(ufem_ns_handle* h) {
       dofs.push_back(dof);
       first.push_back(e.value);
       last.push_back(e.value);
+      ffirst.push_back(e.fn);
+      flast.push_back(e.fn);
     } else {
       last[u] = e.value;
+      flast[u] = e.fn;
     }
   }
   struct Fix {
@@ -260,6 +265,26 @@ int build_bc_plan(ufem_ns_handle* h) {
   UFEM_CUDA_TRY(cudaMemcpy(bp.bc_first, first.data(), first.size() * 8, cudaMemcpyHostToDevice));
   UFEM_CUDA_TRY(cudaMemcpy(bp.bc_last, last.data(), last.size() * 8, cudaMemcpyHostToDevice));
   UFEM_CUDA_TRY(cudaMemcpy(bp.bc_diag, diag.data(), diag.size() * 8, cudaMemcpyHostToDevice));
+  if (!h->fn_code.empty()) {  // function values: per-dof expression ids and the concatenated byte code
+    std::vector<int32_t> code, off(1, 0);
+    std::vector<double> k;
+    for (size_t e = 0; e < h->fn_code.size(); ++e) {
+      const int32_t base = int32_t(k.size());
+      for (int32_t w : h->fn_code[e])  // constant operands are rebased onto the concatenated table
+        code.push_back((w & 255) == kExprPushConst ? (kExprPushConst | (((w >> 8) + base) << 8)) : w);
+      k.insert(k.end(), h->fn_const[e].begin(), h->fn_const[e].end());
+      off.push_back(int32_t(code.size()));
+    }
+    if ((rc = dmalloc(&bp.fn_first, dofs.size(), "fn_first")) || (rc = dmalloc(&bp.fn_last, dofs.size(), "fn_last")) ||
+        (rc = dmalloc(&bp.fn_code, code.size(), "fn_code")) || (rc = dmalloc(&bp.fn_off, off.size(), "fn_off")) ||
+        (rc = dmalloc(&bp.fn_const, std::max<size_t>(k.size(), 1), "fn_const")))
+      return rc;
+    UFEM_CUDA_TRY(cudaMemcpy(bp.fn_first, ffirst.data(), ffirst.size() * 4, cudaMemcpyHostToDevice));
+    UFEM_CUDA_TRY(cudaMemcpy(bp.fn_last, flast.data(), flast.size() * 4, cudaMemcpyHostToDevice));
+    UFEM_CUDA_TRY(cudaMemcpy(bp.fn_code, code.data(), code.size() * 4, cudaMemcpyHostToDevice));
+    UFEM_CUDA_TRY(cudaMemcpy(bp.fn_off, off.data(), off.size() * 4, cudaMemcpyHostToDevice));
+    if (!k.empty()) UFEM_CUDA_TRY(cudaMemcpy(bp.fn_const, k.data(), k.size() * 8, cudaMemcpyHostToDevice));
+  }
   if (!frow.empty()) {
     UFEM_CUDA_TRY(cudaMemcpy(bp.fix_row, frow.data(), frow.size() * 8, cudaMemcpyHostToDevice));
     UFEM_CUDA_TRY(cudaMemcpy(bp.fix_ptr, fptr.data(), fptr.size() * 8, cudaMemcpyHostToDevice));
@@ -808,9 +833,44 @@ int ufem_ns_clear_neumann(ufem_ns_handle* h) {
   return UFEM_OK;
 }
 
+int ufem_ns_add_dirichlet_function(ufem_ns_handle* h, const uint32_t* nodes, int64_t n, int32_t comp,
+                                    const char* expr) {
+  if (!h) return set_error(UFEM_ERR_ARG, "NULL handle");
+  if (!expr) return set_error(UFEM_ERR_ARG, "NULL expression");
+  if (n < 0 || (n > 0 && !nodes)) return set_error(UFEM_ERR_ARG, "invalid node array");
+  if (comp < 0 || comp >= h->neq) return set_error(UFEM_ERR_ARG, "component out of range");
+  for (int64_t i = 0; i < n; ++i)
+    if (int64_t(nodes[i]) >= h->N) return set_error(UFEM_ERR_ARG, "Dirichlet node id out of range");
+  std::vector<int32_t> code;
+  std::vector<double> k;
+  std::string err;
+  if (compile_expression(expr, code, k, err) != UFEM_OK) return set_error(UFEM_ERR_ARG, "Dirichlet function: " + err);
+  const int32_t id = int32_t(h->fn_code.size());
+  h->fn_code.push_back(std::move(code));
+  h->fn_const.push_back(std::move(k));
+  for (int64_t i = 0; i < n; ++i) h->bcs.push_back({nodes[i], comp, 0.0, id});
+  h->bcp.dirty = true;
+  return UFEM_OK;
+}
+
+int ufem_ns_set_time(ufem_ns_handle* h, double t) {
+  if (!h) return set_error(UFEM_ERR_ARG, "NULL handle");
+  if (!std::isfinite(t)) return set_error(UFEM_ERR_ARG, "time must be finite");
+  h->time = t;
+  return UFEM_OK;
+}
+
+int ufem_ns_get_time(const ufem_ns_handle* h, double* t) {
+  if (!h || !t) return set_error(UFEM_ERR_ARG, "NULL argument");
+  *t = h->time;
+  return UFEM_OK;
+}
+
 int ufem_ns_clear_dirichlet(ufem_ns_handle* h) {
   if (!h) return set_error(UFEM_ERR_ARG, "NULL handle");
   h->bcs.clear();
+  h->fn_code.clear();
+  h->fn_const.clear();
   h->bcp.dirty = true;
   return UFEM_OK;
 }
@@ -946,6 +1006,7 @@ int ufem_ns_apply_dirichlet(ufem_ns_handle* h, void* stream) {
     if ((rc = build_bc_plan(h))) return rc;
   }
   record(h, 2, false, s);
+  if ((rc = launch_dirichlet_functions(h, s))) return rc;
   if ((rc = launch_neumann(h, s))) return rc;
   if ((rc = launch_dirichlet(h, s))) return rc;
   record(h, 2, true, s);
@@ -978,6 +1039,7 @@ int ufem_ns_update(ufem_ns_handle* h, void* stream) {
   record(h, 4, false, s);
   int rc = launch_update(h, s);
   record(h, 4, true, s);
+  if (rc == UFEM_OK) h->time += h->opt.dt;  // AdvanceTime after the step (function BCs read the time)
   return rc;
 }
 

@@ -99,6 +99,13 @@ struct DirichletPlan {
   double* vfirst = nullptr;    // per step: bc_first - old
   // constant Neumann faces: per RHS dof (neu_dof), its face contributions in
   // face order (neu_val[neu_ptr[i] .. neu_ptr[i+1]))
+  // function values (BCDirichletFunction): expression of the first / last
+  // application of each dof (-1: constant), byte code of all expressions
+  int32_t* fn_first = nullptr;
+  int32_t* fn_last = nullptr;
+  int32_t* fn_code = nullptr;
+  int32_t* fn_off = nullptr;   // expression e: fn_code[fn_off[e] .. fn_off[e+1])
+  double* fn_const = nullptr;
   int64_t nneu = 0;
   int64_t* neu_dof = nullptr;
   int64_t* neu_ptr = nullptr;
@@ -121,7 +128,10 @@ struct ufem_ns_handle {
   std::vector<int64_t> start_h;   // N+1
   std::vector<int32_t> adj_h;     // bnnz
   std::vector<double> coords_h;   // N x 2, 2D meshes only (constant Neumann faces)
-  struct BCEntry { uint32_t node; int comp; double value; };
+  struct BCEntry { uint32_t node; int comp; double value; int32_t fn = -1; };  // fn: expression id or -1
+  std::vector<std::vector<int32_t>> fn_code;   // compiled Dirichlet function expressions
+  std::vector<std::vector<double>> fn_const;
+  double time = 0.0;                            // current time (function BCs); advanced by dt at each update
   std::vector<BCEntry> bcs;
   struct NeumannFace { uint32_t a, b; int comp; double flux; };
   std::vector<NeumannFace> neumann;  // constant Neumann conditions on Line2D faces
@@ -188,6 +198,14 @@ int launch_assembly_batch(int dim, int precision, bool spec, int warps, int ngro
 int launch_dirichlet(ufem_ns_handle* h, cudaStream_t s);
 // Adds the constant Neumann contributions to the RHS (before the Dirichlet passes).
 int launch_neumann(ufem_ns_handle* h, cudaStream_t s);
+
+// bcfunction.cu: Dirichlet values from expressions of (x, y, z, t)
+constexpr int kExprMaxDepth = 32;
+constexpr int32_t kExprPushConst = 0;  // byte-code word: op | operand << 8
+int compile_expression(const std::string& src, std::vector<int32_t>& code, std::vector<double>& consts,
+                       std::string& err);
+// Evaluates the function values of the first / last applications at h->time.
+int launch_dirichlet_functions(ufem_ns_handle* h, cudaStream_t s);
 int launch_update(ufem_ns_handle* h, cudaStream_t s);
 int assembly_chunk_capacity(int dim, int precision);
 int configure_kernels();

@@ -214,7 +214,8 @@ int ufem_ns_read_restart(ufem_ns_handle* h, const char* path, double* current_ti
     UFEM_CUDA_TRY(cudaMemset(h->d_sol, 0, size_t(h->nrows) * 8));
   else
     UFEM_CUDA_TRY(cudaMemcpy(h->d_sol, sol.data(), size_t(h->nrows) * 8, cudaMemcpyHostToDevice));
-  if (current_time) *current_time = std::strtod(attr(restart, "current_time").c_str(), nullptr);
+  h->time = std::strtod(attr(restart, "current_time").c_str(), nullptr);  // Time::current_time
+  if (current_time) *current_time = h->time;
   if (time_step) *time_step = std::strtod(attr(restart, "time_step").c_str(), nullptr);
   if (iteration) *iteration = std::strtoll(attr(restart, "iteration").c_str(), nullptr, 10);
   return UFEM_OK;

@@ -129,11 +129,13 @@ class NavierStokes:
         nuv = np.broadcast_to(np.asarray(nu, np.float64), (self.nb_nodes,)).copy()
         self.set_state(up, lin, nuv, force)
 
-    def write_restart(self, path: str, current_time: float = 0.0, time_step: float | None = None,
+    def write_restart(self, path: str, current_time: float | None = None, time_step: float | None = None,
                       iteration: int = 0) -> None:
         """WriteRestartFile (solver/actions/WriteRestartFile.cpp:62-90): the
-        device-resident state to `path` (XML) and `path`.bin (tables)."""
+        device-resident state to `path` (XML) and `path`.bin (tables); the time
+        defaults to the handle's."""
         dt = self._opts.dt if time_step is None else time_step
+        current_time = self.time if current_time is None else current_time
         N.check(self._lib.ufem_ns_write_restart(self._h, str(path).encode(), float(current_time), float(dt),
                                                 int(iteration)))
 
@@ -172,6 +174,23 @@ class NavierStokes:
                                                       len(nodes)))
 
     # -- actions -------------------------------------------------------------
+    def add_dirichlet_function(self, nodes: np.ndarray, comp: int, expr: str) -> None:
+        """BCDirichletFunction (BCDirichletFunction.cpp:61-92): component `comp`
+        of `nodes` ends at f(x, y, z, t), `expr` evaluated on the device."""
+        nodes = np.ascontiguousarray(nodes, np.uint32)
+        N.check(self._lib.ufem_ns_add_dirichlet_function(self._h, N.u32ptr(nodes), len(nodes), int(comp),
+                                                         str(expr).encode()))
+
+    @property
+    def time(self) -> float:
+        t = C.c_double()
+        N.check(self._lib.ufem_ns_get_time(self._h, C.byref(t)))
+        return t.value
+
+    @time.setter
+    def time(self, t: float) -> None:
+        N.check(self._lib.ufem_ns_set_time(self._h, float(t)))
+
     def add_neumann(self, faces: np.ndarray, comp: int, flux: float) -> None:
         """BCNeumannConstant (BCNeumannConstant.cpp:54-60) on Line2D faces
         (nfaces x 2 node ids) of a 2D mesh; added before the Dirichlet conditions."""

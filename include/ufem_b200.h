@@ -167,6 +167,23 @@ int ufem_ns_add_dirichlet(ufem_ns_handle* h, const uint32_t* nodes, int64_t n, i
 int ufem_ns_add_dirichlet_dofs(ufem_ns_handle* h, const uint32_t* nodes, const int32_t* comps,
                                const double* values, int64_t n);
 
+/* Dirichlet values from a function of the node coordinates and time:
+ * BCDirichletFunction (plugins/UFEM/src/UFEM/BCDirichletFunction.cpp:61-92 with
+ * solving_for_difference, i.e. dirichlet(var) = f: the component ends at f).
+ * `expr` is a formula in x, y, z (node coordinates; z = 0 in 2D) and t (the
+ * handle's time): numbers, + - * / ^ (right-associative, above unary minus),
+ * parentheses, pi and sin cos tan asin acos atan sinh cosh tanh exp log sqrt
+ * abs.  It is compiled here (UFEM_ERR_ARG with the position of a syntax error)
+ * and evaluated on the device, in FP64 with CUDA's math functions, at every
+ * ufem_ns_apply_dirichlet; the entries join the ordered Dirichlet list exactly
+ * as constant ones (first application moves the columns, last sets the row). */
+int ufem_ns_add_dirichlet_function(ufem_ns_handle* h, const uint32_t* nodes, int64_t n, int32_t comp,
+                                   const char* expr);
+/* The time that function conditions see (Time::current_time).  It starts at 0
+ * and advances by dt at every ufem_ns_update (the reference's AdvanceTime). */
+int ufem_ns_set_time(ufem_ns_handle* h, double t);
+int ufem_ns_get_time(const ufem_ns_handle* h, double* t);
+
 /* Constant Neumann condition: BCNeumannConstant
  * (plugins/UFEM/src/UFEM/BCNeumannConstant.cpp:54-60), defined there on Line2D
  * faces only, so 2D meshes only here (UFEM_ERR_ARG otherwise).  faces: nfaces
@@ -221,7 +238,8 @@ int ufem_ns_step(ufem_ns_handle* h, int32_t nsteps, const ufem_krylov_opts* kopt
  * system's solution vector (the next solve's initial guess).
  * ufem_ns_read_restart replaces ReadRestartFile::execute (ReadRestartFile.cpp:67-110):
  * it checks version, process count, node count and dimension and every table's
- * shape and checksum (UFEM_ERR_IO otherwise), restores the state and returns the
+ * shape and checksum (UFEM_ERR_IO otherwise), restores the state, sets the
+ * handle's time (ufem_ns_set_time) to the file's current_time and returns the
  * time, time step and iteration (each output may be NULL).  Stepping a handle
  * read from a restart gives bitwise the same states as stepping the handle that
  * wrote it. */
