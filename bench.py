@@ -69,6 +69,7 @@ def parse():
     ap.add_argument("--serve-steps", type=int, default=10, help="time steps per served request")
     ap.add_argument("--serve-budget-gb", type=float, default=60.0, help="HBM budget of the server (GB)")
     ap.add_argument("--serve-reps", type=int, default=3, help="served runs per form (the median is reported)")
+    ap.add_argument("--serving-only", action="store_true", help=argparse.SUPPRESS)
     return ap.parse_args()
 
 
@@ -407,7 +408,7 @@ def run_ours(args, rank, world, local):
     ns.close()
     if rank == 0 and world == 1 and not args.no_extras and args.serve_requests > 0:
         # ---- served steps/s with p50/p99 vs the plain per-request path ----------
-        line["serving"] = serving_compare(args)
+        line["serving"] = serving_in_child()
     if rank == 0:
         print(json.dumps(line), flush=True)
 
@@ -418,7 +419,12 @@ def time_steps(ns, pb, args, stream, sptr):
     out = {}
     base_up = pb.up
     results = {}
-    for label, kw in (("plain_fp64", dict(mixed=False)), ("mixed", dict(mixed=True, inner_tol=1e-4))):
+    # the two forms solve to the reference's 1e-10; a third run to 1e-12 is the FP64
+    # answer each form's error is stated against (pressure and velocity apart: the
+    # pinned-pressure system determines the pressure far less well than the velocity)
+    forms = (("plain_fp64", dict(mixed=False, tol=1e-10)), ("mixed", dict(mixed=True, inner_tol=1e-4, tol=1e-10)),
+             ("fp64_1e-12", dict(mixed=False, tol=1e-12)))
+    for label, kw in forms:
         ns.set_state(pb.up, pb.lin, pb.nu)
         ns.set_solution(np.zeros(ns.nb_rows))
         lat = []
@@ -430,7 +436,7 @@ def time_steps(ns, pb, args, stream, sptr):
                 t0 = time.perf_counter()
                 ns.assemble(sptr)
                 ns.apply_dirichlet(sptr)
-                st = ns.solve(sptr, raise_on_failure=False, tol=1e-10, max_iters=3000, **kw)
+                st = ns.solve(sptr, raise_on_failure=False, max_iters=6000, **kw)
                 ns.update(sptr)
                 torch.cuda.synchronize()
                 lat.append((time.perf_counter() - t0) * 1e3)
@@ -445,12 +451,30 @@ def time_steps(ns, pb, args, stream, sptr):
         out[label] = {"steps_per_s": round(1e3 / float(np.mean(lat)), 3), "p50_ms": round(float(np.median(lat)), 2),
                       "max_ms": round(float(np.max(lat)), 2), "krylov_iters": iters,
                       "converged": int(st["converged"]), "status": int(st.get("status", -1))}
-    if "plain_fp64" in results and "mixed" in results:
-        ref = results["plain_fp64"]
-        out["mixed"]["rel_err_vs_plain"] = float(np.linalg.norm(results["mixed"] - ref) / np.linalg.norm(ref))
+    if "fp64_1e-12" in results:
+        ref = results["fp64_1e-12"]
+        for label in ("plain_fp64", "mixed"):
+            if label in results:
+                d = results[label] - ref
+                out[label]["rel_err_vs_fp64_1e-12"] = {
+                    "state": float(np.linalg.norm(d) / np.linalg.norm(ref)),
+                    "velocity": float(np.linalg.norm(d[:, :-1]) / np.linalg.norm(ref[:, :-1])),
+                    "pressure": float(np.linalg.norm(d[:, -1]) / np.linalg.norm(ref[:, -1]))}
     out["steps"] = args.time_steps
     ns.set_state(base_up, pb.lin, pb.nu)
     return out
+
+
+def serving_in_child() -> dict:
+    """serving_compare in a fresh process (same arguments): the served makespan
+    depends on how host threads and CUDA streams interleave, so it is measured
+    apart from the kernel benchmark's process state."""
+    cmd = [sys.executable, os.path.abspath(__file__)] + sys.argv[1:] + ["--serving-only"]
+    proc = subprocess.run(cmd, stdout=subprocess.PIPE, stderr=sys.stderr, text=True)
+    lines = [ln for ln in proc.stdout.strip().splitlines() if ln.startswith("{")]
+    if proc.returncode != 0 or not lines:
+        return {"error": f"serving run exited with {proc.returncode}"}
+    return json.loads(lines[-1])
 
 
 def serving_compare(args):
@@ -509,6 +533,9 @@ def serving_compare(args):
 
 def main():
     args = parse()
+    if args.serving_only:
+        print(json.dumps(serving_compare(args)), flush=True)
+        return
     rank, world, local = dist_init(args.gpus)
     try:
         if args.impl == "reference":
