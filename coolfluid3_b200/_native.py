@@ -81,6 +81,8 @@ SIGNATURES = {
     "ufem_ns_default_options": (None, [C.POINTER(NSOptions)]),
     "ufem_krylov_default_opts": (None, [C.POINTER(KrylovOpts)]),
     "ufem_ns_create": (C.c_int, [C.POINTER(Mesh), C.POINTER(NSOptions), C.POINTER(_P)]),
+    "ufem_ns_create_periodic": (C.c_int, [C.POINTER(Mesh), C.POINTER(NSOptions), _U32, _U32, C.c_int64,
+                                          C.POINTER(_P)]),
     "ufem_ns_set_options": (C.c_int, [_P, C.POINTER(NSOptions)]),
     "ufem_ns_sizes": (C.c_int, [_P, _I64, _I64, _I64]),
     "ufem_ns_csr": (C.c_int, [_P, _I64, _I32]),

@@ -1667,6 +1667,42 @@ int launch_build_csr(ufem_ns_handle* h, cudaStream_t s) {
   return UFEM_OK;
 }
 
+// Tie rows of linked (periodic) nodes, after the assembly: the element
+// contributions at a slave node were assembled into its master's rows and
+// columns; the slave's own rows become x_slave - x_master = 0 (identity block
+// at the slave, minus identity at the master, rhs 0), so the solution and the
+// update give the slave its master's values.
+__global__ void tie_rows_kernel(int64_t ntie, int neq, const int32_t* __restrict__ tie,
+                                const int64_t* __restrict__ start, const int32_t* __restrict__ adj,
+                                double* __restrict__ vals, float* __restrict__ vals32, double* __restrict__ rhs) {
+  const int64_t t = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (t >= ntie) return;
+  const int sl = tie[2 * t], ms = tie[2 * t + 1];
+  const int64_t s0 = start[sl];
+  const int S = int(start[sl + 1] - s0);
+  for (int r = 0; r < neq; ++r) {
+    const int64_t rs = int64_t(neq) * neq * s0 + int64_t(r) * S * neq;
+    for (int k = 0; k < S; ++k) {
+      const int col = adj[s0 + k];
+      for (int c = 0; c < neq; ++c) {
+        const double v = (c != r) ? 0.0 : (col == sl ? 1.0 : (col == ms ? -1.0 : 0.0));
+        vals[rs + k * neq + c] = v;
+        if (vals32 != nullptr) vals32[rs + k * neq + c] = float(v);
+      }
+    }
+    rhs[int64_t(sl) * neq + r] = 0.0;
+  }
+}
+
+int launch_tie_rows(ufem_ns_handle* h, cudaStream_t s, bool write32) {
+  if (h->ntie == 0) return UFEM_OK;
+  tie_rows_kernel<<<unsigned((h->ntie + 127) / 128), 128, 0, s>>>(h->ntie, h->neq, h->d_tie, h->d_start, h->d_adj,
+                                                                  h->d_vals, write32 ? h->d_vals32 : nullptr,
+                                                                  h->d_rhs);
+  UFEM_CUDA_TRY(cudaGetLastError());
+  return UFEM_OK;
+}
+
 // rhs[dof] += contributions of the constant Neumann faces, in face order.
 __global__ void neumann_kernel(int64_t n, const int64_t* __restrict__ dof, const int64_t* __restrict__ ptr,
                                const double* __restrict__ val, double* __restrict__ rhs) {

@@ -1051,6 +1051,7 @@ int ufem_batch_assemble(ufem_batch* b, void* stream) {
     h->vals32_valid = h->d_vals32 != nullptr;
     const AssemblyPlan& big = h->opt.precision == 1 ? h->wplan.big32 : h->wplan.big64;
     if (big.nchunks > 0 && (rc = launch_assembly_big_rows(h, st, h->d_vals32 != nullptr))) return rc;
+    if ((rc = launch_tie_rows(h, st, h->d_vals32 != nullptr))) return rc;
   }
   for (ufem_ns_handle* h : b->members) {  // function values and constant Neumann faces, before the Dirichlet passes
     if ((rc = launch_dirichlet_functions(h, st))) return rc;

@@ -167,8 +167,9 @@ int build_neumann_plan(ufem_ns_handle* h) {
     const double nrm = std::sqrt(nx * nx + ny * ny);
     const double w = 2.0 * detj;
     const double v = w * ((0.5 * f.flux) * nrm);
-    c.push_back({int64_t(f.a) * neq + f.comp, v});
-    c.push_back({int64_t(f.b) * neq + f.comp, v});
+    const int64_t ra = h->p2m_h.empty() ? f.a : h->p2m_h[f.a], rb = h->p2m_h.empty() ? f.b : h->p2m_h[f.b];
+    c.push_back({ra * neq + f.comp, v});
+    c.push_back({rb * neq + f.comp, v});
   }
   std::stable_sort(c.begin(), c.end(), [](const auto& x, const auto& y) { return x.first < y.first; });
   std::vector<int64_t> dof, ptr(1, 0);
@@ -204,8 +205,8 @@ int build_bc_plan(ufem_ns_handle* h) {
   std::vector<int64_t> dofs;
   std::vector<double> first, last;
   std::vector<int32_t> ffirst, flast;  // expression of the first / last application, -1: constant
-  for (const auto& e : h->bcs) {
-    const int64_t dof = int64_t(e.node) * neq + e.comp;
+  for (const auto& e : h->bcs) {  // a linked node's condition acts on its master's row
+    const int64_t dof = int64_t(h->p2m_h.empty() ? e.node : h->p2m_h[e.node]) * neq + e.comp;
     int32_t& u = uid[dof];
     if (u < 0) {
       u = int32_t(dofs.size());
@@ -310,7 +311,7 @@ void destroy_impl(ufem_ns_handle* h) {
   dfree(h->d_nu); dfree(h->d_force); dfree(h->d_node32); dfree(h->d_start); dfree(h->d_adj); dfree(h->d_rowptr);
   dfree(h->d_colidx); dfree(h->d_vals); dfree(h->d_vals32); dfree(h->d_rhs); dfree(h->d_sol);
   dfree(h->d_diagpos); dfree(h->d_row_inc); dfree(h->d_inc_elem); dfree(h->d_inc_info);
-  dfree(h->plan64.chunks); dfree(h->plan32.chunks);
+  dfree(h->plan64.chunks); dfree(h->plan32.chunks); dfree(h->d_tie);
   for (WarpPlan* wp : {&h->wplan, &h->wplan24}) {
     dfree(wp->groups);
     dfree(wp->big64.chunks);
@@ -325,6 +326,335 @@ void destroy_impl(ufem_ns_handle* h) {
 }  // namespace ufem
 
 using namespace ufem;
+
+namespace ufem {
+namespace {
+
+// Periodic links -> node-to-row map (the reference's periodic_links_nodes /
+// periodic_links_active, LSSAction.cpp:245-269): a linked (slave) node's row
+// is its master's; chains resolve to the final master.  Empty map: no links.
+int periodic_map(int64_t N, const uint32_t* slaves, const uint32_t* masters, int64_t nlinks,
+                 std::vector<uint32_t>& p2m) {
+  p2m.clear();
+  if (nlinks == 0) return UFEM_OK;
+  if (nlinks < 0 || !slaves || !masters) return set_error(UFEM_ERR_ARG, "invalid periodic link arrays");
+  std::vector<int64_t> link(size_t(N), -1);
+  for (int64_t i = 0; i < nlinks; ++i) {
+    if (int64_t(slaves[i]) >= N || int64_t(masters[i]) >= N)
+      return set_error(UFEM_ERR_ARG, "periodic link node id out of range");
+    if (slaves[i] == masters[i]) return set_error(UFEM_ERR_ARG, "a node cannot be linked to itself");
+    if (link[slaves[i]] >= 0)
+      return set_error(UFEM_ERR_ARG, "node " + std::to_string(slaves[i]) + " is linked twice");
+    link[slaves[i]] = masters[i];
+  }
+  p2m.resize(size_t(N));
+  for (int64_t i = 0; i < N; ++i) {
+    int64_t cur = i, steps = 0;
+    while (link[cur] >= 0) {
+      cur = link[cur];
+      if (++steps > nlinks) return set_error(UFEM_ERR_ARG, "periodic links form a cycle");
+    }
+    p2m[i] = uint32_t(cur);
+  }
+  return UFEM_OK;
+}
+
+}  // namespace
+}  // namespace ufem
+
+namespace {
+int create_impl(const ufem_mesh* mesh, const ufem_ns_options* opts, const uint32_t* slaves,
+                const uint32_t* masters, int64_t nlinks, ufem_ns_handle** out) {
+  if (!out) return set_error(UFEM_ERR_ARG, "out handle pointer is NULL");
+  *out = nullptr;
+  if (!mesh || !mesh->coords || !mesh->conn) return set_error(UFEM_ERR_ARG, "mesh or its arrays are NULL");
+  if (mesh->dim != 2 && mesh->dim != 3) return set_error(UFEM_ERR_ARG, "dim must be 2 (Triag2D) or 3 (Tetra3D)");
+  if (mesh->nb_nodes <= 0 || mesh->nb_elems <= 0) return set_error(UFEM_ERR_ARG, "empty mesh");
+  int rc;
+  if ((rc = validate_options(opts))) return rc;
+  const int dim = mesh->dim, nn = dim + 1, neq = dim + 1;
+  const int64_t N = mesh->nb_nodes, E = mesh->nb_elems;
+  if (E * nn >= (int64_t(1) << 31) || N >= (int64_t(1) << 31) / neq)
+    return set_error(UFEM_ERR_LIMIT, "mesh too large for 32-bit incidence/column indices");
+  // --- validate connectivity and element Jacobians (non-invertible J is
+  //     rejected, as cf3_assert(is_invertible) does in ElementData.hpp:311-313)
+  {
+    std::atomic<int64_t> bad_elem{-1}, bad_node{-1};
+    parallel_for(E, [&](int64_t a, int64_t b) {
+      for (int64_t e = a; e < b; ++e) {
+        const uint32_t* c = mesh->conn + e * nn;
+        bool ok = true;
+        for (int k = 0; k < nn; ++k)
+          if (int64_t(c[k]) >= N) ok = false;
+        if (!ok) {
+          bad_node = e;
+          continue;
+        }
+        double J[3][3] = {{0}};
+        for (int r = 0; r < dim; ++r)
+          for (int q = 0; q < dim; ++q) J[r][q] = mesh->coords[int64_t(c[r + 1]) * dim + q] - mesh->coords[int64_t(c[0]) * dim + q];
+        const double det = dim == 2 ? J[0][0] * J[1][1] - J[1][0] * J[0][1]
+                                    : J[0][0] * (J[1][1] * J[2][2] - J[1][2] * J[2][1]) -
+                                          J[0][1] * (J[1][0] * J[2][2] - J[1][2] * J[2][0]) +
+                                          J[0][2] * (J[1][0] * J[2][1] - J[1][1] * J[2][0]);
+        if (!(det != 0.0) || !std::isfinite(det)) bad_elem = e;
+      }
+    });
+    if (bad_node >= 0)
+      return set_error(UFEM_ERR_MESH, "element " + std::to_string(int64_t(bad_node)) + " references a node id >= nb_nodes");
+    if (bad_elem >= 0)
+      return set_error(UFEM_ERR_MESH, "element " + std::to_string(int64_t(bad_elem)) + " has a non-invertible Jacobian");
+    // every node must belong to an element: its LSS row would otherwise be empty
+    // (the reference keeps such nodes out of the system via used_node_map)
+    std::vector<uint8_t> used(size_t(N), 0);
+    for (int64_t k = 0; k < E * nn; ++k) used[mesh->conn[k]] = 1;
+    for (int64_t i = 0; i < N; ++i)
+      if (!used[i]) return set_error(UFEM_ERR_MESH, "node " + std::to_string(i) + " is not referenced by any element");
+  }
+  std::vector<uint32_t> p2m;  // row of each node (periodic links); empty: the identity
+  if ((rc = periodic_map(N, slaves, masters, nlinks, p2m))) return rc;
+  auto row_of = [&](uint32_t node) { return p2m.empty() ? node : p2m[node]; };
+  if (!p2m.empty())
+    for (int64_t e = 0; e < E; ++e)
+      for (int a = 0; a < nn; ++a)
+        for (int b = a + 1; b < nn; ++b)
+          if (row_of(mesh->conn[e * nn + a]) == row_of(mesh->conn[e * nn + b]))
+            return set_error(UFEM_ERR_MESH, "element " + std::to_string(e) +
+                                                " holds a node and its periodic partner (the mesh is too thin)");
+  if ((rc = check_device())) return rc;
+  if ((rc = configure_kernels())) return rc;
+
+  ufem_ns_handle* h = new ufem_ns_handle();
+  h->dim = dim;
+  h->nn = nn;
+  h->neq = neq;
+  h->N = N;
+  h->E = E;
+  h->opt = *opts;
+  h->p2m_h = p2m;
+  auto fail = [&](int code) {
+    destroy_impl(h);
+    return code;
+  };
+
+  // --- node -> incident elements, ascending element id (counting sort)
+  std::vector<int32_t> row_inc(N + 1, 0);
+  for (int64_t e = 0; e < E; ++e)
+    for (int a = 0; a < nn; ++a) row_inc[row_of(mesh->conn[e * nn + a]) + 1]++;
+  for (int64_t i = 0; i < N; ++i) row_inc[i + 1] += row_inc[i];
+  std::vector<int32_t> inc_elem(size_t(E) * nn);
+  std::vector<uint8_t> inc_local(size_t(E) * nn);
+  {
+    std::vector<int32_t> fill(row_inc.begin(), row_inc.end() - 1);
+    for (int64_t e = 0; e < E; ++e)
+      for (int a = 0; a < nn; ++a) {
+        const int32_t p = fill[row_of(mesh->conn[e * nn + a])]++;
+        inc_elem[p] = int32_t(e);
+        inc_local[p] = uint8_t(a);
+      }
+  }
+  // --- node graph: sorted unique neighbours incl. self (SparsityBuilder.cpp:157-189)
+  h->start_h.assign(N + 1, 0);
+  {
+    std::vector<int64_t> cnt(N, 0);
+    parallel_for(N, [&](int64_t a, int64_t b) {
+      std::vector<int32_t> tmp;
+      for (int64_t i = a; i < b; ++i) {
+        tmp.clear();
+        for (int32_t p = row_inc[i]; p < row_inc[i + 1]; ++p) {
+          const uint32_t* c = mesh->conn + int64_t(inc_elem[p]) * nn;
+          for (int k = 0; k < nn; ++k) tmp.push_back(int32_t(row_of(c[k])));
+        }
+        if (!p2m.empty() && p2m[i] != uint32_t(i)) {  // linked node: tie row over itself and its master
+          tmp.push_back(int32_t(i));
+          tmp.push_back(int32_t(p2m[i]));
+        }
+        std::sort(tmp.begin(), tmp.end());
+        cnt[i] = std::unique(tmp.begin(), tmp.end()) - tmp.begin();
+      }
+    });
+    for (int64_t i = 0; i < N; ++i) {
+      if (cnt[i] > 63)
+        return fail(set_error(UFEM_ERR_LIMIT, "node " + std::to_string(i) + " has " + std::to_string(cnt[i]) +
+                                                  " graph neighbours; the row-owner plan encodes at most 63"));
+      h->start_h[i + 1] = h->start_h[i] + cnt[i];
+    }
+    h->adj_h.resize(h->start_h[N]);
+    parallel_for(N, [&](int64_t a, int64_t b) {
+      std::vector<int32_t> tmp;
+      for (int64_t i = a; i < b; ++i) {
+        tmp.clear();
+        for (int32_t p = row_inc[i]; p < row_inc[i + 1]; ++p) {
+          const uint32_t* c = mesh->conn + int64_t(inc_elem[p]) * nn;
+          for (int k = 0; k < nn; ++k) tmp.push_back(int32_t(row_of(c[k])));
+        }
+        if (!p2m.empty() && p2m[i] != uint32_t(i)) {  // linked node: tie row over itself and its master
+          tmp.push_back(int32_t(i));
+          tmp.push_back(int32_t(p2m[i]));
+        }
+        std::sort(tmp.begin(), tmp.end());
+        tmp.erase(std::unique(tmp.begin(), tmp.end()), tmp.end());
+        std::copy(tmp.begin(), tmp.end(), h->adj_h.begin() + h->start_h[i]);
+      }
+    });
+  }
+  h->bnnz = h->start_h[N];
+  h->nrows = N * neq;
+  h->nnz = h->bnnz * neq * neq;
+  if (N < 1 || h->nnz >= (int64_t(1) << 40)) return fail(set_error(UFEM_ERR_LIMIT, "system too large"));
+  // --- incidence info: 6-bit slot of each element node in the row's neighbourhood, local index << 24
+  std::vector<uint32_t> inc_info(size_t(E) * nn);
+  parallel_for(N, [&](int64_t a, int64_t b) {
+    for (int64_t i = a; i < b; ++i)
+      for (int32_t p = row_inc[i]; p < row_inc[i + 1]; ++p) {
+        const uint32_t* c = mesh->conn + int64_t(inc_elem[p]) * nn;
+        uint32_t info = uint32_t(inc_local[p]) << 24;
+        for (int k = 0; k < nn; ++k) info |= uint32_t(slot_of(h, i, row_of(c[k]))) << (6 * k);
+        if (nn == 3) info |= 63u << 18;  // no 4th node
+        inc_info[p] = info;
+      }
+  });
+  // --- chunks of whole rows with at most `cap` incidences (and slots), one plan
+  // per kernel width; `only_big` restricts a plan to the rows the warp kernel
+  // leaves out (more than 32 incidences).
+  auto inc_of = [&](int64_t i) { return int64_t(row_inc[i + 1] - row_inc[i]); };
+  auto slots_of = [&](int64_t i) { return h->start_h[i + 1] - h->start_h[i]; };
+  auto make_chunks = [&](int cap, int big_above, std::vector<int2>& chunks) -> bool {
+    const bool only_big = big_above > 0;
+    int64_t i = 0;
+    while (i < N) {
+      // rows without incidences (tie rows of linked nodes) are written by the tie kernel
+      if ((only_big && inc_of(i) <= big_above) || inc_of(i) == 0) { ++i; continue; }
+      const int64_t first = i;
+      int64_t k = 0, sl = 0;  // incidences and neighbourhood slots of the chunk, each <= cap
+      while (i < N && (!only_big || inc_of(i) > big_above) && inc_of(i) > 0 && k + inc_of(i) <= cap &&
+             sl + slots_of(i) <= cap) {
+        k += inc_of(i);
+        sl += slots_of(i);
+        ++i;
+      }
+      if (i == first) return false;
+      chunks.push_back(make_int2(int(first), int(i)));
+    }
+    return true;
+  };
+  std::vector<int2> chunks64, chunks32;
+  if (!make_chunks(assembly_chunk_capacity(dim, 0), 0, chunks64) ||
+      !make_chunks(assembly_chunk_capacity(dim, 1), 0, chunks32))
+    return fail(set_error(UFEM_ERR_LIMIT, "a node has more incident elements than one assembly chunk holds"));
+  h->plan64.cap = assembly_chunk_capacity(dim, 0);
+  h->plan64.nchunks = int(chunks64.size());
+  h->plan32.cap = assembly_chunk_capacity(dim, 1);
+  h->plan32.nchunks = int(chunks32.size());
+  // --- warp groups: consecutive rows with at most `cap` incidences in total;
+  // rows with more go to a chunk plan that lists only them
+  struct WarpPlanHost {
+    std::vector<int4> groups;
+    std::vector<int2> big64, big32;
+  };
+  auto make_warp_plan = [&](int cap, WarpPlan& wp, WarpPlanHost& hp) -> bool {
+    for (int64_t i = 0; i < N;) {
+      if (inc_of(i) > cap || inc_of(i) == 0) { ++i; continue; }
+      const int64_t first = i;
+      int64_t k = 0;
+      while (i < N && inc_of(i) <= cap && inc_of(i) > 0 && k + inc_of(i) <= cap) k += inc_of(i++);
+      hp.groups.push_back(make_int4(int(first), int(i), row_inc[first], int(k)));
+    }
+    if (!make_chunks(assembly_chunk_capacity(dim, 0), cap, hp.big64) ||
+        !make_chunks(assembly_chunk_capacity(dim, 1), cap, hp.big32))
+      return false;
+    wp.cap = cap;
+    wp.ngroups = int(hp.groups.size());
+    wp.big64.cap = h->plan64.cap;
+    wp.big64.nchunks = int(hp.big64.size());
+    wp.big32.cap = h->plan32.cap;
+    wp.big32.nchunks = int(hp.big32.size());
+    return true;
+  };
+  WarpPlanHost wh32, wh24;
+  if (!make_warp_plan(32, h->wplan, wh32) || (dim == 3 && !make_warp_plan(24, h->wplan24, wh24)))
+    return fail(set_error(UFEM_ERR_LIMIT, "a node has more incident elements than one assembly chunk holds"));
+
+  // --- device allocations and uploads
+  DeviceLock device_lock(device_mutex());
+  if (dim == 2) h->coords_h.assign(mesh->coords, mesh->coords + size_t(N) * 2);
+  std::vector<double> c4(size_t(N) * 4, 0.0);
+  for (int64_t i = 0; i < N; ++i)
+    for (int k = 0; k < dim; ++k) c4[i * 4 + k] = mesh->coords[i * dim + k];
+  std::vector<int32_t> conn4(size_t(E) * 4);
+  for (int64_t e = 0; e < E; ++e)
+    for (int k = 0; k < 4; ++k) conn4[e * 4 + k] = int32_t(mesh->conn[e * nn + (k < nn ? k : 0)]);
+  if ((rc = dmalloc(&h->d_coords, c4.size(), "coords")) || (rc = dmalloc(&h->d_conn, conn4.size(), "conn")) ||
+      (rc = dmalloc(&h->d_state, size_t(N) * 4, "state")) || (rc = dmalloc(&h->d_hist, size_t(N) * 12, "history")) ||
+      (rc = dmalloc(&h->d_uadv, size_t(N) * 4, "u_adv")) || (rc = dmalloc(&h->d_nu, size_t(N), "nu")) ||
+      (rc = dmalloc(&h->d_start, size_t(N) + 1, "start")) || (rc = dmalloc(&h->d_adj, size_t(h->bnnz), "adj")) ||
+      (rc = dmalloc(&h->d_rowptr, size_t(h->nrows) + 1, "rowptr")) ||
+      (rc = dmalloc(&h->d_colidx, size_t(h->nnz), "colidx")) || (rc = dmalloc(&h->d_vals, size_t(h->nnz), "vals")) ||
+      (rc = dmalloc(&h->d_rhs, size_t(h->nrows), "rhs")) || (rc = dmalloc(&h->d_sol, size_t(h->nrows), "sol")) ||
+      (rc = dmalloc(&h->d_diagpos, size_t(h->nrows), "diagpos")) ||
+      (rc = dmalloc(&h->d_row_inc, size_t(N) + 1, "row_inc")) ||
+      (rc = dmalloc(&h->d_inc_elem, inc_elem.size(), "inc_elem")) ||
+      (rc = dmalloc(&h->d_inc_info, inc_info.size(), "inc_info")) ||
+      (rc = dmalloc(&h->plan64.chunks, chunks64.size(), "chunks64")) ||
+      (rc = dmalloc(&h->plan32.chunks, chunks32.size(), "chunks32")) ||
+      (rc = dmalloc(&h->d_stage, size_t(N) * 4 * dim, "stage")))
+    return fail(rc);
+  if (opts->precision == 1 && ((rc = dmalloc(&h->d_vals32, size_t(h->nnz), "vals32")) ||
+                               (rc = dmalloc(&h->d_node32, size_t(h->N) * 8, "node32"))))
+    return fail(rc);
+  auto up = [&](void* dst, const void* src, size_t bytes) {
+    return cudaMemcpy(dst, src, bytes, cudaMemcpyHostToDevice);
+  };
+  cudaError_t ce = cudaSuccess;
+  if ((ce = up(h->d_coords, c4.data(), c4.size() * 8)) || (ce = up(h->d_conn, conn4.data(), conn4.size() * 4)) ||
+      (ce = up(h->d_start, h->start_h.data(), h->start_h.size() * 8)) ||
+      (ce = up(h->d_adj, h->adj_h.data(), h->adj_h.size() * 4)) ||
+      (ce = up(h->d_row_inc, row_inc.data(), row_inc.size() * 4)) ||
+      (ce = up(h->d_inc_elem, inc_elem.data(), inc_elem.size() * 4)) ||
+      (ce = up(h->d_inc_info, inc_info.data(), inc_info.size() * 4)) ||
+      (ce = up(h->plan64.chunks, chunks64.data(), chunks64.size() * sizeof(int2))) ||
+      (ce = up(h->plan32.chunks, chunks32.data(), chunks32.size() * sizeof(int2))))
+    return fail(set_error(UFEM_ERR_CUDA, std::string("upload: ") + cudaGetErrorString(ce)));
+  auto upload_warp_plan = [&](WarpPlan& wp, const WarpPlanHost& hp) -> int {
+    int r;
+    if ((r = dmalloc(&wp.groups, std::max<size_t>(hp.groups.size(), 1), "groups")) ||
+        (r = dmalloc(&wp.big64.chunks, std::max<size_t>(hp.big64.size(), 1), "big rows")) ||
+        (r = dmalloc(&wp.big32.chunks, std::max<size_t>(hp.big32.size(), 1), "big rows")))
+      return r;
+    cudaError_t e;
+    if ((e = up(wp.groups, hp.groups.data(), hp.groups.size() * sizeof(int4))) ||
+        (e = up(wp.big64.chunks, hp.big64.data(), hp.big64.size() * sizeof(int2))) ||
+        (e = up(wp.big32.chunks, hp.big32.data(), hp.big32.size() * sizeof(int2))))
+      return set_error(UFEM_ERR_CUDA, std::string("upload: ") + cudaGetErrorString(e));
+    return UFEM_OK;
+  };
+  if ((rc = upload_warp_plan(h->wplan, wh32)) || (dim == 3 && (rc = upload_warp_plan(h->wplan24, wh24))))
+    return fail(rc);
+  if (!p2m.empty()) {  // tie rows of the linked nodes
+    std::vector<int32_t> tie;
+    for (int64_t i = 0; i < N; ++i)
+      if (p2m[i] != uint32_t(i)) {
+        tie.push_back(int32_t(i));
+        tie.push_back(int32_t(p2m[i]));
+      }
+    h->ntie = int64_t(tie.size() / 2);
+    if ((rc = dmalloc(&h->d_tie, std::max<size_t>(tie.size(), 1), "tie rows"))) return fail(rc);
+    if ((ce = up(h->d_tie, tie.data(), tie.size() * 4)))
+      return fail(set_error(UFEM_ERR_CUDA, std::string("upload: ") + cudaGetErrorString(ce)));
+  }
+  if ((ce = cudaMemset(h->d_sol, 0, size_t(h->nrows) * 8)) || (ce = cudaMemset(h->d_state, 0, size_t(N) * 32)) ||
+      (ce = cudaMemset(h->d_hist, 0, size_t(N) * 96)) || (ce = cudaMemset(h->d_uadv, 0, size_t(N) * 32)) ||
+      (ce = cudaMemset(h->d_nu, 0, size_t(N) * 8)) || (ce = cudaMemset(h->d_rhs, 0, size_t(h->nrows) * 8)))
+    return fail(set_error(UFEM_ERR_CUDA, std::string("memset: ") + cudaGetErrorString(ce)));
+  if ((rc = launch_build_csr(h, 0))) return fail(rc);
+  if ((ce = cudaDeviceSynchronize()) != cudaSuccess)
+    return fail(set_error(UFEM_ERR_CUDA, std::string("CSR build: ") + cudaGetErrorString(ce)));
+  for (auto& e : h->ev)
+    if (cudaEventCreate(&e) != cudaSuccess) return fail(set_error(UFEM_ERR_CUDA, "cudaEventCreate failed"));
+  *out = h;
+  return UFEM_OK;
+}
+}  // namespace
 
 extern "C" {
 
@@ -422,261 +752,14 @@ int ufem_mesh_cube_tets(int32_t n, double jitter, uint64_t seed, double* coords,
 }
 
 int ufem_ns_create(const ufem_mesh* mesh, const ufem_ns_options* opts, ufem_ns_handle** out) {
-  if (!out) return set_error(UFEM_ERR_ARG, "out handle pointer is NULL");
-  *out = nullptr;
-  if (!mesh || !mesh->coords || !mesh->conn) return set_error(UFEM_ERR_ARG, "mesh or its arrays are NULL");
-  if (mesh->dim != 2 && mesh->dim != 3) return set_error(UFEM_ERR_ARG, "dim must be 2 (Triag2D) or 3 (Tetra3D)");
-  if (mesh->nb_nodes <= 0 || mesh->nb_elems <= 0) return set_error(UFEM_ERR_ARG, "empty mesh");
-  int rc;
-  if ((rc = validate_options(opts))) return rc;
-  const int dim = mesh->dim, nn = dim + 1, neq = dim + 1;
-  const int64_t N = mesh->nb_nodes, E = mesh->nb_elems;
-  if (E * nn >= (int64_t(1) << 31) || N >= (int64_t(1) << 31) / neq)
-    return set_error(UFEM_ERR_LIMIT, "mesh too large for 32-bit incidence/column indices");
-  // --- validate connectivity and element Jacobians (non-invertible J is
-  //     rejected, as cf3_assert(is_invertible) does in ElementData.hpp:311-313)
-  {
-    std::atomic<int64_t> bad_elem{-1}, bad_node{-1};
-    parallel_for(E, [&](int64_t a, int64_t b) {
-      for (int64_t e = a; e < b; ++e) {
-        const uint32_t* c = mesh->conn + e * nn;
-        bool ok = true;
-        for (int k = 0; k < nn; ++k)
-          if (int64_t(c[k]) >= N) ok = false;
-        if (!ok) {
-          bad_node = e;
-          continue;
-        }
-        double J[3][3] = {{0}};
-        for (int r = 0; r < dim; ++r)
-          for (int q = 0; q < dim; ++q) J[r][q] = mesh->coords[int64_t(c[r + 1]) * dim + q] - mesh->coords[int64_t(c[0]) * dim + q];
-        const double det = dim == 2 ? J[0][0] * J[1][1] - J[1][0] * J[0][1]
-                                    : J[0][0] * (J[1][1] * J[2][2] - J[1][2] * J[2][1]) -
-                                          J[0][1] * (J[1][0] * J[2][2] - J[1][2] * J[2][0]) +
-                                          J[0][2] * (J[1][0] * J[2][1] - J[1][1] * J[2][0]);
-        if (!(det != 0.0) || !std::isfinite(det)) bad_elem = e;
-      }
-    });
-    if (bad_node >= 0)
-      return set_error(UFEM_ERR_MESH, "element " + std::to_string(int64_t(bad_node)) + " references a node id >= nb_nodes");
-    if (bad_elem >= 0)
-      return set_error(UFEM_ERR_MESH, "element " + std::to_string(int64_t(bad_elem)) + " has a non-invertible Jacobian");
-    // every node must belong to an element: its LSS row would otherwise be empty
-    // (the reference keeps such nodes out of the system via used_node_map)
-    std::vector<uint8_t> used(size_t(N), 0);
-    for (int64_t k = 0; k < E * nn; ++k) used[mesh->conn[k]] = 1;
-    for (int64_t i = 0; i < N; ++i)
-      if (!used[i]) return set_error(UFEM_ERR_MESH, "node " + std::to_string(i) + " is not referenced by any element");
-  }
-  if ((rc = check_device())) return rc;
-  if ((rc = configure_kernels())) return rc;
+  return create_impl(mesh, opts, nullptr, nullptr, 0, out);
+}
 
-  ufem_ns_handle* h = new ufem_ns_handle();
-  h->dim = dim;
-  h->nn = nn;
-  h->neq = neq;
-  h->N = N;
-  h->E = E;
-  h->opt = *opts;
-  auto fail = [&](int code) {
-    destroy_impl(h);
-    return code;
-  };
-
-  // --- node -> incident elements, ascending element id (counting sort)
-  std::vector<int32_t> row_inc(N + 1, 0);
-  for (int64_t e = 0; e < E; ++e)
-    for (int a = 0; a < nn; ++a) row_inc[mesh->conn[e * nn + a] + 1]++;
-  for (int64_t i = 0; i < N; ++i) row_inc[i + 1] += row_inc[i];
-  std::vector<int32_t> inc_elem(size_t(E) * nn);
-  std::vector<uint8_t> inc_local(size_t(E) * nn);
-  {
-    std::vector<int32_t> fill(row_inc.begin(), row_inc.end() - 1);
-    for (int64_t e = 0; e < E; ++e)
-      for (int a = 0; a < nn; ++a) {
-        const int32_t p = fill[mesh->conn[e * nn + a]]++;
-        inc_elem[p] = int32_t(e);
-        inc_local[p] = uint8_t(a);
-      }
-  }
-  // --- node graph: sorted unique neighbours incl. self (SparsityBuilder.cpp:157-189)
-  h->start_h.assign(N + 1, 0);
-  {
-    std::vector<int64_t> cnt(N, 0);
-    parallel_for(N, [&](int64_t a, int64_t b) {
-      std::vector<int32_t> tmp;
-      for (int64_t i = a; i < b; ++i) {
-        tmp.clear();
-        for (int32_t p = row_inc[i]; p < row_inc[i + 1]; ++p) {
-          const uint32_t* c = mesh->conn + int64_t(inc_elem[p]) * nn;
-          for (int k = 0; k < nn; ++k) tmp.push_back(int32_t(c[k]));
-        }
-        std::sort(tmp.begin(), tmp.end());
-        cnt[i] = std::unique(tmp.begin(), tmp.end()) - tmp.begin();
-      }
-    });
-    for (int64_t i = 0; i < N; ++i) {
-      if (cnt[i] > 63)
-        return fail(set_error(UFEM_ERR_LIMIT, "node " + std::to_string(i) + " has " + std::to_string(cnt[i]) +
-                                                  " graph neighbours; the row-owner plan encodes at most 63"));
-      h->start_h[i + 1] = h->start_h[i] + cnt[i];
-    }
-    h->adj_h.resize(h->start_h[N]);
-    parallel_for(N, [&](int64_t a, int64_t b) {
-      std::vector<int32_t> tmp;
-      for (int64_t i = a; i < b; ++i) {
-        tmp.clear();
-        for (int32_t p = row_inc[i]; p < row_inc[i + 1]; ++p) {
-          const uint32_t* c = mesh->conn + int64_t(inc_elem[p]) * nn;
-          for (int k = 0; k < nn; ++k) tmp.push_back(int32_t(c[k]));
-        }
-        std::sort(tmp.begin(), tmp.end());
-        tmp.erase(std::unique(tmp.begin(), tmp.end()), tmp.end());
-        std::copy(tmp.begin(), tmp.end(), h->adj_h.begin() + h->start_h[i]);
-      }
-    });
-  }
-  h->bnnz = h->start_h[N];
-  h->nrows = N * neq;
-  h->nnz = h->bnnz * neq * neq;
-  if (N < 1 || h->nnz >= (int64_t(1) << 40)) return fail(set_error(UFEM_ERR_LIMIT, "system too large"));
-  // --- incidence info: 6-bit slot of each element node in the row's neighbourhood, local index << 24
-  std::vector<uint32_t> inc_info(size_t(E) * nn);
-  parallel_for(N, [&](int64_t a, int64_t b) {
-    for (int64_t i = a; i < b; ++i)
-      for (int32_t p = row_inc[i]; p < row_inc[i + 1]; ++p) {
-        const uint32_t* c = mesh->conn + int64_t(inc_elem[p]) * nn;
-        uint32_t info = uint32_t(inc_local[p]) << 24;
-        for (int k = 0; k < nn; ++k) info |= uint32_t(slot_of(h, i, c[k])) << (6 * k);
-        if (nn == 3) info |= 63u << 18;  // no 4th node
-        inc_info[p] = info;
-      }
-  });
-  // --- chunks of whole rows with at most `cap` incidences (and slots), one plan
-  // per kernel width; `only_big` restricts a plan to the rows the warp kernel
-  // leaves out (more than 32 incidences).
-  auto inc_of = [&](int64_t i) { return int64_t(row_inc[i + 1] - row_inc[i]); };
-  auto slots_of = [&](int64_t i) { return h->start_h[i + 1] - h->start_h[i]; };
-  auto make_chunks = [&](int cap, int big_above, std::vector<int2>& chunks) -> bool {
-    const bool only_big = big_above > 0;
-    int64_t i = 0;
-    while (i < N) {
-      if (only_big && inc_of(i) <= big_above) { ++i; continue; }
-      const int64_t first = i;
-      int64_t k = 0, sl = 0;  // incidences and neighbourhood slots of the chunk, each <= cap
-      while (i < N && (!only_big || inc_of(i) > big_above) && k + inc_of(i) <= cap && sl + slots_of(i) <= cap) {
-        k += inc_of(i);
-        sl += slots_of(i);
-        ++i;
-      }
-      if (i == first) return false;
-      chunks.push_back(make_int2(int(first), int(i)));
-    }
-    return true;
-  };
-  std::vector<int2> chunks64, chunks32;
-  if (!make_chunks(assembly_chunk_capacity(dim, 0), 0, chunks64) ||
-      !make_chunks(assembly_chunk_capacity(dim, 1), 0, chunks32))
-    return fail(set_error(UFEM_ERR_LIMIT, "a node has more incident elements than one assembly chunk holds"));
-  h->plan64.cap = assembly_chunk_capacity(dim, 0);
-  h->plan64.nchunks = int(chunks64.size());
-  h->plan32.cap = assembly_chunk_capacity(dim, 1);
-  h->plan32.nchunks = int(chunks32.size());
-  // --- warp groups: consecutive rows with at most `cap` incidences in total;
-  // rows with more go to a chunk plan that lists only them
-  struct WarpPlanHost {
-    std::vector<int4> groups;
-    std::vector<int2> big64, big32;
-  };
-  auto make_warp_plan = [&](int cap, WarpPlan& wp, WarpPlanHost& hp) -> bool {
-    for (int64_t i = 0; i < N;) {
-      if (inc_of(i) > cap) { ++i; continue; }
-      const int64_t first = i;
-      int64_t k = 0;
-      while (i < N && inc_of(i) <= cap && k + inc_of(i) <= cap) k += inc_of(i++);
-      hp.groups.push_back(make_int4(int(first), int(i), row_inc[first], int(k)));
-    }
-    if (!make_chunks(assembly_chunk_capacity(dim, 0), cap, hp.big64) ||
-        !make_chunks(assembly_chunk_capacity(dim, 1), cap, hp.big32))
-      return false;
-    wp.cap = cap;
-    wp.ngroups = int(hp.groups.size());
-    wp.big64.cap = h->plan64.cap;
-    wp.big64.nchunks = int(hp.big64.size());
-    wp.big32.cap = h->plan32.cap;
-    wp.big32.nchunks = int(hp.big32.size());
-    return true;
-  };
-  WarpPlanHost wh32, wh24;
-  if (!make_warp_plan(32, h->wplan, wh32) || (dim == 3 && !make_warp_plan(24, h->wplan24, wh24)))
-    return fail(set_error(UFEM_ERR_LIMIT, "a node has more incident elements than one assembly chunk holds"));
-
-  // --- device allocations and uploads
-  DeviceLock device_lock(device_mutex());
-  if (dim == 2) h->coords_h.assign(mesh->coords, mesh->coords + size_t(N) * 2);
-  std::vector<double> c4(size_t(N) * 4, 0.0);
-  for (int64_t i = 0; i < N; ++i)
-    for (int k = 0; k < dim; ++k) c4[i * 4 + k] = mesh->coords[i * dim + k];
-  std::vector<int32_t> conn4(size_t(E) * 4);
-  for (int64_t e = 0; e < E; ++e)
-    for (int k = 0; k < 4; ++k) conn4[e * 4 + k] = int32_t(mesh->conn[e * nn + (k < nn ? k : 0)]);
-  if ((rc = dmalloc(&h->d_coords, c4.size(), "coords")) || (rc = dmalloc(&h->d_conn, conn4.size(), "conn")) ||
-      (rc = dmalloc(&h->d_state, size_t(N) * 4, "state")) || (rc = dmalloc(&h->d_hist, size_t(N) * 12, "history")) ||
-      (rc = dmalloc(&h->d_uadv, size_t(N) * 4, "u_adv")) || (rc = dmalloc(&h->d_nu, size_t(N), "nu")) ||
-      (rc = dmalloc(&h->d_start, size_t(N) + 1, "start")) || (rc = dmalloc(&h->d_adj, size_t(h->bnnz), "adj")) ||
-      (rc = dmalloc(&h->d_rowptr, size_t(h->nrows) + 1, "rowptr")) ||
-      (rc = dmalloc(&h->d_colidx, size_t(h->nnz), "colidx")) || (rc = dmalloc(&h->d_vals, size_t(h->nnz), "vals")) ||
-      (rc = dmalloc(&h->d_rhs, size_t(h->nrows), "rhs")) || (rc = dmalloc(&h->d_sol, size_t(h->nrows), "sol")) ||
-      (rc = dmalloc(&h->d_diagpos, size_t(h->nrows), "diagpos")) ||
-      (rc = dmalloc(&h->d_row_inc, size_t(N) + 1, "row_inc")) ||
-      (rc = dmalloc(&h->d_inc_elem, inc_elem.size(), "inc_elem")) ||
-      (rc = dmalloc(&h->d_inc_info, inc_info.size(), "inc_info")) ||
-      (rc = dmalloc(&h->plan64.chunks, chunks64.size(), "chunks64")) ||
-      (rc = dmalloc(&h->plan32.chunks, chunks32.size(), "chunks32")) ||
-      (rc = dmalloc(&h->d_stage, size_t(N) * 4 * dim, "stage")))
-    return fail(rc);
-  if (opts->precision == 1 && ((rc = dmalloc(&h->d_vals32, size_t(h->nnz), "vals32")) ||
-                               (rc = dmalloc(&h->d_node32, size_t(h->N) * 8, "node32"))))
-    return fail(rc);
-  auto up = [&](void* dst, const void* src, size_t bytes) {
-    return cudaMemcpy(dst, src, bytes, cudaMemcpyHostToDevice);
-  };
-  cudaError_t ce = cudaSuccess;
-  if ((ce = up(h->d_coords, c4.data(), c4.size() * 8)) || (ce = up(h->d_conn, conn4.data(), conn4.size() * 4)) ||
-      (ce = up(h->d_start, h->start_h.data(), h->start_h.size() * 8)) ||
-      (ce = up(h->d_adj, h->adj_h.data(), h->adj_h.size() * 4)) ||
-      (ce = up(h->d_row_inc, row_inc.data(), row_inc.size() * 4)) ||
-      (ce = up(h->d_inc_elem, inc_elem.data(), inc_elem.size() * 4)) ||
-      (ce = up(h->d_inc_info, inc_info.data(), inc_info.size() * 4)) ||
-      (ce = up(h->plan64.chunks, chunks64.data(), chunks64.size() * sizeof(int2))) ||
-      (ce = up(h->plan32.chunks, chunks32.data(), chunks32.size() * sizeof(int2))))
-    return fail(set_error(UFEM_ERR_CUDA, std::string("upload: ") + cudaGetErrorString(ce)));
-  auto upload_warp_plan = [&](WarpPlan& wp, const WarpPlanHost& hp) -> int {
-    int r;
-    if ((r = dmalloc(&wp.groups, std::max<size_t>(hp.groups.size(), 1), "groups")) ||
-        (r = dmalloc(&wp.big64.chunks, std::max<size_t>(hp.big64.size(), 1), "big rows")) ||
-        (r = dmalloc(&wp.big32.chunks, std::max<size_t>(hp.big32.size(), 1), "big rows")))
-      return r;
-    cudaError_t e;
-    if ((e = up(wp.groups, hp.groups.data(), hp.groups.size() * sizeof(int4))) ||
-        (e = up(wp.big64.chunks, hp.big64.data(), hp.big64.size() * sizeof(int2))) ||
-        (e = up(wp.big32.chunks, hp.big32.data(), hp.big32.size() * sizeof(int2))))
-      return set_error(UFEM_ERR_CUDA, std::string("upload: ") + cudaGetErrorString(e));
-    return UFEM_OK;
-  };
-  if ((rc = upload_warp_plan(h->wplan, wh32)) || (dim == 3 && (rc = upload_warp_plan(h->wplan24, wh24))))
-    return fail(rc);
-  if ((ce = cudaMemset(h->d_sol, 0, size_t(h->nrows) * 8)) || (ce = cudaMemset(h->d_state, 0, size_t(N) * 32)) ||
-      (ce = cudaMemset(h->d_hist, 0, size_t(N) * 96)) || (ce = cudaMemset(h->d_uadv, 0, size_t(N) * 32)) ||
-      (ce = cudaMemset(h->d_nu, 0, size_t(N) * 8)) || (ce = cudaMemset(h->d_rhs, 0, size_t(h->nrows) * 8)))
-    return fail(set_error(UFEM_ERR_CUDA, std::string("memset: ") + cudaGetErrorString(ce)));
-  if ((rc = launch_build_csr(h, 0))) return fail(rc);
-  if ((ce = cudaDeviceSynchronize()) != cudaSuccess)
-    return fail(set_error(UFEM_ERR_CUDA, std::string("CSR build: ") + cudaGetErrorString(ce)));
-  for (auto& e : h->ev)
-    if (cudaEventCreate(&e) != cudaSuccess) return fail(set_error(UFEM_ERR_CUDA, "cudaEventCreate failed"));
-  *out = h;
-  return UFEM_OK;
+int ufem_ns_create_periodic(const ufem_mesh* mesh, const ufem_ns_options* opts, const uint32_t* slaves,
+                            const uint32_t* masters, int64_t nlinks, ufem_ns_handle** out) {
+  if (nlinks < 0 || (nlinks > 0 && (!slaves || !masters)))
+    return set_error(UFEM_ERR_ARG, "invalid periodic link arrays");
+  return create_impl(mesh, opts, slaves, masters, nlinks, out);
 }
 
 int ufem_ns_set_options(ufem_ns_handle* h, const ufem_ns_options* opts) {
@@ -910,6 +993,7 @@ int ufem_ns_assemble(ufem_ns_handle* h, void* stream) {
   record(h, 1, false, s);
   const bool w32 = h->d_vals32 != nullptr;
   if ((rc = launch_assembly(h, s, w32))) return rc;
+  if ((rc = launch_tie_rows(h, s, w32))) return rc;
   record(h, 1, true, s);
   h->vals32_valid = w32;
   return UFEM_OK;

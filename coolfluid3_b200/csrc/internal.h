@@ -128,6 +128,7 @@ struct ufem_ns_handle {
   std::vector<int64_t> start_h;   // N+1
   std::vector<int32_t> adj_h;     // bnnz
   std::vector<double> coords_h;   // N x 2, 2D meshes only (constant Neumann faces)
+  std::vector<uint32_t> p2m_h;    // periodic links: row node of each node (empty: no links)
   struct BCEntry { uint32_t node; int comp; double value; int32_t fn = -1; };  // fn: expression id or -1
   std::vector<std::vector<int32_t>> fn_code;   // compiled Dirichlet function expressions
   std::vector<std::vector<double>> fn_const;
@@ -156,6 +157,9 @@ struct ufem_ns_handle {
   double* d_rhs = nullptr;
   double* d_sol = nullptr;
   int64_t* d_diagpos = nullptr; // nrows
+
+  int64_t ntie = 0;               // linked (slave) nodes: tie rows x_slave - x_master = 0
+  int32_t* d_tie = nullptr;       // ntie x 2: slave, master
 
   // row-owner incidences
   int32_t* d_row_inc = nullptr;   // N+1
@@ -211,6 +215,8 @@ int assembly_chunk_capacity(int dim, int precision);
 int configure_kernels();
 
 int launch_assembly_big_rows(ufem_ns_handle* h, cudaStream_t s, bool write32);
+// Tie rows of periodic (slave) nodes: identity at the slave, minus identity at its master, rhs 0.
+int launch_tie_rows(ufem_ns_handle* h, cudaStream_t s, bool write32);
 
 // host.cu
 int build_bc_plan(ufem_ns_handle* h);

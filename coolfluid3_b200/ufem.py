@@ -50,7 +50,9 @@ class NavierStokes:
     def __init__(self, coords: np.ndarray, conn: np.ndarray, *, dt: float, density: float = 1.0,
                  use_specializations: bool = True, supg_type: str = "metric", theta: float = 1.0,
                  c1: float = 1.0, c2: float = 16.0, alpha_ps: float = 1.0, alpha_su: float = 1.0,
-                 alpha_bu: float = 1.0, u_ref: float = 1.0, precision: str = "fp64"):
+                 alpha_bu: float = 1.0, u_ref: float = 1.0, precision: str = "fp64", periodic_links=None):
+        """periodic_links: optional (slaves, masters) node arrays; see
+        ufem_ns_create_periodic."""
         self._lib = N.lib()
         coords = np.ascontiguousarray(coords, np.float64)
         conn = np.ascontiguousarray(conn, np.uint32)
@@ -67,7 +69,15 @@ class NavierStokes:
                               alpha_su=alpha_su, alpha_bu=alpha_bu, u_ref=u_ref, precision=precision))
         mesh = N.Mesh(self.dim, 0, self.nb_nodes, self.nb_elems, N.dptr(coords), N.u32ptr(conn))
         h = C.c_void_p()
-        N.check(self._lib.ufem_ns_create(C.byref(mesh), C.byref(self._opts), C.byref(h)))
+        if periodic_links is None:
+            N.check(self._lib.ufem_ns_create(C.byref(mesh), C.byref(self._opts), C.byref(h)))
+        else:
+            sl = np.ascontiguousarray(periodic_links[0], np.uint32)
+            ms = np.ascontiguousarray(periodic_links[1], np.uint32)
+            if sl.shape != ms.shape:
+                raise ValueError("periodic_links: slaves and masters must have the same length")
+            N.check(self._lib.ufem_ns_create_periodic(C.byref(mesh), C.byref(self._opts), N.u32ptr(sl), N.u32ptr(ms),
+                                                      len(sl), C.byref(h)))
         self._h = h
         nr, nnz, bnnz = C.c_int64(), C.c_int64(), C.c_int64()
         N.check(self._lib.ufem_ns_sizes(self._h, C.byref(nr), C.byref(nnz), C.byref(bnnz)))

@@ -130,6 +130,18 @@ void ufem_krylov_default_opts(ufem_krylov_opts* opts);
  * (System.cpp:82-110): copies the mesh to the device, builds the node graph,
  * the point CSR pattern and the row-owner assembly plan. */
 int ufem_ns_create(const ufem_mesh* mesh, const ufem_ns_options* opts, ufem_ns_handle** out);
+/* Periodic links (the mesh dictionary's periodic_links_nodes / periodic_links_active,
+ * LSSAction.cpp:245-269, made by PeriodicMeshPartitioner::create_link_periodic_nodes):
+ * node slaves[i] is the same unknown as masters[i].  As in the reference's map,
+ * element contributions at a slave are assembled into its master's rows and
+ * columns (chains of links resolve to the final master); the slave keeps rows of
+ * its own that tie it to the master (x_slave - x_master = 0, rhs 0), so the
+ * solve and the update give it the master's values and dof numbering stays
+ * node*neq + comp.  Boundary conditions on a slave act on its master's row.
+ * UFEM_ERR_ARG for a node linked twice, a cycle or an id out of range;
+ * UFEM_ERR_MESH when an element holds a node and its partner. */
+int ufem_ns_create_periodic(const ufem_mesh* mesh, const ufem_ns_options* opts, const uint32_t* slaves,
+                            const uint32_t* masters, int64_t nlinks, ufem_ns_handle** out);
 /* NavierStokes option triggers (trigger_assembly, NavierStokes.cpp:130-192). */
 int ufem_ns_set_options(ufem_ns_handle* h, const ufem_ns_options* opts);
 /* Device memory held by the handle (bytes, approximate to a few percent). */

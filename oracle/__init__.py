@@ -34,6 +34,8 @@ _SIG = {
     "orc_mesh_rectangle_tris": (None, [C.c_int, C.c_int, C.c_double, C.c_uint64, _D, _U32]),
     "orc_mesh_cube_tets": (None, [C.c_int, C.c_double, C.c_uint64, _D, _U32]),
     "orc_create": (C.c_void_p, [C.c_int, C.c_int64, C.c_int64, _D, _U32, C.POINTER(OrcOptions)]),
+    "orc_create_periodic": (C.c_void_p, [C.c_int, C.c_int64, C.c_int64, _D, _U32, C.POINTER(OrcOptions), _U32, _U32,
+                                         C.c_int64]),
     "orc_destroy": (None, [C.c_void_p]),
     "orc_create_lss": (C.c_void_p, [C.c_int64, C.c_int, _I64, _U32]),
     "orc_set_row": (None, [C.c_void_p, C.c_int64, C.c_int, C.c_double, C.c_double]),
@@ -174,7 +176,8 @@ class LSS:
 class Oracle:
     """Serial FP64 restatement of one NavierStokes action + its LSS."""
 
-    def __init__(self, coords, conn, opts: OrcOptions):
+    def __init__(self, coords, conn, opts: OrcOptions, periodic_links=None):
+        """periodic_links: (slaves, masters) node arrays (LSSAction.cpp:245-269)."""
         coords = np.ascontiguousarray(coords, np.float64)
         conn = np.ascontiguousarray(conn, np.uint32)
         self.dim = coords.shape[1]
@@ -182,7 +185,13 @@ class Oracle:
         self.N = coords.shape[0]
         self.E = conn.shape[0]
         self.opts = opts
-        self._h = lib().orc_create(self.dim, self.N, self.E, _d(coords), conn.ctypes.data_as(_U32), C.byref(opts))
+        if periodic_links is None:
+            self._h = lib().orc_create(self.dim, self.N, self.E, _d(coords), conn.ctypes.data_as(_U32), C.byref(opts))
+        else:
+            sl = np.ascontiguousarray(periodic_links[0], np.uint32)
+            ms = np.ascontiguousarray(periodic_links[1], np.uint32)
+            self._h = lib().orc_create_periodic(self.dim, self.N, self.E, _d(coords), conn.ctypes.data_as(_U32),
+                                                C.byref(opts), sl.ctypes.data_as(_U32), ms.ctypes.data_as(_U32), len(sl))
         if not self._h:
             raise ValueError("oracle: invalid mesh")
         self.nnz = lib().orc_nnz(self._h)

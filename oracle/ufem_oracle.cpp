@@ -86,6 +86,9 @@ struct Oracle {
   std::vector<double> force;     // body_force N x dim (empty = zero)
   std::vector<BC> bcs;
   std::vector<NeumannFace> neumann;
+  // periodic links: LSS row node of each mesh node (empty: identity)
+  std::vector<uint32_t> p2m;
+  uint32_t row_of(uint32_t node) const { return p2m.empty() ? node : p2m[node]; }
   // node -> incident elements (for the node-partitioned multi-thread baseline)
   std::vector<int64_t> inc_start;
   std::vector<uint32_t> inc_elem;
@@ -675,12 +678,12 @@ void assemble_element(Oracle& S, int64_t e, int64_t own0, int64_t own1) {
   // scatter: element row (comp*n + a) -> global (node_a*neq + comp)
   const uint32_t* cn = &S.conn[e * n];
   for (int a = 0; a < n; ++a) {
-    const int64_t ra = cn[a];
+    const int64_t ra = S.row_of(cn[a]);
     if (ra < own0 || ra >= own1) continue;
     for (int comp = 0; comp < neq; ++comp) {
       const int er = comp * n + a;
       for (int b = 0; b < n; ++b) {
-        const int64_t base = csr_pos(S, ra, comp, cn[b], 0);
+        const int64_t base = csr_pos(S, ra, comp, S.row_of(cn[b]), 0);
         for (int c = 0; c < neq; ++c) S.vals[base + c] += M[er * nd + c * n + b];
       }
       S.rhs[ra * neq + comp] += re[er];
@@ -690,10 +693,18 @@ void assemble_element(Oracle& S, int64_t e, int64_t own0, int64_t own1) {
 
 void build_graph(Oracle& S) {
   // SparsityBuilder.cpp:157-189: per-node sorted set of nodes sharing an element.
+  // With periodic links (LSSAction.cpp:245-269) a node's row is its master's:
+  // element nodes are mapped to their rows first; a linked node keeps a row
+  // that ties it to its master.
   std::vector<std::set<uint32_t>> sets(S.N);
   for (int64_t e = 0; e < S.E; ++e)
     for (int a = 0; a < S.nn; ++a)
-      for (int b = 0; b < S.nn; ++b) sets[S.conn[e * S.nn + a]].insert(S.conn[e * S.nn + b]);
+      for (int b = 0; b < S.nn; ++b) sets[S.row_of(S.conn[e * S.nn + a])].insert(S.row_of(S.conn[e * S.nn + b]));
+  for (int64_t i = 0; i < S.N; ++i)
+    if (S.row_of((uint32_t)i) != (uint32_t)i) {
+      sets[i].insert((uint32_t)i);
+      sets[i].insert(S.row_of((uint32_t)i));
+    }
   S.start.assign(S.N + 1, 0);
   for (int64_t i = 0; i < S.N; ++i) S.start[i + 1] = S.start[i] + (int64_t)sets[i].size();
   S.adj.resize(S.start[S.N]);
@@ -717,12 +728,12 @@ void build_graph(Oracle& S) {
   // node -> elements, elements ascending
   S.inc_start.assign(S.N + 1, 0);
   for (int64_t e = 0; e < S.E; ++e)
-    for (int a = 0; a < S.nn; ++a) S.inc_start[S.conn[e * S.nn + a] + 1]++;
+    for (int a = 0; a < S.nn; ++a) S.inc_start[S.row_of(S.conn[e * S.nn + a]) + 1]++;
   for (int64_t i = 0; i < S.N; ++i) S.inc_start[i + 1] += S.inc_start[i];
   S.inc_elem.resize(S.inc_start[S.N]);
   std::vector<int64_t> fill(S.inc_start.begin(), S.inc_start.end() - 1);
   for (int64_t e = 0; e < S.E; ++e)
-    for (int a = 0; a < S.nn; ++a) S.inc_elem[fill[S.conn[e * S.nn + a]]++] = (uint32_t)e;
+    for (int a = 0; a < S.nn; ++a) S.inc_elem[fill[S.row_of(S.conn[e * S.nn + a])]++] = (uint32_t)e;
 }
 
 // LinearizeU (NavierStokes.cpp:105): u_adv = 2.1875u - 2.1875u1 + 1.3125u2 - 0.3125u3
@@ -756,6 +767,19 @@ void assemble_range(Oracle& S, int64_t own0, int64_t own1, bool all_elements) {
   }
 }
 
+// Tie rows of linked nodes: x_slave - x_master = 0, rhs 0.
+void tie_rows(Oracle& S) {
+  for (int64_t i = 0; i < S.N; ++i) {
+    const uint32_t m = S.row_of((uint32_t)i);
+    if (m == (uint32_t)i) continue;
+    for (int c = 0; c < S.neq; ++c) {
+      S.vals[csr_pos(S, i, c, i, c)] = 1.0;
+      S.vals[csr_pos(S, i, c, m, c)] = -1.0;
+      S.rhs[i * S.neq + c] = 0.0;
+    }
+  }
+}
+
 // ZeroLSS (math/LSS/ZeroLSS.cpp:56-82, reset_solution=false) + LinearizeU + Assembly
 void assemble(Oracle& S, int nthreads) {
   std::fill(S.vals.begin(), S.vals.end(), 0.0);
@@ -763,6 +787,7 @@ void assemble(Oracle& S, int nthreads) {
   linearize(S);
   if (nthreads <= 1) {
     assemble_range(S, 0, S.N, true);
+    tie_rows(S);
     return;
   }
   // Node-partitioned overlap assembly: each thread owns a node range and adds
@@ -773,6 +798,7 @@ void assemble(Oracle& S, int nthreads) {
     th.emplace_back([&S, a, b] { assemble_range(S, a, b, false); });
   }
   for (auto& x : th) x.join();
+  tie_rows(S);
 }
 
 // System::dirichlet with preserve_symmetry (System.cpp:240-255) ->
@@ -819,8 +845,8 @@ void apply_neumann(Oracle& S) {
     const double nrm = std::sqrt(nx * nx + ny * ny);
     const double w = 2.0 * detj;
     const double c = w * ((0.5 * f.flux) * nrm);
-    S.rhs[(size_t)f.a * S.neq + f.comp] += c;
-    S.rhs[(size_t)f.b * S.neq + f.comp] += c;
+    S.rhs[(size_t)S.row_of(f.a) * S.neq + f.comp] += c;
+    S.rhs[(size_t)S.row_of(f.b) * S.neq + f.comp] += c;
   }
 }
 
@@ -828,9 +854,10 @@ void apply_neumann(Oracle& S) {
 // Dirichlet conditions in the order they were added.
 void apply_bcs(Oracle& S) {
   apply_neumann(S);
-  for (const BC& bc : S.bcs) {
-    const double old = S.up[(int64_t)bc.node * S.neq + bc.comp];
-    symmetric_dirichlet(S, bc.node, bc.comp, bc.value - old);
+  for (const BC& bc : S.bcs) {  // a linked node's condition acts on its master's row
+    const uint32_t row = S.row_of(bc.node);
+    const double old = S.up[(int64_t)row * S.neq + bc.comp];
+    symmetric_dirichlet(S, row, bc.comp, bc.value - old);
   }
 }
 
@@ -1047,10 +1074,29 @@ void orc_mesh_cube_tets(int n, double jitter, uint64_t seed, double* coords, uin
       }
 }
 
+void* orc_create_periodic(int dim, int64_t nb_nodes, int64_t nb_elems, const double* coords, const uint32_t* conn,
+                          const orc_options* opts, const uint32_t* slaves, const uint32_t* masters, int64_t nlinks);
+
 void* orc_create(int dim, int64_t nb_nodes, int64_t nb_elems, const double* coords, const uint32_t* conn,
                  const orc_options* opts) {
+  return orc_create_periodic(dim, nb_nodes, nb_elems, coords, conn, opts, nullptr, nullptr, 0);
+}
+
+// Periodic links slave -> master, chains resolved to the final master.
+void* orc_create_periodic(int dim, int64_t nb_nodes, int64_t nb_elems, const double* coords, const uint32_t* conn,
+                          const orc_options* opts, const uint32_t* slaves, const uint32_t* masters, int64_t nlinks) {
   if (dim != 2 && dim != 3) return nullptr;
   Oracle* S = new Oracle();
+  if (nlinks > 0) {
+    std::vector<int64_t> link(nb_nodes, -1);
+    for (int64_t i = 0; i < nlinks; ++i) link[slaves[i]] = masters[i];
+    S->p2m.resize(nb_nodes);
+    for (int64_t i = 0; i < nb_nodes; ++i) {
+      int64_t cur = i;
+      while (link[cur] >= 0) cur = link[cur];
+      S->p2m[i] = (uint32_t)cur;
+    }
+  }
   S->dim = dim;
   S->nn = dim + 1;
   S->neq = dim + 1;

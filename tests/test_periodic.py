@@ -1,0 +1,120 @@
+"""Periodic links (periodic_links_nodes / periodic_links_active of the mesh
+dictionary, LSSAction.cpp:245-269; PeriodicMeshPartitioner in the reference's
+periodic channel test): a linked node's element contributions go to its
+master's rows and columns, and its own rows tie it to the master.
+
+Stated tolerances: CSR pattern BIT-EXACT with the oracle's; assembled values
+within 1e-11 of each row's largest |entry| (the assembly parity bar); two
+time steps of a body-force-driven periodic channel within 1e-6 of the oracle,
+with every slave's state equal to its master's to 1e-10; a batch member
+assembles the same system as its own handle to 1e-14; bad links are refused.
+"""
+import numpy as np
+import pytest
+
+import oracle as O
+from coolfluid3_b200 import Batch, NavierStokes, problems as P
+from coolfluid3_b200._native import UfemError
+
+from .util import row_scaled_error, vec_rel_error
+
+
+def channel(n):
+    """2D channel on the unit square: the right wall (i = n) is linked to the
+    left wall (i = 0); no-slip bottom and top walls; pressure pinned at node 0;
+    a unit body force along x drives the flow."""
+    pb = P.make_problem(2, n, nu=1e-2, dt=0.01)
+    j = np.arange(n + 1)
+    slaves = (j * (n + 1) + n).astype(np.uint32)
+    masters = (j * (n + 1)).astype(np.uint32)
+    up, lin = pb.up.copy(), pb.lin.copy()
+    up[slaves], lin[slaves] = up[masters], lin[masters]  # linked nodes carry their master's fields
+    bottom = np.arange(n + 1, dtype=np.uint32)
+    top = np.arange(n * (n + 1), (n + 1) * (n + 1), dtype=np.uint32)
+    walls = np.concatenate([bottom, top])
+    nodes = np.concatenate([np.repeat(walls, 2), [0]]).astype(np.uint32)
+    comps = np.concatenate([np.tile([0, 1], len(walls)), [2]]).astype(np.int32)
+    values = np.zeros(len(nodes))
+    force = np.tile([1.0, 0.0], (pb.nb_nodes, 1))
+    return pb, (slaves, masters), up, lin, (nodes, comps, values), force
+
+
+def gpu(pb, links, up, lin, bcs, force):
+    ns = NavierStokes(pb.coords, pb.conn, dt=pb.dt, use_specializations=False, periodic_links=links)
+    ns.set_state(up, lin, pb.nu, force)
+    ns.add_dirichlet(*bcs)
+    return ns
+
+
+def orc(pb, links, up, lin, bcs, force):
+    o = O.Oracle(pb.coords, pb.conn, O.options(dt=pb.dt, use_specializations=False), periodic_links=links)
+    o.set_state(up, lin, pb.nu, force)
+    o.add_dirichlet(*bcs)
+    return o
+
+
+@pytest.mark.gpu
+def test_pattern_and_assembly_match_oracle():
+    case = channel(12)
+    ns, o = gpu(*case), orc(*case)
+    rp, ci = ns.csr()
+    orp, oci = o.csr()
+    assert np.array_equal(rp, orp) and np.array_equal(ci, oci)
+    ns.assemble()
+    o.assemble()
+    v, r = ns.system()
+    ov, orr = o.system()
+    assert row_scaled_error(v, ov, rp) <= 1e-11
+    assert vec_rel_error(r, orr) <= 1e-11
+    slaves, masters = case[1]
+    for s, m in zip(slaves[:3], masters[:3]):  # tie rows: x_s - x_m = 0
+        row = int(s) * 3
+        cols = ci[rp[row]:rp[row + 1]]
+        vals = v[rp[row]:rp[row + 1]]
+        assert vals[list(cols).index(int(s) * 3)] == 1.0 and vals[list(cols).index(int(m) * 3)] == -1.0
+        assert np.count_nonzero(vals) == 2 and r[row] == 0.0
+    ns.close()
+
+
+@pytest.mark.gpu
+def test_channel_steps_match_oracle_and_slaves_follow_masters():
+    case = channel(10)
+    ns, o = gpu(*case), orc(*case)
+    for _ in range(2):
+        st = ns.execute(tol=1e-12, max_iters=5000)
+        assert st["converged"] == 1
+    o.step(2, tol=1e-13)
+    up, lin = ns.state()
+    oup, olin = o.state()
+    assert vec_rel_error(up, oup) <= 1e-6 and vec_rel_error(lin, olin) <= 1e-6
+    slaves, masters = case[1]
+    assert vec_rel_error(up[slaves], up[masters]) <= 1e-10
+    assert np.max(up[:, 0]) > 0  # the body force drives the flow along x
+    ns.close()
+
+
+@pytest.mark.gpu
+def test_batch_member_with_links():
+    case = channel(8)
+    a, s = gpu(*case), gpu(*case)
+    b = Batch([a])
+    b.assemble()
+    s.assemble()
+    s.apply_dirichlet()
+    v, r = a.system()
+    vs, rs = s.system()
+    rp, _ = s.csr()
+    assert row_scaled_error(v, vs, rp) <= 1e-14 and vec_rel_error(r, rs) <= 1e-14
+    b.close()
+
+
+def test_bad_links_are_refused():
+    """Host-side validation, before any device work (runs without a GPU)."""
+    pb = P.make_problem(2, 4, nu=1e-2, dt=0.01)
+    with pytest.raises(UfemError, match="linked twice"):
+        NavierStokes(pb.coords, pb.conn, dt=pb.dt, periodic_links=([4, 4], [0, 5]))
+    with pytest.raises(UfemError, match="cycle"):
+        NavierStokes(pb.coords, pb.conn, dt=pb.dt, periodic_links=([4, 0], [0, 4]))
+    one = P.make_problem(2, 1, nu=1e-2, dt=0.01)  # a single cell: a node and its partner share an element
+    with pytest.raises(UfemError, match="too thin"):
+        NavierStokes(one.coords, one.conn, dt=one.dt, periodic_links=([1, 3], [0, 2]))
