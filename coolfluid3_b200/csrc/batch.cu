@@ -879,13 +879,20 @@ int bicgstab_b(ufem_batch* b, int pkind, double tol, int maxit, bool use_outer, 
     if (ie != cudaSuccess) return set_error(UFEM_ERR_CUDA, std::string("graph instantiate: ") + cudaGetErrorString(ie));
     b->block_pkind[slot] = pkind;
   }
+  // The host reads the members' flags after 1, then 2, 4 and at most 8 replays
+  // of the 8-iteration block: few synchronisations on long solves, little
+  // overshoot on short ones (finished members' kernels return at once).  The
+  // schedule depends on the iteration count only, so a member's arithmetic
+  // (replacements included) is the same alone and in any batch.
   int blocks = 0;
-  for (int it = 0; it < maxit + kBlockIters; it += kBlockIters) {
-    if (use_graph) {
-      UFEM_CUDA_TRY(cudaGraphLaunch(b->block_exec[slot], st));
-    } else {
-      for (int k = 0; k < kBlockIters; ++k)
-        if ((rc = bicg_iteration<MT, XL>(b, pkind, xw, st))) return rc;
+  for (int it = 0, reps = 1; it < maxit + kBlockIters; it += reps * kBlockIters, reps = std::min(2 * reps, 8)) {
+    for (int r = 0; r < reps; ++r) {
+      if (use_graph) {
+        UFEM_CUDA_TRY(cudaGraphLaunch(b->block_exec[slot], st));
+      } else {
+        for (int k = 0; k < kBlockIters; ++k)
+          if ((rc = bicg_iteration<MT, XL>(b, pkind, xw, st))) return rc;
+      }
     }
     ++blocks;
     UFEM_CUDA_TRY(cudaMemcpyAsync(b->h_ictl, b->ictl, sizeof(int) * kIc * b->nmesh, cudaMemcpyDeviceToHost, st));

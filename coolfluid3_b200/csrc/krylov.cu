@@ -728,7 +728,7 @@ int gmres(ufem_ns_handle* h, const MT* vals, const BT* b, VT* x, VT* V, VT* w, V
 }
 
 // Right-preconditioned BiCGStab with device-side scalars; the host checks the
-// done flag every `check` iterations.
+// done flag between blocks of iterations of growing length.
 template <typename VT, typename MT, typename BT>
 int bicgstab(ufem_ns_handle* h, KrylovWork& kw, const MT* vals, const BT* b, VT* x, VT* r, VT* rh, VT* p, VT* v,
              VT* sv, VT* tv, VT* ph, VT* sh, VT* dinv, int pkind, double tol, int maxit, cudaStream_t st,
@@ -749,8 +749,11 @@ int bicgstab(ufem_ns_handle* h, KrylovWork& kw, const MT* vals, const BT* b, VT*
   bicg_init_kernel<<<1, 1, 0, st>>>(kw.dctl, kw.ictl, tol);
   UFEM_CUDA_TRY(cudaGetLastError());
   const double alpha_max = std::is_same<VT, float>::value ? 1e20 : 1e150;
-  const int check = 8;
-  for (int it = 0; it < maxit; it += check) {
+  // The host reads the done flag after 8, then 16, 32 and at most 64 more
+  // iterations: few synchronisations on long solves, little overshoot on short
+  // ones (iterations after convergence return at once on the device flag).
+  int check = 8;
+  for (int it = 0; it < maxit; it += check, check = std::min(2 * check, 64)) {
     for (int k = 0; k < check; ++k) {
       bicg_p_kernel<VT><<<g1, kRedThreads, 0, st>>>(n, pkind, dinv, r, v, p, ph, kw.dctl, kw.ictl);
       if (pkind == 2 && (rc = precond<VT>(h, pkind, dinv, p, ph, kw.ictl, st))) return rc;
