@@ -175,7 +175,15 @@ class Server:
     def __init__(self, hbm_budget_bytes: int, max_slots: int = 64, precision: str = "fp64", mixed: bool = True,
                  krylov: dict | None = None, graphs: bool = True, creators: int = 2,
                  use_specializations: bool = False, realtime: bool = True, large_rows: int = 200_000,
-                 large_workers: int = 2, small_priority: bool = True):
+                 large_workers: int = 2, small_priority: bool = True, mixed_scope: str = "large"):
+        """mixed: solve with the FP32 operator copy and FP64 residual replacement.
+        mixed_scope "large" applies it to the requests of the large workers only
+        (their solves are bandwidth-bound, so the halved operator bytes pay);
+        the batched small requests, whose iterations are latency-bound, keep the
+        FP64 operator, where the FP32 operator's extra iterations would only
+        cost time.  "all" applies it to every request."""
+        if mixed_scope not in ("large", "all"):
+            raise ValueError("mixed_scope must be 'large' or 'all'")
         if precision not in ("fp32", "fp64"):
             raise ValueError("precision must be fp32 or fp64")
         self.budget = int(hbm_budget_bytes)
@@ -189,9 +197,9 @@ class Server:
         self.large_workers = int(large_workers)
         self.small_priority = bool(small_priority)
         self.krylov = dict(method="bicgstab", precond="jacobi", tol=1e-10, max_iters=3000)
-        if mixed:
-            self.krylov.update(mixed=True, inner_tol=1e-6, max_refine=20)
         self.krylov.update(krylov or {})
+        self.krylov_mixed = dict(self.krylov, mixed=True, inner_tol=1e-6, max_refine=20) if mixed else self.krylov
+        self.mixed_scope = mixed_scope
         self._lock = threading.Condition()
         self._used = 0
         self._slots = 0
@@ -267,7 +275,8 @@ class Server:
                     for a in active:
                         if a.done_steps == 0 and a.result.started == 0.0:
                             a.result.started = ts - t0
-                    sts = batch.step(stream, **self.krylov)
+                    kr = self.krylov_mixed if (key[1] == "large" or self.mixed_scope == "all") else self.krylov
+                    sts = batch.step(stream, **kr)
                     stream.synchronize()
                     ms = (time.perf_counter() - ts) * 1e3
                     finished = []

@@ -36,14 +36,14 @@ def workload(n=8, seed=5, steps=3):
 @pytest.mark.parametrize("precision,mixed", [("fp64", False), ("fp64", True), ("fp32", True)])
 def test_results_identical_alone_and_in_the_mix(precision, mixed):
     reqs = workload()
-    srv = S.Server(8 * GB, precision=precision, mixed=mixed, realtime=False)
+    srv = S.Server(8 * GB, precision=precision, mixed=mixed, realtime=False, mixed_scope="all")
     mix, stats = srv.run(reqs)
     assert stats["requests"] == len(reqs) and stats["rejected"] == 0
     assert srv.max_batch >= 2  # requests really ran together
     for r in mix:
         assert r.ok, r.statuses
     for req in reqs[:4]:
-        alone, _ = S.Server(8 * GB, precision=precision, mixed=mixed, realtime=False).run([req])
+        alone, _ = S.Server(8 * GB, precision=precision, mixed=mixed, realtime=False, mixed_scope="all").run([req])
         assert np.array_equal(alone[0].state, mix[req.rid].state), req.rid
 
 
@@ -62,7 +62,7 @@ def test_served_error_against_the_fp64_oracle(precision, tol):
     FP64 path at the reference's 1e-10 is shown beside it (its own error is
     the solver tolerance amplified by the pressure conditioning)."""
     reqs = workload(n=6, seed=9)
-    served, sstats = S.Server(8 * GB, precision=precision, mixed=True, realtime=False,
+    served, sstats = S.Server(8 * GB, precision=precision, mixed=True, realtime=False, mixed_scope="all",
                               krylov=dict(tol=1e-12)).run(reqs)
     plain, pstats = S.run_plain(reqs, realtime=False)
     worst_plain = 0.0
