@@ -110,6 +110,9 @@ SIGNATURES = {
     "ufem_ns_write_restart": (C.c_int, [_P, C.c_char_p, C.c_double, C.c_double, C.c_int64]),
     "ufem_ns_read_restart": (C.c_int, [_P, C.c_char_p, C.POINTER(C.c_double), C.POINTER(C.c_double),
                                        C.POINTER(C.c_int64)]),
+    "ufem_ns_stage_state": (C.c_int, [_P, _D, _D, _D, _P]),
+    "ufem_ns_commit_state": (C.c_int, [_P, _P]),
+    "ufem_ns_fetch_rhs": (C.c_int, [_P, _D, _P, _P]),
     "ufem_ns_get_system": (C.c_int, [_P, _D, _D]),
     "ufem_ns_download_system": (C.c_int, [_P, _D, _D, _P]),
     "ufem_ns_device_view_get": (C.c_int, [_P, C.POINTER(DeviceView)]),

@@ -306,6 +306,7 @@ void record(ufem_ns_handle* h, int phase, bool stop, cudaStream_t s) {
 void destroy_impl(ufem_ns_handle* h) {
   DeviceLock lk(device_mutex());
   krylov_free(h);
+  free_stage_pipe(h);
   free_bc_plan(h->bcp);
   dfree(h->d_coords); dfree(h->d_conn); dfree(h->d_state); dfree(h->d_hist); dfree(h->d_uadv);
   dfree(h->d_nu); dfree(h->d_force); dfree(h->d_node32); dfree(h->d_start); dfree(h->d_adj); dfree(h->d_rowptr);

@@ -115,6 +115,16 @@ struct DirichletPlan {
 
 struct KrylovWork;
 
+// Double-buffered host transfers of pipeline.cu (staged inputs, RHS outputs).
+struct StagePipe {
+  double* buf[2] = {nullptr, nullptr};  // N x (neq + 4 dim + 1): up | lin | nu
+  double* out[2] = {nullptr, nullptr};  // nrows: RHS copies being read back
+  cudaEvent_t staged[2] = {}, consumed[2] = {}, out_ready[2] = {}, out_free[2] = {};
+  bool consumed_rec[2] = {false, false}, out_free_rec[2] = {false, false};
+  int pending[2] = {0, 0};
+  int npending = 0, next = 0, out_next = 0;
+};
+
 }  // namespace ufem
 
 struct ufem_ns_handle {
@@ -173,6 +183,7 @@ struct ufem_ns_handle {
   int asm_variant = ufem::kAsmWarp;
   int asm_warps = 4;               // warps per CTA of the warp kernel
   ufem::DirichletPlan bcp;
+  ufem::StagePipe pipe;
   ufem::KrylovWork* kw = nullptr;
   bool vals32_valid = false;            // d_vals32 holds the current system (written by the assembly)
 
@@ -228,5 +239,7 @@ void krylov_free(ufem_ns_handle* h);
 // Allocates the FP32 copy of the values (converted from the current FP64
 // values); later assemblies write both.
 int ensure_vals32(ufem_ns_handle* h, cudaStream_t s);
+// pipeline.cu: frees the staging and output buffers and their events.
+void free_stage_pipe(ufem_ns_handle* h);
 
 }  // namespace ufem

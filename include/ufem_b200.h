@@ -260,6 +260,30 @@ int ufem_ns_write_restart(ufem_ns_handle* h, const char* path, double current_ti
 int ufem_ns_read_restart(ufem_ns_handle* h, const char* path, double* current_time, double* time_step,
                          int64_t* iteration);
 
+/* Overlapped host transfers.  No counterpart in the reference (its fields are
+ * host tables its CPU assembly reads in place).  For callers that keep each
+ * step's fields in host memory and want each step's RHS back: the copies of
+ * one step overlap the assembly of another.
+ *  - ufem_ns_stage_state copies up, lin, nu (the ufem_ns_set_state layouts; the
+ *    body force is left as set) into one of two device staging buffers on
+ *    `copy_stream` and returns; UFEM_ERR_STATE if two staged states are still
+ *    uncommitted.
+ *  - ufem_ns_commit_state makes `stream` wait for the oldest staged copy and
+ *    unpacks it into the handle's fields (the values ufem_ns_upload_state writes);
+ *    UFEM_ERR_STATE if nothing is staged.
+ *  - ufem_ns_fetch_rhs copies the RHS into one of two device output buffers on
+ *    `stream` (after the work queued there) and reads it into `rhs` (nb_rows
+ *    doubles) on `copy_stream`; it is complete when `copy_stream` is.
+ * Host buffers should be pinned for the copies to overlap.  A staged buffer is
+ * reused only after its commit has read it and an output buffer only after its
+ * read-back, so each host buffer may be reused once the copy stream has passed
+ * its copy.  The buffers (2 x N x (neq + 4 dim + 1) + 2 x nb_rows doubles) are
+ * allocated on the first call. */
+int ufem_ns_stage_state(ufem_ns_handle* h, const double* up, const double* lin, const double* nu,
+                        void* copy_stream);
+int ufem_ns_commit_state(ufem_ns_handle* h, void* stream);
+int ufem_ns_fetch_rhs(ufem_ns_handle* h, double* rhs, void* stream, void* copy_stream);
+
 /* Host copies of the assembled system (vals nnz, rhs nb_rows); either may be NULL. */
 int ufem_ns_get_system(ufem_ns_handle* h, double* vals, double* rhs);
 int ufem_ns_download_system(ufem_ns_handle* h, double* vals, double* rhs, void* stream);
