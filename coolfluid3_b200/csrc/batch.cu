@@ -264,6 +264,31 @@ __global__ void __launch_bounds__(256, 6) spmv_batch_kernel(int64_t total_nodes,
   spmv_node<NEQ, MT, double, double>(vals + int64_t(NEQ) * NEQ * s0, S, M.adj + s0, x, lane, y + node * NEQ);
 }
 
+// Triangles: 4 nodes per warp over all members (spmv_node3_group); each
+// 8-lane group finds its own member.
+template <typename MT, int XL>
+__global__ void __launch_bounds__(256) spmv3_batch_kernel(int64_t total_nodes, int nmesh,
+                                                          const int64_t* __restrict__ node_prefix,
+                                                          const BatchMesh* __restrict__ bm, double* xwork,
+                                                          double* __restrict__ ywork, const int* __restrict__ ictl,
+                                                          int skip_flag) {
+  const int64_t t = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+  if ((t >> 5) * 4 >= total_nodes) return;  // whole warp
+  const int64_t gnode = t >> 3;
+  const int sub = int(t & 7);
+  bool valid = gnode < total_nodes;
+  const int m = valid ? find_mesh(node_prefix, nmesh, gnode) : 0;
+  if (valid && ictl[m * kIc + skip_flag]) valid = false;
+  const BatchMesh& M = bm[m];
+  const int64_t node = valid ? gnode - node_prefix[m] : 0;
+  const MT* vals;
+  if constexpr (std::is_same<MT, float>::value) vals = M.vals32; else vals = M.vals;
+  const int64_t s0 = valid ? __ldg(M.start + node) : 0;
+  const int S = valid ? int(__ldg(M.start + node + 1) - s0) : 0;
+  spmv_node3_group<MT, double, double>(vals + 9 * s0, S, M.adj + s0, vec<XL>(M, xwork), sub, valid,
+                                       ywork + M.row_off + node * 3);
+}
+
 // dinv = 1 / diag (point Jacobi) of the operator the solve uses.
 template <typename MT>
 __global__ void jacobi_batch_kernel(const Chunk* __restrict__ chunks, const BatchMesh* __restrict__ bm,
@@ -790,7 +815,8 @@ int spmv_b(ufem_batch* b, double* x, double* y, cudaStream_t st, int skip_flag =
     spmv_batch_kernel<4, MT, XL><<<grid, 256, 0, st>>>(b->total_nodes, b->nmesh, b->d_node_prefix, b->d_mesh, x, y,
                                                        b->ictl, skip_flag);
   else
-    spmv_batch_kernel<3, MT, XL><<<grid, 256, 0, st>>>(b->total_nodes, b->nmesh, b->d_node_prefix, b->d_mesh, x, y,
+    spmv3_batch_kernel<MT, XL><<<blocks_for(b->total_nodes * 8, 256), 256, 0, st>>>(
+        b->total_nodes, b->nmesh, b->d_node_prefix, b->d_mesh, x, y,
                                                        b->ictl, skip_flag);
   UFEM_CUDA_TRY(cudaGetLastError());
   return UFEM_OK;

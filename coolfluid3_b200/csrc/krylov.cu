@@ -98,6 +98,24 @@ __global__ void __launch_bounds__(256, 6) spmv_kernel(int64_t N, const int64_t* 
   spmv_node<NEQ, MT, VT, VT>(vals + int64_t(NEQ) * NEQ * s0, S, adj + s0, x, lane, y + node * NEQ);
 }
 
+// y = A x for triangles (NEQ = 3): 4 nodes per warp (spmv_node3_group).
+template <typename VT, typename MT>
+__global__ void __launch_bounds__(256) spmv3_kernel(int64_t N, const int64_t* __restrict__ start,
+                                                    const int32_t* __restrict__ adj, const MT* __restrict__ vals,
+                                                    const VT* __restrict__ x, VT* __restrict__ y,
+                                                    const int* __restrict__ done) {
+  const int64_t t = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+  if ((t >> 5) * 4 >= N) return;  // whole warp
+  const int stop = done ? *done : 0;
+  if (stop) return;
+  const int64_t node = t >> 3;
+  const int sub = int(t & 7);
+  const bool valid = node < N;
+  const int64_t s0 = valid ? __ldg(start + node) : 0;
+  const int S = valid ? int(__ldg(start + node + 1) - s0) : 0;
+  spmv_node3_group<MT, VT, VT>(vals + 9 * s0, S, adj + s0, x, sub, valid, y + node * 3);
+}
+
 template <typename MT, typename VT>
 __global__ void jacobi_kernel(int64_t n, const int64_t* __restrict__ diagpos, const MT* __restrict__ vals,
                               VT* __restrict__ dinv) {
@@ -604,7 +622,8 @@ int spmv(ufem_ns_handle* h, const MT* vals, const VT* x, VT* y, const int* done,
   if (h->neq == 4)
     spmv_kernel<4, VT, MT><<<grid, 256, 0, s>>>(h->N, h->d_start, h->d_adj, vals, x, y, done);
   else
-    spmv_kernel<3, VT, MT><<<grid, 256, 0, s>>>(h->N, h->d_start, h->d_adj, vals, x, y, done);
+    spmv3_kernel<VT, MT><<<unsigned((h->N * 8 + 255) / 256), 256, 0, s>>>(h->N, h->d_start, h->d_adj, vals, x, y,
+                                                                          done);
   UFEM_CUDA_TRY(cudaGetLastError());
   return UFEM_OK;
 }

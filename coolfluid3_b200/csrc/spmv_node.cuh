@@ -96,5 +96,39 @@ __device__ __forceinline__ void spmv_node(const MT* __restrict__ row, int S, con
   if ((lane & 7) == 0 && r < NEQ) y[r] = YT(sum);
 }
 
+// Triangles (NEQ = 3): a node's block row is short (about 7 neighbours x 3
+// columns), so a warp serves 4 nodes, 8 lanes each; lane `sub` of a group owns
+// the neighbours sub, sub + 8, ...: their 3 x entries and the 3 x 3 values of
+// each neighbour block.  The group's sums are reduced over its 8 lanes in a
+// fixed order; lanes 0..2 of the group write the node's 3 rows.  Every lane
+// of the warp takes part in the shuffles (`valid` false: a group past the end).
+template <typename MT, typename VT, typename YT>
+__device__ __forceinline__ void spmv_node3_group(const MT* __restrict__ row, int S, const int32_t* __restrict__ adj,
+                                                 const VT* __restrict__ x, int sub, bool valid,
+                                                 YT* __restrict__ y) {
+  constexpr unsigned FULL = 0xffffffffu;
+  double acc[3] = {0.0, 0.0, 0.0};
+  if (valid) {
+    const int len = 3 * S;
+#pragma unroll 1
+    for (int s = sub; s < S; s += 8) {
+      const int64_t col = __ldg(adj + s);
+      double xv[3];
+#pragma unroll
+      for (int c = 0; c < 3; ++c) xv[c] = double(__ldg(x + col * 3 + c));
+#pragma unroll
+      for (int r = 0; r < 3; ++r)
+#pragma unroll
+        for (int c = 0; c < 3; ++c) acc[r] = fma(double(__ldcs(row + r * len + s * 3 + c)), xv[c], acc[r]);
+    }
+  }
+#pragma unroll
+  for (int r = 0; r < 3; ++r) {
+    acc[r] += __shfl_xor_sync(FULL, acc[r], 4);
+    acc[r] += __shfl_xor_sync(FULL, acc[r], 2);
+    acc[r] += __shfl_xor_sync(FULL, acc[r], 1);
+  }
+  if (valid && sub < 3) y[sub] = YT(sub == 0 ? acc[0] : (sub == 1 ? acc[1] : acc[2]));
+}
 
 }  // namespace ufem
