@@ -126,6 +126,7 @@ SIGNATURES = {
     "ufem_batch_size": (C.c_int, [_P, C.POINTER(C.c_int32), C.POINTER(C.c_int64)]),
     "ufem_batch_set_graphs": (C.c_int, [_P, C.c_int32]),
     "ufem_batch_set_assembly_warps": (C.c_int, [_P, C.c_int32]),
+    "ufem_batch_tune_assembly": (C.c_int, [_P, C.c_void_p, C.c_int32, C.POINTER(C.c_int32), C.POINTER(C.c_float)]),
     "ufem_batch_assemble": (C.c_int, [_P, C.c_void_p]),
     "ufem_batch_solve": (C.c_int, [_P, C.POINTER(KrylovOpts), C.POINTER(KrylovStatus), C.c_void_p]),
     "ufem_batch_update": (C.c_int, [_P, C.c_void_p]),

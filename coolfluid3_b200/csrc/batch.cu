@@ -1066,6 +1066,62 @@ int ufem_batch_set_assembly_warps(ufem_batch* b, int32_t warps_per_cta) {
   return UFEM_OK;
 }
 
+int ufem_batch_tune_assembly(ufem_batch* b, void* stream, int32_t reps, int32_t* warps_per_cta,
+                              float* ms_per_launch) {
+  if (!b) return set_error(UFEM_ERR_ARG, "NULL batch");
+  for (const ufem_ns_handle* h : b->members)
+    if (!h->state_set) return set_error(UFEM_ERR_STATE, "every member's state must be set before tuning");
+  if (reps < 1) reps = 5;
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  int rc;
+  if (batch_dirty(b)) {
+    UFEM_CUDA_TRY(cudaStreamSynchronize(st));
+    if ((rc = batch_refresh(b))) return rc;
+  }
+  linearize_batch_kernel<<<blocks_for(b->total_nodes, 256), 256, 0, st>>>(b->total_nodes, b->nmesh,
+                                                                          b->d_node_prefix, b->d_mesh);
+  UFEM_CUDA_TRY(cudaGetLastError());
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  UFEM_CUDA_TRY(cudaEventCreate(&e0));
+  if (cudaEventCreate(&e1) != cudaSuccess) {
+    cudaEventDestroy(e0);
+    return set_error(UFEM_ERR_CUDA, "cudaEventCreate failed");
+  }
+  float best = -1.0f;
+  int pick = b->warps;
+  rc = UFEM_OK;
+  for (int w : {2, 4, 8}) {
+    auto launch = [&] {
+      return launch_assembly_batch(b->dim, b->precision, b->spec != 0, w, b->ngroups, b->nmesh, b->d_asm,
+                                   b->d_gprefix, st);
+    };
+    if ((rc = launch())) break;  // warm-up
+    cudaEventRecord(e0, st);
+    for (int r = 0; r < reps && rc == UFEM_OK; ++r) rc = launch();
+    if (rc) break;
+    cudaEventRecord(e1, st);
+    cudaError_t ce = cudaEventSynchronize(e1);
+    float ms = 0.0f;
+    if (ce == cudaSuccess) ce = cudaEventElapsedTime(&ms, e0, e1);
+    if (ce != cudaSuccess) {
+      rc = set_error(UFEM_ERR_CUDA, std::string("batch assembly tuning: ") + cudaGetErrorString(ce));
+      break;
+    }
+    ms /= float(reps);
+    if (best < 0.0f || ms < best) {
+      best = ms;
+      pick = w;
+    }
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  if (rc) return rc;
+  b->warps = pick;
+  if (warps_per_cta) *warps_per_cta = pick;
+  if (ms_per_launch) *ms_per_launch = best;
+  return UFEM_OK;  // the members' systems are overwritten: assemble before solving
+}
+
 int ufem_batch_assemble(ufem_batch* b, void* stream) {
   if (!b) return set_error(UFEM_ERR_ARG, "NULL batch");
   cudaStream_t st = static_cast<cudaStream_t>(stream);

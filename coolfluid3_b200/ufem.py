@@ -360,6 +360,13 @@ class Batch:
     def set_graphs(self, on: bool) -> None:
         N.check(self._lib.ufem_batch_set_graphs(self._b, 1 if on else 0))
 
+    def tune_assembly(self, reps: int = 5, stream=None) -> dict:
+        """Time the batched assembly with 2, 4 and 8 warps per CTA and keep the
+        fastest (the members' systems are overwritten; assemble afterwards)."""
+        w, ms = C.c_int32(), C.c_float()
+        N.check(self._lib.ufem_batch_tune_assembly(self._b, _stream(stream), int(reps), C.byref(w), C.byref(ms)))
+        return {"warps_per_cta": w.value, "ms": ms.value}
+
     def assemble(self, stream=None) -> None:
         N.check(self._lib.ufem_batch_assemble(self._b, _stream(stream)))
 

@@ -326,6 +326,13 @@ int ufem_batch_create(ufem_ns_handle* const* members, int32_t n, ufem_batch** ou
 int ufem_batch_size(const ufem_batch* b, int32_t* n, int64_t* rows);
 int ufem_batch_set_graphs(ufem_batch* b, int32_t enable);
 int ufem_batch_set_assembly_warps(ufem_batch* b, int32_t warps_per_cta);
+/* Batch autotuner (project-written, no counterpart in the reference): times the
+ * batched warp assembly with 2, 4 and 8 warps per CTA on the members' own meshes
+ * and states (warm-up + `reps` launches, CUDA events on `stream`), keeps the
+ * fastest for this batch and returns it with its time per launch (outputs may be
+ * NULL).  The members' systems are overwritten: assemble before solving. */
+int ufem_batch_tune_assembly(ufem_batch* b, void* stream, int32_t reps, int32_t* warps_per_cta,
+                             float* ms_per_launch);
 /* LinearizeU + assembly + symmetric Dirichlet of every member. */
 int ufem_batch_assemble(ufem_batch* b, void* stream);
 /* statuses: one per member, or NULL. */

@@ -125,3 +125,23 @@ def test_batch_rejects_incompatible_members():
         Batch([a, c])
     with pytest.raises(UfemError):
         Batch([a, a])
+
+
+@pytest.mark.parametrize("specs", [SIZES_2D, SIZES_3D])
+def test_batch_autotuner(specs):
+    """The batch autotuner keeps one of its candidates, and the assembly with
+    the chosen width matches the default one to rounding (1e-14 of the row)."""
+    ms = [member(*s) for s in specs]
+    ref_ms = [member(*s) for s in specs]
+    b, ref = Batch(ms), Batch(ref_ms)
+    t = b.tune_assembly(reps=2)
+    assert t["warps_per_cta"] in (2, 4, 8) and t["ms"] > 0
+    b.assemble()
+    ref.assemble()
+    for m, r in zip(ms, ref_ms):
+        v, rhs = m.system()
+        vr, rhsr = r.system()
+        rp, _ = r.csr()
+        assert row_scaled_error(v, vr, rp) <= 1e-14 and vec_rel_error(rhs, rhsr) <= 1e-14
+    b.close()
+    ref.close()
