@@ -783,6 +783,8 @@ int ufem_ns_device_bytes(const ufem_ns_handle* h, int64_t* bytes) {
   if (h->d_vals32) b += Z * 4;
   if (h->d_node32) b += N * 32;
   if (h->kw) b += R * 8 * 13;  // Krylov vectors once a solve has run
+  if (h->pipe.buf[0]) b += 2 * (N * (h->neq + 4 * h->dim + 1) + R) * 8;  // overlapped-transfer buffers, once used
+  if (h->d_tie) b += h->ntie * 8;
   b += h->bcp.nbc * 40 + h->bcp.nfix_rows * 16 + h->bcp.nfix * 12;
   *bytes = b;
   return UFEM_OK;
