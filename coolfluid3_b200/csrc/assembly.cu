@@ -1369,39 +1369,51 @@ __global__ void dirichlet_values_kernel(int64_t nbc, int neq, const int64_t* __r
 
 // Part 2: rows that are not constrained move their constrained columns to the
 // RHS in first-application order (the order of the sequential reference).
-// One warp per row: the lanes load the row's constrained entries in parallel,
-// lane 0 adds them to the RHS one by one in first-application order (the
-// rounding of the sequential form: no FMA, no reassociation), then the lanes
-// zero the entries.
+// Eight lanes per row, four rows per warp: the lanes load eight of the row's
+// constrained entries at a time, the terms are added to the RHS one by one in
+// first-application order (the rounding of the sequential form: no FMA, no
+// reassociation), then the lanes zero the entries.
 __global__ void dirichlet_columns_kernel(int64_t nrows, const int64_t* __restrict__ fix_row,
                                          const int64_t* __restrict__ fix_ptr, const int64_t* __restrict__ fix_pos,
                                          const int32_t* __restrict__ fix_bc, const double* __restrict__ vfirst,
                                          double* __restrict__ vals, float* __restrict__ vals32,
                                          double* __restrict__ rhs) {
-  const int64_t q = (int64_t(blockIdx.x) * blockDim.x + threadIdx.x) >> 5;
-  const int lane = threadIdx.x & 31;
-  if (q >= nrows) return;  // whole warp
-  const int64_t row = fix_row[q];
-  const int64_t k0 = fix_ptr[q], k1 = fix_ptr[q + 1];
-  double r = rhs[row];
-  for (int64_t kb = k0; kb < k1; kb += 32) {
-    const int n = int(k1 - kb < 32 ? k1 - kb : 32);
+  constexpr unsigned FULL = 0xffffffffu;
+  const int64_t t = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+  if ((t >> 5) * 4 >= nrows) return;  // whole warp
+  const int64_t q = t >> 3;
+  const int sub = int(t & 7), gbase = int(threadIdx.x & 31) & ~7;
+  const bool valid = q < nrows;
+  int64_t row = 0, k0 = 0;
+  int len = 0;
+  double r = 0.0;
+  if (valid) {
+    row = fix_row[q];
+    k0 = fix_ptr[q];
+    len = int(fix_ptr[q + 1] - k0);
+    r = rhs[row];
+  }
+  int maxlen = len;  // the warp's longest row: every lane runs the same shuffles
+  maxlen = max(maxlen, __shfl_xor_sync(FULL, maxlen, 8));
+  maxlen = max(maxlen, __shfl_xor_sync(FULL, maxlen, 16));
+  for (int kb = 0; kb < maxlen; kb += 8) {
+    const int n = len - kb;  // this row's terms left
     double term = 0.0;
     int64_t pos = -1;
-    if (lane < n) {
-      pos = fix_pos[kb + lane];
-      term = __dmul_rn(-vals[pos], vfirst[fix_bc[kb + lane]]);
+    if (sub < n) {
+      pos = fix_pos[k0 + kb + sub];
+      term = __dmul_rn(-vals[pos], vfirst[fix_bc[k0 + kb + sub]]);
     }
-    for (int j = 0; j < n; ++j) {
-      const double tj = __shfl_sync(0xffffffffu, term, j);
-      r = __dadd_rn(r, tj);
+    for (int j = 0; j < 8; ++j) {  // added one by one, in first-application order
+      const double tj = __shfl_sync(FULL, term, gbase + j);
+      if (j < n) r = __dadd_rn(r, tj);
     }
-    if (lane < n) {
+    if (sub < n) {
       vals[pos] = 0.0;
       if (vals32) vals32[pos] = 0.0f;
     }
   }
-  if (lane == 0) rhs[row] = r;
+  if (valid && sub == 0) rhs[row] = r;
 }
 
 // Part 3: constrained rows become identity rows; rhs = sol = last value - old.
@@ -1729,7 +1741,7 @@ int launch_dirichlet(ufem_ns_handle* h, cudaStream_t s) {
                                                                          h->d_state, bp.vfirst);
   UFEM_CUDA_TRY(cudaGetLastError());
   if (bp.nfix_rows > 0) {
-    dirichlet_columns_kernel<<<unsigned((bp.nfix_rows * 32 + 255) / 256), 256, 0, s>>>(
+    dirichlet_columns_kernel<<<unsigned((bp.nfix_rows * 8 + 255) / 256), 256, 0, s>>>(
         bp.nfix_rows, bp.fix_row, bp.fix_ptr, bp.fix_pos, bp.fix_bc, bp.vfirst, h->d_vals, h->d_vals32, h->d_rhs);
     UFEM_CUDA_TRY(cudaGetLastError());
   }

@@ -178,30 +178,45 @@ __global__ void dirichlet_values_batch_kernel(int64_t total, int nmesh, const in
 
 __global__ void dirichlet_columns_batch_kernel(int64_t total, int nmesh, const int64_t* __restrict__ fix_prefix,
                                                const BatchMesh* __restrict__ bm) {
-  const int64_t g = (int64_t(blockIdx.x) * blockDim.x + threadIdx.x) >> 5;  // one warp per row
-  const int lane = threadIdx.x & 31;
-  if (g >= total) return;
-  const int m = find_mesh(fix_prefix, nmesh, g);
+  constexpr unsigned FULL = 0xffffffffu;
+  const int64_t t = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;  // 8 lanes per row, as the one-mesh kernel
+  if ((t >> 5) * 4 >= total) return;  // whole warp
+  const int64_t g = t >> 3;
+  const int sub = int(t & 7), gbase = int(threadIdx.x & 31) & ~7;
+  const bool valid = g < total;
+  const int m = valid ? find_mesh(fix_prefix, nmesh, g) : 0;
   const BatchMesh& M = bm[m];
-  const int64_t q = g - fix_prefix[m];
-  const int64_t row = M.fix_row[q];
-  const int64_t k0 = M.fix_ptr[q], k1 = M.fix_ptr[q + 1];
-  double r = M.rhs[row];
-  for (int64_t kb = k0; kb < k1; kb += 32) {
-    const int n = int(k1 - kb < 32 ? k1 - kb : 32);
+  int64_t row = 0, k0 = 0;
+  int len = 0;
+  double r = 0.0;
+  if (valid) {
+    const int64_t q = g - fix_prefix[m];
+    row = M.fix_row[q];
+    k0 = M.fix_ptr[q];
+    len = int(M.fix_ptr[q + 1] - k0);
+    r = M.rhs[row];
+  }
+  int maxlen = len;
+  maxlen = max(maxlen, __shfl_xor_sync(FULL, maxlen, 8));
+  maxlen = max(maxlen, __shfl_xor_sync(FULL, maxlen, 16));
+  for (int kb = 0; kb < maxlen; kb += 8) {
+    const int n = len - kb;
     double term = 0.0;
     int64_t pos = -1;
-    if (lane < n) {
-      pos = M.fix_pos[kb + lane];
-      term = __dmul_rn(-M.vals[pos], M.vfirst[M.fix_bc[kb + lane]]);
+    if (sub < n) {
+      pos = M.fix_pos[k0 + kb + sub];
+      term = __dmul_rn(-M.vals[pos], M.vfirst[M.fix_bc[k0 + kb + sub]]);
     }
-    for (int j = 0; j < n; ++j) r = __dadd_rn(r, __shfl_sync(0xffffffffu, term, j));  // first-application order
-    if (lane < n) {
+    for (int j = 0; j < 8; ++j) {  // first-application order
+      const double tj = __shfl_sync(FULL, term, gbase + j);
+      if (j < n) r = __dadd_rn(r, tj);
+    }
+    if (sub < n) {
       M.vals[pos] = 0.0;
       if (M.vals32) M.vals32[pos] = 0.0f;
     }
   }
-  if (lane == 0) M.rhs[row] = r;
+  if (valid && sub == 0) M.rhs[row] = r;
 }
 
 __global__ void dirichlet_rows_batch_kernel(int64_t total, int nmesh, const int64_t* __restrict__ bc_prefix,
@@ -1150,7 +1165,7 @@ int ufem_batch_assemble(ufem_batch* b, void* stream) {
     dirichlet_values_batch_kernel<<<blocks_for(b->total_bc, 256), 256, 0, st>>>(b->total_bc, b->nmesh,
                                                                                  b->d_bc_prefix, b->d_mesh);
     if (b->total_fix > 0)
-      dirichlet_columns_batch_kernel<<<blocks_for(b->total_fix * 32, 256), 256, 0, st>>>(b->total_fix, b->nmesh,
+      dirichlet_columns_batch_kernel<<<blocks_for(b->total_fix * 8, 256), 256, 0, st>>>(b->total_fix, b->nmesh,
                                                                                          b->d_fix_prefix, b->d_mesh);
     dirichlet_rows_batch_kernel<<<blocks_for(b->total_bc * 32, 256), 256, 0, st>>>(b->total_bc, b->nmesh,
                                                                                    b->d_bc_prefix, b->d_mesh);
