@@ -1417,24 +1417,25 @@ __global__ void dirichlet_columns_kernel(int64_t nrows, const int64_t* __restric
 }
 
 // Part 3: constrained rows become identity rows; rhs = sol = last value - old.
-// One warp per constrained dof: the lanes zero the row (the diagonal entry is
+// Eight lanes per constrained dof: the lanes zero the row (the diagonal entry is
 // written 1 in the same pass, so no ordering between lanes is needed).
 __global__ void dirichlet_rows_kernel(int64_t nbc, int neq, const int64_t* __restrict__ bc_dof,
                                       const double* __restrict__ last, const int64_t* __restrict__ bc_diag,
                                       const int64_t* __restrict__ rowptr, const double* __restrict__ state,
                                       double* __restrict__ vals, float* __restrict__ vals32,
                                       double* __restrict__ rhs, double* __restrict__ sol) {
-  const int64_t u = (int64_t(blockIdx.x) * blockDim.x + threadIdx.x) >> 5;
-  const int lane = threadIdx.x & 31;
+  const int64_t t = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+  const int64_t u = t >> 3;  // eight lanes per constrained dof
+  const int sub = int(t & 7);
   if (u >= nbc) return;
   const int64_t dof = bc_dof[u];
   const int64_t diag = bc_diag[u];
-  for (int64_t p = rowptr[dof] + lane; p < rowptr[dof + 1]; p += 32) {
+  for (int64_t p = rowptr[dof] + sub; p < rowptr[dof + 1]; p += 8) {
     const double v = (p == diag) ? 1.0 : 0.0;
     vals[p] = v;
     if (vals32) vals32[p] = float(v);
   }
-  if (lane == 0) {
+  if (sub == 0) {
     const int64_t node = dof / neq;
     const int comp = int(dof - node * neq);
     const double v = __dsub_rn(last[u], state[4 * node + comp]);
@@ -1745,7 +1746,7 @@ int launch_dirichlet(ufem_ns_handle* h, cudaStream_t s) {
         bp.nfix_rows, bp.fix_row, bp.fix_ptr, bp.fix_pos, bp.fix_bc, bp.vfirst, h->d_vals, h->d_vals32, h->d_rhs);
     UFEM_CUDA_TRY(cudaGetLastError());
   }
-  dirichlet_rows_kernel<<<unsigned((bp.nbc * 32 + 255) / 256), 256, 0, s>>>(bp.nbc, h->neq, bp.bc_dof, bp.bc_last,
+  dirichlet_rows_kernel<<<unsigned((bp.nbc * 8 + 255) / 256), 256, 0, s>>>(bp.nbc, h->neq, bp.bc_dof, bp.bc_last,
                                                                             bp.bc_diag,
                                                         h->d_rowptr, h->d_state, h->d_vals, h->d_vals32, h->d_rhs,
                                                         h->d_sol);

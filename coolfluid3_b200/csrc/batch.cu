@@ -221,20 +221,21 @@ __global__ void dirichlet_columns_batch_kernel(int64_t total, int nmesh, const i
 
 __global__ void dirichlet_rows_batch_kernel(int64_t total, int nmesh, const int64_t* __restrict__ bc_prefix,
                                             const BatchMesh* __restrict__ bm) {
-  const int64_t g = (int64_t(blockIdx.x) * blockDim.x + threadIdx.x) >> 5;  // one warp per constrained dof
-  const int lane = threadIdx.x & 31;
+  const int64_t t = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+  const int64_t g = t >> 3;  // eight lanes per constrained dof
+  const int sub = int(t & 7);
   if (g >= total) return;
   const int m = find_mesh(bc_prefix, nmesh, g);
   const BatchMesh& M = bm[m];
   const int64_t u = g - bc_prefix[m];
   const int64_t dof = M.bc_dof[u];
   const int64_t diag = M.bc_diag[u];
-  for (int64_t p = M.rowptr[dof] + lane; p < M.rowptr[dof + 1]; p += 32) {
+  for (int64_t p = M.rowptr[dof] + sub; p < M.rowptr[dof + 1]; p += 8) {
     const double v = (p == diag) ? 1.0 : 0.0;
     M.vals[p] = v;
     if (M.vals32) M.vals32[p] = float(v);
   }
-  if (lane == 0) {
+  if (sub == 0) {
     const int64_t node = dof / M.neq;
     const int comp = int(dof - node * M.neq);
     const double v = __dsub_rn(M.bc_last[u], M.state[4 * node + comp]);
@@ -1167,7 +1168,7 @@ int ufem_batch_assemble(ufem_batch* b, void* stream) {
     if (b->total_fix > 0)
       dirichlet_columns_batch_kernel<<<blocks_for(b->total_fix * 8, 256), 256, 0, st>>>(b->total_fix, b->nmesh,
                                                                                          b->d_fix_prefix, b->d_mesh);
-    dirichlet_rows_batch_kernel<<<blocks_for(b->total_bc * 32, 256), 256, 0, st>>>(b->total_bc, b->nmesh,
+    dirichlet_rows_batch_kernel<<<blocks_for(b->total_bc * 8, 256), 256, 0, st>>>(b->total_bc, b->nmesh,
                                                                                    b->d_bc_prefix, b->d_mesh);
     UFEM_CUDA_TRY(cudaGetLastError());
   }
