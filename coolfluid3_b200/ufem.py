@@ -184,6 +184,30 @@ class NavierStokes:
                                                       len(nodes)))
 
     # -- actions -------------------------------------------------------------
+    # -- overlapped host transfers (ufem_ns_stage_state / commit_state / fetch_rhs) --
+    @staticmethod
+    def _host_ptr(a):
+        """Address of a host buffer: a (pinned) torch tensor or a C-contiguous
+        float64 numpy array, which must stay alive until its copy is done."""
+        if hasattr(a, "data_ptr"):
+            return N.raw_dptr(a.data_ptr())
+        if not (isinstance(a, np.ndarray) and a.dtype == np.float64 and a.flags.c_contiguous):
+            raise ValueError("host buffers must be C-contiguous float64 arrays or tensors")
+        return N.dptr(a)
+
+    def stage_state(self, up, lin, nu, copy_stream) -> None:
+        """Queue the upload of the next state on `copy_stream` (two staging buffers)."""
+        N.check(self._lib.ufem_ns_stage_state(self._h, self._host_ptr(up), self._host_ptr(lin), self._host_ptr(nu),
+                                              _stream(copy_stream)))
+
+    def commit_state(self, stream) -> None:
+        """Make `stream` wait for the oldest staged state and unpack it into the fields."""
+        N.check(self._lib.ufem_ns_commit_state(self._h, _stream(stream)))
+
+    def fetch_rhs(self, out, stream, copy_stream) -> None:
+        """Read the RHS back into `out` (nb_rows float64) on `copy_stream`, after `stream`'s work."""
+        N.check(self._lib.ufem_ns_fetch_rhs(self._h, self._host_ptr(out), _stream(stream), _stream(copy_stream)))
+
     def add_dirichlet_function(self, nodes: np.ndarray, comp: int, expr: str) -> None:
         """BCDirichletFunction (BCDirichletFunction.cpp:61-92): component `comp`
         of `nodes` ends at f(x, y, z, t), `expr` evaluated on the device."""
