@@ -1,18 +1,17 @@
 """Overlapped host transfers (ufem_ns_stage_state / commit_state / fetch_rhs).
 
-Stated tolerance: BITWISE -- pipelined steps on two streams (the upload of
+Through the Python wrappers over the C ABI.  Stated tolerance: BITWISE --
+pipelined steps on two streams (the upload of
 step k+1 queued before step k is assembled, every RHS read back on the copy
 stream) give each step exactly the RHS of the sequential path
 (ufem_ns_set_state, assembly, Dirichlet, system read).  Misuse (a commit with
 nothing staged, a third stage) is refused with UFEM_ERR_STATE.
 """
-import ctypes as C
-
 import numpy as np
 import pytest
 import torch
 
-from coolfluid3_b200 import NavierStokes, _native as Nat, problems as P
+from coolfluid3_b200 import NavierStokes, problems as P
 from coolfluid3_b200._native import UfemError
 
 pytestmark = pytest.mark.gpu
@@ -37,37 +36,33 @@ def test_pipelined_steps_equal_sequential(dim, n):
         ns.apply_dirichlet()
         ref.append(ns.system()[1].copy())
 
-    lib = Nat.lib()
     comp, copy = torch.cuda.Stream(), torch.cuda.Stream()
-    sp, cp = C.c_void_p(comp.cuda_stream), C.c_void_p(copy.cuda_stream)
     host = [tuple(torch.from_numpy(np.ascontiguousarray(a)).pin_memory() for a in st) for st in states]
     outs = [torch.empty(ns.nb_rows, dtype=torch.float64).pin_memory() for _ in states]
-    ptr = lambda t: Nat.raw_dptr(t.data_ptr())  # noqa: E731
 
     def stage(k):
-        up, lin, nu = host[k]
-        Nat.check(lib.ufem_ns_stage_state(ns.handle, ptr(up), ptr(lin), ptr(nu), cp))
+        ns.stage_state(*host[k], copy.cuda_stream)
 
     stage(0)
     for k in range(len(states)):
         if k + 1 < len(states):
             stage(k + 1)
-        Nat.check(lib.ufem_ns_commit_state(ns.handle, sp))
+        ns.commit_state(comp.cuda_stream)
         ns.assemble(comp.cuda_stream)
         ns.apply_dirichlet(comp.cuda_stream)
-        Nat.check(lib.ufem_ns_fetch_rhs(ns.handle, ptr(outs[k]), sp, cp))
+        ns.fetch_rhs(outs[k], comp.cuda_stream, copy.cuda_stream)
     copy.synchronize()
     comp.synchronize()
     for k in range(len(states)):
         assert np.array_equal(outs[k].numpy(), ref[k]), k
 
     with pytest.raises(UfemError, match="no staged state"):
-        Nat.check(lib.ufem_ns_commit_state(ns.handle, sp))
+        ns.commit_state(comp.cuda_stream)
     stage(0)
     stage(1)
     with pytest.raises(UfemError, match="two staged states"):
         stage(2)
-    Nat.check(lib.ufem_ns_commit_state(ns.handle, sp))
-    Nat.check(lib.ufem_ns_commit_state(ns.handle, sp))
+    ns.commit_state(comp.cuda_stream)
+    ns.commit_state(comp.cuda_stream)
     comp.synchronize()
     ns.close()
