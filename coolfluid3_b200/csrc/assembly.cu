@@ -624,6 +624,14 @@ __device__ __forceinline__ void spec_tri_row(const int (&ids)[4], int ai, const 
   const T nix = nx[0], niy = ny[0];  // row node at local position 0
   const T u_ni = u_avg[0] * nix + u_avg[1] * niy;
   const T rho = kp.rho;
+  // j-independent factors evaluated once (the same expressions as below)
+  const T su4 = tau_su / (T(4) * volume), ps4 = tau_ps / (T(4) * volume);
+  const T fsu4 = fc * tau_su / (T(4) * volume), fps4 = fc * tau_ps / (T(4) * volume);
+  const T nu4 = nu / (T(4) * volume), rho6 = T(1) / (T(6) * rho);
+  const T surho4 = tau_su / (T(4) * rho * volume), lap4 = T(1) / (T(4) * rho * volume);
+  const T bulk4 = tau_bulk / (T(4) * volume), v12 = volume / T(12);
+  const T su6 = tau_su / T(6), ps6 = tau_ps / T(6);
+  const T third = T(1. / 3.);  // the reference divides these products by 3
   T rhs[3] = {0, 0, 0};
 #pragma unroll
   for (int j = 0; j < 3; ++j) {
@@ -635,36 +643,36 @@ __device__ __forceinline__ void spec_tri_row(const int (&ids)[4], int ai, const 
     const T uk = u_avg[0], vk = u_avg[1];
     const T uknj = uk * nx[j] + vk * ny[j];
     T val = T(1. / 6.) * uknj;
-    val += tau_su / (T(4) * volume) * uknj * u_ni;
+    val += su4 * uknj * u_ni;
     A[0][0] += val; A[1][1] += val;
-    val = tau_ps / (T(4) * volume) * uknj;
+    val = ps4 * uknj;
     A[2][0] += val * nix; A[2][1] += val * niy;
     val = fc / T(6);
-    val += fc * tau_su / (T(4) * volume) * u_ni;
+    val += fsu4 * u_ni;
     A[0][0] += val * uk * nx[j]; A[0][1] += val * uk * ny[j];
     A[1][0] += val * vk * nx[j]; A[1][1] += val * vk * ny[j];
-    val = fc * tau_ps / (T(4) * volume);
+    val = fps4;
     A[2][0] += val * nix * uk * nx[j]; A[2][1] += val * nix * uk * ny[j];
     A[2][0] += val * niy * vk * nx[j]; A[2][1] += val * niy * vk * ny[j];
-    val = nu / (T(4) * volume);
+    val = nu4;
     A[0][0] += val * (T(4. / 3.) * nix * nx[j] + niy * ny[j]);
-    A[0][1] += val * nix * ny[j] / T(3);
-    A[1][0] += val * niy * nx[j] / T(3);
+    A[0][1] += val * nix * ny[j] * third;
+    A[1][0] += val * niy * nx[j] * third;
     A[1][1] += val * (nix * nx[j] + T(4. / 3.) * niy * ny[j]);
-    val = T(1) / (T(6) * rho);
-    val += tau_su / (T(4) * rho * volume) * u_ni;
+    val = rho6;
+    val += surho4 * u_ni;
     A[0][2] += nx[j] * val; A[1][2] += ny[j] * val;
-    const T laplacian = T(1) / (T(4) * rho * volume) * (nix * nx[j] + niy * ny[j]);
+    const T laplacian = lap4 * (nix * nx[j] + niy * ny[j]);
     A[2][2] += tau_ps * laplacian;
     val = T(1. / 6.);
     A[2][0] += val * nx[j]; A[2][1] += val * ny[j];
-    val = tau_bulk / (T(4) * volume);
+    val = bulk4;
     A[0][0] += val * nix * nx[j]; A[0][1] += val * nix * ny[j];
     A[1][0] += val * niy * nx[j]; A[1][1] += val * niy * ny[j];
-    val = volume / T(12) * (T(1) + (j == 0 ? T(1) : T(0)));
-    val += tau_su / T(6) * u_ni;
+    val = v12 * (T(1) + (j == 0 ? T(1) : T(0)));
+    val += su6 * u_ni;
     Tm[0][0] += val; Tm[1][1] += val;
-    val = tau_ps / T(6);
+    val = ps6;
     Tm[2][0] += val * nix; Tm[2][1] += val * niy;
     T xb[3];
     load_state<2, T>(nd, ids[j], xb);
@@ -724,6 +732,15 @@ __device__ __forceinline__ void spec_tet_row(const int (&ids)[4], int ai, const 
   }
   const T u_ni = u_avg[XX] * ni[XX] + u_avg[YY] * ni[YY] + u_avg[ZZ] * ni[ZZ];
   const T rho = kp.rho;
+  // The reference's j-independent factors, evaluated once (the same expressions
+  // as in the loop below, so the same values); FP64 divisions are expensive.
+  const T su9 = tau_su / (T(9) * volume), ps9 = tau_ps / (T(9) * volume);
+  const T fsu9 = fc * tau_su / (T(9) * volume), fps9 = fc * tau_ps / (T(9) * volume);
+  const T nu9 = nu / (T(9) * volume), rho12 = T(1) / (T(12) * rho);
+  const T surho9 = tau_su / (T(9) * rho * volume), psrho9 = tau_ps / (T(9) * rho * volume);
+  const T bulk9 = tau_bulk / (T(9) * volume), v20 = volume / T(20);
+  const T su12 = tau_su / T(12), ps12 = tau_ps / T(12);
+  const T third = T(1. / 3.);  // the reference divides these products by 3
   T rhs[4] = {0, 0, 0, 0};
   // local rows/cols: 0 = U, 1 = V, 2 = W, 3 = P
 #pragma unroll
@@ -737,48 +754,48 @@ __device__ __forceinline__ void spec_tet_row(const int (&ids)[4], int ai, const 
     const T* nj = nr[j];
     const T uknj = uk * nj[XX] + vk * nj[YY] + wk * nj[ZZ];
     T val = T(1. / 12.) * uknj;
-    val += tau_su / (T(9) * volume) * uknj * u_ni;
+    val += su9 * uknj * u_ni;
     A[0][0] += val; A[1][1] += val; A[2][2] += val;
-    val = tau_ps / (T(9) * volume) * uknj;
+    val = ps9 * uknj;
     A[3][0] += val * ni[XX]; A[3][1] += val * ni[YY]; A[3][2] += val * ni[ZZ];
     val = fc / T(12);
-    val += fc * tau_su / (T(9) * volume) * u_ni;
+    val += fsu9 * u_ni;
     A[0][0] += val * uk * nj[XX]; A[0][1] += val * uk * nj[YY]; A[0][2] += val * uk * nj[ZZ];
     A[1][0] += val * vk * nj[XX]; A[1][1] += val * vk * nj[YY]; A[1][2] += val * vk * nj[ZZ];
     A[2][0] += val * vk * nj[XX]; A[2][1] += val * vk * nj[YY]; A[2][2] += val * vk * nj[ZZ];
-    val = fc * tau_ps / (T(9) * volume);
+    val = fps9;
     A[3][0] += val * ni[XX] * uk * nj[XX]; A[3][1] += val * ni[XX] * uk * nj[YY];
     A[3][2] += val * ni[XX] * uk * nj[ZZ]; A[3][0] += val * ni[YY] * vk * nj[XX];
     A[3][1] += val * ni[YY] * vk * nj[YY]; A[3][2] += val * ni[YY] * vk * nj[ZZ];
     A[3][0] += val * ni[ZZ] * vk * nj[XX]; A[3][1] += val * ni[ZZ] * vk * nj[YY];
     A[3][2] += val * ni[ZZ] * vk * nj[ZZ];
-    val = nu / (T(9) * volume);
+    val = nu9;
     A[0][0] += val * (T(4. / 3.) * ni[XX] * nj[XX] + ni[YY] * nj[YY] + ni[ZZ] * nj[ZZ]);
-    A[0][1] += val * ni[XX] * nj[YY] / T(3);
-    A[0][2] += val * ni[XX] * nj[ZZ] / T(3);
-    A[1][0] += val * ni[YY] * nj[XX] / T(3);
+    A[0][1] += val * ni[XX] * nj[YY] * third;
+    A[0][2] += val * ni[XX] * nj[ZZ] * third;
+    A[1][0] += val * ni[YY] * nj[XX] * third;
     A[1][1] += val * (ni[XX] * nj[XX] + T(4. / 3.) * ni[YY] * nj[YY] + ni[ZZ] * nj[ZZ]);
-    A[1][2] += val * ni[YY] * nj[ZZ] / T(3);
-    A[2][0] += val * ni[ZZ] * nj[XX] / T(3);
-    A[2][1] += val * ni[ZZ] * nj[YY] / T(3);
+    A[1][2] += val * ni[YY] * nj[ZZ] * third;
+    A[2][0] += val * ni[ZZ] * nj[XX] * third;
+    A[2][1] += val * ni[ZZ] * nj[YY] * third;
     A[2][2] += val * (ni[XX] * nj[XX] + ni[YY] * nj[YY] + T(4. / 3.) * ni[ZZ] * nj[ZZ]);
-    val = T(1) / (T(12) * rho);
-    val += tau_su / (T(9) * rho * volume) * u_ni;
+    val = rho12;
+    val += surho9 * u_ni;
     A[0][3] += nj[XX] * val; A[1][3] += nj[YY] * val; A[2][3] += nj[ZZ] * val;
-    val = tau_ps / (T(9) * rho * volume) * (ni[XX] * nj[XX] + ni[YY] * nj[YY] + ni[ZZ] * nj[ZZ]);
+    val = psrho9 * (ni[XX] * nj[XX] + ni[YY] * nj[YY] + ni[ZZ] * nj[ZZ]);
     A[3][3] += val;
     val = T(1. / 12.);
     A[3][0] += val * nj[XX]; A[3][1] += val * nj[YY]; A[3][2] += val * nj[ZZ];
-    val = tau_bulk / (T(9) * volume);
+    val = bulk9;
     A[0][0] += val * ni[XX] * nj[XX]; A[0][1] += val * ni[XX] * nj[YY];
     A[0][2] += val * ni[XX] * nj[ZZ]; A[1][0] += val * ni[YY] * nj[XX];
     A[1][1] += val * ni[YY] * nj[YY]; A[1][2] += val * ni[YY] * nj[ZZ];
     A[2][0] += val * ni[ZZ] * nj[XX]; A[2][1] += val * ni[ZZ] * nj[YY];
     A[2][2] += val * ni[ZZ] * nj[ZZ];
-    val = volume / T(20) * (T(1) + (j == 0 ? T(1) : T(0)));
-    val += tau_su / T(12) * u_ni;
+    val = v20 * (T(1) + (j == 0 ? T(1) : T(0)));
+    val += su12 * u_ni;
     Tm[0][0] += val; Tm[1][1] += val; Tm[2][2] += val;
-    val = tau_ps / T(12);
+    val = ps12;
     Tm[3][0] += val * ni[XX]; Tm[3][1] += val * ni[YY]; Tm[3][2] += val * ni[ZZ];
     T xb[4];
     load_state<3, T>(nd, ids[j], xb);
