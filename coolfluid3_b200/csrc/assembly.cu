@@ -554,8 +554,10 @@ __device__ __forceinline__ void generic_row(const int (&ids)[4], int a, const No
 template <int D, typename T>
 __device__ __forceinline__ void spec_tau_common(const KParams<T>& kp, const Elem<D, T>& el, int a,
                                                 const NodeData& nd, const int (&ids)[4], T nu,
+                                                const T (&Ji)[D][D], T det, T (&xs)[D + 1][D + 1],
                                                 T& tps, T& tsu, T& tbu) {
-  // tau of the solution velocity u
+  // tau of the solution velocity u; the nodal states are returned in xs (the
+  // caller's A x needs them) and J^-1, det J come from the caller
   constexpr int n = D + 1;
   T Nc[n];
   centroid_N<D, T>(Nc);
@@ -564,17 +566,10 @@ __device__ __forceinline__ void spec_tau_common(const KParams<T>& kp, const Elem
   for (int k = 0; k < D; ++k) uc[k] = 0;
 #pragma unroll
   for (int b = 0; b < n; ++b) {
-    T x[D + 1];
-    load_state<D, T>(nd, ids[b], x);
+    load_state<D, T>(nd, ids[b], xs[b]);
 #pragma unroll
-    for (int k = 0; k < D; ++k) uc[k] += Nc[b] * x[k];
+    for (int k = 0; k < D; ++k) uc[k] += Nc[b] * xs[b][k];
   }
-  T J[D][D], Ji[D][D], det;
-#pragma unroll
-  for (int r = 0; r < D; ++r)
-#pragma unroll
-    for (int c = 0; c < D; ++c) J[r][c] = el.Xr[r + 1][c];
-  inverse_det<T>(J, Ji, det);
   T G[D][D + 1];
 #pragma unroll
   for (int r = 0; r < D; ++r) {
@@ -620,7 +615,14 @@ __device__ __forceinline__ void spec_tri_row(const int (&ids)[4], int ai, const 
   nx[1] = X[2][1] - X[0][1]; ny[1] = X[0][0] - X[2][0];
   nx[2] = X[0][1] - X[1][1]; ny[2] = X[1][0] - X[0][0];
   T tau_ps, tau_su, tau_bulk;
-  spec_tau_common<2, T>(kp, el, ai, nd, ids, nu, tau_ps, tau_su, tau_bulk);
+  T J[2][2], Ji[2][2], det;
+#pragma unroll
+  for (int r = 0; r < 2; ++r)
+#pragma unroll
+    for (int c = 0; c < 2; ++c) J[r][c] = X[r + 1][c];
+  inverse_det<T>(J, Ji, det);
+  T xs[3][3];
+  spec_tau_common<2, T>(kp, el, ai, nd, ids, nu, Ji, det, xs, tau_ps, tau_su, tau_bulk);
   const T nix = nx[0], niy = ny[0];  // row node at local position 0
   const T u_ni = u_avg[0] * nix + u_avg[1] * niy;
   const T rho = kp.rho;
@@ -674,9 +676,7 @@ __device__ __forceinline__ void spec_tri_row(const int (&ids)[4], int ai, const 
     Tm[0][0] += val; Tm[1][1] += val;
     val = ps6;
     Tm[2][0] += val * nix; Tm[2][1] += val * niy;
-    T xb[3];
-    load_state<2, T>(nd, ids[j], xb);
-    stage_block<2, T>(A, Tm, xb, kp, rhs, st, j, CH);
+    stage_block<2, T>(A, Tm, xs[j], kp, rhs, st, j, CH);
   }
   put_row<3, T>(rst, 0, CH, rhs);
 }
@@ -723,7 +723,8 @@ __device__ __forceinline__ void spec_tet_row(const int (&ids)[4], int ai, const 
   nr[3][YY] = ((X[1][ZZ]-X[0][ZZ])*(X[2][XX]-X[0][XX]) - (X[2][ZZ]-X[0][ZZ])*(X[1][XX]-X[0][XX])) / T(2);
   nr[3][ZZ] = ((X[1][XX]-X[0][XX])*(X[2][YY]-X[0][YY]) - (X[2][XX]-X[0][XX])*(X[1][YY]-X[0][YY])) / T(2);
   T tau_ps, tau_su, tau_bulk;
-  spec_tau_common<3, T>(kp, el, ai, nd, ids, nu, tau_ps, tau_su, tau_bulk);
+  T xs[4][4];
+  spec_tau_common<3, T>(kp, el, ai, nd, ids, nu, Ji, det, xs, tau_ps, tau_su, tau_bulk);
   T ni[3];
 #pragma unroll
   for (int k = 0; k < 3; ++k) {
@@ -797,9 +798,7 @@ __device__ __forceinline__ void spec_tet_row(const int (&ids)[4], int ai, const 
     Tm[0][0] += val; Tm[1][1] += val; Tm[2][2] += val;
     val = ps12;
     Tm[3][0] += val * ni[XX]; Tm[3][1] += val * ni[YY]; Tm[3][2] += val * ni[ZZ];
-    T xb[4];
-    load_state<3, T>(nd, ids[j], xb);
-    stage_block<3, T>(A, Tm, xb, kp, rhs, st, j, CH);
+    stage_block<3, T>(A, Tm, xs[j], kp, rhs, st, j, CH);
   }
   put_row<4, T>(rst, 0, CH, rhs);
 }
