@@ -6,7 +6,7 @@ NavierStokes solver-action interface for Python callers and tests.
 """
 from ._native import UfemError, lib  # noqa: F401
 from .problems import Problem, config, cube_tets, lid_driven_bcs, make_problem, rectangle_tris  # noqa: F401
-from .ufem import Batch, NavierStokes, krylov_options  # noqa: F401
+from .ufem import Batch, NavierStokes, NavierStokesSemiImplicit, krylov_options  # noqa: F401
 
-__all__ = ["NavierStokes", "Batch", "UfemError", "Problem", "config", "make_problem", "rectangle_tris", "cube_tets",
+__all__ = ["NavierStokes", "NavierStokesSemiImplicit", "Batch", "UfemError", "Problem", "config", "make_problem", "rectangle_tris", "cube_tets",
            "lid_driven_bcs", "krylov_options", "lib"]

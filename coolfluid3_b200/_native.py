@@ -135,6 +135,23 @@ SIGNATURES = {
     "ufem_ns_enable_timing": (C.c_int, [_P, C.c_int32]),
     "ufem_ns_get_timings": (C.c_int, [_P, C.POINTER(Timings)]),
     "ufem_ns_destroy": (None, [_P]),
+    "ufem_nssi_create": (C.c_int, [C.POINTER(Mesh), C.POINTER(NSOptions), C.c_int32, _U32, _U32, C.c_int64,
+                                   C.POINTER(_P)]),
+    "ufem_nssi_set_krylov": (C.c_int, [_P, C.POINTER(KrylovOpts), C.POINTER(KrylovOpts)]),
+    "ufem_nssi_set_state": (C.c_int, [_P, _D, _D, _D, _D]),
+    "ufem_nssi_get_state": (C.c_int, [_P, _D, _D]),
+    "ufem_nssi_add_velocity_dirichlet": (C.c_int, [_P, _U32, C.c_int64, C.c_int32, _D]),
+    "ufem_nssi_add_pressure_dirichlet": (C.c_int, [_P, _U32, C.c_int64, _D]),
+    "ufem_nssi_clear_dirichlet": (C.c_int, [_P]),
+    "ufem_nssi_initialize": (C.c_int, [_P, C.c_int32, _P]),
+    "ufem_nssi_step": (C.c_int, [_P, C.c_int32, C.POINTER(KrylovStatus), C.POINTER(KrylovStatus), _P]),
+    "ufem_nssi_get_time": (C.c_int, [_P, C.POINTER(C.c_double)]),
+    "ufem_nssi_sizes": (C.c_int, [_P, _I64, _I64]),
+    "ufem_nssi_get_system": (C.c_int, [_P, C.c_int32, _I64, _I32, _D, _D, _D]),
+    "ufem_nssi_assemble_velocity_matrix": (C.c_int, [_P, _P]),
+    "ufem_nssi_get_lumped_inverse": (C.c_int, [_P, _D]),
+    "ufem_nssi_device_bytes": (C.c_int64, [_P]),
+    "ufem_nssi_destroy": (None, [_P]),
 }
 
 _lib = None

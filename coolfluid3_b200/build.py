@@ -16,7 +16,8 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 BUILD = os.path.join(HERE, "_build")
 LIB = os.path.join(HERE, "libufem_b200.so")
-SOURCES = ["assembly.cu", "krylov.cu", "host.cu", "batch.cu", "restart.cu", "bcfunction.cu", "pipeline.cu"]
+SOURCES = ["assembly.cu", "krylov.cu", "host.cu", "batch.cu", "restart.cu", "bcfunction.cu", "pipeline.cu",
+           "semi.cu"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_FLAGS = ["-O3", "-std=c++17", "-lineinfo", "--expt-relaxed-constexpr", "-Xcompiler", "-fPIC,-O3",
               "-Xcompiler", "-Wall,-Wno-unused-function"]

@@ -305,6 +305,12 @@ void record(ufem_ns_handle* h, int phase, bool stop, cudaStream_t s) {
 
 void destroy_impl(ufem_ns_handle* h) {
   DeviceLock lk(device_mutex());
+  if (h->view) {  // a system view borrows the graph, fields and tie list of its base handle
+    h->d_start = nullptr;
+    h->d_adj = nullptr;
+    h->d_state = nullptr;
+    h->d_tie = nullptr;
+  }
   krylov_free(h);
   free_stage_pipe(h);
   free_bc_plan(h->bcp);
@@ -365,7 +371,7 @@ int periodic_map(int64_t N, const uint32_t* slaves, const uint32_t* masters, int
 
 namespace {
 int create_impl(const ufem_mesh* mesh, const ufem_ns_options* opts, const uint32_t* slaves,
-                const uint32_t* masters, int64_t nlinks, ufem_ns_handle** out) {
+                const uint32_t* masters, int64_t nlinks, ufem_ns_handle** out, bool coupled = true) {
   if (!out) return set_error(UFEM_ERR_ARG, "out handle pointer is NULL");
   *out = nullptr;
   if (!mesh || !mesh->coords || !mesh->conn) return set_error(UFEM_ERR_ARG, "mesh or its arrays are NULL");
@@ -589,10 +595,12 @@ int create_impl(const ufem_mesh* mesh, const ufem_ns_options* opts, const uint32
       (rc = dmalloc(&h->d_state, size_t(N) * 4, "state")) || (rc = dmalloc(&h->d_hist, size_t(N) * 12, "history")) ||
       (rc = dmalloc(&h->d_uadv, size_t(N) * 4, "u_adv")) || (rc = dmalloc(&h->d_nu, size_t(N), "nu")) ||
       (rc = dmalloc(&h->d_start, size_t(N) + 1, "start")) || (rc = dmalloc(&h->d_adj, size_t(h->bnnz), "adj")) ||
-      (rc = dmalloc(&h->d_rowptr, size_t(h->nrows) + 1, "rowptr")) ||
-      (rc = dmalloc(&h->d_colidx, size_t(h->nnz), "colidx")) || (rc = dmalloc(&h->d_vals, size_t(h->nnz), "vals")) ||
-      (rc = dmalloc(&h->d_rhs, size_t(h->nrows), "rhs")) || (rc = dmalloc(&h->d_sol, size_t(h->nrows), "sol")) ||
-      (rc = dmalloc(&h->d_diagpos, size_t(h->nrows), "diagpos")) ||
+      (coupled && ((rc = dmalloc(&h->d_rowptr, size_t(h->nrows) + 1, "rowptr")) ||
+                   (rc = dmalloc(&h->d_colidx, size_t(h->nnz), "colidx")) ||
+                   (rc = dmalloc(&h->d_vals, size_t(h->nnz), "vals")) ||
+                   (rc = dmalloc(&h->d_rhs, size_t(h->nrows), "rhs")) ||
+                   (rc = dmalloc(&h->d_sol, size_t(h->nrows), "sol")) ||
+                   (rc = dmalloc(&h->d_diagpos, size_t(h->nrows), "diagpos")))) ||
       (rc = dmalloc(&h->d_row_inc, size_t(N) + 1, "row_inc")) ||
       (rc = dmalloc(&h->d_inc_elem, inc_elem.size(), "inc_elem")) ||
       (rc = dmalloc(&h->d_inc_info, inc_info.size(), "inc_info")) ||
@@ -600,7 +608,7 @@ int create_impl(const ufem_mesh* mesh, const ufem_ns_options* opts, const uint32
       (rc = dmalloc(&h->plan32.chunks, chunks32.size(), "chunks32")) ||
       (rc = dmalloc(&h->d_stage, size_t(N) * 4 * dim, "stage")))
     return fail(rc);
-  if (opts->precision == 1 && ((rc = dmalloc(&h->d_vals32, size_t(h->nnz), "vals32")) ||
+  if (coupled && opts->precision == 1 && ((rc = dmalloc(&h->d_vals32, size_t(h->nnz), "vals32")) ||
                                (rc = dmalloc(&h->d_node32, size_t(h->N) * 8, "node32"))))
     return fail(rc);
   auto up = [&](void* dst, const void* src, size_t bytes) {
@@ -643,11 +651,12 @@ int create_impl(const ufem_mesh* mesh, const ufem_ns_options* opts, const uint32
     if ((ce = up(h->d_tie, tie.data(), tie.size() * 4)))
       return fail(set_error(UFEM_ERR_CUDA, std::string("upload: ") + cudaGetErrorString(ce)));
   }
-  if ((ce = cudaMemset(h->d_sol, 0, size_t(h->nrows) * 8)) || (ce = cudaMemset(h->d_state, 0, size_t(N) * 32)) ||
-      (ce = cudaMemset(h->d_hist, 0, size_t(N) * 96)) || (ce = cudaMemset(h->d_uadv, 0, size_t(N) * 32)) ||
-      (ce = cudaMemset(h->d_nu, 0, size_t(N) * 8)) || (ce = cudaMemset(h->d_rhs, 0, size_t(h->nrows) * 8)))
+  if ((coupled && ((ce = cudaMemset(h->d_sol, 0, size_t(h->nrows) * 8)) ||
+                   (ce = cudaMemset(h->d_rhs, 0, size_t(h->nrows) * 8)))) ||
+      (ce = cudaMemset(h->d_state, 0, size_t(N) * 32)) || (ce = cudaMemset(h->d_hist, 0, size_t(N) * 96)) ||
+      (ce = cudaMemset(h->d_uadv, 0, size_t(N) * 32)) || (ce = cudaMemset(h->d_nu, 0, size_t(N) * 8)))
     return fail(set_error(UFEM_ERR_CUDA, std::string("memset: ") + cudaGetErrorString(ce)));
-  if ((rc = launch_build_csr(h, 0))) return fail(rc);
+  if (coupled && (rc = launch_build_csr(h, 0))) return fail(rc);
   if ((ce = cudaDeviceSynchronize()) != cudaSuccess)
     return fail(set_error(UFEM_ERR_CUDA, std::string("CSR build: ") + cudaGetErrorString(ce)));
   for (auto& e : h->ev)
@@ -656,6 +665,70 @@ int create_impl(const ufem_mesh* mesh, const ufem_ns_options* opts, const uint32
   return UFEM_OK;
 }
 }  // namespace
+
+namespace ufem {
+
+int create_base(const ufem_mesh* mesh, const ufem_ns_options* opts, const uint32_t* slaves, const uint32_t* masters,
+                int64_t nlinks, ufem_ns_handle** out) {
+  return create_impl(mesh, opts, slaves, masters, nlinks, out, false);
+}
+
+int make_system_view(ufem_ns_handle* base, int neq, int state_offset, ufem_ns_handle** out) {
+  *out = nullptr;
+  ufem_ns_handle* v = new ufem_ns_handle();
+  v->view = true;
+  v->dim = base->dim;
+  v->nn = base->nn;
+  v->neq = neq;
+  v->N = base->N;
+  v->E = base->E;
+  v->opt = base->opt;
+  v->start_h = base->start_h;
+  v->adj_h = base->adj_h;
+  v->p2m_h = base->p2m_h;
+  v->bnnz = base->bnnz;
+  v->nrows = base->N * neq;
+  v->nnz = base->bnnz * neq * neq;
+  v->d_start = base->d_start;
+  v->d_adj = base->d_adj;
+  v->d_state = base->d_state + state_offset;
+  v->ntie = base->ntie;
+  v->d_tie = base->d_tie;
+  int rc;
+  {
+    DeviceLock device_lock(device_mutex());
+    if ((rc = dmalloc(&v->d_rowptr, size_t(v->nrows) + 1, "rowptr")) ||
+        (rc = dmalloc(&v->d_colidx, size_t(v->nnz), "colidx")) || (rc = dmalloc(&v->d_vals, size_t(v->nnz), "vals")) ||
+        (rc = dmalloc(&v->d_rhs, size_t(v->nrows), "rhs")) || (rc = dmalloc(&v->d_sol, size_t(v->nrows), "sol")) ||
+        (rc = dmalloc(&v->d_diagpos, size_t(v->nrows), "diagpos"))) {
+      destroy_impl(v);
+      return rc;
+    }
+    cudaError_t ce;
+    if ((ce = cudaMemset(v->d_sol, 0, size_t(v->nrows) * 8)) || (ce = cudaMemset(v->d_rhs, 0, size_t(v->nrows) * 8)) ||
+        (ce = cudaMemset(v->d_vals, 0, size_t(v->nnz) * 8))) {
+      destroy_impl(v);
+      return set_error(UFEM_ERR_CUDA, std::string("memset: ") + cudaGetErrorString(ce));
+    }
+  }
+  if ((rc = launch_build_csr(v, 0))) {
+    destroy_impl(v);
+    return rc;
+  }
+  cudaError_t ce = cudaDeviceSynchronize();
+  if (ce != cudaSuccess) {
+    destroy_impl(v);
+    return set_error(UFEM_ERR_CUDA, std::string("CSR build: ") + cudaGetErrorString(ce));
+  }
+  *out = v;
+  return UFEM_OK;
+}
+
+void destroy_handle(ufem_ns_handle* h) {
+  if (h) destroy_impl(h);
+}
+
+}  // namespace ufem
 
 extern "C" {
 

@@ -133,6 +133,7 @@ struct ufem_ns_handle {
   int64_t nrows = 0, nnz = 0, bnnz = 0;
   ufem_ns_options opt{};
   bool state_set = false;
+  bool view = false;  // a system over another handle's graph and fields (semi-implicit scheme)
 
   // host copies used by planning
   std::vector<int64_t> start_h;   // N+1
@@ -231,6 +232,15 @@ int launch_tie_rows(ufem_ns_handle* h, cudaStream_t s, bool write32);
 
 // host.cu
 int build_bc_plan(ufem_ns_handle* h);
+// A handle with the mesh, fields, node graph and incidences but no coupled
+// system (the semi-implicit scheme keeps its systems in views).
+int create_base(const ufem_mesh* mesh, const ufem_ns_options* opts, const uint32_t* slaves, const uint32_t* masters,
+                int64_t nlinks, ufem_ns_handle** out);
+// A system of `neq` equations per node over the base handle's node graph; its
+// Dirichlet kernels read the field component at `state_offset` of the base's
+// node records.
+int make_system_view(ufem_ns_handle* base, int neq, int state_offset, ufem_ns_handle** out);
+void destroy_handle(ufem_ns_handle* h);
 
 // Krylov (krylov.cu)
 int krylov_solve(ufem_ns_handle* h, const ufem_krylov_opts* ko, ufem_krylov_status* st, cudaStream_t s);

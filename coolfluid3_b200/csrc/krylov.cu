@@ -98,12 +98,12 @@ __global__ void __launch_bounds__(256, 6) spmv_kernel(int64_t N, const int64_t* 
   spmv_node<NEQ, MT, VT, VT>(vals + int64_t(NEQ) * NEQ * s0, S, adj + s0, x, lane, y + node * NEQ);
 }
 
-// y = A x for triangles (NEQ = 3): 4 nodes per warp (spmv_node3_group).
-template <typename VT, typename MT>
-__global__ void __launch_bounds__(256) spmv3_kernel(int64_t N, const int64_t* __restrict__ start,
-                                                    const int32_t* __restrict__ adj, const MT* __restrict__ vals,
-                                                    const VT* __restrict__ x, VT* __restrict__ y,
-                                                    const int* __restrict__ done) {
+// y = A x for block rows of NEQ <= 3 equations: 4 nodes per warp (spmv_node_group).
+template <int NEQ, typename VT, typename MT>
+__global__ void __launch_bounds__(256) spmv_small_kernel(int64_t N, const int64_t* __restrict__ start,
+                                                         const int32_t* __restrict__ adj, const MT* __restrict__ vals,
+                                                         const VT* __restrict__ x, VT* __restrict__ y,
+                                                         const int* __restrict__ done) {
   const int64_t t = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
   if ((t >> 5) * 4 >= N) return;  // whole warp
   const int stop = done ? *done : 0;
@@ -113,7 +113,7 @@ __global__ void __launch_bounds__(256) spmv3_kernel(int64_t N, const int64_t* __
   const bool valid = node < N;
   const int64_t s0 = valid ? __ldg(start + node) : 0;
   const int S = valid ? int(__ldg(start + node + 1) - s0) : 0;
-  spmv_node3_group<MT, VT, VT>(vals + 9 * s0, S, adj + s0, x, sub, valid, y + node * 3);
+  spmv_node_group<NEQ, MT, VT, VT>(vals + NEQ * NEQ * s0, S, adj + s0, x, sub, valid, y + node * NEQ);
 }
 
 template <typename MT, typename VT>
@@ -544,6 +544,117 @@ __global__ void bicg_init_kernel(double* dctl, int* ictl, double tol) {
   ictl[3] = 0;
 }
 
+// ---- CG kernels (symmetric positive definite systems) -------------------------
+// Scalars in dctl: rho = r . z, alpha, omega slot = beta.  Five launches per
+// iteration: SpMV, p.q partials, alpha, x/r/z update with r.r and r.z
+// partials, and the fold that tests convergence and forms beta; the direction
+// update is folded into the next iteration's first kernel.
+
+// p = z + beta p (skipped on the first iteration: beta = 0, p = z).
+template <typename VT>
+__global__ void cg_p_kernel(int64_t n, const VT* __restrict__ z, VT* __restrict__ p,
+                            const double* __restrict__ dctl, const int* __restrict__ ictl) {
+  if (ictl[0]) return;
+  const double beta = dctl[kOmega];
+  GRID_STRIDE(i, n) p[i] = VT(double(z[i]) + beta * double(p[i]));
+}
+
+// alpha = rho / (p . q); a non-positive p . q stops the solve (not SPD).
+__global__ void cg_alpha_kernel(int nblk, const double* __restrict__ part, double* __restrict__ dctl,
+                                int* __restrict__ ictl) {
+  if (ictl[0]) return;
+  __shared__ double sm[32];
+  double sv = 0.0;
+  for (int b = threadIdx.x; b < nblk; b += blockDim.x) sv += part[b];
+  const double d = block_sum(sv, sm);
+  if (threadIdx.x != 0) return;
+  if (!isfinite(d)) {
+    ictl[0] = 1;
+    ictl[2] = 3;
+    return;
+  }
+  if (!(d > 0.0)) {
+    ictl[0] = 1;
+    ictl[2] = 2;
+    return;
+  }
+  dctl[kAlpha] = dctl[kRho] / d;
+}
+
+// x += alpha p ; r -= alpha q ; z = M^-1 r (point Jacobi or identity inline) ;
+// partials of r.r and r.z.  With block Jacobi (pkind 2) z is formed afterwards.
+template <typename VT>
+__global__ void cg_xr_kernel(int64_t n, int pkind, const VT* __restrict__ dinv, const VT* __restrict__ p,
+                             const VT* __restrict__ q, VT* __restrict__ x, VT* __restrict__ r, VT* __restrict__ z,
+                             const double* __restrict__ dctl, const int* __restrict__ ictl,
+                             double* __restrict__ part) {
+  if (ictl[0]) return;
+  __shared__ double sm[32];
+  const double al = dctl[kAlpha];
+  double rr = 0.0, rz = 0.0;
+  GRID_STRIDE(i, n) {
+    x[i] = VT(double(x[i]) + al * double(p[i]));
+    const VT ri = VT(double(r[i]) - al * double(q[i]));
+    r[i] = ri;
+    rr += double(ri) * double(ri);
+    if (pkind != 2) {
+      const VT zi = (pkind == 1) ? VT(dinv[i] * ri) : ri;
+      z[i] = zi;
+      rz += double(ri) * double(zi);
+    }
+  }
+  rr = block_sum(rr, sm);
+  rz = block_sum(rz, sm);
+  if (threadIdx.x == 0) {
+    part[blockIdx.x] = rr;
+    part[gridDim.x + blockIdx.x] = rz;
+  }
+}
+
+// ||r||, rho_new = r . z, beta = rho_new / rho; convergence and iteration count.
+__global__ void cg_end_kernel(int nblk, const double* __restrict__ part, double* __restrict__ dctl,
+                              int* __restrict__ ictl, double tol, int maxit) {
+  if (ictl[0]) return;
+  __shared__ double sm[32];
+  double a = 0.0, b = 0.0;
+  for (int k = threadIdx.x; k < nblk; k += blockDim.x) {
+    a += part[k];
+    b += part[nblk + k];
+  }
+  const double nn = block_sum(a, sm);
+  const double rho_new = block_sum(b, sm);
+  if (threadIdx.x != 0) return;
+  const double rn = sqrt(nn);
+  dctl[kEst] = rn;
+  dctl[kOmega] = rho_new / dctl[kRho];
+  dctl[kRho] = rho_new;
+  ictl[3] += 1;
+  if (!isfinite(rn) || !isfinite(rho_new)) {
+    ictl[0] = 1;
+    ictl[2] = 3;
+  } else if (rn <= tol * dctl[kBnorm]) {
+    ictl[0] = 1;
+  } else if (!(rho_new > 0.0)) {  // indefinite preconditioner or exact breakdown
+    ictl[0] = 1;
+    ictl[2] = 2;
+  } else if (ictl[3] >= maxit) {
+    ictl[0] = 1;
+    ictl[2] = 1;
+  }
+}
+
+// rho = r0 . z0 (from the partials), beta = 0, converged test.
+__global__ void cg_init_kernel(int nblk, const double* __restrict__ part, double* dctl, int* ictl, double tol) {
+  double s = 0.0;
+  for (int b = 0; b < nblk; ++b) s += part[b];
+  dctl[kRho] = s;
+  dctl[kOmega] = 0.0;
+  ictl[0] = (dctl[kBeta] <= tol * dctl[kBnorm] || dctl[kBnorm] == 0.0) ? 1 : 0;
+  ictl[2] = isfinite(dctl[kBeta]) ? 0 : 3;
+  if (ictl[2]) ictl[0] = 1;
+  ictl[3] = 0;
+}
+
 // ---------------------------------------------------------------------------
 template <typename T>
 int dalloc(T** p, size_t count) {
@@ -619,11 +730,15 @@ template <typename VT, typename MT>
 int spmv(ufem_ns_handle* h, const MT* vals, const VT* x, VT* y, const int* done, cudaStream_t s) {
   const int64_t threads = h->N * 32;
   const unsigned grid = unsigned((threads + 255) / 256);
+  const unsigned grid8 = unsigned((h->N * 8 + 255) / 256);  // 8 lanes per node
   if (h->neq == 4)
     spmv_kernel<4, VT, MT><<<grid, 256, 0, s>>>(h->N, h->d_start, h->d_adj, vals, x, y, done);
+  else if (h->neq == 3)
+    spmv_small_kernel<3, VT, MT><<<grid8, 256, 0, s>>>(h->N, h->d_start, h->d_adj, vals, x, y, done);
+  else if (h->neq == 2)
+    spmv_small_kernel<2, VT, MT><<<grid8, 256, 0, s>>>(h->N, h->d_start, h->d_adj, vals, x, y, done);
   else
-    spmv3_kernel<VT, MT><<<unsigned((h->N * 8 + 255) / 256), 256, 0, s>>>(h->N, h->d_start, h->d_adj, vals, x, y,
-                                                                          done);
+    spmv_small_kernel<1, VT, MT><<<grid8, 256, 0, s>>>(h->N, h->d_start, h->d_adj, vals, x, y, done);
   UFEM_CUDA_TRY(cudaGetLastError());
   return UFEM_OK;
 }
@@ -814,6 +929,68 @@ int bicgstab(ufem_ns_handle* h, KrylovWork& kw, const MT* vals, const BT* b, VT*
   return UFEM_OK;
 }
 
+// Preconditioned conjugate gradients with device-side scalars (the Belos
+// "Block CG" of the reference's semi-implicit velocity and pressure solves,
+// block size 1); the host checks the done flag as in bicgstab().
+template <typename VT, typename MT, typename BT>
+int cg(ufem_ns_handle* h, KrylovWork& kw, const MT* vals, const BT* b, VT* x, VT* r, VT* z, VT* p, VT* q, VT* dinv,
+       int pkind, double tol, int maxit, cudaStream_t st, SolveResult& res) {
+  const int64_t n = h->nrows;
+  const int nblk = kw.nblk;
+  const unsigned g1 = unsigned(nblk);
+  int rc;
+  if ((rc = setup_precond<VT, MT>(h, pkind, vals, dinv, st))) return rc;
+  res = SolveResult();
+  if ((rc = spmv<VT, MT>(h, vals, x, q, nullptr, st))) return rc;
+  residual_kernel<VT, BT><<<g1, kRedThreads, 0, st>>>(n, b, q, r, kw.part, kw.part + nblk);
+  finalize_norm_kernel<<<1, 1, 0, st>>>(nblk, kw.part, kw.dctl, kBeta, 1);
+  finalize_norm_kernel<<<1, 1, 0, st>>>(nblk, kw.part + nblk, kw.dctl, kBnorm, 1);
+  if ((rc = precond<VT>(h, pkind, dinv, r, z, nullptr, st))) return rc;
+  dot_partials_kernel<VT><<<dim3(g1, 1), kRedThreads, 0, st>>>(n, r, n, z, kw.part, nullptr);
+  cg_init_kernel<<<1, 1, 0, st>>>(nblk, kw.part, kw.dctl, kw.ictl, tol);
+  fill_kernel<VT><<<g1, kRedThreads, 0, st>>>(n, VT(0), p);
+  UFEM_CUDA_TRY(cudaGetLastError());
+  int check = 8;
+  for (int it = 0; it < maxit; it += check, check = std::min(2 * check, 64)) {
+    for (int k = 0; k < check; ++k) {
+      cg_p_kernel<VT><<<g1, kRedThreads, 0, st>>>(n, z, p, kw.dctl, kw.ictl);
+      if ((rc = spmv<VT, MT>(h, vals, p, q, kw.ictl, st))) return rc;
+      dot_partials_kernel<VT><<<dim3(g1, 1), kRedThreads, 0, st>>>(n, p, n, q, kw.part, kw.ictl);
+      cg_alpha_kernel<<<1, 256, 0, st>>>(nblk, kw.part, kw.dctl, kw.ictl);
+      cg_xr_kernel<VT><<<g1, kRedThreads, 0, st>>>(n, pkind, dinv, p, q, x, r, z, kw.dctl, kw.ictl, kw.part);
+      if (pkind == 2) {
+        if ((rc = precond<VT>(h, pkind, dinv, r, z, kw.ictl, st))) return rc;
+        dot_partials_kernel<VT><<<dim3(g1, 1), kRedThreads, 0, st>>>(n, r, n, z, kw.part + nblk, kw.ictl);
+      }
+      cg_end_kernel<<<1, 256, 0, st>>>(nblk, kw.part, kw.dctl, kw.ictl, tol, maxit);
+      UFEM_CUDA_TRY(cudaGetLastError());
+    }
+    UFEM_CUDA_TRY(cudaMemcpyAsync(kw.h_ictl, kw.ictl, 4 * sizeof(int), cudaMemcpyDeviceToHost, st));
+    UFEM_CUDA_TRY(cudaStreamSynchronize(st));
+    if (kw.h_ictl[0]) break;
+  }
+  UFEM_CUDA_TRY(cudaMemcpyAsync(kw.h_ictl, kw.ictl, 4 * sizeof(int), cudaMemcpyDeviceToHost, st));
+  UFEM_CUDA_TRY(cudaMemcpyAsync(kw.h_dctl, kw.dctl, 16 * sizeof(double), cudaMemcpyDeviceToHost, st));
+  UFEM_CUDA_TRY(cudaStreamSynchronize(st));
+  res.iters = kw.h_ictl[3];
+  res.status = kw.h_ictl[2];
+  const double bnorm = kw.h_dctl[kBnorm];
+  if (bnorm == 0.0) {
+    fill_kernel<VT><<<g1, kRedThreads, 0, st>>>(n, VT(0), x);
+    UFEM_CUDA_TRY(cudaGetLastError());
+    res.converged = true;
+    res.status = 0;
+    return UFEM_OK;
+  }
+  double rr;
+  if ((rc = true_residual<VT, MT, BT>(h, kw, vals, b, x, q, r, bnorm, st, &rr))) return rc;
+  res.relres = rr;
+  res.converged = rr <= tol;
+  if (res.converged) res.status = 0;
+  else if (res.status == 0) res.status = 1;
+  return UFEM_OK;
+}
+
 // dst32 = src64 * (1 / dctl[idx])
 __global__ void to32_scaled_kernel(int64_t n, const double* __restrict__ src, float* __restrict__ dst,
                                    const double* __restrict__ dctl, int idx) {
@@ -835,9 +1012,11 @@ int krylov_solve(ufem_ns_handle* h, const ufem_krylov_opts* ko, ufem_krylov_stat
   if (o.max_refine <= 0) o.max_refine = 20;
   if (o.inner_tol <= 0) o.inner_tol = 1e-3;
   if (o.precond < 0 || o.precond > 2) return set_error(UFEM_ERR_ARG, "precond must be 0, 1 or 2");
-  if (o.method < 0 || o.method > 1) return set_error(UFEM_ERR_ARG, "method must be 0 (GMRES) or 1 (BiCGStab)");
+  if (o.method < 0 || o.method > 2)
+    return set_error(UFEM_ERR_ARG, "method must be 0 (GMRES), 1 (BiCGStab) or 2 (CG)");
   const bool mixed = o.mixed != 0;
-  const bool bicg = o.method == 1;
+  const bool use_cg = o.method == 2;
+  const bool bicg = o.method == 1 || use_cg;  // CG uses the BiCGStab work vectors
   int rc;
   if ((rc = ensure_work(h, o.restart, mixed, bicg))) return rc;
   KrylovWork& kw = *h->kw;
@@ -846,7 +1025,10 @@ int krylov_solve(ufem_ns_handle* h, const ufem_krylov_opts* ko, ufem_krylov_stat
   ufem_krylov_status out{};
   if (!mixed) {
     SolveResult r;
-    if (bicg) {
+    if (use_cg) {
+      rc = cg<double, double, double>(h, kw, h->d_vals, h->d_rhs, h->d_sol, kw.r, kw.bs, kw.bp, kw.bv, kw.dinv,
+                                      o.precond, o.tol, o.max_iters, s, r);
+    } else if (bicg) {
       // A breakdown (rho or omega ~ 0) leaves a finite iterate: restart from it
       // while iterations remain.
       int used = 0;
@@ -914,7 +1096,14 @@ int krylov_solve(ufem_ns_handle* h, const ufem_krylov_opts* ko, ufem_krylov_stat
       // FP32-attainable accuracy, so a capped inner solve followed by a fresh
       // FP64 residual makes steadier progress than one long FP32 run.
       const int inner_iters = std::min(o.max_iters, kInnerIterCap);
-      if (bicg) {
+      if (use_cg) {
+        // FP32 operator, FP64 vectors and scalars (as for BiCGStab below)
+        scale_kernel<double><<<g1, kRedThreads, 0, s>>>(n, kw.r, kw.t, kw.dctl, kScale, nullptr);
+        fill_kernel<double><<<g1, kRedThreads, 0, s>>>(n, 0.0, kw.z);
+        UFEM_CUDA_TRY(cudaGetLastError());
+        rc = cg<double, float, double>(h, kw, h->d_vals32, kw.t, kw.z, kw.w, kw.bs, kw.bp, kw.bv, kw.dinv,
+                                       o.precond, o.inner_tol, inner_iters, s, ir);
+      } else if (bicg) {
         // FP32 operator (half the SpMV traffic), FP64 vectors and scalars: the
         // recurrences keep FP64 accuracy, only the operator is rounded, so the
         // refinement contracts by about cond(A) * 2^-24 per pass.

@@ -96,39 +96,55 @@ __device__ __forceinline__ void spmv_node(const MT* __restrict__ row, int S, con
   if ((lane & 7) == 0 && r < NEQ) y[r] = YT(sum);
 }
 
-// Triangles (NEQ = 3): a node's block row is short (about 7 neighbours x 3
-// columns), so a warp serves 4 nodes, 8 lanes each; lane `sub` of a group owns
-// the neighbours sub, sub + 8, ...: their 3 x entries and the 3 x 3 values of
-// each neighbour block.  The group's sums are reduced over its 8 lanes in a
-// fixed order; lanes 0..2 of the group write the node's 3 rows.  Every lane
-// of the warp takes part in the shuffles (`valid` false: a group past the end).
-template <typename MT, typename VT, typename YT>
-__device__ __forceinline__ void spmv_node3_group(const MT* __restrict__ row, int S, const int32_t* __restrict__ adj,
-                                                 const VT* __restrict__ x, int sub, bool valid,
-                                                 YT* __restrict__ y) {
+// Short block rows (NEQ <= 3: the coupled triangle system, and the velocity
+// and pressure systems of the semi-implicit scheme): a warp serves 4 nodes,
+// 8 lanes each; lane `sub` of a group owns the neighbours sub, sub + 8, ...:
+// their NEQ x entries and the NEQ x NEQ values of each neighbour block.  The
+// group's sums are reduced over its 8 lanes in a fixed order; lanes 0..NEQ-1
+// of the group write the node's rows.  Every lane of the warp takes part in
+// the shuffles (`valid` false: a group past the end).
+template <int NEQ, typename MT, typename VT, typename YT>
+__device__ __forceinline__ void spmv_node_group(const MT* __restrict__ row, int S, const int32_t* __restrict__ adj,
+                                                const VT* __restrict__ x, int sub, bool valid,
+                                                YT* __restrict__ y) {
+  static_assert(NEQ >= 1 && NEQ <= 3, "8-lane groups serve block rows of 1 to 3 equations");
   constexpr unsigned FULL = 0xffffffffu;
-  double acc[3] = {0.0, 0.0, 0.0};
+  double acc[NEQ];
+#pragma unroll
+  for (int r = 0; r < NEQ; ++r) acc[r] = 0.0;
   if (valid) {
-    const int len = 3 * S;
+    const int len = NEQ * S;
 #pragma unroll 1
     for (int s = sub; s < S; s += 8) {
       const int64_t col = __ldg(adj + s);
-      double xv[3];
+      double xv[NEQ];
 #pragma unroll
-      for (int c = 0; c < 3; ++c) xv[c] = double(__ldg(x + col * 3 + c));
+      for (int c = 0; c < NEQ; ++c) xv[c] = double(__ldg(x + col * NEQ + c));
 #pragma unroll
-      for (int r = 0; r < 3; ++r)
+      for (int r = 0; r < NEQ; ++r)
 #pragma unroll
-        for (int c = 0; c < 3; ++c) acc[r] = fma(double(__ldcs(row + r * len + s * 3 + c)), xv[c], acc[r]);
+        for (int c = 0; c < NEQ; ++c) acc[r] = fma(double(__ldcs(row + r * len + s * NEQ + c)), xv[c], acc[r]);
     }
   }
 #pragma unroll
-  for (int r = 0; r < 3; ++r) {
+  for (int r = 0; r < NEQ; ++r) {
     acc[r] += __shfl_xor_sync(FULL, acc[r], 4);
     acc[r] += __shfl_xor_sync(FULL, acc[r], 2);
     acc[r] += __shfl_xor_sync(FULL, acc[r], 1);
   }
-  if (valid && sub < 3) y[sub] = YT(sub == 0 ? acc[0] : (sub == 1 ? acc[1] : acc[2]));
+  double mine = acc[0];
+#pragma unroll
+  for (int r = 1; r < NEQ; ++r)
+    if (sub == r) mine = acc[r];
+  if (valid && sub < NEQ) y[sub] = YT(mine);
+}
+
+// Triangles of the coupled system (NEQ = 3).
+template <typename MT, typename VT, typename YT>
+__device__ __forceinline__ void spmv_node3_group(const MT* __restrict__ row, int S, const int32_t* __restrict__ adj,
+                                                 const VT* __restrict__ x, int sub, bool valid,
+                                                 YT* __restrict__ y) {
+  spmv_node_group<3, MT, VT, YT>(row, S, adj, x, sub, valid, y);
 }
 
 }  // namespace ufem

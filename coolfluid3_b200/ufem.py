@@ -33,7 +33,7 @@ def _stream(stream) -> C.c_void_p | None:
 def krylov_options(method: str = "bicgstab", restart: int = 30, max_iters: int = 3000, precond: str = "jacobi",
                    tol: float = 1e-10, mixed: bool = False, max_refine: int = 20, inner_tol: float = 1e-3):
     o = N.KrylovOpts()
-    o.method = {"gmres": 0, "bicgstab": 1}[method]
+    o.method = {"gmres": 0, "bicgstab": 1, "cg": 2}[method]
     o.restart = restart
     o.max_iters = max_iters
     o.precond = {"none": 0, "jacobi": 1, "block_jacobi": 2}[precond]
@@ -342,6 +342,162 @@ class NavierStokes:
     def close(self) -> None:
         if getattr(self, "_h", None):
             self._lib.ufem_ns_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+
+class NavierStokesSemiImplicit:
+    """UFEM's semi-implicit solver (``cf3.UFEM.NavierStokesSemiImplicit``,
+    plugins/UFEM/src/UFEM/ns_semi_implicit/implementation/NavierStokesSemiImplicit.cpp):
+    a velocity system and a pressure system, ``nb_iterations`` predictor /
+    corrector passes per time step.  Options follow the reference's
+    (``theta``, ``nb_iterations``, ``supg_type``, ``alpha_*``, ``c1``, ``c2``,
+    ``u_ref``); the body force term is on when a force field is given
+    (``enable_body_force``).  Velocity and pressure conditions are added to
+    ``VelocityLSS.BC`` / ``PressureLSS.BC`` through ``add_velocity_dirichlet`` and
+    ``add_pressure_dirichlet``."""
+
+    def __init__(self, coords: np.ndarray, conn: np.ndarray, *, dt: float, theta: float = 1.0,
+                 nb_iterations: int = 2, supg_type: str = "metric", c1: float = 1.0, c2: float = 16.0,
+                 alpha_ps: float = 1.0, alpha_su: float = 1.0, alpha_bu: float = 1.0, u_ref: float = 1.0,
+                 periodic_links=None):
+        self._lib = N.lib()
+        coords = np.ascontiguousarray(coords, np.float64)
+        conn = np.ascontiguousarray(conn, np.uint32)
+        self.dim = coords.shape[1]
+        self.nb_nodes = coords.shape[0]
+        self.nb_elems = conn.shape[0]
+        if conn.shape[1] != self.dim + 1:
+            raise ValueError("connectivity must have dim+1 columns (P1 triangles or tetrahedra)")
+        o = N.NSOptions()
+        self._lib.ufem_ns_default_options(C.byref(o))
+        if supg_type not in SUPG_TYPES:
+            raise ValueError(f"supg_type must be one of {sorted(SUPG_TYPES)}")
+        o.dt, o.theta, o.supg_type = float(dt), float(theta), SUPG_TYPES[supg_type]
+        o.c1, o.c2, o.alpha_ps, o.alpha_su, o.alpha_bu, o.u_ref = c1, c2, alpha_ps, alpha_su, alpha_bu, u_ref
+        self.dt = float(dt)
+        mesh = N.Mesh(self.dim, 0, self.nb_nodes, self.nb_elems, N.dptr(coords), N.u32ptr(conn))
+        sl = ms = None
+        n = 0
+        if periodic_links is not None:
+            sl = np.ascontiguousarray(periodic_links[0], np.uint32)
+            ms = np.ascontiguousarray(periodic_links[1], np.uint32)
+            if sl.shape != ms.shape:
+                raise ValueError("periodic_links: slaves and masters must have the same length")
+            n = len(sl)
+        h = C.c_void_p()
+        N.check(self._lib.ufem_nssi_create(C.byref(mesh), C.byref(o), int(nb_iterations),
+                                           None if sl is None else N.u32ptr(sl),
+                                           None if ms is None else N.u32ptr(ms), n, C.byref(h)))
+        self._h = h
+        self._keep = (sl, ms)
+        vn, pn = C.c_int64(), C.c_int64()
+        N.check(self._lib.ufem_nssi_sizes(self._h, C.byref(vn), C.byref(pn)))
+        self.velocity_nnz, self.pressure_nnz = vn.value, pn.value
+        self.set_krylov()
+
+    def set_krylov(self, velocity: dict | None = None, pressure: dict | None = None) -> None:
+        """Krylov options of the two solves (default: CG, point Jacobi, 1e-10)."""
+        kv = krylov_options(**{"method": "cg", **(velocity or {})})
+        kp = krylov_options(**{"method": "cg", **(pressure or {})})
+        N.check(self._lib.ufem_nssi_set_krylov(self._h, C.byref(kv), C.byref(kp)))
+
+    def initial_conditions(self, u: np.ndarray, nu: float | np.ndarray, p: np.ndarray | None = None,
+                           force: np.ndarray | None = None) -> None:
+        """Fields and the solver's initial conditions (NavierStokesSemiImplicit.cpp:400-455):
+        u_adv = u1 = u2 = u3 = u, nu_eff = nu, the pressure matrix and the lumped mass."""
+        u = np.ascontiguousarray(u, np.float64)
+        up = np.zeros((self.nb_nodes, self.dim + 1))
+        up[:, : self.dim] = u
+        if p is not None:
+            up[:, self.dim] = p
+        lin = np.tile(u, (1, 4))
+        nuv = np.ascontiguousarray(np.broadcast_to(np.asarray(nu, np.float64), (self.nb_nodes,)))
+        self.set_state(up, lin, nuv, force)
+        self.initialize(reset_history=True)
+
+    def set_state(self, up, lin, nu, force=None) -> None:
+        up = np.ascontiguousarray(up, np.float64)
+        lin = np.ascontiguousarray(lin, np.float64)
+        nu = np.ascontiguousarray(nu, np.float64)
+        if up.shape != (self.nb_nodes, self.dim + 1) or lin.shape != (self.nb_nodes, 4 * self.dim) or \
+                nu.shape != (self.nb_nodes,):
+            raise ValueError("field shapes must be (N, dim+1), (N, 4*dim), (N,)")
+        f = None if force is None else np.ascontiguousarray(force, np.float64)
+        N.check(self._lib.ufem_nssi_set_state(self._h, N.dptr(up), N.dptr(lin), N.dptr(nu), N.dptr(f)))
+
+    def initialize(self, reset_history: bool = True, stream=None) -> None:
+        N.check(self._lib.ufem_nssi_initialize(self._h, 1 if reset_history else 0, _stream(stream)))
+
+    @property
+    def state(self):
+        up = np.empty((self.nb_nodes, self.dim + 1))
+        lin = np.empty((self.nb_nodes, 4 * self.dim))
+        N.check(self._lib.ufem_nssi_get_state(self._h, N.dptr(up), N.dptr(lin)))
+        return up, lin
+
+    @property
+    def time(self) -> float:
+        t = C.c_double()
+        N.check(self._lib.ufem_nssi_get_time(self._h, C.byref(t)))
+        return t.value
+
+    def add_velocity_dirichlet(self, nodes, comp: int, values) -> None:
+        nodes = np.ascontiguousarray(nodes, np.uint32)
+        values = np.ascontiguousarray(np.broadcast_to(np.asarray(values, np.float64), nodes.shape))
+        N.check(self._lib.ufem_nssi_add_velocity_dirichlet(self._h, N.u32ptr(nodes), len(nodes), int(comp),
+                                                           N.dptr(values)))
+
+    def add_pressure_dirichlet(self, nodes, values) -> None:
+        nodes = np.ascontiguousarray(nodes, np.uint32)
+        values = np.ascontiguousarray(np.broadcast_to(np.asarray(values, np.float64), nodes.shape))
+        N.check(self._lib.ufem_nssi_add_pressure_dirichlet(self._h, N.u32ptr(nodes), len(nodes), N.dptr(values)))
+
+    def clear_dirichlet(self) -> None:
+        N.check(self._lib.ufem_nssi_clear_dirichlet(self._h))
+
+    def step(self, nsteps: int = 1, stream=None) -> tuple[dict, dict]:
+        """nsteps time steps; returns the folded (velocity, pressure) solve statuses."""
+        sv, sp = N.KrylovStatus(), N.KrylovStatus()
+        N.check(self._lib.ufem_nssi_step(self._h, int(nsteps), C.byref(sv), C.byref(sp), _stream(stream)))
+        return sv.as_dict(), sp.as_dict()
+
+    def system(self, which: str):
+        """(rowptr, colidx, vals, rhs, sol) of the "velocity" or "pressure" system."""
+        w = {"velocity": 0, "pressure": 1}[which]
+        nrows = self.nb_nodes * (self.dim if w == 0 else 1)
+        nnz = self.velocity_nnz if w == 0 else self.pressure_nnz
+        rp, ci = np.empty(nrows + 1, np.int64), np.empty(nnz, np.int32)
+        v, r, s = np.empty(nnz), np.empty(nrows), np.empty(nrows)
+        N.check(self._lib.ufem_nssi_get_system(self._h, w, N.i64ptr(rp), N.i32ptr(ci), N.dptr(v), N.dptr(r),
+                                               N.dptr(s)))
+        return rp, ci, v, r, s
+
+    def assemble_velocity_matrix(self, stream=None) -> None:
+        N.check(self._lib.ufem_nssi_assemble_velocity_matrix(self._h, _stream(stream)))
+
+    def lumped_inverse(self) -> np.ndarray:
+        out = np.empty((self.nb_nodes, self.dim))
+        N.check(self._lib.ufem_nssi_get_lumped_inverse(self._h, N.dptr(out)))
+        return out
+
+    def device_bytes(self) -> int:
+        return int(self._lib.ufem_nssi_device_bytes(self._h))
+
+    def close(self) -> None:
+        if getattr(self, "_h", None):
+            self._lib.ufem_nssi_destroy(self._h)
             self._h = None
 
     def __del__(self):

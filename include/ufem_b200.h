@@ -70,7 +70,7 @@ typedef struct ufem_ns_options {
 
 /* Krylov options (SolveLSS / Belos GMRES replacement). */
 typedef struct ufem_krylov_opts {
-  int32_t method;      /* 0: GMRES(restart)  1: BiCGStab (default)                */
+  int32_t method;      /* 0: GMRES(restart)  1: BiCGStab (default)  2: CG (SPD)   */
   int32_t restart;     /* GMRES restart length, default 30                         */
   int32_t max_iters;   /* total Krylov iterations (per refinement pass), 3000    */
   int32_t precond;     /* 0 none, 1 point Jacobi (default), 2 node-block Jacobi   */
@@ -345,6 +345,56 @@ int ufem_ns_enable_timing(ufem_ns_handle* h, int32_t enable);
 int ufem_ns_get_timings(ufem_ns_handle* h, ufem_ns_timings* t);
 
 void ufem_ns_destroy(ufem_ns_handle* h);
+
+/* ---------------------------------------------------------------------------
+ * Semi-implicit (pressure-correction) scheme: NavierStokesSemiImplicit
+ * (plugins/UFEM/src/UFEM/ns_semi_implicit/implementation/NavierStokesSemiImplicit.cpp).
+ * Two systems over the node graph -- velocity (dim equations per node, matrix
+ * T + theta dt M reassembled every step, MatrixAssembly.hpp:52-149) and pressure
+ * (one equation, theta (tau_ps + dt) grad N^T grad N assembled once,
+ * PressureSystem.cpp:110-140) -- and nb_iterations predictor/corrector passes
+ * per step (InnerLoop::execute, NavierStokesSemiImplicit.cpp:104-191).  Element
+ * expressions in FP64 (opts->precision is ignored); both systems are solved by
+ * Jacobi-preconditioned CG unless ufem_nssi_set_krylov says otherwise.
+ * Fields use the coupled handle's layouts (up N x (dim+1), lin N x 4 dim, nu N,
+ * force N x dim or NULL: enable_body_force off). */
+typedef struct ufem_nssi_handle ufem_nssi_handle;
+/* NavierStokesSemiImplicit constructor + regions (on_regions_set, :418-497);
+ * nb_iterations is the "nb_iterations" option (default 2); periodic links as in
+ * ufem_ns_create_periodic (nlinks 0: none). */
+int ufem_nssi_create(const ufem_mesh* mesh, const ufem_ns_options* opts, int32_t nb_iterations,
+                     const uint32_t* slaves, const uint32_t* masters, int64_t nlinks, ufem_nssi_handle** out);
+/* Krylov options of the velocity and pressure solves (SolveUSystem /
+ * SolvePSystem, :99-100); NULL keeps the current one. */
+int ufem_nssi_set_krylov(ufem_nssi_handle* h, const ufem_krylov_opts* velocity, const ufem_krylov_opts* pressure);
+int ufem_nssi_set_state(ufem_nssi_handle* h, const double* up, const double* lin, const double* nu,
+                        const double* force);
+int ufem_nssi_get_state(ufem_nssi_handle* h, double* up, double* lin);
+/* VelocityLSS.BC / PressureLSS.BC constant conditions, in call order. */
+int ufem_nssi_add_velocity_dirichlet(ufem_nssi_handle* h, const uint32_t* nodes, int64_t n, int32_t comp,
+                                     const double* values);
+int ufem_nssi_add_pressure_dirichlet(ufem_nssi_handle* h, const uint32_t* nodes, int64_t n, const double* values);
+int ufem_nssi_clear_dirichlet(ufem_nssi_handle* h);
+/* The solver's initial conditions (trigger_initial_conditions, :400-455):
+ * nu_eff into the element records, with reset_history u_adv = u1 = u2 = u3 = u,
+ * the pressure matrix (tau from the current u) and the lumped velocity mass. */
+int ufem_nssi_initialize(ufem_nssi_handle* h, int32_t reset_history, void* stream);
+/* nsteps time steps: LinearizeU, velocity assembly, SetSolution, InnerLoop,
+ * Update (:329-375).  Statuses fold all solves of the call (iterations summed,
+ * worst status, largest residual); may be NULL. */
+int ufem_nssi_step(ufem_nssi_handle* h, int32_t nsteps, ufem_krylov_status* velocity, ufem_krylov_status* pressure,
+                   void* stream);
+int ufem_nssi_get_time(const ufem_nssi_handle* h, double* t);
+int ufem_nssi_sizes(const ufem_nssi_handle* h, int64_t* velocity_nnz, int64_t* pressure_nnz);
+/* Inspection (no counterpart; parity tests): host copies of one system
+ * (which 0: velocity, 1: pressure; any pointer may be NULL), the velocity
+ * matrix of the current state without conditions, the lumped-mass reciprocal. */
+int ufem_nssi_get_system(ufem_nssi_handle* h, int32_t which, int64_t* rowptr, int32_t* colidx, double* vals,
+                         double* rhs, double* sol);
+int ufem_nssi_assemble_velocity_matrix(ufem_nssi_handle* h, void* stream);
+int ufem_nssi_get_lumped_inverse(ufem_nssi_handle* h, double* minv);
+int64_t ufem_nssi_device_bytes(const ufem_nssi_handle* h);
+void ufem_nssi_destroy(ufem_nssi_handle* h);
 
 #ifdef __cplusplus
 }

@@ -65,6 +65,19 @@ _SIG = {
     "orc_time_assembly": (C.c_double, [C.c_void_p, C.c_int, C.c_int]),
     "orc_element": (None, [C.c_void_p, C.c_int64, _D, _D, _D]),
     "orc_tau": (None, [C.c_int, C.c_int, _D, _D, C.c_double, C.c_double, C.c_double, C.c_double, _D]),
+    "orc_semi_create": (C.c_void_p, [C.c_int, C.c_int64, C.c_int64, _D, _U32, C.POINTER(OrcOptions), C.c_int, _U32,
+                                     _U32, C.c_int64]),
+    "orc_semi_destroy": (None, [C.c_void_p]),
+    "orc_semi_set_state": (None, [C.c_void_p, _D, _D, _D, _D]),
+    "orc_semi_get_state": (None, [C.c_void_p, _D, _D]),
+    "orc_semi_add_dirichlet": (None, [C.c_void_p, C.c_int, _U32, C.c_int64, C.c_int, _D]),
+    "orc_semi_initialize": (None, [C.c_void_p, C.c_int]),
+    "orc_semi_step": (C.c_int, [C.c_void_p, C.c_int, C.c_double, _I32, _D]),
+    "orc_semi_velocity_matrix": (None, [C.c_void_p]),
+    "orc_semi_rhs": (None, [C.c_void_p, C.c_int, _D, _D, _D, _D, _D, _D]),
+    "orc_semi_nnz": (C.c_int64, [C.c_void_p, C.c_int]),
+    "orc_semi_get_system": (None, [C.c_void_p, C.c_int, _D, _D, _D]),
+    "orc_semi_lumped_inverse": (None, [C.c_void_p, _D]),
 }
 
 _lib = None
@@ -298,6 +311,105 @@ class Oracle:
     def close(self):
         if self._h:
             lib().orc_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class SemiImplicit:
+    """The semi-implicit scheme (NavierStokesSemiImplicit) restated in FP64."""
+
+    def __init__(self, coords, conn, opts: OrcOptions, nb_iterations: int = 2, periodic_links=None):
+        self._lib = lib()
+        self.coords = np.ascontiguousarray(coords, np.float64)
+        self.conn = np.ascontiguousarray(conn, np.uint32)
+        self.dim = self.coords.shape[1]
+        self.N = self.coords.shape[0]
+        sl = ms = None
+        n = 0
+        if periodic_links is not None:
+            sl = np.ascontiguousarray(periodic_links[0], np.uint32)
+            ms = np.ascontiguousarray(periodic_links[1], np.uint32)
+            n = len(sl)
+        self._keep = (sl, ms)
+        self._h = self._lib.orc_semi_create(self.dim, self.N, self.conn.shape[0], _d(self.coords),
+                                            self.conn.ctypes.data_as(_U32), C.byref(opts), int(nb_iterations),
+                                            None if sl is None else sl.ctypes.data_as(_U32),
+                                            None if ms is None else ms.ctypes.data_as(_U32), n)
+        if not self._h:
+            raise RuntimeError("orc_semi_create failed")
+
+    def initial_conditions(self, u, nu, p=None, force=None):
+        up = np.zeros((self.N, self.dim + 1))
+        up[:, : self.dim] = u
+        if p is not None:
+            up[:, self.dim] = p
+        lin = np.tile(np.asarray(u, np.float64), (1, 4))
+        nuv = np.ascontiguousarray(np.broadcast_to(np.asarray(nu, np.float64), (self.N,)))
+        self.set_state(up, lin, nuv, force)
+        self._lib.orc_semi_initialize(self._h, 1)
+
+    def set_state(self, up, lin, nu, force=None):
+        up, lin, nu = (np.ascontiguousarray(a, np.float64) for a in (up, lin, nu))
+        f = None if force is None else np.ascontiguousarray(force, np.float64)
+        self._lib.orc_semi_set_state(self._h, _d(up), _d(lin), _d(nu), None if f is None else _d(f))
+
+    def initialize(self, reset_history=True):
+        self._lib.orc_semi_initialize(self._h, 1 if reset_history else 0)
+
+    def state(self):
+        up = np.empty((self.N, self.dim + 1))
+        lin = np.empty((self.N, 4 * self.dim))
+        self._lib.orc_semi_get_state(self._h, _d(up), _d(lin))
+        return up, lin
+
+    def add_velocity_dirichlet(self, nodes, comp, values):
+        nodes = np.ascontiguousarray(nodes, np.uint32)
+        values = np.ascontiguousarray(np.broadcast_to(np.asarray(values, np.float64), nodes.shape))
+        self._lib.orc_semi_add_dirichlet(self._h, 0, nodes.ctypes.data_as(_U32), len(nodes), int(comp), _d(values))
+
+    def add_pressure_dirichlet(self, nodes, values):
+        nodes = np.ascontiguousarray(nodes, np.uint32)
+        values = np.ascontiguousarray(np.broadcast_to(np.asarray(values, np.float64), nodes.shape))
+        self._lib.orc_semi_add_dirichlet(self._h, 1, nodes.ctypes.data_as(_U32), len(nodes), 0, _d(values))
+
+    def step(self, nsteps=1, tol=1e-13):
+        iters = np.zeros(2, np.int32)
+        worst = C.c_double()
+        rc = self._lib.orc_semi_step(self._h, int(nsteps), tol, iters.ctypes.data_as(_I32), C.byref(worst))
+        return rc, (int(iters[0]), int(iters[1])), worst.value
+
+    def velocity_matrix(self):
+        self._lib.orc_semi_velocity_matrix(self._h)
+        return self.system("velocity")[0]
+
+    def rhs(self, kind: str, uvec, avec, pvec, dpsum, da, dp):
+        """Element right-hand side `kind` ("velocity", "pressure", "aup") on the given vectors."""
+        arrs = [np.ascontiguousarray(a, np.float64).ravel() for a in (uvec, avec, pvec, dpsum, da, dp)]
+        k = {"velocity": 0, "pressure": 1, "aup": 2}[kind]
+        self._lib.orc_semi_rhs(self._h, k, *[_d(a) for a in arrs])
+        return self.system("pressure" if k == 1 else "velocity")[1]
+
+    def system(self, which: str):
+        w = {"velocity": 0, "pressure": 1}[which]
+        nnz = self._lib.orc_semi_nnz(self._h, w)
+        nrows = self.N * (self.dim if w == 0 else 1)
+        v, r, s = np.empty(nnz), np.empty(nrows), np.empty(nrows)
+        self._lib.orc_semi_get_system(self._h, w, _d(v), _d(r), _d(s))
+        return v, r, s
+
+    def lumped_inverse(self):
+        out = np.empty((self.N, self.dim))
+        self._lib.orc_semi_lumped_inverse(self._h, _d(out))
+        return out
+
+    def close(self):
+        if getattr(self, "_h", None):
+            self._lib.orc_semi_destroy(self._h)
             self._h = None
 
     def __del__(self):

@@ -1294,3 +1294,618 @@ void orc_tau(int dim, int type, const double* X, const double* uc, double nu, do
 }
 
 }  // extern "C"
+
+// ===========================================================================
+// Semi-implicit (pressure-correction) scheme: NavierStokesSemiImplicit
+// (plugins/UFEM/src/UFEM/ns_semi_implicit/).  Element expressions from
+// MatrixAssembly.hpp, the pressure matrix from PressureSystem.cpp:110-140, the
+// step from implementation/NavierStokesSemiImplicit.cpp:96-198 and :329-375.
+// Triangles and tetrahedra take IntegralOrder 1 (MatrixAssembly.hpp:28-46):
+// the operators at the centroid, the mass terms with the order-2 rule.  Each
+// element vector/matrix is formed completely, then added to the global rows in
+// element order (as Proto's ElementLooper + BlockAccumulator do).  Linked
+// (periodic) nodes keep identity rows with a zero right-hand side and receive
+// their master's values after every solve.
+// ===========================================================================
+namespace {
+
+struct Semi {
+  Oracle F;  // mesh, options, fields: up N x (D+1), lin N x 4D, nu, force; periodic map
+  Oracle U;  // velocity LSS (neq = D)
+  Oracle P;  // pressure LSS (neq = 1)
+  int nb_iterations = 2;
+  double tol = 1e-13;
+  std::vector<double> uvec, avec, pvec, dpsum, minv;
+  int iters_u = 0, iters_p = 0;
+  double worst_relres = 0.0;
+};
+
+void make_lss(const Oracle& F, int neq, Oracle& S) {
+  S.dim = F.dim;
+  S.nn = F.nn;
+  S.neq = neq;
+  S.N = F.N;
+  S.E = F.E;
+  S.coords = F.coords;
+  S.conn = F.conn;
+  S.o = F.o;
+  S.p2m = F.p2m;
+  build_graph(S);
+}
+
+template <int D>
+constexpr double w1_ref() { return D == 2 ? 0.5 : 1.0 / 6.0; }  // GaussMappedCoords<1>: one point
+
+template <int D>
+struct SemiElem {
+  static constexpr int n = D + 1;
+  uint32_t node[n];
+  double X[n][D], G[D][n], det;
+  double tps, tsu, tbu;
+  double nuc;   // nu_eff at the centroid
+  double uc[D]; // tau velocity at the centroid
+};
+
+// Geometry and ComputeTauImpl (SUPG.hpp:140-219) on u_adv (`adv`) or on the
+// velocity solution u.
+template <int D>
+void semi_elem(const Semi& M, int64_t e, bool adv, SemiElem<D>& s) {
+  constexpr int n = D + 1;
+  const Oracle& F = M.F;
+  double U[n][D], NU[n];
+  for (int b = 0; b < n; ++b) {
+    const uint32_t node = F.conn[e * n + b];
+    s.node[b] = node;
+    for (int k = 0; k < D; ++k) {
+      s.X[b][k] = F.coords[(size_t)node * D + k];
+      U[b][k] = adv ? F.lin[(size_t)node * 4 * D + k] : F.up[(size_t)node * (D + 1) + k];
+    }
+    NU[b] = F.nu[node];
+  }
+  double J[D][D], Ji[D][D];
+  jacobian<D>(s.X, J);
+  inverse_det<D>(J, Ji, s.det);
+  gradient<D>(Ji, s.G);
+  double xi[D], Nc[n];
+  centroid<D>(xi);
+  shape_values<D>(xi, Nc);
+  double nsum = 0.0;
+  s.nuc = 0.0;
+  for (int b = 0; b < n; ++b) {
+    nsum += NU[b];
+    s.nuc += Nc[b] * NU[b];
+  }
+  for (int k = 0; k < D; ++k) {
+    double t = 0.0;
+    for (int b = 0; b < n; ++b) t += Nc[b] * U[b][k];
+    s.uc[k] = t;
+  }
+  const TauParams tp{F.o.supg_type, F.o.c1, F.o.c2, F.o.alpha_ps, F.o.alpha_su, F.o.alpha_bu, F.o.u_ref};
+  compute_tau<D>(tp, s.X, s.uc, std::fabs(nsum / n), F.o.dt, s.tps, s.tsu, s.tbu);
+}
+
+template <int D>
+double gdot(const SemiElem<D>& s, int a, int b) {
+  double t = 0.0;
+  for (int k = 0; k < D; ++k) t += s.G[k][a] * s.G[k][b];
+  return t;
+}
+
+// Linked nodes: identity rows, zero right-hand side.
+void semi_identity_rows(Oracle& S) {
+  for (int64_t i = 0; i < S.N; ++i) {
+    if (S.row_of((uint32_t)i) == (uint32_t)i) continue;
+    for (int c = 0; c < S.neq; ++c) {
+      const int64_t r = i * S.neq + c;
+      for (int64_t p = S.rowptr[r]; p < S.rowptr[r + 1]; ++p) S.vals[p] = 0.0;
+      S.vals[csr_pos(S, i, c, i, c)] = 1.0;
+      S.rhs[r] = 0.0;
+    }
+  }
+}
+
+void semi_sync(const Oracle& S, std::vector<double>& v, int neq) {
+  for (int64_t i = 0; i < S.N; ++i) {
+    const uint32_t m = S.row_of((uint32_t)i);
+    if (m == (uint32_t)i) continue;
+    for (int c = 0; c < neq; ++c) v[i * neq + c] = v[(int64_t)m * neq + c];
+  }
+}
+
+// VelocityAssembly (MatrixAssembly.hpp:52-149) + system_matrix += T + theta dt M
+// (:428-432), after ZeroLSS of the matrix and the RHS.
+template <int D>
+void semi_velocity_matrix(Semi& M) {
+  constexpr int n = D + 1, nd = n * D;
+  Oracle& U = M.U;
+  std::fill(U.vals.begin(), U.vals.end(), 0.0);
+  std::fill(U.rhs.begin(), U.rhs.end(), 0.0);
+  const double thdt = M.F.o.theta * M.F.o.dt;
+  for (int64_t e = 0; e < M.F.E; ++e) {
+    SemiElem<D> s;
+    semi_elem<D>(M, e, true, s);
+    double T[nd][nd] = {}, Mm[nd][nd] = {};
+    for (int q = 0; q < Gauss2<D>::np; ++q) {  // mass, always order 2
+      double xi[D], N[n];
+      Gauss2<D>::point(q, xi);
+      shape_values<D>(xi, N);
+      const double w = Gauss2<D>::weight() * s.det;
+      for (int a = 0; a < n; ++a)
+        for (int b = 0; b < n; ++b) {
+          const double v = (w * N[a]) * N[b];
+          for (int i = 0; i < D; ++i) T[i * n + a][i * n + b] += v;
+        }
+    }
+    const double w = w1_ref<D>() * s.det;
+    const double bulk = w * s.tbu;
+    for (int i = 0; i < D; ++i)  // laplacian + diagonal bulk blocks, centroid
+      for (int a = 0; a < n; ++a)
+        for (int b = 0; b < n; ++b)
+          Mm[i * n + a][i * n + b] += (w * s.nuc) * gdot<D>(s, a, b) + (bulk * s.G[i][a]) * s.G[i][b];
+    for (int i = 0; i < D; ++i)  // off-diagonal bulk blocks
+      for (int j = i + 1; j < D; ++j)
+        for (int a = 0; a < n; ++a)
+          for (int b = 0; b < n; ++b) {
+            const double v = (bulk * s.G[i][a]) * s.G[j][b];
+            Mm[i * n + a][j * n + b] += v;
+            Mm[j * n + b][i * n + a] += v;
+          }
+    for (int a = 0; a < n; ++a) {
+      const int64_t ra = U.row_of(s.node[a]);
+      for (int i = 0; i < D; ++i)
+        for (int b = 0; b < n; ++b) {
+          const int64_t base = csr_pos(U, ra, i, U.row_of(s.node[b]), 0);
+          for (int j = 0; j < D; ++j) U.vals[base + j] += T[i * n + a][j * n + b] + thdt * Mm[i * n + a][j * n + b];
+        }
+    }
+  }
+  semi_identity_rows(U);
+}
+
+// PressureSystemAssembly::assemble_pp (PressureSystem.cpp:128-140), tau from u.
+template <int D>
+void semi_pressure_matrix(Semi& M) {
+  constexpr int n = D + 1;
+  Oracle& P = M.P;
+  std::fill(P.vals.begin(), P.vals.end(), 0.0);
+  std::fill(P.rhs.begin(), P.rhs.end(), 0.0);
+  std::fill(P.sol.begin(), P.sol.end(), 0.0);
+  for (int64_t e = 0; e < M.F.E; ++e) {
+    SemiElem<D> s;
+    semi_elem<D>(M, e, false, s);
+    const double coef = M.F.o.theta * (s.tps + M.F.o.dt);
+    for (int a = 0; a < n; ++a)
+      for (int b = 0; b < n; ++b) {
+        double A = 0.0;
+        for (int q = 0; q < Gauss2<D>::np; ++q) A += (Gauss2<D>::weight() * s.det) * gdot<D>(s, a, b);
+        P.vals[csr_pos(P, P.row_of(s.node[a]), 0, P.row_of(s.node[b]), 0)] += coef * A;
+      }
+  }
+  semi_identity_rows(P);
+}
+
+// Lumped mass (MatrixAssembly.hpp:411-420) and its reciprocal
+// (NavierStokesSemiImplicit.cpp:238-247).
+template <int D>
+void semi_lumped_mass(Semi& M) {
+  constexpr int n = D + 1;
+  std::vector<double> diag(M.F.N * D, 0.0);
+  for (int64_t e = 0; e < M.F.E; ++e) {
+    SemiElem<D> s;
+    semi_elem<D>(M, e, true, s);
+    double Me[n][n] = {};
+    for (int q = 0; q < Gauss2<D>::np; ++q) {
+      double xi[D], N[n];
+      Gauss2<D>::point(q, xi);
+      shape_values<D>(xi, N);
+      const double w = Gauss2<D>::weight() * s.det;
+      for (int a = 0; a < n; ++a)
+        for (int b = 0; b < n; ++b) Me[a][b] += (w * N[a]) * N[b];
+    }
+    for (int a = 0; a < n; ++a) {
+      double rs = 0.0;
+      for (int b = 0; b < n; ++b) rs += Me[a][b];
+      for (int i = 0; i < D; ++i) diag[(size_t)M.U.row_of(s.node[a]) * D + i] += rs;
+    }
+  }
+  M.minv.assign(M.F.N * D, 0.0);
+  for (size_t k = 0; k < diag.size(); ++k) M.minv[k] = 1.0 / diag[k];
+  semi_sync(M.U, M.minv, D);
+}
+
+// VelocityRHS (MatrixAssembly.hpp:212-360) into U.rhs (zeroed first).
+template <int D>
+void semi_velocity_rhs(Semi& M) {
+  constexpr int n = D + 1;
+  Oracle& U = M.U;
+  std::fill(U.rhs.begin(), U.rhs.end(), 0.0);
+  const double theta = M.F.o.theta, dt = M.F.o.dt;
+  const double dtl = dt * (1. - theta), omt = 1. - theta;
+  for (int64_t e = 0; e < M.F.E; ++e) {
+    SemiElem<D> s;
+    semi_elem<D>(M, e, true, s);
+    double Ua[n][D], AV[n][D], DAU[n][D], PP[n], Fo[n][D];
+    for (int b = 0; b < n; ++b) {
+      const uint32_t node = s.node[b];
+      for (int k = 0; k < D; ++k) {
+        Ua[b][k] = M.F.lin[(size_t)node * 4 * D + k];
+        AV[b][k] = M.avec[(size_t)node * D + k];
+        DAU[b][k] = dtl * AV[b][k] - M.uvec[(size_t)node * D + k];
+        Fo[b][k] = M.F.force.empty() ? 0.0 : M.F.force[(size_t)node * D + k];
+      }
+      PP[b] = omt * M.dpsum[node] - M.pvec[node];
+    }
+    double res[D][n] = {};
+    for (int q = 0; q < Gauss2<D>::np; ++q) {  // mass part, order 2
+      double xi[D], N[n];
+      Gauss2<D>::point(q, xi);
+      shape_values<D>(xi, N);
+      const double w = Gauss2<D>::weight() * s.det;
+      double uq[D], adv[n], npa[n];
+      for (int k = 0; k < D; ++k) {
+        uq[k] = 0.0;
+        for (int b = 0; b < n; ++b) uq[k] += N[b] * Ua[b][k];
+      }
+      for (int b = 0; b < n; ++b) {
+        adv[b] = 0.0;
+        for (int k = 0; k < D; ++k) adv[b] += uq[k] * s.G[k][b];
+        npa[b] = s.tsu * adv[b] + N[b];
+      }
+      double f = 0.0;
+      for (int i = 0; i < D; ++i)
+        for (int b = 0; b < n; ++b) f += s.G[i][b] * DAU[b][i];
+      f *= w;
+      const double fs = 0.5 * f;
+      for (int i = 0; i < D; ++i) {
+        double c = 0.0, ee = 0.0;
+        for (int b = 0; b < n; ++b) {
+          c += N[b] * AV[b][i];
+          ee += adv[b] * DAU[b][i];
+        }
+        c = -w * c;
+        ee = w * ee;
+        for (int a = 0; a < n; ++a) res[i][a] += npa[a] * (c + ee + fs * uq[i]);
+      }
+    }
+    {  // operator part, centroid
+      double xi[D], N[n];
+      centroid<D>(xi);
+      shape_values<D>(xi, N);
+      const double w = w1_ref<D>() * s.det;
+      const double wv = w * s.nuc, tw = w * s.tsu;
+      double adv[n];
+      for (int b = 0; b < n; ++b) {
+        adv[b] = 0.0;
+        for (int k = 0; k < D; ++k) adv[b] += s.uc[k] * s.G[k][b];
+      }
+      double bb = 0.0;
+      for (int b = 0; b < n; ++b) bb += N[b] * PP[b];
+      bb = -w * bb;
+      double f = 0.0;
+      for (int i = 0; i < D; ++i)
+        for (int b = 0; b < n; ++b) f += s.G[i][b] * DAU[b][i];
+      f *= w;
+      const double fb = s.tbu * f;
+      for (int i = 0; i < D; ++i) {
+        double av = 0.0;
+        for (int b = 0; b < n; ++b) av += s.G[i][b] * PP[b];
+        av = tw * av;
+        double d[D];
+        for (int k = 0; k < D; ++k) {
+          double t = 0.0;
+          for (int b = 0; b < n; ++b) t += s.G[k][b] * DAU[b][i];
+          d[k] = wv * t;
+        }
+        for (int a = 0; a < n; ++a) {
+          double visc = 0.0;
+          for (int k = 0; k < D; ++k) visc += s.G[k][a] * d[k];
+          res[i][a] += adv[a] * av + s.G[i][a] * (bb + fb) + visc;
+        }
+      }
+    }
+    if (!M.F.force.empty()) {  // body force, order 2 (MatrixAssembly.hpp:344-360)
+      for (int q = 0; q < Gauss2<D>::np; ++q) {
+        double xi[D], N[n];
+        Gauss2<D>::point(q, xi);
+        shape_values<D>(xi, N);
+        const double w = Gauss2<D>::weight() * s.det;
+        for (int i = 0; i < D; ++i) {
+          double g = 0.0;
+          for (int b = 0; b < n; ++b) g += N[b] * Fo[b][i];
+          for (int a = 0; a < n; ++a) res[i][a] += N[a] * g * w;
+        }
+      }
+    }
+    for (int a = 0; a < n; ++a)
+      for (int i = 0; i < D; ++i) U.rhs[(size_t)U.row_of(s.node[a]) * D + i] += res[i][a];
+  }
+}
+
+// PressureRHS (MatrixAssembly.hpp:153-210) into P.rhs (zeroed first); tau_ps from u.
+template <int D>
+void semi_pressure_rhs(Semi& M) {
+  constexpr int n = D + 1;
+  Oracle& P = M.P;
+  std::fill(P.rhs.begin(), P.rhs.end(), 0.0);
+  const double dt = M.F.o.dt;
+  for (int64_t e = 0; e < M.F.E; ++e) {
+    SemiElem<D> s;
+    semi_elem<D>(M, e, false, s);
+    double Ua[n][D], UP[n][D], APD[n][D], PV[n];
+    for (int b = 0; b < n; ++b) {
+      const uint32_t node = s.node[b];
+      for (int k = 0; k < D; ++k) {
+        const size_t r = (size_t)node * D + k;
+        Ua[b][k] = M.F.lin[(size_t)node * 4 * D + k];
+        UP[b][k] = M.uvec[r] + dt * M.U.sol[r];
+        APD[b][k] = M.avec[r] + M.U.sol[r];
+      }
+      PV[b] = M.pvec[node];
+    }
+    double xi[D], N[n];
+    centroid<D>(xi);
+    shape_values<D>(xi, N);
+    const double w = w1_ref<D>() * s.det, tw = w * s.tps;
+    double adv[n];
+    double ua[D];
+    for (int k = 0; k < D; ++k) {
+      ua[k] = 0.0;
+      for (int b = 0; b < n; ++b) ua[k] += N[b] * Ua[b][k];
+    }
+    for (int b = 0; b < n; ++b) {
+      adv[b] = 0.0;
+      for (int k = 0; k < D; ++k) adv[b] += (s.tps * ua[k]) * s.G[k][b];
+    }
+    double res[n] = {};
+    for (int i = 0; i < D; ++i) {
+      double av = 0.0, bv = 0.0, cv = 0.0;
+      for (int b = 0; b < n; ++b) {
+        av += s.G[i][b] * UP[b][i];
+        bv += adv[b] * UP[b][i];
+        cv += N[b] * APD[b][i];
+      }
+      av *= w;
+      bv *= w;
+      cv *= tw;
+      for (int a = 0; a < n; ++a) res[a] -= av * (N[a] + adv[a] * 0.5) + (bv + cv) * s.G[i][a];
+    }
+    for (int a = 0; a < n; ++a) {
+      double t = 0.0;
+      for (int b = 0; b < n; ++b) t += (tw * gdot<D>(s, a, b)) * PV[b];
+      res[a] -= t;
+    }
+    for (int a = 0; a < n; ++a) P.rhs[P.row_of(s.node[a])] += res[a];
+  }
+}
+
+// ApplyAup (MatrixAssembly.hpp:364-404) into U.rhs (zeroed first); tau_su from u_adv.
+template <int D>
+void semi_apply_aup(Semi& M) {
+  constexpr int n = D + 1;
+  Oracle& U = M.U;
+  std::fill(U.rhs.begin(), U.rhs.end(), 0.0);
+  for (int64_t e = 0; e < M.F.E; ++e) {
+    SemiElem<D> s;
+    semi_elem<D>(M, e, true, s);
+    double dp[n];
+    for (int b = 0; b < n; ++b) dp[b] = M.P.sol[s.node[b]];
+    double xi[D], N[n];
+    centroid<D>(xi);
+    shape_values<D>(xi, N);
+    const double w = M.F.o.theta * w1_ref<D>() * s.det;
+    double adv[n];
+    for (int b = 0; b < n; ++b) {
+      double t = 0.0;
+      for (int k = 0; k < D; ++k) t += s.uc[k] * s.G[k][b];
+      adv[b] = (w * s.tsu) * t;
+    }
+    double bb = 0.0;
+    for (int b = 0; b < n; ++b) bb += N[b] * dp[b];
+    bb = -w * bb;
+    for (int i = 0; i < D; ++i) {
+      double av = 0.0;
+      for (int b = 0; b < n; ++b) av += s.G[i][b] * dp[b];
+      for (int a = 0; a < n; ++a) U.rhs[(size_t)U.row_of(s.node[a]) * D + i] += av * adv[a] + bb * s.G[i][a];
+    }
+  }
+}
+
+// BoundaryConditions of one system: symmetric Dirichlet in list order with
+// value - field (Proto/DirichletBC.hpp:34-39); `field(node, comp)` reads u or p.
+template <typename FieldT>
+void semi_apply_bcs(Oracle& S, FieldT field) {
+  for (const BC& bc : S.bcs) {
+    const uint32_t row = S.row_of(bc.node);
+    symmetric_dirichlet(S, row, bc.comp, bc.value - field(row, bc.comp));
+  }
+}
+
+void semi_zero_bc_rows(const Oracle& S, std::vector<double>& v) {
+  for (const BC& bc : S.bcs) v[(size_t)S.row_of(bc.node) * S.neq + bc.comp] = 0.0;
+}
+
+int semi_solve(Semi& M, Oracle& S, int& iters) {
+  const int rc = gmres_ilu0(S, M.tol, 20000, 200);
+  iters += S.last_iters;
+  M.worst_relres = std::max(M.worst_relres, S.last_relres);
+  return rc;
+}
+
+// One time step (NavierStokesSemiImplicit.cpp:329-375 with InnerLoop::execute :104-191).
+template <int D>
+int semi_step(Semi& M) {
+  Oracle& F = M.F;
+  const int64_t N = F.N;
+  const double dt = F.o.dt;
+  int rc = 0;
+  linearize(F);
+  semi_velocity_matrix<D>(M);
+  M.uvec.assign(N * D, 0.0);
+  M.avec.assign(N * D, 0.0);
+  M.pvec.assign(N, 0.0);
+  M.dpsum.assign(N, 0.0);
+  for (int64_t i = 0; i < N; ++i) {
+    for (int k = 0; k < D; ++k) M.uvec[i * D + k] = F.up[i * (D + 1) + k];
+    M.pvec[i] = F.up[i * (D + 1) + D];
+  }
+  auto ufield = [&](uint32_t node, int comp) { return F.up[(size_t)node * (D + 1) + comp]; };
+  auto pfield = [&](uint32_t node, int) { return F.up[(size_t)node * (D + 1) + D]; };
+  for (int it = 0; it < M.nb_iterations; ++it) {
+    semi_velocity_rhs<D>(M);
+    if (it == 0) {
+      for (double& r : M.U.rhs) r *= dt;
+      semi_apply_bcs(M.U, ufield);
+      for (double& r : M.U.rhs) r *= 1. / dt;
+    } else {
+      semi_zero_bc_rows(M.U, M.U.rhs);
+    }
+    std::fill(M.U.sol.begin(), M.U.sol.end(), 0.0);
+    rc |= semi_solve(M, M.U, M.iters_u);
+    semi_sync(M.U, M.U.sol, D);
+    semi_pressure_rhs<D>(M);
+    std::fill(M.P.sol.begin(), M.P.sol.end(), 0.0);
+    if (it == 0) semi_apply_bcs(M.P, pfield);
+    else semi_zero_bc_rows(M.P, M.P.rhs);
+    rc |= semi_solve(M, M.P, M.iters_p);
+    semi_sync(M.P, M.P.sol, 1);
+    semi_apply_aup<D>(M);
+    semi_zero_bc_rows(M.U, M.U.rhs);
+    for (int64_t r = 0; r < N * D; ++r) M.U.sol[r] = M.U.sol[r] - M.minv[r] * M.U.rhs[r];
+    semi_sync(M.U, M.U.sol, D);
+    for (int64_t i = 0; i < N; ++i) {
+      for (int k = 0; k < D; ++k) {
+        const int64_t r = i * D + k;
+        M.avec[r] = M.avec[r] + M.U.sol[r];
+        M.uvec[r] = M.uvec[r] + dt * M.U.sol[r];
+      }
+      M.pvec[i] = M.pvec[i] + M.P.sol[i];
+      M.dpsum[i] = M.dpsum[i] + M.P.sol[i];
+    }
+  }
+  for (int64_t i = 0; i < N; ++i) {  // Update
+    double* L = &F.lin[i * 4 * D];
+    for (int k = 0; k < D; ++k) {
+      L[3 * D + k] = L[2 * D + k];
+      L[2 * D + k] = L[D + k];
+      L[D + k] = F.up[i * (D + 1) + k];
+      F.up[i * (D + 1) + k] = M.uvec[i * D + k];
+    }
+    F.up[i * (D + 1) + D] = M.pvec[i];
+  }
+  return rc;
+}
+
+}  // namespace
+
+extern "C" {
+
+void* orc_semi_create(int dim, int64_t nb_nodes, int64_t nb_elems, const double* coords, const uint32_t* conn,
+                      const orc_options* opts, int nb_iterations, const uint32_t* slaves, const uint32_t* masters,
+                      int64_t nlinks) {
+  Oracle* F = static_cast<Oracle*>(
+      orc_create_periodic(dim, nb_nodes, nb_elems, coords, conn, opts, slaves, masters, nlinks));
+  if (!F) return nullptr;
+  Semi* M = new Semi();
+  M->F = std::move(*F);
+  delete F;
+  M->nb_iterations = nb_iterations;
+  make_lss(M->F, dim, M->U);
+  make_lss(M->F, 1, M->P);
+  return M;
+}
+
+void orc_semi_destroy(void* h) { delete static_cast<Semi*>(h); }
+
+void orc_semi_set_state(void* h, const double* up, const double* lin, const double* nu, const double* force) {
+  orc_set_state(&static_cast<Semi*>(h)->F, up, lin, nu, force);
+}
+
+void orc_semi_get_state(void* h, double* up, double* lin) { orc_get_state(&static_cast<Semi*>(h)->F, up, lin); }
+
+void orc_semi_add_dirichlet(void* h, int which, const uint32_t* nodes, int64_t n, int comp, const double* values) {
+  Semi* M = static_cast<Semi*>(h);
+  Oracle& S = which == 0 ? M->U : M->P;
+  for (int64_t i = 0; i < n; ++i) S.bcs.push_back(BC{nodes[i], comp, values[i]});
+}
+
+// Initial conditions (NavierStokesSemiImplicit.cpp:400-455): with reset,
+// u_adv = u1 = u2 = u3 = u; the pressure matrix and the lumped mass.
+void orc_semi_initialize(void* h, int reset_history) {
+  Semi* M = static_cast<Semi*>(h);
+  Oracle& F = M->F;
+  const int D = F.dim;
+  if (reset_history)
+    for (int64_t i = 0; i < F.N; ++i)
+      for (int j = 0; j < 4; ++j)
+        for (int k = 0; k < D; ++k) F.lin[i * 4 * D + j * D + k] = F.up[i * (D + 1) + k];
+  if (D == 2) {
+    semi_pressure_matrix<2>(*M);
+    semi_lumped_mass<2>(*M);
+  } else {
+    semi_pressure_matrix<3>(*M);
+    semi_lumped_mass<3>(*M);
+  }
+}
+
+// nsteps steps; returns 0 when every solve converged.  iters: (velocity, pressure) totals.
+int orc_semi_step(void* h, int nsteps, double tol, int* iters, double* worst_relres) {
+  Semi* M = static_cast<Semi*>(h);
+  M->tol = tol;
+  M->iters_u = M->iters_p = 0;
+  M->worst_relres = 0.0;
+  int rc = 0;
+  for (int k = 0; k < nsteps; ++k) rc |= (M->F.dim == 2 ? semi_step<2>(*M) : semi_step<3>(*M));
+  if (iters) {
+    iters[0] = M->iters_u;
+    iters[1] = M->iters_p;
+  }
+  if (worst_relres) *worst_relres = M->worst_relres;
+  return rc;
+}
+
+// The velocity matrix of the current state (LinearizeU + VelocityAssembly), no BCs.
+void orc_semi_velocity_matrix(void* h) {
+  Semi* M = static_cast<Semi*>(h);
+  linearize(M->F);
+  if (M->F.dim == 2) semi_velocity_matrix<2>(*M);
+  else semi_velocity_matrix<3>(*M);
+}
+
+// Element right-hand sides on given inner-loop vectors (parity of the vector
+// expressions): kind 0 velocity RHS, 1 pressure RHS (da = delta_a),
+// 2 A_up dp.  Results land in the system's rhs (read with orc_semi_get_system).
+void orc_semi_rhs(void* h, int kind, const double* uvec, const double* avec, const double* pvec, const double* dpsum,
+                  const double* da, const double* dp) {
+  Semi* M = static_cast<Semi*>(h);
+  const int D = M->F.dim;
+  const int64_t N = M->F.N;
+  M->uvec.assign(uvec, uvec + N * D);
+  M->avec.assign(avec, avec + N * D);
+  M->pvec.assign(pvec, pvec + N);
+  M->dpsum.assign(dpsum, dpsum + N);
+  std::copy(da, da + N * D, M->U.sol.begin());
+  std::copy(dp, dp + N, M->P.sol.begin());
+  if (kind == 0) (D == 2) ? semi_velocity_rhs<2>(*M) : semi_velocity_rhs<3>(*M);
+  else if (kind == 1) (D == 2) ? semi_pressure_rhs<2>(*M) : semi_pressure_rhs<3>(*M);
+  else (D == 2) ? semi_apply_aup<2>(*M) : semi_apply_aup<3>(*M);
+}
+
+int64_t orc_semi_nnz(void* h, int which) {
+  Semi* M = static_cast<Semi*>(h);
+  return (int64_t)(which == 0 ? M->U : M->P).vals.size();
+}
+
+void orc_semi_get_system(void* h, int which, double* vals, double* rhs, double* sol) {
+  Semi* M = static_cast<Semi*>(h);
+  const Oracle& S = which == 0 ? M->U : M->P;
+  if (vals) std::copy(S.vals.begin(), S.vals.end(), vals);
+  if (rhs) std::copy(S.rhs.begin(), S.rhs.end(), rhs);
+  if (sol) std::copy(S.sol.begin(), S.sol.end(), sol);
+}
+
+void orc_semi_lumped_inverse(void* h, double* out) {
+  Semi* M = static_cast<Semi*>(h);
+  std::copy(M->minv.begin(), M->minv.end(), out);
+}
+
+}  // extern "C"
