@@ -16,7 +16,7 @@ GPU parity against the oracle (stated tolerances): velocity matrix, pressure
 matrix and lumped inverse within 1e-12 of each row's largest |entry|; three
 time steps of a lid-driven cavity (2D and 3D, the three tau types) within 1e-8
 of the largest field value with both solvers at 1e-12; the channel case within
-1e-7 of the oracle and inside the reference's bounds; two runs bitwise equal.
+1e-7 of the oracle (pressure solves at 1e-10) and inside the reference's bounds; two runs bitwise equal.
 """
 import numpy as np
 import pytest
@@ -217,7 +217,9 @@ def test_laminar_channel_acceptance_gpu():
     c, t, links, walls, center, force = channel_case()
     G, S = _pair(c, t, 2, "metric", theta=0.5, dt=0.5, nb_iterations=2, links=links, alpha_su=0.0)
     with G:
-        G.set_krylov(velocity=dict(tol=1e-12, max_iters=10000), pressure=dict(tol=1e-12, max_iters=10000))
+        # the pressure increments shrink to rounding level as the flow settles:
+        # 1e-10 of their norm is the attainable Jacobi-CG accuracy there
+        G.set_krylov(velocity=dict(tol=1e-12, max_iters=10000), pressure=dict(tol=1e-10, max_iters=20000))
         for X in (G, S):
             setup_channel(X, c, walls, center, force)
         sv, sp = G.step(50)
