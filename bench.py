@@ -73,6 +73,7 @@ def parse():
     ap.add_argument("--serve-budget-gb", type=float, default=60.0, help="HBM budget of the server (GB)")
     ap.add_argument("--serve-reps", type=int, default=3, help="served runs per form (the median is reported)")
     ap.add_argument("--serving-only", action="store_true", help=argparse.SUPPRESS)
+    ap.add_argument("--si-n", type=int, default=32, help="cube side of the semi-implicit comparison")
     return ap.parse_args()
 
 
@@ -443,6 +444,11 @@ def run_ours(args, rank, world, local):
                                 "all_cores": {"value": round(vall, 3), "cores": threads, "seconds": round(tall, 3)}}
         # ---- full time steps: plain FP64 vs mixed precision ---------------------
         line["time_step"] = time_steps(ns, pb, args, stream, sptr)
+        # ---- the semi-implicit scheme, B200 vs the FP64 oracle ------------------
+        try:
+            line["semi_implicit"] = semi_implicit_compare(args.si_n)
+        except Exception as exc:  # reported, not fatal: the assembly metric above stands
+            line["semi_implicit"] = {"error": str(exc)}
     ns.close()
     if rank == 0 and world == 1 and not args.no_extras and args.serve_requests > 0:
         # ---- served steps/s with p50/p99 vs the plain per-request path ----------
@@ -501,6 +507,57 @@ def time_steps(ns, pb, args, stream, sptr):
     out["steps"] = args.time_steps
     ns.set_state(base_up, pb.lin, pb.nu)
     return out
+
+
+def semi_implicit_compare(n: int, steps: int = 3) -> dict:
+    """The semi-implicit scheme (NavierStokesSemiImplicit) on a 3D lid-driven
+    cavity of n^3 x 6 tets: ms per time step on the B200 (device-resident, all
+    kernels and both CG solves), and the FP64 oracle's step on this host's
+    cores (ILU(0)-GMRES), both solving to 1e-8."""
+    import torch
+    from coolfluid3_b200 import NavierStokesSemiImplicit, problems as P
+    coords, conn = P.cube_tets(n)
+    nodes, comps, vals = P.lid_driven_bcs(3, n, pin_pressure=False)
+    u0 = np.zeros((coords.shape[0], 3))
+    lid = P.structured_index(3, n)[2] == n
+    u0[lid, 0] = 1.0
+    dt, theta, nb_it, tol = 0.01, 0.5, 2, 1e-8
+
+    def setup(X):
+        X.initial_conditions(u0, 0.01)
+        for comp in range(3):
+            sel = comps == comp
+            X.add_velocity_dirichlet(nodes[sel], comp, vals[sel])
+        X.add_pressure_dirichlet(np.array([0], np.uint32), 0.0)
+
+    G = NavierStokesSemiImplicit(coords, conn, dt=dt, theta=theta, nb_iterations=nb_it)
+    try:
+        G.set_krylov(velocity=dict(tol=tol, max_iters=5000), pressure=dict(tol=tol, max_iters=20000))
+        setup(G)
+        G.step(1)  # warm-up
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        sv, sp = G.step(steps)
+        torch.cuda.synchronize()
+        gpu_ms = (time.perf_counter() - t0) * 1e3 / steps
+        gpu_up = G.state[0]
+    finally:
+        G.close()
+    import oracle as O  # CPU baseline leg only
+    S = O.SemiImplicit(coords, conn, O.options(dt=dt, theta=theta), nb_it)
+    setup(S)
+    t0 = time.perf_counter()
+    rc, iters, _ = S.step(1, tol=tol)
+    cpu_s = time.perf_counter() - t0
+    return {"workload": f"3D lid-driven cavity {n}^3x6 ({conn.shape[0]} tets, {coords.shape[0]} nodes), dt {dt}, "
+                        f"theta {theta}, {nb_it} inner passes, velocity and pressure solved to {tol}",
+            "ms_per_step": round(gpu_ms, 3), "steps_per_s": round(1e3 / gpu_ms, 2),
+            "velocity_cg_iters_per_step": round(sv["iterations"] / steps, 1),
+            "pressure_cg_iters_per_step": round(sp["iterations"] / steps, 1),
+            "converged": bool(sv["converged"] and sp["converged"]),
+            "cpu_baseline": {"ms_per_step": round(cpu_s * 1e3, 1), "cores": 1, "kind": "port",
+                             "sample": "first time step of the same cavity (FP64 oracle, ILU(0)-GMRES(200))",
+                             "gmres_iters": list(iters), "converged": rc == 0}}
 
 
 def serving_in_child() -> dict:
