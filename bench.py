@@ -74,6 +74,7 @@ def parse():
     ap.add_argument("--serve-reps", type=int, default=3, help="served runs per form (the median is reported)")
     ap.add_argument("--serving-only", action="store_true", help=argparse.SUPPRESS)
     ap.add_argument("--si-n", type=int, default=32, help="cube side of the semi-implicit comparison")
+    ap.add_argument("--si-only", action="store_true", help="run only the semi-implicit comparison (one JSON line)")
     return ap.parse_args()
 
 
@@ -633,6 +634,9 @@ def main():
     args = parse()
     if args.serving_only:
         print(json.dumps(serving_compare(args)), flush=True)
+        return
+    if args.si_only:
+        print(json.dumps({"semi_implicit": semi_implicit_compare(args.si_n)}), flush=True)
         return
     rank, world, local = dist_init(args.gpus)
     try:

@@ -43,6 +43,16 @@ struct KrylovWork {
   int* ictl = nullptr;     // [0]=done [1]=jcount [2]=status [3]=iterations (BiCGStab)
   double* h_dctl = nullptr;  // pinned mirrors
   int* h_ictl = nullptr;
+  // CUDA graph of an 8-iteration CG block per operator type (FP64, FP32),
+  // captured for one set of operands and replayed between host checks.
+  struct CGGraph {
+    cudaGraphExec_t exec = nullptr;
+    const void* key[9] = {};
+    int pkind = -1, maxit = 0;
+    double tol = 0.0;
+  };
+  CGGraph cg_graph[2];
+  cudaStream_t capture_stream = nullptr;
 };
 
 namespace {
@@ -929,12 +939,38 @@ int bicgstab(ufem_ns_handle* h, KrylovWork& kw, const MT* vals, const BT* b, VT*
   return UFEM_OK;
 }
 
+// One CG iteration (five launches; a sixth and seventh with block Jacobi).
+template <typename VT, typename MT>
+int cg_iteration(ufem_ns_handle* h, KrylovWork& kw, const MT* vals, VT* x, VT* r, VT* z, VT* p, VT* q, VT* dinv,
+                 int pkind, double tol, int maxit, cudaStream_t st) {
+  const int64_t n = h->nrows;
+  const int nblk = kw.nblk;
+  const unsigned g1 = unsigned(nblk);
+  int rc;
+  cg_p_kernel<VT><<<g1, kRedThreads, 0, st>>>(n, z, p, kw.dctl, kw.ictl);
+  if ((rc = spmv<VT, MT>(h, vals, p, q, kw.ictl, st))) return rc;
+  dot_partials_kernel<VT><<<dim3(g1, 1), kRedThreads, 0, st>>>(n, p, n, q, kw.part, kw.ictl);
+  cg_alpha_kernel<<<1, 256, 0, st>>>(nblk, kw.part, kw.dctl, kw.ictl);
+  cg_xr_kernel<VT><<<g1, kRedThreads, 0, st>>>(n, pkind, dinv, p, q, x, r, z, kw.dctl, kw.ictl, kw.part);
+  if (pkind == 2) {
+    if ((rc = precond<VT>(h, pkind, dinv, r, z, kw.ictl, st))) return rc;
+    dot_partials_kernel<VT><<<dim3(g1, 1), kRedThreads, 0, st>>>(n, r, n, z, kw.part + nblk, kw.ictl);
+  }
+  cg_end_kernel<<<1, 256, 0, st>>>(nblk, kw.part, kw.dctl, kw.ictl, tol, maxit);
+  UFEM_CUDA_TRY(cudaGetLastError());
+  return UFEM_OK;
+}
+
 // Preconditioned conjugate gradients with device-side scalars (the Belos
 // "Block CG" of the reference's semi-implicit velocity and pressure solves,
-// block size 1); the host checks the done flag as in bicgstab().
+// block size 1).  The iterations are small, latency-bound launches on
+// systems of a few hundred thousand rows, so a block of 8 is captured once in
+// a CUDA graph (per operand set) and replayed 1, 2, 4 and then 8 times between
+// host checks of the done flag; iterations after convergence return at once.
 template <typename VT, typename MT, typename BT>
 int cg(ufem_ns_handle* h, KrylovWork& kw, const MT* vals, const BT* b, VT* x, VT* r, VT* z, VT* p, VT* q, VT* dinv,
        int pkind, double tol, int maxit, cudaStream_t st, SolveResult& res) {
+  constexpr int kCGBlock = 8;
   const int64_t n = h->nrows;
   const int nblk = kw.nblk;
   const unsigned g1 = unsigned(nblk);
@@ -950,21 +986,38 @@ int cg(ufem_ns_handle* h, KrylovWork& kw, const MT* vals, const BT* b, VT* x, VT
   cg_init_kernel<<<1, 1, 0, st>>>(nblk, kw.part, kw.dctl, kw.ictl, tol);
   fill_kernel<VT><<<g1, kRedThreads, 0, st>>>(n, VT(0), p);
   UFEM_CUDA_TRY(cudaGetLastError());
-  int check = 8;
-  for (int it = 0; it < maxit; it += check, check = std::min(2 * check, 64)) {
-    for (int k = 0; k < check; ++k) {
-      cg_p_kernel<VT><<<g1, kRedThreads, 0, st>>>(n, z, p, kw.dctl, kw.ictl);
-      if ((rc = spmv<VT, MT>(h, vals, p, q, kw.ictl, st))) return rc;
-      dot_partials_kernel<VT><<<dim3(g1, 1), kRedThreads, 0, st>>>(n, p, n, q, kw.part, kw.ictl);
-      cg_alpha_kernel<<<1, 256, 0, st>>>(nblk, kw.part, kw.dctl, kw.ictl);
-      cg_xr_kernel<VT><<<g1, kRedThreads, 0, st>>>(n, pkind, dinv, p, q, x, r, z, kw.dctl, kw.ictl, kw.part);
-      if (pkind == 2) {
-        if ((rc = precond<VT>(h, pkind, dinv, r, z, kw.ictl, st))) return rc;
-        dot_partials_kernel<VT><<<dim3(g1, 1), kRedThreads, 0, st>>>(n, r, n, z, kw.part + nblk, kw.ictl);
-      }
-      cg_end_kernel<<<1, 256, 0, st>>>(nblk, kw.part, kw.dctl, kw.ictl, tol, maxit);
-      UFEM_CUDA_TRY(cudaGetLastError());
+  KrylovWork::CGGraph& gr = kw.cg_graph[std::is_same<MT, float>::value ? 1 : 0];
+  const void* key[9] = {vals, b, x, r, z, p, q, dinv, h->d_start};
+  const bool cached = gr.exec && gr.pkind == pkind && gr.tol == tol && gr.maxit == maxit &&
+                      std::equal(key, key + 9, gr.key);
+  if (!cached) {
+    DeviceLock lk(device_mutex());  // no implicit device synchronisation from other threads during capture
+    if (gr.exec) {
+      cudaGraphExecDestroy(gr.exec);
+      gr.exec = nullptr;
     }
+    if (!kw.capture_stream) UFEM_CUDA_TRY(cudaStreamCreateWithFlags(&kw.capture_stream, cudaStreamNonBlocking));
+    cudaGraph_t g = nullptr;
+    UFEM_CUDA_TRY(cudaStreamBeginCapture(kw.capture_stream, cudaStreamCaptureModeThreadLocal));
+    int crc = UFEM_OK;
+    for (int k = 0; k < kCGBlock && crc == UFEM_OK; ++k)
+      crc = cg_iteration<VT, MT>(h, kw, vals, x, r, z, p, q, dinv, pkind, tol, maxit, kw.capture_stream);
+    const cudaError_t ce = cudaStreamEndCapture(kw.capture_stream, &g);
+    if (crc) {
+      if (g) cudaGraphDestroy(g);
+      return crc;
+    }
+    if (ce != cudaSuccess) return set_error(UFEM_ERR_CUDA, std::string("graph capture: ") + cudaGetErrorString(ce));
+    const cudaError_t ie = cudaGraphInstantiate(&gr.exec, g, 0);
+    cudaGraphDestroy(g);
+    if (ie != cudaSuccess) return set_error(UFEM_ERR_CUDA, std::string("graph instantiate: ") + cudaGetErrorString(ie));
+    gr.pkind = pkind;
+    gr.tol = tol;
+    gr.maxit = maxit;
+    std::copy(key, key + 9, gr.key);
+  }
+  for (int it = 0, reps = 1; it < maxit; it += reps * kCGBlock, reps = std::min(2 * reps, 8)) {
+    for (int k = 0; k < reps; ++k) UFEM_CUDA_TRY(cudaGraphLaunch(gr.exec, st));
     UFEM_CUDA_TRY(cudaMemcpyAsync(kw.h_ictl, kw.ictl, 4 * sizeof(int), cudaMemcpyDeviceToHost, st));
     UFEM_CUDA_TRY(cudaStreamSynchronize(st));
     if (kw.h_ictl[0]) break;
@@ -1165,6 +1218,9 @@ void krylov_free(ufem_ns_handle* h) {
   dfree(k.part); dfree(k.hbuf); dfree(k.H); dfree(k.cs); dfree(k.sn); dfree(k.g); dfree(k.y);
   dfree(k.dctl); dfree(k.ictl);
   DeviceLock lk(device_mutex());
+  for (auto& g : k.cg_graph)
+    if (g.exec) cudaGraphExecDestroy(g.exec);
+  if (k.capture_stream) cudaStreamDestroy(k.capture_stream);
   if (k.h_dctl) cudaFreeHost(k.h_dctl);
   if (k.h_ictl) cudaFreeHost(k.h_ictl);
   delete h->kw;
