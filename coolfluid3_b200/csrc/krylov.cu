@@ -53,6 +53,8 @@ struct KrylovWork {
   };
   CGGraph cg_graph[2];
   cudaStream_t capture_stream = nullptr;
+  int cg_nblk = 0;             // blocks of the fused CG kernels (more than nblk: they are latency-bound)
+  int* cg_counter = nullptr;   // last-block ticket of the fused CG folds
 };
 
 namespace {
@@ -63,6 +65,7 @@ constexpr int kRho = 5, kRhoOld = 6, kAlpha = 7, kOmega = 8, kRhV = 9, kTS = 10,
 constexpr int kRedThreads = 256;
 constexpr int kInnerIterCap = 400;  // iterations of one FP32 inner solve of the mixed path
 constexpr int kMaxRestarts = 10;    // BiCGStab restarts after breakdowns in one solve
+constexpr int kCGMaxBlocks = 8 * 148;  // blocks of the fused CG kernels
 
 template <typename T>
 __device__ __forceinline__ T warp_sum(T v) {
@@ -665,6 +668,104 @@ __global__ void cg_init_kernel(int nblk, const double* __restrict__ part, double
   ictl[3] = 0;
 }
 
+// ---- fused CG iteration (point Jacobi or no preconditioner) ------------------
+// Each reduction kernel writes its block partials, and the last block to finish
+// (an atomic ticket on a per-solve counter, reset by that block) folds them in
+// block order and updates the scalars: deterministic, and no block waits for
+// another.  Four launches per iteration: p update, SpMV, p.q with the alpha
+// fold, x/r/z update with the convergence/beta fold.
+
+__device__ __forceinline__ bool last_block(int* counter, int* s_flag) {
+  __threadfence();
+  __syncthreads();
+  if (threadIdx.x == 0) *s_flag = (atomicAdd(counter, 1) == int(gridDim.x) - 1) ? 1 : 0;
+  __syncthreads();
+  if (*s_flag == 0) return false;
+  __threadfence();
+  if (threadIdx.x == 0) *counter = 0;  // ready for the next launch
+  return true;
+}
+
+template <typename VT>
+__global__ void cg_pq_fold_kernel(int64_t n, const VT* __restrict__ p, const VT* __restrict__ q,
+                                  double* __restrict__ part, int* __restrict__ counter, double* __restrict__ dctl,
+                                  int* __restrict__ ictl) {
+  if (ictl[0]) return;  // read before any block of this launch can change it
+  __shared__ double sm[32];
+  __shared__ int flag;
+  double s = 0.0;
+  GRID_STRIDE(i, n) s += double(p[i]) * double(q[i]);
+  s = block_sum(s, sm);
+  if (threadIdx.x == 0) part[blockIdx.x] = s;
+  if (!last_block(counter, &flag)) return;
+  double sv = 0.0;
+  for (int b = threadIdx.x; b < int(gridDim.x); b += blockDim.x) sv += __ldcg(part + b);
+  const double d = block_sum(sv, sm);
+  if (threadIdx.x != 0) return;
+  if (!isfinite(d)) {
+    ictl[0] = 1;
+    ictl[2] = 3;
+  } else if (!(d > 0.0)) {
+    ictl[0] = 1;
+    ictl[2] = 2;
+  } else {
+    dctl[kAlpha] = dctl[kRho] / d;
+  }
+}
+
+template <typename VT>
+__global__ void cg_xr_fold_kernel(int64_t n, int pkind, const VT* __restrict__ dinv, const VT* __restrict__ p,
+                                  const VT* __restrict__ q, VT* __restrict__ x, VT* __restrict__ r,
+                                  VT* __restrict__ z, double* __restrict__ part, int* __restrict__ counter,
+                                  double* __restrict__ dctl, int* __restrict__ ictl, double tol, int maxit) {
+  if (ictl[0]) return;
+  __shared__ double sm[32];
+  __shared__ int flag;
+  const double al = dctl[kAlpha];
+  double rr = 0.0, rz = 0.0;
+  GRID_STRIDE(i, n) {
+    x[i] = VT(double(x[i]) + al * double(p[i]));
+    const VT ri = VT(double(r[i]) - al * double(q[i]));
+    r[i] = ri;
+    const VT zi = (pkind == 1) ? VT(dinv[i] * ri) : ri;
+    z[i] = zi;
+    rr += double(ri) * double(ri);
+    rz += double(ri) * double(zi);
+  }
+  rr = block_sum(rr, sm);
+  rz = block_sum(rz, sm);
+  if (threadIdx.x == 0) {
+    part[blockIdx.x] = rr;
+    part[gridDim.x + blockIdx.x] = rz;
+  }
+  if (!last_block(counter, &flag)) return;
+  double a = 0.0, b = 0.0;
+  for (int k = threadIdx.x; k < int(gridDim.x); k += blockDim.x) {
+    a += __ldcg(part + k);
+    b += __ldcg(part + gridDim.x + k);
+  }
+  const double nn = block_sum(a, sm);
+  const double rho_new = block_sum(b, sm);
+  if (threadIdx.x != 0) return;
+  const double rn = sqrt(nn);
+  dctl[kEst] = rn;
+  dctl[kOmega] = rho_new / dctl[kRho];
+  dctl[kRho] = rho_new;
+  ictl[3] += 1;
+  if (!isfinite(rn) || !isfinite(rho_new)) {
+    ictl[0] = 1;
+    ictl[2] = 3;
+  } else if (rn <= tol * dctl[kBnorm]) {
+    ictl[0] = 1;
+  } else if (!(rho_new > 0.0)) {
+    ictl[0] = 1;
+    ictl[2] = 2;
+  } else if (ictl[3] >= maxit) {
+    ictl[0] = 1;
+    ictl[2] = 1;
+  }
+}
+
 // ---------------------------------------------------------------------------
 template <typename T>
 int dalloc(T** p, size_t count) {
@@ -694,12 +795,18 @@ int ensure_work(ufem_ns_handle* h, int m, bool need32, bool bicg) {
   kw.m = std::max(kw.m, m);
   kw.n = n;
   kw.nblk = int(std::min<int64_t>(296, std::max<int64_t>(1, (n + 2047) / 2048)));
+  kw.cg_nblk = int(std::min<int64_t>(kCGMaxBlocks, std::max<int64_t>(1, (n + 511) / 512)));
   const int M = kw.m;
   const size_t nd = size_t(n);
   const size_t ndinv = size_t(h->N) * h->neq * h->neq;
+  const size_t npart = std::max(size_t(M + 2) * kw.nblk, size_t(2) * kCGMaxBlocks);
   int rc;
+  if (!kw.cg_counter) {
+    if ((rc = dalloc(&kw.cg_counter, 1))) return rc;
+    UFEM_CUDA_TRY(cudaMemset(kw.cg_counter, 0, sizeof(int)));
+  }
   if ((rc = dalloc(&kw.w, nd)) || (rc = dalloc(&kw.z, nd)) || (rc = dalloc(&kw.t, nd)) || (rc = dalloc(&kw.r, nd)) ||
-      (rc = dalloc(&kw.dinv, ndinv)) || (rc = dalloc(&kw.part, size_t(M + 2) * kw.nblk)) ||
+      (rc = dalloc(&kw.dinv, ndinv)) || (rc = dalloc(&kw.part, npart)) ||
       (rc = dalloc(&kw.hbuf, size_t(2) * (M + 2))) || (rc = dalloc(&kw.H, size_t(M + 1) * M)) ||
       (rc = dalloc(&kw.cs, size_t(M))) || (rc = dalloc(&kw.sn, size_t(M))) || (rc = dalloc(&kw.g, size_t(M + 1))) ||
       (rc = dalloc(&kw.y, size_t(M))) || (rc = dalloc(&kw.dctl, 16)) || (rc = dalloc(&kw.ictl, 8)))
@@ -947,6 +1054,16 @@ int cg_iteration(ufem_ns_handle* h, KrylovWork& kw, const MT* vals, VT* x, VT* r
   const int nblk = kw.nblk;
   const unsigned g1 = unsigned(nblk);
   int rc;
+  if (pkind != 2) {
+    const unsigned gc = unsigned(kw.cg_nblk);
+    cg_p_kernel<VT><<<gc, kRedThreads, 0, st>>>(n, z, p, kw.dctl, kw.ictl);
+    if ((rc = spmv<VT, MT>(h, vals, p, q, kw.ictl, st))) return rc;
+    cg_pq_fold_kernel<VT><<<gc, kRedThreads, 0, st>>>(n, p, q, kw.part, kw.cg_counter, kw.dctl, kw.ictl);
+    cg_xr_fold_kernel<VT><<<gc, kRedThreads, 0, st>>>(n, pkind, dinv, p, q, x, r, z, kw.part, kw.cg_counter,
+                                                     kw.dctl, kw.ictl, tol, maxit);
+    UFEM_CUDA_TRY(cudaGetLastError());
+    return UFEM_OK;
+  }
   cg_p_kernel<VT><<<g1, kRedThreads, 0, st>>>(n, z, p, kw.dctl, kw.ictl);
   if ((rc = spmv<VT, MT>(h, vals, p, q, kw.ictl, st))) return rc;
   dot_partials_kernel<VT><<<dim3(g1, 1), kRedThreads, 0, st>>>(n, p, n, q, kw.part, kw.ictl);
@@ -1216,7 +1333,7 @@ void krylov_free(ufem_ns_handle* h) {
   dfree(k.V32); dfree(k.w32); dfree(k.z32); dfree(k.t32); dfree(k.r32); dfree(k.x32); dfree(k.q32); dfree(k.dinv32);
   dfree(k.bp); dfree(k.bv); dfree(k.bs); dfree(k.bt); dfree(k.brh); dfree(k.bph); dfree(k.bsh);
   dfree(k.part); dfree(k.hbuf); dfree(k.H); dfree(k.cs); dfree(k.sn); dfree(k.g); dfree(k.y);
-  dfree(k.dctl); dfree(k.ictl);
+  dfree(k.dctl); dfree(k.ictl); dfree(k.cg_counter);
   DeviceLock lk(device_mutex());
   for (auto& g : k.cg_graph)
     if (g.exec) cudaGraphExecDestroy(g.exec);
