@@ -143,6 +143,12 @@ SIGNATURES = {
     "ufem_nssi_add_velocity_dirichlet": (C.c_int, [_P, _U32, C.c_int64, C.c_int32, _D]),
     "ufem_nssi_add_pressure_dirichlet": (C.c_int, [_P, _U32, C.c_int64, _D]),
     "ufem_nssi_clear_dirichlet": (C.c_int, [_P]),
+    "ufem_nssi_add_velocity_dirichlet_function": (C.c_int, [_P, _U32, C.c_int64, C.c_int32, C.c_char_p]),
+    "ufem_nssi_add_pressure_dirichlet_function": (C.c_int, [_P, _U32, C.c_int64, C.c_char_p]),
+    "ufem_nssi_set_time": (C.c_int, [_P, C.c_double]),
+    "ufem_nssi_write_restart": (C.c_int, [_P, C.c_char_p, C.c_double, C.c_double, C.c_int64]),
+    "ufem_nssi_read_restart": (C.c_int, [_P, C.c_char_p, C.POINTER(C.c_double), C.POINTER(C.c_double),
+                                         C.POINTER(C.c_int64)]),
     "ufem_nssi_initialize": (C.c_int, [_P, C.c_int32, _P]),
     "ufem_nssi_step": (C.c_int, [_P, C.c_int32, C.POINTER(KrylovStatus), C.POINTER(KrylovStatus), _P]),
     "ufem_nssi_get_time": (C.c_int, [_P, C.POINTER(C.c_double)]),

@@ -310,6 +310,7 @@ void destroy_impl(ufem_ns_handle* h) {
     h->d_adj = nullptr;
     h->d_state = nullptr;
     h->d_tie = nullptr;
+    h->d_coords = nullptr;
   }
   krylov_free(h);
   free_stage_pipe(h);
@@ -692,6 +693,7 @@ int make_system_view(ufem_ns_handle* base, int neq, int state_offset, ufem_ns_ha
   v->d_start = base->d_start;
   v->d_adj = base->d_adj;
   v->d_state = base->d_state + state_offset;
+  v->d_coords = base->d_coords;  // function Dirichlet values
   v->ntie = base->ntie;
   v->d_tie = base->d_tie;
   int rc;

@@ -103,7 +103,7 @@ int ufem_ns_write_restart(ufem_ns_handle* h, const char* path, double current_ti
   int rc;
   if ((rc = ufem_ns_get_state(h, tables[0].data.data(), tables[1].data.data()))) return rc;
   UFEM_CUDA_TRY(cudaMemcpy(tables[2].data.data(), h->d_nu, size_t(N) * 8, cudaMemcpyDeviceToHost));
-  {
+  if (h->d_sol) {  // the coupled system's solution vector (a semi-implicit base handle has none)
     FieldTable x{"lss_solution", N, neq, std::vector<double>(size_t(h->nrows))};
     UFEM_CUDA_TRY(cudaMemcpy(x.data.data(), h->d_sol, size_t(h->nrows) * 8, cudaMemcpyDeviceToHost));
     tables.push_back(std::move(x));
@@ -194,7 +194,7 @@ int ufem_ns_read_restart(ufem_ns_handle* h, const char* path, double* current_ti
     else if (name == "linearized_velocity") { dst = &lin; want = 4 * d; }
     else if (name == "navier_stokes_viscosity") { dst = &nu; want = 1; }
     else if (name == "body_force") { dst = &force; want = d; }
-    else if (name == "lss_solution") { dst = &sol; want = neq; }
+    else if (name == "lss_solution" && h->d_sol) { dst = &sol; want = neq; }
     else return set_error(UFEM_ERR_IO, "restart field " + name + " is not a field of this solver");
     if (rows != N || cols != want) return set_error(UFEM_ERR_IO, "restart field " + name + " has the wrong shape");
     const size_t bytes = size_t(rows) * cols * 8;
@@ -210,9 +210,9 @@ int ufem_ns_read_restart(ufem_ns_handle* h, const char* path, double* current_ti
   int rc;
   if ((rc = ufem_ns_set_state(h, up.data(), lin.data(), nu.data(), force.empty() ? nullptr : force.data())))
     return rc;
-  if (sol.empty())
+  if (h->d_sol && sol.empty())
     UFEM_CUDA_TRY(cudaMemset(h->d_sol, 0, size_t(h->nrows) * 8));
-  else
+  else if (h->d_sol)
     UFEM_CUDA_TRY(cudaMemcpy(h->d_sol, sol.data(), size_t(h->nrows) * 8, cudaMemcpyHostToDevice));
   h->time = std::strtod(attr(restart, "current_time").c_str(), nullptr);  // Time::current_time
   if (current_time) *current_time = h->time;

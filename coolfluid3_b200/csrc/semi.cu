@@ -803,6 +803,8 @@ int step_one(ufem_nssi_handle* h, cudaStream_t s) {
     if ((rc = launch_velocity_rhs<D>(h, s))) return rc;
     if (it == 0) {  // the velocity BC acts on velocities: scale the acceleration RHS around it
       si_scale_kernel<<<si_vec_blocks(us->nrows), 256, 0, s>>>(us->nrows, dt, us->d_rhs);
+      us->time = b->time;  // function values at the step's start time
+      if ((rc = launch_dirichlet_functions(us, s))) return rc;
       if ((rc = launch_dirichlet(us, s))) return rc;
       si_scale_kernel<<<si_vec_blocks(us->nrows), 256, 0, s>>>(us->nrows, 1.0 / dt, us->d_rhs);
       UFEM_CUDA_TRY(cudaGetLastError());
@@ -820,6 +822,8 @@ int step_one(ufem_nssi_handle* h, cudaStream_t s) {
     si_fill_kernel<<<si_vec_blocks(ps->nrows), 256, 0, s>>>(ps->nrows, ps->d_sol);
     UFEM_CUDA_TRY(cudaGetLastError());
     if (it == 0) {
+      ps->time = b->time;
+      if ((rc = launch_dirichlet_functions(ps, s))) return rc;
       if ((rc = launch_dirichlet(ps, s))) return rc;
     } else if ((rc = zero_bc_dofs(ps, ps->d_rhs, s))) {
       return rc;
@@ -945,6 +949,42 @@ int ufem_nssi_add_velocity_dirichlet(ufem_nssi_handle* h, const uint32_t* nodes,
 int ufem_nssi_add_pressure_dirichlet(ufem_nssi_handle* h, const uint32_t* nodes, int64_t n, const double* values) {
   if (!h) return set_error(UFEM_ERR_ARG, "NULL handle");
   return ufem_ns_add_dirichlet(h->ps, nodes, n, 0, values);
+}
+
+int ufem_nssi_add_velocity_dirichlet_function(ufem_nssi_handle* h, const uint32_t* nodes, int64_t n, int32_t comp,
+                                              const char* expr) {
+  if (!h) return set_error(UFEM_ERR_ARG, "NULL handle");
+  return ufem_ns_add_dirichlet_function(h->us, nodes, n, comp, expr);
+}
+
+int ufem_nssi_add_pressure_dirichlet_function(ufem_nssi_handle* h, const uint32_t* nodes, int64_t n,
+                                              const char* expr) {
+  if (!h) return set_error(UFEM_ERR_ARG, "NULL handle");
+  return ufem_ns_add_dirichlet_function(h->ps, nodes, n, 0, expr);
+}
+
+int ufem_nssi_set_time(ufem_nssi_handle* h, double t) {
+  if (!h) return set_error(UFEM_ERR_ARG, "NULL handle");
+  return ufem_ns_set_time(h->base, t);
+}
+
+// Restart files of the fields the reference lists as the solver's restart
+// tags (NavierStokesSemiImplicit.cpp:277-278: u, p, linearized velocity,
+// viscosity; plus the body force when set).  After reading, the caller runs
+// ufem_nssi_initialize(h, 0, ...) as the reference's initial conditions do
+// after their Restarts component: the pressure matrix then follows the
+// restarted velocity.
+int ufem_nssi_write_restart(ufem_nssi_handle* h, const char* path, double current_time, double time_step,
+                            int64_t iteration) {
+  if (!h) return set_error(UFEM_ERR_ARG, "NULL handle");
+  return ufem_ns_write_restart(h->base, path, current_time, time_step, iteration);
+}
+
+int ufem_nssi_read_restart(ufem_nssi_handle* h, const char* path, double* current_time, double* time_step,
+                           int64_t* iteration) {
+  if (!h) return set_error(UFEM_ERR_ARG, "NULL handle");
+  h->initialized = false;
+  return ufem_ns_read_restart(h->base, path, current_time, time_step, iteration);
 }
 
 int ufem_nssi_clear_dirichlet(ufem_nssi_handle* h) {

@@ -464,6 +464,35 @@ class NavierStokesSemiImplicit:
         values = np.ascontiguousarray(np.broadcast_to(np.asarray(values, np.float64), nodes.shape))
         N.check(self._lib.ufem_nssi_add_pressure_dirichlet(self._h, N.u32ptr(nodes), len(nodes), N.dptr(values)))
 
+    def add_velocity_dirichlet_function(self, nodes, comp: int, expr: str) -> None:
+        nodes = np.ascontiguousarray(nodes, np.uint32)
+        N.check(self._lib.ufem_nssi_add_velocity_dirichlet_function(self._h, N.u32ptr(nodes), len(nodes), int(comp),
+                                                                    expr.encode()))
+
+    def add_pressure_dirichlet_function(self, nodes, expr: str) -> None:
+        nodes = np.ascontiguousarray(nodes, np.uint32)
+        N.check(self._lib.ufem_nssi_add_pressure_dirichlet_function(self._h, N.u32ptr(nodes), len(nodes),
+                                                                    expr.encode()))
+
+    @time.setter
+    def time(self, t: float) -> None:
+        N.check(self._lib.ufem_nssi_set_time(self._h, float(t)))
+
+    def write_restart(self, path: str, current_time: float | None = None, time_step: float | None = None,
+                      iteration: int = 0) -> None:
+        t = self.time if current_time is None else current_time
+        N.check(self._lib.ufem_nssi_write_restart(self._h, path.encode(), t,
+                                                  self.dt if time_step is None else time_step, int(iteration)))
+
+    def read_restart(self, path: str, initialize: bool = True) -> tuple[float, float, int]:
+        """Reads the fields and (by default) reruns the initial-condition assemblies
+        without resetting the history; returns (time, time_step, iteration)."""
+        t, dt, it = C.c_double(), C.c_double(), C.c_int64()
+        N.check(self._lib.ufem_nssi_read_restart(self._h, path.encode(), C.byref(t), C.byref(dt), C.byref(it)))
+        if initialize:
+            self.initialize(reset_history=False)
+        return t.value, dt.value, it.value
+
     def clear_dirichlet(self) -> None:
         N.check(self._lib.ufem_nssi_clear_dirichlet(self._h))
 

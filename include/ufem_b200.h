@@ -374,7 +374,22 @@ int ufem_nssi_get_state(ufem_nssi_handle* h, double* up, double* lin);
 int ufem_nssi_add_velocity_dirichlet(ufem_nssi_handle* h, const uint32_t* nodes, int64_t n, int32_t comp,
                                      const double* values);
 int ufem_nssi_add_pressure_dirichlet(ufem_nssi_handle* h, const uint32_t* nodes, int64_t n, const double* values);
+/* BCDirichletFunction values (formula in x, y, z, t, as ufem_ns_add_dirichlet_function),
+ * evaluated at the step's start time; the time advances by dt per step. */
+int ufem_nssi_add_velocity_dirichlet_function(ufem_nssi_handle* h, const uint32_t* nodes, int64_t n, int32_t comp,
+                                              const char* expr);
+int ufem_nssi_add_pressure_dirichlet_function(ufem_nssi_handle* h, const uint32_t* nodes, int64_t n,
+                                              const char* expr);
+int ufem_nssi_set_time(ufem_nssi_handle* h, double t);
 int ufem_nssi_clear_dirichlet(ufem_nssi_handle* h);
+/* WriteRestartFile / ReadRestartFile of the solver's restart fields (u, p,
+ * linearized velocity, viscosity, force).  After a read, call
+ * ufem_nssi_initialize(h, 0, stream): the pressure matrix follows the read
+ * velocity, as the reference's initial conditions after Restarts do. */
+int ufem_nssi_write_restart(ufem_nssi_handle* h, const char* path, double current_time, double time_step,
+                            int64_t iteration);
+int ufem_nssi_read_restart(ufem_nssi_handle* h, const char* path, double* current_time, double* time_step,
+                           int64_t* iteration);
 /* The solver's initial conditions (trigger_initial_conditions, :400-455):
  * nu_eff into the element records, with reset_history u_adv = u1 = u2 = u3 = u,
  * the pressure matrix (tau from the current u) and the lumped velocity mass. */

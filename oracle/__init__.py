@@ -72,6 +72,8 @@ _SIG = {
     "orc_semi_get_state": (None, [C.c_void_p, _D, _D]),
     "orc_semi_add_dirichlet": (None, [C.c_void_p, C.c_int, _U32, C.c_int64, C.c_int, _D]),
     "orc_semi_initialize": (None, [C.c_void_p, C.c_int]),
+    "orc_semi_clear_dirichlet": (None, [C.c_void_p, C.c_int]),
+    "orc_semi_set_fields": (None, [C.c_void_p, _D, _D]),
     "orc_semi_step": (C.c_int, [C.c_void_p, C.c_int, C.c_double, _I32, _D]),
     "orc_semi_velocity_matrix": (None, [C.c_void_p]),
     "orc_semi_rhs": (None, [C.c_void_p, C.c_int, _D, _D, _D, _D, _D, _D]),
@@ -376,6 +378,15 @@ class SemiImplicit:
         nodes = np.ascontiguousarray(nodes, np.uint32)
         values = np.ascontiguousarray(np.broadcast_to(np.asarray(values, np.float64), nodes.shape))
         self._lib.orc_semi_add_dirichlet(self._h, 1, nodes.ctypes.data_as(_U32), len(nodes), 0, _d(values))
+
+    def clear_dirichlet(self):
+        self._lib.orc_semi_clear_dirichlet(self._h, 0)
+        self._lib.orc_semi_clear_dirichlet(self._h, 1)
+
+    def set_fields(self, up, lin):
+        """Solution and linearised-velocity fields only (viscosity and force kept)."""
+        up, lin = (np.ascontiguousarray(a, np.float64) for a in (up, lin))
+        self._lib.orc_semi_set_fields(self._h, _d(up), _d(lin))
 
     def step(self, nsteps=1, tol=1e-13):
         iters = np.zeros(2, np.int32)

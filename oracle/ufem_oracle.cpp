@@ -1828,6 +1828,17 @@ void orc_semi_add_dirichlet(void* h, int which, const uint32_t* nodes, int64_t n
   for (int64_t i = 0; i < n; ++i) S.bcs.push_back(BC{nodes[i], comp, values[i]});
 }
 
+void orc_semi_clear_dirichlet(void* h, int which) {
+  Semi* M = static_cast<Semi*>(h);
+  (which == 0 ? M->U : M->P).bcs.clear();
+}
+
+void orc_semi_set_fields(void* h, const double* up, const double* lin) {
+  Semi* M = static_cast<Semi*>(h);
+  M->F.up.assign(up, up + M->F.N * (M->F.dim + 1));
+  M->F.lin.assign(lin, lin + M->F.N * 4 * M->F.dim);
+}
+
 // Initial conditions (NavierStokesSemiImplicit.cpp:400-455): with reset,
 // u_adv = u1 = u2 = u3 = u; the pressure matrix and the lumped mass.
 void orc_semi_initialize(void* h, int reset_history) {

@@ -253,3 +253,83 @@ def test_deterministic_and_errors():
         assert G.device_bytes() > 0
     with pytest.raises(UfemError):
         NavierStokesSemiImplicit(c, t, dt=0.02, nb_iterations=0)
+
+
+def _fn_bcs(c, t):
+    """Time-dependent conditions of a unit-square flow: lid u = sin(pi x) (1 + t),
+    walls at rest, pressure 0.1 t at node 0 (as numpy evaluates the formulas)."""
+    return (np.sin(np.pi * c[:, 0]) * (1.0 + t), 0.1 * t)
+
+
+@pytest.mark.gpu
+def test_function_bcs_match_oracle():
+    c, tri, u0, p0, nu, walls, lid = cavity(2, 8)
+    dt = 0.02
+    G, S = _pair(c, tri, 2, "metric", theta=0.5, dt=dt)
+    with G:
+        G.set_krylov(velocity=dict(tol=1e-12, max_iters=5000), pressure=dict(tol=1e-12, max_iters=5000))
+        u0 = u0.copy()
+        u0[lid, 0] = np.sin(np.pi * c[lid, 0])
+        for X in (G, S):
+            X.initial_conditions(u0, nu, p0)
+        for k in range(2):
+            G.add_velocity_dirichlet(walls, k, 0.0)
+        G.add_velocity_dirichlet_function(lid, 0, "sin(pi*x) * (1 + t)")
+        G.add_velocity_dirichlet(lid, 1, 0.0)
+        G.add_pressure_dirichlet_function(np.array([0]), "0.1 * t")
+        for step in range(3):
+            tk = step * dt
+            ulid, p_pin = _fn_bcs(c[lid], tk)
+            S.clear_dirichlet()
+            for k in range(2):
+                S.add_velocity_dirichlet(walls, k, 0.0)
+            S.add_velocity_dirichlet(lid, 0, ulid)
+            S.add_velocity_dirichlet(lid, 1, 0.0)
+            S.add_pressure_dirichlet(np.array([0]), p_pin)
+            S.step(1)
+        sv, sp = G.step(3)
+        assert sv["converged"] and sp["converged"]
+        gu, _ = G.state
+        ou, _ = S.state()
+        assert np.abs(gu - ou).max() <= 1e-8 * np.abs(ou).max()
+        # constrained values come out of the solves (identity rows), to solver accuracy
+        assert abs(gu[lid, 0] - np.sin(np.pi * c[lid, 0]) * (1 + 2 * dt)).max() <= 1e-10
+        assert abs(gu[0, 2] - 0.1 * 2 * dt) <= 1e-10
+
+
+@pytest.mark.gpu
+def test_restart_continuation(tmp_path):
+    """atest-ufem-navier-stokes-restart.py for the semi-implicit solver: six
+    steps in one run against three + restart + three.  As in the reference, the
+    restarted run rebuilds the pressure matrix from the restarted velocity, so
+    the runs agree to solver accuracy, not bitwise (the reference allows 1e9 ulps);
+    the restarted run matches the oracle restarted the same way within 1e-8."""
+    c, tri, u0, p0, nu, walls, lid = cavity(2, 8)
+    kw = dict(velocity=dict(tol=1e-12, max_iters=5000), pressure=dict(tol=1e-12, max_iters=5000))
+    path = str(tmp_path / "si.cf3restart")
+    with NavierStokesSemiImplicit(c, tri, dt=0.01, theta=0.5) as A:
+        A.set_krylov(**kw)
+        A.initial_conditions(u0, nu, p0)
+        add_cavity_bcs(A, 2, walls, lid)
+        A.step(3)
+        A.write_restart(path, iteration=3)
+        mid_up, mid_lin = A.state
+        A.step(3)
+        full = A.state[0]
+    with NavierStokesSemiImplicit(c, tri, dt=0.01, theta=0.5) as B:
+        B.set_krylov(**kw)
+        add_cavity_bcs(B, 2, walls, lid)
+        t, dt, it = B.read_restart(path)
+        assert (it, dt) == (3, 0.01) and abs(t - 0.03) < 1e-15 and abs(B.time - 0.03) < 1e-15
+        up, lin = B.state
+        assert np.array_equal(up, mid_up) and np.array_equal(lin, mid_lin)
+        B.step(3)
+        restarted = B.state[0]
+    assert np.abs(restarted - full).max() <= 1e-5 * np.abs(full).max()
+    S = O.SemiImplicit(c, tri, O.options(dt=0.01, theta=0.5), 2)
+    S.set_state(mid_up, mid_lin, np.ascontiguousarray(nu))
+    S.initialize(reset_history=False)
+    add_cavity_bcs(S, 2, walls, lid)
+    S.step(3)
+    ou, _ = S.state()
+    assert np.abs(restarted - ou).max() <= 1e-8 * np.abs(ou).max()
