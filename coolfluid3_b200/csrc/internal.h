@@ -246,6 +246,12 @@ void destroy_handle(ufem_ns_handle* h);
 int krylov_solve(ufem_ns_handle* h, const ufem_krylov_opts* ko, ufem_krylov_status* st, cudaStream_t s);
 int krylov_apply(ufem_ns_handle* h, const double* d_x, double* d_y, cudaStream_t s);
 void krylov_free(ufem_ns_handle* h);
+// Aggregates of the two-level CG preconditioner (precond 3) of a one-equation
+// system: agg[row] in [0, nc) or -1; builds and inverts the Galerkin coarse
+// matrix from the system's current values.  If that matrix is not positive
+// definite the coarse space is left empty (krylov_coarse_size returns 0).
+int krylov_set_coarse(ufem_ns_handle* h, const std::vector<int32_t>& agg, int nc, cudaStream_t s);
+int krylov_coarse_size(const ufem_ns_handle* h);
 // Allocates the FP32 copy of the values (converted from the current FP64
 // values); later assemblies write both.
 int ensure_vals32(ufem_ns_handle* h, cudaStream_t s);

@@ -47,7 +47,7 @@ struct KrylovWork {
   // captured for one set of operands and replayed between host checks.
   struct CGGraph {
     cudaGraphExec_t exec = nullptr;
-    const void* key[9] = {};
+    const void* key[10] = {};
     int pkind = -1, maxit = 0;
     double tol = 0.0;
   };
@@ -55,6 +55,17 @@ struct KrylovWork {
   cudaStream_t capture_stream = nullptr;
   int cg_nblk = 0;             // blocks of the fused CG kernels (more than nblk: they are latency-bound)
   int* cg_counter = nullptr;   // last-block ticket of the fused CG folds
+  // Two-level preconditioner (precond 3; CG on one-equation systems): point
+  // Jacobi plus a piecewise-constant correction on aggregates of rows,
+  // z = D^-1 r + R Ac^-1 R^T r with the Galerkin coarse matrix Ac = R^T A R.
+  int nc = 0;                  // aggregates (0: not set up)
+  int coarse_version = 0;
+  int32_t* agg = nullptr;      // nrows: aggregate of each row, -1 for none
+  int32_t* agg_ptr = nullptr;  // nc + 1
+  int32_t* agg_rows = nullptr; // the members of each aggregate, ascending
+  double* ainv = nullptr;      // nc x nc, row-major
+  double* cvec = nullptr;      // nc: R^T r
+  double* yvec = nullptr;      // nc: Ac^-1 R^T r
 };
 
 namespace {
@@ -686,6 +697,37 @@ __device__ __forceinline__ bool last_block(int* counter, int* s_flag) {
   return true;
 }
 
+// Last block of a CG iteration: ||r|| and rho_new = r.z from the block partials
+// part[0..grid) and part[grid..2 grid), beta, convergence and iteration count.
+__device__ __forceinline__ void cg_fold_end(const double* __restrict__ part, double* __restrict__ dctl,
+                                            int* __restrict__ ictl, double tol, int maxit, double* sm) {
+  double a = 0.0, b = 0.0;
+  for (int k = threadIdx.x; k < int(gridDim.x); k += blockDim.x) {
+    a += __ldcg(part + k);
+    b += __ldcg(part + gridDim.x + k);
+  }
+  const double nn = block_sum(a, sm);
+  const double rho_new = block_sum(b, sm);
+  if (threadIdx.x != 0) return;
+  const double rn = sqrt(nn);
+  dctl[kEst] = rn;
+  dctl[kOmega] = rho_new / dctl[kRho];
+  dctl[kRho] = rho_new;
+  ictl[3] += 1;
+  if (!isfinite(rn) || !isfinite(rho_new)) {
+    ictl[0] = 1;
+    ictl[2] = 3;
+  } else if (rn <= tol * dctl[kBnorm]) {
+    ictl[0] = 1;
+  } else if (!(rho_new > 0.0)) {
+    ictl[0] = 1;
+    ictl[2] = 2;
+  } else if (ictl[3] >= maxit) {
+    ictl[0] = 1;
+    ictl[2] = 1;
+  }
+}
+
 template <typename VT>
 __global__ void cg_pq_fold_kernel(int64_t n, const VT* __restrict__ p, const VT* __restrict__ q,
                                   double* __restrict__ part, int* __restrict__ counter, double* __restrict__ dctl,
@@ -739,31 +781,88 @@ __global__ void cg_xr_fold_kernel(int64_t n, int pkind, const VT* __restrict__ d
     part[gridDim.x + blockIdx.x] = rz;
   }
   if (!last_block(counter, &flag)) return;
-  double a = 0.0, b = 0.0;
-  for (int k = threadIdx.x; k < int(gridDim.x); k += blockDim.x) {
-    a += __ldcg(part + k);
-    b += __ldcg(part + gridDim.x + k);
+  cg_fold_end(part, dctl, ictl, tol, maxit, sm);
+}
+
+// x += alpha p ; r -= alpha q ; partials of r.r (the z update follows the
+// coarse correction of the two-level preconditioner).
+template <typename VT>
+__global__ void cg_xr_plain_kernel(int64_t n, const VT* __restrict__ p, const VT* __restrict__ q, VT* __restrict__ x,
+                                   VT* __restrict__ r, double* __restrict__ part, const double* __restrict__ dctl,
+                                   const int* __restrict__ ictl) {
+  if (ictl[0]) return;
+  __shared__ double sm[32];
+  const double al = dctl[kAlpha];
+  double rr = 0.0;
+  GRID_STRIDE(i, n) {
+    x[i] = VT(double(x[i]) + al * double(p[i]));
+    const VT ri = VT(double(r[i]) - al * double(q[i]));
+    r[i] = ri;
+    rr += double(ri) * double(ri);
   }
-  const double nn = block_sum(a, sm);
-  const double rho_new = block_sum(b, sm);
-  if (threadIdx.x != 0) return;
-  const double rn = sqrt(nn);
-  dctl[kEst] = rn;
-  dctl[kOmega] = rho_new / dctl[kRho];
-  dctl[kRho] = rho_new;
-  ictl[3] += 1;
-  if (!isfinite(rn) || !isfinite(rho_new)) {
-    ictl[0] = 1;
-    ictl[2] = 3;
-  } else if (rn <= tol * dctl[kBnorm]) {
-    ictl[0] = 1;
-  } else if (!(rho_new > 0.0)) {
-    ictl[0] = 1;
-    ictl[2] = 2;
-  } else if (ictl[3] >= maxit) {
-    ictl[0] = 1;
-    ictl[2] = 1;
+  rr = block_sum(rr, sm);
+  if (threadIdx.x == 0) part[blockIdx.x] = rr;
+}
+
+// c[I] = sum of r over the rows of aggregate I (ascending), one warp per aggregate.
+template <typename VT>
+__global__ void restrict_kernel(int nc, const int32_t* __restrict__ agg_ptr, const int32_t* __restrict__ agg_rows,
+                                const VT* __restrict__ r, double* __restrict__ c, const int* __restrict__ done) {
+  if (done && *done) return;
+  const int I = int((int64_t(blockIdx.x) * blockDim.x + threadIdx.x) >> 5);
+  const int lane = threadIdx.x & 31;
+  if (I >= nc) return;  // whole warps: blockDim is a multiple of 32
+  double s = 0.0;
+  for (int k = agg_ptr[I] + lane; k < agg_ptr[I + 1]; k += 32) s += double(r[agg_rows[k]]);
+  s = warp_sum(s);
+  if (lane == 0) c[I] = s;
+}
+
+// y = Ac^-1 c, one warp per row.
+__global__ void coarse_kernel(int nc, const double* __restrict__ ainv, const double* __restrict__ c,
+                              double* __restrict__ y, const int* __restrict__ done) {
+  if (done && *done) return;
+  const int I = int((int64_t(blockIdx.x) * blockDim.x + threadIdx.x) >> 5);
+  const int lane = threadIdx.x & 31;
+  if (I >= nc) return;
+  double s = 0.0;
+  for (int J = lane; J < nc; J += 32) s += ainv[int64_t(I) * nc + J] * c[J];
+  s = warp_sum(s);
+  if (lane == 0) y[I] = s;
+}
+
+// z = D^-1 r + y[agg]
+template <typename VT>
+__global__ void prolong_kernel(int64_t n, const VT* __restrict__ dinv, const int32_t* __restrict__ agg,
+                               const double* __restrict__ y, const VT* __restrict__ r, VT* __restrict__ z) {
+  GRID_STRIDE(i, n) {
+    const int a = agg[i];
+    z[i] = VT(double(dinv[i]) * double(r[i]) + (a >= 0 ? y[a] : 0.0));
   }
+}
+
+// z = D^-1 r + y[agg] ; partials of r.z ; the last block folds r.r (written by
+// cg_xr_plain_kernel with the same grid) and r.z into the convergence test and beta.
+template <typename VT>
+__global__ void cg_prolong_fold_kernel(int64_t n, const VT* __restrict__ dinv, const int32_t* __restrict__ agg,
+                                       const double* __restrict__ y, const VT* __restrict__ r, VT* __restrict__ z,
+                                       double* __restrict__ part, int* __restrict__ counter,
+                                       double* __restrict__ dctl, int* __restrict__ ictl, double tol, int maxit) {
+  if (ictl[0]) return;
+  __shared__ double sm[32];
+  __shared__ int flag;
+  double rz = 0.0;
+  GRID_STRIDE(i, n) {
+    const int a = agg[i];
+    const double ri = double(r[i]);
+    const VT zi = VT(double(dinv[i]) * ri + (a >= 0 ? y[a] : 0.0));
+    z[i] = zi;
+    rz += ri * double(zi);
+  }
+  rz = block_sum(rz, sm);
+  if (threadIdx.x == 0) part[gridDim.x + blockIdx.x] = rz;
+  if (!last_block(counter, &flag)) return;
+  cg_fold_end(part, dctl, ictl, tol, maxit, sm);
 }
 
 // ---------------------------------------------------------------------------
@@ -862,7 +961,7 @@ int spmv(ufem_ns_handle* h, const MT* vals, const VT* x, VT* y, const int* done,
 
 template <typename VT, typename MT>
 int setup_precond(ufem_ns_handle* h, int kind, const MT* vals, VT* dinv, cudaStream_t s) {
-  if (kind == 1)
+  if (kind == 1 || kind == 3)
     jacobi_kernel<MT, VT><<<grid_for(h->nrows, 256), 256, 0, s>>>(h->nrows, h->d_diagpos, vals, dinv);
   else if (kind == 2)
     block_jacobi_kernel<MT, VT><<<grid_for(h->N, 128), 128, 0, s>>>(h->N, h->neq, h->d_diagpos, vals, dinv);
@@ -1054,6 +1153,20 @@ int cg_iteration(ufem_ns_handle* h, KrylovWork& kw, const MT* vals, VT* x, VT* r
   const int nblk = kw.nblk;
   const unsigned g1 = unsigned(nblk);
   int rc;
+  if (pkind == 3) {
+    const unsigned gc = unsigned(kw.cg_nblk);
+    const unsigned gw = unsigned((int64_t(kw.nc) * 32 + 255) / 256);
+    cg_p_kernel<VT><<<gc, kRedThreads, 0, st>>>(n, z, p, kw.dctl, kw.ictl);
+    if ((rc = spmv<VT, MT>(h, vals, p, q, kw.ictl, st))) return rc;
+    cg_pq_fold_kernel<VT><<<gc, kRedThreads, 0, st>>>(n, p, q, kw.part, kw.cg_counter, kw.dctl, kw.ictl);
+    cg_xr_plain_kernel<VT><<<gc, kRedThreads, 0, st>>>(n, p, q, x, r, kw.part, kw.dctl, kw.ictl);
+    restrict_kernel<VT><<<gw, 256, 0, st>>>(kw.nc, kw.agg_ptr, kw.agg_rows, r, kw.cvec, kw.ictl);
+    coarse_kernel<<<gw, 256, 0, st>>>(kw.nc, kw.ainv, kw.cvec, kw.yvec, kw.ictl);
+    cg_prolong_fold_kernel<VT><<<gc, kRedThreads, 0, st>>>(n, dinv, kw.agg, kw.yvec, r, z, kw.part, kw.cg_counter,
+                                                          kw.dctl, kw.ictl, tol, maxit);
+    UFEM_CUDA_TRY(cudaGetLastError());
+    return UFEM_OK;
+  }
   if (pkind != 2) {
     const unsigned gc = unsigned(kw.cg_nblk);
     cg_p_kernel<VT><<<gc, kRedThreads, 0, st>>>(n, z, p, kw.dctl, kw.ictl);
@@ -1098,15 +1211,24 @@ int cg(ufem_ns_handle* h, KrylovWork& kw, const MT* vals, const BT* b, VT* x, VT
   residual_kernel<VT, BT><<<g1, kRedThreads, 0, st>>>(n, b, q, r, kw.part, kw.part + nblk);
   finalize_norm_kernel<<<1, 1, 0, st>>>(nblk, kw.part, kw.dctl, kBeta, 1);
   finalize_norm_kernel<<<1, 1, 0, st>>>(nblk, kw.part + nblk, kw.dctl, kBnorm, 1);
-  if ((rc = precond<VT>(h, pkind, dinv, r, z, nullptr, st))) return rc;
+  if (pkind == 3) {
+    const unsigned gw = unsigned((int64_t(kw.nc) * 32 + 255) / 256);
+    restrict_kernel<VT><<<gw, 256, 0, st>>>(kw.nc, kw.agg_ptr, kw.agg_rows, r, kw.cvec, nullptr);
+    coarse_kernel<<<gw, 256, 0, st>>>(kw.nc, kw.ainv, kw.cvec, kw.yvec, nullptr);
+    prolong_kernel<VT><<<g1, kRedThreads, 0, st>>>(n, dinv, kw.agg, kw.yvec, r, z);
+    UFEM_CUDA_TRY(cudaGetLastError());
+  } else if ((rc = precond<VT>(h, pkind, dinv, r, z, nullptr, st))) {
+    return rc;
+  }
   dot_partials_kernel<VT><<<dim3(g1, 1), kRedThreads, 0, st>>>(n, r, n, z, kw.part, nullptr);
   cg_init_kernel<<<1, 1, 0, st>>>(nblk, kw.part, kw.dctl, kw.ictl, tol);
   fill_kernel<VT><<<g1, kRedThreads, 0, st>>>(n, VT(0), p);
   UFEM_CUDA_TRY(cudaGetLastError());
   KrylovWork::CGGraph& gr = kw.cg_graph[std::is_same<MT, float>::value ? 1 : 0];
-  const void* key[9] = {vals, b, x, r, z, p, q, dinv, h->d_start};
+  const void* key[10] = {vals, b, x, r, z, p, q, dinv, h->d_start,
+                         reinterpret_cast<const void*>(intptr_t(pkind == 3 ? kw.coarse_version : 0))};
   const bool cached = gr.exec && gr.pkind == pkind && gr.tol == tol && gr.maxit == maxit &&
-                      std::equal(key, key + 9, gr.key);
+                      std::equal(key, key + 10, gr.key);
   if (!cached) {
     DeviceLock lk(device_mutex());  // no implicit device synchronisation from other threads during capture
     if (gr.exec) {
@@ -1131,7 +1253,7 @@ int cg(ufem_ns_handle* h, KrylovWork& kw, const MT* vals, const BT* b, VT* x, VT
     gr.pkind = pkind;
     gr.tol = tol;
     gr.maxit = maxit;
-    std::copy(key, key + 9, gr.key);
+    std::copy(key, key + 10, gr.key);
   }
   for (int it = 0, reps = 1; it < maxit; it += reps * kCGBlock, reps = std::min(2 * reps, 8)) {
     for (int k = 0; k < reps; ++k) UFEM_CUDA_TRY(cudaGraphLaunch(gr.exec, st));
@@ -1181,7 +1303,9 @@ int krylov_solve(ufem_ns_handle* h, const ufem_krylov_opts* ko, ufem_krylov_stat
   if (o.tol <= 0) o.tol = 1e-10;
   if (o.max_refine <= 0) o.max_refine = 20;
   if (o.inner_tol <= 0) o.inner_tol = 1e-3;
-  if (o.precond < 0 || o.precond > 2) return set_error(UFEM_ERR_ARG, "precond must be 0, 1 or 2");
+  if (o.precond < 0 || o.precond > 3) return set_error(UFEM_ERR_ARG, "precond must be 0, 1, 2 or 3");
+  if (o.precond == 3 && (o.method != 2 || h->neq != 1 || !h->kw || h->kw->nc == 0))
+    return set_error(UFEM_ERR_ARG, "the two-level preconditioner needs CG on a one-equation system with aggregates set");
   if (o.method < 0 || o.method > 2)
     return set_error(UFEM_ERR_ARG, "method must be 0 (GMRES), 1 (BiCGStab) or 2 (CG)");
   const bool mixed = o.mixed != 0;
@@ -1322,6 +1446,95 @@ int ensure_vals32(ufem_ns_handle* h, cudaStream_t s) {
   return UFEM_OK;
 }
 
+namespace {
+
+// In-place inverse of an SPD matrix through its Cholesky factor; false if a
+// pivot is not positive (the coarse matrix of a system without conditions
+// that fix its constant mode is singular).
+bool spd_inverse(std::vector<double>& A, int n) {
+  std::vector<double> L(size_t(n) * n, 0.0);
+  for (int j = 0; j < n; ++j) {
+    double d = A[size_t(j) * n + j];
+    for (int k = 0; k < j; ++k) d -= L[size_t(j) * n + k] * L[size_t(j) * n + k];
+    if (!(d > 0.0) || !std::isfinite(d)) return false;
+    const double ljj = std::sqrt(d);
+    L[size_t(j) * n + j] = ljj;
+    for (int i = j + 1; i < n; ++i) {
+      double s = A[size_t(i) * n + j];
+      for (int k = 0; k < j; ++k) s -= L[size_t(i) * n + k] * L[size_t(j) * n + k];
+      L[size_t(i) * n + j] = s / ljj;
+    }
+  }
+  std::vector<double> col(n);
+  for (int c = 0; c < n; ++c) {  // solve L L^T x = e_c
+    for (int i = 0; i < n; ++i) {
+      double s = (i == c) ? 1.0 : 0.0;
+      for (int k = 0; k < i; ++k) s -= L[size_t(i) * n + k] * col[k];
+      col[i] = s / L[size_t(i) * n + i];
+    }
+    for (int i = n - 1; i >= 0; --i) {
+      double s = col[i];
+      for (int k = i + 1; k < n; ++k) s -= L[size_t(k) * n + i] * col[k];
+      col[i] = s / L[size_t(i) * n + i];
+    }
+    for (int i = 0; i < n; ++i) A[size_t(i) * n + c] = col[i];
+  }
+  return true;
+}
+
+}  // namespace
+
+int krylov_set_coarse(ufem_ns_handle* h, const std::vector<int32_t>& agg, int nc, cudaStream_t s) {
+  if (h->neq != 1) return set_error(UFEM_ERR_ARG, "aggregates are defined for one-equation systems");
+  if (int64_t(agg.size()) != h->nrows) return set_error(UFEM_ERR_ARG, "one aggregate id per row expected");
+  int rc;
+  if ((rc = ensure_work(h, 30, false, true))) return rc;
+  KrylovWork& kw = *h->kw;
+  dfree(kw.agg); dfree(kw.agg_ptr); dfree(kw.agg_rows); dfree(kw.ainv); dfree(kw.cvec); dfree(kw.yvec);
+  kw.nc = 0;
+  ++kw.coarse_version;
+  if (nc <= 0) return UFEM_OK;
+  std::vector<int32_t> ptr(size_t(nc) + 1, 0), rows;
+  for (int32_t a : agg) {
+    if (a >= nc) return set_error(UFEM_ERR_ARG, "aggregate id out of range");
+    if (a >= 0) ++ptr[size_t(a) + 1];
+  }
+  for (int I = 0; I < nc; ++I) ptr[size_t(I) + 1] += ptr[size_t(I)];
+  rows.resize(size_t(ptr[size_t(nc)]));
+  {
+    std::vector<int32_t> fill(ptr.begin(), ptr.end() - 1);
+    for (int64_t i = 0; i < h->nrows; ++i)
+      if (agg[size_t(i)] >= 0) rows[size_t(fill[size_t(agg[size_t(i)])]++)] = int32_t(i);
+  }
+  // Galerkin coarse matrix R^T A R from the system's current values, summed in
+  // row and column order on the host (deterministic), then inverted.
+  std::vector<double> vals(size_t(h->nnz));
+  UFEM_CUDA_TRY(cudaStreamSynchronize(s));
+  UFEM_CUDA_TRY(cudaMemcpy(vals.data(), h->d_vals, size_t(h->nnz) * 8, cudaMemcpyDeviceToHost));
+  std::vector<double> A(size_t(nc) * nc, 0.0);
+  for (int64_t i = 0; i < h->nrows; ++i) {
+    const int32_t I = agg[size_t(i)];
+    if (I < 0) continue;
+    for (int64_t q = h->start_h[size_t(i)]; q < h->start_h[size_t(i) + 1]; ++q) {
+      const int32_t J = agg[size_t(h->adj_h[size_t(q)])];
+      if (J >= 0) A[size_t(I) * nc + J] += vals[size_t(q)];
+    }
+  }
+  if (!spd_inverse(A, nc)) return UFEM_OK;  // nc stays 0: the caller falls back to point Jacobi
+  if ((rc = dalloc(&kw.agg, size_t(h->nrows))) || (rc = dalloc(&kw.agg_ptr, ptr.size())) ||
+      (rc = dalloc(&kw.agg_rows, std::max<size_t>(rows.size(), 1))) || (rc = dalloc(&kw.ainv, A.size())) ||
+      (rc = dalloc(&kw.cvec, size_t(nc))) || (rc = dalloc(&kw.yvec, size_t(nc))))
+    return rc;
+  UFEM_CUDA_TRY(cudaMemcpy(kw.agg, agg.data(), agg.size() * 4, cudaMemcpyHostToDevice));
+  UFEM_CUDA_TRY(cudaMemcpy(kw.agg_ptr, ptr.data(), ptr.size() * 4, cudaMemcpyHostToDevice));
+  if (!rows.empty()) UFEM_CUDA_TRY(cudaMemcpy(kw.agg_rows, rows.data(), rows.size() * 4, cudaMemcpyHostToDevice));
+  UFEM_CUDA_TRY(cudaMemcpy(kw.ainv, A.data(), A.size() * 8, cudaMemcpyHostToDevice));
+  kw.nc = nc;
+  return UFEM_OK;
+}
+
+int krylov_coarse_size(const ufem_ns_handle* h) { return h->kw ? h->kw->nc : 0; }
+
 int krylov_apply(ufem_ns_handle* h, const double* d_x, double* d_y, cudaStream_t s) {
   return spmv<double, double>(h, h->d_vals, d_x, d_y, nullptr, s);
 }
@@ -1334,6 +1547,7 @@ void krylov_free(ufem_ns_handle* h) {
   dfree(k.bp); dfree(k.bv); dfree(k.bs); dfree(k.bt); dfree(k.brh); dfree(k.bph); dfree(k.bsh);
   dfree(k.part); dfree(k.hbuf); dfree(k.H); dfree(k.cs); dfree(k.sn); dfree(k.g); dfree(k.y);
   dfree(k.dctl); dfree(k.ictl); dfree(k.cg_counter);
+  dfree(k.agg); dfree(k.agg_ptr); dfree(k.agg_rows); dfree(k.ainv); dfree(k.cvec); dfree(k.yvec);
   DeviceLock lk(device_mutex());
   for (auto& g : k.cg_graph)
     if (g.exec) cudaGraphExecDestroy(g.exec);

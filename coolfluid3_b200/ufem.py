@@ -36,7 +36,7 @@ def krylov_options(method: str = "bicgstab", restart: int = 30, max_iters: int =
     o.method = {"gmres": 0, "bicgstab": 1, "cg": 2}[method]
     o.restart = restart
     o.max_iters = max_iters
-    o.precond = {"none": 0, "jacobi": 1, "block_jacobi": 2}[precond]
+    o.precond = {"none": 0, "jacobi": 1, "block_jacobi": 2, "two_level": 3}[precond]
     o.tol = tol
     o.mixed = 1 if mixed else 0
     o.max_refine = max_refine
@@ -408,9 +408,10 @@ class NavierStokesSemiImplicit:
         self.set_krylov()
 
     def set_krylov(self, velocity: dict | None = None, pressure: dict | None = None) -> None:
-        """Krylov options of the two solves (default: CG, point Jacobi, 1e-10)."""
+        """Krylov options of the two solves (default: CG to 1e-10; point Jacobi
+        for the velocity, the two-level preconditioner for the pressure)."""
         kv = krylov_options(**{"method": "cg", **(velocity or {})})
-        kp = krylov_options(**{"method": "cg", **(pressure or {})})
+        kp = krylov_options(**{"method": "cg", "precond": "two_level", **(pressure or {})})
         N.check(self._lib.ufem_nssi_set_krylov(self._h, C.byref(kv), C.byref(kp)))
 
     def initial_conditions(self, u: np.ndarray, nu: float | np.ndarray, p: np.ndarray | None = None,

@@ -73,7 +73,8 @@ typedef struct ufem_krylov_opts {
   int32_t method;      /* 0: GMRES(restart)  1: BiCGStab (default)  2: CG (SPD)   */
   int32_t restart;     /* GMRES restart length, default 30                         */
   int32_t max_iters;   /* total Krylov iterations (per refinement pass), 3000    */
-  int32_t precond;     /* 0 none, 1 point Jacobi (default), 2 node-block Jacobi   */
+  int32_t precond;     /* 0 none, 1 point Jacobi (default), 2 node-block Jacobi,
+                          3 two-level (CG, semi-implicit pressure only)          */
   double tol;          /* ||b - A x|| / ||b|| target, default 1e-10                */
   int32_t mixed;       /* 0: all FP64; 1: FP32 inner Krylov + FP64 refinement     */
   int32_t max_refine;  /* outer refinement passes when mixed, default 20          */
@@ -365,7 +366,11 @@ typedef struct ufem_nssi_handle ufem_nssi_handle;
 int ufem_nssi_create(const ufem_mesh* mesh, const ufem_ns_options* opts, int32_t nb_iterations,
                      const uint32_t* slaves, const uint32_t* masters, int64_t nlinks, ufem_nssi_handle** out);
 /* Krylov options of the velocity and pressure solves (SolveUSystem /
- * SolvePSystem, :99-100); NULL keeps the current one. */
+ * SolvePSystem, :99-100); NULL keeps the current one.  Defaults: CG with point
+ * Jacobi for the velocity, CG with the two-level preconditioner (precond 3:
+ * point Jacobi plus a Galerkin coarse correction on geometric aggregates,
+ * built from the pressure matrix once its conditions are applied; point Jacobi
+ * if that coarse matrix is singular) for the pressure, both to 1e-10. */
 int ufem_nssi_set_krylov(ufem_nssi_handle* h, const ufem_krylov_opts* velocity, const ufem_krylov_opts* pressure);
 int ufem_nssi_set_state(ufem_nssi_handle* h, const double* up, const double* lin, const double* nu,
                         const double* force);
