@@ -794,6 +794,30 @@ void fold_status(ufem_krylov_status& acc, const ufem_krylov_status& s, bool firs
   acc.rel_residual = std::max(acc.rel_residual, s.rel_residual);
 }
 
+// Aggregates of the pressure rows: the node's box, except rows the conditions
+// or the periodic links decouple (identity rows); empty boxes are dropped.
+int build_pressure_coarse(ufem_nssi_handle* h, cudaStream_t s) {
+  ufem_ns_handle* ps = h->ps;
+  const int64_t N = ps->N;
+  std::vector<int32_t> agg(h->box);
+  for (const auto& e : ps->bcs) agg[ps->p2m_h.empty() ? e.node : ps->p2m_h[e.node]] = -1;
+  if (!ps->p2m_h.empty())
+    for (int64_t i = 0; i < N; ++i)
+      if (ps->p2m_h[size_t(i)] != uint32_t(i)) agg[size_t(i)] = -1;
+  std::vector<int32_t> ren(size_t(h->nbox), -1);
+  int nc = 0;
+  for (int32_t& a : agg)
+    if (a >= 0) {
+      if (ren[size_t(a)] < 0) ren[size_t(a)] = nc++;
+      a = ren[size_t(a)];
+    }
+  int rc;
+  if ((rc = krylov_set_coarse(ps, agg, nc, s))) return rc;
+  h->coarse_ok = krylov_coarse_size(ps) > 0;
+  h->coarse_ready = true;
+  return UFEM_OK;
+}
+
 template <int D>
 int step_one(ufem_nssi_handle* h, cudaStream_t s) {
   ufem_ns_handle* b = h->base;
@@ -857,30 +881,6 @@ int step_one(ufem_nssi_handle* h, cudaStream_t s) {
   si_update_kernel<<<si_vec_blocks(N), 256, 0, s>>>(N, D, h->d_uvec, h->d_pvec, b->d_state, b->d_hist);
   UFEM_CUDA_TRY(cudaGetLastError());
   b->time += dt;
-  return UFEM_OK;
-}
-
-// Aggregates of the pressure rows: the node's box, except rows the conditions
-// or the periodic links decouple (identity rows); empty boxes are dropped.
-int build_pressure_coarse(ufem_nssi_handle* h, cudaStream_t s) {
-  ufem_ns_handle* ps = h->ps;
-  const int64_t N = ps->N;
-  std::vector<int32_t> agg(h->box);
-  for (const auto& e : ps->bcs) agg[ps->p2m_h.empty() ? e.node : ps->p2m_h[e.node]] = -1;
-  if (!ps->p2m_h.empty())
-    for (int64_t i = 0; i < N; ++i)
-      if (ps->p2m_h[size_t(i)] != uint32_t(i)) agg[size_t(i)] = -1;
-  std::vector<int32_t> ren(size_t(h->nbox), -1);
-  int nc = 0;
-  for (int32_t& a : agg)
-    if (a >= 0) {
-      if (ren[size_t(a)] < 0) ren[size_t(a)] = nc++;
-      a = ren[size_t(a)];
-    }
-  int rc;
-  if ((rc = krylov_set_coarse(ps, agg, nc, s))) return rc;
-  h->coarse_ok = krylov_coarse_size(ps) > 0;
-  h->coarse_ready = true;
   return UFEM_OK;
 }
 
