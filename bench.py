@@ -513,8 +513,9 @@ def time_steps(ns, pb, args, stream, sptr):
 def semi_implicit_compare(n: int, steps: int = 3) -> dict:
     """The semi-implicit scheme (NavierStokesSemiImplicit) on a 3D lid-driven
     cavity of n^3 x 6 tets: ms per time step on the B200 (device-resident, all
-    kernels and both CG solves), and the FP64 oracle's step on this host's
-    cores (ILU(0)-GMRES), both solving to 1e-8."""
+    kernels, velocity CG with point Jacobi, pressure CG with the two-level
+    preconditioner), and the FP64 oracle's step on one host core
+    (ILU(0)-GMRES), both solving to 1e-8."""
     import torch
     from coolfluid3_b200 import NavierStokesSemiImplicit, problems as P
     coords, conn = P.cube_tets(n)
