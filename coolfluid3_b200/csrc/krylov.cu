@@ -47,11 +47,13 @@ struct KrylovWork {
   // captured for one set of operands and replayed between host checks.
   struct CGGraph {
     cudaGraphExec_t exec = nullptr;
-    const void* key[10] = {};
+    const void* key[16] = {};
     int pkind = -1, maxit = 0;
     double tol = 0.0;
   };
   CGGraph cg_graph[2];
+  CGGraph bicg_graph[2];   // the same for BiCGStab
+  bool use_graph = true;   // false for the allocation-free solve (instantiation allocates)
   cudaStream_t capture_stream = nullptr;
   int cg_nblk = 0;             // blocks of the fused CG kernels (more than nblk: they are latency-bound)
   int* cg_counter = nullptr;   // last-block ticket of the fused CG folds
@@ -1099,25 +1101,71 @@ int bicgstab(ufem_ns_handle* h, KrylovWork& kw, const MT* vals, const BT* b, VT*
   bicg_init_kernel<<<1, 1, 0, st>>>(kw.dctl, kw.ictl, tol);
   UFEM_CUDA_TRY(cudaGetLastError());
   const double alpha_max = std::is_same<VT, float>::value ? 1e20 : 1e150;
+  auto iteration = [&](cudaStream_t s2) -> int {
+    int irc;
+    bicg_p_kernel<VT><<<g1, kRedThreads, 0, s2>>>(n, pkind, dinv, r, v, p, ph, kw.dctl, kw.ictl);
+    if (pkind == 2 && (irc = precond<VT>(h, pkind, dinv, p, ph, kw.ictl, s2))) return irc;
+    if ((irc = spmv<VT, MT>(h, vals, ph, v, kw.ictl, s2))) return irc;
+    dot_partials_kernel<VT><<<dim3(g1, 1), kRedThreads, 0, s2>>>(n, rh, n, v, kw.part, kw.ictl);
+    bicg_alpha_kernel<<<1, 256, 0, s2>>>(nblk, kw.part, kw.dctl, kw.ictl, alpha_max);
+    bicg_s_kernel<VT><<<g1, kRedThreads, 0, s2>>>(n, pkind, dinv, r, v, sv, sh, kw.dctl, kw.ictl);
+    if (pkind == 2 && (irc = precond<VT>(h, pkind, dinv, sv, sh, kw.ictl, s2))) return irc;
+    if ((irc = spmv<VT, MT>(h, vals, sh, tv, kw.ictl, s2))) return irc;
+    dot2_partials_kernel<VT><<<g1, kRedThreads, 0, s2>>>(n, tv, sv, kw.part, kw.ictl);
+    bicg_omega_kernel<<<1, 256, 0, s2>>>(nblk, kw.part, kw.dctl, kw.ictl);
+    bicg_xr_kernel<VT><<<g1, kRedThreads, 0, s2>>>(n, ph, sh, sv, tv, rh, x, r, kw.dctl, kw.ictl, kw.part);
+    bicg_end_kernel<<<1, 256, 0, s2>>>(nblk, kw.part, kw.dctl, kw.ictl, tol, maxit);
+    UFEM_CUDA_TRY(cudaGetLastError());
+    return UFEM_OK;
+  };
+  // Blocks of 8 iterations, captured once per operand set in a CUDA graph and
+  // replayed (the same launches in the same order: the same arithmetic).
+  constexpr int kBlock = 8;
+  KrylovWork::CGGraph* gr = nullptr;
+  if (kw.use_graph) {
+    gr = &kw.bicg_graph[std::is_same<MT, float>::value ? 1 : 0];
+    const void* key[16] = {vals, b, x, r, rh, p, v, sv, tv, ph, sh, dinv, h->d_start};
+    const bool cached = gr->exec && gr->pkind == pkind && gr->tol == tol && gr->maxit == maxit &&
+                        std::equal(key, key + 16, gr->key);
+    if (!cached) {
+      DeviceLock lk(device_mutex());  // no implicit device synchronisation from other threads during capture
+      if (gr->exec) {
+        cudaGraphExecDestroy(gr->exec);
+        gr->exec = nullptr;
+      }
+      if (!kw.capture_stream) UFEM_CUDA_TRY(cudaStreamCreateWithFlags(&kw.capture_stream, cudaStreamNonBlocking));
+      cudaGraph_t g = nullptr;
+      UFEM_CUDA_TRY(cudaStreamBeginCapture(kw.capture_stream, cudaStreamCaptureModeThreadLocal));
+      int crc = UFEM_OK;
+      for (int k = 0; k < kBlock && crc == UFEM_OK; ++k) crc = iteration(kw.capture_stream);
+      const cudaError_t ce = cudaStreamEndCapture(kw.capture_stream, &g);
+      if (crc) {
+        if (g) cudaGraphDestroy(g);
+        return crc;
+      }
+      if (ce != cudaSuccess) return set_error(UFEM_ERR_CUDA, std::string("graph capture: ") + cudaGetErrorString(ce));
+      const cudaError_t ie = cudaGraphInstantiate(&gr->exec, g, 0);
+      cudaGraphDestroy(g);
+      if (ie != cudaSuccess)
+        return set_error(UFEM_ERR_CUDA, std::string("graph instantiate: ") + cudaGetErrorString(ie));
+      gr->pkind = pkind;
+      gr->tol = tol;
+      gr->maxit = maxit;
+      std::copy(key, key + 16, gr->key);
+    }
+  }
   // The host reads the done flag after 8, then 16, 32 and at most 64 more
   // iterations: few synchronisations on long solves, little overshoot on short
   // ones (iterations after convergence return at once on the device flag).
-  int check = 8;
+  int check = kBlock;
   for (int it = 0; it < maxit; it += check, check = std::min(2 * check, 64)) {
-    for (int k = 0; k < check; ++k) {
-      bicg_p_kernel<VT><<<g1, kRedThreads, 0, st>>>(n, pkind, dinv, r, v, p, ph, kw.dctl, kw.ictl);
-      if (pkind == 2 && (rc = precond<VT>(h, pkind, dinv, p, ph, kw.ictl, st))) return rc;
-      if ((rc = spmv<VT, MT>(h, vals, ph, v, kw.ictl, st))) return rc;
-      dot_partials_kernel<VT><<<dim3(g1, 1), kRedThreads, 0, st>>>(n, rh, n, v, kw.part, kw.ictl);
-      bicg_alpha_kernel<<<1, 256, 0, st>>>(nblk, kw.part, kw.dctl, kw.ictl, alpha_max);
-      bicg_s_kernel<VT><<<g1, kRedThreads, 0, st>>>(n, pkind, dinv, r, v, sv, sh, kw.dctl, kw.ictl);
-      if (pkind == 2 && (rc = precond<VT>(h, pkind, dinv, sv, sh, kw.ictl, st))) return rc;
-      if ((rc = spmv<VT, MT>(h, vals, sh, tv, kw.ictl, st))) return rc;
-      dot2_partials_kernel<VT><<<g1, kRedThreads, 0, st>>>(n, tv, sv, kw.part, kw.ictl);
-      bicg_omega_kernel<<<1, 256, 0, st>>>(nblk, kw.part, kw.dctl, kw.ictl);
-      bicg_xr_kernel<VT><<<g1, kRedThreads, 0, st>>>(n, ph, sh, sv, tv, rh, x, r, kw.dctl, kw.ictl, kw.part);
-      bicg_end_kernel<<<1, 256, 0, st>>>(nblk, kw.part, kw.dctl, kw.ictl, tol, maxit);
-      UFEM_CUDA_TRY(cudaGetLastError());
+    for (int k = 0; k < check; k += kBlock) {
+      if (gr) {
+        UFEM_CUDA_TRY(cudaGraphLaunch(gr->exec, st));
+      } else {
+        for (int j = 0; j < kBlock; ++j)
+          if ((rc = iteration(st))) return rc;
+      }
     }
     UFEM_CUDA_TRY(cudaMemcpyAsync(kw.h_ictl, kw.ictl, 4 * sizeof(int), cudaMemcpyDeviceToHost, st));
     UFEM_CUDA_TRY(cudaStreamSynchronize(st));
@@ -1225,10 +1273,10 @@ int cg(ufem_ns_handle* h, KrylovWork& kw, const MT* vals, const BT* b, VT* x, VT
   fill_kernel<VT><<<g1, kRedThreads, 0, st>>>(n, VT(0), p);
   UFEM_CUDA_TRY(cudaGetLastError());
   KrylovWork::CGGraph& gr = kw.cg_graph[std::is_same<MT, float>::value ? 1 : 0];
-  const void* key[10] = {vals, b, x, r, z, p, q, dinv, h->d_start,
+  const void* key[16] = {vals, b, x, r, z, p, q, dinv, h->d_start,
                          reinterpret_cast<const void*>(intptr_t(pkind == 3 ? kw.coarse_version : 0))};
   const bool cached = gr.exec && gr.pkind == pkind && gr.tol == tol && gr.maxit == maxit &&
-                      std::equal(key, key + 10, gr.key);
+                      std::equal(key, key + 16, gr.key);
   if (!cached) {
     DeviceLock lk(device_mutex());  // no implicit device synchronisation from other threads during capture
     if (gr.exec) {
@@ -1253,7 +1301,7 @@ int cg(ufem_ns_handle* h, KrylovWork& kw, const MT* vals, const BT* b, VT* x, VT
     gr.pkind = pkind;
     gr.tol = tol;
     gr.maxit = maxit;
-    std::copy(key, key + 10, gr.key);
+    std::copy(key, key + 16, gr.key);
   }
   for (int it = 0, reps = 1; it < maxit; it += reps * kCGBlock, reps = std::min(2 * reps, 8)) {
     for (int k = 0; k < reps; ++k) UFEM_CUDA_TRY(cudaGraphLaunch(gr.exec, st));
@@ -1551,6 +1599,8 @@ void krylov_free(ufem_ns_handle* h) {
   DeviceLock lk(device_mutex());
   for (auto& g : k.cg_graph)
     if (g.exec) cudaGraphExecDestroy(g.exec);
+  for (auto& g : k.bicg_graph)
+    if (g.exec) cudaGraphExecDestroy(g.exec);
   if (k.capture_stream) cudaStreamDestroy(k.capture_stream);
   if (k.h_dctl) cudaFreeHost(k.h_dctl);
   if (k.h_ictl) cudaFreeHost(k.h_ictl);
@@ -1617,6 +1667,7 @@ extern "C" int ufem_ns_solve_noalloc(ufem_ns_handle* h, const ufem_krylov_opts* 
   double h_d[16];
   int h_i[8];
   KrylovWork kw;  // a view of the fixed scratch; owns nothing
+  kw.use_graph = false;  // graph instantiation would allocate
   kw.n = n;
   kw.nblk = int(std::min<int64_t>(kMaxPartials, std::max<int64_t>(1, (n + 2047) / 2048)));
   double* vec[9];
