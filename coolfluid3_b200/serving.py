@@ -196,9 +196,7 @@ class Server:
         self.large_rows = int(large_rows)
         self.large_workers = int(large_workers)
         self.small_priority = bool(small_priority)
-        # 6000: the finest 2D requests need close to 3000 Jacobi-BiCGStab iterations,
-        # and a batched member's reductions round differently from its own handle's
-        self.krylov = dict(method="bicgstab", precond="jacobi", tol=1e-10, max_iters=6000)
+        self.krylov = dict(method="bicgstab", precond="jacobi", tol=1e-10, max_iters=3000)
         self.krylov.update(krylov or {})
         self.krylov_mixed = dict(self.krylov, mixed=True, inner_tol=1e-6, max_refine=20) if mixed else self.krylov
         self.mixed_scope = mixed_scope
@@ -383,7 +381,7 @@ def run_plain(requests: list[Request], krylov: dict | None = None, realtime: boo
               use_specializations: bool = False) -> tuple[list[Result], dict]:
     """The same requests one at a time in arrival order through the plain
     FP64 one-handle path (assemble, Dirichlet, BiCGStab + Jacobi, update)."""
-    kr = dict(method="bicgstab", precond="jacobi", tol=1e-10, max_iters=6000)  # as Server
+    kr = dict(method="bicgstab", precond="jacobi", tol=1e-10, max_iters=3000)  # as Server
     kr.update(krylov or {})
     reqs = sorted(requests, key=lambda r: r.arrival)
     results = []
