@@ -584,11 +584,7 @@ def serving_compare(args):
     reqs = S.poisson_workload(args.serve_requests, rate=args.serve_rate, elems=elems, nu=(1e-4, 1e-2),
                               nsteps=args.serve_steps, seed=20261203)
     gen_s = time.perf_counter() - t0
-    # FP64 solves may take up to 6000 iterations (the finest 2D requests need close
-    # to 3000, and a batched member's reductions round differently from its own
-    # handle's); the mixed form keeps the 3000 of its FP32-operator stage
-    kr64 = dict(tol=1e-10, max_iters=6000)
-    plain, pst = S.run_plain(reqs, krylov=kr64, realtime=True)
+    plain, pst = S.run_plain(reqs, krylov=dict(tol=1e-10), realtime=True)
 
     def pick(st, res):
         return {"steps_per_s": round(st["steps_per_s"], 3), "seconds": round(st["seconds"], 3),
@@ -610,8 +606,8 @@ def serving_compare(args):
         # the median throughput is reported (with the range)
         runs = []
         for _ in range(max(1, args.serve_reps)):
-            srv = S.Server(int(args.serve_budget_gb * 1e9), precision="fp64", mixed=mixed,
-                           krylov=dict(tol=1e-10) if mixed else kr64, realtime=True)
+            srv = S.Server(int(args.serve_budget_gb * 1e9), precision="fp64", mixed=mixed, krylov=dict(tol=1e-10),
+                           realtime=True)
             res, st = srv.run(reqs)
             runs.append((st["steps_per_s"], st, res, srv))
         runs.sort(key=lambda x: x[0])
