@@ -1241,9 +1241,14 @@ int ufem_batch_solve(ufem_batch* b, const ufem_krylov_opts* kopts, ufem_krylov_s
       refines[m] += b->h_ictl[m * kIc + fRepl];
     }
   }
-  if (mixed) {
-    // members the FP32-operator iteration did not bring to the FP64 tolerance
-    // finish with the FP64 operator, from their current iterate
+  {
+    // Members whose iteration ended above the FP64 tolerance finish with the
+    // FP64 operator from their current iterate: every such member of the mixed
+    // form (its FP32-operator stage), and a plain FP64 member that stopped
+    // before its iteration limit because its recursive residual met the
+    // tolerance while the true one had drifted above it (a fresh start
+    // recomputes r = b - A x).  The finish has max_iters of its own for every
+    // member, so no member's arithmetic depends on the others in its batch.
     if ((rc = true_residual_b(b, st))) return rc;
     UFEM_CUDA_TRY(cudaMemcpyAsync(b->h_dctl, b->dctl, sizeof(double) * kDc * b->nmesh, cudaMemcpyDeviceToHost, st));
     UFEM_CUDA_TRY(cudaStreamSynchronize(st));
@@ -1251,7 +1256,7 @@ int ufem_batch_solve(ufem_batch* b, const ufem_krylov_opts* kopts, ufem_krylov_s
     std::vector<int> redo(b->nmesh, 0);
     for (int m = 0; m < b->nmesh; ++m) {
       const double rr = b->h_dctl[m * kDc + sTrue];
-      redo[m] = !(std::isfinite(rr) && rr <= o.tol) && std::isfinite(rr) ? 1 : 0;
+      redo[m] = !(std::isfinite(rr) && rr <= o.tol) && std::isfinite(rr) && (mixed || iters[m] < o.max_iters) ? 1 : 0;
       any = any || redo[m];
     }
     if (any) {

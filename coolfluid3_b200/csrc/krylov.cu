@@ -1379,7 +1379,9 @@ int krylov_solve(ufem_ns_handle* h, const ufem_krylov_opts* ko, ufem_krylov_stat
                                               kw.bt, kw.bph, kw.bsh, kw.dinv, o.precond, o.tol, o.max_iters - used, s, r);
         if (rc) return rc;
         used += r.iters;
-        if (r.status == 2 && !r.converged && std::isfinite(r.relres) && used < o.max_iters &&
+        // also restart a solve that stopped early because its recursive
+        // residual met the tolerance while the true one had drifted above it
+        if ((r.status == 2 || r.status == 1) && !r.converged && std::isfinite(r.relres) && used < o.max_iters &&
             restarts < kMaxRestarts)
           continue;
         break;
