@@ -20,9 +20,11 @@ oracle timed on this host as the baseline, full time steps per second
 and the mixed-precision path, and `serving`: served time steps per second with
 p50/p99 step and request latency for a seeded Poisson workload of 2D/3D
 requests (continuous batching, mixed-precision solve) against the plain path
-that serves the same requests one at a time.
+that serves the same requests one at a time.  `semi_implicit`: time steps of the
+semi-implicit scheme (NavierStokesSemiImplicit) on a 3D cavity beside the FP64
+oracle's step on one host core (`--si-only` runs it alone).
 
-Multi-GPU: the path does not shard in this build (one GPU per mesh), so
+Multi-GPU: one mesh is not split across GPUs (one GPU per mesh), so
 `--gpus N` (under torchrun) runs N independent replicas; value is the sum over
 ranks of the elements assembled divided by the max-over-ranks time.
 
