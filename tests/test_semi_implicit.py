@@ -9,6 +9,8 @@ Pins of the oracle (CPU):
     alpha_su 0, nu 1, force (2, 0), dt 0.5, 50 steps, pressure 10 at the centre):
     |u - y (2 - y)| <= 1e-2 and |v| <= 1e-3, the test's own bounds (the
     reference meshes the blocks with quadrilaterals, here triangles);
+  - the same flow in 3D (plane Poiseuille between two walls, periodic in x and z,
+    tetrahedra): u = g / (2 nu) y (H - y) to 1e-3, v = w = 0;
   - closed forms: the lumped mass of a node is the sum of |element| / (dim + 1)
     over its elements; the pressure matrix rows sum to zero; both systems are
     symmetric.
@@ -99,6 +101,45 @@ def test_oracle_laminar_channel_acceptance():
     assert np.abs(up[:, 0] - y * (2 - y)).max() <= 1e-2
     assert np.abs(up[:, 1]).max() <= 1e-3
     assert np.allclose(up[links[0]], up[links[1]], rtol=0, atol=1e-12)  # slaves carry their masters' values
+
+
+def test_oracle_plane_poiseuille_3d():
+    """The 3D counterpart of the channel case: flow between two walls (y = 0, 2)
+    driven by a body force along x, periodic in x and z (edge nodes linked twice,
+    chains resolved to the final master), on tetrahedra.  The steady solution is
+    u = g / (2 nu) y (H - y), v = w = 0."""
+    c, t = O.mesh_cube_tets(8, 0.0, 1)
+    c = c.copy()
+    H, g, nu = 2.0, 2.0, 1.0
+    c[:, 1] *= H
+    N = c.shape[0]
+
+    def side(k, v):
+        return np.abs(c[:, k] - v) < 1e-9
+
+    key = {tuple(np.round(p, 9)): i for i, p in enumerate(c)}
+    sl, ms = [], []
+    for i in np.where(side(0, 1.0))[0]:
+        sl.append(i)
+        ms.append(key[(0.0, round(c[i, 1], 9), round(c[i, 2], 9))])
+    for i in np.where(side(2, 1.0) & ~side(0, 1.0))[0]:
+        sl.append(i)
+        ms.append(key[(round(c[i, 0], 9), round(c[i, 1], 9), 0.0)])
+    links = (np.array(sl), np.array(ms))
+    S = O.SemiImplicit(c, t, O.options(dt=0.5, theta=0.5, alpha_su=0.0), 2, periodic_links=links)
+    force = np.zeros((N, 3))
+    force[:, 0] = g
+    S.initial_conditions(np.zeros((N, 3)), nu, force=force)
+    walls = np.where(side(1, 0.0) | side(1, H))[0]
+    for k in range(3):
+        S.add_velocity_dirichlet(walls, k, 0.0)
+    S.add_pressure_dirichlet(np.array([np.argmin(np.linalg.norm(c - [0.5, 1.0, 0.5], axis=1))]), 10.0)
+    rc, _, worst = S.step(40)
+    assert rc == 0 and worst <= 1e-12
+    up, _ = S.state()
+    y = c[:, 1]
+    assert np.abs(up[:, 0] - g / (2 * nu) * y * (H - y)).max() <= 1e-3
+    assert np.abs(up[:, 1:3]).max() <= 1e-12
 
 
 @pytest.mark.parametrize("dim", [2, 3])
