@@ -35,6 +35,21 @@ def test_library_exports_every_declared_symbol():
     assert set(names) == set(N.SIGNATURES)
 
 
+@pytest.mark.parametrize("lang,std", [("c", "-std=c99"), ("c++", "-std=c++17")])
+def test_header_is_plain_c(tmp_path, lang, std):
+    """The boundary header compiles as ISO C99 and as C++ without warnings: plain
+    pointers, sizes and status codes, no CUDA or torch types."""
+    src = tmp_path / "use_header.c"
+    src.write_text('#include "ufem_b200.h"\nint main(void) { ufem_ns_handle* a = 0; ufem_nssi_handle* b = 0; '
+                   'ufem_batch* c = 0; (void)a; (void)b; (void)c; return 0; }\n')
+    cc = "gcc" if lang == "c" else "g++"
+    proc = subprocess.run([cc, std, "-Wall", "-Wextra", "-Werror", "-pedantic", "-x", lang, "-c", str(src),
+                           "-I", os.path.dirname(HEADER), "-o", str(tmp_path / "o.o")], capture_output=True, text=True)
+    assert proc.returncode == 0, proc.stderr
+    includes = re.findall(r"#include\s*[<\"]([^>\"]+)", open(HEADER).read())
+    assert all(not i.startswith(("cuda", "torch", "ATen")) for i in includes), includes
+
+
 def test_version_and_defaults():
     lib = N.lib()
     assert b"sm_100a" in lib.ufem_version()
