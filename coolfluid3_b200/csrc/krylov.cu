@@ -1628,11 +1628,16 @@ constexpr int kMaxDevices = 64;
 
 // Device address of g_noalloc_scratch on the current device, looked up once per
 // device (the host-side symbol is only a stand-in and must not reach a kernel).
+// The cache is read and written under a mutex, so first calls from several host
+// threads do not race.  cudaDeviceReset ends every handle of the library and the
+// cached addresses with them: the library is not used after a reset.
 int noalloc_scratch(double** out) {
+  static std::mutex mu;
   static double* addr[kMaxDevices] = {};
   int dev = 0;
   UFEM_CUDA_TRY(cudaGetDevice(&dev));
   if (dev < 0 || dev >= kMaxDevices) return set_error(UFEM_ERR_LIMIT, "device ordinal out of range");
+  std::lock_guard<std::mutex> lk(mu);
   if (!addr[dev]) {
     void* p = nullptr;
     UFEM_CUDA_TRY(cudaGetSymbolAddress(&p, g_noalloc_scratch));
@@ -1680,9 +1685,21 @@ extern "C" int ufem_ns_solve_noalloc(ufem_ns_handle* h, const ufem_krylov_opts* 
   kw.h_dctl = h_d;
   kw.h_ictl = h_i;
   SolveResult r;
-  rc = bicgstab<double, double, double>(h, kw, h->d_vals, h->d_rhs, h->d_sol, vec[0], vec[1], vec[2], vec[3], vec[4],
-                                        vec[5], vec[6], vec[7], vec[8], o.precond, o.tol, o.max_iters, s, r);
-  if (rc) return rc;
+  // the restart rule of ufem_ns_solve: after a breakdown, or when the recursive
+  // residual met the tolerance while the true one had drifted above it, restart
+  // from the current iterate while iterations remain
+  int used = 0;
+  for (int restarts = 0;; ++restarts) {
+    rc = bicgstab<double, double, double>(h, kw, h->d_vals, h->d_rhs, h->d_sol, vec[0], vec[1], vec[2], vec[3], vec[4],
+                                          vec[5], vec[6], vec[7], vec[8], o.precond, o.tol, o.max_iters - used, s, r);
+    if (rc) return rc;
+    used += r.iters;
+    if ((r.status == 2 || r.status == 1) && !r.converged && std::isfinite(r.relres) && used < o.max_iters &&
+        restarts < kMaxRestarts)
+      continue;
+    break;
+  }
+  r.iters = used;
   ufem_krylov_status st{};
   st.converged = r.converged;
   st.status = r.status;

@@ -225,7 +225,8 @@ int ufem_ns_solve(ufem_ns_handle* h, const ufem_krylov_opts* kopts, ufem_krylov_
  * of device memory, held on every GPU that loads the library until the process
  * exits) and calls no cudaMalloc, cudaFree or allocating library routine.
  *  - Solves the system the handle holds: BiCGStab (method 1) with point Jacobi or
- *    no preconditioner, FP64 (mixed = 0); other options give UFEM_ERR_ARG.
+ *    no preconditioner, FP64 (mixed = 0), restarted from its iterate after a
+ *    breakdown as ufem_ns_solve restarts it; other options give UFEM_ERR_ARG.
  *  - At most UFEM_NOALLOC_MAX_ROWS rows; larger systems give UFEM_ERR_LIMIT.
  *  - The first call on a device looks up the scratch area's device address; make
  *    that first call before any stream capture.

@@ -63,6 +63,7 @@ _SIG = {
     "orc_update": (None, [C.c_void_p]),
     "orc_step": (C.c_int, [C.c_void_p, C.c_int, C.c_double, C.c_int, C.c_int, C.c_int]),
     "orc_time_assembly": (C.c_double, [C.c_void_p, C.c_int, C.c_int]),
+    "orc_time_step_assembly": (C.c_double, [C.c_void_p, C.c_int, C.c_int]),
     "orc_element": (None, [C.c_void_p, C.c_int64, _D, _D, _D]),
     "orc_tau": (None, [C.c_int, C.c_int, _D, _D, C.c_double, C.c_double, C.c_double, C.c_double, _D]),
     "orc_semi_create": (C.c_void_p, [C.c_int, C.c_int64, C.c_int64, _D, _U32, C.POINTER(OrcOptions), C.c_int, _U32,
@@ -137,6 +138,57 @@ def tau(dim, supg_type, X, uc, nu, dt, c1=1.0, c2=16.0):
     out = np.empty(3)
     lib().orc_tau(dim, supg_type, _d(X), _d(uc), nu, dt, c1, c2, _d(out))
     return out  # tau_ps, tau_su, tau_bulk
+
+
+def lid_driven_problem(dim, n, nu, dt, seed=20261203):
+    """The seeded lid-driven cavity of the benchmark, built without the product
+    library: the oracle's own mesh generators (bitwise equal to the product's),
+    sine-mode initial velocities (4 modes in 2D, 6 in 3D, phases and wavenumbers
+    from numpy's default_rng(seed + 1)), the NavierStokes initial conditions and
+    the ordered Dirichlet list (walls, then the lid, pressure pinned at node 0).
+    Returns a dict of the arrays; tests/test_oracle.py checks it against the
+    product's problem generator bitwise."""
+    import math
+    if dim == 2:
+        coords, conn = mesh_rectangle_tris(n, n, 0.2, seed)
+        modes = 4
+    else:
+        coords, conn = mesh_cube_tets(n, 0.15, seed)
+        modes = 6
+    npts = coords.shape[0]
+    rng = np.random.default_rng(seed + 1)
+    u = np.zeros((npts, dim))
+    for _ in range(modes):
+        for c in range(dim):
+            k = rng.integers(1, 4, size=dim)
+            ph = rng.uniform(0.0, 2.0 * math.pi, size=dim)
+            term = np.ones(npts)
+            for a in range(dim):
+                term = term * np.sin(math.pi * k[a] * coords[:, a] + ph[a])
+            u[:, c] += (1.0 / modes) * term
+    up = np.zeros((npts, dim + 1))
+    up[:, :dim] = u
+    lin = np.ascontiguousarray(np.tile(u, (1, 4)))
+    nuv = np.full(npts, nu)
+    s = n + 1
+    idx = np.arange(s ** dim)
+    ijk = (idx % s, idx // s) if dim == 2 else (idx % s, (idx // s) % s, idx // (s * s))
+    walls = [ijk[0] == 0, ijk[0] == n, ijk[1] == 0] + ([] if dim == 2 else [ijk[1] == n, ijk[2] == 0])
+    lid = ijk[1] == n if dim == 2 else ijk[2] == n
+    nodes, comps, vals = [], [], []
+    for mask, v in [(m, 0.0) for m in walls] + [(lid, 1.0)]:
+        ids = np.nonzero(mask)[0].astype(np.uint32)
+        cc = np.tile(np.arange(dim, dtype=np.int32), len(ids))
+        vv = np.zeros(len(ids) * dim)
+        vv[cc == 0] = v
+        nodes.append(np.repeat(ids, dim))
+        comps.append(cc)
+        vals.append(vv)
+    nodes.append(np.array([0], np.uint32))
+    comps.append(np.array([dim], np.int32))
+    vals.append(np.array([0.0]))
+    return dict(coords=coords, conn=conn, up=up, lin=lin, nu=nuv, dt=dt,
+                bc_nodes=np.concatenate(nodes), bc_comps=np.concatenate(comps), bc_values=np.concatenate(vals))
 
 
 class LSS:
@@ -301,6 +353,10 @@ class Oracle:
 
     def time_assembly(self, nthreads=1, reps=1) -> float:
         return lib().orc_time_assembly(self._h, nthreads, reps)
+
+    def time_step_assembly(self, nthreads=1, reps=1) -> float:
+        """Seconds for `reps` of ZeroLSS + LinearizeU + assembly + symmetric Dirichlet."""
+        return lib().orc_time_step_assembly(self._h, nthreads, reps)
 
     def element(self, e):
         nd = (self.dim + 1) ** 2

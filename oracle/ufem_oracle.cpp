@@ -1262,6 +1262,21 @@ double orc_time_assembly(void* h, int nthreads, int reps) {
   return std::chrono::duration<double>(t1 - t0).count();
 }
 
+// The GPU benchmark's step on the host: ZeroLSS + LinearizeU + assembly
+// (nthreads node-partitioned threads) + the symmetric Dirichlet conditions in
+// their order, as DirichletBC applies them after the assembly
+// (Proto/DirichletBC.hpp:34-51).  Seconds for `reps` steps.
+double orc_time_step_assembly(void* h, int nthreads, int reps) {
+  Oracle* S = static_cast<Oracle*>(h);
+  const auto t0 = std::chrono::steady_clock::now();
+  for (int r = 0; r < reps; ++r) {
+    assemble(*S, nthreads);
+    apply_bcs(*S);
+  }
+  const auto t1 = std::chrono::steady_clock::now();
+  return std::chrono::duration<double>(t1 - t0).count();
+}
+
 // Element-level access for known-answer tests: A, T (nd x nd) and a (nd) of one
 // element before the combine step, element-major dof order.
 void orc_element(void* h, int64_t e, double* A, double* T, double* av) {

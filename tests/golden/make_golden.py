@@ -5,8 +5,8 @@ build_commpattern, the set_row / symmetric_dirichlet calls and every
 BOOST_CHECK_EQUAL of test_complete_system), with each rank's local indices
 mapped to global node ids.  Note the reference's get_value(icol, irow) order.
 
-Run where the reference tree is available:
-    python tests/golden/make_golden.py /root/reference
+Run where the reference tree is available, with its root as the argument:
+    python tests/golden/make_golden.py <reference root>
 """
 from __future__ import annotations
 
@@ -51,7 +51,9 @@ def parse(text: str) -> dict:
 
 
 def main():
-    root = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+    if len(sys.argv) != 2:
+        sys.exit("usage: make_golden.py <reference root>")
+    root = sys.argv[1]
     text = open(os.path.join(root, SRC)).read()
     out = os.path.join(os.path.dirname(os.path.abspath(__file__)), "lss_symmetric_dirichlet_kat.json")
     with open(out, "w") as f:

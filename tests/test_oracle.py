@@ -389,3 +389,13 @@ def test_linearize_first_step_is_u():
     o.assemble()
     _, lin = o.state()
     np.testing.assert_allclose(lin[:, :3], pb.up[:, :3], rtol=0, atol=4e-16)
+
+
+def test_oracle_problem_builder_matches_product_generator():
+    # the reference arm of the benchmark builds its inputs without the product library
+    for dim, n in ((2, 8), (3, 4)):
+        a = P.make_problem(dim, n, nu=1e-3, dt=5e-3)
+        b = O.lid_driven_problem(dim, n, 1e-3, 5e-3)
+        for k in ("coords", "conn", "up", "lin", "nu", "bc_nodes", "bc_comps", "bc_values"):
+            x, y = getattr(a, k), b[k]
+            assert x.dtype == y.dtype and np.array_equal(x, y), k

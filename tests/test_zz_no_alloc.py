@@ -49,12 +49,20 @@ def test_noalloc_solve_matches_allocating_solve(dim, n):
     assert st_ref["converged"] == 1
 
     ns = _system(dim, n)  # a second handle that never allocates a Krylov workspace
+    import torch
+    bytes0 = ns.device_bytes()  # counts the handle's Krylov workspace once one exists
+    free0, _ = torch.cuda.mem_get_info()
     results = []
     for _ in range(2):  # two calls in a row share the scratch area
         ns.set_solution(np.zeros(ns.nb_rows))
         st = _noalloc(ns, opts)
         assert st.converged == 1 and st.rel_residual <= 1e-12
         results.append(ns.solution())
+    torch.cuda.synchronize()
+    free1, _ = torch.cuda.mem_get_info()
+    # nothing was allocated: no Krylov workspace on the handle, no drop in free device memory
+    assert ns.device_bytes() == bytes0
+    assert free1 >= free0, (free0, free1)
     for x in results:
         assert np.linalg.norm(x - x_ref) <= 1e-10 * np.linalg.norm(x_ref)
     ns.close()
