@@ -42,12 +42,26 @@ __device__ __forceinline__ void put_row(T* __restrict__ st, int idx, int CH, con
   }
 }
 
+// Where the element routines send their results.  StageSink stages each row
+// of the element row block and the RHS row in shared memory for the reduction
+// (put_row); the residual kernel's sink folds them into b - M dx instead.
+template <typename T>
+struct StageSink {
+  T* __restrict__ st;
+  T* __restrict__ rst;
+  int CH;
+  template <int NEQ>
+  __device__ __forceinline__ void row(int idx, const T (&v)[NEQ]) { put_row<NEQ, T>(st, idx, CH, v); }
+  template <int NEQ>
+  __device__ __forceinline__ void rhs(const T (&v)[NEQ]) { put_row<NEQ, T>(rst, 0, CH, v); }
+};
+
 // Shared tail of both element forms: rhs row a, M = invdt*T + theta*A with the
 // p row of A divided by theta first (NavierStokesAssembly.hpp:69-71), staged.
-template <int D, typename T>
+template <int D, typename T, typename Sink>
 __device__ __forceinline__ void stage_block(const T (&A)[D + 1][D + 1], const T (&Tm)[D + 1][D + 1],
                                             const T (&xb)[D + 1], const KParams<T>& kp, T (&rhs)[D + 1],
-                                            T* __restrict__ st, int b, int CH) {
+                                            Sink& sk, int b) {
   constexpr int neq = D + 1;
 #pragma unroll
   for (int r = 0; r < neq; ++r) {
@@ -61,7 +75,7 @@ __device__ __forceinline__ void stage_block(const T (&A)[D + 1][D + 1], const T 
       const T a = (r == D) ? A[r][c] * kp.inv_theta : A[r][c];  // _A(p) / theta
       row[c] = kp.invdt * Tm[r][c] + kp.theta * a;
     }
-    put_row<neq, T>(st, (b * neq + r) * neq, CH, row);
+    sk.template row<neq>((b * neq + r) * neq, row);
   }
 }
 
@@ -101,10 +115,9 @@ __device__ __forceinline__ void load_state(const NodeData& nd, int node, T (&x)[
 // (tests/test_gpu_parity.py checks the result against the oracle's literal
 // quadrature).
 // ---------------------------------------------------------------------------
-template <int D, typename T>
+template <int D, typename T, typename Sink>
 __device__ __forceinline__ void generic_row(const int (&ids)[4], int a, const NodeData& nd,
-                                            const double* __restrict__ force, const KParams<T>& kp,
-                                            T* __restrict__ st, T* __restrict__ rst, int CH) {
+                                            const double* __restrict__ force, const KParams<T>& kp, Sink& sk) {
   constexpr int n = D + 1, neq = D + 1;
   const T inv_n = T(1.0 / n);
   const T nT = T(n), n2 = T(n * n);
@@ -245,7 +258,7 @@ __device__ __forceinline__ void generic_row(const int (&ids)[4], int a, const No
 #pragma unroll
       for (int j = 0; j < D; ++j) row[j] = tg * G[j][b] + (i == j ? diag : T(0));
       row[D] = G[i][b] * thS;
-      put_row<neq, T>(st, (b * neq + i) * neq, CH, row);
+      sk.template row<neq>((b * neq + i) * neq, row);
     }
     // row p: theta * (A / theta) + invdt * T = A + invdt * T
     {
@@ -253,7 +266,7 @@ __device__ __forceinline__ void generic_row(const int (&ids)[4], int a, const No
 #pragma unroll
       for (int j = 0; j < D; ++j) row[j] = G[j][b] * sWSp + (cj[j] * Vab + ej[j]);
       row[D] = D0[b] * tpv;
-      put_row<neq, T>(st, (b * neq + D) * neq, CH, row);
+      sk.template row<neq>((b * neq + D) * neq, row);
     }
     // pieces of A x
 #pragma unroll
@@ -275,7 +288,7 @@ __device__ __forceinline__ void generic_row(const int (&ids)[4], int a, const No
     g0gp += G[k][0] * gradp[k];
   }
   rrow[D] = -(sWSp * div + tps * g0ax + tps * V * inv_rho * g0gp);
-  put_row<neq, T>(rst, 0, CH, rrow);
+  sk.template rhs<neq>(rrow);
 }
 
 // ---------------------------------------------------------------------------
@@ -323,8 +336,9 @@ __device__ __forceinline__ void spec_tau_common(const KParams<T>& kp, const Elem
   compute_tau<D, T>(dk, el, uc, nu, G, g, det, tps, tsu, tbu);
 }
 
-template <typename T>
-__device__ __forceinline__ void spec_tri_row(const int (&ids)[4], int ai, const NodeData& nd, const KParams<T>& kp, T* __restrict__ st, T* __restrict__ rst, int CH) {
+template <typename T, typename Sink>
+__device__ __forceinline__ void spec_tri_row(const int (&ids)[4], int ai, const NodeData& nd, const KParams<T>& kp,
+                                             Sink& sk) {
   Elem<2, T> el;
   gather_geometry_uadv<2, T>(ids, nd, el);
   T u_avg[2];
@@ -408,15 +422,16 @@ __device__ __forceinline__ void spec_tri_row(const int (&ids)[4], int ai, const 
     Tm[0][0] += val; Tm[1][1] += val;
     val = ps6;
     Tm[2][0] += val * nix; Tm[2][1] += val * niy;
-    stage_block<2, T>(A, Tm, xs[j], kp, rhs, st, j, CH);
+    stage_block<2, T>(A, Tm, xs[j], kp, rhs, sk, j);
   }
-  put_row<3, T>(rst, 0, CH, rhs);
+  sk.template rhs<3>(rhs);
 }
 
 // Specialised tetrahedra, NavierStokesSpecializations.hpp:150-302, row i = a,
 // including the reference's use of vk in the W rows (:224-226, :236-238).
-template <typename T>
-__device__ __forceinline__ void spec_tet_row(const int (&ids)[4], int ai, const NodeData& nd, const KParams<T>& kp, T* __restrict__ st, T* __restrict__ rst, int CH) {
+template <typename T, typename Sink>
+__device__ __forceinline__ void spec_tet_row(const int (&ids)[4], int ai, const NodeData& nd, const KParams<T>& kp,
+                                             Sink& sk) {
   Elem<3, T> el;
   gather_geometry_uadv<3, T>(ids, nd, el);
   T u_avg[3];
@@ -530,9 +545,9 @@ __device__ __forceinline__ void spec_tet_row(const int (&ids)[4], int ai, const 
     Tm[0][0] += val; Tm[1][1] += val; Tm[2][2] += val;
     val = ps12;
     Tm[3][0] += val * ni[XX]; Tm[3][1] += val * ni[YY]; Tm[3][2] += val * ni[ZZ];
-    stage_block<3, T>(A, Tm, xs[j], kp, rhs, st, j, CH);
+    stage_block<3, T>(A, Tm, xs[j], kp, rhs, sk, j);
   }
-  put_row<4, T>(rst, 0, CH, rhs);
+  sk.template rhs<4>(rhs);
 }
 
 // Shared memory of one chunk: staged row blocks [value][incidence] (T), staged
@@ -616,11 +631,12 @@ __global__ void __launch_bounds__(CH) ns_assembly_kernel(
     s_info[t] = pslots;
     const KParams<T> kp = make_kparams<T>(p);
     const NodeData nd{coords, uadv, state, node32};
+    StageSink<T> sk{st + t, rst + t, CH};
     if constexpr (SPEC) {
-      if constexpr (D == 2) spec_tri_row<T>(ids, a, nd, kp, st + t, rst + t, CH);
-      else spec_tet_row<T>(ids, a, nd, kp, st + t, rst + t, CH);
+      if constexpr (D == 2) spec_tri_row<T>(ids, a, nd, kp, sk);
+      else spec_tet_row<T>(ids, a, nd, kp, sk);
     } else {
-      generic_row<D, T>(ids, a, nd, force, kp, st + t, rst + t, CH);
+      generic_row<D, T>(ids, a, nd, force, kp, sk);
     }
     // contributor masks: bit = position of this incidence within its row
     int lo = 0, hi = R - 1;
@@ -925,11 +941,12 @@ __global__ void __launch_bounds__(32 * WPB, warp_min_blocks<D, T, KC, WPB>()) ns
       T* st = stage + lane * LS;
       const KParams<T> kp = make_kparams<T>(UFEM_F(cs, p));
       const NodeData nd{UFEM_F(cs, coords), UFEM_F(cs, uadv), UFEM_F(cs, state), UFEM_F(cs, node32)};
+      StageSink<T> sk{st, st + nvals, 1};
       if constexpr (SPEC) {
-        if constexpr (D == 2) spec_tri_row<T>(ids, a, nd, kp, st, st + nvals, 1);
-        else spec_tet_row<T>(ids, a, nd, kp, st, st + nvals, 1);
+        if constexpr (D == 2) spec_tri_row<T>(ids, a, nd, kp, sk);
+        else spec_tet_row<T>(ids, a, nd, kp, sk);
       } else {
-        generic_row<D, T>(ids, a, nd, UFEM_F(cs, force), kp, st, st + nvals, 1);
+        generic_row<D, T>(ids, a, nd, UFEM_F(cs, force), kp, sk);
       }
 #pragma unroll
       for (int q = 1; q < n; ++q) atomicOr(s_mask + (q - 1) * 64 + ((pslots >> (8 * q)) & 0xFFu), 1u << lane);
@@ -1326,6 +1343,117 @@ int set_smem_attr() {
   return UFEM_OK;
 }
 
+// ---------------------------------------------------------------------------
+// Matrix-free FP64 residual.  The refinement residual of the mixed-precision
+// solve when the element matrices are assembled in FP32: for the current
+// increment dx, r = b - M dx of the FP64 system that the FP64 assembly and the
+// symmetric Dirichlet conditions would have built, evaluated element by element
+// without forming M.  Per incidence (row node, element) the FP64 element
+// routines run with a sink that applies each row of M = invdt T + theta A
+// (NavierStokesAssembly.hpp:69-71) to the element's increment instead of staging
+// it, and keeps the RHS row a - A x (the reference's system_rhs += -_A _x + _a,
+// :69); the rows' contributions are then summed in element order.
+// Constrained columns take the value of their dof's first application (what the
+// symmetric Dirichlet pass moves to the RHS), constrained rows get r = 0 (their
+// increment already holds the row value, which the inner corrections keep).
+// ---------------------------------------------------------------------------
+template <int D>
+struct ResidSink {
+  double dl[D + 1][D + 1];  // increment of the relabelled element nodes (u, v, [w], p)
+  double acc[D + 1];        // (M dx) of the row
+  double rr[D + 1];         // a - A x of the row
+  template <int NEQ>
+  __device__ __forceinline__ void row(int idx, const double (&v)[NEQ]) {
+    const int b = idx / (NEQ * NEQ), r = (idx / NEQ) % NEQ;
+    double s = 0.0;
+#pragma unroll
+    for (int c = 0; c < NEQ; ++c) s += v[c] * dl[b][c];
+    acc[r] += s;
+  }
+  template <int NEQ>
+  __device__ __forceinline__ void rhs(const double (&v)[NEQ]) {
+#pragma unroll
+    for (int r = 0; r < NEQ; ++r) rr[r] = v[r];
+  }
+};
+
+// One CTA per chunk of whole rows (the chunk plan), one thread per incidence.
+template <int D, int CH, bool SPEC>
+__global__ void __launch_bounds__(CH) ns_residual_kernel(
+    const int2* __restrict__ chunk_rows, const int32_t* __restrict__ row_inc, const int32_t* __restrict__ inc_elem,
+    const uint32_t* __restrict__ inc_info, const int4* __restrict__ conn, const double* __restrict__ coords,
+    const double* __restrict__ uadv, const double* __restrict__ state, const double* __restrict__ force, NSParams p,
+    const double* __restrict__ dx, double* __restrict__ res) {
+  constexpr int n = D + 1, neq = D + 1;
+  __shared__ double s_res[neq * CH];
+  __shared__ int s_rowinc[CH + 1];
+  const int2 cr = chunk_rows[blockIdx.x];
+  const int row0 = cr.x, R = cr.y - cr.x;  // 1 <= R <= K <= CH
+  const int inc0 = row_inc[row0];
+  const int K = row_inc[cr.y] - inc0;
+  const int t = threadIdx.x;
+  for (int rl = t; rl <= R; rl += CH) s_rowinc[rl] = row_inc[row0 + rl] - inc0;
+  if (t < K) {
+    const int k = inc0 + t;
+    const int e = __ldg(inc_elem + k);
+    const int a = int(__ldg(inc_info + k) >> 24) & 3;
+    const int4 cn = __ldg(conn + e);
+    const int ids0[4] = {cn.x, cn.y, cn.z, cn.w};
+    int ids[4];
+#pragma unroll
+    for (int q = 0; q < 4; ++q) ids[q] = ids0[(D == 3) ? (q ^ a) : (q < 3 ? (q + a) % 3 : 3)];
+    ResidSink<D> sk;
+#pragma unroll
+    for (int q = 0; q < n; ++q)
+#pragma unroll
+      for (int c = 0; c < neq; ++c) sk.dl[q][c] = __ldg(dx + int64_t(ids[q]) * neq + c);
+#pragma unroll
+    for (int r = 0; r < neq; ++r) sk.acc[r] = 0.0;
+    const KParams<double> kp = make_kparams<double>(p);
+    const NodeData nd{coords, uadv, state, nullptr};
+    if constexpr (SPEC) {
+      if constexpr (D == 2) spec_tri_row<double>(ids, a, nd, kp, sk);
+      else spec_tet_row<double>(ids, a, nd, kp, sk);
+    } else {
+      generic_row<D, double>(ids, a, nd, force, kp, sk);
+    }
+#pragma unroll
+    for (int r = 0; r < neq; ++r) s_res[r * CH + t] = sk.rr[r] - sk.acc[r];
+  }
+  __syncthreads();
+  for (int it = t; it < R * neq; it += CH) {  // sums over the row's incidences in element order
+    const int rl = it / neq, r = it - rl * neq;
+    double acc = 0.0;
+    for (int kk = s_rowinc[rl]; kk < s_rowinc[rl + 1]; ++kk) acc += s_res[r * CH + kk];
+    res[int64_t(row0 + rl) * neq + r] = acc;
+  }
+}
+
+// dx' = dx with each constrained dof replaced by its first application's value
+// (value - old), the column value the symmetric Dirichlet pass moves to the RHS.
+__global__ void mf_columns_kernel(int64_t nbc, const int64_t* __restrict__ bc_dof, const double* __restrict__ vfirst,
+                                  double* __restrict__ dxp) {
+  const int64_t u = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (u < nbc) dxp[bc_dof[u]] = vfirst[u];
+}
+
+__global__ void mf_rows_kernel(int64_t nbc, const int64_t* __restrict__ bc_dof, double* __restrict__ res) {
+  const int64_t u = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (u < nbc) res[bc_dof[u]] = 0.0;
+}
+
+template <int D, int CH, bool SPEC>
+int launch_residual_t(ufem_ns_handle* h, const double* dxp, double* res, cudaStream_t s) {
+  NSParams p;
+  fill_params(h, p);
+  if (h->plan64.cap != CH) return set_error(UFEM_ERR_STATE, "chunk plan does not match the residual kernel width");
+  ns_residual_kernel<D, CH, SPEC><<<h->plan64.nchunks, CH, 0, s>>>(
+      h->plan64.chunks, h->d_row_inc, h->d_inc_elem, h->d_inc_info, reinterpret_cast<const int4*>(h->d_conn),
+      h->d_coords, h->d_uadv, h->d_state, h->d_force, p, dxp, res);
+  UFEM_CUDA_TRY(cudaGetLastError());
+  return UFEM_OK;
+}
+
 constexpr int kChunk2D = 256;
 constexpr int kChunk3D64 = 128;
 constexpr int kChunk3D32 = 256;
@@ -1499,6 +1627,38 @@ int launch_dirichlet(ufem_ns_handle* h, cudaStream_t s) {
                                                         h->d_rowptr, h->d_state, h->d_vals, h->d_vals32, h->d_rhs,
                                                         h->d_sol);
   UFEM_CUDA_TRY(cudaGetLastError());
+  return UFEM_OK;
+}
+
+}  // namespace ufem
+
+namespace ufem {
+
+int launch_mf_residual(ufem_ns_handle* h, double* dx_work, double* res, cudaStream_t s) {
+  if (h->ntie > 0)
+    return set_error(UFEM_ERR_ARG, "the matrix-free FP64 residual does not support periodic node links");
+  const DirichletPlan& bp = h->bcp;
+  UFEM_CUDA_TRY(cudaMemcpyAsync(dx_work, h->d_sol, size_t(h->nrows) * 8, cudaMemcpyDeviceToDevice, s));
+  if (bp.nbc > 0) {
+    mf_columns_kernel<<<unsigned((bp.nbc + 255) / 256), 256, 0, s>>>(bp.nbc, bp.bc_dof, bp.vfirst, dx_work);
+    UFEM_CUDA_TRY(cudaGetLastError());
+  }
+  const bool spec = h->opt.use_specializations != 0;
+  int rc;
+  if (h->dim == 2)
+    rc = spec ? launch_residual_t<2, kChunk2D, true>(h, dx_work, res, s) : launch_residual_t<2, kChunk2D, false>(h, dx_work, res, s);
+  else
+    rc = spec ? launch_residual_t<3, kChunk3D64, true>(h, dx_work, res, s)
+              : launch_residual_t<3, kChunk3D64, false>(h, dx_work, res, s);
+  if (rc) return rc;
+  if (bp.nneu > 0) {
+    neumann_kernel<<<unsigned((bp.nneu + 255) / 256), 256, 0, s>>>(bp.nneu, bp.neu_dof, bp.neu_ptr, bp.neu_val, res);
+    UFEM_CUDA_TRY(cudaGetLastError());
+  }
+  if (bp.nbc > 0) {
+    mf_rows_kernel<<<unsigned((bp.nbc + 255) / 256), 256, 0, s>>>(bp.nbc, bp.bc_dof, res);
+    UFEM_CUDA_TRY(cudaGetLastError());
+  }
   return UFEM_OK;
 }
 

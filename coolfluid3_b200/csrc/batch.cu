@@ -1186,6 +1186,8 @@ int ufem_batch_solve(ufem_batch* b, const ufem_krylov_opts* kopts, ufem_krylov_s
   if (o.tol <= 0) o.tol = 1e-10;
   if (o.max_refine <= 0) o.max_refine = 20;
   if (o.inner_tol <= 0) o.inner_tol = 1e-3;
+  if (o.mixed < 0 || o.mixed > 1)
+    return set_error(UFEM_ERR_ARG, "batches refine with the FP64 residual of the stored system: mixed must be 0 or 1");
   const bool mixed = o.mixed != 0;
   cudaStream_t st = static_cast<cudaStream_t>(stream);
   int rc;

@@ -1195,6 +1195,12 @@ int ufem_ns_solve(ufem_ns_handle* h, const ufem_krylov_opts* kopts, ufem_krylov_
   return UFEM_OK;
 }
 
+int ufem_ns_fp64_residual(ufem_ns_handle* h, double* r, void* stream) {
+  if (!h || !r) return set_error(UFEM_ERR_ARG, "NULL argument");
+  if (!h->state_set) return set_error(UFEM_ERR_STATE, "set the state before asking for the residual");
+  return krylov_fp64_residual(h, r, static_cast<cudaStream_t>(stream));
+}
+
 int ufem_ns_update(ufem_ns_handle* h, void* stream) {
   if (!h) return set_error(UFEM_ERR_ARG, "NULL handle");
   cudaStream_t s = static_cast<cudaStream_t>(stream);
@@ -1258,6 +1264,11 @@ int ufem_ns_apply(ufem_ns_handle* h, const double* x, double* y) {
   if ((rc = krylov_apply(h, h->d_x, h->d_y, nullptr))) return rc;
   UFEM_CUDA_TRY(cudaMemcpy(y, h->d_y, size_t(h->nrows) * 8, cudaMemcpyDeviceToHost));
   return UFEM_OK;
+}
+
+int ufem_ns_apply_device(ufem_ns_handle* h, const double* d_x, double* d_y, void* stream) {
+  if (!h || !d_x || !d_y) return set_error(UFEM_ERR_ARG, "NULL argument");
+  return krylov_apply(h, d_x, d_y, static_cast<cudaStream_t>(stream));
 }
 
 int ufem_ns_enable_timing(ufem_ns_handle* h, int32_t enable) {

@@ -214,6 +214,9 @@ int launch_assembly_batch(int dim, int precision, bool spec, int warps, int ngro
 int launch_dirichlet(ufem_ns_handle* h, cudaStream_t s);
 // Adds the constant Neumann contributions to the RHS (before the Dirichlet passes).
 int launch_neumann(ufem_ns_handle* h, cudaStream_t s);
+// r = b - M dx of the FP64 system (FP64 element pass, no matrix), dx = h->d_sol;
+// dx_work: nrows scratch doubles (assembly.cu).
+int launch_mf_residual(ufem_ns_handle* h, double* dx_work, double* res, cudaStream_t s);
 
 // bcfunction.cu: Dirichlet values from expressions of (x, y, z, t)
 constexpr int kExprMaxDepth = 32;
@@ -245,6 +248,7 @@ void destroy_handle(ufem_ns_handle* h);
 // Krylov (krylov.cu)
 int krylov_solve(ufem_ns_handle* h, const ufem_krylov_opts* ko, ufem_krylov_status* st, cudaStream_t s);
 int krylov_apply(ufem_ns_handle* h, const double* d_x, double* d_y, cudaStream_t s);
+int krylov_fp64_residual(ufem_ns_handle* h, double* r_host, cudaStream_t s);
 void krylov_free(ufem_ns_handle* h);
 // Aggregates of the two-level CG preconditioner (precond 3) of a one-equation
 // system: agg[row] in [0, nc) or -1; builds and inverts the Galerkin coarse

@@ -331,6 +331,21 @@ __global__ void residual_kernel(int64_t n, const BT* __restrict__ b, const VT* _
   }
 }
 
+// Partial sums of ||r||^2 and ||b||^2 (per block), no update.
+__global__ void norm2_partials_kernel(int64_t n, const double* __restrict__ r, const double* __restrict__ b,
+                                      double* __restrict__ rpart, double* __restrict__ bpart) {
+  __shared__ double sm[32];
+  double s2 = 0.0, b2 = 0.0;
+  GRID_STRIDE(i, n) {
+    s2 += r[i] * r[i];
+    b2 += b[i] * b[i];
+  }
+  s2 = block_sum(s2, sm);
+  if (threadIdx.x == 0) rpart[blockIdx.x] = s2;
+  b2 = block_sum(b2, sm);
+  if (threadIdx.x == 0) bpart[blockIdx.x] = b2;
+}
+
 // Restart: beta = ||r||, g = beta e1, done if converged.
 __global__ void restart_setup_kernel(int nblk, int m, const double* __restrict__ normpart,
                                      const double* __restrict__ bpart, int first, double* __restrict__ g,
@@ -1356,6 +1371,7 @@ int krylov_solve(ufem_ns_handle* h, const ufem_krylov_opts* ko, ufem_krylov_stat
     return set_error(UFEM_ERR_ARG, "the two-level preconditioner needs CG on a one-equation system with aggregates set");
   if (o.method < 0 || o.method > 2)
     return set_error(UFEM_ERR_ARG, "method must be 0 (GMRES), 1 (BiCGStab) or 2 (CG)");
+  if (o.mixed < 0 || o.mixed > 2) return set_error(UFEM_ERR_ARG, "mixed must be 0, 1 or 2");
   const bool mixed = o.mixed != 0;
   const bool use_cg = o.method == 2;
   const bool bicg = o.method == 1 || use_cg;  // CG uses the BiCGStab work vectors
@@ -1412,10 +1428,18 @@ int krylov_solve(ufem_ns_handle* h, const ufem_krylov_opts* ko, ufem_krylov_stat
     double relres = 0.0;
     bool conv = false;
     for (ref = 0; ref <= o.max_refine; ++ref) {
-      // r = b - A x in FP64
-      if ((rc = spmv<double, double>(h, h->d_vals, h->d_sol, kw.w, nullptr, s))) return rc;
-      residual_kernel<double, double><<<g1, kRedThreads, 0, s>>>(n, h->d_rhs, kw.w, kw.r, kw.part,
-                                                                 kw.part + kw.nblk);
+      if (o.mixed == 2) {
+        // r = b - M x of the FP64 system from the FP64 element pass (no FP64
+        // matrix needed: the stored one may hold FP32 element arithmetic);
+        // ||b|| is taken from the assembled RHS
+        if ((rc = launch_mf_residual(h, kw.w, kw.r, s))) return rc;
+        norm2_partials_kernel<<<g1, kRedThreads, 0, s>>>(n, kw.r, h->d_rhs, kw.part, kw.part + kw.nblk);
+      } else {
+        // r = b - A x in FP64
+        if ((rc = spmv<double, double>(h, h->d_vals, h->d_sol, kw.w, nullptr, s))) return rc;
+        residual_kernel<double, double><<<g1, kRedThreads, 0, s>>>(n, h->d_rhs, kw.w, kw.r, kw.part,
+                                                                   kw.part + kw.nblk);
+      }
       finalize_norm_kernel<<<1, 1, 0, s>>>(kw.nblk, kw.part, kw.dctl, kScale, 1);
       finalize_norm_kernel<<<1, 1, 0, s>>>(kw.nblk, kw.part + kw.nblk, kw.dctl, kR2, 1);
       UFEM_CUDA_TRY(cudaMemcpyAsync(kw.h_dctl, kw.dctl, 16 * sizeof(double), cudaMemcpyDeviceToHost, s));
@@ -1584,6 +1608,16 @@ int krylov_set_coarse(ufem_ns_handle* h, const std::vector<int32_t>& agg, int nc
 }
 
 int krylov_coarse_size(const ufem_ns_handle* h) { return h->kw ? h->kw->nc : 0; }
+
+int krylov_fp64_residual(ufem_ns_handle* h, double* r_host, cudaStream_t s) {
+  int rc;
+  if ((rc = ensure_work(h, 30, false, true))) return rc;
+  KrylovWork& kw = *h->kw;
+  if ((rc = launch_mf_residual(h, kw.w, kw.r, s))) return rc;
+  UFEM_CUDA_TRY(cudaMemcpyAsync(r_host, kw.r, size_t(h->nrows) * 8, cudaMemcpyDeviceToHost, s));
+  UFEM_CUDA_TRY(cudaStreamSynchronize(s));
+  return UFEM_OK;
+}
 
 int krylov_apply(ufem_ns_handle* h, const double* d_x, double* d_y, cudaStream_t s) {
   return spmv<double, double>(h, h->d_vals, d_x, d_y, nullptr, s);

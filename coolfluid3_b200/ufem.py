@@ -31,14 +31,23 @@ def _stream(stream) -> C.c_void_p | None:
 
 
 def krylov_options(method: str = "bicgstab", restart: int = 30, max_iters: int = 3000, precond: str = "jacobi",
-                   tol: float = 1e-10, mixed: bool = False, max_refine: int = 20, inner_tol: float = 1e-3):
+                   tol: float = 1e-10, mixed: bool | str = False, max_refine: int = 20, inner_tol: float = 1e-3):
+    """mixed: False (FP64), True (FP32 inner solves, FP64 residual of the stored
+    system) or "matrix_free" (FP32 inner solves on the stored system, FP64
+    residual of the FP64 element expressions: with precision="fp32" elements
+    the answer is the FP64 system's)."""
     o = N.KrylovOpts()
     o.method = {"gmres": 0, "bicgstab": 1, "cg": 2}[method]
     o.restart = restart
     o.max_iters = max_iters
     o.precond = {"none": 0, "jacobi": 1, "block_jacobi": 2, "two_level": 3}[precond]
     o.tol = tol
-    o.mixed = 1 if mixed else 0
+    if isinstance(mixed, str):
+        if mixed != "matrix_free":
+            raise ValueError("mixed must be a bool or 'matrix_free'")
+        o.mixed = 2
+    else:
+        o.mixed = 1 if mixed else 0
     o.max_refine = max_refine
     o.inner_tol = inner_tol
     return o
@@ -285,6 +294,13 @@ class NavierStokes:
         rhs = np.empty(self.nb_rows)
         N.check(self._lib.ufem_ns_get_system(self._h, N.dptr(vals), N.dptr(rhs)))
         return vals, rhs
+
+    def fp64_residual(self, stream=None) -> np.ndarray:
+        """b - M x of the FP64 system for the current solution vector, evaluated
+        element by element without a matrix (after assemble and apply_dirichlet)."""
+        r = np.empty(self.nb_rows)
+        N.check(self._lib.ufem_ns_fp64_residual(self._h, N.dptr(r), _stream(stream)))
+        return r
 
     def apply(self, x: np.ndarray) -> np.ndarray:
         x = np.ascontiguousarray(x, np.float64)

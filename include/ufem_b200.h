@@ -76,7 +76,13 @@ typedef struct ufem_krylov_opts {
   int32_t precond;     /* 0 none, 1 point Jacobi (default), 2 node-block Jacobi,
                           3 two-level (CG, semi-implicit pressure only)          */
   double tol;          /* ||b - A x|| / ||b|| target, default 1e-10                */
-  int32_t mixed;       /* 0: all FP64; 1: FP32 inner Krylov + FP64 refinement     */
+  int32_t mixed;       /* 0: all FP64; 1: FP32 inner Krylov + FP64 refinement
+                          whose residual is b - A x of the stored system; 2: the
+                          same with the residual of the FP64 system evaluated
+                          element by element (no FP64 matrix: the FP32-element
+                          system of precision 1 becomes the inner operator and
+                          the answer is the FP64 system's); single handles only,
+                          no periodic links                                       */
   int32_t max_refine;  /* outer refinement passes when mixed, default 20          */
   double inner_tol;    /* relative tolerance of each inner FP32 solve, 1e-3       */
 } ufem_krylov_opts;
@@ -236,6 +242,15 @@ int ufem_ns_solve(ufem_ns_handle* h, const ufem_krylov_opts* kopts, ufem_krylov_
 #define UFEM_NOALLOC_MAX_ROWS 131072
 int ufem_ns_solve_noalloc(ufem_ns_handle* h, const ufem_krylov_opts* kopts, ufem_krylov_status* status,
                           void* stream);
+/* Residual of the FP64 system for the current solution vector x, evaluated
+ * element by element in FP64 without a matrix (NavierStokesAssembly.hpp:69-71:
+ * b = a - A u over the elements, M = invdt T + theta A): r = b - M x with the
+ * symmetric Dirichlet conditions as ufem_ns_apply_dirichlet sets them
+ * (constrained columns at their first application's value, constrained rows
+ * r = 0) and the Neumann contributions in b.  It is the refinement residual of
+ * mixed = 2 solves.  Call after ufem_ns_assemble and ufem_ns_apply_dirichlet of
+ * the step; r: host buffer of nb_rows doubles.  Not for periodic links. */
+int ufem_ns_fp64_residual(ufem_ns_handle* h, double* r, void* stream);
 /* UpdateActions (NavierStokes.cpp:172-179). */
 int ufem_ns_update(ufem_ns_handle* h, void* stream);
 /* nsteps full time steps; status of the last solve. */
@@ -292,6 +307,10 @@ int ufem_ns_download_system(ufem_ns_handle* h, double* vals, double* rhs, void* 
 int ufem_ns_device_view_get(const ufem_ns_handle* h, ufem_ns_device_view* view);
 /* y = A x (FP64, host buffers) -- LSS::Matrix::apply with alpha=1, beta=0. */
 int ufem_ns_apply(ufem_ns_handle* h, const double* x, double* y);
+/* y = A x with device buffers of nb_rows doubles on `stream` (the SpMV of the
+ * solvers) -- LSS::Matrix::apply (math/LSS/Matrix.hpp) for device-resident
+ * callers such as the distributed solve of a decomposed mesh. */
+int ufem_ns_apply_device(ufem_ns_handle* h, const double* d_x, double* d_y, void* stream);
 
 /* Assembly kernel selection.  No counterpart in the reference (one code path
  * there).  variant 0: warp per group of consecutive rows holding at most 32
