@@ -126,6 +126,7 @@ SIGNATURES = {
     "ufem_ns_device_bytes": (C.c_int, [_P, C.POINTER(C.c_int64)]),
     "ufem_batch_create": (C.c_int, [C.POINTER(_P), C.c_int32, C.POINTER(_P)]),
     "ufem_batch_size": (C.c_int, [_P, C.POINTER(C.c_int32), C.POINTER(C.c_int64)]),
+    "ufem_batch_set_active": (C.c_int, [_P, C.POINTER(C.c_int32)]),
     "ufem_batch_set_graphs": (C.c_int, [_P, C.c_int32]),
     "ufem_batch_set_assembly_warps": (C.c_int, [_P, C.c_int32]),
     "ufem_batch_tune_assembly": (C.c_int, [_P, C.c_void_p, C.c_int32, C.POINTER(C.c_int32), C.POINTER(C.c_float)]),

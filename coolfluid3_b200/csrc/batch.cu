@@ -78,6 +78,7 @@ struct BatchMesh {
   const int64_t* fix_ptr;
   const int64_t* fix_pos;
   const int32_t* fix_bc;
+  int active;  // 0: held (ufem_batch_set_active): no solve, no update
 };
 
 struct Chunk {
@@ -146,6 +147,7 @@ __global__ void update_batch_kernel(int64_t total, int nmesh, const int64_t* __r
   if (g >= total) return;
   const int m = find_mesh(node_prefix, nmesh, g);
   const BatchMesh& M = bm[m];
+  if (!M.active) return;
   const int64_t i = g - node_prefix[m];
   const int dim = M.dim, neq = M.neq;
   double* u1 = M.hist;
@@ -714,6 +716,8 @@ using namespace ufem;
 
 struct ufem_batch {
   std::vector<ufem_ns_handle*> members;
+  std::vector<int32_t> active;  // per member: 1 stepped, 0 held
+  bool active_dirty = false;
   int dim = 0, neq = 0, precision = 0, spec = 0, warps = 4;
   int nmesh = 0;
   int64_t total_nodes = 0, total_rows = 0, total_bc = 0, total_fix = 0;
@@ -799,6 +803,7 @@ int batch_refresh(ufem_batch* b) {
     M.fix_ptr = P.fix_ptr;
     M.fix_pos = P.fix_pos;
     M.fix_bc = P.fix_bc;
+    M.active = b->active[m];
     bcp[m + 1] = bcp[m] + P.nbc;
     fxp[m + 1] = fxp[m] + P.nfix_rows;
   }
@@ -813,10 +818,12 @@ int batch_refresh(ufem_batch* b) {
   UFEM_CUDA_TRY(cudaMemcpy(b->d_mesh, bm.data(), bm.size() * sizeof(BatchMesh), cudaMemcpyHostToDevice));
   UFEM_CUDA_TRY(cudaMemcpy(b->d_bc_prefix, bcp.data(), bcp.size() * 8, cudaMemcpyHostToDevice));
   UFEM_CUDA_TRY(cudaMemcpy(b->d_fix_prefix, fxp.data(), fxp.size() * 8, cudaMemcpyHostToDevice));
+  b->active_dirty = false;
   return UFEM_OK;
 }
 
 bool batch_dirty(const ufem_batch* b) {
+  if (b->active_dirty) return true;
   for (const ufem_ns_handle* h : b->members)
     if (h->bcp.dirty) return true;
   return false;
@@ -1002,6 +1009,7 @@ int ufem_batch_create(ufem_ns_handle* const* members, int32_t n, ufem_batch** ou
   }
   ufem_batch* b = new ufem_batch();
   b->members.assign(members, members + n);
+  b->active.assign(size_t(n), 1);
   b->nmesh = n;
   b->dim = members[0]->dim;
   b->neq = members[0]->neq;
@@ -1058,6 +1066,18 @@ int ufem_batch_create(ufem_ns_handle* const* members, int32_t n, ufem_batch** ou
     return rc;
   }
   *out = b;
+  return UFEM_OK;
+}
+
+int ufem_batch_set_active(ufem_batch* b, const int32_t* active) {
+  if (!b || !active) return set_error(UFEM_ERR_ARG, "NULL argument");
+  for (int m = 0; m < b->nmesh; ++m) {
+    const int32_t a = active[m] ? 1 : 0;
+    if (a != b->active[m]) {
+      b->active[m] = a;
+      b->active_dirty = true;
+    }
+  }
   return UFEM_OK;
 }
 
@@ -1210,7 +1230,17 @@ int ufem_batch_solve(ufem_batch* b, const ufem_krylov_opts* kopts, ufem_krylov_s
     return mixed ? bicgstab_b<float, kSol, kRhs>(b, o.precond, o.tol, maxit, outer, 1, st, true)
                  : bicgstab_b<double, kSol, kRhs>(b, o.precond, o.tol, maxit, outer, 0, st, false);
   };
-  if ((rc = run(o.max_iters, false))) return rc;
+  bool all_active = true;
+  for (int m = 0; m < b->nmesh; ++m) all_active = all_active && b->active[m];
+  if (all_active) {
+    if ((rc = run(o.max_iters, false))) return rc;
+  } else {  // held members keep their outer flag set: their kernels return at once
+    for (int m = 0; m < b->nmesh; ++m) {
+      for (int q = 0; q < kIc; ++q) b->h_ictl[m * kIc + q] = 0;
+      b->h_ictl[m * kIc + fOuter] = b->active[m] ? 0 : 1;
+    }
+    if ((rc = run(o.max_iters, true))) return rc;
+  }
   UFEM_CUDA_TRY(cudaMemcpyAsync(b->h_ictl, b->ictl, sizeof(int) * kIc * b->nmesh, cudaMemcpyDeviceToHost, st));
   UFEM_CUDA_TRY(cudaStreamSynchronize(st));
   for (int m = 0; m < b->nmesh; ++m) {
@@ -1224,14 +1254,14 @@ int ufem_batch_solve(ufem_batch* b, const ufem_krylov_opts* kopts, ufem_krylov_s
     int used = 0;
     bool any = false;
     for (int m = 0; m < b->nmesh; ++m)
-      if (status[m] == 2 && iters[m] < o.max_iters) {
+      if (b->active[m] && status[m] == 2 && iters[m] < o.max_iters) {
         any = true;
         used = std::max(used, iters[m]);
       }
     if (!any) break;
     for (int m = 0; m < b->nmesh; ++m) {
       for (int q = 0; q < kIc; ++q) b->h_ictl[m * kIc + q] = 0;
-      b->h_ictl[m * kIc + fOuter] = (status[m] == 2 && iters[m] < o.max_iters) ? 0 : 1;
+      b->h_ictl[m * kIc + fOuter] = (b->active[m] && status[m] == 2 && iters[m] < o.max_iters) ? 0 : 1;
     }
     if ((rc = run(o.max_iters - used, true))) return rc;
     UFEM_CUDA_TRY(cudaMemcpyAsync(b->h_ictl, b->ictl, sizeof(int) * kIc * b->nmesh, cudaMemcpyDeviceToHost, st));
@@ -1258,7 +1288,8 @@ int ufem_batch_solve(ufem_batch* b, const ufem_krylov_opts* kopts, ufem_krylov_s
     std::vector<int> redo(b->nmesh, 0);
     for (int m = 0; m < b->nmesh; ++m) {
       const double rr = b->h_dctl[m * kDc + sTrue];
-      redo[m] = !(std::isfinite(rr) && rr <= o.tol) && std::isfinite(rr) && (mixed || iters[m] < o.max_iters) ? 1 : 0;
+      redo[m] = b->active[m] && !(std::isfinite(rr) && rr <= o.tol) && std::isfinite(rr) &&
+                        (mixed || iters[m] < o.max_iters) ? 1 : 0;
       any = any || redo[m];
     }
     if (any) {
@@ -1284,6 +1315,11 @@ int ufem_batch_solve(ufem_batch* b, const ufem_krylov_opts* kopts, ufem_krylov_s
     for (int m = 0; m < b->nmesh; ++m) {
       const double rr = b->h_dctl[m * kDc + sTrue];
       ufem_krylov_status& s = statuses[m];
+      if (!b->active[m]) {  // held: nothing was solved
+        s = ufem_krylov_status{};
+        s.converged = 1;
+        continue;
+      }
       s.iterations = iters[m];
       s.refinements = refines[m];
       s.rel_residual = rr;
@@ -1300,7 +1336,8 @@ int ufem_batch_update(ufem_batch* b, void* stream) {
   update_batch_kernel<<<blocks_for(b->total_nodes, 256), 256, 0, st>>>(b->total_nodes, b->nmesh, b->d_node_prefix,
                                                                        b->d_mesh);
   UFEM_CUDA_TRY(cudaGetLastError());
-  for (ufem_ns_handle* h : b->members) h->time += h->opt.dt;  // as ufem_ns_update
+  for (int m = 0; m < b->nmesh; ++m)
+    if (b->active[m]) b->members[m]->time += b->members[m]->opt.dt;  // as ufem_ns_update
   return UFEM_OK;
 }
 

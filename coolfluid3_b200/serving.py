@@ -20,7 +20,12 @@ steps) arrive over time.  The server
     overlap on the device (the batching workers' streams have the higher
     priority: their kernels are short and latency-bound, the large requests'
     are bandwidth-bound and fill the gaps); requests that arrive while others
-    run join at the next tick, finished ones leave;
+    run join at the next tick (the batch is rebuilt with them); finished ones
+    are held in place (``Batch.set_active``) and leave at the next rebuild, so
+    a finish does not stall the other members;
+  * in the mixed form, the large requests assemble FP32 element matrices and
+    refine their FP32 inner solves against the matrix-free FP64 residual, so
+    their answers stay the FP64 system's;
   * reports throughput (time steps per second) beside p50/p99 step latency
     and request latency.
 
@@ -176,12 +181,14 @@ class Server:
                  krylov: dict | None = None, graphs: bool = True, creators: int = 2,
                  use_specializations: bool = False, realtime: bool = True, large_rows: int = 200_000,
                  large_workers: int = 2, small_priority: bool = True, mixed_scope: str = "large"):
-        """mixed: solve with the FP32 operator copy and FP64 residual replacement.
-        mixed_scope "large" applies it to the requests of the large workers only
-        (their solves are bandwidth-bound, so the halved operator bytes pay);
-        the batched small requests, whose iterations are latency-bound, keep the
-        FP64 operator, where the FP32 operator's extra iterations would only
-        cost time.  "all" applies it to every request."""
+        """mixed: the mixed-precision form.  Requests of at least `large_rows`
+        rows (stepped one at a time by the large workers; their solves are
+        bandwidth-bound) assemble FP32 element matrices and solve with FP32
+        inner BiCGStab refined against the matrix-free FP64 residual, so their
+        answers are the FP64 system's.  The batched small requests, whose
+        iterations are latency-bound, keep FP64 elements and the FP64 operator
+        with mixed_scope "large"; with "all" they iterate with an FP32 copy of
+        the operator and FP64 residual replacement."""
         if mixed_scope not in ("large", "all"):
             raise ValueError("mixed_scope must be 'large' or 'all'")
         if precision not in ("fp32", "fp64"):
@@ -198,8 +205,14 @@ class Server:
         self.small_priority = bool(small_priority)
         self.krylov = dict(method="bicgstab", precond="jacobi", tol=1e-10, max_iters=3000)
         self.krylov.update(krylov or {})
+        self.mixed = bool(mixed)
         self.krylov_mixed = dict(self.krylov, mixed=True, inner_tol=1e-6, max_refine=20) if mixed else self.krylov
+        # large requests of the mixed form: FP32 element matrices, FP32 inner
+        # solves refined against the matrix-free FP64 residual
+        self.krylov_large = (dict(self.krylov, mixed="matrix_free", inner_tol=1e-5, max_refine=30) if mixed
+                             else self.krylov)
         self.mixed_scope = mixed_scope
+        self._starved = False
         self._lock = threading.Condition()
         self._used = 0
         self._slots = 0
@@ -248,11 +261,70 @@ class Server:
         t0 = time.perf_counter()
         now = lambda: time.perf_counter() - t0  # noqa: E731
 
+        def finish(a: _Active, held: bool) -> None:
+            a.result.state = a.ns.state()[0]
+            a.result.finished = now()
+            if not held:  # a held handle is closed (and its budget freed) when its batch is rebuilt
+                a.ns.close()
+                self._release(a.reserved)
+            with self._lock:
+                results.append(a.result)
+                state["open"] -= 1
+                self._lock.notify_all()
+
+        def large_worker(key: tuple):
+            # one request at a time through the one-handle path; with the mixed
+            # form its element matrices are FP32 and the solve refines against
+            # the matrix-free FP64 residual (mixed = "matrix_free")
+            stream = torch.cuda.Stream()
+            kr = self.krylov_large
+            try:
+                while True:
+                    with self._lock:
+                        while not inbox[key] and state["open"] > 0:
+                            self._lock.wait(0.05)
+                        if not inbox[key]:
+                            break
+                        a = inbox[key].popleft()
+                    a.result.started = time.perf_counter() - t0
+                    for _ in range(a.req.nsteps):
+                        ts = time.perf_counter()
+                        a.ns.assemble(stream)
+                        a.ns.apply_dirichlet(stream)
+                        st = a.ns.solve(stream, raise_on_failure=False, **kr)
+                        a.ns.update(stream)
+                        stream.synchronize()
+                        a.result.step_ms.append((time.perf_counter() - ts) * 1e3)
+                        a.result.statuses.append(st)
+                        self.max_batch = max(self.max_batch, 1)
+                    finish(a, held=False)
+            except Exception as e:  # surface worker failures to the caller
+                with self._lock:
+                    self.errors.append(e)
+                    state["open"] = -10 ** 9
+                    self._lock.notify_all()
+
         def worker(key: tuple, capacity: int):
-            stream = small_streams[key] if key[1] == "small" else torch.cuda.Stream()
+            # continuous batching of the small requests: newcomers join at the
+            # next tick (the batch is rebuilt with them); finished members are
+            # held in place (ufem_batch_set_active), so a finish does not stall
+            # the others, and leave at the next rebuild -- when newcomers join,
+            # when admission waits for memory, or when no member is left
+            stream = small_streams[key]
             active: list[_Active] = []
+            held: list[_Active] = []
             batch = None
-            members = None
+
+            def drop_batch():
+                nonlocal batch
+                if batch is not None:
+                    batch.close()
+                    batch = None
+                for h in held:
+                    h.ns.close()
+                    self._release(h.reserved)
+                held.clear()
+
             try:
                 while True:
                     with self._lock:
@@ -260,27 +332,31 @@ class Server:
                             self._lock.wait(0.05)
                         if not inbox[key] and not active and state["open"] <= 0:
                             break
-                        while inbox[key] and len(active) < capacity:
+                        joined = False
+                        while inbox[key] and len(active) + len(held) < capacity:
                             active.append(inbox[key].popleft())
+                            joined = True
+                        starved = self._starved
                     if not active:
+                        drop_batch()
                         continue
-                    ids = tuple(id(a.ns) for a in active)
-                    if ids != members:
-                        if batch is not None:
-                            batch.close()
+                    if batch is None or joined or (held and starved):
+                        drop_batch()
                         batch = Batch([a.ns for a in active], graphs=self.graphs)
-                        members = ids
+                        members = list(active)
                         self.max_batch = max(self.max_batch, len(active))
                     ts = time.perf_counter()
                     for a in active:
                         if a.done_steps == 0 and a.result.started == 0.0:
                             a.result.started = ts - t0
-                    kr = self.krylov_mixed if (key[1] == "large" or self.mixed_scope == "all") else self.krylov
+                    kr = self.krylov_mixed if self.mixed_scope == "all" else self.krylov
                     sts = batch.step(stream, **kr)
                     stream.synchronize()
                     ms = (time.perf_counter() - ts) * 1e3
                     finished = []
-                    for a, st in zip(active, sts):
+                    for a, st in zip(members, sts):
+                        if a not in active:
+                            continue
                         a.result.step_ms.append(ms)
                         a.result.statuses.append(st)
                         a.done_steps += 1
@@ -288,30 +364,22 @@ class Server:
                             finished.append(a)
                     for a in finished:
                         active.remove(a)
-                    if finished:
-                        batch.close()
-                        batch, members = None, None
-                    for a in finished:
-                        a.result.state = a.ns.state()[0]
-                        a.ns.close()
-                        a.result.finished = now()
-                        self._release(a.reserved)
-                        with self._lock:
-                            results.append(a.result)
-                            state["open"] -= 1
-                            self._lock.notify_all()
+                        held.append(a)
+                        finish(a, held=True)
+                    if finished and active:
+                        batch.set_active([a in active for a in members])
             except Exception as e:  # surface worker failures to the caller
                 with self._lock:
                     self.errors.append(e)
                     state["open"] = -10 ** 9
                     self._lock.notify_all()
             finally:
-                if batch is not None:
-                    batch.close()
+                drop_batch()
 
         def create(req: Request, est: int, admitted: float):
             try:
-                ns = _new_handle(req, self.precision, self.spec)
+                large = req.coords.shape[0] * (req.dim + 1) >= self.large_rows
+                ns = _new_handle(req, "fp32" if (large and self.mixed) else self.precision, self.spec)
             except Exception as e:  # the request is rejected; the others go on
                 self._release(est)
                 with self._lock:
@@ -330,7 +398,7 @@ class Server:
                 self._lock.notify_all()
 
         workers = [threading.Thread(target=worker, args=((d, "small"), self.max_slots), daemon=True) for d in (2, 3)]
-        workers += [threading.Thread(target=worker, args=((d, "large"), 1), daemon=True)
+        workers += [threading.Thread(target=large_worker, args=((d, "large"),), daemon=True)
                     for d in (2, 3) for _ in range(self.large_workers)]
         for w in workers:
             w.start()
@@ -351,6 +419,9 @@ class Server:
                         waiting.remove(req)
                         pool.submit(create, req, est, now())
                         admitted_any = True
+                with self._lock:
+                    # admission waits for memory: batching workers drop their finished members
+                    self._starved = bool(waiting) and not admitted_any
                 if not admitted_any:
                     with self._lock:
                         timeout = 0.01

@@ -586,6 +586,12 @@ class Batch:
     def set_graphs(self, on: bool) -> None:
         N.check(self._lib.ufem_batch_set_graphs(self._b, 1 if on else 0))
 
+    def set_active(self, active) -> None:
+        """Hold (False) or resume (True) members without rebuilding the batch; a
+        held member is neither solved nor updated."""
+        arr = (C.c_int32 * len(self.members))(*[1 if a else 0 for a in active])
+        N.check(self._lib.ufem_batch_set_active(self._b, arr))
+
     def tune_assembly(self, reps: int = 5, stream=None) -> dict:
         """Time the batched assembly with 2, 4 and 8 warps per CTA and keep the
         fastest (the members' systems are overwritten; assemble afterwards)."""

@@ -344,6 +344,13 @@ int ufem_ns_tune_assembly(ufem_ns_handle* h, void* stream, int32_t reps, int32_t
  * accepting convergence (status.refinements counts the replacements). */
 typedef struct ufem_batch ufem_batch;
 int ufem_batch_create(ufem_ns_handle* const* members, int32_t n, ufem_batch** out);
+/* Holds or resumes members (active[m] = 0: held) without rebuilding the batch.
+ * No counterpart in the reference.  A held member is not solved and not updated
+ * (its state and time stay as they are; its status reads converged with 0
+ * iterations); assembly and the Dirichlet passes still run over it.  The handle
+ * of a held member must stay alive until the batch is destroyed.  Lets a
+ * serving loop retire finished requests without stalling the others. */
+int ufem_batch_set_active(ufem_batch* b, const int32_t* active);
 int ufem_batch_size(const ufem_batch* b, int32_t* n, int64_t* rows);
 int ufem_batch_set_graphs(ufem_batch* b, int32_t enable);
 int ufem_batch_set_assembly_warps(ufem_batch* b, int32_t warps_per_cta);
