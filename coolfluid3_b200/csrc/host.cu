@@ -197,6 +197,7 @@ int build_bc_plan(ufem_ns_handle* h) {
   DirichletPlan& bp = h->bcp;
   free_bc_plan(bp);
   bp.dirty = false;
+  ++bp.version;
   int rc;
   if ((rc = build_neumann_plan(h))) return rc;
   if (h->bcs.empty()) return UFEM_OK;
@@ -585,7 +586,7 @@ int create_impl(const ufem_mesh* mesh, const ufem_ns_options* opts, const uint32
 
   // --- device allocations and uploads
   DeviceLock device_lock(device_mutex());
-  if (dim == 2) h->coords_h.assign(mesh->coords, mesh->coords + size_t(N) * 2);
+  h->coords_h.assign(mesh->coords, mesh->coords + size_t(N) * dim);
   std::vector<double> c4(size_t(N) * 4, 0.0);
   for (int64_t i = 0; i < N; ++i)
     for (int k = 0; k < dim; ++k) c4[i * 4 + k] = mesh->coords[i * dim + k];

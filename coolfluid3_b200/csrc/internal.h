@@ -111,6 +111,7 @@ struct DirichletPlan {
   int64_t* neu_ptr = nullptr;
   double* neu_val = nullptr;
   bool dirty = true;
+  int64_t version = 0;         // incremented at every rebuild of the plan
 };
 
 struct KrylovWork;
@@ -138,7 +139,7 @@ struct ufem_ns_handle {
   // host copies used by planning
   std::vector<int64_t> start_h;   // N+1
   std::vector<int32_t> adj_h;     // bnnz
-  std::vector<double> coords_h;   // N x 2, 2D meshes only (constant Neumann faces)
+  std::vector<double> coords_h;   // N x dim (constant Neumann faces, coarse-preconditioner aggregates)
   std::vector<uint32_t> p2m_h;    // periodic links: row node of each node (empty: no links)
   struct BCEntry { uint32_t node; int comp; double value; int32_t fn = -1; };  // fn: expression id or -1
   std::vector<std::vector<int32_t>> fn_code;   // compiled Dirichlet function expressions

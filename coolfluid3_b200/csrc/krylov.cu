@@ -68,6 +68,20 @@ struct KrylovWork {
   double* ainv = nullptr;      // nc x nc, row-major
   double* cvec = nullptr;      // nc: R^T r
   double* yvec = nullptr;      // nc: Ac^-1 R^T r
+  // Two-level preconditioner of the coupled system (precond 4): point Jacobi
+  // plus the same piecewise-constant correction on aggregates of pressure rows
+  // (agg .. yvec above, built for the coupled rows).  Its coarse matrix, the
+  // Galerkin product of the pressure-pressure block, is rebuilt at every solve
+  // on the device: the block's CSR positions are sorted once by (aggregate of
+  // the row, aggregate of the column) and each segment is summed by one warp.
+  int64_t* cp_pos = nullptr;   // sorted CSR positions of the coarse pressure-pressure entries
+  int32_t* cp_seg = nullptr;   // cp_nseg + 1 segment starts
+  int32_t* cp_dst = nullptr;   // dense index I * nc + J of each segment
+  int cp_nseg = 0;
+  double* acd = nullptr;       // nc x nc coarse matrix on the device
+  double* h_ac = nullptr;      // pinned host copy (nc x nc)
+  int64_t cp_bc_version = -1;  // Dirichlet plan the structure was built for
+  bool cp_spd = false;         // the last coarse matrix was positive definite
 };
 
 namespace {
@@ -98,6 +112,53 @@ __device__ __forceinline__ double block_sum(double v, double* sm) {
     for (int k = 0; k < int(blockDim.x >> 5); ++k) s += sm[k];
   __syncthreads();
   return s;
+}
+
+// In-place inverse of an SPD matrix (row-major, n x n) through its Cholesky
+// factor L: L^-1 row by row, then A^-1 = L^-T L^-1 as a sum of rank-one
+// updates; every inner loop runs over contiguous memory.  False if a pivot is
+// not positive (a coarse matrix of a system without conditions that fix its
+// constant mode is singular).
+bool spd_invert(double* A, int n) {
+  std::vector<double> L(size_t(n) * n, 0.0), M(size_t(n) * n, 0.0);
+  for (int j = 0; j < n; ++j) {
+    const double* Lj = &L[size_t(j) * n];
+    double d = A[size_t(j) * n + j];
+    for (int k = 0; k < j; ++k) d -= Lj[k] * Lj[k];
+    if (!(d > 0.0) || !std::isfinite(d)) return false;
+    const double ljj = std::sqrt(d);
+    L[size_t(j) * n + j] = ljj;
+    for (int i = j + 1; i < n; ++i) {
+      const double* Li = &L[size_t(i) * n];
+      double s = A[size_t(i) * n + j];
+      for (int k = 0; k < j; ++k) s -= Li[k] * Lj[k];
+      L[size_t(i) * n + j] = s / ljj;
+    }
+  }
+  for (int i = 0; i < n; ++i) {  // M = L^-1: row i = (e_i - sum_{k<i} L[i][k] M[k]) / L[i][i]
+    double* Mi = &M[size_t(i) * n];
+    Mi[i] = 1.0;
+    for (int k = 0; k < i; ++k) {
+      const double lik = L[size_t(i) * n + k];
+      const double* Mk = &M[size_t(k) * n];
+      for (int j = 0; j <= k; ++j) Mi[j] -= lik * Mk[j];
+    }
+    const double inv = 1.0 / L[size_t(i) * n + i];
+    for (int j = 0; j <= i; ++j) Mi[j] *= inv;
+  }
+  std::fill(A, A + size_t(n) * n, 0.0);
+  for (int k = 0; k < n; ++k) {  // A^-1 = sum_k M[k]^T M[k] (lower triangle, then mirrored)
+    const double* Mk = &M[size_t(k) * n];
+    for (int i = 0; i <= k; ++i) {
+      const double mki = Mk[i];
+      if (mki == 0.0) continue;
+      double* Ai = A + size_t(i) * n;
+      for (int j = 0; j <= i; ++j) Ai[j] += mki * Mk[j];
+    }
+  }
+  for (int i = 0; i < n; ++i)
+    for (int j = 0; j < i; ++j) A[size_t(j) * n + i] = A[size_t(i) * n + j];
+  return true;
 }
 
 #define GRID_STRIDE(i, n) \
@@ -858,6 +919,33 @@ __global__ void prolong_kernel(int64_t n, const VT* __restrict__ dinv, const int
   }
 }
 
+// z += y[agg] on the rows of the coarse space (the coupled two-level form:
+// z already holds D^-1 r).
+template <typename VT>
+__global__ void prolong_add_kernel(int64_t n, const int32_t* __restrict__ agg, const double* __restrict__ y,
+                                   VT* __restrict__ z, const int* __restrict__ done) {
+  if (done && *done) return;
+  GRID_STRIDE(i, n) {
+    const int a = agg[i];
+    if (a >= 0) z[i] = VT(double(z[i]) + y[a]);
+  }
+}
+
+// Coarse pressure matrix of the coupled two-level form: ac[dst[q]] = the sum of
+// the values at the segment's sorted CSR positions (one warp per segment; the
+// lane partition and the shuffle tree are fixed, so the sum is deterministic).
+__global__ void coarse_matrix_kernel(int nseg, const int32_t* __restrict__ seg, const int32_t* __restrict__ dst,
+                                     const int64_t* __restrict__ pos, const double* __restrict__ vals,
+                                     double* __restrict__ ac) {
+  const int q = int((int64_t(blockIdx.x) * blockDim.x + threadIdx.x) >> 5);
+  const int lane = threadIdx.x & 31;
+  if (q >= nseg) return;  // whole warps
+  double s = 0.0;
+  for (int k = seg[q] + lane; k < seg[q + 1]; k += 32) s += vals[pos[k]];
+  s = warp_sum(s);
+  if (lane == 0) ac[dst[q]] = s;
+}
+
 // z = D^-1 r + y[agg] ; partials of r.z ; the last block folds r.r (written by
 // cg_xr_plain_kernel with the same grid) and r.z into the convergence test and beta.
 template <typename VT>
@@ -978,7 +1066,7 @@ int spmv(ufem_ns_handle* h, const MT* vals, const VT* x, VT* y, const int* done,
 
 template <typename VT, typename MT>
 int setup_precond(ufem_ns_handle* h, int kind, const MT* vals, VT* dinv, cudaStream_t s) {
-  if (kind == 1 || kind == 3)
+  if (kind == 1 || kind == 3 || kind == 4)
     jacobi_kernel<MT, VT><<<grid_for(h->nrows, 256), 256, 0, s>>>(h->nrows, h->d_diagpos, vals, dinv);
   else if (kind == 2)
     block_jacobi_kernel<MT, VT><<<grid_for(h->N, 128), 128, 0, s>>>(h->N, h->neq, h->d_diagpos, vals, dinv);
@@ -986,10 +1074,24 @@ int setup_precond(ufem_ns_handle* h, int kind, const MT* vals, VT* dinv, cudaStr
   return UFEM_OK;
 }
 
+// z += R Ac^-1 R^T v: the coarse correction of the coupled two-level form.
+template <typename VT>
+int coarse_correct(ufem_ns_handle* h, const VT* v, VT* z, const int* done, cudaStream_t s) {
+  KrylovWork& kw = *h->kw;
+  const unsigned gw = unsigned((int64_t(kw.nc) * 32 + 255) / 256);
+  restrict_kernel<VT><<<gw, 256, 0, s>>>(kw.nc, kw.agg_ptr, kw.agg_rows, v, kw.cvec, done);
+  coarse_kernel<<<gw, 256, 0, s>>>(kw.nc, kw.ainv, kw.cvec, kw.yvec, done);
+  prolong_add_kernel<VT><<<unsigned(kw.nblk), kRedThreads, 0, s>>>(h->nrows, kw.agg, kw.yvec, z, done);
+  UFEM_CUDA_TRY(cudaGetLastError());
+  return UFEM_OK;
+}
+
 template <typename VT>
 int precond(ufem_ns_handle* h, int kind, const VT* dinv, const VT* v, VT* z, const int* done, cudaStream_t s) {
-  precond_kernel<VT><<<grid_for(h->nrows, 256), 256, 0, s>>>(h->nrows, h->neq, kind, dinv, v, z, done);
+  precond_kernel<VT><<<grid_for(h->nrows, 256), 256, 0, s>>>(h->nrows, h->neq, kind == 4 ? 1 : kind, dinv, v, z,
+                                                              done);
   UFEM_CUDA_TRY(cudaGetLastError());
+  if (kind == 4) return coarse_correct<VT>(h, v, z, done, s);
   return UFEM_OK;
 }
 
@@ -1118,13 +1220,16 @@ int bicgstab(ufem_ns_handle* h, KrylovWork& kw, const MT* vals, const BT* b, VT*
   const double alpha_max = std::is_same<VT, float>::value ? 1e20 : 1e150;
   auto iteration = [&](cudaStream_t s2) -> int {
     int irc;
-    bicg_p_kernel<VT><<<g1, kRedThreads, 0, s2>>>(n, pkind, dinv, r, v, p, ph, kw.dctl, kw.ictl);
+    const int pk = pkind == 4 ? 1 : pkind;  // the two-level form: point Jacobi plus the coarse correction
+    bicg_p_kernel<VT><<<g1, kRedThreads, 0, s2>>>(n, pk, dinv, r, v, p, ph, kw.dctl, kw.ictl);
     if (pkind == 2 && (irc = precond<VT>(h, pkind, dinv, p, ph, kw.ictl, s2))) return irc;
+    if (pkind == 4 && (irc = coarse_correct<VT>(h, p, ph, kw.ictl, s2))) return irc;
     if ((irc = spmv<VT, MT>(h, vals, ph, v, kw.ictl, s2))) return irc;
     dot_partials_kernel<VT><<<dim3(g1, 1), kRedThreads, 0, s2>>>(n, rh, n, v, kw.part, kw.ictl);
     bicg_alpha_kernel<<<1, 256, 0, s2>>>(nblk, kw.part, kw.dctl, kw.ictl, alpha_max);
-    bicg_s_kernel<VT><<<g1, kRedThreads, 0, s2>>>(n, pkind, dinv, r, v, sv, sh, kw.dctl, kw.ictl);
+    bicg_s_kernel<VT><<<g1, kRedThreads, 0, s2>>>(n, pk, dinv, r, v, sv, sh, kw.dctl, kw.ictl);
     if (pkind == 2 && (irc = precond<VT>(h, pkind, dinv, sv, sh, kw.ictl, s2))) return irc;
+    if (pkind == 4 && (irc = coarse_correct<VT>(h, sv, sh, kw.ictl, s2))) return irc;
     if ((irc = spmv<VT, MT>(h, vals, sh, tv, kw.ictl, s2))) return irc;
     dot2_partials_kernel<VT><<<g1, kRedThreads, 0, s2>>>(n, tv, sv, kw.part, kw.ictl);
     bicg_omega_kernel<<<1, 256, 0, s2>>>(nblk, kw.part, kw.dctl, kw.ictl);
@@ -1139,7 +1244,8 @@ int bicgstab(ufem_ns_handle* h, KrylovWork& kw, const MT* vals, const BT* b, VT*
   KrylovWork::CGGraph* gr = nullptr;
   if (kw.use_graph) {
     gr = &kw.bicg_graph[std::is_same<MT, float>::value ? 1 : 0];
-    const void* key[16] = {vals, b, x, r, rh, p, v, sv, tv, ph, sh, dinv, h->d_start};
+    const void* key[16] = {vals, b, x, r, rh, p, v, sv, tv, ph, sh, dinv, h->d_start,
+                           reinterpret_cast<const void*>(intptr_t(pkind == 4 ? kw.coarse_version : 0))};
     const bool cached = gr->exec && gr->pkind == pkind && gr->tol == tol && gr->maxit == maxit &&
                         std::equal(key, key + 16, gr->key);
     if (!cached) {
@@ -1359,6 +1465,146 @@ __global__ void vals_to32_kernel(int64_t n, const double* __restrict__ v, float*
 
 }  // namespace
 
+namespace {
+
+// Aggregates of the coupled two-level form: k^dim boxes of the mesh's bounding
+// box (k chosen for at least 64 nodes a box, at most 7 boxes a side in 3D and
+// 20 in 2D, so the coarse matrix stays small enough to invert on the host at
+// every solve); the coarse space holds the pressure rows of the nodes whose
+// pressure is neither a Dirichlet dof nor a periodic slave.  Built once per
+// Dirichlet plan: the aggregate of each row, the rows of each aggregate, and
+// the pressure-pressure CSR positions sorted by (row aggregate, column
+// aggregate, position) with their segments.
+int coupled_coarse_build(ufem_ns_handle* h) {
+  KrylovWork& kw = *h->kw;
+  dfree(kw.agg); dfree(kw.agg_ptr); dfree(kw.agg_rows); dfree(kw.ainv); dfree(kw.cvec); dfree(kw.yvec);
+  dfree(kw.cp_pos); dfree(kw.cp_seg); dfree(kw.cp_dst); dfree(kw.acd);
+  if (kw.h_ac) {
+    DeviceLock lk(device_mutex());
+    cudaFreeHost(kw.h_ac);
+    kw.h_ac = nullptr;
+  }
+  kw.nc = 0;
+  kw.cp_nseg = 0;
+  kw.cp_bc_version = h->bcp.version;
+  ++kw.coarse_version;
+  const int dim = h->dim, neq = h->neq;
+  const int64_t N = h->N;
+  if (int64_t(h->coords_h.size()) != N * dim) return UFEM_OK;  // no coordinates: point Jacobi
+  std::vector<char> in(size_t(N), 1);
+  for (const auto& bc : h->bcs)
+    if (bc.comp == dim) in[bc.node] = 0;
+  if (!h->p2m_h.empty())
+    for (int64_t i = 0; i < N; ++i)
+      if (h->p2m_h[size_t(i)] != uint32_t(i)) in[size_t(i)] = 0;
+  double lo[3] = {1e300, 1e300, 1e300}, hi[3] = {-1e300, -1e300, -1e300};
+  for (int64_t i = 0; i < N; ++i)
+    for (int d = 0; d < dim; ++d) {
+      lo[d] = std::min(lo[d], h->coords_h[size_t(i * dim + d)]);
+      hi[d] = std::max(hi[d], h->coords_h[size_t(i * dim + d)]);
+    }
+  int k = int(std::floor(std::pow(double(N) / 64.0, 1.0 / dim)));
+  k = std::max(1, std::min(k, dim == 3 ? 7 : 20));
+  std::vector<int32_t> box(size_t(N), -1), id(size_t(std::pow(k, dim)) + 1, -1);
+  int nc = 0;
+  for (int64_t i = 0; i < N; ++i) {
+    if (!in[size_t(i)]) continue;
+    int b = 0, mul = 1;
+    for (int d = 0; d < dim; ++d) {
+      const double span = hi[d] > lo[d] ? hi[d] - lo[d] : 1.0;
+      const int c = std::min(k - 1, std::max(0, int((h->coords_h[size_t(i * dim + d)] - lo[d]) / span * k)));
+      b += c * mul;
+      mul *= k;
+    }
+    if (id[size_t(b)] < 0) id[size_t(b)] = nc++;
+    box[size_t(i)] = id[size_t(b)];
+  }
+  if (nc == 0) return UFEM_OK;
+  std::vector<int32_t> agg(size_t(h->nrows), -1), ptr(size_t(nc) + 1, 0), rows;
+  for (int64_t i = 0; i < N; ++i)
+    if (box[size_t(i)] >= 0) {
+      agg[size_t(i * neq + dim)] = box[size_t(i)];
+      ++ptr[size_t(box[size_t(i)]) + 1];
+    }
+  for (int a = 0; a < nc; ++a) ptr[size_t(a) + 1] += ptr[size_t(a)];
+  rows.resize(size_t(ptr[size_t(nc)]));
+  {
+    std::vector<int32_t> fill(ptr.begin(), ptr.end() - 1);
+    for (int64_t i = 0; i < N; ++i)  // ascending rows within each aggregate
+      if (box[size_t(i)] >= 0) rows[size_t(fill[size_t(box[size_t(i)])]++)] = int32_t(i * neq + dim);
+  }
+  struct Entry { int64_t key, pos; };
+  std::vector<Entry> ent;
+  for (int64_t i = 0; i < N; ++i) {
+    if (box[size_t(i)] < 0) continue;
+    const int64_t s0 = h->start_h[size_t(i)], S = h->start_h[size_t(i) + 1] - s0;
+    for (int64_t q = 0; q < S; ++q) {
+      const int32_t j = h->adj_h[size_t(s0 + q)];
+      if (box[size_t(j)] < 0) continue;
+      ent.push_back({int64_t(box[size_t(i)]) * nc + box[size_t(j)],
+                     int64_t(neq) * neq * s0 + (int64_t(dim) * S + q) * neq + dim});
+    }
+  }
+  std::sort(ent.begin(), ent.end(), [](const Entry& a, const Entry& b) {
+    return a.key != b.key ? a.key < b.key : a.pos < b.pos;
+  });
+  std::vector<int64_t> pos(ent.size());
+  std::vector<int32_t> seg, dst;
+  for (size_t q = 0; q < ent.size(); ++q) {
+    pos[q] = ent[q].pos;
+    if (q == 0 || ent[q].key != ent[q - 1].key) {
+      seg.push_back(int32_t(q));
+      dst.push_back(int32_t(ent[q].key));
+    }
+  }
+  seg.push_back(int32_t(ent.size()));
+  int rc;
+  if ((rc = dalloc(&kw.agg, agg.size())) || (rc = dalloc(&kw.agg_ptr, ptr.size())) ||
+      (rc = dalloc(&kw.agg_rows, std::max<size_t>(rows.size(), 1))) || (rc = dalloc(&kw.ainv, size_t(nc) * nc)) ||
+      (rc = dalloc(&kw.cvec, size_t(nc))) || (rc = dalloc(&kw.yvec, size_t(nc))) ||
+      (rc = dalloc(&kw.cp_pos, std::max<size_t>(pos.size(), 1))) || (rc = dalloc(&kw.cp_seg, seg.size())) ||
+      (rc = dalloc(&kw.cp_dst, std::max<size_t>(dst.size(), 1))) || (rc = dalloc(&kw.acd, size_t(nc) * nc)))
+    return rc;
+  {
+    DeviceLock lk(device_mutex());
+    UFEM_CUDA_TRY(cudaMallocHost(reinterpret_cast<void**>(&kw.h_ac), size_t(nc) * nc * sizeof(double)));
+  }
+  UFEM_CUDA_TRY(cudaMemcpy(kw.agg, agg.data(), agg.size() * 4, cudaMemcpyHostToDevice));
+  UFEM_CUDA_TRY(cudaMemcpy(kw.agg_ptr, ptr.data(), ptr.size() * 4, cudaMemcpyHostToDevice));
+  if (!rows.empty()) UFEM_CUDA_TRY(cudaMemcpy(kw.agg_rows, rows.data(), rows.size() * 4, cudaMemcpyHostToDevice));
+  if (!pos.empty()) UFEM_CUDA_TRY(cudaMemcpy(kw.cp_pos, pos.data(), pos.size() * 8, cudaMemcpyHostToDevice));
+  UFEM_CUDA_TRY(cudaMemcpy(kw.cp_seg, seg.data(), seg.size() * 4, cudaMemcpyHostToDevice));
+  if (!dst.empty()) UFEM_CUDA_TRY(cudaMemcpy(kw.cp_dst, dst.data(), dst.size() * 4, cudaMemcpyHostToDevice));
+  kw.cp_nseg = int(dst.size());
+  kw.nc = nc;
+  return UFEM_OK;
+}
+
+// The coarse matrix of the current system (FP64 values, after the Dirichlet
+// pass), its inverse on the host, uploaded for the solve; cp_spd false (point
+// Jacobi for this solve) when it is not positive definite.
+int coupled_coarse_refresh(ufem_ns_handle* h, cudaStream_t s) {
+  KrylovWork& kw = *h->kw;
+  int rc;
+  if (kw.cp_bc_version != h->bcp.version && (rc = coupled_coarse_build(h))) return rc;
+  kw.cp_spd = false;
+  const int nc = kw.nc;
+  if (nc == 0) return UFEM_OK;
+  const size_t bytes = size_t(nc) * nc * sizeof(double);
+  UFEM_CUDA_TRY(cudaMemsetAsync(kw.acd, 0, bytes, s));
+  if (kw.cp_nseg > 0)
+    coarse_matrix_kernel<<<unsigned((int64_t(kw.cp_nseg) * 32 + 255) / 256), 256, 0, s>>>(
+        kw.cp_nseg, kw.cp_seg, kw.cp_dst, kw.cp_pos, h->d_vals, kw.acd);
+  UFEM_CUDA_TRY(cudaGetLastError());
+  UFEM_CUDA_TRY(cudaMemcpyAsync(kw.h_ac, kw.acd, bytes, cudaMemcpyDeviceToHost, s));
+  UFEM_CUDA_TRY(cudaStreamSynchronize(s));
+  kw.cp_spd = spd_invert(kw.h_ac, nc);
+  if (kw.cp_spd) UFEM_CUDA_TRY(cudaMemcpyAsync(kw.ainv, kw.h_ac, bytes, cudaMemcpyHostToDevice, s));
+  return UFEM_OK;
+}
+
+}  // namespace
+
 int krylov_solve(ufem_ns_handle* h, const ufem_krylov_opts* ko, ufem_krylov_status* st, cudaStream_t s) {
   ufem_krylov_opts o = *ko;
   if (o.restart <= 0) o.restart = 30;
@@ -1366,7 +1612,9 @@ int krylov_solve(ufem_ns_handle* h, const ufem_krylov_opts* ko, ufem_krylov_stat
   if (o.tol <= 0) o.tol = 1e-10;
   if (o.max_refine <= 0) o.max_refine = 20;
   if (o.inner_tol <= 0) o.inner_tol = 1e-3;
-  if (o.precond < 0 || o.precond > 3) return set_error(UFEM_ERR_ARG, "precond must be 0, 1, 2 or 3");
+  if (o.precond < 0 || o.precond > 4) return set_error(UFEM_ERR_ARG, "precond must be 0, 1, 2, 3 or 4");
+  if (o.precond == 4 && (h->neq < 2 || o.method == 2))
+    return set_error(UFEM_ERR_ARG, "the coupled two-level preconditioner (4) is for BiCGStab or GMRES on the coupled system");
   if (o.precond == 3 && (o.method != 2 || h->neq != 1 || !h->kw || h->kw->nc == 0))
     return set_error(UFEM_ERR_ARG, "the two-level preconditioner needs CG on a one-equation system with aggregates set");
   if (o.method < 0 || o.method > 2)
@@ -1377,6 +1625,10 @@ int krylov_solve(ufem_ns_handle* h, const ufem_krylov_opts* ko, ufem_krylov_stat
   const bool bicg = o.method == 1 || use_cg;  // CG uses the BiCGStab work vectors
   int rc;
   if ((rc = ensure_work(h, o.restart, mixed, bicg))) return rc;
+  if (o.precond == 4) {  // coarse matrix of this system; point Jacobi when it is not positive definite
+    if ((rc = coupled_coarse_refresh(h, s))) return rc;
+    if (!h->kw->cp_spd) o.precond = 1;
+  }
   KrylovWork& kw = *h->kw;
   const int64_t n = h->nrows;
   const unsigned g1 = unsigned(kw.nblk);
@@ -1525,36 +1777,7 @@ namespace {
 // In-place inverse of an SPD matrix through its Cholesky factor; false if a
 // pivot is not positive (the coarse matrix of a system without conditions
 // that fix its constant mode is singular).
-bool spd_inverse(std::vector<double>& A, int n) {
-  std::vector<double> L(size_t(n) * n, 0.0);
-  for (int j = 0; j < n; ++j) {
-    double d = A[size_t(j) * n + j];
-    for (int k = 0; k < j; ++k) d -= L[size_t(j) * n + k] * L[size_t(j) * n + k];
-    if (!(d > 0.0) || !std::isfinite(d)) return false;
-    const double ljj = std::sqrt(d);
-    L[size_t(j) * n + j] = ljj;
-    for (int i = j + 1; i < n; ++i) {
-      double s = A[size_t(i) * n + j];
-      for (int k = 0; k < j; ++k) s -= L[size_t(i) * n + k] * L[size_t(j) * n + k];
-      L[size_t(i) * n + j] = s / ljj;
-    }
-  }
-  std::vector<double> col(n);
-  for (int c = 0; c < n; ++c) {  // solve L L^T x = e_c
-    for (int i = 0; i < n; ++i) {
-      double s = (i == c) ? 1.0 : 0.0;
-      for (int k = 0; k < i; ++k) s -= L[size_t(i) * n + k] * col[k];
-      col[i] = s / L[size_t(i) * n + i];
-    }
-    for (int i = n - 1; i >= 0; --i) {
-      double s = col[i];
-      for (int k = i + 1; k < n; ++k) s -= L[size_t(k) * n + i] * col[k];
-      col[i] = s / L[size_t(i) * n + i];
-    }
-    for (int i = 0; i < n; ++i) A[size_t(i) * n + c] = col[i];
-  }
-  return true;
-}
+bool spd_inverse(std::vector<double>& A, int n) { return spd_invert(A.data(), n); }
 
 }  // namespace
 
@@ -1632,7 +1855,9 @@ void krylov_free(ufem_ns_handle* h) {
   dfree(k.part); dfree(k.hbuf); dfree(k.H); dfree(k.cs); dfree(k.sn); dfree(k.g); dfree(k.y);
   dfree(k.dctl); dfree(k.ictl); dfree(k.cg_counter);
   dfree(k.agg); dfree(k.agg_ptr); dfree(k.agg_rows); dfree(k.ainv); dfree(k.cvec); dfree(k.yvec);
+  dfree(k.cp_pos); dfree(k.cp_seg); dfree(k.cp_dst); dfree(k.acd);
   DeviceLock lk(device_mutex());
+  if (k.h_ac) cudaFreeHost(k.h_ac);
   for (auto& g : k.cg_graph)
     if (g.exec) cudaGraphExecDestroy(g.exec);
   for (auto& g : k.bicg_graph)

@@ -40,7 +40,7 @@ def krylov_options(method: str = "bicgstab", restart: int = 30, max_iters: int =
     o.method = {"gmres": 0, "bicgstab": 1, "cg": 2}[method]
     o.restart = restart
     o.max_iters = max_iters
-    o.precond = {"none": 0, "jacobi": 1, "block_jacobi": 2, "two_level": 3}[precond]
+    o.precond = {"none": 0, "jacobi": 1, "block_jacobi": 2, "two_level": 3, "two_level_coupled": 4}[precond]
     o.tol = tol
     if isinstance(mixed, str):
         if mixed != "matrix_free":

@@ -74,7 +74,11 @@ typedef struct ufem_krylov_opts {
   int32_t restart;     /* GMRES restart length, default 30                         */
   int32_t max_iters;   /* total Krylov iterations (per refinement pass), 3000    */
   int32_t precond;     /* 0 none, 1 point Jacobi (default), 2 node-block Jacobi,
-                          3 two-level (CG, semi-implicit pressure only)          */
+                          3 two-level (CG, semi-implicit pressure only),
+                          4 two-level for the coupled system (BiCGStab, GMRES):
+                            point Jacobi + a coarse correction on box aggregates
+                            of the pressure rows, coarse matrix = Galerkin
+                            product of the pressure block, rebuilt per solve   */
   double tol;          /* ||b - A x|| / ||b|| target, default 1e-10                */
   int32_t mixed;       /* 0: all FP64; 1: FP32 inner Krylov + FP64 refinement
                           whose residual is b - A x of the stored system; 2: the

@@ -1,0 +1,91 @@
+"""The coupled two-level preconditioner (precond 4, "two_level_coupled"): point
+Jacobi plus a coarse correction on box aggregates of the pressure rows, with
+the Galerkin product of the pressure block as coarse matrix (rebuilt at every
+solve).  The reference preconditions the coupled solve with Ifpack ILU
+(BelosGMRESParameters.cpp:39-40); with point Jacobi alone BiCGStab needs
+hundreds of iterations per step and stalls on fine 2D meshes.
+
+Tolerances as in the other solve tests: residual 1e-12, solution within 1e-6
+of the oracle's ILU-GMRES solve to 1e-13.
+"""
+import numpy as np
+import pytest
+
+from coolfluid3_b200 import NavierStokes
+from coolfluid3_b200 import problems as P
+
+from .util import oracle_for, small_problem, vec_rel_error
+
+pytestmark = pytest.mark.gpu
+
+
+def _system(pb):
+    ns = NavierStokes(pb.coords, pb.conn, dt=pb.dt, use_specializations=False)
+    ns.set_state(pb.up, pb.lin, pb.nu)
+    ns.add_dirichlet(pb.bc_nodes, pb.bc_comps, pb.bc_values)
+    ns.assemble()
+    ns.apply_dirichlet()
+    return ns
+
+
+@pytest.mark.parametrize("dim,n", [(2, 32), (3, 8)])
+@pytest.mark.parametrize("method,mixed", [("bicgstab", False), ("gmres", False), ("bicgstab", True)])
+def test_two_level_solution_matches_oracle_with_fewer_iterations(dim, n, method, mixed):
+    pb = small_problem(dim, n)
+    o = oracle_for(pb, use_specializations=False)
+    o.assemble()
+    o.apply_dirichlet()
+    assert o.solve(tol=1e-13)["rc"] == 0
+    its = {}
+    for pre in ("jacobi", "two_level_coupled"):
+        ns = _system(pb)
+        ns.set_solution(np.zeros(ns.nb_rows))
+        st = ns.solve(method=method, precond=pre, mixed=mixed, tol=1e-12, inner_tol=1e-4, max_iters=6000, restart=60)
+        assert st["converged"] == 1, (pre, st)
+        assert vec_rel_error(ns.solution(), o.solution()) <= 1e-6
+        its[pre] = st["iterations"]
+        ns.close()
+    assert its["two_level_coupled"] * 2 <= its["jacobi"], its
+
+
+def test_two_level_steps_match_oracle_and_are_deterministic():
+    pb = small_problem(3, 6)
+    o = oracle_for(pb, use_specializations=False)
+    runs = []
+    for _ in range(2):
+        ns = _system(pb)
+        for k in range(3):
+            if k:
+                ns.assemble()
+                ns.apply_dirichlet()
+            st = ns.solve(precond="two_level_coupled", tol=1e-12, max_iters=5000)
+            assert st["converged"] == 1
+            ns.update()
+        runs.append(ns.state()[0])
+        ns.close()
+    assert np.array_equal(runs[0], runs[1])  # bitwise repeatable
+    for _ in range(3):
+        o.assemble()
+        o.apply_dirichlet()
+        o.solve(tol=1e-13)
+        o.update()
+    assert vec_rel_error(runs[0], o.state()[0]) <= 1e-6
+
+
+def test_two_level_converges_where_jacobi_stalls():
+    """A 2D lid-driven mesh of 256^2 x 2 triangles (dt = 0.01), where
+    Jacobi-BiCGStab does not reach 1e-10 in 3000 iterations."""
+    pb = P.make_problem(2, 256)
+    ns = _system(pb)
+    st = ns.solve(precond="two_level_coupled", tol=1e-10, max_iters=3000, raise_on_failure=False)
+    assert st["converged"] == 1, st
+    ns.close()
+
+
+def test_two_level_rejects_cg():
+    pb = small_problem(2, 8)
+    ns = _system(pb)
+    from coolfluid3_b200 import UfemError
+    with pytest.raises(UfemError):
+        ns.solve(method="cg", precond="two_level_coupled")
+    ns.close()
