@@ -180,7 +180,8 @@ class Server:
     def __init__(self, hbm_budget_bytes: int, max_slots: int = 64, precision: str = "fp64", mixed: bool = True,
                  krylov: dict | None = None, graphs: bool = True, creators: int = 2,
                  use_specializations: bool = False, realtime: bool = True, large_rows: int = 200_000,
-                 large_workers: int = 2, small_priority: bool = True, mixed_scope: str = "large"):
+                 large_workers: int = 2, small_priority: bool = True, mixed_scope: str = "large",
+                 large_precond: str = "jacobi"):
         """mixed: the mixed-precision form.  Requests of at least `large_rows`
         rows (stepped one at a time by the large workers; their solves are
         bandwidth-bound) assemble FP32 element matrices and solve with FP32
@@ -188,7 +189,9 @@ class Server:
         answers are the FP64 system's.  The batched small requests, whose
         iterations are latency-bound, keep FP64 elements and the FP64 operator
         with mixed_scope "large"; with "all" they iterate with an FP32 copy of
-        the operator and FP64 residual replacement."""
+        the operator and FP64 residual replacement.  large_precond: the
+        preconditioner of the large requests' one-handle solves ("jacobi" or
+        "two_level_coupled"; batches use point Jacobi)."""
         if mixed_scope not in ("large", "all"):
             raise ValueError("mixed_scope must be 'large' or 'all'")
         if precision not in ("fp32", "fp64"):
@@ -210,7 +213,8 @@ class Server:
         # large requests of the mixed form: FP32 element matrices, FP32 inner
         # solves refined against the matrix-free FP64 residual
         self.krylov_large = (dict(self.krylov, mixed="matrix_free", inner_tol=1e-5, max_refine=30) if mixed
-                             else self.krylov)
+                             else dict(self.krylov))
+        self.krylov_large["precond"] = large_precond  # e.g. "two_level_coupled" (one-handle solves only)
         self.mixed_scope = mixed_scope
         self._starved = False
         self._lock = threading.Condition()

@@ -145,3 +145,30 @@ def test_batch_autotuner(specs):
         assert row_scaled_error(v, vr, rp) <= 1e-14 and vec_rel_error(rhs, rhsr) <= 1e-14
     b.close()
     ref.close()
+
+
+def test_sixty_four_members_of_mixed_sizes_identical_alone_and_in_the_mix():
+    """64 2D members of 4..24 cells a side (log-uniform node counts, seeded
+    viscosities): every member's state after two batched steps equals the same
+    member stepped alone, bitwise; a held member (set_active) keeps its state."""
+    rng = np.random.default_rng(64)
+    sides = np.unique(np.round(np.exp(rng.uniform(np.log(4), np.log(24), 64))).astype(int), return_counts=False)
+    specs = [(2, int(sides[k % len(sides)]), 100 + k) for k in range(64)]
+    mixed, sts = run_batch(specs, 2, tol=1e-10, max_iters=3000)
+    assert all(s["converged"] for step in sts for s in step)
+    for k in (0, 17, 40, 63):
+        alone, _ = run_batch([specs[k]], 2, tol=1e-10, max_iters=3000)
+        assert np.array_equal(alone[0], mixed[k]), specs[k]
+    # hold every other member after the first step: the others go on exactly as alone
+    ms = [member(*s) for s in specs[:8]]
+    b = Batch(ms)
+    b.step(tol=1e-10, max_iters=3000)
+    held = [m.state()[0].copy() for m in ms]
+    b.set_active([k % 2 == 0 for k in range(8)])
+    st = b.step(tol=1e-10, max_iters=3000)
+    for k, m in enumerate(ms):
+        if k % 2:
+            assert np.array_equal(m.state()[0], held[k]) and st[k]["iterations"] == 0
+        else:
+            assert np.array_equal(m.state()[0], mixed[k])
+    b.close()

@@ -13,10 +13,13 @@ Tolerances:
  - assembly, FP32 elements: 2e-5 of the row scale, RHS 1e-4 relative (FP32
    rounding of the element arithmetic);
  - states after each step: velocity within 1e-6 relative (the solve tolerance
-   times the system's conditioning), pressure within 1e-4 relative: the cavity's
-   pressure is pinned at one corner node and these systems determine it about
-   three orders of magnitude less well than the velocity (a 1e-12 residual moves
-   it by ~1e-4); the oracle solves to 1e-13, the GPU to 1e-13.
+   times the system's conditioning); pressure within 1e-3 relative, and within
+   1e-5 once the mean offset over the sampled nodes is removed: the cavity's
+   pressure is pinned at one corner node, so its constant mode is determined far
+   less well than the rest (on this mesh a 1e-12 residual moves the pressure by
+   4e-4 relative, almost all of it a constant offset, and the pressure without
+   the offset by 6e-6).  The oracle solves to 1e-13 (ILU-GMRES), the GPU to
+   1e-13 (FP64 refinement of FP32 inner BiCGStab).
 """
 import json
 import os
@@ -52,10 +55,14 @@ def test_cfg2_ten_steps_match_oracle():
         want = np.asarray(rs["samples"])
         ev = max(vec_rel_error(got[:, :3], want[:, :3]), max(abs(a - b) / b for a, b in zip(norms[:3], rs["norms"][:3])))
         ep = max(vec_rel_error(got[:, 3], want[:, 3]), abs(norms[3] - rs["norms"][3]) / rs["norms"][3])
+        dp = got[:, 3] - want[:, 3]
+        eo = float(np.linalg.norm(dp - dp.mean()) / np.linalg.norm(want[:, 3]))
         worst["velocity"] = max(worst["velocity"], ev)
         worst["pressure"] = max(worst["pressure"], ep)
+        worst["pressure_without_offset"] = max(worst.get("pressure_without_offset", 0.0), eo)
         assert ev <= 1e-6, (k, ev)
-        assert ep <= 1e-4, (k, ep)
+        assert ep <= 1e-3, (k, ep)
+        assert eo <= 1e-5, (k, eo)
     print("cfg2 ten steps, worst relative error", worst)
     ns.close()
 
