@@ -69,8 +69,8 @@ def parse():
     ap.add_argument("--serve-elems-3d", type=float, nargs=2, default=[1e4, 2e6],
                     help="log-uniform element-count range of the served 3D requests")
     ap.add_argument("--serve-elems-2d", type=float, nargs=2, default=[1e4, 3e4],
-                    help="log-uniform element-count range of the served 2D requests (Jacobi-BiCGStab does not "
-                         "converge on larger 2D lid-driven meshes at dt = 0.01)")
+                    help="log-uniform element-count range of the served 2D requests (point-Jacobi BiCGStab, the "
+                         "plain path's solver, stalls on larger 2D lid-driven meshes at dt = 0.01)")
     ap.add_argument("--serve-steps", type=int, default=10, help="time steps per served request")
     ap.add_argument("--serve-budget-gb", type=float, default=60.0, help="HBM budget of the server (GB)")
     ap.add_argument("--serve-reps", type=int, default=3, help="served runs per form (the median is reported)")
@@ -592,30 +592,37 @@ def semi_implicit_compare(n: int, steps: int = 3) -> dict:
                              "gmres_iters": list(iters), "converged": rc == 0}}
 
 
-def cfg3_precision(steps: int = 3) -> dict:
+def cfg3_precision(steps: int = 2) -> dict:
     """The precision configuration: 128^3 x 6 tets (12,582,912 tets, 2,146,689
     nodes, 508,839,952 CSR values), nu drawn log-uniform in [1e-4, 1e-2] from the
-    seed.  The product form assembles FP32 element matrices (FP64 scatter) and
-    solves with FP32 inner BiCGStab + Jacobi refined to 1e-8 against the
-    matrix-free FP64 residual; each step's state is compared with an FP64-element
-    handle stepped from the same start with an FP64 BiCGStab to 1e-12."""
+    seed, FP32 element matrices with FP64 scatter.  Two solve forms step from the
+    same start: "configured" -- FP32 inner BiCGStab + Jacobi refined to 1e-8
+    against the matrix-free FP64 residual (the configuration's Jacobi and 1e-8;
+    BiCGStab because GMRES(30) does not converge on these systems) -- and
+    "product" -- the same refinement with the coupled two-level preconditioner to
+    1e-12.  Each step's state is compared with an FP64-element handle refined to
+    1e-13 (velocity, pressure, and pressure without its mean offset: the
+    pressure's constant mode is pinned at one node only)."""
     import torch
     from coolfluid3_b200 import NavierStokes, problems as P
     t0 = time.perf_counter()
     pb = P.config("cfg3")
     gen_s = time.perf_counter() - t0
+    forms = {"configured": ("fp32", dict(mixed="matrix_free", tol=1e-8, inner_tol=1e-4, max_iters=8000)),
+             "product": ("fp32", dict(mixed="matrix_free", tol=1e-12, inner_tol=1e-5, max_iters=8000,
+                                      precond="two_level_coupled")),
+             "fp64_1e-13": ("fp64", dict(mixed=True, tol=1e-13, inner_tol=1e-5, max_iters=8000, max_refine=40,
+                                         precond="two_level_coupled"))}
     hs = {}
-    for label, prec in (("fp32_elements", "fp32"), ("fp64", "fp64")):
+    for label, (prec, _) in forms.items():
         ns = NavierStokes(pb.coords, pb.conn, dt=pb.dt, use_specializations=False, precision=prec)
         ns.set_state(pb.up, pb.lin, pb.nu)
         ns.add_dirichlet(pb.bc_nodes, pb.bc_comps, pb.bc_values)
         ns.enable_timing(True)
         hs[label] = ns
-    out = {"workload": f"3D P1 tets 128^3x6 ({pb.nb_elems} tets, {pb.nb_nodes} nodes, {hs['fp64'].nnz} CSR values), "
-                       f"nu {pb.nu[0]:.3e}, dt {pb.dt}", "setup_s": round(time.perf_counter() - t0, 1),
+    out = {"workload": f"3D P1 tets 128^3x6 ({pb.nb_elems} tets, {pb.nb_nodes} nodes, {hs['product'].nnz} CSR "
+                       f"values), nu {pb.nu[0]:.3e}, dt {pb.dt}", "setup_s": round(time.perf_counter() - t0, 1),
            "generate_s": round(gen_s, 1), "steps": []}
-    forms = {"fp32_elements": dict(mixed="matrix_free", tol=1e-8, inner_tol=1e-4, max_iters=8000),
-             "fp64": dict(tol=1e-12, max_iters=12000)}
     for k in range(steps):
         row = {}
         for label, ns in hs.items():
@@ -624,23 +631,26 @@ def cfg3_precision(steps: int = 3) -> dict:
             ns.assemble()
             asm_ms = ns.timings()["assembly_ms"]
             ns.apply_dirichlet()
-            st = ns.solve(raise_on_failure=False, **forms[label])
+            st = ns.solve(raise_on_failure=False, **forms[label][1])
             ns.update()
             torch.cuda.synchronize()
             row[label] = {"step_ms": round((time.perf_counter() - t) * 1e3, 1), "assembly_ms": round(asm_ms, 3),
                           "krylov_iters": st["iterations"], "refinements": st.get("refinements", 0),
                           "converged": int(st["converged"]), "rel_residual": st["rel_residual"]}
-        a, b = hs["fp32_elements"].state()[0], hs["fp64"].state()[0]
-        d = a - b
-        row["rel_err_vs_fp64"] = {"state": float(np.linalg.norm(d) / np.linalg.norm(b)),
-                                  "velocity": float(np.linalg.norm(d[:, :3]) / np.linalg.norm(b[:, :3])),
-                                  "pressure": float(np.linalg.norm(d[:, 3]) / np.linalg.norm(b[:, 3]))}
+        ref = hs["fp64_1e-13"].state()[0]
+        for label in ("configured", "product"):
+            d = hs[label].state()[0] - ref
+            dp = d[:, 3] - d[:, 3].mean()
+            row[label]["rel_err_vs_fp64"] = {
+                "velocity": float(np.linalg.norm(d[:, :3]) / np.linalg.norm(ref[:, :3])),
+                "pressure": float(np.linalg.norm(d[:, 3]) / np.linalg.norm(ref[:, 3])),
+                "pressure_without_offset": float(np.linalg.norm(dp) / np.linalg.norm(ref[:, 3]))}
         out["steps"].append(row)
     for ns in hs.values():
         ns.close()
-    out["form"] = ("FP32 element arithmetic, FP64 scatter; FP32-operator BiCGStab + Jacobi inner solves (to 1e-4) "
-                   "refined to 1e-8 with the matrix-free FP64 residual; reference: FP64 elements, FP64 BiCGStab + "
-                   "Jacobi to 1e-12 (GMRES(30) does not converge on these systems)")
+    out["form"] = ("FP32 element arithmetic, FP64 scatter; FP32-operator BiCGStab inner solves refined with the "
+                   "matrix-free FP64 residual; configured: point Jacobi to 1e-8; product: coupled two-level "
+                   "preconditioner to 1e-12; reference: FP64 elements refined to 1e-13")
     return out
 
 
@@ -757,7 +767,8 @@ def serving_compare(args):
                               nsteps=args.serve_steps, seed=20261203)
     gen_s = time.perf_counter() - t0
     tol = 1e-12  # both sides at the residual that keeps the state within 1e-6 of the FP64 oracle
-    plain, pst = S.run_plain(reqs, krylov=dict(tol=tol, max_iters=6000), realtime=True)
+    plain, pst = S.run_plain(reqs, krylov=dict(tol=tol, max_iters=20000), realtime=True)
+    plain2, pst2 = S.run_plain(reqs, krylov=dict(tol=tol, max_iters=20000, precond="two_level_coupled"), realtime=True)
 
     def pick(st, res):
         return {"steps_per_s": round(st["steps_per_s"], 3), "seconds": round(st["seconds"], 3),
@@ -770,10 +781,13 @@ def serving_compare(args):
         "workload": (f"{len(reqs)} lid-driven requests, Poisson arrivals {args.serve_rate}/s, 3D tets with "
                      f"{elems[3][0]:.0e}..{elems[3][1]:.0e} elements and 2D tris with {elems[2][0]:.0e}.."
                      f"{elems[2][1]:.0e} (log-uniform; total {sum(r.nb_elems for r in reqs)}), nu log-uniform "
-                     f"1e-4..1e-2, {args.serve_steps} steps each, relative residual 1e-10"),
+                     f"1e-4..1e-2, {args.serve_steps} steps each, relative residual {tol:g}"),
         "plain": dict(pick(pst, plain), form="FP64 elements, FP64 BiCGStab + Jacobi, one request at a time"),
+        "plain_two_level": dict(pick(pst2, plain2),
+                                form="FP64 elements, FP64 BiCGStab + the coupled two-level preconditioner, one request "
+                                     "at a time"),
     }
-    forms = (("served_fp64", False, "jacobi"), ("served_mixed", True, "two_level_coupled"))
+    forms = (("served_fp64", False, "two_level_coupled"), ("served_mixed", True, "two_level_coupled"))
     for label, mixed, lpre in forms:
         # the served makespan depends on how the threads and streams interleave on
         # the device, so each form is served `serve_reps` times and the run with
@@ -781,7 +795,8 @@ def serving_compare(args):
         runs = []
         for _ in range(max(1, args.serve_reps)):
             srv = S.Server(int(args.serve_budget_gb * 1e9), precision="fp64", mixed=mixed,
-                           krylov=dict(tol=tol, max_iters=6000), realtime=True, large_precond=lpre)
+                           krylov=dict(tol=tol, max_iters=20000), realtime=True, large_precond=lpre,
+                           large_rows_2d=40_000)
             res, st = srv.run(reqs)
             runs.append((st["steps_per_s"], st, res, srv))
         runs.sort(key=lambda x: x[0])
@@ -790,6 +805,7 @@ def serving_compare(args):
                  for a, b in zip(res, plain) if a.ok and b.ok]
         out[label] = dict(pick(st, res), max_batch=srv.max_batch, peak_reserved_gb=round(srv.peak_bytes / 1e9, 3),
                           speedup_steps_per_s=round(st["steps_per_s"] / pst["steps_per_s"], 3),
+                          speedup_vs_plain_two_level=round(st["steps_per_s"] / pst2["steps_per_s"], 3),
                           runs_steps_per_s=[round(r[0], 2) for r in runs],
                           max_rel_diff_vs_plain=max(diffs) if diffs else None,
                           form=(("large requests: FP32 element matrices, FP32 inner BiCGStab with the coupled "
@@ -806,13 +822,14 @@ def serving_compare(args):
     for rate in args.serve_sweep:
         rq = S.poisson_workload(args.serve_requests, rate=rate, elems=elems, nu=(1e-4, 1e-2),
                                 nsteps=args.serve_steps, seed=20261203 + int(rate))
-        _, ps = S.run_plain(rq, krylov=dict(tol=tol, max_iters=6000), realtime=True)
+        _, ps = S.run_plain(rq, krylov=dict(tol=tol, max_iters=20000), realtime=True)
         row = {"rate_per_s": rate, "plain": {"steps_per_s": round(ps["steps_per_s"], 2),
                                              "step_ms_p50": round(ps["step_ms"]["p50"], 2),
                                              "step_ms_p99": round(ps["step_ms"]["p99"], 2)}}
         for label, mixed, lpre in forms:
             srv = S.Server(int(args.serve_budget_gb * 1e9), precision="fp64", mixed=mixed,
-                           krylov=dict(tol=tol, max_iters=6000), realtime=True, large_precond=lpre)
+                           krylov=dict(tol=tol, max_iters=20000), realtime=True, large_precond=lpre,
+                           large_rows_2d=40_000)
             _, st = srv.run(rq)
             row[label] = {"steps_per_s": round(st["steps_per_s"], 2), "step_ms_p50": round(st["step_ms"]["p50"], 2),
                           "step_ms_p99": round(st["step_ms"]["p99"], 2),

@@ -166,19 +166,21 @@ __device__ __forceinline__ void generic_row(const int (&ids)[4], int a, const No
   const T V = det * T(D == 2 ? 0.5 : 1.0 / 6.0);
   const T m1 = V * inv_n;
   const T m2 = V * T(1.0 / (n * (n + 1)));
-  // alpha_b and w_b here; c_0b and D0_b are formed inside the column loop below
-  // (the same sums), which keeps fewer values live across it
-  T alpha[n], w[n];
+  T alpha[n], w[n], c0[n], D0[n];
 #pragma unroll
   for (int b = 0; b < n; ++b) {
-    T a = 0, ww = 0;
+    T a = 0, ww = 0, cc = 0, dd = 0;
 #pragma unroll
     for (int k = 0; k < D; ++k) {
       a += ub[k] * G[k][b];
       ww += el.U[b][k] * G[k][0];
+      cc += el.U[0][k] * G[k][b];
+      dd += G[k][0] * G[k][b];
     }
     alpha[b] = a;
     w[b] = ww;
+    c0[b] = cc;
+    D0[b] = dd;
   }
   T q[D];
 #pragma unroll
@@ -218,7 +220,10 @@ __device__ __forceinline__ void generic_row(const int (&ids)[4], int a, const No
       au[i] = m2 * (nT * gbar + F[0][i]) + tsum2 * (n2 * gbar * alpha[0] + gw);
     }
   }
-  // A x for the RHS from the nodal state (u, p), read column by column
+  // nodal state (u, p) of the element: A x for the RHS
+  T xs[n][neq];
+#pragma unroll
+  for (int b = 0; b < n; ++b) load_state<D, T>(nd, ids[b], xs[b]);
   T div = 0, gradp[D], kx[D], ax[D];
 #pragma unroll
   for (int i = 0; i < D; ++i) {
@@ -237,16 +242,7 @@ __device__ __forceinline__ void generic_row(const int (&ids)[4], int a, const No
   }
 #pragma unroll
   for (int b = 0; b < n; ++b) {
-    T xb[neq];
-    load_state<D, T>(nd, ids[b], xb);
-    T cc = 0, dd = 0;
-#pragma unroll
-    for (int k = 0; k < D; ++k) {
-      cc += el.U[0][k] * G[k][b];
-      dd += G[k][0] * G[k][b];
-    }
-    const T c0b = cc, D0b = dd;
-    const T Kd = nu_bar * V * D0b + m2 * (nT * alpha[b] + c0b);
+    const T Kd = nu_bar * V * D0[b] + m2 * (nT * alpha[b] + c0[b]);
     T qg = 0;
 #pragma unroll
     for (int k = 0; k < D; ++k) qg += q[k] * G[k][b];
@@ -269,16 +265,16 @@ __device__ __forceinline__ void generic_row(const int (&ids)[4], int a, const No
       T row[neq];
 #pragma unroll
       for (int j = 0; j < D; ++j) row[j] = G[j][b] * sWSp + (cj[j] * Vab + ej[j]);
-      row[D] = D0b * tpv;
+      row[D] = D0[b] * tpv;
       sk.template row<neq>((b * neq + D) * neq, row);
     }
     // pieces of A x
 #pragma unroll
     for (int k = 0; k < D; ++k) {
-      div += G[k][b] * xb[k];
-      gradp[k] += G[k][b] * xb[D];
-      kx[k] += Kdb * xb[k];
-      ax[k] += Vab * xb[k];
+      div += G[k][b] * xs[b][k];
+      gradp[k] += G[k][b] * xs[b][D];
+      kx[k] += Kdb * xs[b][k];
+      ax[k] += Vab * xs[b][k];
     }
   }
   // rhs row 0 = a - A x  (A before the theta combination)

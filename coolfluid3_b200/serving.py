@@ -181,7 +181,7 @@ class Server:
                  krylov: dict | None = None, graphs: bool = True, creators: int = 2,
                  use_specializations: bool = False, realtime: bool = True, large_rows: int = 200_000,
                  large_workers: int = 2, small_priority: bool = True, mixed_scope: str = "large",
-                 large_precond: str = "jacobi"):
+                 large_precond: str = "jacobi", large_rows_2d: int | None = None):
         """mixed: the mixed-precision form.  Requests of at least `large_rows`
         rows (stepped one at a time by the large workers; their solves are
         bandwidth-bound) assemble FP32 element matrices and solve with FP32
@@ -204,6 +204,9 @@ class Server:
         self.spec = use_specializations
         self.realtime = realtime
         self.large_rows = int(large_rows)
+        # 2D requests go to the one-handle path from a lower size: the batched
+        # solve is point-Jacobi BiCGStab, which stalls on fine 2D lid-driven meshes
+        self.large_rows_2d = self.large_rows if large_rows_2d is None else int(large_rows_2d)
         self.large_workers = int(large_workers)
         self.small_priority = bool(small_priority)
         self.krylov = dict(method="bicgstab", precond="jacobi", tol=1e-10, max_iters=3000)
@@ -223,6 +226,9 @@ class Server:
         self.peak_bytes = 0
         self.max_batch = 0
         self.errors: list = []
+
+    def _is_large(self, dim: int, rows: int) -> bool:
+        return rows >= (self.large_rows_2d if dim == 2 else self.large_rows)
 
     # -- budget ---------------------------------------------------------------
     def _try_reserve(self, nbytes: int) -> bool:
@@ -382,7 +388,7 @@ class Server:
 
         def create(req: Request, est: int, admitted: float):
             try:
-                large = req.coords.shape[0] * (req.dim + 1) >= self.large_rows
+                large = self._is_large(req.dim, req.coords.shape[0] * (req.dim + 1))
                 ns = _new_handle(req, "fp32" if (large and self.mixed) else self.precision, self.spec)
             except Exception as e:  # the request is rejected; the others go on
                 self._release(est)
@@ -397,7 +403,7 @@ class Server:
             a = _Active(req, ns, admitted, actual)
             a.result.ready = now()
             with self._lock:
-                cls = "large" if ns.nb_rows >= self.large_rows else "small"
+                cls = "large" if self._is_large(req.dim, ns.nb_rows) else "small"
                 inbox[(req.dim, cls)].append(a)
                 self._lock.notify_all()
 

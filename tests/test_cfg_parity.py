@@ -11,15 +11,15 @@ Tolerances:
  - assembly, FP64 elements: 1e-11 of each CSR row's largest |entry|; RHS 1e-11
    relative (the same bound as the small-mesh parity tests);
  - assembly, FP32 elements: 2e-5 of the row scale, RHS 1e-4 relative (FP32
-   rounding of the element arithmetic);
- - states after each step: velocity within 1e-6 relative (the solve tolerance
-   times the system's conditioning); pressure within 1e-3 relative, and within
-   1e-5 once the mean offset over the sampled nodes is removed: the cavity's
-   pressure is pinned at one corner node, so its constant mode is determined far
-   less well than the rest (on this mesh a 1e-12 residual moves the pressure by
-   4e-4 relative, almost all of it a constant offset, and the pressure without
-   the offset by 6e-6).  The oracle solves to 1e-13 (ILU-GMRES), the GPU to
-   1e-13 (FP64 refinement of FP32 inner BiCGStab).
+   rounding of the element arithmetic; measured 1.9e-7 and 4.7e-6);
+ - states after each step: velocity within 1e-6 relative; pressure within 1e-4
+   relative, and within 1e-6 once the mean offset over the sampled nodes is
+   removed: the cavity's pressure is pinned at one corner node, so its constant
+   mode is determined far less well than the rest (on this mesh a 1e-12 residual
+   moves the pressure by 4e-4 relative, almost all of it a constant offset).  The
+   oracle solves to 1e-13 (ILU-GMRES), the GPU to 1e-13 (FP64 refinement of FP32
+   inner BiCGStab); measured: velocity 6.3e-9, pressure 4.8e-6, pressure without
+   the offset 1.2e-7.
 """
 import json
 import os
@@ -61,8 +61,8 @@ def test_cfg2_ten_steps_match_oracle():
         worst["pressure"] = max(worst["pressure"], ep)
         worst["pressure_without_offset"] = max(worst.get("pressure_without_offset", 0.0), eo)
         assert ev <= 1e-6, (k, ev)
-        assert ep <= 1e-3, (k, ep)
-        assert eo <= 1e-5, (k, eo)
+        assert ep <= 1e-4, (k, ep)
+        assert eo <= 1e-6, (k, eo)
     print("cfg2 ten steps, worst relative error", worst)
     ns.close()
 
