@@ -79,6 +79,13 @@ struct BatchMesh {
   const int64_t* fix_pos;
   const int32_t* fix_bc;
   int active;  // 0: held (ufem_batch_set_active): no solve, no update
+  // coarse space of the coupled two-level preconditioner (nc = 0: none)
+  int nc;
+  int64_t c_off;  // first coarse dof in the concatenated coarse vectors
+  const int32_t* agg;
+  const int32_t* agg_ptr;
+  const int32_t* agg_rows;
+  const double* ainv;
 };
 
 struct Chunk {
@@ -560,11 +567,65 @@ __global__ void bicg_p_batch_kernel(const Chunk* __restrict__ chunks, const Batc
     const int64_t k = off + i;
     const double pi = r[k] + beta * (p[k] - om * v[k]);
     p[k] = pi;
-    ph[k] = pkind == 1 ? dinv[k] * pi : pi;
+    ph[k] = (pkind == 1 || pkind == 4) ? dinv[k] * pi : pi;
   }
 }
 
 
+
+// Coupled two-level preconditioner over the batch (z += R Ac^-1 R^T v per
+// member).  Restriction: one warp per coarse dof of all members, the sum over
+// its aggregate's rows (ascending) in a fixed lane partition and shuffle tree.
+__global__ void restrict_batch_kernel(int64_t total_c, int nmesh, const int64_t* __restrict__ cprefix,
+                                      const BatchMesh* __restrict__ bm, const double* __restrict__ v,
+                                      double* __restrict__ c, const int* __restrict__ ictl) {
+  const int64_t q = (int64_t(blockIdx.x) * blockDim.x + threadIdx.x) >> 5;
+  const int lane = threadIdx.x & 31;
+  if (q >= total_c) return;  // whole warps
+  const int m = find_mesh(cprefix, nmesh, q);
+  if (ictl[m * kIc + fDone]) return;
+  const BatchMesh& M = bm[m];
+  const int I = int(q - cprefix[m]);
+  double s = 0.0;
+  for (int k = M.agg_ptr[I] + lane; k < M.agg_ptr[I + 1]; k += 32) s += v[M.row_off + M.agg_rows[k]];
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
+  if (lane == 0) c[q] = s;
+}
+
+// y = Ac^-1 c per member, one warp per coarse row.
+__global__ void coarse_batch_kernel(int64_t total_c, int nmesh, const int64_t* __restrict__ cprefix,
+                                    const BatchMesh* __restrict__ bm, const double* __restrict__ c,
+                                    double* __restrict__ y, const int* __restrict__ ictl) {
+  const int64_t q = (int64_t(blockIdx.x) * blockDim.x + threadIdx.x) >> 5;
+  const int lane = threadIdx.x & 31;
+  if (q >= total_c) return;
+  const int m = find_mesh(cprefix, nmesh, q);
+  if (ictl[m * kIc + fDone]) return;
+  const BatchMesh& M = bm[m];
+  const int I = int(q - cprefix[m]);
+  const double* row = M.ainv + int64_t(I) * M.nc;
+  const double* cm = c + M.c_off;
+  double s = 0.0;
+  for (int J = lane; J < M.nc; J += 32) s += row[J] * cm[J];
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
+  if (lane == 0) y[q] = s;
+}
+
+// z += y[agg] on the coarse rows of each chunk's member.
+__global__ void prolong_add_batch_kernel(const Chunk* __restrict__ chunks, const BatchMesh* __restrict__ bm,
+                                         const double* __restrict__ y, double* __restrict__ z,
+                                         const int* __restrict__ ictl) {
+  const Chunk c = chunks[blockIdx.x];
+  if (ictl[c.mesh * kIc + fDone]) return;
+  const BatchMesh& M = bm[c.mesh];
+  if (M.nc == 0) return;
+  for (int i = c.lo + threadIdx.x; i < c.hi; i += blockDim.x) {
+    const int a = M.agg[i];
+    if (a >= 0) z[M.row_off + i] += y[M.c_off + a];
+  }
+}
 
 // s = r - alpha v, sh = D^-1 s
 __global__ void bicg_s_batch_kernel(const Chunk* __restrict__ chunks, const BatchMesh* __restrict__ bm, int pkind,
@@ -580,7 +641,7 @@ __global__ void bicg_s_batch_kernel(const Chunk* __restrict__ chunks, const Batc
     const int64_t k = off + i;
     const double si = r[k] - al * v[k];
     s[k] = si;
-    sh[k] = pkind == 1 ? dinv[k] * si : si;
+    sh[k] = (pkind == 1 || pkind == 4) ? dinv[k] * si : si;
   }
 }
 
@@ -718,6 +779,12 @@ struct ufem_batch {
   std::vector<ufem_ns_handle*> members;
   std::vector<int32_t> active;  // per member: 1 stepped, 0 held
   bool active_dirty = false;
+  std::vector<CoarseView> coarse;  // per member (two-level preconditioner); nc = 0: none
+  int64_t total_c = 0;             // coarse dofs of all members
+  int64_t* d_coarse_prefix = nullptr;
+  double* cvec = nullptr;          // total_c: R^T v of every member
+  double* yvec = nullptr;          // total_c: Ac^-1 R^T v
+  int64_t c_cap = 0;
   int dim = 0, neq = 0, precision = 0, spec = 0, warps = 4;
   int nmesh = 0;
   int64_t total_nodes = 0, total_rows = 0, total_bc = 0, total_fix = 0;
@@ -757,6 +824,7 @@ void batch_free(ufem_batch* b) {
   dfr(b->d_fix_prefix); dfr(b->d_chunks); dfr(b->d_cprefix);
   dfr(b->r); dfr(b->rh); dfr(b->p); dfr(b->v); dfr(b->s); dfr(b->t); dfr(b->ph); dfr(b->sh); dfr(b->dinv);
   dfr(b->w); dfr(b->part); dfr(b->counters); dfr(b->dctl); dfr(b->ictl);
+  dfr(b->d_coarse_prefix); dfr(b->cvec); dfr(b->yvec);
   if (b->h_dctl) cudaFreeHost(b->h_dctl);
   if (b->h_ictl) cudaFreeHost(b->h_ictl);
   delete b;
@@ -804,14 +872,40 @@ int batch_refresh(ufem_batch* b) {
     M.fix_pos = P.fix_pos;
     M.fix_bc = P.fix_bc;
     M.active = b->active[m];
+    const CoarseView cv = m < int(b->coarse.size()) ? b->coarse[m] : CoarseView{};
+    M.nc = cv.nc;
+    M.agg = cv.agg;
+    M.agg_ptr = cv.agg_ptr;
+    M.agg_rows = cv.agg_rows;
+    M.ainv = cv.ainv;
     bcp[m + 1] = bcp[m] + P.nbc;
     fxp[m + 1] = fxp[m] + P.nfix_rows;
   }
   int64_t off = 0;
+  std::vector<int64_t> cpre(size_t(b->nmesh) + 1, 0);
   for (int m = 0; m < b->nmesh; ++m) {
     bm[m].row_off = off;
     off += bm[m].nrows;
+    bm[m].c_off = cpre[size_t(m)];
+    cpre[size_t(m) + 1] = cpre[size_t(m)] + bm[m].nc;
   }
+  if (cpre[size_t(b->nmesh)] != b->total_c) {  // the coarse kernels' grids change: recapture the iteration graphs
+    DeviceLock lk(device_mutex());
+    for (int k = 0; k < 2; ++k)
+      if (b->block_exec[k]) {
+        cudaGraphExecDestroy(b->block_exec[k]);
+        b->block_exec[k] = nullptr;
+      }
+  }
+  b->total_c = cpre[size_t(b->nmesh)];
+  if (b->total_c > b->c_cap) {
+    dfr(b->cvec);
+    dfr(b->yvec);
+    if ((rc = dmal(&b->cvec, size_t(b->total_c))) || (rc = dmal(&b->yvec, size_t(b->total_c)))) return rc;
+    b->c_cap = b->total_c;
+  }
+  if (!b->d_coarse_prefix && (rc = dmal(&b->d_coarse_prefix, size_t(b->nmesh) + 1))) return rc;
+  UFEM_CUDA_TRY(cudaMemcpy(b->d_coarse_prefix, cpre.data(), cpre.size() * 8, cudaMemcpyHostToDevice));
   b->total_bc = bcp[b->nmesh];
   b->total_fix = fxp[b->nmesh];
   UFEM_CUDA_TRY(cudaMemcpy(b->d_asm, ad.data(), ad.size() * sizeof(AsmDesc), cudaMemcpyHostToDevice));
@@ -845,6 +939,18 @@ int spmv_b(ufem_batch* b, double* x, double* y, cudaStream_t st, int skip_flag =
   return UFEM_OK;
 }
 
+// z += R Ac^-1 R^T v for every member with a coarse space (two-level form).
+int coarse_correct_b(ufem_batch* b, const double* v, double* z, cudaStream_t st) {
+  if (b->total_c == 0) return UFEM_OK;
+  const unsigned gw = unsigned((b->total_c * 32 + 255) / 256);
+  restrict_batch_kernel<<<gw, 256, 0, st>>>(b->total_c, b->nmesh, b->d_coarse_prefix, b->d_mesh, v, b->cvec, b->ictl);
+  coarse_batch_kernel<<<gw, 256, 0, st>>>(b->total_c, b->nmesh, b->d_coarse_prefix, b->d_mesh, b->cvec, b->yvec,
+                                          b->ictl);
+  prolong_add_batch_kernel<<<unsigned(b->nchunks), kThreads, 0, st>>>(b->d_chunks, b->d_mesh, b->yvec, z, b->ictl);
+  UFEM_CUDA_TRY(cudaGetLastError());
+  return UFEM_OK;
+}
+
 // One BiCGStab iteration for every member that is not done: seven launches
 // (p update; SpMV; rh.v + alpha; s update; SpMV; t.s, t.t + omega; x, r update
 // + rho and convergence), the scalars computed by each mesh's last CTA.
@@ -854,11 +960,13 @@ int bicg_iteration(ufem_batch* b, int pkind, double* xwork, cudaStream_t st) {
   int rc;
   bicg_p_batch_kernel<<<nc, kThreads, 0, st>>>(b->d_chunks, b->d_mesh, pkind, b->dinv, b->r, b->v, b->p, b->ph,
                                                 b->dctl, b->ictl);
+  if (pkind == 4 && (rc = coarse_correct_b(b, b->p, b->ph, st))) return rc;
   if ((rc = spmv_b<MT, kWork>(b, b->ph, b->v, st))) return rc;
   dot_fold_batch_kernel<1><<<nc, kThreads, 0, st>>>(b->d_chunks, b->d_mesh, b->d_cprefix, b->rh, b->v, b->part,
                                                      b->nchunks, b->dctl, b->ictl, b->counters);
   bicg_s_batch_kernel<<<nc, kThreads, 0, st>>>(b->d_chunks, b->d_mesh, pkind, b->dinv, b->r, b->v, b->s, b->sh,
                                                 b->dctl, b->ictl);
+  if (pkind == 4 && (rc = coarse_correct_b(b, b->s, b->sh, st))) return rc;
   if ((rc = spmv_b<MT, kWork>(b, b->sh, b->t, st))) return rc;
   dot_fold_batch_kernel<2><<<nc, kThreads, 0, st>>>(b->d_chunks, b->d_mesh, b->d_cprefix, b->t, b->s, b->part,
                                                      b->nchunks, b->dctl, b->ictl, b->counters);
@@ -896,7 +1004,8 @@ int bicgstab_b(ufem_batch* b, int pkind, double tol, int maxit, bool use_outer, 
     UFEM_CUDA_TRY(cudaMemcpyAsync(b->ictl, b->h_ictl, sizeof(int) * kIc * b->nmesh, cudaMemcpyHostToDevice, st));
   else
     UFEM_CUDA_TRY(cudaMemsetAsync(b->ictl, 0, sizeof(int) * kIc * b->nmesh, st));
-  if (pkind == 1) jacobi_batch_kernel<MT><<<nc, kThreads, 0, st>>>(b->d_chunks, b->d_mesh, b->dinv, b->ictl);
+  if (pkind == 1 || pkind == 4)
+    jacobi_batch_kernel<MT><<<nc, kThreads, 0, st>>>(b->d_chunks, b->d_mesh, b->dinv, b->ictl);
   // the initial residual is FP64 in a mixed solve (residual replacement)
   if ((rc = reliable ? residual_b<double, XL, BL>(b, xw, bw, true, false, st)
                      : residual_b<MT, XL, BL>(b, xw, bw, true, false, st)))
@@ -1201,7 +1310,8 @@ int ufem_batch_solve(ufem_batch* b, const ufem_krylov_opts* kopts, ufem_krylov_s
   ufem_krylov_default_opts(&o);
   if (kopts) o = *kopts;
   if (o.method != 1) return set_error(UFEM_ERR_ARG, "the batched solve is BiCGStab (method 1)");
-  if (o.precond != 0 && o.precond != 1) return set_error(UFEM_ERR_ARG, "the batched solve supports precond 0 or 1");
+  if (o.precond != 0 && o.precond != 1 && o.precond != 4)
+    return set_error(UFEM_ERR_ARG, "the batched solve supports precond 0, 1 or 4");
   if (o.max_iters <= 0) o.max_iters = 3000;
   if (o.tol <= 0) o.tol = 1e-10;
   if (o.max_refine <= 0) o.max_refine = 20;
@@ -1222,6 +1332,30 @@ int ufem_batch_solve(ufem_batch* b, const ufem_krylov_opts* kopts, ufem_krylov_s
       UFEM_CUDA_TRY(cudaStreamSynchronize(st));
       if ((rc = batch_refresh(b))) return rc;
     }
+  }
+  if (o.precond == 4) {
+    // every member's coarse space and coarse matrix (of its current system);
+    // aggregates capped at 12 x 12 (2D) and 5^3 (3D) boxes, so that the host
+    // inversions of all members stay short
+    if (b->coarse.size() != size_t(b->nmesh)) b->coarse.assign(size_t(b->nmesh), CoarseView{});
+    bool any_new = false;
+    for (int m = 0; m < b->nmesh; ++m) {
+      if (!b->active[m]) continue;
+      bool rebuilt = false;
+      CoarseView cv;
+      if ((rc = krylov_coupled_coarse(b->members[m], st, 12, 5, &rebuilt, &cv))) return rc;
+      const CoarseView& old = b->coarse[m];
+      if (rebuilt || cv.nc != old.nc || cv.ainv != old.ainv || cv.agg != old.agg) any_new = true;
+      b->coarse[m] = cv;
+    }
+    if (any_new) {
+      UFEM_CUDA_TRY(cudaStreamSynchronize(st));
+      if ((rc = batch_refresh(b))) return rc;
+    }
+  } else if (!b->coarse.empty()) {  // back to point Jacobi: no coarse spaces in the descriptors
+    b->coarse.clear();
+    UFEM_CUDA_TRY(cudaStreamSynchronize(st));
+    if ((rc = batch_refresh(b))) return rc;
   }
   std::vector<int> iters(b->nmesh, 0), status(b->nmesh, 0), refines(b->nmesh, 0);  // refines: FP64 replacements
   // Plain: FP64 operator.  Mixed: FP32 copy of the operator in the

@@ -250,6 +250,19 @@ void destroy_handle(ufem_ns_handle* h);
 int krylov_solve(ufem_ns_handle* h, const ufem_krylov_opts* ko, ufem_krylov_status* st, cudaStream_t s);
 int krylov_apply(ufem_ns_handle* h, const double* d_x, double* d_y, cudaStream_t s);
 int krylov_fp64_residual(ufem_ns_handle* h, double* r_host, cudaStream_t s);
+// Coarse space of the coupled two-level preconditioner of one handle, rebuilt
+// when its Dirichlet plan or the aggregate caps change (rebuilt = true) and its
+// coarse matrix refreshed from the current system (krylov.cu).  nc = 0: no
+// usable coarse space (point Jacobi).
+struct CoarseView {
+  int nc = 0;
+  const int32_t* agg = nullptr;
+  const int32_t* agg_ptr = nullptr;
+  const int32_t* agg_rows = nullptr;
+  const double* ainv = nullptr;
+};
+int krylov_coupled_coarse(ufem_ns_handle* h, cudaStream_t s, int max_side_2d, int max_side_3d, bool* rebuilt,
+                          CoarseView* view);
 void krylov_free(ufem_ns_handle* h);
 // Aggregates of the two-level CG preconditioner (precond 3) of a one-equation
 // system: agg[row] in [0, nc) or -1; builds and inverts the Galerkin coarse

@@ -81,6 +81,7 @@ struct KrylovWork {
   double* acd = nullptr;       // nc x nc coarse matrix on the device
   double* h_ac = nullptr;      // pinned host copy (nc x nc)
   int64_t cp_bc_version = -1;  // Dirichlet plan the structure was built for
+  int cp_caps = -1;            // aggregate caps it was built with (2D side * 1000 + 3D side)
   bool cp_spd = false;         // the last coarse matrix was positive definite
 };
 
@@ -1475,8 +1476,9 @@ namespace {
 // Dirichlet plan: the aggregate of each row, the rows of each aggregate, and
 // the pressure-pressure CSR positions sorted by (row aggregate, column
 // aggregate, position) with their segments.
-int coupled_coarse_build(ufem_ns_handle* h) {
+int coupled_coarse_build(ufem_ns_handle* h, int max_side_2d, int max_side_3d) {
   KrylovWork& kw = *h->kw;
+  kw.cp_caps = max_side_2d * 1000 + max_side_3d;
   dfree(kw.agg); dfree(kw.agg_ptr); dfree(kw.agg_rows); dfree(kw.ainv); dfree(kw.cvec); dfree(kw.yvec);
   dfree(kw.cp_pos); dfree(kw.cp_seg); dfree(kw.cp_dst); dfree(kw.acd);
   if (kw.h_ac) {
@@ -1504,7 +1506,7 @@ int coupled_coarse_build(ufem_ns_handle* h) {
       hi[d] = std::max(hi[d], h->coords_h[size_t(i * dim + d)]);
     }
   int k = int(std::floor(std::pow(double(N) / 64.0, 1.0 / dim)));
-  k = std::max(1, std::min(k, dim == 3 ? 7 : 20));
+  k = std::max(1, std::min(k, dim == 3 ? max_side_3d : max_side_2d));
   std::vector<int32_t> box(size_t(N), -1), id(size_t(std::pow(k, dim)) + 1, -1);
   int nc = 0;
   for (int64_t i = 0; i < N; ++i) {
@@ -1583,10 +1585,13 @@ int coupled_coarse_build(ufem_ns_handle* h) {
 // The coarse matrix of the current system (FP64 values, after the Dirichlet
 // pass), its inverse on the host, uploaded for the solve; cp_spd false (point
 // Jacobi for this solve) when it is not positive definite.
-int coupled_coarse_refresh(ufem_ns_handle* h, cudaStream_t s) {
+int coupled_coarse_refresh(ufem_ns_handle* h, cudaStream_t s, int max_side_2d = 20, int max_side_3d = 7,
+                           bool* rebuilt = nullptr) {
   KrylovWork& kw = *h->kw;
   int rc;
-  if (kw.cp_bc_version != h->bcp.version && (rc = coupled_coarse_build(h))) return rc;
+  const bool stale = kw.cp_bc_version != h->bcp.version || kw.cp_caps != max_side_2d * 1000 + max_side_3d;
+  if (rebuilt) *rebuilt = stale;
+  if (stale && (rc = coupled_coarse_build(h, max_side_2d, max_side_3d))) return rc;
   kw.cp_spd = false;
   const int nc = kw.nc;
   if (nc == 0) return UFEM_OK;
@@ -1604,6 +1609,20 @@ int coupled_coarse_refresh(ufem_ns_handle* h, cudaStream_t s) {
 }
 
 }  // namespace
+
+int krylov_coupled_coarse(ufem_ns_handle* h, cudaStream_t s, int max_side_2d, int max_side_3d, bool* rebuilt,
+                          CoarseView* view) {
+  if (!h->kw) h->kw = new KrylovWork();  // coarse data only: batch members keep their vectors in the batch
+  int rc;
+  if ((rc = coupled_coarse_refresh(h, s, max_side_2d, max_side_3d, rebuilt))) return rc;
+  const KrylovWork& kw = *h->kw;
+  view->nc = kw.cp_spd ? kw.nc : 0;
+  view->agg = kw.agg;
+  view->agg_ptr = kw.agg_ptr;
+  view->agg_rows = kw.agg_rows;
+  view->ainv = kw.ainv;
+  return UFEM_OK;
+}
 
 int krylov_solve(ufem_ns_handle* h, const ufem_krylov_opts* ko, ufem_krylov_status* st, cudaStream_t s) {
   ufem_krylov_opts o = *ko;
