@@ -976,10 +976,10 @@ __global__ void __launch_bounds__(32 * WPB, warp_min_blocks<D, T, KC, WPB>()) ns
         const int S = int(__ldg(start + row + 1) - s0);
         const int self = int(s_pslots[kb] & 0xFFu);
         const int64_t pos = int64_t(neq) * neq * s0 + int64_t(r * S + self) * neq + c;
-        vals[pos] = acc;
-        if (vals32 != nullptr) vals32[pos] = float(acc);
+        __stcs(vals + pos, acc);  // streamed: keep L2 for the node data the element phase gathers
+        if (vals32 != nullptr) __stcs(vals32 + pos, float(acc));
       } else {
-        rhs[int64_t(row) * neq + (j - neq * neq)] = acc;
+        __stcs(rhs + int64_t(row) * neq + (j - neq * neq), acc);
       }
     }
 
@@ -1026,17 +1026,17 @@ __global__ void __launch_bounds__(32 * WPB, warp_min_blocks<D, T, KC, WPB>()) ns
         const int r = rg * RPI + rr;
         const int64_t pos = int64_t(neq) * neq * s0 + int64_t(r * S + s) * neq;
         if constexpr (neq == 4) {
-          reinterpret_cast<double2*>(vals + pos)[0] = make_double2(acc[4 * rr], acc[4 * rr + 1]);
-          reinterpret_cast<double2*>(vals + pos)[1] = make_double2(acc[4 * rr + 2], acc[4 * rr + 3]);
+          __stcs(reinterpret_cast<double2*>(vals + pos), make_double2(acc[4 * rr], acc[4 * rr + 1]));
+          __stcs(reinterpret_cast<double2*>(vals + pos) + 1, make_double2(acc[4 * rr + 2], acc[4 * rr + 3]));
           if (vals32 != nullptr)
-            *reinterpret_cast<float4*>(vals32 + pos) =
-                make_float4(float(acc[4 * rr]), float(acc[4 * rr + 1]), float(acc[4 * rr + 2]), float(acc[4 * rr + 3]));
+            __stcs(reinterpret_cast<float4*>(vals32 + pos),
+                   make_float4(float(acc[4 * rr]), float(acc[4 * rr + 1]), float(acc[4 * rr + 2]), float(acc[4 * rr + 3])));
         } else {
 #pragma unroll
-          for (int c = 0; c < neq; ++c) vals[pos + c] = acc[rr * neq + c];
+          for (int c = 0; c < neq; ++c) __stcs(vals + pos + c, acc[rr * neq + c]);
           if (vals32 != nullptr) {
 #pragma unroll
-            for (int c = 0; c < neq; ++c) vals32[pos + c] = float(acc[rr * neq + c]);
+            for (int c = 0; c < neq; ++c) __stcs(vals32 + pos + c, float(acc[rr * neq + c]));
           }
         }
       }

@@ -266,52 +266,51 @@ __device__ __forceinline__ double* vec(const BatchMesh& M, double* work) {
   else return work + M.row_off;
 }
 
-// y = A x, one warp per node over all members (spmv_node, as spmv_kernel).
+// y = A x over the solver chunks (one CTA per chunk of at most kChunkNodes
+// nodes of one member; spmv_node per node, as spmv_kernel, and for triangles
+// spmv_node3_group with 4 nodes per warp): a finished member's chunks return
+// after one flag read, so an iteration costs what the members still iterating
+// need, not a launch over every node of the batch.
 template <int NEQ, typename MT, int XL>
-__global__ void __launch_bounds__(256, 6) spmv_batch_kernel(int64_t total_nodes, int nmesh,
-                                                         const int64_t* __restrict__ node_prefix,
+__global__ void __launch_bounds__(256) spmv_chunk_kernel(const Chunk* __restrict__ chunks,
                                                          const BatchMesh* __restrict__ bm, double* xwork,
                                                          double* __restrict__ ywork, const int* __restrict__ ictl,
                                                          int skip_flag) {
-  const int64_t gnode = (int64_t(blockIdx.x) * blockDim.x + threadIdx.x) >> 5;
-  const int lane = threadIdx.x & 31;
-  if (gnode >= total_nodes) return;
-  const int m = find_mesh(node_prefix, nmesh, gnode);
-  if (ictl[m * kIc + skip_flag]) return;
-  const BatchMesh& M = bm[m];
-  const int64_t node = gnode - node_prefix[m];
+  const Chunk c = chunks[blockIdx.x];
+  if (ictl[c.mesh * kIc + skip_flag]) return;
+  const BatchMesh& M = bm[c.mesh];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const double* x = vec<XL>(M, xwork);
   double* y = ywork + M.row_off;
   const MT* vals;
   if constexpr (std::is_same<MT, float>::value) vals = M.vals32; else vals = M.vals;
-  const int64_t s0 = __ldg(M.start + node);
-  const int S = int(__ldg(M.start + node + 1) - s0);
-  spmv_node<NEQ, MT, double, double>(vals + int64_t(NEQ) * NEQ * s0, S, M.adj + s0, x, lane, y + node * NEQ);
+  for (int node = c.lo / NEQ + warp; node < c.hi / NEQ; node += int(blockDim.x >> 5)) {
+    const int64_t s0 = __ldg(M.start + node);
+    const int S = int(__ldg(M.start + node + 1) - s0);
+    spmv_node<NEQ, MT, double, double>(vals + int64_t(NEQ) * NEQ * s0, S, M.adj + s0, x, lane, y + int64_t(node) * NEQ);
+  }
 }
 
-// Triangles: 4 nodes per warp over all members (spmv_node3_group); each
-// 8-lane group finds its own member.
 template <typename MT, int XL>
-__global__ void __launch_bounds__(256) spmv3_batch_kernel(int64_t total_nodes, int nmesh,
-                                                          const int64_t* __restrict__ node_prefix,
+__global__ void __launch_bounds__(256) spmv3_chunk_kernel(const Chunk* __restrict__ chunks,
                                                           const BatchMesh* __restrict__ bm, double* xwork,
                                                           double* __restrict__ ywork, const int* __restrict__ ictl,
                                                           int skip_flag) {
-  const int64_t t = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
-  if ((t >> 5) * 4 >= total_nodes) return;  // whole warp
-  const int64_t gnode = t >> 3;
-  const int sub = int(t & 7);
-  bool valid = gnode < total_nodes;
-  const int m = valid ? find_mesh(node_prefix, nmesh, gnode) : 0;
-  if (valid && ictl[m * kIc + skip_flag]) valid = false;
-  const BatchMesh& M = bm[m];
-  const int64_t node = valid ? gnode - node_prefix[m] : 0;
+  const Chunk c = chunks[blockIdx.x];
+  if (ictl[c.mesh * kIc + skip_flag]) return;
+  const BatchMesh& M = bm[c.mesh];
+  const int grp = threadIdx.x >> 3, sub = threadIdx.x & 7;  // 4 nodes per warp, 8 lanes each
   const MT* vals;
   if constexpr (std::is_same<MT, float>::value) vals = M.vals32; else vals = M.vals;
-  const int64_t s0 = valid ? __ldg(M.start + node) : 0;
-  const int S = valid ? int(__ldg(M.start + node + 1) - s0) : 0;
-  spmv_node3_group<MT, double, double>(vals + 9 * s0, S, M.adj + s0, vec<XL>(M, xwork), sub, valid,
-                                       ywork + M.row_off + node * 3);
+  const int n0 = c.lo / 3, n1 = c.hi / 3;
+  for (int base = n0; base < n1; base += int(blockDim.x >> 3)) {  // the same trip count for every lane
+    const int node = base + grp;
+    const bool valid = node < n1;
+    const int64_t s0 = valid ? __ldg(M.start + node) : 0;
+    const int S = valid ? int(__ldg(M.start + node + 1) - s0) : 0;
+    spmv_node3_group<MT, double, double>(vals + 9 * s0, S, M.adj + s0, vec<XL>(M, xwork), sub, valid,
+                                         ywork + M.row_off + int64_t(valid ? node : 0) * 3);
+  }
 }
 
 // dinv = 1 / diag (point Jacobi) of the operator the solve uses.
@@ -927,14 +926,11 @@ inline unsigned blocks_for(int64_t n, int threads) { return unsigned((n + thread
 
 template <typename MT, int XL>
 int spmv_b(ufem_batch* b, double* x, double* y, cudaStream_t st, int skip_flag = fDone) {
-  const unsigned grid = blocks_for(b->total_nodes * 32, 256);
+  const unsigned nc = unsigned(b->nchunks);
   if (b->neq == 4)
-    spmv_batch_kernel<4, MT, XL><<<grid, 256, 0, st>>>(b->total_nodes, b->nmesh, b->d_node_prefix, b->d_mesh, x, y,
-                                                       b->ictl, skip_flag);
+    spmv_chunk_kernel<4, MT, XL><<<nc, 256, 0, st>>>(b->d_chunks, b->d_mesh, x, y, b->ictl, skip_flag);
   else
-    spmv3_batch_kernel<MT, XL><<<blocks_for(b->total_nodes * 8, 256), 256, 0, st>>>(
-        b->total_nodes, b->nmesh, b->d_node_prefix, b->d_mesh, x, y,
-                                                       b->ictl, skip_flag);
+    spmv3_chunk_kernel<MT, XL><<<nc, 256, 0, st>>>(b->d_chunks, b->d_mesh, x, y, b->ictl, skip_flag);
   UFEM_CUDA_TRY(cudaGetLastError());
   return UFEM_OK;
 }

@@ -1535,31 +1535,39 @@ int coupled_coarse_build(ufem_ns_handle* h, int max_side_2d, int max_side_3d) {
     for (int64_t i = 0; i < N; ++i)  // ascending rows within each aggregate
       if (box[size_t(i)] >= 0) rows[size_t(fill[size_t(box[size_t(i)])]++)] = int32_t(i * neq + dim);
   }
-  struct Entry { int64_t key, pos; };
-  std::vector<Entry> ent;
-  for (int64_t i = 0; i < N; ++i) {
-    if (box[size_t(i)] < 0) continue;
-    const int64_t s0 = h->start_h[size_t(i)], S = h->start_h[size_t(i) + 1] - s0;
-    for (int64_t q = 0; q < S; ++q) {
-      const int32_t j = h->adj_h[size_t(s0 + q)];
-      if (box[size_t(j)] < 0) continue;
-      ent.push_back({int64_t(box[size_t(i)]) * nc + box[size_t(j)],
-                     int64_t(neq) * neq * s0 + (int64_t(dim) * S + q) * neq + dim});
+  std::vector<int64_t> pos_sorted, starts;
+  // counting sort by (row aggregate, column aggregate): the positions are
+  // generated in ascending order (nodes and slots ascending), so each key's
+  // positions stay ascending
+  const int64_t nkey = int64_t(nc) * nc;
+  std::vector<int64_t> cnt(size_t(nkey) + 1, 0);
+  for (int pass = 0; pass < 2; ++pass) {
+    for (int64_t i = 0; i < N; ++i) {
+      if (box[size_t(i)] < 0) continue;
+      const int64_t s0 = h->start_h[size_t(i)], S = h->start_h[size_t(i) + 1] - s0;
+      const int64_t rowkey = int64_t(box[size_t(i)]) * nc;
+      for (int64_t q = 0; q < S; ++q) {
+        const int32_t j = h->adj_h[size_t(s0 + q)];
+        if (box[size_t(j)] < 0) continue;
+        const int64_t key = rowkey + box[size_t(j)];
+        if (pass == 0) ++cnt[size_t(key) + 1];
+        else pos_sorted[size_t(cnt[size_t(key)]++)] = int64_t(neq) * neq * s0 + (int64_t(dim) * S + q) * neq + dim;
+      }
+    }
+    if (pass == 0) {
+      for (int64_t k = 0; k < nkey; ++k) cnt[size_t(k) + 1] += cnt[size_t(k)];
+      pos_sorted.resize(size_t(cnt[size_t(nkey)]));
+      starts.assign(cnt.begin(), cnt.end());
     }
   }
-  std::sort(ent.begin(), ent.end(), [](const Entry& a, const Entry& b) {
-    return a.key != b.key ? a.key < b.key : a.pos < b.pos;
-  });
-  std::vector<int64_t> pos(ent.size());
+  std::vector<int64_t>& pos = pos_sorted;
   std::vector<int32_t> seg, dst;
-  for (size_t q = 0; q < ent.size(); ++q) {
-    pos[q] = ent[q].pos;
-    if (q == 0 || ent[q].key != ent[q - 1].key) {
-      seg.push_back(int32_t(q));
-      dst.push_back(int32_t(ent[q].key));
+  for (int64_t k = 0; k < nkey; ++k)
+    if (starts[size_t(k) + 1] > starts[size_t(k)]) {
+      seg.push_back(int32_t(starts[size_t(k)]));
+      dst.push_back(int32_t(k));
     }
-  }
-  seg.push_back(int32_t(ent.size()));
+  seg.push_back(int32_t(pos.size()));
   int rc;
   if ((rc = dalloc(&kw.agg, agg.size())) || (rc = dalloc(&kw.agg_ptr, ptr.size())) ||
       (rc = dalloc(&kw.agg_rows, std::max<size_t>(rows.size(), 1))) || (rc = dalloc(&kw.ainv, size_t(nc) * nc)) ||
