@@ -15,6 +15,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstdint>
+#include <thread>
 #include <type_traits>
 #include <vector>
 
@@ -116,12 +117,14 @@ __device__ __forceinline__ double block_sum(double v, double* sm) {
 }
 
 // In-place inverse of an SPD matrix (row-major, n x n) through its Cholesky
-// factor L: L^-1 row by row, then A^-1 = L^-T L^-1 as a sum of rank-one
-// updates; every inner loop runs over contiguous memory.  False if a pivot is
-// not positive (a coarse matrix of a system without conditions that fix its
-// constant mode is singular).
+// factor: L row by row (contiguous inner products), then each column of A^-1
+// by forward and back substitution with L and L^T (stored transposed, so every
+// inner loop runs over contiguous memory).  The columns are independent and are
+// split over host threads; each column's arithmetic is the same whatever the
+// split.  False if a pivot is not positive (a coarse matrix of a system without
+// conditions that fix its constant mode is singular).
 bool spd_invert(double* A, int n) {
-  std::vector<double> L(size_t(n) * n, 0.0), M(size_t(n) * n, 0.0);
+  std::vector<double> L(size_t(n) * n, 0.0), U(size_t(n) * n, 0.0);
   for (int j = 0; j < n; ++j) {
     const double* Lj = &L[size_t(j) * n];
     double d = A[size_t(j) * n + j];
@@ -136,29 +139,38 @@ bool spd_invert(double* A, int n) {
       L[size_t(i) * n + j] = s / ljj;
     }
   }
-  for (int i = 0; i < n; ++i) {  // M = L^-1: row i = (e_i - sum_{k<i} L[i][k] M[k]) / L[i][i]
-    double* Mi = &M[size_t(i) * n];
-    Mi[i] = 1.0;
-    for (int k = 0; k < i; ++k) {
-      const double lik = L[size_t(i) * n + k];
-      const double* Mk = &M[size_t(k) * n];
-      for (int j = 0; j <= k; ++j) Mi[j] -= lik * Mk[j];
-    }
-    const double inv = 1.0 / L[size_t(i) * n + i];
-    for (int j = 0; j <= i; ++j) Mi[j] *= inv;
-  }
-  std::fill(A, A + size_t(n) * n, 0.0);
-  for (int k = 0; k < n; ++k) {  // A^-1 = sum_k M[k]^T M[k] (lower triangle, then mirrored)
-    const double* Mk = &M[size_t(k) * n];
-    for (int i = 0; i <= k; ++i) {
-      const double mki = Mk[i];
-      if (mki == 0.0) continue;
-      double* Ai = A + size_t(i) * n;
-      for (int j = 0; j <= i; ++j) Ai[j] += mki * Mk[j];
-    }
-  }
   for (int i = 0; i < n; ++i)
-    for (int j = 0; j < i; ++j) A[size_t(j) * n + i] = A[size_t(i) * n + j];
+    for (int k = 0; k <= i; ++k) U[size_t(k) * n + i] = L[size_t(i) * n + k];  // U = L^T
+  auto columns = [&](int c0, int c1) {
+    std::vector<double> col(static_cast<size_t>(n));
+    for (int c = c0; c < c1; ++c) {  // L L^T x = e_c
+      for (int i = 0; i < n; ++i) {
+        const double* Li = &L[size_t(i) * n];
+        double s = (i == c) ? 1.0 : 0.0;
+        for (int k = 0; k < i; ++k) s -= Li[k] * col[size_t(k)];
+        col[size_t(i)] = s / Li[i];
+      }
+      for (int i = n - 1; i >= 0; --i) {
+        const double* Ui = &U[size_t(i) * n];
+        double s = col[size_t(i)];
+        for (int k = i + 1; k < n; ++k) s -= Ui[k] * col[size_t(k)];
+        col[size_t(i)] = s / Ui[i];
+      }
+      for (int i = 0; i < n; ++i) A[size_t(i) * n + c] = col[size_t(i)];
+    }
+  };
+  const int nt = int(std::max(1u, std::min(16u, std::thread::hardware_concurrency())));
+  const int per = (n + nt - 1) / nt;
+  if (nt == 1 || n < 64) {
+    columns(0, n);
+  } else {
+    std::vector<std::thread> th;
+    for (int t = 0; t < nt; ++t) {
+      const int c0 = t * per, c1 = std::min(n, c0 + per);
+      if (c0 < c1) th.emplace_back(columns, c0, c1);
+    }
+    for (auto& x : th) x.join();
+  }
   return true;
 }
 
