@@ -159,7 +159,8 @@ bool spd_invert(double* A, int n) {
       for (int i = 0; i < n; ++i) A[size_t(i) * n + c] = col[size_t(i)];
     }
   };
-  const int nt = int(std::max(1u, std::min(16u, std::thread::hardware_concurrency())));
+  // a few threads: several handles may refresh their coarse spaces at once
+  const int nt = int(std::max(1u, std::min(4u, std::thread::hardware_concurrency())));
   const int per = (n + nt - 1) / nt;
   if (nt == 1 || n < 64) {
     columns(0, n);

@@ -4,10 +4,12 @@ Stated tolerances: a request's final state is BITWISE the same when it is
 served alone and when it is served in a mix (FP64, mixed-precision solve, FP32
 elements); the served mixed-precision form (FP64 elements, FP32 Krylov
 operator, FP64 refinement) is within 1e-6 relative of the plain FP64 path
-(`run_plain`); with FP32 element arithmetic the served state is within 1e-3
-(the perturbation of the system by FP32 element rounding, amplified by the
-conditioning of the incompressible system, chiefly in the pressure);
-admission never reserves more than the budget.
+(`run_plain`); with FP32 element arithmetic on the batched path (which
+refines against the stored FP32-element system) the served state is within
+1e-3 (the perturbation of the system by FP32 element rounding, amplified by the
+conditioning of the incompressible system, chiefly in the pressure), and on the
+large-request path (refined against the matrix-free FP64 residual) within 1e-6
+of the oracle; admission never reserves more than the budget.
 """
 import numpy as np
 import pytest
@@ -113,3 +115,21 @@ def test_poisson_arrivals_realtime():
     res, stats = S.Server(8 * GB, mixed=True, realtime=True).run(reqs)
     assert stats["requests"] == 6 and all(r.ok for r in res)
     assert stats["steps_per_s"] > 0 and stats["request_s"]["p99"] >= stats["request_s"]["p50"]
+
+
+def test_large_path_fp32_elements_with_fp64_answers():
+    """The mixed form's large-request path (one handle per request on the large
+    workers: FP32 element matrices, FP32 inner BiCGStab with the coupled
+    two-level preconditioner refined against the matrix-free FP64 residual to
+    1e-12): every request within 1e-6 of the FP64 oracle and bitwise the same
+    alone and in the mix.  large_rows = 1 sends every request down that path."""
+    reqs = workload(n=6, seed=13)
+    kw = dict(precision="fp64", mixed=True, realtime=False, krylov=dict(tol=1e-12), large_rows=1,
+              large_rows_2d=1, large_precond="two_level_coupled")
+    served, stats = S.Server(8 * GB, **kw).run(reqs)
+    assert stats["rejected"] == 0 and all(r.ok for r in served)
+    for r, req in zip(served, reqs):
+        assert vec_rel_error(r.state, oracle_state(req)) <= 1e-6, r.rid
+    for req in reqs[:3]:
+        alone, _ = S.Server(8 * GB, **kw).run([req])
+        assert np.array_equal(alone[0].state, served[req.rid].state), req.rid
