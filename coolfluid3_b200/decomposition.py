@@ -183,21 +183,12 @@ class DistributedNS:
         self.halo.exchange(xl)
         return self.engine.spmv(xl)[: self.m]
 
-    def solve(self, tol: float = 1e-10, max_iters: int = 3000) -> dict:
-        """Point-Jacobi BiCGStab on the owned rows; the initial guess is the
-        engine's solution vector (the previous increment, with the condition
-        values in the constrained rows)."""
+    def _bicgstab(self, x, b, dinv, bnorm, tol, max_iters):
+        """One BiCGStab run from x; returns (x, iterations, status)."""
         import torch
-        m = self.m
-        x = self.engine.solution()[:m].clone()
-        b = self.engine.rhs()[:m].clone()
-        d = self.engine.diag()[:m]
-        dinv = torch.where(d != 0, 1.0 / d, torch.ones_like(d))
         r = b - self._apply(x)
         rhat = r.clone()
-        bn2, rn2 = _allreduce([b @ b, r @ r]).tolist()
-        bnorm = bn2 ** 0.5 if bn2 > 0 else 1.0
-        relres = rn2 ** 0.5 / bnorm
+        relres = float(_allreduce([r @ r])[0]) ** 0.5 / bnorm
         p = torch.zeros_like(r)
         v = torch.zeros_like(r)
         rho = alpha = omega = 1.0
@@ -205,7 +196,7 @@ class DistributedNS:
         while relres > tol and it < max_iters:
             rho_new = float(_allreduce([rhat @ r])[0])
             if rho_new == 0.0 or omega == 0.0:
-                status = 2
+                status = 2  # breakdown: the caller restarts from x
                 break
             beta = (rho_new / rho) * (alpha / omega)
             p = r + beta * (p - omega * v)
@@ -225,15 +216,38 @@ class DistributedNS:
             if not np.isfinite(relres):
                 status = 3
                 break
-        true = b - self._apply(x)  # the true residual decides convergence
-        relres = float(_allreduce([true @ true])[0]) ** 0.5 / bnorm
+        return x, it, status
+
+    def solve(self, tol: float = 1e-10, max_iters: int = 3000, max_restarts: int = 10) -> dict:
+        """Point-Jacobi BiCGStab on the owned rows; the initial guess is the
+        engine's solution vector (the previous increment, with the condition
+        values in the constrained rows).  Convergence is decided on the true
+        residual: after a breakdown, or when the recursive residual met the
+        tolerance while the true one had drifted above it, BiCGStab restarts
+        from its iterate while iterations remain (as the library's solve)."""
+        import torch
+        m = self.m
+        x = self.engine.solution()[:m].clone()
+        b = self.engine.rhs()[:m].clone()
+        d = self.engine.diag()[:m]
+        dinv = torch.where(d != 0, 1.0 / d, torch.ones_like(d))
+        bn2 = float(_allreduce([b @ b])[0])
+        bnorm = bn2 ** 0.5 if bn2 > 0 else 1.0
+        used, status = 0, 0
+        for _ in range(max_restarts + 1):
+            x, it, status = self._bicgstab(x, b, dinv, bnorm, tol, max_iters - used)
+            used += it
+            true = b - self._apply(x)
+            relres = float(_allreduce([true @ true])[0]) ** 0.5 / bnorm
+            if relres <= tol or status == 3 or not np.isfinite(relres) or used >= max_iters:
+                break
         xl = torch.zeros(self.engine.nb_rows, dtype=torch.float64, device=self.engine.device)
         xl[:m] = x
         self.halo.exchange(xl)  # ghosts take their owners' increments
         self.engine.set_solution(xl)
-        conv = bool(relres <= tol * 10)
-        return {"converged": int(conv), "iterations": it, "rel_residual": relres,
-                "status": status if status else (0 if conv else 1)}
+        conv = bool(relres <= tol)
+        return {"converged": int(conv), "iterations": used, "rel_residual": relres,
+                "status": 0 if conv else (status if status else 1)}
 
     def update(self) -> None:
         self.engine.update()
