@@ -15,6 +15,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstdint>
+#include <cstring>
 #include <thread>
 #include <type_traits>
 #include <vector>
@@ -83,7 +84,16 @@ struct KrylovWork {
   double* h_ac = nullptr;      // pinned host copy (nc x nc)
   int64_t cp_bc_version = -1;  // Dirichlet plan the structure was built for
   int cp_caps = -1;            // aggregate caps it was built with (2D side * 1000 + 3D side)
-  bool cp_spd = false;         // the last coarse matrix was positive definite
+  bool cp_spd = false;         // the coarse inverse on the device is valid
+  // Lagged refresh: the coarse matrix of solve k is inverted on a host thread
+  // while solve k runs with the inverse from solve k-1 (the first solve after a
+  // (re)build inverts its own matrix before it starts).
+  std::thread cp_thread;
+  bool cp_pending = false;     // cp_thread holds the next inverse in h_ac2
+  bool cp_lag_ready = false;   // the device inverse is the latest solve's: the next lagged solve keeps it
+  bool cp_next_spd = false;
+  double* h_ac2 = nullptr;     // pinned: the inverse the thread produces
+  cudaEvent_t cp_event = nullptr;
 };
 
 namespace {
@@ -1491,6 +1501,14 @@ namespace {
 // aggregate, position) with their segments.
 int coupled_coarse_build(ufem_ns_handle* h, int max_side_2d, int max_side_3d) {
   KrylovWork& kw = *h->kw;
+  if (kw.cp_thread.joinable()) kw.cp_thread.join();
+  kw.cp_pending = false;
+  kw.cp_lag_ready = false;
+  if (kw.h_ac2) {
+    DeviceLock lk(device_mutex());
+    cudaFreeHost(kw.h_ac2);
+    kw.h_ac2 = nullptr;
+  }
   kw.cp_caps = max_side_2d * 1000 + max_side_3d;
   dfree(kw.agg); dfree(kw.agg_ptr); dfree(kw.agg_rows); dfree(kw.ainv); dfree(kw.cvec); dfree(kw.yvec);
   dfree(kw.cp_pos); dfree(kw.cp_seg); dfree(kw.cp_dst); dfree(kw.acd);
@@ -1607,25 +1625,59 @@ int coupled_coarse_build(ufem_ns_handle* h, int max_side_2d, int max_side_3d) {
 // pass), its inverse on the host, uploaded for the solve; cp_spd false (point
 // Jacobi for this solve) when it is not positive definite.
 int coupled_coarse_refresh(ufem_ns_handle* h, cudaStream_t s, int max_side_2d = 20, int max_side_3d = 7,
-                           bool* rebuilt = nullptr) {
+                           bool* rebuilt = nullptr, bool lag = false) {
   KrylovWork& kw = *h->kw;
   int rc;
   const bool stale = kw.cp_bc_version != h->bcp.version || kw.cp_caps != max_side_2d * 1000 + max_side_3d;
   if (rebuilt) *rebuilt = stale;
-  if (stale && (rc = coupled_coarse_build(h, max_side_2d, max_side_3d))) return rc;
-  kw.cp_spd = false;
+  if (stale && (rc = coupled_coarse_build(h, max_side_2d, max_side_3d))) return rc;  // (joins the thread)
   const int nc = kw.nc;
-  if (nc == 0) return UFEM_OK;
+  if (nc == 0) {
+    kw.cp_spd = false;
+    return UFEM_OK;
+  }
   const size_t bytes = size_t(nc) * nc * sizeof(double);
+  // lagged: an inverse of the previous solve's coarse matrix exists (on the
+  // device, or on its way from the host thread); this solve uses it
+  const bool lagged = lag && !stale && (kw.cp_pending || kw.cp_lag_ready);
+  if (lagged && kw.cp_pending) {
+    kw.cp_thread.join();
+    kw.cp_pending = false;
+    kw.cp_spd = kw.cp_next_spd;
+    if (kw.cp_spd) UFEM_CUDA_TRY(cudaMemcpyAsync(kw.ainv, kw.h_ac2, bytes, cudaMemcpyHostToDevice, s));
+  }
   UFEM_CUDA_TRY(cudaMemsetAsync(kw.acd, 0, bytes, s));
   if (kw.cp_nseg > 0)
     coarse_matrix_kernel<<<unsigned((int64_t(kw.cp_nseg) * 32 + 255) / 256), 256, 0, s>>>(
         kw.cp_nseg, kw.cp_seg, kw.cp_dst, kw.cp_pos, h->d_vals, kw.acd);
   UFEM_CUDA_TRY(cudaGetLastError());
   UFEM_CUDA_TRY(cudaMemcpyAsync(kw.h_ac, kw.acd, bytes, cudaMemcpyDeviceToHost, s));
-  UFEM_CUDA_TRY(cudaStreamSynchronize(s));
-  kw.cp_spd = spd_invert(kw.h_ac, nc);
-  if (kw.cp_spd) UFEM_CUDA_TRY(cudaMemcpyAsync(kw.ainv, kw.h_ac, bytes, cudaMemcpyHostToDevice, s));
+  if (!lagged) {  // invert this solve's own matrix before the solve starts
+    UFEM_CUDA_TRY(cudaStreamSynchronize(s));
+    kw.cp_spd = spd_invert(kw.h_ac, nc);
+    if (kw.cp_spd) UFEM_CUDA_TRY(cudaMemcpyAsync(kw.ainv, kw.h_ac, bytes, cudaMemcpyHostToDevice, s));
+    kw.cp_lag_ready = lag;  // the next lagged solve keeps this inverse
+    return UFEM_OK;
+  }
+  // the next solve's inverse: this solve's matrix, inverted on a host thread
+  // once its copy has landed, while this solve runs
+  if (!kw.h_ac2) {
+    DeviceLock lk(device_mutex());
+    UFEM_CUDA_TRY(cudaMallocHost(reinterpret_cast<void**>(&kw.h_ac2), bytes));
+  }
+  if (!kw.cp_event) UFEM_CUDA_TRY(cudaEventCreateWithFlags(&kw.cp_event, cudaEventDisableTiming));
+  UFEM_CUDA_TRY(cudaEventRecord(kw.cp_event, s));
+  double* src = kw.h_ac;
+  double* dst = kw.h_ac2;
+  cudaEvent_t ev = kw.cp_event;
+  KrylovWork* kwp = &kw;
+  kw.cp_thread = std::thread([src, dst, bytes, nc, ev, kwp]() {
+    const bool ok = cudaEventSynchronize(ev) == cudaSuccess;
+    if (ok) std::memcpy(dst, src, bytes);
+    kwp->cp_next_spd = ok && spd_invert(dst, nc);
+  });
+  kw.cp_pending = true;
+  kw.cp_lag_ready = false;
   return UFEM_OK;
 }
 
@@ -1666,7 +1718,9 @@ int krylov_solve(ufem_ns_handle* h, const ufem_krylov_opts* ko, ufem_krylov_stat
   int rc;
   if ((rc = ensure_work(h, o.restart, mixed, bicg))) return rc;
   if (o.precond == 4) {  // coarse matrix of this system; point Jacobi when it is not positive definite
-    if ((rc = coupled_coarse_refresh(h, s))) return rc;
+    // lagged: from the second solve on, each solve uses the previous solve's coarse
+    // inverse while its own matrix is inverted on a host thread for the next one
+    if ((rc = coupled_coarse_refresh(h, s, 20, 7, nullptr, true))) return rc;
     if (!h->kw->cp_spd) o.precond = 1;
   }
   KrylovWork& kw = *h->kw;
@@ -1895,9 +1949,12 @@ void krylov_free(ufem_ns_handle* h) {
   dfree(k.part); dfree(k.hbuf); dfree(k.H); dfree(k.cs); dfree(k.sn); dfree(k.g); dfree(k.y);
   dfree(k.dctl); dfree(k.ictl); dfree(k.cg_counter);
   dfree(k.agg); dfree(k.agg_ptr); dfree(k.agg_rows); dfree(k.ainv); dfree(k.cvec); dfree(k.yvec);
+  if (k.cp_thread.joinable()) k.cp_thread.join();
   dfree(k.cp_pos); dfree(k.cp_seg); dfree(k.cp_dst); dfree(k.acd);
   DeviceLock lk(device_mutex());
   if (k.h_ac) cudaFreeHost(k.h_ac);
+  if (k.h_ac2) cudaFreeHost(k.h_ac2);
+  if (k.cp_event) cudaEventDestroy(k.cp_event);
   for (auto& g : k.cg_graph)
     if (g.exec) cudaGraphExecDestroy(g.exec);
   for (auto& g : k.bicg_graph)

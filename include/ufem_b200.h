@@ -78,7 +78,10 @@ typedef struct ufem_krylov_opts {
                           4 two-level for the coupled system (BiCGStab, GMRES):
                             point Jacobi + a coarse correction on box aggregates
                             of the pressure rows, coarse matrix = Galerkin
-                            product of the pressure block, rebuilt per solve   */
+                            product of the pressure block, summed on the device
+                            at every solve; from a handle's second solve on, a
+                            solve uses the previous solve's coarse inverse while
+                            its own is inverted on a host thread              */
   double tol;          /* ||b - A x|| / ||b|| target, default 1e-10                */
   int32_t mixed;       /* 0: all FP64; 1: FP32 inner Krylov + FP64 refinement
                           whose residual is b - A x of the stored system; 2: the
