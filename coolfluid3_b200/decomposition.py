@@ -22,9 +22,9 @@ synchronised after each loop (common/PE/CommPattern.cpp:567-599).  Here:
 * A local engine does the per-rank work.  ``GPUEngine`` is a ``NavierStokes``
   handle on the local mesh whose vectors stay in device memory (the SpMV is the
   library's, ``ufem_ns_apply_device``); any object with the same methods can
-  stand in (the CPU tests use the FP64 oracle).  No TMA and no multicast are
-  involved: ghost values arrive in each GPU's own memory before the SpMV reads
-  them.
+  stand in (the CPU tests use the FP64 oracle).  Ghost values arrive in each
+  GPU's own memory before the SpMV reads them; no kernel reads another GPU's
+  memory.
 """
 from __future__ import annotations
 
