@@ -798,7 +798,7 @@ def serving_compare(args):
         for _ in range(max(1, args.serve_reps)):
             srv = S.Server(int(args.serve_budget_gb * 1e9), precision="fp64", mixed=mixed,
                            krylov=dict(tol=tol, max_iters=20000), realtime=True, large_precond=lpre,
-                           large_rows_2d=40_000)
+                           small_precond=lpre, large_rows_2d=40_000)
             res, st = srv.run(reqs)
             runs.append((st["steps_per_s"], st, res, srv))
         runs.sort(key=lambda x: x[0])
@@ -831,7 +831,7 @@ def serving_compare(args):
         for label, mixed, lpre in forms:
             srv = S.Server(int(args.serve_budget_gb * 1e9), precision="fp64", mixed=mixed,
                            krylov=dict(tol=tol, max_iters=20000), realtime=True, large_precond=lpre,
-                           large_rows_2d=40_000)
+                           small_precond=lpre, large_rows_2d=40_000)
             _, st = srv.run(rq)
             row[label] = {"steps_per_s": round(st["steps_per_s"], 2), "step_ms_p50": round(st["step_ms"]["p50"], 2),
                           "step_ms_p99": round(st["step_ms"]["p99"], 2),

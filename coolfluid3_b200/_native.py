@@ -108,6 +108,7 @@ SIGNATURES = {
     "ufem_ns_update": (C.c_int, [_P, _P]),
     "ufem_ns_fp64_residual": (C.c_int, [_P, C.POINTER(C.c_double), _P]),
     "ufem_ns_apply_device": (C.c_int, [_P, _P, _P, _P]),
+    "ufem_ns_prepare_solve": (C.c_int, [_P, C.POINTER(KrylovOpts), C.c_int32]),
     "ufem_ns_step": (C.c_int, [_P, C.c_int32, C.POINTER(KrylovOpts), C.POINTER(KrylovStatus), _P]),
     "ufem_ns_write_restart": (C.c_int, [_P, C.c_char_p, C.c_double, C.c_double, C.c_int64]),
     "ufem_ns_read_restart": (C.c_int, [_P, C.c_char_p, C.POINTER(C.c_double), C.POINTER(C.c_double),

@@ -985,6 +985,7 @@ int ufem_ns_add_neumann(ufem_ns_handle* h, const uint32_t* faces, int64_t nfaces
     if (int64_t(faces[i]) >= h->N) return set_error(UFEM_ERR_ARG, "Neumann face node id out of range");
   for (int64_t i = 0; i < nfaces; ++i) h->neumann.push_back({faces[2 * i], faces[2 * i + 1], comp, flux});
   h->bcp.dirty = true;
+  ++h->bc_list_version;
   return UFEM_OK;
 }
 
@@ -992,6 +993,7 @@ int ufem_ns_clear_neumann(ufem_ns_handle* h) {
   if (!h) return set_error(UFEM_ERR_ARG, "NULL handle");
   h->neumann.clear();
   h->bcp.dirty = true;
+  ++h->bc_list_version;
   return UFEM_OK;
 }
 
@@ -1012,6 +1014,7 @@ int ufem_ns_add_dirichlet_function(ufem_ns_handle* h, const uint32_t* nodes, int
   h->fn_const.push_back(std::move(k));
   for (int64_t i = 0; i < n; ++i) h->bcs.push_back({nodes[i], comp, 0.0, id});
   h->bcp.dirty = true;
+  ++h->bc_list_version;
   return UFEM_OK;
 }
 
@@ -1034,6 +1037,7 @@ int ufem_ns_clear_dirichlet(ufem_ns_handle* h) {
   h->fn_code.clear();
   h->fn_const.clear();
   h->bcp.dirty = true;
+  ++h->bc_list_version;
   return UFEM_OK;
 }
 
@@ -1045,6 +1049,7 @@ int ufem_ns_add_dirichlet(ufem_ns_handle* h, const uint32_t* nodes, int64_t n, i
     if (int64_t(nodes[i]) >= h->N) return set_error(UFEM_ERR_ARG, "Dirichlet node id out of range");
   for (int64_t i = 0; i < n; ++i) h->bcs.push_back({nodes[i], comp, values[i]});
   h->bcp.dirty = true;
+  ++h->bc_list_version;
   return UFEM_OK;
 }
 
@@ -1058,6 +1063,7 @@ int ufem_ns_add_dirichlet_dofs(ufem_ns_handle* h, const uint32_t* nodes, const i
   }
   for (int64_t i = 0; i < n; ++i) h->bcs.push_back({nodes[i], comps[i], values[i]});
   h->bcp.dirty = true;
+  ++h->bc_list_version;
   return UFEM_OK;
 }
 
@@ -1194,6 +1200,14 @@ int ufem_ns_solve(ufem_ns_handle* h, const ufem_krylov_opts* kopts, ufem_krylov_
                                          ", relative residual " + std::to_string(st.rel_residual));
   }
   return UFEM_OK;
+}
+
+int ufem_ns_prepare_solve(ufem_ns_handle* h, const ufem_krylov_opts* kopts, int32_t batched) {
+  if (!h) return set_error(UFEM_ERR_ARG, "NULL handle");
+  ufem_krylov_opts o;
+  ufem_krylov_default_opts(&o);
+  if (kopts) o = *kopts;
+  return krylov_prepare(h, &o, batched);
 }
 
 int ufem_ns_fp64_residual(ufem_ns_handle* h, double* r, void* stream) {

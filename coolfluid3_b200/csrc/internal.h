@@ -146,6 +146,7 @@ struct ufem_ns_handle {
   std::vector<std::vector<double>> fn_const;
   double time = 0.0;                            // current time (function BCs); advanced by dt at each update
   std::vector<BCEntry> bcs;
+  int64_t bc_list_version = 0;  // incremented whenever the condition lists change
   struct NeumannFace { uint32_t a, b; int comp; double flux; };
   std::vector<NeumannFace> neumann;  // constant Neumann conditions on Line2D faces
 
@@ -263,6 +264,9 @@ struct CoarseView {
 };
 int krylov_coupled_coarse(ufem_ns_handle* h, cudaStream_t s, int max_side_2d, int max_side_3d, bool* rebuilt,
                           CoarseView* view);
+// Allocations and static preconditioner structure of the solves `ko` describes,
+// ahead of the first solve (batched: for a batch member).
+int krylov_prepare(ufem_ns_handle* h, const ufem_krylov_opts* ko, int batched);
 void krylov_free(ufem_ns_handle* h);
 // Aggregates of the two-level CG preconditioner (precond 3) of a one-equation
 // system: agg[row] in [0, nc) or -1; builds and inverts the Galerkin coarse

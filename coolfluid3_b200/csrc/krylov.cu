@@ -82,7 +82,7 @@ struct KrylovWork {
   int cp_nseg = 0;
   double* acd = nullptr;       // nc x nc coarse matrix on the device
   double* h_ac = nullptr;      // pinned host copy (nc x nc)
-  int64_t cp_bc_version = -1;  // Dirichlet plan the structure was built for
+  int64_t cp_bc_version = -1;  // condition lists the structure was built for (bc_list_version)
   int cp_caps = -1;            // aggregate caps it was built with (2D side * 1000 + 3D side)
   bool cp_spd = false;         // the coarse inverse on the device is valid
   // Lagged refresh: the coarse matrix of solve k is inverted on a host thread
@@ -1519,7 +1519,7 @@ int coupled_coarse_build(ufem_ns_handle* h, int max_side_2d, int max_side_3d) {
   }
   kw.nc = 0;
   kw.cp_nseg = 0;
-  kw.cp_bc_version = h->bcp.version;
+  kw.cp_bc_version = h->bc_list_version;
   ++kw.coarse_version;
   const int dim = h->dim, neq = h->neq;
   const int64_t N = h->N;
@@ -1628,7 +1628,7 @@ int coupled_coarse_refresh(ufem_ns_handle* h, cudaStream_t s, int max_side_2d = 
                            bool* rebuilt = nullptr, bool lag = false) {
   KrylovWork& kw = *h->kw;
   int rc;
-  const bool stale = kw.cp_bc_version != h->bcp.version || kw.cp_caps != max_side_2d * 1000 + max_side_3d;
+  const bool stale = kw.cp_bc_version != h->bc_list_version || kw.cp_caps != max_side_2d * 1000 + max_side_3d;
   if (rebuilt) *rebuilt = stale;
   if (stale && (rc = coupled_coarse_build(h, max_side_2d, max_side_3d))) return rc;  // (joins the thread)
   const int nc = kw.nc;
@@ -1682,6 +1682,26 @@ int coupled_coarse_refresh(ufem_ns_handle* h, cudaStream_t s, int max_side_2d = 
 }
 
 }  // namespace
+
+int krylov_prepare(ufem_ns_handle* h, const ufem_krylov_opts* ko, int batched) {
+  ufem_krylov_opts o = *ko;
+  if (o.restart <= 0) o.restart = 30;
+  int rc;
+  if (!batched) {
+    if ((rc = ensure_work(h, o.restart, o.mixed != 0, o.method != 0))) return rc;
+  } else {
+    if (!h->kw) h->kw = new KrylovWork();  // batch members keep their vectors in the batch
+    if (o.mixed != 0 && (rc = dalloc(&h->d_vals32, size_t(h->nnz)))) return rc;
+  }
+  KrylovWork& kw = *h->kw;
+  if (o.precond == 4 && h->neq > 1) {
+    const int s2 = batched ? 12 : 20, s3 = batched ? 5 : 7;
+    if ((kw.cp_bc_version != h->bc_list_version || kw.cp_caps != s2 * 1000 + s3) &&
+        (rc = coupled_coarse_build(h, s2, s3)))
+      return rc;
+  }
+  return UFEM_OK;
+}
 
 int krylov_coupled_coarse(ufem_ns_handle* h, cudaStream_t s, int max_side_2d, int max_side_3d, bool* rebuilt,
                           CoarseView* view) {

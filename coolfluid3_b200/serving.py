@@ -181,7 +181,7 @@ class Server:
                  krylov: dict | None = None, graphs: bool = True, creators: int = 2,
                  use_specializations: bool = False, realtime: bool = True, large_rows: int = 200_000,
                  large_workers: int = 2, small_priority: bool = True, mixed_scope: str = "large",
-                 large_precond: str = "jacobi", large_rows_2d: int | None = None):
+                 large_precond: str = "jacobi", large_rows_2d: int | None = None, small_precond: str = "jacobi"):
         """mixed: the mixed-precision form.  Requests of at least `large_rows`
         rows (stepped one at a time by the large workers; their solves are
         bandwidth-bound) assemble FP32 element matrices and solve with FP32
@@ -191,7 +191,7 @@ class Server:
         with mixed_scope "large"; with "all" they iterate with an FP32 copy of
         the operator and FP64 residual replacement.  large_precond: the
         preconditioner of the large requests' one-handle solves ("jacobi" or
-        "two_level_coupled"; batches use point Jacobi)."""
+        "two_level_coupled"), small_precond that of the batched solves."""
         if mixed_scope not in ("large", "all"):
             raise ValueError("mixed_scope must be 'large' or 'all'")
         if precision not in ("fp32", "fp64"):
@@ -209,7 +209,7 @@ class Server:
         self.large_rows_2d = self.large_rows if large_rows_2d is None else int(large_rows_2d)
         self.large_workers = int(large_workers)
         self.small_priority = bool(small_priority)
-        self.krylov = dict(method="bicgstab", precond="jacobi", tol=1e-10, max_iters=3000)
+        self.krylov = dict(method="bicgstab", precond=small_precond, tol=1e-10, max_iters=3000)
         self.krylov.update(krylov or {})
         self.mixed = bool(mixed)
         self.krylov_mixed = dict(self.krylov, mixed=True, inner_tol=1e-6, max_refine=20) if mixed else self.krylov
@@ -390,6 +390,10 @@ class Server:
             try:
                 large = self._is_large(req.dim, req.coords.shape[0] * (req.dim + 1))
                 ns = _new_handle(req, "fp32" if (large and self.mixed) else self.precision, self.spec)
+                # solver workspace and preconditioner structure on this host thread,
+                # not on the worker that steps the request
+                kr = self.krylov_large if large else (self.krylov_mixed if self.mixed_scope == "all" else self.krylov)
+                ns.prepare_solve(batched=not large, **kr)
             except Exception as e:  # the request is rejected; the others go on
                 self._release(est)
                 with self._lock:

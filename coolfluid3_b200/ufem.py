@@ -295,6 +295,11 @@ class NavierStokes:
         N.check(self._lib.ufem_ns_get_system(self._h, N.dptr(vals), N.dptr(rhs)))
         return vals, rhs
 
+    def prepare_solve(self, batched: bool = False, **krylov) -> None:
+        """Allocate the solver workspace and build the preconditioner structure
+        ahead of the first solve (optional)."""
+        N.check(self._lib.ufem_ns_prepare_solve(self._h, C.byref(krylov_options(**krylov)), 1 if batched else 0))
+
     def fp64_residual(self, stream=None) -> np.ndarray:
         """b - M x of the FP64 system for the current solution vector, evaluated
         element by element without a matrix (after assemble and apply_dirichlet)."""

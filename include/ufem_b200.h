@@ -229,6 +229,13 @@ int ufem_ns_apply_dirichlet(ufem_ns_handle* h, void* stream);
 /* SolveLSS (SolveLSS.cpp:44-55): Krylov solve for the increment. */
 int ufem_ns_solve(ufem_ns_handle* h, const ufem_krylov_opts* kopts, ufem_krylov_status* status,
                   void* stream);
+/* Optional: allocate the Krylov workspace and build the static structure of the
+ * preconditioner that solves with `kopts` will use (the coarse space of precond
+ * 4), ahead of the first solve -- e.g. on the host thread that created the
+ * handle, while the GPU steps other handles.  batched = 1 prepares a future
+ * batch member (no one-handle vectors; the batch's aggregate caps).  No
+ * counterpart in the reference. */
+int ufem_ns_prepare_solve(ufem_ns_handle* h, const ufem_krylov_opts* kopts, int32_t batched);
 /* Allocation-free variant of ufem_ns_solve.  No counterpart in the reference.
  * For callers that cannot call cudaMalloc: applications that hand all device
  * memory to their own pool or enforce a fixed device-memory budget, and loops
