@@ -584,8 +584,17 @@ int create_impl(const ufem_mesh* mesh, const ufem_ns_options* opts, const uint32
   if (!make_warp_plan(32, h->wplan, wh32) || (dim == 3 && !make_warp_plan(24, h->wplan24, wh24)))
     return fail(set_error(UFEM_ERR_LIMIT, "a node has more incident elements than one assembly chunk holds"));
 
-  // --- device allocations and uploads
-  DeviceLock device_lock(device_mutex());
+  // --- device allocations and uploads.  Allocations take the library's device
+  // mutex one by one (dmalloc); the uploads, the zeroing and the CSR build run on
+  // a private stream that this call waits for alone, so building a handle does
+  // not wait for (or hold up) the work other host threads have on the device.
+  cudaStream_t cs = nullptr;
+  if (cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking) != cudaSuccess)
+    return fail(set_error(UFEM_ERR_CUDA, "cudaStreamCreate failed"));
+  struct StreamGuard {
+    cudaStream_t s;
+    ~StreamGuard() { cudaStreamDestroy(s); }
+  } stream_guard{cs};
   h->coords_h.assign(mesh->coords, mesh->coords + size_t(N) * dim);
   std::vector<double> c4(size_t(N) * 4, 0.0);
   for (int64_t i = 0; i < N; ++i)
@@ -614,7 +623,7 @@ int create_impl(const ufem_mesh* mesh, const ufem_ns_options* opts, const uint32
                                (rc = dmalloc(&h->d_node32, size_t(h->N) * 8, "node32"))))
     return fail(rc);
   auto up = [&](void* dst, const void* src, size_t bytes) {
-    return cudaMemcpy(dst, src, bytes, cudaMemcpyHostToDevice);
+    return cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, cs);  // pageable source: staged before return
   };
   cudaError_t ce = cudaSuccess;
   if ((ce = up(h->d_coords, c4.data(), c4.size() * 8)) || (ce = up(h->d_conn, conn4.data(), conn4.size() * 4)) ||
@@ -653,13 +662,14 @@ int create_impl(const ufem_mesh* mesh, const ufem_ns_options* opts, const uint32
     if ((ce = up(h->d_tie, tie.data(), tie.size() * 4)))
       return fail(set_error(UFEM_ERR_CUDA, std::string("upload: ") + cudaGetErrorString(ce)));
   }
-  if ((coupled && ((ce = cudaMemset(h->d_sol, 0, size_t(h->nrows) * 8)) ||
-                   (ce = cudaMemset(h->d_rhs, 0, size_t(h->nrows) * 8)))) ||
-      (ce = cudaMemset(h->d_state, 0, size_t(N) * 32)) || (ce = cudaMemset(h->d_hist, 0, size_t(N) * 96)) ||
-      (ce = cudaMemset(h->d_uadv, 0, size_t(N) * 32)) || (ce = cudaMemset(h->d_nu, 0, size_t(N) * 8)))
+  if ((coupled && ((ce = cudaMemsetAsync(h->d_sol, 0, size_t(h->nrows) * 8, cs)) ||
+                   (ce = cudaMemsetAsync(h->d_rhs, 0, size_t(h->nrows) * 8, cs)))) ||
+      (ce = cudaMemsetAsync(h->d_state, 0, size_t(N) * 32, cs)) ||
+      (ce = cudaMemsetAsync(h->d_hist, 0, size_t(N) * 96, cs)) ||
+      (ce = cudaMemsetAsync(h->d_uadv, 0, size_t(N) * 32, cs)) || (ce = cudaMemsetAsync(h->d_nu, 0, size_t(N) * 8, cs)))
     return fail(set_error(UFEM_ERR_CUDA, std::string("memset: ") + cudaGetErrorString(ce)));
-  if (coupled && (rc = launch_build_csr(h, 0))) return fail(rc);
-  if ((ce = cudaDeviceSynchronize()) != cudaSuccess)
+  if (coupled && (rc = launch_build_csr(h, cs))) return fail(rc);
+  if ((ce = cudaStreamSynchronize(cs)) != cudaSuccess)
     return fail(set_error(UFEM_ERR_CUDA, std::string("CSR build: ") + cudaGetErrorString(ce)));
   for (auto& e : h->ev)
     if (cudaEventCreate(&e) != cudaSuccess) return fail(set_error(UFEM_ERR_CUDA, "cudaEventCreate failed"));
