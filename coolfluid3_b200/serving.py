@@ -271,12 +271,23 @@ class Server:
         t0 = time.perf_counter()
         now = lambda: time.perf_counter() - t0  # noqa: E731
 
+        # Handles and batches are destroyed on one reaper thread: freeing device
+        # memory waits for the device, which would otherwise stall the worker that
+        # finished a request; a handle's budget is released once it is freed.
+        reaper = ThreadPoolExecutor(max_workers=1)
+
+        def reap(obj, reserved: int | None) -> None:
+            def job():
+                obj.close()
+                if reserved is not None:
+                    self._release(reserved)
+            reaper.submit(job)
+
         def finish(a: _Active, held: bool) -> None:
             a.result.state = a.ns.state()[0]
             a.result.finished = now()
             if not held:  # a held handle is closed (and its budget freed) when its batch is rebuilt
-                a.ns.close()
-                self._release(a.reserved)
+                reap(a.ns, a.reserved)
             with self._lock:
                 results.append(a.result)
                 state["open"] -= 1
@@ -328,11 +339,11 @@ class Server:
             def drop_batch():
                 nonlocal batch
                 if batch is not None:
-                    batch.close()
+                    stream.synchronize()
+                    reap(batch, None)  # before its members' handles (FIFO reaper)
                     batch = None
                 for h in held:
-                    h.ns.close()
-                    self._release(h.reserved)
+                    reap(h.ns, h.reserved)
                 held.clear()
 
             try:
@@ -453,6 +464,7 @@ class Server:
                 self._lock.notify_all()
             for w in workers:
                 w.join()
+            reaper.shutdown(wait=True)  # every handle and batch freed before run() returns
         if self.errors:
             raise self.errors[0]
         t_end = max((r.finished for r in results), default=now())
