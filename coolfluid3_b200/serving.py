@@ -178,7 +178,7 @@ class Server:
     """Continuous-batching server for one GPU (see the module docstring)."""
 
     def __init__(self, hbm_budget_bytes: int, max_slots: int = 64, precision: str = "fp64", mixed: bool = True,
-                 krylov: dict | None = None, graphs: bool = True, creators: int = 2,
+                 krylov: dict | None = None, graphs: bool = True, creators: int | None = None,
                  use_specializations: bool = False, realtime: bool = True, large_rows: int = 200_000,
                  large_workers: int = 2, small_priority: bool = True, mixed_scope: str = "large",
                  large_precond: str = "jacobi", large_rows_2d: int | None = None, small_precond: str = "jacobi"):
@@ -200,7 +200,10 @@ class Server:
         self.max_slots = int(max_slots)
         self.precision = precision
         self.graphs = graphs
-        self.creators = creators
+        # handle creation (mesh planning on the host) runs on these threads; by
+        # default half the host cores, 2 to 8
+        import os
+        self.creators = int(creators) if creators else max(2, min(8, (os.cpu_count() or 4) // 2))
         self.spec = use_specializations
         self.realtime = realtime
         self.large_rows = int(large_rows)
