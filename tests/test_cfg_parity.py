@@ -91,3 +91,24 @@ def test_cfg3_assembly_matches_oracle(precision):
         assert err <= 2e-5 and rerr <= 1e-4
     ns.close()
     o.close()
+
+
+def test_cfg2_specialized_assembly_matches_oracle():
+    """The reference's default element form (use_specializations = true, the
+    closed-form tetrahedron of NavierStokesSpecializations.hpp) on the full cfg2
+    mesh: FP64 values within 1e-11 of each row's scale, RHS within 1e-11."""
+    pb = P.config("cfg2")
+    ns = NavierStokes(pb.coords, pb.conn, dt=pb.dt, use_specializations=True)
+    ns.set_state(pb.up, pb.lin, pb.nu)
+    ns.add_dirichlet(pb.bc_nodes, pb.bc_comps, pb.bc_values)
+    o = oracle_for(pb, use_specializations=True)
+    ns.assemble()
+    o.assemble(os.cpu_count() or 1)
+    gv, gr = ns.system()
+    ov, orr = o.system()
+    orp, _ = o.csr()
+    err, rerr = row_scaled_error(gv, ov, orp), vec_rel_error(gr, orr)
+    print(f"cfg2 specialised: row-scaled matrix error {err:.3e}, RHS {rerr:.3e}")
+    assert err <= 1e-11 and rerr <= 1e-11
+    ns.close()
+    o.close()
