@@ -1331,15 +1331,16 @@ int ufem_batch_solve(ufem_batch* b, const ufem_krylov_opts* kopts, ufem_krylov_s
   }
   if (o.precond == 4) {
     // every member's coarse space and coarse matrix (of its current system);
-    // aggregates capped at 12 x 12 (2D) and 5^3 (3D) boxes, so that the host
-    // inversions of all members stay short
+    // aggregates capped at kBatchCoarseSide2D^2 (2D) and kBatchCoarseSide3D^3
+    // (3D) boxes, so that the host inversions of all members stay short
     if (b->coarse.size() != size_t(b->nmesh)) b->coarse.assign(size_t(b->nmesh), CoarseView{});
     bool any_new = false;
     for (int m = 0; m < b->nmesh; ++m) {
       if (!b->active[m]) continue;
       bool rebuilt = false;
       CoarseView cv;
-      if ((rc = krylov_coupled_coarse(b->members[m], st, 12, 5, &rebuilt, &cv))) return rc;
+      if ((rc = krylov_coupled_coarse(b->members[m], st, kBatchCoarseSide2D, kBatchCoarseSide3D, &rebuilt, &cv)))
+        return rc;
       const CoarseView& old = b->coarse[m];
       if (rebuilt || cv.nc != old.nc || cv.ainv != old.ainv || cv.agg != old.agg) any_new = true;
       b->coarse[m] = cv;

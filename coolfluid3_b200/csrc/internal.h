@@ -264,6 +264,11 @@ struct CoarseView {
 };
 int krylov_coupled_coarse(ufem_ns_handle* h, cudaStream_t s, int max_side_2d, int max_side_3d, bool* rebuilt,
                           CoarseView* view);
+// Aggregate caps (boxes a side) of the coupled two-level preconditioner: one
+// handle (its coarse inverse is computed on a host thread while the previous
+// one is used), and batch members (every member's inverse before the batch solve).
+constexpr int kCoarseSide2D = 20, kCoarseSide3D = 8;
+constexpr int kBatchCoarseSide2D = 16, kBatchCoarseSide3D = 5;
 // Allocations and static preconditioner structure of the solves `ko` describes,
 // ahead of the first solve (batched: for a batch member).
 int krylov_prepare(ufem_ns_handle* h, const ufem_krylov_opts* ko, int batched);

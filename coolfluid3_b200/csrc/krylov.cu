@@ -1492,11 +1492,11 @@ __global__ void vals_to32_kernel(int64_t n, const double* __restrict__ v, float*
 namespace {
 
 // Aggregates of the coupled two-level form: k^dim boxes of the mesh's bounding
-// box (k chosen for at least 64 nodes a box, at most 7 boxes a side in 3D and
-// 20 in 2D, so the coarse matrix stays small enough to invert on the host at
-// every solve); the coarse space holds the pressure rows of the nodes whose
-// pressure is neither a Dirichlet dof nor a periodic slave.  Built once per
-// Dirichlet plan: the aggregate of each row, the rows of each aggregate, and
+// box (k chosen for at least 64 nodes a box, at most max_side_3d boxes a side
+// in 3D and max_side_2d in 2D, so the coarse matrix stays small enough to invert
+// on the host at every solve); the coarse space holds the pressure rows of the
+// nodes whose pressure is neither a Dirichlet dof nor a periodic slave.  Built
+// once per condition list: the aggregate of each row, the rows of each aggregate, and
 // the pressure-pressure CSR positions sorted by (row aggregate, column
 // aggregate, position) with their segments.
 int coupled_coarse_build(ufem_ns_handle* h, int max_side_2d, int max_side_3d) {
@@ -1624,7 +1624,8 @@ int coupled_coarse_build(ufem_ns_handle* h, int max_side_2d, int max_side_3d) {
 // The coarse matrix of the current system (FP64 values, after the Dirichlet
 // pass), its inverse on the host, uploaded for the solve; cp_spd false (point
 // Jacobi for this solve) when it is not positive definite.
-int coupled_coarse_refresh(ufem_ns_handle* h, cudaStream_t s, int max_side_2d = 20, int max_side_3d = 7,
+int coupled_coarse_refresh(ufem_ns_handle* h, cudaStream_t s, int max_side_2d = kCoarseSide2D,
+                           int max_side_3d = kCoarseSide3D,
                            bool* rebuilt = nullptr, bool lag = false) {
   KrylovWork& kw = *h->kw;
   int rc;
@@ -1695,7 +1696,7 @@ int krylov_prepare(ufem_ns_handle* h, const ufem_krylov_opts* ko, int batched) {
   }
   KrylovWork& kw = *h->kw;
   if (o.precond == 4 && h->neq > 1) {
-    const int s2 = batched ? 12 : 20, s3 = batched ? 5 : 7;
+    const int s2 = batched ? kBatchCoarseSide2D : kCoarseSide2D, s3 = batched ? kBatchCoarseSide3D : kCoarseSide3D;
     if ((kw.cp_bc_version != h->bc_list_version || kw.cp_caps != s2 * 1000 + s3) &&
         (rc = coupled_coarse_build(h, s2, s3)))
       return rc;
@@ -1740,7 +1741,7 @@ int krylov_solve(ufem_ns_handle* h, const ufem_krylov_opts* ko, ufem_krylov_stat
   if (o.precond == 4) {  // coarse matrix of this system; point Jacobi when it is not positive definite
     // lagged: from the second solve on, each solve uses the previous solve's coarse
     // inverse while its own matrix is inverted on a host thread for the next one
-    if ((rc = coupled_coarse_refresh(h, s, 20, 7, nullptr, true))) return rc;
+    if ((rc = coupled_coarse_refresh(h, s, kCoarseSide2D, kCoarseSide3D, nullptr, true))) return rc;
     if (!h->kw->cp_spd) o.precond = 1;
   }
   KrylovWork& kw = *h->kw;

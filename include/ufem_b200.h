@@ -379,7 +379,7 @@ int ufem_batch_tune_assembly(ufem_batch* b, void* stream, int32_t reps, int32_t*
 int ufem_batch_assemble(ufem_batch* b, void* stream);
 /* statuses: one per member, or NULL.  BiCGStab (method 1) with precond 0, 1 or
  * 4 (the coupled two-level preconditioner, each member with its own coarse
- * space on at most 12 x 12 (2D) or 5^3 (3D) aggregates, coarse matrices
+ * space on at most 16 x 16 (2D) or 5^3 (3D) aggregates, coarse matrices
  * refreshed at every solve); mixed 0 or 1. */
 int ufem_batch_solve(ufem_batch* b, const ufem_krylov_opts* kopts, ufem_krylov_status* statuses, void* stream);
 int ufem_batch_update(ufem_batch* b, void* stream);
