@@ -9,10 +9,11 @@ inputs resident in HBM; the metric is elements assembled per second (Melem/s).
 
 `e2e` is the same metric through the public C ABI with host buffers: every step
 copies its fields from pinned host memory to the device and reads its RHS back.
-The value is the pipelined form (ufem_ns_stage_state on a copy stream,
+The value is the pipelined form (ufem_ns_stage_state on an upload stream,
 ufem_ns_commit_state + assembly + BCs on the compute stream, ufem_ns_fetch_rhs
-back on the copy stream), in which one step's copies overlap its neighbours'
-assembly; `e2e.sequential` is upload, assembly and read-back in turn.
+on a read-back stream), in which one step's copies overlap each other and
+their neighbours' assembly; `e2e.sequential` is upload, assembly and read-back
+in turn.
 
 Also reported (extra keys): the roofline of the assembly kernel, the FP64 CPU
 oracle timed on this host as the baseline, full time steps per second
@@ -81,6 +82,12 @@ def parse():
     ap.add_argument("--si-only", action="store_true", help="run only the semi-implicit comparison (one JSON line)")
     ap.add_argument("--cfg3-only", action="store_true", help="run only the 128^3 precision comparison (one JSON line)")
     ap.add_argument("--cfg4-only", action="store_true", help="run only the 256-mesh batch comparison (one JSON line)")
+    ap.add_argument("--ts-only", action="store_true",
+                    help="after the assembly measurement run only the full time steps (no CPU baseline, cfg3, cfg4, "
+                         "semi-implicit or serving)")
+    ap.add_argument("--ts-forms", nargs="*", default=None,
+                    help="time-step forms to run (plain_fp64, two_level, two_level_1e-12, mixed_two_level_1e-12, "
+                         "fp64_1e-13; default all)")
     return ap.parse_args()
 
 
@@ -367,16 +374,19 @@ def run_ours(args, rank, world, local):
     # ---- end to end through the C ABI with pinned host buffers ----------------
     # Every step copies its fields from pinned host memory and reads its RHS
     # back.  Sequential form: upload, assemble, read back, one after the other.
-    # Pipelined form (the e2e value): ufem_ns_stage_state / commit_state /
-    # fetch_rhs on a copy stream and the compute stream, so step k+1's upload
-    # and step k-1's read-back overlap step k's assembly.
+    # Pipelined form (the e2e value): ufem_ns_stage_state on an upload stream,
+    # commit_state + assembly on the compute stream, fetch_rhs on a read-back
+    # stream, so step k+1's upload and step k-1's read-back overlap step k's
+    # assembly and each other.
     up_h = torch.from_numpy(pb.up).pin_memory()
     lin_h = torch.from_numpy(pb.lin).pin_memory()
     nu_h = torch.from_numpy(pb.nu).pin_memory()
     rhs_h = [torch.empty(ns.nb_rows, dtype=torch.float64).pin_memory() for _ in range(2)]
     lib = Nat.lib()
-    cstream = torch.cuda.Stream(device=dev)
+    cstream = torch.cuda.Stream(device=dev)  # uploads
+    dstream = torch.cuda.Stream(device=dev)  # read-backs: the other direction of the host link
     cptr = Nat.C.c_void_p(cstream.cuda_stream)
+    dptr = Nat.C.c_void_p(dstream.cuda_stream)
     P_ = Nat.raw_dptr
 
     def e2e_step():
@@ -397,7 +407,7 @@ def run_ours(args, rank, world, local):
                 stage()
             Nat.check(lib.ufem_ns_commit_state(ns.handle, Nat.C.c_void_p(sptr)))
             assemble_step()
-            Nat.check(lib.ufem_ns_fetch_rhs(ns.handle, P_(rhs_h[k % 2].data_ptr()), Nat.C.c_void_p(sptr), cptr))
+            Nat.check(lib.ufem_ns_fetch_rhs(ns.handle, P_(rhs_h[k % 2].data_ptr()), Nat.C.c_void_p(sptr), dptr))
 
     for _ in range(args.warmup):
         e2e_step()
@@ -418,6 +428,7 @@ def run_ours(args, rank, world, local):
     p1 = torch.cuda.Event(enable_timing=True)
     p0.record(cstream)  # before the first upload
     e2e_pipelined(args.steps)
+    cstream.wait_stream(dstream)
     p1.record(cstream)  # after the last read-back
     p1.synchronize()
     torch.cuda.synchronize()
@@ -443,14 +454,16 @@ def run_ours(args, rank, world, local):
                      "traffic": traffic_bytes, "algorithmic_bytes": B, "kernel_ms": round(kern_ms, 4)},
         "e2e": {"value": round(E * world / (e2e_ms / 1e3) / 1e6, 3), "unit": "Melem/s",
                 "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h), "ms_per_step": round(e2e_ms, 3),
-                "form": "ufem_ns_stage_state (copy stream) / commit_state + assembly + BCs / fetch_rhs (copy stream): "
-                        "uploads and read-backs overlap the neighbouring steps' assembly",
+                "form": "ufem_ns_stage_state (upload stream) / commit_state + assembly + BCs / fetch_rhs (read-back "
+                        "stream): uploads and read-backs overlap each other and the neighbouring steps' assembly",
                 "sequential": {"value": round(E * world / (e2e_seq_ms / 1e3) / 1e6, 3), "ms_per_step": round(e2e_seq_ms, 3),
                                "form": "ufem_ns_upload_state, assembly + BCs, ufem_ns_download_system, in turn"}},
         "clocks": clk.summary(),
     }
 
-    if rank == 0 and world == 1 and not args.no_extras:
+    if rank == 0 and world == 1 and not args.no_extras and args.ts_only:
+        line["time_step"] = time_steps(ns, pb, args, stream, sptr)
+    elif rank == 0 and world == 1 and not args.no_extras:
         # ---- CPU baseline: the FP64 oracle on this host -------------------------
         v1, t1 = cpu_baseline(pb, 1)
         threads = os.cpu_count() or 1
@@ -476,7 +489,7 @@ def run_ours(args, rank, world, local):
         except Exception as exc:  # reported, not fatal: the assembly metric above stands
             line["semi_implicit"] = {"error": str(exc)}
     ns.close()
-    if rank == 0 and world == 1 and not args.no_extras and args.serve_requests > 0:
+    if rank == 0 and world == 1 and not args.no_extras and not args.ts_only and args.serve_requests > 0:
         # ---- served steps/s with p50/p99 vs the plain per-request path ----------
         line["serving"] = serving_in_child()
     if rank == 0:
@@ -500,13 +513,17 @@ def time_steps(ns, pb, args, stream, sptr):
              ("mixed_two_level_1e-12", dict(mixed=True, inner_tol=1e-5, tol=1e-12, precond="two_level_coupled")),
              ("fp64_1e-13", dict(mixed=True, inner_tol=1e-5, tol=1e-13, max_refine=40, precond="two_level_coupled")))
     for label, kw in forms:
+        if args.ts_forms is not None and label not in args.ts_forms:
+            continue
         ns.set_state(pb.up, pb.lin, pb.nu)
         ns.set_solution(np.zeros(ns.nb_rows))
         lat = []
         iters = []
         st = {"converged": 0}
         try:
-            for k in range(args.time_steps):
+            # one untimed step first: the form's one-time set-up (workspace,
+            # coarse-space structure, graph captures) is not a step's cost
+            for k in range(1 + args.time_steps):
                 torch.cuda.synchronize()
                 t0 = time.perf_counter()
                 ns.assemble(sptr)
@@ -514,12 +531,16 @@ def time_steps(ns, pb, args, stream, sptr):
                 st = ns.solve(sptr, raise_on_failure=False, max_iters=6000, **kw)
                 ns.update(sptr)
                 torch.cuda.synchronize()
-                lat.append((time.perf_counter() - t0) * 1e3)
-                iters.append(st["iterations"])
+                if k:
+                    lat.append((time.perf_counter() - t0) * 1e3)
+                    iters.append(st["iterations"])
                 if not st["converged"]:
                     break
         except Exception as exc:  # reported, not fatal: the assembly metric above stands
             out[label] = {"error": str(exc)}
+            continue
+        if not lat:
+            out[label] = {"error": "the untimed first step did not converge", "status": int(st.get("status", -1))}
             continue
         up, _ = ns.state()
         results[label] = up
@@ -536,6 +557,8 @@ def time_steps(ns, pb, args, stream, sptr):
                     "velocity": float(np.linalg.norm(d[:, :-1]) / np.linalg.norm(ref[:, :-1])),
                     "pressure": float(np.linalg.norm(d[:, -1]) / np.linalg.norm(ref[:, -1]))}
     out["steps"] = args.time_steps
+    out["note"] = ("each form starts from the same state, takes one untimed step, then the timed steps; errors "
+                   "compare the states after those steps")
     ns.set_state(base_up, pb.lin, pb.nu)
     return out
 
@@ -769,6 +792,20 @@ def serving_compare(args):
                               nsteps=args.serve_steps, seed=20261203)
     gen_s = time.perf_counter() - t0
     tol = 1e-12  # both sides at the residual that keeps the state within 1e-6 of the FP64 oracle
+
+    def server(mixed, lpre):
+        return S.Server(int(args.serve_budget_gb * 1e9), precision="fp64", mixed=mixed,
+                        krylov=dict(tol=tol, max_iters=20000), realtime=True, large_precond=lpre,
+                        small_precond=lpre, large_rows_2d=40_000)
+
+    forms = (("served_fp64", False, "two_level_coupled"), ("served_mixed", True, "two_level_coupled"))
+    # untimed warm-up of every form on a few of the requests (first launches of
+    # each kernel, graph captures, host thread pools, pinned buffers)
+    warm = S.poisson_workload(6, rate=args.serve_rate, elems=elems, nu=(1e-4, 1e-2), nsteps=2, seed=20261202)
+    S.run_plain(warm, krylov=dict(tol=tol, max_iters=20000), realtime=False)
+    S.run_plain(warm, krylov=dict(tol=tol, max_iters=20000, precond="two_level_coupled"), realtime=False)
+    for _, mixed, lpre in forms:
+        server(mixed, lpre).run(warm)
     plain, pst = S.run_plain(reqs, krylov=dict(tol=tol, max_iters=20000), realtime=True)
     plain2, pst2 = S.run_plain(reqs, krylov=dict(tol=tol, max_iters=20000, precond="two_level_coupled"), realtime=True)
 
@@ -789,16 +826,13 @@ def serving_compare(args):
                                 form="FP64 elements, FP64 BiCGStab + the coupled two-level preconditioner, one request "
                                      "at a time"),
     }
-    forms = (("served_fp64", False, "two_level_coupled"), ("served_mixed", True, "two_level_coupled"))
     for label, mixed, lpre in forms:
         # the served makespan depends on how the threads and streams interleave on
         # the device, so each form is served `serve_reps` times and the run with
         # the median throughput is reported (with the range)
         runs = []
         for _ in range(max(1, args.serve_reps)):
-            srv = S.Server(int(args.serve_budget_gb * 1e9), precision="fp64", mixed=mixed,
-                           krylov=dict(tol=tol, max_iters=20000), realtime=True, large_precond=lpre,
-                           small_precond=lpre, large_rows_2d=40_000)
+            srv = server(mixed, lpre)
             res, st = srv.run(reqs)
             runs.append((st["steps_per_s"], st, res, srv))
         runs.sort(key=lambda x: x[0])
@@ -810,11 +844,11 @@ def serving_compare(args):
                           speedup_vs_plain_two_level=round(st["steps_per_s"] / pst2["steps_per_s"], 3),
                           runs_steps_per_s=[round(r[0], 2) for r in runs],
                           max_rel_diff_vs_plain=max(diffs) if diffs else None,
-                          form=(("large requests: FP32 element matrices, FP32 inner BiCGStab with the coupled "
-                                 "two-level preconditioner refined against the matrix-free FP64 residual; batched "
-                                 "small requests: FP64 elements, FP64 BiCGStab + Jacobi" if mixed else
-                                 "FP64 elements, FP64 BiCGStab + Jacobi")
-                                + ", continuous batching (small requests batched, large ones concurrent)"))
+                          form=(("large requests: FP32 element matrices, FP32 inner BiCGStab refined against the "
+                                 "matrix-free FP64 residual; batched small requests: FP64 elements, FP64 BiCGStab"
+                                 if mixed else "FP64 elements, FP64 BiCGStab")
+                                + "; the coupled two-level preconditioner throughout; continuous batching (small "
+                                  "requests batched, large ones concurrent)"))
     out["note"] = ("every form solves to a 1e-12 relative FP64 residual, the tolerance at which the parity tests keep "
                    "the state within 1e-6 of the FP64 oracle (tests/test_serving.py, tests/test_matrix_free.py); "
                    "max_rel_diff_vs_plain is each served request's final state against the plain path's")
@@ -829,10 +863,7 @@ def serving_compare(args):
                                              "step_ms_p50": round(ps["step_ms"]["p50"], 2),
                                              "step_ms_p99": round(ps["step_ms"]["p99"], 2)}}
         for label, mixed, lpre in forms:
-            srv = S.Server(int(args.serve_budget_gb * 1e9), precision="fp64", mixed=mixed,
-                           krylov=dict(tol=tol, max_iters=20000), realtime=True, large_precond=lpre,
-                           small_precond=lpre, large_rows_2d=40_000)
-            _, st = srv.run(rq)
+            _, st = server(mixed, lpre).run(rq)
             row[label] = {"steps_per_s": round(st["steps_per_s"], 2), "step_ms_p50": round(st["step_ms"]["p50"], 2),
                           "step_ms_p99": round(st["step_ms"]["p99"], 2),
                           "speedup": round(st["steps_per_s"] / ps["steps_per_s"], 2)}

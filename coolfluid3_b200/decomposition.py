@@ -17,8 +17,9 @@ synchronised after each loop (common/PE/CommPattern.cpp:567-599).  Here:
   owned row moves its constrained ghost columns exactly as the single mesh does.
 * ``DistributedNS.solve``: BiCGStab with point Jacobi on the owned rows.  Before
   each SpMV the ghost values are fetched from their owners
-  (``torch.distributed`` point-to-point: NCCL between GPUs, gloo on CPU) into the
-  local vector; dot products are local sums all-reduced over the ranks.
+  (``torch.distributed`` point-to-point: NCCL between GPUs, gloo on CPU; device
+  vectors under gloo travel through host copies) into the local vector; dot
+  products are local sums all-reduced over the ranks.
 * A local engine does the per-rank work.  ``GPUEngine`` is a ``NavierStokes``
   handle on the local mesh whose vectors stay in device memory (the SpMV is the
   library's, ``ufem_ns_apply_device``); any object with the same methods can
@@ -120,19 +121,27 @@ class Halo:
         import torch.distributed as dist
         if not self.send and not self.recv:
             return
+        # gloo moves host memory only: device vectors go through host copies
+        wire = torch.device("cpu") if _host_wire(x) else x.device
         ops, inbox, outbox = [], {}, []
         for p, idx in self.send.items():
-            buf = x[idx].contiguous()
+            buf = x[idx].to(wire).contiguous()
             outbox.append(buf)
             ops.append(dist.P2POp(dist.isend, buf, p))
         for p, idx in self.recv.items():
-            buf = torch.empty(len(idx), dtype=x.dtype, device=x.device)
+            buf = torch.empty(len(idx), dtype=x.dtype, device=wire)
             inbox[p] = buf
             ops.append(dist.P2POp(dist.irecv, buf, p))
         for req in dist.batch_isend_irecv(ops):
             req.wait()
         for p, buf in inbox.items():
-            x[self.recv[p]] = buf
+            x[self.recv[p]] = buf.to(x.device)
+
+
+def _host_wire(x) -> bool:
+    """True when x lives in device memory and the process group is gloo."""
+    import torch.distributed as dist
+    return x.device.type != "cpu" and dist.is_initialized() and dist.get_backend() == "gloo"
 
 
 def _allreduce(vals):
@@ -141,6 +150,8 @@ def _allreduce(vals):
     import torch.distributed as dist
     t = torch.stack([v.reshape(()) for v in vals]).to(torch.float64)
     if dist.is_available() and dist.is_initialized() and dist.get_world_size() > 1:
+        if _host_wire(t):
+            t = t.cpu()
         dist.all_reduce(t)
     return t
 

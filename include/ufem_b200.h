@@ -305,7 +305,10 @@ int ufem_ns_read_restart(ufem_ns_handle* h, const char* path, double* current_ti
  *  - ufem_ns_fetch_rhs copies the RHS into one of two device output buffers on
  *    `stream` (after the work queued there) and reads it into `rhs` (nb_rows
  *    doubles) on `copy_stream`; it is complete when `copy_stream` is.
- * Host buffers should be pinned for the copies to overlap.  A staged buffer is
+ * Host buffers should be pinned for the copies to overlap.  Giving
+ * ufem_ns_fetch_rhs a copy stream of its own (not the one ufem_ns_stage_state
+ * uses) lets the read-backs run concurrently with the uploads (the host link
+ * carries both directions at once).  A staged buffer is
  * reused only after its commit has read it and an output buffer only after its
  * read-back, so each host buffer may be reused once the copy stream has passed
  * its copy.  The buffers (2 x N x (neq + 4 dim + 1) + 2 x nb_rows doubles) are

@@ -96,7 +96,17 @@ def test_cfg3_assembly_matches_oracle(precision):
 def test_cfg2_specialized_assembly_matches_oracle():
     """The reference's default element form (use_specializations = true, the
     closed-form tetrahedron of NavierStokesSpecializations.hpp) on the full cfg2
-    mesh: FP64 values within 1e-11 of each row's scale, RHS within 1e-11."""
+    mesh (64^3 x 6 tets).
+
+    The closed form takes the tetrahedron's volume from the 24-term expansion of
+    the determinant in absolute coordinates (Tetra3D.cpp:104-128): terms of
+    order one cancel down to a volume of order h^3 = n^-3, so either side's
+    rounding is of order eps * n^3 relative to the volume, and everything
+    divided by it inherits that.  Measured against the oracle: 0.34, 0.45 and
+    0.44 eps * n^3 at n = 16, 32, 64 (3.1e-13, 3.3e-12, 2.5e-11).  Bound: 4 eps
+    n^3 (2.3e-10 at n = 64) for the row-scaled values and the RHS; the generic
+    form, which takes coordinate differences first, stays within 1e-11 at every
+    size (the tests above)."""
     pb = P.config("cfg2")
     ns = NavierStokes(pb.coords, pb.conn, dt=pb.dt, use_specializations=True)
     ns.set_state(pb.up, pb.lin, pb.nu)
@@ -109,6 +119,7 @@ def test_cfg2_specialized_assembly_matches_oracle():
     orp, _ = o.csr()
     err, rerr = row_scaled_error(gv, ov, orp), vec_rel_error(gr, orr)
     print(f"cfg2 specialised: row-scaled matrix error {err:.3e}, RHS {rerr:.3e}")
-    assert err <= 1e-11 and rerr <= 1e-11
+    tol = 4 * np.finfo(np.float64).eps * 64**3
+    assert err <= tol and rerr <= tol
     ns.close()
     o.close()

@@ -94,14 +94,20 @@ def _problem():
     return P.make_problem(3, 5)
 
 
-def _rank(rank, world, port, q):
+def _rank(rank, world, port, q, engine="oracle"):
     import torch.distributed as dist
     sys.path.insert(0, ROOT)
     os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
     dist.init_process_group("gloo", rank=rank, world_size=world, timeout=datetime.timedelta(seconds=120))
     try:
         pb = _problem()
-        dn = D.DistributedNS(pb.coords, pb.conn, lambda c, e: OracleEngine(c, e, pb.dt), rank=rank, world=world)
+        if engine == "gpu":
+            def factory(c, e):
+                return D.GPUEngine(c, e, dt=pb.dt, use_specializations=False)
+        else:
+            def factory(c, e):
+                return OracleEngine(c, e, pb.dt)
+        dn = D.DistributedNS(pb.coords, pb.conn, factory, rank=rank, world=world)
         dn.set_state(pb.up, pb.lin, pb.nu)
         dn.add_dirichlet(pb.bc_nodes, pb.bc_comps, pb.bc_values)
         dn.assemble()
@@ -113,6 +119,8 @@ def _rank(rank, world, port, q):
             stats.append(dn.step(1, tol=1e-12, max_iters=5000))
         nodes, up = dn.owned_state()
         q.put((rank, system, nodes, up, stats))
+        if engine == "gpu":
+            dn.engine.close()
     finally:
         dist.destroy_process_group()
 
@@ -149,20 +157,49 @@ def test_partition_covers_and_matches_halos():
                 assert np.array_equal(p.nodes[pos], q.nodes[q.send[p.rank]])
 
 
-@pytest.mark.parametrize("world", [2, 3])
-def test_distributed_assembly_and_steps_match_single_mesh(world):
+def _run_ranks(world, engine):
     ctx = mp.get_context("spawn")
     q = ctx.Queue()
     port = _free_port()
-    procs = [ctx.Process(target=_rank, args=(r, world, port, q)) for r in range(world)]
+    procs = [ctx.Process(target=_rank, args=(r, world, port, q, engine)) for r in range(world)]
     for p in procs:
         p.start()
     out = [q.get(timeout=300) for _ in range(world)]
     for p in procs:
         p.join(timeout=60)
         assert p.exitcode == 0
+    _check_against_single_mesh(out, engine)
+
+
+@pytest.mark.parametrize("world", [2, 3])
+def test_distributed_assembly_and_steps_match_single_mesh(world):
+    _run_ranks(world, "oracle")
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("world", [2, 3])
+def test_gpu_engine_ranks_match_single_mesh(world):
+    """The same check with the device-resident engine on every rank: the ranks
+    share the one GPU of this machine, each with its own context and handle;
+    the ghost values and the dot products go between them through gloo on the
+    host (no kernel waits on another rank)."""
+    _run_ranks(world, "gpu")
+
+
+def _check_against_single_mesh(out, engine):
+    """Owned rows bitwise equal to the single mesh's system assembled by the
+    same engine; the state after three steps within 1e-6 of the oracle's."""
     pb = _problem()
     rp, ci, vals, rhs, up_ref = _single_mesh(pb, 3)
+    if engine == "gpu":
+        from coolfluid3_b200 import NavierStokes
+        ns = NavierStokes(pb.coords, pb.conn, dt=pb.dt, use_specializations=False)
+        ns.set_state(pb.up, pb.lin, pb.nu)
+        ns.add_dirichlet(pb.bc_nodes, pb.bc_comps, pb.bc_values)
+        ns.assemble()
+        ns.apply_dirichlet()
+        vals, rhs = ns.system()
+        ns.close()
     neq = pb.dim + 1
     rows = np.repeat(np.arange(len(rp) - 1), np.diff(rp))
     ref = dict(zip(zip(rows.tolist(), ci.tolist()), vals.tolist()))
