@@ -55,6 +55,12 @@ struct KrylovWork {
   };
   CGGraph cg_graph[2];
   CGGraph bicg_graph[2];   // the same for BiCGStab
+  // Iterations of the previous BiCGStab solve per operator type: the host's
+  // first look at the done flag comes after that many (rounded down to a
+  // graph block), so a solve like the last one launches few iterations past
+  // its convergence.
+  int bicg_expect[2] = {0, 0};
+  int cg_expect[2] = {0, 0};   // the same for CG
   bool use_graph = true;   // false for the allocation-free solve (instantiation allocates)
   cudaStream_t capture_stream = nullptr;
   int cg_nblk = 0;             // blocks of the fused CG kernels (more than nblk: they are latency-bound)
@@ -1299,11 +1305,15 @@ int bicgstab(ufem_ns_handle* h, KrylovWork& kw, const MT* vals, const BT* b, VT*
       std::copy(key, key + 16, gr->key);
     }
   }
-  // The host reads the done flag after 8, then 16, 32 and at most 64 more
-  // iterations: few synchronisations on long solves, little overshoot on short
-  // ones (iterations after convergence return at once on the device flag).
-  int check = kBlock;
-  for (int it = 0; it < maxit; it += check, check = std::min(2 * check, 64)) {
+  // The host reads the done flag first after the previous solve's iteration
+  // count (rounded down to a block of 8; 8 for the handle's first solve), then
+  // after 8, 16, 32 and at most 64 more iterations: few synchronisations on
+  // long solves, little overshoot on short ones or ones like the last
+  // (iterations after convergence return at once on the device flag, so the
+  // cadence changes no result).
+  int& expect = kw.bicg_expect[std::is_same<MT, float>::value ? 1 : 0];
+  int check = std::max(kBlock, expect / kBlock * kBlock);
+  for (int it = 0, next = kBlock; it < maxit; it += check, check = next, next = std::min(2 * next, 64)) {
     for (int k = 0; k < check; k += kBlock) {
       if (gr) {
         UFEM_CUDA_TRY(cudaGraphLaunch(gr->exec, st));
@@ -1321,6 +1331,7 @@ int bicgstab(ufem_ns_handle* h, KrylovWork& kw, const MT* vals, const BT* b, VT*
   UFEM_CUDA_TRY(cudaStreamSynchronize(st));
   res.iters = kw.h_ictl[3];
   res.status = kw.h_ictl[2];
+  expect = res.iters;
   const double bnorm = kw.h_dctl[kBnorm];
   if (bnorm == 0.0) {
     fill_kernel<VT><<<g1, kRedThreads, 0, st>>>(n, VT(0), x);
@@ -1388,8 +1399,9 @@ int cg_iteration(ufem_ns_handle* h, KrylovWork& kw, const MT* vals, VT* x, VT* r
 // "Block CG" of the reference's semi-implicit velocity and pressure solves,
 // block size 1).  The iterations are small, latency-bound launches on
 // systems of a few hundred thousand rows, so a block of 8 is captured once in
-// a CUDA graph (per operand set) and replayed 1, 2, 4 and then 8 times between
-// host checks of the done flag; iterations after convergence return at once.
+// a CUDA graph (per operand set) and replayed between host checks of the done
+// flag: first as many blocks as the previous solve needed, then 1, 2, 4 and
+// then 8; iterations after convergence return at once.
 template <typename VT, typename MT, typename BT>
 int cg(ufem_ns_handle* h, KrylovWork& kw, const MT* vals, const BT* b, VT* x, VT* r, VT* z, VT* p, VT* q, VT* dinv,
        int pkind, double tol, int maxit, cudaStream_t st, SolveResult& res) {
@@ -1448,7 +1460,11 @@ int cg(ufem_ns_handle* h, KrylovWork& kw, const MT* vals, const BT* b, VT* x, VT
     gr.maxit = maxit;
     std::copy(key, key + 16, gr.key);
   }
-  for (int it = 0, reps = 1; it < maxit; it += reps * kCGBlock, reps = std::min(2 * reps, 8)) {
+  // first look at the done flag after the previous solve's iteration count
+  // (rounded down to a block), then after 1, 2, 4 and at most 8 more blocks
+  int& expect = kw.cg_expect[std::is_same<MT, float>::value ? 1 : 0];
+  int reps = std::max(1, expect / kCGBlock);
+  for (int it = 0, next = 1; it < maxit; it += reps * kCGBlock, reps = next, next = std::min(2 * next, 8)) {
     for (int k = 0; k < reps; ++k) UFEM_CUDA_TRY(cudaGraphLaunch(gr.exec, st));
     UFEM_CUDA_TRY(cudaMemcpyAsync(kw.h_ictl, kw.ictl, 4 * sizeof(int), cudaMemcpyDeviceToHost, st));
     UFEM_CUDA_TRY(cudaStreamSynchronize(st));
@@ -1459,6 +1475,7 @@ int cg(ufem_ns_handle* h, KrylovWork& kw, const MT* vals, const BT* b, VT* x, VT
   UFEM_CUDA_TRY(cudaStreamSynchronize(st));
   res.iters = kw.h_ictl[3];
   res.status = kw.h_ictl[2];
+  expect = res.iters;
   const double bnorm = kw.h_dctl[kBnorm];
   if (bnorm == 0.0) {
     fill_kernel<VT><<<g1, kRedThreads, 0, st>>>(n, VT(0), x);
