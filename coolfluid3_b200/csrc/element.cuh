@@ -38,6 +38,13 @@ __device__ __forceinline__ KParams<T> make_kparams(const NSParams& p) {
 
 __device__ __forceinline__ double tsqrt(double x) { return sqrt(x); }
 __device__ __forceinline__ float tsqrt(float x) { return sqrtf(x); }
+// 1/sqrt(x) and 1/x through CUDA's reciprocal square root and correctly rounded
+// reciprocal: one short dependent sequence each instead of a square root or
+// a division followed by another (the element routines are latency-bound)
+__device__ __forceinline__ double trsqrt(double x) { return rsqrt(x); }
+__device__ __forceinline__ float trsqrt(float x) { return rsqrtf(x); }
+__device__ __forceinline__ double trcp(double x) { return __drcp_rn(x); }
+__device__ __forceinline__ float trcp(float x) { return __frcp_rn(x); }
 __device__ __forceinline__ double tabs(double x) { return fabs(x); }
 __device__ __forceinline__ float tabs(float x) { return fabsf(x); }
 __device__ __forceinline__ double tcbrt_pow(double x) { return pow(x, 1. / 3.); }
@@ -63,7 +70,7 @@ __device__ __forceinline__ void ld4(const double* __restrict__ p, double& a, dou
 template <typename T>
 __device__ __forceinline__ void inverse_det(const T (&J)[2][2], T (&Ji)[2][2], T& det) {
   det = J[0][0] * J[1][1] - J[1][0] * J[0][1];
-  const T inv = T(1) / det;
+  const T inv = trcp(det);
   Ji[0][0] = J[1][1] * inv;
   Ji[1][0] = -J[1][0] * inv;
   Ji[0][1] = -J[0][1] * inv;
@@ -80,7 +87,7 @@ __device__ __forceinline__ void inverse_det(const T (&m)[3][3], T (&Ji)[3][3], T
       cof[i][j] = m[i1][j1] * m[i2][j2] - m[i1][j2] * m[i2][j1];
     }
   det = (cof[0][0] * m[0][0] + cof[1][0] * m[1][0]) + cof[2][0] * m[2][0];
-  const T inv = T(1) / det;
+  const T inv = trcp(det);
 #pragma unroll
   for (int i = 0; i < 3; ++i)
 #pragma unroll
@@ -209,10 +216,10 @@ __device__ __forceinline__ void compute_tau(const KParams<T>& kp, const Elem<D, 
     }
     const T adv_sq = tabs(adv);
     const T diff = element_nu * element_nu * sq;
-    tsu = T(1) / tsqrt(kp.tau_c1 + adv_sq + c2 * diff);  // tau_c1 = 4 c1^2 / dt^2
+    tsu = trsqrt(kp.tau_c1 + adv_sq + c2 * diff);  // tau_c1 = 4 c1^2 / dt^2
     tps = tsu;
     // 1 / tau_su of the standard constants (tau_std = 4 / dt^2)
-    tbu = tsqrt(kp.tau_std + adv_sq + T(16) * diff) / tr;
+    tbu = tsqrt(kp.tau_std + adv_sq + T(16) * diff) * trcp(tr);
   } else {  // CF2
     const T volume = (D == 2) ? det / T(2) : det / T(6);
     const T pi = T(3.141592654);
