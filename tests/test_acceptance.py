@@ -14,6 +14,14 @@ the parity tests):
     pressure imposed at the centre through a function condition), checked at
     the last step as the test does (:321-326): |u|, |v| errors <= 1.4e-3,
     |p| error <= 3.3e-3.
+  - plugins/UFEM/test/atest-ufem-navier-stokes-periodic-channel-2d.py -- a
+    10 x 1 channel, periodic in x (right linked to left), no-slip walls,
+    driven by the body force a_tau = Re_tau^2 nu^2 / h^3 (Re_tau 50, h 0.5,
+    nu 1e-4), dt 1000 to t = 20000 (20 steps), no pressure condition, solved
+    to 1e-5 as the test does: the largest u within 0.05 of the laminar
+    centre-line velocity U_c = a_tau / nu * h^2 / 2 = 0.25 (:158-163); the
+    reference's mesh is 10 x 20 quadrilaterals graded towards the walls, here
+    10 x 20 uniform cells split into triangles.
 The reference runs these on quadrilaterals (its Taylor-Green test also
 offers triangles); here the meshes are triangles.  The coupled scheme meets
 every bound as published.  The semi-implicit scheme meets the velocity
@@ -133,3 +141,36 @@ def test_taylor_green_semi_implicit():
         assert M.step(1)[0] == 0
     eu, ev, ep = tg.errors(M.state()[0], tg.nsteps)
     assert eu <= 1.4e-3 and ev <= 1.4e-3 and ep <= 3.6e-3, (eu, ev, ep)
+
+
+class PeriodicChannel:
+    h, re_tau, nu, dt, nsteps, tol = 0.5, 50.0, 1e-4, 1000.0, 20, 1e-5
+
+    def __init__(self, nx=10, ny=20):
+        c, t = O.mesh_rectangle_tris(nx, ny, 0.0, 1)
+        self.c = c.copy()
+        self.c[:, 0] *= 10.0
+        self.t = t
+        self.a_tau = self.re_tau ** 2 * self.nu ** 2 / self.h ** 3
+        self.Uc = self.a_tau / self.nu * self.h ** 2 / 2.0
+        key = {tuple(np.round(p, 9)): i for i, p in enumerate(self.c)}
+        right = np.where(np.abs(self.c[:, 0] - 10.0) < 1e-9)[0]
+        self.links = (right, np.array([key[(0.0, round(self.c[i, 1], 9))] for i in right]))
+        wall = np.where((np.abs(self.c[:, 1]) < 1e-9) | (np.abs(self.c[:, 1] - 1.0) < 1e-9))[0]
+        self.bcs = (np.repeat(wall, 2), np.tile([0, 1], len(wall)), np.zeros(2 * len(wall)))
+        N = self.c.shape[0]
+        self.up = np.zeros((N, 3))
+        self.lin = np.zeros((N, 8))
+        self.nuv = np.full(N, self.nu)
+        self.force = np.tile([self.a_tau, 0.0], (N, 1))
+
+
+def test_periodic_channel_laminar_profile():
+    pc = PeriodicChannel()
+    S = O.Oracle(pc.c, pc.t, O.options(dt=pc.dt, use_specializations=False), periodic_links=pc.links)
+    S.set_state(pc.up, pc.lin, pc.nuv, pc.force)
+    S.add_dirichlet(*pc.bcs)
+    for _ in range(pc.nsteps):
+        assert S.step(1, tol=pc.tol) == 0
+    u = S.state()[0]
+    assert abs(u[:, 0].max() - pc.Uc) <= 0.05, u[:, 0].max()

@@ -118,3 +118,32 @@ def test_bad_links_are_refused():
     one = P.make_problem(2, 1, nu=1e-2, dt=0.01)  # a single cell: a node and its partner share an element
     with pytest.raises(UfemError, match="too thin"):
         NavierStokes(one.coords, one.conn, dt=one.dt, periodic_links=([1, 3], [0, 2]))
+
+
+@pytest.mark.gpu
+def test_periodic_channel_acceptance_gpu():
+    """The reference's periodic-channel acceptance case (the oracle replay in
+    tests/test_acceptance.py) on the library: 20 steps at dt 1000, BiCGStab to
+    the reference's 1e-5, the largest u within 0.05 of the laminar centre-line
+    velocity 0.25 and within 1e-3 of the oracle's."""
+    from .test_acceptance import PeriodicChannel
+    pc = PeriodicChannel()
+    links = (pc.links[0].astype(np.uint32), pc.links[1].astype(np.uint32))
+    bcs = (pc.bcs[0].astype(np.uint32), pc.bcs[1].astype(np.int32), pc.bcs[2])
+    ns = NavierStokes(pc.c, pc.t, dt=pc.dt, use_specializations=False, periodic_links=links)
+    ns.set_state(pc.up, pc.lin, pc.nuv, pc.force)
+    ns.add_dirichlet(*bcs)
+    for _ in range(pc.nsteps):
+        st = ns.execute(tol=pc.tol, max_iters=5000)
+        assert st["converged"] == 1, st
+    u = ns.state()[0]
+    ns.close()
+    o = O.Oracle(pc.c, pc.t, O.options(dt=pc.dt, use_specializations=False), periodic_links=pc.links)
+    o.set_state(pc.up, pc.lin, pc.nuv, pc.force)
+    o.add_dirichlet(*pc.bcs)
+    for _ in range(pc.nsteps):
+        assert o.step(1, tol=pc.tol) == 0
+    uo = o.state()[0]
+    o.close()
+    assert abs(u[:, 0].max() - pc.Uc) <= 0.05, u[:, 0].max()
+    assert abs(u[:, 0].max() - uo[:, 0].max()) <= 1e-3, (u[:, 0].max(), uo[:, 0].max())
