@@ -1339,7 +1339,10 @@ int ufem_batch_solve(ufem_batch* b, const ufem_krylov_opts* kopts, ufem_krylov_s
       if (!b->active[m]) continue;
       bool rebuilt = false;
       CoarseView cv;
-      if ((rc = krylov_coupled_coarse(b->members[m], st, kBatchCoarseSide2D, kBatchCoarseSide3D, &rebuilt, &cv)))
+      // not lagged: a member's inverse is of its current matrix (with the
+      // previous step's, the hardest cfg4-like members converged less often)
+      if ((rc = krylov_coupled_coarse(b->members[m], st, kBatchCoarseSide2D, kBatchCoarseSide3D, &rebuilt, &cv,
+                                      false)))
         return rc;
       const CoarseView& old = b->coarse[m];
       if (rebuilt || cv.nc != old.nc || cv.ainv != old.ainv || cv.agg != old.agg) any_new = true;

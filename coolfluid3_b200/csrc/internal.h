@@ -253,8 +253,10 @@ int krylov_apply(ufem_ns_handle* h, const double* d_x, double* d_y, cudaStream_t
 int krylov_fp64_residual(ufem_ns_handle* h, double* r_host, cudaStream_t s);
 // Coarse space of the coupled two-level preconditioner of one handle, rebuilt
 // when its Dirichlet plan or the aggregate caps change (rebuilt = true) and its
-// coarse matrix refreshed from the current system (krylov.cu).  nc = 0: no
-// usable coarse space (point Jacobi).
+// coarse matrix refreshed from the current system (krylov.cu).  lag: from the
+// handle's second refresh on, the inverse is the previous refresh's matrix's,
+// and this refresh's matrix is inverted on a host thread for the next one.
+// nc = 0: no usable coarse space (point Jacobi).
 struct CoarseView {
   int nc = 0;
   const int32_t* agg = nullptr;
@@ -263,7 +265,7 @@ struct CoarseView {
   const double* ainv = nullptr;
 };
 int krylov_coupled_coarse(ufem_ns_handle* h, cudaStream_t s, int max_side_2d, int max_side_3d, bool* rebuilt,
-                          CoarseView* view);
+                          CoarseView* view, bool lag);
 // Aggregate caps (boxes a side) of the coupled two-level preconditioner: one
 // handle (its coarse inverse is computed on a host thread while the previous
 // one is used), and batch members (every member's inverse before the batch solve).

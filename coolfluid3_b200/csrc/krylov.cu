@@ -1722,10 +1722,10 @@ int krylov_prepare(ufem_ns_handle* h, const ufem_krylov_opts* ko, int batched) {
 }
 
 int krylov_coupled_coarse(ufem_ns_handle* h, cudaStream_t s, int max_side_2d, int max_side_3d, bool* rebuilt,
-                          CoarseView* view) {
+                          CoarseView* view, bool lag) {
   if (!h->kw) h->kw = new KrylovWork();  // coarse data only: batch members keep their vectors in the batch
   int rc;
-  if ((rc = coupled_coarse_refresh(h, s, max_side_2d, max_side_3d, rebuilt))) return rc;
+  if ((rc = coupled_coarse_refresh(h, s, max_side_2d, max_side_3d, rebuilt, lag))) return rc;
   const KrylovWork& kw = *h->kw;
   view->nc = kw.cp_spd ? kw.nc : 0;
   view->agg = kw.agg;
