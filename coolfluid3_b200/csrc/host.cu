@@ -1091,6 +1091,7 @@ int ufem_ns_assemble(ufem_ns_handle* h, void* stream) {
   if ((rc = launch_tie_rows(h, s, w32))) return rc;
   record(h, 1, true, s);
   h->vals32_valid = w32;
+  h->conditioned = false;
   return UFEM_OK;
 }
 
@@ -1189,6 +1190,7 @@ int ufem_ns_apply_dirichlet(ufem_ns_handle* h, void* stream) {
   if ((rc = launch_neumann(h, s))) return rc;
   if ((rc = launch_dirichlet(h, s))) return rc;
   record(h, 2, true, s);
+  h->conditioned = true;
   return UFEM_OK;
 }
 

@@ -189,6 +189,7 @@ struct ufem_ns_handle {
   ufem::StagePipe pipe;
   ufem::KrylovWork* kw = nullptr;
   bool vals32_valid = false;            // d_vals32 holds the current system (written by the assembly)
+  bool conditioned = false;             // the Dirichlet conditions ran after the latest assembly
 
   // transfer staging (reference field layouts <-> padded node records)
   double* d_stage = nullptr;      // N x 4*dim doubles

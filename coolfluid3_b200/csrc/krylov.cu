@@ -1717,6 +1717,18 @@ int krylov_prepare(ufem_ns_handle* h, const ufem_krylov_opts* ko, int batched) {
     if ((kw.cp_bc_version != h->bc_list_version || kw.cp_caps != s2 * 1000 + s3) &&
         (rc = coupled_coarse_build(h, s2, s3)))
       return rc;
+    if (!batched && h->conditioned) {
+      // the coarse inverse of the system as it stands, which the next solve
+      // takes as its lagged inverse: the first solve after this does not wait
+      // for a host inversion (on a private stream; nothing else is touched)
+      cudaStream_t ps = nullptr;
+      UFEM_CUDA_TRY(cudaStreamCreateWithFlags(&ps, cudaStreamNonBlocking));
+      rc = coupled_coarse_refresh(h, ps, s2, s3, nullptr, true);
+      const cudaError_t ce = cudaStreamSynchronize(ps);
+      cudaStreamDestroy(ps);
+      if (rc) return rc;
+      if (ce != cudaSuccess) return set_error(UFEM_ERR_CUDA, std::string("prepare: ") + cudaGetErrorString(ce));
+    }
   }
   return UFEM_OK;
 }

@@ -404,8 +404,16 @@ class Server:
             try:
                 large = self._is_large(req.dim, req.coords.shape[0] * (req.dim + 1))
                 ns = _new_handle(req, "fp32" if (large and self.mixed) else self.precision, self.spec)
-                # solver workspace and preconditioner structure on this host thread,
-                # not on the worker that steps the request
+                # the one-time work of the first step on this host thread, not on
+                # the worker that steps the request: the Dirichlet plan (built by
+                # the first conditioning of an assembled system), the solver
+                # workspace, the preconditioner structure and, for one handle,
+                # the coarse inverse of the first system (which its first solve
+                # would otherwise compute first); the state is unchanged
+                s = torch.cuda.Stream()
+                ns.assemble(s)
+                ns.apply_dirichlet(s)
+                s.synchronize()
                 kr = self.krylov_large if large else (self.krylov_mixed if self.mixed_scope == "all" else self.krylov)
                 ns.prepare_solve(batched=not large, **kr)
             except Exception as e:  # the request is rejected; the others go on

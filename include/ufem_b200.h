@@ -233,8 +233,12 @@ int ufem_ns_solve(ufem_ns_handle* h, const ufem_krylov_opts* kopts, ufem_krylov_
  * preconditioner that solves with `kopts` will use (the coarse space of precond
  * 4), ahead of the first solve -- e.g. on the host thread that created the
  * handle, while the GPU steps other handles.  batched = 1 prepares a future
- * batch member (no one-handle vectors; the batch's aggregate caps).  No
- * counterpart in the reference. */
+ * batch member (no one-handle vectors; the batch's aggregate caps).  For one
+ * handle (batched = 0) whose system has been assembled and conditioned
+ * (ufem_ns_assemble, then ufem_ns_apply_dirichlet), precond 4 also gets the
+ * coarse inverse of that system, which the next solve uses as its lagged
+ * inverse, so that the first solve does not wait for a host inversion; the
+ * call returns when it is done.  No counterpart in the reference. */
 int ufem_ns_prepare_solve(ufem_ns_handle* h, const ufem_krylov_opts* kopts, int32_t batched);
 /* Allocation-free variant of ufem_ns_solve.  No counterpart in the reference.
  * For callers that cannot call cudaMalloc: applications that hand all device
