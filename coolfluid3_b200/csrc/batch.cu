@@ -23,6 +23,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstdint>
+#include <memory>
 #include <string>
 #include <vector>
 
@@ -1335,18 +1336,18 @@ int ufem_batch_solve(ufem_batch* b, const ufem_krylov_opts* kopts, ufem_krylov_s
     // (3D) boxes, so that the host inversions of all members stay short
     if (b->coarse.size() != size_t(b->nmesh)) b->coarse.assign(size_t(b->nmesh), CoarseView{});
     bool any_new = false;
+    std::vector<CoarseView> cv(size_t(b->nmesh));
+    std::unique_ptr<bool[]> rebuilt(new bool[size_t(b->nmesh)]);
+    // not lagged: each member's inverse is of its current matrix (with the
+    // previous step's, the hardest cfg4-like members converged less often)
+    if ((rc = krylov_coupled_coarse_members(b->members.data(), b->active.data(), b->nmesh, st, kBatchCoarseSide2D,
+                                            kBatchCoarseSide3D, rebuilt.get(), cv.data())))
+      return rc;
     for (int m = 0; m < b->nmesh; ++m) {
       if (!b->active[m]) continue;
-      bool rebuilt = false;
-      CoarseView cv;
-      // not lagged: a member's inverse is of its current matrix (with the
-      // previous step's, the hardest cfg4-like members converged less often)
-      if ((rc = krylov_coupled_coarse(b->members[m], st, kBatchCoarseSide2D, kBatchCoarseSide3D, &rebuilt, &cv,
-                                      false)))
-        return rc;
       const CoarseView& old = b->coarse[m];
-      if (rebuilt || cv.nc != old.nc || cv.ainv != old.ainv || cv.agg != old.agg) any_new = true;
-      b->coarse[m] = cv;
+      if (rebuilt[m] || cv[m].nc != old.nc || cv[m].ainv != old.ainv || cv[m].agg != old.agg) any_new = true;
+      b->coarse[m] = cv[m];
     }
     if (any_new) {
       UFEM_CUDA_TRY(cudaStreamSynchronize(st));

@@ -267,6 +267,12 @@ struct CoarseView {
 };
 int krylov_coupled_coarse(ufem_ns_handle* h, cudaStream_t s, int max_side_2d, int max_side_3d, bool* rebuilt,
                           CoarseView* view, bool lag);
+// The same for the active members of a batch, not lagged: every member's
+// coarse matrix summed and copied on `s`, one synchronisation, the inversions
+// on host threads in parallel (each the one-handle inversion, bitwise), the
+// inverses uploaded on `s`.
+int krylov_coupled_coarse_members(ufem_ns_handle* const* hs, const int32_t* active, int n, cudaStream_t s,
+                                  int max_side_2d, int max_side_3d, bool* rebuilt, CoarseView* views);
 // Aggregate caps (boxes a side) of the coupled two-level preconditioner: one
 // handle (its coarse inverse is computed on a host thread while the previous
 // one is used), and batch members (every member's inverse before the batch solve).

@@ -13,6 +13,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <atomic>
 #include <cmath>
 #include <cstdint>
 #include <cstring>
@@ -139,7 +140,7 @@ __device__ __forceinline__ double block_sum(double v, double* sm) {
 // split over host threads; each column's arithmetic is the same whatever the
 // split.  False if a pivot is not positive (a coarse matrix of a system without
 // conditions that fix its constant mode is singular).
-bool spd_invert(double* A, int n) {
+bool spd_invert(double* A, int n, int threads = 0) {
   std::vector<double> L(size_t(n) * n, 0.0), U(size_t(n) * n, 0.0);
   for (int j = 0; j < n; ++j) {
     const double* Lj = &L[size_t(j) * n];
@@ -175,8 +176,9 @@ bool spd_invert(double* A, int n) {
       for (int i = 0; i < n; ++i) A[size_t(i) * n + c] = col[size_t(i)];
     }
   };
-  // a few threads: several handles may refresh their coarse spaces at once
-  const int nt = int(std::max(1u, std::min(4u, std::thread::hardware_concurrency())));
+  // a few threads (several handles may refresh their coarse spaces at once),
+  // or the caller's count
+  const int nt = threads > 0 ? threads : int(std::max(1u, std::min(4u, std::thread::hardware_concurrency())));
   const int per = (n + nt - 1) / nt;
   if (nt == 1 || n < 64) {
     columns(0, n);
@@ -1729,6 +1731,80 @@ int krylov_prepare(ufem_ns_handle* h, const ufem_krylov_opts* ko, int batched) {
       if (rc) return rc;
       if (ce != cudaSuccess) return set_error(UFEM_ERR_CUDA, std::string("prepare: ") + cudaGetErrorString(ce));
     }
+  }
+  return UFEM_OK;
+}
+
+int krylov_coupled_coarse_members(ufem_ns_handle* const* hs, const int32_t* active, int n, cudaStream_t s,
+                                  int max_side_2d, int max_side_3d, bool* rebuilt, CoarseView* views) {
+  // (1) every active member's coarse matrix, summed on the device and copied
+  // to its pinned host buffer, all on `s`
+  int rc;
+  for (int m = 0; m < n; ++m) {
+    rebuilt[m] = false;
+    if (!active[m]) continue;
+    ufem_ns_handle* h = hs[m];
+    if (!h->kw) h->kw = new KrylovWork();  // coarse data only: batch members keep their vectors in the batch
+    KrylovWork& kw = *h->kw;
+    if (kw.cp_pending) {  // a lagged inversion from solves of the handle on its own
+      kw.cp_thread.join();
+      kw.cp_pending = false;
+    }
+    const bool stale = kw.cp_bc_version != h->bc_list_version || kw.cp_caps != max_side_2d * 1000 + max_side_3d;
+    rebuilt[m] = stale;
+    if (stale && (rc = coupled_coarse_build(h, max_side_2d, max_side_3d))) return rc;
+    if (kw.nc == 0) continue;
+    const size_t bytes = size_t(kw.nc) * kw.nc * sizeof(double);
+    UFEM_CUDA_TRY(cudaMemsetAsync(kw.acd, 0, bytes, s));
+    if (kw.cp_nseg > 0)
+      coarse_matrix_kernel<<<unsigned((int64_t(kw.cp_nseg) * 32 + 255) / 256), 256, 0, s>>>(
+          kw.cp_nseg, kw.cp_seg, kw.cp_dst, kw.cp_pos, h->d_vals, kw.acd);
+    UFEM_CUDA_TRY(cudaGetLastError());
+    UFEM_CUDA_TRY(cudaMemcpyAsync(kw.h_ac, kw.acd, bytes, cudaMemcpyDeviceToHost, s));
+  }
+  // (2) one synchronisation, (3) the inversions on host threads, one member
+  // per thread at a time (each inversion's arithmetic is the one-handle
+  // refresh's: the same inverse, bitwise), (4) the inverses uploaded
+  UFEM_CUDA_TRY(cudaStreamSynchronize(s));
+  std::vector<int> todo;
+  for (int m = 0; m < n; ++m)
+    if (active[m] && hs[m]->kw->nc > 0) todo.push_back(m);
+  std::vector<char> spd(size_t(n), 0);
+  const size_t hw = std::max(1u, std::thread::hardware_concurrency());
+  const int nt = int(std::max<size_t>(1, std::min(todo.size(), hw)));
+  std::atomic<size_t> next{0};
+  auto work = [&]() {
+    for (size_t q = next++; q < todo.size(); q = next++) {
+      const int m = todo[q];
+      KrylovWork& kw = *hs[m]->kw;
+      spd[size_t(m)] = spd_invert(kw.h_ac, kw.nc, 1) ? 1 : 0;
+    }
+  };
+  if (nt <= 1) {
+    work();
+  } else {
+    std::vector<std::thread> th;
+    for (int t = 0; t < nt; ++t) th.emplace_back(work);
+    for (auto& x : th) x.join();
+  }
+  for (int m = 0; m < n; ++m) {
+    views[m] = CoarseView{};
+    if (!active[m]) continue;
+    KrylovWork& kw = *hs[m]->kw;
+    if (kw.nc == 0) {
+      kw.cp_spd = false;
+    } else {
+      kw.cp_spd = spd[size_t(m)] != 0;
+      if (kw.cp_spd)
+        UFEM_CUDA_TRY(cudaMemcpyAsync(kw.ainv, kw.h_ac, size_t(kw.nc) * kw.nc * sizeof(double),
+                                      cudaMemcpyHostToDevice, s));
+      kw.cp_lag_ready = false;
+    }
+    views[m].nc = kw.cp_spd ? kw.nc : 0;
+    views[m].agg = kw.agg;
+    views[m].agg_ptr = kw.agg_ptr;
+    views[m].agg_rows = kw.agg_rows;
+    views[m].ainv = kw.ainv;
   }
   return UFEM_OK;
 }
