@@ -91,3 +91,25 @@ def test_two_level_rejects_cg():
     with pytest.raises(UfemError):
         ns.solve(method="cg", precond="two_level_coupled")
     ns.close()
+
+
+def test_prepared_first_inverse_changes_no_result():
+    """ufem_ns_prepare_solve on an assembled and conditioned system computes the
+    coarse inverse the first solve would compute (the serving loop does this on
+    its creator threads): three steps with it are bitwise the steps without."""
+    pb = small_problem(3, 8)
+    kr = dict(precond="two_level_coupled", tol=1e-12, max_iters=5000)
+    runs = []
+    for prepared in (False, True):
+        ns = NavierStokes(pb.coords, pb.conn, dt=pb.dt, use_specializations=False)
+        ns.set_state(pb.up, pb.lin, pb.nu)
+        ns.add_dirichlet(pb.bc_nodes, pb.bc_comps, pb.bc_values)
+        if prepared:
+            ns.assemble()
+            ns.apply_dirichlet()
+            ns.prepare_solve(**kr)
+        its = [ns.execute(**kr)["iterations"] for _ in range(3)]
+        runs.append((ns.state()[0], its))
+        ns.close()
+    assert np.array_equal(runs[0][0], runs[1][0])
+    assert runs[0][1] == runs[1][1]
