@@ -306,9 +306,15 @@ class Server:
                     items = list(graveyard)
                     graveyard.clear()
                 for obj, reserved in items:
-                    obj.close()
-                    if reserved is not None:
-                        self._release(reserved)
+                    try:
+                        obj.close()
+                    except Exception as e:  # surfaced to the caller; the budget is released all the same
+                        with self._lock:
+                            self.errors.append(e)
+                            self._lock.notify_all()
+                    finally:
+                        if reserved is not None:
+                            self._release(reserved)
 
         reaper = threading.Thread(target=reclaimer, daemon=True)
         reaper.start()
@@ -429,6 +435,7 @@ class Server:
                 drop_batch()
 
         def create(req: Request, est: int, admitted: float):
+            ns = None
             try:
                 large = self._is_large(req.dim, req.coords.shape[0] * (req.dim + 1))
                 ns = _new_handle(req, "fp32" if (large and self.mixed) else self.precision, self.spec)
@@ -445,6 +452,8 @@ class Server:
                 kr = self.krylov_large if large else (self.krylov_mixed if self.mixed_scope == "all" else self.krylov)
                 ns.prepare_solve(batched=not large, **kr)
             except Exception as e:  # the request is rejected; the others go on
+                if ns is not None:
+                    ns.close()
                 self._release(est)
                 with self._lock:
                     results.append(Result(req.rid, None, arrival=req.arrival, admitted=admitted, finished=now(),
