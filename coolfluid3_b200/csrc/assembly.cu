@@ -773,14 +773,17 @@ static_assert(warp_stage_bytes<2, float>() % 16 == 0 && warp_stage_bytes<2, doub
                   warp_stage_bytes<3, float, 32, true>() % 16 == 0 && warp_stage_bytes<3, double, 32, true>() % 16 == 0,
               "per-warp staging slices must stay 16-byte aligned");
 
-// Resident-CTA hints (register budgets) of the 24-lane tetrahedron variants,
-// matched to the warps their smaller staging lets an SM hold: FP64 16 warps
-// (<= 128 registers), FP32 20 warps (<= 102).  The 32-lane variants keep the
-// compiler's choice (their staging caps the warps anyway).
+// Resident-CTA hints (register budgets) of the 24-lane tetrahedron variants:
+// FP32 20 warps (<= 102 registers); FP64 14 warps, which with 4-warp CTAs asks
+// for 3 CTAs (12 warps, no register cap: the variant's smaller staging then
+// leaves more of the SM's shared/L1 array to the node-data gathers than the
+// 32-lane kernel at the same warps) and with 2-warp CTAs for 7 (a 128-register
+// budget that spills; the autotuner passes it over).  The 32-lane variants keep
+// the compiler's choice (their staging caps the warps anyway).
 template <int D, typename T, int KC, int WPB>
 constexpr int warp_min_blocks() {
   if (D != 3 || KC == 32) return 0;  // 0: no hint
-  const int warps = sizeof(T) == 8 ? 16 : 20;
+  const int warps = sizeof(T) == 8 ? 14 : 20;
   return warps / WPB > 0 ? warps / WPB : 1;
 }
 
