@@ -73,6 +73,8 @@ def parse():
                     help="log-uniform element-count range of the served 2D requests (point-Jacobi BiCGStab, the "
                          "plain path's solver, stalls on larger 2D lid-driven meshes at dt = 0.01)")
     ap.add_argument("--serve-steps", type=int, default=10, help="time steps per served request")
+    ap.add_argument("--serve-nu", type=float, nargs=2, default=[1e-4, 1e-1],
+                    help="log-uniform viscosity range of the served requests")
     ap.add_argument("--serve-budget-gb", type=float, default=60.0, help="HBM budget of the server (GB)")
     ap.add_argument("--serve-reps", type=int, default=3, help="served runs per form (the median is reported)")
     ap.add_argument("--serve-sweep", type=float, nargs="*", default=[10.0, 50.0, 200.0, 500.0],
@@ -828,7 +830,7 @@ def serving_compare(args):
     from coolfluid3_b200 import serving as S
     t0 = time.perf_counter()
     elems = {2: tuple(args.serve_elems_2d), 3: tuple(args.serve_elems_3d)}
-    reqs = S.poisson_workload(args.serve_requests, rate=args.serve_rate, elems=elems, nu=(1e-4, 1e-2),
+    reqs = S.poisson_workload(args.serve_requests, rate=args.serve_rate, elems=elems, nu=tuple(args.serve_nu),
                               nsteps=args.serve_steps, seed=20261203)
     gen_s = time.perf_counter() - t0
     tol = 1e-12  # both sides at the residual that keeps the state within 1e-6 of the FP64 oracle
@@ -841,7 +843,7 @@ def serving_compare(args):
     forms = (("served_fp64", False, "two_level_coupled"), ("served_mixed", True, "two_level_coupled"))
     # untimed warm-up of every form on a few of the requests (first launches of
     # each kernel, graph captures, host thread pools, pinned buffers)
-    warm = S.poisson_workload(6, rate=args.serve_rate, elems=elems, nu=(1e-4, 1e-2), nsteps=2, seed=20261202)
+    warm = S.poisson_workload(6, rate=args.serve_rate, elems=elems, nu=tuple(args.serve_nu), nsteps=2, seed=20261202)
     S.run_plain(warm, krylov=dict(tol=tol, max_iters=20000), realtime=False)
     S.run_plain(warm, krylov=dict(tol=tol, max_iters=20000, precond="two_level_coupled"), realtime=False)
     for _, mixed, lpre in forms:
@@ -860,7 +862,8 @@ def serving_compare(args):
         "workload": (f"{len(reqs)} lid-driven requests, Poisson arrivals {args.serve_rate}/s, 3D tets with "
                      f"{elems[3][0]:.0e}..{elems[3][1]:.0e} elements and 2D tris with {elems[2][0]:.0e}.."
                      f"{elems[2][1]:.0e} (log-uniform; total {sum(r.nb_elems for r in reqs)}), nu log-uniform "
-                     f"1e-4..1e-2, {args.serve_steps} steps each, relative residual {tol:g}"),
+                     f"{args.serve_nu[0]:g}..{args.serve_nu[1]:g}, {args.serve_steps} steps each, relative residual "
+                     f"{tol:g}"),
         "plain": dict(pick(pst, plain), form="FP64 elements, FP64 BiCGStab + Jacobi, one request at a time"),
         "plain_two_level": dict(pick(pst2, plain2),
                                 form="FP64 elements, FP64 BiCGStab + the coupled two-level preconditioner, one request "
@@ -896,7 +899,7 @@ def serving_compare(args):
     # ---- arrival-rate sweep (one run per form and rate) ----------------------
     sweep = []
     for rate in args.serve_sweep:
-        rq = S.poisson_workload(args.serve_requests, rate=rate, elems=elems, nu=(1e-4, 1e-2),
+        rq = S.poisson_workload(args.serve_requests, rate=rate, elems=elems, nu=tuple(args.serve_nu),
                                 nsteps=args.serve_steps, seed=20261203 + int(rate))
         _, ps = S.run_plain(rq, krylov=dict(tol=tol, max_iters=20000), realtime=True)
         row = {"rate_per_s": rate, "plain": {"steps_per_s": round(ps["steps_per_s"], 2),
