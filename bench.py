@@ -808,6 +808,29 @@ def cfg4_batch(members: int = 256, steps: int = 2, tol: float = 1e-10) -> dict:
     b.close()
     for h in hs:
         h.close()
+    # the configuration's element precision: FP32 element arithmetic with FP64
+    # accumulation into the FP64 values (assembly only: the batched solve has no
+    # matrix-free FP64 refinement, so FP32-element batch solves stop at the
+    # FP32-element system's ~3e-4 error)
+    hs32 = []
+    for pb in probs:
+        ns = NavierStokes(pb.coords, pb.conn, dt=pb.dt, use_specializations=False, precision="fp32")
+        ns.set_state(pb.up, pb.lin, pb.nu)
+        ns.add_dirichlet(pb.bc_nodes, pb.bc_comps, pb.bc_values)
+        hs32.append(ns)
+    b32 = Batch(hs32)
+    tuned32 = b32.tune_assembly(reps=3)
+    ms_batch32 = timed(b32.assemble)
+    ms_one32 = timed(lambda: [h.assemble() for h in hs32])
+    out["assembly_fp32_elements"] = {"batched_ms": round(ms_batch32, 3),
+                                     "batched_melem_s": round(E / ms_batch32 / 1e3, 1),
+                                     "one_by_one_ms": round(ms_one32, 3),
+                                     "one_by_one_melem_s": round(E / ms_one32 / 1e3, 1),
+                                     "speedup": round(ms_one32 / ms_batch32, 2),
+                                     "warps_per_cta": tuned32["warps_per_cta"]}
+    b32.close()
+    for h in hs32:
+        h.close()
     return out
 
 
