@@ -143,3 +143,36 @@ def test_config_shapes():
     np.testing.assert_array_equal(pb.lin[:, :3], pb.up[:, :3])
     np.testing.assert_array_equal(pb.lin[:, 9:], pb.up[:, :3])
     assert np.abs(pb.up[:, :3]).max() <= 1.0
+
+
+def _create_raw(dim, nb_nodes, nb_elems, coords, conn):
+    lib = N.lib()
+    o = N.NSOptions()
+    lib.ufem_ns_default_options(C.byref(o))
+    mesh = N.Mesh(dim, 0, nb_nodes, nb_elems, coords, conn)
+    h = C.c_void_p()
+    rc = lib.ufem_ns_create(C.byref(mesh), C.byref(o), C.byref(h))
+    if rc == 0:
+        lib.ufem_ns_destroy(h)
+    return rc, lib.ufem_last_error().decode()
+
+
+def test_empty_invalid_and_oversized_meshes_are_refused_before_any_device_work():
+    c, e = P.rectangle_tris(2)
+    c = np.ascontiguousarray(c, np.float64)
+    e = np.ascontiguousarray(e, np.uint32)
+    cp, ep = N.dptr(c), N.u32ptr(e)
+    rc, msg = _create_raw(2, c.shape[0], 0, cp, ep)  # no elements
+    assert rc == -1 and "empty" in msg
+    rc, msg = _create_raw(2, 0, e.shape[0], cp, ep)  # no nodes
+    assert rc == -1 and "empty" in msg
+    rc, msg = _create_raw(4, c.shape[0], e.shape[0], cp, ep)  # only Triag2D and Tetra3D
+    assert rc == -1 and "dim" in msg
+    rc, msg = _create_raw(2, c.shape[0], e.shape[0], None, ep)
+    assert rc == -1 and "NULL" in msg
+    # 2^29 tetrahedra: 2^31 incidences overflow the 32-bit incidence and column
+    # indices; refused from the sizes alone (the arrays are not read)
+    t = np.zeros((1, 4), np.uint32)
+    x = np.zeros((4, 3))
+    rc, msg = _create_raw(3, 4, 1 << 29, N.dptr(x), N.u32ptr(t))
+    assert rc == -6 and "32-bit" in msg

@@ -236,3 +236,34 @@ def test_error_paths_do_not_hang():
     ns.assemble()
     st = ns.solve(raise_on_failure=False, tol=1e-10)
     assert st["converged"] == 0 and st["status"] == 3
+
+
+@pytest.mark.parametrize("dim", [2, 3])
+@pytest.mark.parametrize("spec", [False, True])
+def test_single_element_meshes_match_oracle(dim, spec):
+    """The smallest inputs: one triangle and one tetrahedron (every node a row
+    with a single incidence, one warp group holding all rows), assembled with
+    a random state, against the oracle."""
+    rng = np.random.default_rng(7 + dim)
+    coords = np.array([[0.0, 0.0], [1.0, 0.1], [0.2, 0.9]]) if dim == 2 else \
+        np.array([[0.0, 0.0, 0.0], [1.0, 0.1, 0.0], [0.1, 0.9, 0.1], [0.2, 0.1, 1.1]])
+    conn = np.arange(dim + 1, dtype=np.uint32)[None, :]
+    N = dim + 1
+    up = rng.standard_normal((N, dim + 1))
+    lin = np.tile(up[:, :dim], (1, 4)) + 0.1 * rng.standard_normal((N, 4 * dim))
+    nu = np.full(N, 1e-2)
+    ns = NavierStokes(coords, conn, dt=0.01, use_specializations=spec)
+    ns.set_state(up, lin, nu)
+    o = O.Oracle(coords, conn, O.options(dt=0.01, use_specializations=spec))
+    o.set_state(up, lin, nu)
+    rp, ci = ns.csr()
+    orp, oci = o.csr()
+    assert np.array_equal(rp, orp) and np.array_equal(ci, oci)
+    ns.assemble()
+    o.assemble()
+    gv, gr = ns.system()
+    ov, orr = o.system()
+    assert row_scaled_error(gv, ov, orp) <= 1e-11
+    assert vec_rel_error(gr, orr) <= 1e-11
+    ns.close()
+    o.close()
