@@ -865,7 +865,7 @@ def serving_compare(args):
     def server(mixed, lpre):
         return S.Server(int(args.serve_budget_gb * 1e9), precision="fp64", mixed=mixed,
                         krylov=dict(tol=tol, max_iters=20000), realtime=True, large_precond=lpre,
-                        small_precond=lpre, large_rows_2d=40_000)
+                        small_precond=lpre, large_rows_2d=40_000, mixed_scope="elements")
 
     forms = (("served_fp64", False, "two_level_coupled"), ("served_mixed", True, "two_level_coupled"))
     # untimed warm-up of every form on a few of the requests (first launches of
@@ -914,8 +914,9 @@ def serving_compare(args):
                           speedup_vs_plain_two_level=round(st["steps_per_s"] / pst2["steps_per_s"], 3),
                           runs_steps_per_s=[round(r[0], 2) for r in runs],
                           max_rel_diff_vs_plain=max(diffs) if diffs else None,
-                          form=(("large requests: FP32 element matrices, FP32 inner BiCGStab refined against the "
-                                 "matrix-free FP64 residual; batched small requests: FP64 elements, FP64 BiCGStab"
+                          form=(("FP32 element matrices for every request, FP32-operator inner BiCGStab refined "
+                                 "against each request's matrix-free FP64 residual (one handle for the large "
+                                 "requests, batched for the small ones)"
                                  if mixed else "FP64 elements, FP64 BiCGStab")
                                 + "; the coupled two-level preconditioner throughout; continuous batching (small "
                                   "requests batched, large ones concurrent)"))

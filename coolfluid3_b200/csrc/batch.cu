@@ -42,7 +42,7 @@ constexpr int kMaxRestarts = 10;  // BiCGStab restarts after breakdowns in one s
 
 // per-mesh scalar slots (dctl[m * kDc + ...])
 constexpr int sBnorm = 0, sBeta = 1, sEst = 2, sRho = 5, sRhoOld = 6, sAlpha = 7, sOmega = 8, sTrue = 9,
-              sTol = 10, sTS = 11, sTT = 12, sLastTrue = 13;
+              sTol = 10, sTS = 11, sTT = 12, sLastTrue = 13, sRnorm = 14;
 // per-mesh flags (ictl[m * kIc + ...])
 constexpr int fDone = 0, fStatus = 2, fIters = 3, fMaxit = 4, fOuter = 5, fFinal = 6, fRepl = 7, fLastRepl = 8,
               fSkipRepl = 9;
@@ -52,6 +52,14 @@ constexpr int fDone = 0, fStatus = 2, fIters = 3, fMaxit = 4, fOuter = 5, fFinal
 // replacement perturbs the BiCGStab recurrences; on the lid-driven systems a
 // period of 32 cost 1.9x the FP64 iterations, 128 1.57x, 512 1.49x.
 constexpr int kReplaceIters = 512;
+// Matrix-free refinement (mixed = 2): iterations of one FP32-operator inner
+// solve, as the one-handle refinement caps them (FP32 recurrences stagnate
+// near the FP32-attainable accuracy; a fresh FP64 residual does better).
+constexpr int kInnerIterCap = 400;
+// graph slots of the captured iteration blocks: FP64, FP32 operator, and the
+// matrix-free refinement's inner solve (its operands are the batch's own
+// correction and scaled-residual vectors)
+constexpr int kSlotMf = 2;
 
 struct BatchMesh {
   int64_t N, nrows, row_off;  // row_off: first row in the concatenated solver vectors
@@ -753,6 +761,78 @@ __global__ void zero_batch_kernel(const Chunk* __restrict__ chunks, const BatchM
   }
 }
 
+// ---- matrix-free refinement (mixed = 2) --------------------------------------
+// The refinement of the one-handle solve, for every member at once: r = b - M x
+// of each member's FP64 system from the element pass (launch_mf_residual, one
+// launch per member), the members' norms, the FP32-operator inner solve of
+// A32 z = r / ||r|| (batched BiCGStab), x += ||r|| z.  Members outside the pass
+// (converged, stopped or held) carry fOuter.
+
+// chunk partials of r.r and b.b (b: the member's assembled RHS); members outside
+// the pass write zeros
+__global__ void mf_norm_batch_kernel(const Chunk* __restrict__ chunks, const BatchMesh* __restrict__ bm,
+                                     const double* __restrict__ r, double* __restrict__ part, int nchunks,
+                                     const int* __restrict__ ictl) {
+  __shared__ double sm[32];
+  const Chunk c = chunks[blockIdx.x];
+  const BatchMesh& M = bm[c.mesh];
+  double s2 = 0.0, b2 = 0.0;
+  if (!ictl[c.mesh * kIc + fOuter]) {  // uniform per CTA
+    const int64_t off = M.row_off;
+    for (int i = c.lo + threadIdx.x; i < c.hi; i += blockDim.x) {
+      const double ri = r[off + i], bi = M.rhs[i];
+      s2 += ri * ri;
+      b2 += bi * bi;
+    }
+  }
+  s2 = block_sum(s2, sm);
+  b2 = block_sum(b2, sm);
+  if (threadIdx.x == 0) {
+    part[blockIdx.x] = s2;
+    part[nchunks + blockIdx.x] = b2;
+  }
+}
+
+// per member, one warp, chunk order: ||r||, ||b|| and ||r|| / ||b||
+__global__ void mf_fold_batch_kernel(int nmesh, const int* __restrict__ cprefix, const double* __restrict__ part,
+                                     int nchunks, double* __restrict__ dctl) {
+  const int m = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  if (m >= nmesh) return;
+  double rr, bb;
+  fold2(part, nchunks, cprefix[m], cprefix[m + 1], rr, bb);
+  if ((threadIdx.x & 31) != 0) return;
+  const double rn = sqrt(rr), bn = sqrt(bb);
+  dctl[m * kDc + sRnorm] = rn;
+  dctl[m * kDc + sBnorm] = bn;
+  dctl[m * kDc + sTrue] = bn > 0.0 ? rn / bn : (isfinite(rr) ? 0.0 : NAN);
+}
+
+// inner right-hand side r / ||r|| and a zero correction, members in the pass
+__global__ void mf_scale_batch_kernel(const Chunk* __restrict__ chunks, const BatchMesh* __restrict__ bm,
+                                      const double* __restrict__ r, double* __restrict__ bin,
+                                      double* __restrict__ z, const double* __restrict__ dctl,
+                                      const int* __restrict__ ictl) {
+  const Chunk c = chunks[blockIdx.x];
+  if (ictl[c.mesh * kIc + fOuter]) return;
+  const int64_t off = bm[c.mesh].row_off;
+  const double inv = 1.0 / dctl[c.mesh * kDc + sRnorm];
+  for (int i = c.lo + threadIdx.x; i < c.hi; i += blockDim.x) {
+    bin[off + i] = r[off + i] * inv;
+    z[off + i] = 0.0;
+  }
+}
+
+// x += ||r|| z, members in the pass
+__global__ void mf_update_batch_kernel(const Chunk* __restrict__ chunks, const BatchMesh* __restrict__ bm,
+                                       const double* __restrict__ z, const double* __restrict__ dctl,
+                                       const int* __restrict__ ictl) {
+  const Chunk c = chunks[blockIdx.x];
+  if (ictl[c.mesh * kIc + fOuter]) return;
+  const BatchMesh& M = bm[c.mesh];
+  const double sc = dctl[c.mesh * kDc + sRnorm];
+  for (int i = c.lo + threadIdx.x; i < c.hi; i += blockDim.x) M.sol[i] += sc * z[M.row_off + i];
+}
+
 template <typename T>
 int dmal(T** p, size_t n) {
   DeviceLock lk(device_mutex());
@@ -807,10 +887,13 @@ struct ufem_batch {
   int* ictl = nullptr;
   double* h_dctl = nullptr;
   int* h_ictl = nullptr;
-  // captured iteration blocks: [mixed]
-  cudaGraphExec_t block_exec[2] = {nullptr, nullptr};
+  // captured iteration blocks: [FP64, FP32 operator, matrix-free inner solve]
+  cudaGraphExec_t block_exec[3] = {nullptr, nullptr, nullptr};
   cudaStream_t capture_stream = nullptr;
-  int block_pkind[2] = {-1, -1};
+  int block_pkind[3] = {-1, -1, -1};
+  // matrix-free refinement (mixed = 2): the members' FP64 residuals, the inner
+  // solve's right-hand sides (residual / its norm) and corrections
+  double *mfr = nullptr, *mfb = nullptr, *mfz = nullptr;
 };
 
 namespace {
@@ -825,6 +908,7 @@ void batch_free(ufem_batch* b) {
   dfr(b->r); dfr(b->rh); dfr(b->p); dfr(b->v); dfr(b->s); dfr(b->t); dfr(b->ph); dfr(b->sh); dfr(b->dinv);
   dfr(b->w); dfr(b->part); dfr(b->counters); dfr(b->dctl); dfr(b->ictl);
   dfr(b->d_coarse_prefix); dfr(b->cvec); dfr(b->yvec);
+  dfr(b->mfr); dfr(b->mfb); dfr(b->mfz);
   if (b->h_dctl) cudaFreeHost(b->h_dctl);
   if (b->h_ictl) cudaFreeHost(b->h_ictl);
   delete b;
@@ -891,7 +975,7 @@ int batch_refresh(ufem_batch* b) {
   }
   if (cpre[size_t(b->nmesh)] != b->total_c) {  // the coarse kernels' grids change: recapture the iteration graphs
     DeviceLock lk(device_mutex());
-    for (int k = 0; k < 2; ++k)
+    for (int k = 0; k < 3; ++k)
       if (b->block_exec[k]) {
         cudaGraphExecDestroy(b->block_exec[k]);
         b->block_exec[k] = nullptr;
@@ -990,12 +1074,12 @@ int residual_b(ufem_batch* b, double* x, double* bw, bool init_rh, bool skip_don
 // locations; `use_outer`: skip meshes already converged in refinement.
 template <typename MT, int XL, int BL>
 int bicgstab_b(ufem_batch* b, int pkind, double tol, int maxit, bool use_outer, int slot, cudaStream_t st,
-               bool reliable = false) {
+               bool reliable = false, double* xw = nullptr, double* bw = nullptr) {
+  // xw / bw: the solution and RHS when they are batch work vectors (kWork);
+  // for kSol / kRhs they are the members' own arrays and these stay null
   const unsigned nc = unsigned(b->nchunks);
   const unsigned gm = blocks_for(int64_t(b->nmesh) * 32, 256);
   int rc;
-  double* xw = nullptr;  // solution and RHS are the members' own arrays (kSol, kRhs)
-  double* bw = nullptr;
   // every mesh takes part in the set-up (flags are reset by the init kernel)
   if (use_outer)  // flags prepared by the caller in the host mirror: fOuter set, the rest zero
     UFEM_CUDA_TRY(cudaMemcpyAsync(b->ictl, b->h_ictl, sizeof(int) * kIc * b->nmesh, cudaMemcpyHostToDevice, st));
@@ -1093,6 +1177,118 @@ int true_residual_b(ufem_batch* b, cudaStream_t st) {
   true_res_batch_kernel<<<blocks_for(int64_t(b->nmesh) * 32, 256), 256, 0, st>>>(b->nmesh, b->d_cprefix, b->part,
                                                                                  b->nchunks, b->dctl);
   UFEM_CUDA_TRY(cudaGetLastError());
+  return UFEM_OK;
+}
+
+// mixed = 2: FP32-operator inner solves refined against each member's FP64
+// residual from the element pass (the one-handle refinement of krylov.cu, for
+// every member at once).  The pass count and every member's arithmetic depend
+// only on that member's own residuals, so a member's result is the same alone
+// and in any batch.
+int batch_mf_solve(ufem_batch* b, const ufem_krylov_opts& o, ufem_krylov_status* statuses, cudaStream_t st) {
+  const int n = b->nmesh;
+  const unsigned nc = unsigned(b->nchunks);
+  const unsigned gm = blocks_for(int64_t(n) * 32, 256);
+  const size_t R = size_t(b->total_rows);
+  int rc;
+  if (!b->mfr && ((rc = dmal(&b->mfr, R)) || (rc = dmal(&b->mfb, R)) || (rc = dmal(&b->mfz, R)))) return rc;
+  std::vector<int64_t> off(size_t(n) + 1, 0);
+  for (int m = 0; m < n; ++m) off[size_t(m) + 1] = off[size_t(m)] + b->members[m]->nrows;
+  std::vector<int> done(n, 0), conv(n, 0), iters(n, 0), refs(n, 0), status(n, 0);
+  std::vector<double> relres(n, NAN);
+  for (int m = 0; m < n; ++m)
+    if (!b->active[m]) done[m] = 1;  // held: nothing to solve
+  auto put_outer = [&]() -> int {
+    for (int m = 0; m < n; ++m) {
+      for (int q = 0; q < kIc; ++q) b->h_ictl[m * kIc + q] = 0;
+      b->h_ictl[m * kIc + fOuter] = done[m];
+    }
+    UFEM_CUDA_TRY(cudaMemcpyAsync(b->ictl, b->h_ictl, sizeof(int) * kIc * n, cudaMemcpyHostToDevice, st));
+    return UFEM_OK;
+  };
+  const int inner_iters = std::min(o.max_iters, kInnerIterCap);
+  for (int ref = 0; ref <= o.max_refine; ++ref) {
+    // FP64 residuals of the members still refining, then their norms
+    for (int m = 0; m < n; ++m)
+      if (!done[m] && (rc = launch_mf_residual(b->members[m], b->w + off[size_t(m)], b->mfr + off[size_t(m)], st)))
+        return rc;
+    if ((rc = put_outer())) return rc;
+    mf_norm_batch_kernel<<<nc, kThreads, 0, st>>>(b->d_chunks, b->d_mesh, b->mfr, b->part, b->nchunks, b->ictl);
+    mf_fold_batch_kernel<<<gm, 256, 0, st>>>(n, b->d_cprefix, b->part, b->nchunks, b->dctl);
+    UFEM_CUDA_TRY(cudaGetLastError());
+    UFEM_CUDA_TRY(cudaMemcpyAsync(b->h_dctl, b->dctl, sizeof(double) * kDc * n, cudaMemcpyDeviceToHost, st));
+    UFEM_CUDA_TRY(cudaStreamSynchronize(st));
+    bool any = false;
+    for (int m = 0; m < n; ++m) {
+      if (done[m]) continue;
+      const double rr = b->h_dctl[m * kDc + sTrue], bn = b->h_dctl[m * kDc + sBnorm];
+      if (!std::isfinite(rr)) {
+        status[m] = 3;
+        done[m] = 1;
+        continue;
+      }
+      relres[m] = rr;
+      if (bn == 0.0) {  // zero right-hand side: the increment is zero
+        UFEM_CUDA_TRY(cudaMemsetAsync(b->members[m]->d_sol, 0, size_t(b->members[m]->nrows) * 8, st));
+        relres[m] = 0.0;
+        conv[m] = 1;
+        done[m] = 1;
+        continue;
+      }
+      if (rr <= o.tol) {
+        conv[m] = 1;
+        done[m] = 1;
+        continue;
+      }
+      if (ref == o.max_refine || iters[m] >= o.max_iters * (o.max_refine + 1)) {
+        status[m] = 1;
+        done[m] = 1;
+        continue;
+      }
+      any = true;
+    }
+    if (!any) break;
+    // inner: A32 z = r / ||r|| for the members in this pass, then x += ||r|| z
+    if ((rc = put_outer())) return rc;
+    mf_scale_batch_kernel<<<nc, kThreads, 0, st>>>(b->d_chunks, b->d_mesh, b->mfr, b->mfb, b->mfz, b->dctl, b->ictl);
+    UFEM_CUDA_TRY(cudaGetLastError());
+    if ((rc = bicgstab_b<float, kWork, kWork>(b, o.precond, o.inner_tol, inner_iters, true, kSlotMf, st, false,
+                                              b->mfz, b->mfb)))
+      return rc;
+    UFEM_CUDA_TRY(cudaMemcpyAsync(b->h_ictl, b->ictl, sizeof(int) * kIc * n, cudaMemcpyDeviceToHost, st));
+    UFEM_CUDA_TRY(cudaStreamSynchronize(st));
+    for (int m = 0; m < n; ++m) {
+      if (done[m]) continue;
+      iters[m] += b->h_ictl[m * kIc + fIters];
+      ++refs[m];
+      // a breakdown leaves a finite partial correction, applied; a non-finite
+      // inner iterate is never applied
+      if (b->h_ictl[m * kIc + fStatus] == 3) {
+        status[m] = 3;
+        relres[m] = NAN;
+        done[m] = 1;
+      }
+    }
+    if ((rc = put_outer())) return rc;
+    mf_update_batch_kernel<<<nc, kThreads, 0, st>>>(b->d_chunks, b->d_mesh, b->mfz, b->dctl, b->ictl);
+    UFEM_CUDA_TRY(cudaGetLastError());
+  }
+  UFEM_CUDA_TRY(cudaStreamSynchronize(st));
+  if (statuses) {
+    for (int m = 0; m < n; ++m) {
+      ufem_krylov_status& sm = statuses[m];
+      sm = ufem_krylov_status{};
+      if (!b->active[m]) {  // held: nothing was solved
+        sm.converged = 1;
+        continue;
+      }
+      sm.iterations = iters[m];
+      sm.refinements = refs[m];
+      sm.rel_residual = relres[m];
+      sm.converged = conv[m];
+      sm.status = conv[m] ? 0 : (status[m] ? status[m] : 1);
+    }
+  }
   return UFEM_OK;
 }
 
@@ -1313,8 +1509,7 @@ int ufem_batch_solve(ufem_batch* b, const ufem_krylov_opts* kopts, ufem_krylov_s
   if (o.tol <= 0) o.tol = 1e-10;
   if (o.max_refine <= 0) o.max_refine = 20;
   if (o.inner_tol <= 0) o.inner_tol = 1e-3;
-  if (o.mixed < 0 || o.mixed > 1)
-    return set_error(UFEM_ERR_ARG, "batches refine with the FP64 residual of the stored system: mixed must be 0 or 1");
+  if (o.mixed < 0 || o.mixed > 2) return set_error(UFEM_ERR_ARG, "mixed must be 0, 1 or 2");
   const bool mixed = o.mixed != 0;
   cudaStream_t st = static_cast<cudaStream_t>(stream);
   int rc;
@@ -1358,6 +1553,7 @@ int ufem_batch_solve(ufem_batch* b, const ufem_krylov_opts* kopts, ufem_krylov_s
     UFEM_CUDA_TRY(cudaStreamSynchronize(st));
     if ((rc = batch_refresh(b))) return rc;
   }
+  if (o.mixed == 2) return batch_mf_solve(b, o, statuses, st);
   std::vector<int> iters(b->nmesh, 0), status(b->nmesh, 0), refines(b->nmesh, 0);  // refines: FP64 replacements
   // Plain: FP64 operator.  Mixed: FP32 copy of the operator in the
   // iterations, FP64 vectors, dot products and residual replacement.

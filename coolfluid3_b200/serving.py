@@ -183,20 +183,22 @@ class Server:
     def __init__(self, hbm_budget_bytes: int, max_slots: int = 64, precision: str = "fp64", mixed: bool = True,
                  krylov: dict | None = None, graphs: bool = True, creators: int | None = None,
                  use_specializations: bool = False, realtime: bool = True, large_rows: int = 200_000,
-                 large_workers: int = 2, small_priority: bool = True, mixed_scope: str = "large",
+                 large_workers: int = 2, small_priority: bool = True, mixed_scope: str = "elements",
                  large_precond: str = "jacobi", large_rows_2d: int | None = None, small_precond: str = "jacobi"):
         """mixed: the mixed-precision form.  Requests of at least `large_rows`
         rows (stepped one at a time by the large workers; their solves are
         bandwidth-bound) assemble FP32 element matrices and solve with FP32
         inner BiCGStab refined against the matrix-free FP64 residual, so their
-        answers are the FP64 system's.  The batched small requests, whose
-        iterations are latency-bound, keep FP64 elements and the FP64 operator
-        with mixed_scope "large"; with "all" they iterate with an FP32 copy of
-        the operator and FP64 residual replacement.  large_precond: the
+        answers are the FP64 system's.  With mixed_scope "elements" (default)
+        the batched small requests also assemble FP32 element matrices and every
+        member is refined against its own matrix-free FP64 residual (the
+        batched form of the large requests' solve); with "large" they keep FP64
+        elements and the FP64 operator; with "all" FP64 elements and an FP32
+        copy of the operator with FP64 residual replacement.  large_precond: the
         preconditioner of the large requests' one-handle solves ("jacobi" or
         "two_level_coupled"), small_precond that of the batched solves."""
-        if mixed_scope not in ("large", "all"):
-            raise ValueError("mixed_scope must be 'large' or 'all'")
+        if mixed_scope not in ("large", "all", "elements"):
+            raise ValueError("mixed_scope must be 'large', 'all' or 'elements'")
         if precision not in ("fp32", "fp64"):
             raise ValueError("precision must be fp32 or fp64")
         self.budget = int(hbm_budget_bytes)
@@ -218,7 +220,12 @@ class Server:
         self.krylov = dict(method="bicgstab", precond=small_precond, tol=1e-10, max_iters=3000)
         self.krylov.update(krylov or {})
         self.mixed = bool(mixed)
-        self.krylov_mixed = dict(self.krylov, mixed=True, inner_tol=1e-6, max_refine=20) if mixed else self.krylov
+        if not mixed:
+            self.krylov_mixed = self.krylov
+        elif mixed_scope == "elements":
+            self.krylov_mixed = dict(self.krylov, mixed="matrix_free", inner_tol=1e-5, max_refine=30)
+        else:
+            self.krylov_mixed = dict(self.krylov, mixed=True, inner_tol=1e-6, max_refine=20)
         # large requests of the mixed form: FP32 element matrices, FP32 inner
         # solves refined against the matrix-free FP64 residual
         self.krylov_large = (dict(self.krylov, mixed="matrix_free", inner_tol=1e-5, max_refine=30) if mixed
@@ -407,7 +414,7 @@ class Server:
                     for a in active:
                         if a.done_steps == 0 and a.result.started == 0.0:
                             a.result.started = ts - t0
-                    kr = self.krylov_mixed if self.mixed_scope == "all" else self.krylov
+                    kr = self.krylov_mixed if self.mixed_scope != "large" else self.krylov
                     sts = batch.step(stream, **kr)
                     stream.synchronize()
                     ms = (time.perf_counter() - ts) * 1e3
@@ -438,7 +445,8 @@ class Server:
             ns = None
             try:
                 large = self._is_large(req.dim, req.coords.shape[0] * (req.dim + 1))
-                ns = _new_handle(req, "fp32" if (large and self.mixed) else self.precision, self.spec)
+                fp32_elements = self.mixed and (large or self.mixed_scope == "elements")
+                ns = _new_handle(req, "fp32" if fp32_elements else self.precision, self.spec)
                 # the one-time work of the first step on this host thread, not on
                 # the worker that steps the request: the Dirichlet plan (built by
                 # the first conditioning of an assembled system), the solver
@@ -449,7 +457,7 @@ class Server:
                 ns.assemble(s)
                 ns.apply_dirichlet(s)
                 s.synchronize()
-                kr = self.krylov_large if large else (self.krylov_mixed if self.mixed_scope == "all" else self.krylov)
+                kr = self.krylov_large if large else (self.krylov_mixed if self.mixed_scope != "large" else self.krylov)
                 ns.prepare_solve(batched=not large, **kr)
             except Exception as e:  # the request is rejected; the others go on
                 if ns is not None:

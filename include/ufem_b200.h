@@ -387,7 +387,11 @@ int ufem_batch_assemble(ufem_batch* b, void* stream);
 /* statuses: one per member, or NULL.  BiCGStab (method 1) with precond 0, 1 or
  * 4 (the coupled two-level preconditioner, each member with its own coarse
  * space on at most 16 x 16 (2D) or 5^3 (3D) aggregates, coarse matrices
- * refreshed at every solve); mixed 0 or 1. */
+ * refreshed at every solve).  mixed 0: FP64 operator; 1: FP32 copy of the
+ * operator with FP64 residual replacement; 2: FP32-operator inner solves refined
+ * against each member's matrix-free FP64 residual (as ufem_ns_solve with mixed 2:
+ * for members with FP32 element matrices, whose answers are then the FP64
+ * systems'; members without periodic links; inner_tol and max_refine apply). */
 int ufem_batch_solve(ufem_batch* b, const ufem_krylov_opts* kopts, ufem_krylov_status* statuses, void* stream);
 int ufem_batch_update(ufem_batch* b, void* stream);
 int ufem_batch_step(ufem_batch* b, const ufem_krylov_opts* kopts, ufem_krylov_status* statuses, void* stream);

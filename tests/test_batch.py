@@ -197,3 +197,29 @@ def test_batched_two_level_preconditioner():
     assert sum(s["iterations"] for s in s2[0]) * 2 <= sum(s["iterations"] for s in sj[0])
     mixed3, sts3 = run_batch([specs[3]], 2, tol=1e-12, max_iters=6000, precond="two_level_coupled")
     assert all(s["converged"] for step in sts3 for s in step)
+
+
+@pytest.mark.parametrize("specs", [SIZES_2D, SIZES_3D])
+def test_matrix_free_batched_solve_fp32_elements(specs):
+    """FP32 element matrices, each member refined against its own matrix-free
+    FP64 residual (mixed = "matrix_free", the one-handle refinement for the
+    whole batch): every member reaches the 1e-12 FP64 residual, lands within
+    1e-6 of the FP64 oracle after two steps, and is bitwise the same alone and
+    in the mix."""
+    from .util import oracle_for
+    kr = dict(tol=1e-12, mixed="matrix_free", inner_tol=1e-5, max_iters=3000)
+    mixed, sts = run_batch(specs, 2, precision="fp32", **kr)
+    for k, s in enumerate(specs):
+        assert sts[-1][k]["converged"] and sts[-1][k]["rel_residual"] <= 1e-12, sts[-1][k]
+        assert sts[-1][k]["refinements"] >= 1
+        alone, _ = run_batch([s], 2, precision="fp32", **kr)
+        assert np.array_equal(alone[0], mixed[k]), s
+        pb = P.make_problem(s[0], s[1], nu=1e-2, dt=0.01, seed=s[2])
+        o = oracle_for(pb, use_specializations=False)
+        for _ in range(2):
+            o.assemble()
+            o.apply_dirichlet()
+            assert o.solve(tol=1e-13)["rc"] == 0
+            o.update()
+        assert vec_rel_error(mixed[k], o.state()[0]) <= 1e-6, s
+        o.close()

@@ -133,3 +133,23 @@ def test_large_path_fp32_elements_with_fp64_answers():
     for req in reqs[:3]:
         alone, _ = S.Server(8 * GB, **kw).run([req])
         assert np.array_equal(alone[0].state, served[req.rid].state), req.rid
+
+
+def test_fp32_elements_on_every_request_meet_the_fp64_oracle():
+    """mixed_scope="elements": the batched small requests also assemble FP32
+    element matrices and each member is refined against its own matrix-free
+    FP64 residual (the large requests' solve, batched).  Every served state is
+    within 1e-6 of the FP64 oracle at a 1e-12 residual, and bitwise the same
+    served alone and in the mix."""
+    reqs = workload(n=6, seed=9)
+    srv = S.Server(8 * GB, precision="fp64", mixed=True, realtime=False, mixed_scope="elements",
+                   krylov=dict(tol=1e-12))
+    served, _ = srv.run(reqs)
+    assert srv.max_batch >= 2
+    for a, req in zip(served, reqs):
+        assert a.ok, a.statuses
+        assert vec_rel_error(a.state, oracle_state(req)) <= 1e-6, a.rid
+    for req in reqs[:3]:
+        alone, _ = S.Server(8 * GB, precision="fp64", mixed=True, realtime=False, mixed_scope="elements",
+                            krylov=dict(tol=1e-12)).run([req])
+        assert np.array_equal(alone[0].state, served[req.rid].state), req.rid
