@@ -868,7 +868,7 @@ int ufem_ns_device_bytes(const ufem_ns_handle* h, int64_t* bytes) {
   if (h->d_force) b += N * 32;
   if (h->d_vals32) b += Z * 4;
   if (h->d_node32) b += N * 32;
-  if (h->kw) b += R * 8 * 13;  // Krylov vectors once a solve has run
+  b += krylov_device_bytes(h);  // solver workspace allocated so far (none for a batch member's vectors)
   if (h->pipe.buf[0]) b += 2 * (N * (h->neq + 4 * h->dim + 1) + R) * 8;  // overlapped-transfer buffers, once used
   if (h->d_tie) b += h->ntie * 8;
   b += h->bcp.nbc * 40 + h->bcp.nfix_rows * 16 + h->bcp.nfix * 12;

@@ -282,6 +282,9 @@ constexpr int kBatchCoarseSide2D = 16, kBatchCoarseSide3D = 5;
 // ahead of the first solve (batched: for a batch member).
 int krylov_prepare(ufem_ns_handle* h, const ufem_krylov_opts* ko, int batched);
 void krylov_free(ufem_ns_handle* h);
+// Device bytes the handle's solver workspace holds (vectors allocated so far,
+// coarse-space data); 0 without one.
+int64_t krylov_device_bytes(const ufem_ns_handle* h);
 // Aggregates of the two-level CG preconditioner (precond 3) of a one-equation
 // system: agg[row] in [0, nc) or -1; builds and inverts the Galerkin coarse
 // matrix from the system's current values.  If that matrix is not positive

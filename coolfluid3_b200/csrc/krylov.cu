@@ -2066,6 +2066,23 @@ int krylov_apply(ufem_ns_handle* h, const double* d_x, double* d_y, cudaStream_t
   return spmv<double, double>(h, h->d_vals, d_x, d_y, nullptr, s);
 }
 
+int64_t krylov_device_bytes(const ufem_ns_handle* h) {
+  if (!h->kw) return 0;
+  const KrylovWork& k = *h->kw;
+  const int64_t R = h->nrows;
+  int64_t b = 0;
+  for (const double* p : {k.w, k.z, k.t, k.r, k.dinv, k.bp, k.bv, k.bs, k.bt, k.brh, k.bph, k.bsh})
+    if (p) b += R * 8;
+  for (const float* p : {k.w32, k.z32, k.t32, k.r32, k.x32, k.q32, k.dinv32})
+    if (p) b += R * 4;
+  if (k.V) b += int64_t(k.m + 1) * R * 8;    // GMRES basis
+  if (k.V32) b += int64_t(k.m + 1) * R * 4;
+  if (k.agg) b += R * 4 * 2;                // aggregate of each row, members of each aggregate
+  if (k.ainv) b += int64_t(k.nc) * k.nc * 8 * 2;  // coarse inverse and coarse matrix
+  if (k.cp_pos) b += int64_t(k.cp_nseg) * 12 + R * 8;  // coarse-matrix segments (an upper bound)
+  return b;
+}
+
 void krylov_free(ufem_ns_handle* h) {
   if (!h->kw) return;
   KrylovWork& k = *h->kw;

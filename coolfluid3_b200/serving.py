@@ -104,7 +104,9 @@ def estimate_bytes(req: Request, precision: str = "fp64") -> int:
     nnz = bnnz * neq * neq
     rows = n_nodes * neq
     per_value = 16  # FP64 values, column indices, FP32 operator copy
-    return n_nodes * 256 + n_elems * 40 + bnnz * 4 + nnz * per_value + rows * 8 * 16
+    # node records (FP64 state, history, u_adv, coordinates, and the FP32 mirror
+    # of FP32 element arithmetic), incidences, graph, values, solver vectors
+    return n_nodes * 288 + n_elems * 40 + bnnz * 4 + nnz * per_value + rows * 8 * 16
 
 
 def make_request(rid: int, dim: int, n_elems: float, nu: float, seed: int, nsteps: int = 10,
