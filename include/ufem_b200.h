@@ -158,7 +158,9 @@ int ufem_ns_create_periodic(const ufem_mesh* mesh, const ufem_ns_options* opts, 
                             const uint32_t* masters, int64_t nlinks, ufem_ns_handle** out);
 /* NavierStokes option triggers (trigger_assembly, NavierStokes.cpp:130-192). */
 int ufem_ns_set_options(ufem_ns_handle* h, const ufem_ns_options* opts);
-/* Device memory held by the handle (bytes, approximate to a few percent). */
+/* Device memory held by the handle (bytes, approximate to a few percent): its
+ * mesh, graph, system and field arrays, and the solver workspace allocated so
+ * far (none for the vectors of a batch member, which live in its batch). */
 int ufem_ns_device_bytes(const ufem_ns_handle* h, int64_t* bytes);
 int ufem_ns_sizes(const ufem_ns_handle* h, int64_t* nb_rows, int64_t* nnz, int64_t* block_nnz);
 /* Host copies of the CSR pattern (rowptr nb_rows+1, colidx nnz). */
