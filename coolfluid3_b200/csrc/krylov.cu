@@ -523,15 +523,9 @@ __global__ void bicg_p_kernel(int64_t n, int pkind, const VT* __restrict__ dinv,
   }
 }
 
-// alpha = rho / (rh . v) from the block partials of rh . v.
-__global__ void bicg_alpha_kernel(int nblk, const double* __restrict__ part, double* __restrict__ dctl,
-                                  int* __restrict__ ictl, double alpha_max) {
-  if (ictl[0]) return;
-  __shared__ double sm[32];
-  double sv = 0.0;
-  for (int b = threadIdx.x; b < nblk; b += blockDim.x) sv += part[b];
-  const double d = block_sum(sv, sm);
-  if (threadIdx.x != 0) return;
+// alpha = rho / (rh . v), given d = rh . v (one thread).
+__device__ __forceinline__ void bicg_alpha_update(double d, double* __restrict__ dctl, int* __restrict__ ictl,
+                                                  double alpha_max) {
   dctl[kRhV] = d;
   if (d == 0.0 || !isfinite(d)) {
     ictl[0] = 1;
@@ -545,6 +539,18 @@ __global__ void bicg_alpha_kernel(int nblk, const double* __restrict__ part, dou
     return;
   }
   dctl[kAlpha] = a;
+}
+
+// alpha from the block partials of rh . v (a fixed-order fold).
+__global__ void bicg_alpha_kernel(int nblk, const double* __restrict__ part, double* __restrict__ dctl,
+                                  int* __restrict__ ictl, double alpha_max) {
+  if (ictl[0]) return;
+  __shared__ double sm[32];
+  double sv = 0.0;
+  for (int b = threadIdx.x; b < nblk; b += blockDim.x) sv += part[b];
+  const double d = block_sum(sv, sm);
+  if (threadIdx.x != 0) return;
+  bicg_alpha_update(d, dctl, ictl, alpha_max);
 }
 
 // s = r - alpha v ; sh = M^-1 s
@@ -581,18 +587,9 @@ __global__ void dot2_partials_kernel(int64_t n, const VT* __restrict__ t, const 
   }
 }
 
-__global__ void bicg_omega_kernel(int nblk, const double* __restrict__ part, double* __restrict__ dctl,
-                                  int* __restrict__ ictl) {
-  if (ictl[0]) return;
-  __shared__ double sm[32];
-  double a = 0.0, b = 0.0;
-  for (int k = threadIdx.x; k < nblk; k += blockDim.x) {
-    a += part[k];
-    b += part[nblk + k];
-  }
-  const double ts = block_sum(a, sm);
-  const double tt = block_sum(b, sm);
-  if (threadIdx.x != 0) return;
+// omega = (t . s) / (t . t) (one thread).
+__device__ __forceinline__ void bicg_omega_update(double ts, double tt, double* __restrict__ dctl,
+                                                  int* __restrict__ ictl) {
   const double om = (tt != 0.0) ? ts / tt : 0.0;
   dctl[kTS] = ts;
   dctl[kTT] = tt;
@@ -605,6 +602,21 @@ __global__ void bicg_omega_kernel(int nblk, const double* __restrict__ part, dou
     // x is still advanced by alpha*ph in bicg_xr_kernel before stopping
     ictl[2] = 2;
   }
+}
+
+__global__ void bicg_omega_kernel(int nblk, const double* __restrict__ part, double* __restrict__ dctl,
+                                  int* __restrict__ ictl) {
+  if (ictl[0]) return;
+  __shared__ double sm[32];
+  double a = 0.0, b = 0.0;
+  for (int k = threadIdx.x; k < nblk; k += blockDim.x) {
+    a += part[k];
+    b += part[nblk + k];
+  }
+  const double ts = block_sum(a, sm);
+  const double tt = block_sum(b, sm);
+  if (threadIdx.x != 0) return;
+  bicg_omega_update(ts, tt, dctl, ictl);
 }
 
 // x += alpha ph + omega sh ; r = s - omega t ; partials of r.r and rh.r
@@ -632,19 +644,9 @@ __global__ void bicg_xr_kernel(int64_t n, const VT* __restrict__ ph, const VT* _
   }
 }
 
-// ||r|| and the next rho = rh . r; convergence and iteration count.
-__global__ void bicg_end_kernel(int nblk, const double* __restrict__ part, double* __restrict__ dctl,
-                                int* __restrict__ ictl, double tol, int maxit) {
-  if (ictl[0]) return;
-  __shared__ double sm[32];
-  double a = 0.0, b = 0.0;
-  for (int k = threadIdx.x; k < nblk; k += blockDim.x) {
-    a += part[k];
-    b += part[nblk + k];
-  }
-  const double nn = block_sum(a, sm);
-  const double rho_new = block_sum(b, sm);
-  if (threadIdx.x != 0) return;
+// ||r|| and the next rho = rh . r; convergence and iteration count (one thread).
+__device__ __forceinline__ void bicg_end_update(double nn, double rho_new, double* __restrict__ dctl,
+                                                int* __restrict__ ictl, double tol, int maxit) {
   const double rn = sqrt(nn);
   dctl[kEst] = rn;
   dctl[kRhoOld] = dctl[kRho];
@@ -664,6 +666,21 @@ __global__ void bicg_end_kernel(int nblk, const double* __restrict__ part, doubl
     ictl[0] = 1;
     ictl[2] = 1;
   }
+}
+
+__global__ void bicg_end_kernel(int nblk, const double* __restrict__ part, double* __restrict__ dctl,
+                                int* __restrict__ ictl, double tol, int maxit) {
+  if (ictl[0]) return;
+  __shared__ double sm[32];
+  double a = 0.0, b = 0.0;
+  for (int k = threadIdx.x; k < nblk; k += blockDim.x) {
+    a += part[k];
+    b += part[nblk + k];
+  }
+  const double nn = block_sum(a, sm);
+  const double rho_new = block_sum(b, sm);
+  if (threadIdx.x != 0) return;
+  bicg_end_update(nn, rho_new, dctl, ictl, tol, maxit);
 }
 
 // rho = ||r0||^2 (rh = r0), rho_old = alpha = omega = 1, converged test.
@@ -805,6 +822,104 @@ __device__ __forceinline__ bool last_block(int* counter, int* s_flag) {
   __threadfence();
   if (threadIdx.x == 0) *counter = 0;  // ready for the next launch
   return true;
+}
+
+// BiCGStab's reductions with their scalar updates folded in: the launch's last
+// block (an atomic ticket, reset by that block; no block waits for another)
+// folds the block partials exactly as the separate single-block kernels do --
+// the same grid, the same 256-thread strided sums and block tree -- so the
+// arithmetic is theirs, bitwise, with one launch fewer per reduction.
+
+// rh . v partials, then alpha
+template <typename VT>
+__global__ void bicg_vdot_fold_kernel(int64_t n, const VT* __restrict__ rh, const VT* __restrict__ v,
+                                      double* __restrict__ part, int* __restrict__ counter,
+                                      double* __restrict__ dctl, int* __restrict__ ictl, double alpha_max) {
+  if (ictl[0]) return;  // read before any block of this launch can change it
+  __shared__ double sm[32];
+  __shared__ int flag;
+  double s = 0.0;
+  GRID_STRIDE(i, n) s += double(rh[i]) * double(v[i]);
+  s = block_sum(s, sm);
+  if (threadIdx.x == 0) part[blockIdx.x] = s;
+  if (!last_block(counter, &flag)) return;
+  double sv = 0.0;
+  for (int b = threadIdx.x; b < int(gridDim.x); b += blockDim.x) sv += __ldcg(part + b);
+  const double d = block_sum(sv, sm);
+  if (threadIdx.x != 0) return;
+  bicg_alpha_update(d, dctl, ictl, alpha_max);
+}
+
+// t . s and t . t partials, then omega
+template <typename VT>
+__global__ void bicg_ts_fold_kernel(int64_t n, const VT* __restrict__ t, const VT* __restrict__ s,
+                                    double* __restrict__ part, int* __restrict__ counter,
+                                    double* __restrict__ dctl, int* __restrict__ ictl) {
+  if (ictl[0]) return;
+  __shared__ double sm[32];
+  __shared__ int flag;
+  double ts = 0.0, tt = 0.0;
+  GRID_STRIDE(i, n) {
+    const double ti = double(t[i]);
+    ts += ti * double(s[i]);
+    tt += ti * ti;
+  }
+  ts = block_sum(ts, sm);
+  tt = block_sum(tt, sm);
+  if (threadIdx.x == 0) {
+    part[blockIdx.x] = ts;
+    part[gridDim.x + blockIdx.x] = tt;
+  }
+  if (!last_block(counter, &flag)) return;
+  const int nb = int(gridDim.x);
+  double a = 0.0, b = 0.0;
+  for (int k = threadIdx.x; k < nb; k += blockDim.x) {
+    a += __ldcg(part + k);
+    b += __ldcg(part + nb + k);
+  }
+  const double fts = block_sum(a, sm);
+  const double ftt = block_sum(b, sm);
+  if (threadIdx.x != 0) return;
+  bicg_omega_update(fts, ftt, dctl, ictl);
+}
+
+// x += alpha ph + omega sh ; r = s - omega t with the partials of r.r and
+// rh.r, then the convergence test and the next rho
+template <typename VT>
+__global__ void bicg_xr_fold_kernel(int64_t n, const VT* __restrict__ ph, const VT* __restrict__ sh,
+                                    const VT* __restrict__ s, const VT* __restrict__ t, const VT* __restrict__ rh,
+                                    VT* __restrict__ x, VT* __restrict__ r, double* __restrict__ dctl,
+                                    int* __restrict__ ictl, double* __restrict__ part, int* __restrict__ counter,
+                                    double tol, int maxit) {
+  if (ictl[0]) return;
+  __shared__ double sm[32];
+  __shared__ int flag;
+  const double al = dctl[kAlpha], om = dctl[kOmega];
+  double rr = 0.0, hr = 0.0;
+  GRID_STRIDE(i, n) {
+    x[i] = VT(double(x[i]) + al * double(ph[i]) + om * double(sh[i]));
+    const VT ri = VT(double(s[i]) - om * double(t[i]));
+    r[i] = ri;
+    rr += double(ri) * double(ri);
+    hr += double(rh[i]) * double(ri);
+  }
+  rr = block_sum(rr, sm);
+  hr = block_sum(hr, sm);
+  if (threadIdx.x == 0) {
+    part[blockIdx.x] = rr;
+    part[gridDim.x + blockIdx.x] = hr;
+  }
+  if (!last_block(counter, &flag)) return;
+  const int nb = int(gridDim.x);
+  double a = 0.0, b = 0.0;
+  for (int k = threadIdx.x; k < nb; k += blockDim.x) {
+    a += __ldcg(part + k);
+    b += __ldcg(part + nb + k);
+  }
+  const double nn = block_sum(a, sm);
+  const double rho_new = block_sum(b, sm);
+  if (threadIdx.x != 0) return;
+  bicg_end_update(nn, rho_new, dctl, ictl, tol, maxit);
 }
 
 // Last block of a CG iteration: ||r|| and rho_new = r.z from the block partials
@@ -1250,6 +1365,10 @@ int bicgstab(ufem_ns_handle* h, KrylovWork& kw, const MT* vals, const BT* b, VT*
   bicg_init_kernel<<<1, 1, 0, st>>>(kw.dctl, kw.ictl, tol);
   UFEM_CUDA_TRY(cudaGetLastError());
   const double alpha_max = std::is_same<VT, float>::value ? 1e20 : 1e150;
+  // the reductions with their scalar updates folded in (three launches fewer an
+  // iteration), where the workspace has the fold counter (not the
+  // allocation-free solve's)
+  const bool fused = kw.cg_counter != nullptr;
   auto iteration = [&](cudaStream_t s2) -> int {
     int irc;
     const int pk = pkind == 4 ? 1 : pkind;  // the two-level form: point Jacobi plus the coarse correction
@@ -1257,16 +1376,27 @@ int bicgstab(ufem_ns_handle* h, KrylovWork& kw, const MT* vals, const BT* b, VT*
     if (pkind == 2 && (irc = precond<VT>(h, pkind, dinv, p, ph, kw.ictl, s2))) return irc;
     if (pkind == 4 && (irc = coarse_correct<VT>(h, p, ph, kw.ictl, s2))) return irc;
     if ((irc = spmv<VT, MT>(h, vals, ph, v, kw.ictl, s2))) return irc;
-    dot_partials_kernel<VT><<<dim3(g1, 1), kRedThreads, 0, s2>>>(n, rh, n, v, kw.part, kw.ictl);
-    bicg_alpha_kernel<<<1, 256, 0, s2>>>(nblk, kw.part, kw.dctl, kw.ictl, alpha_max);
+    if (fused) {
+      bicg_vdot_fold_kernel<VT><<<g1, kRedThreads, 0, s2>>>(n, rh, v, kw.part, kw.cg_counter, kw.dctl, kw.ictl,
+                                                           alpha_max);
+    } else {
+      dot_partials_kernel<VT><<<dim3(g1, 1), kRedThreads, 0, s2>>>(n, rh, n, v, kw.part, kw.ictl);
+      bicg_alpha_kernel<<<1, 256, 0, s2>>>(nblk, kw.part, kw.dctl, kw.ictl, alpha_max);
+    }
     bicg_s_kernel<VT><<<g1, kRedThreads, 0, s2>>>(n, pk, dinv, r, v, sv, sh, kw.dctl, kw.ictl);
     if (pkind == 2 && (irc = precond<VT>(h, pkind, dinv, sv, sh, kw.ictl, s2))) return irc;
     if (pkind == 4 && (irc = coarse_correct<VT>(h, sv, sh, kw.ictl, s2))) return irc;
     if ((irc = spmv<VT, MT>(h, vals, sh, tv, kw.ictl, s2))) return irc;
-    dot2_partials_kernel<VT><<<g1, kRedThreads, 0, s2>>>(n, tv, sv, kw.part, kw.ictl);
-    bicg_omega_kernel<<<1, 256, 0, s2>>>(nblk, kw.part, kw.dctl, kw.ictl);
-    bicg_xr_kernel<VT><<<g1, kRedThreads, 0, s2>>>(n, ph, sh, sv, tv, rh, x, r, kw.dctl, kw.ictl, kw.part);
-    bicg_end_kernel<<<1, 256, 0, s2>>>(nblk, kw.part, kw.dctl, kw.ictl, tol, maxit);
+    if (fused) {
+      bicg_ts_fold_kernel<VT><<<g1, kRedThreads, 0, s2>>>(n, tv, sv, kw.part, kw.cg_counter, kw.dctl, kw.ictl);
+      bicg_xr_fold_kernel<VT><<<g1, kRedThreads, 0, s2>>>(n, ph, sh, sv, tv, rh, x, r, kw.dctl, kw.ictl, kw.part,
+                                                         kw.cg_counter, tol, maxit);
+    } else {
+      dot2_partials_kernel<VT><<<g1, kRedThreads, 0, s2>>>(n, tv, sv, kw.part, kw.ictl);
+      bicg_omega_kernel<<<1, 256, 0, s2>>>(nblk, kw.part, kw.dctl, kw.ictl);
+      bicg_xr_kernel<VT><<<g1, kRedThreads, 0, s2>>>(n, ph, sh, sv, tv, rh, x, r, kw.dctl, kw.ictl, kw.part);
+      bicg_end_kernel<<<1, 256, 0, s2>>>(nblk, kw.part, kw.dctl, kw.ictl, tol, maxit);
+    }
     UFEM_CUDA_TRY(cudaGetLastError());
     return UFEM_OK;
   };
