@@ -133,63 +133,130 @@ __device__ __forceinline__ double block_sum(double v, double* sm) {
   return s;
 }
 
-// In-place inverse of an SPD matrix (row-major, n x n) through its Cholesky
-// factor: L row by row (contiguous inner products), then each column of A^-1
-// by forward and back substitution with L and L^T (stored transposed, so every
-// inner loop runs over contiguous memory).  The columns are independent and are
-// split over host threads; each column's arithmetic is the same whatever the
-// split.  False if a pivot is not positive (a coarse matrix of a system without
-// conditions that fix its constant mode is singular).
+// Runs fn(lo, hi) on nt threads over [n0, n) cut into ranges of equal work
+// (cost(u): the work of unit u); each unit's arithmetic is the same whatever
+// the cut.
+template <typename F, typename C>
+void parallel_ranges(int nt, int n0, int n, C&& cost, F&& fn) {
+  if (nt <= 1 || n - n0 < 2) {
+    fn(n0, n);
+    return;
+  }
+  double total = 0.0;
+  for (int u = n0; u < n; ++u) total += cost(u);
+  std::vector<std::thread> th;
+  int lo = n0;
+  double acc = 0.0;
+  for (int t = 0; t < nt && lo < n; ++t) {
+    int hi = lo;
+    const double goal = total * (t + 1) / nt;
+    while (hi < n && (t + 1 == nt || acc + 0.5 * cost(hi) < goal)) acc += cost(hi++);
+    if (hi == lo) continue;
+    if (hi == n) fn(lo, hi);  // the last range on the calling thread
+    else th.emplace_back(fn, lo, hi);
+    lo = hi;
+  }
+  for (auto& x : th) x.join();
+}
+
+// In-place inverse of an SPD matrix (row-major, n x n): A = L L^T, X = L^-1,
+// A^-1 = X^T X (the LAPACK potrf / trtri / lauum sequence, n^3 / 2
+// multiply-adds), every inner loop a contiguous multiply-add over rows that
+// stay in cache (the Cholesky in panels of 32 columns, L^-1 in groups of 8
+// columns, the product in groups of 8 rows).  From n = 256 the three phases
+// are split over `threads` host threads (default: up to 4, since several
+// handles may refresh their coarse spaces at once), in ranges of equal work;
+// every element's arithmetic is the same whatever the split.  False if a pivot
+// is not positive (a coarse matrix of a system without conditions that fix its
+// constant mode is singular).
 bool spd_invert(double* A, int n, int threads = 0) {
-  std::vector<double> L(size_t(n) * n, 0.0), U(size_t(n) * n, 0.0);
-  for (int j = 0; j < n; ++j) {
-    const double* Lj = &L[size_t(j) * n];
-    double d = A[size_t(j) * n + j];
-    for (int k = 0; k < j; ++k) d -= Lj[k] * Lj[k];
-    if (!(d > 0.0) || !std::isfinite(d)) return false;
-    const double ljj = std::sqrt(d);
-    L[size_t(j) * n + j] = ljj;
-    for (int i = j + 1; i < n; ++i) {
-      const double* Li = &L[size_t(i) * n];
-      double s = A[size_t(i) * n + j];
-      for (int k = 0; k < j; ++k) s -= Li[k] * Lj[k];
-      L[size_t(i) * n + j] = s / ljj;
-    }
-  }
-  for (int i = 0; i < n; ++i)
-    for (int k = 0; k <= i; ++k) U[size_t(k) * n + i] = L[size_t(i) * n + k];  // U = L^T
-  auto columns = [&](int c0, int c1) {
-    std::vector<double> col(static_cast<size_t>(n));
-    for (int c = c0; c < c1; ++c) {  // L L^T x = e_c
-      for (int i = 0; i < n; ++i) {
-        const double* Li = &L[size_t(i) * n];
-        double s = (i == c) ? 1.0 : 0.0;
-        for (int k = 0; k < i; ++k) s -= Li[k] * col[size_t(k)];
-        col[size_t(i)] = s / Li[i];
+  const int nt = n < 256 ? 1
+                         : (threads > 0 ? threads
+                                        : int(std::max(1u, std::min(4u, std::thread::hardware_concurrency()))));
+  // Cholesky A = L L^T, right-looking in panels of kPanel columns: every
+  // element receives its updates L[i][k] L[j][k] in ascending k (the order of
+  // the column-by-column algorithm).  The panel is factored in a contiguous
+  // copy P (row i: its kPanel columns); Lt row k holds column k of L.
+  constexpr int kPanel = 32;
+  std::vector<double> W(A, A + size_t(n) * n), Lt(size_t(n) * n, 0.0), P(size_t(n) * kPanel);
+  for (int p0 = 0; p0 < n; p0 += kPanel) {
+    const int p1 = std::min(n, p0 + kPanel), b = p1 - p0;
+    for (int i = p0; i < n; ++i)
+      for (int q = 0; q < b; ++q) P[size_t(i) * kPanel + q] = W[size_t(i) * n + p0 + q];
+    for (int k = p0; k < p1; ++k) {
+      const int kq = k - p0;
+      const double d = P[size_t(k) * kPanel + kq];
+      if (!(d > 0.0) || !std::isfinite(d)) return false;
+      const double lkk = std::sqrt(d);
+      P[size_t(k) * kPanel + kq] = lkk;
+      for (int i = k + 1; i < n; ++i) P[size_t(i) * kPanel + kq] /= lkk;
+      for (int i = k + 1; i < n; ++i) {  // the panel's remaining columns
+        double* __restrict__ pi = &P[size_t(i) * kPanel];
+        const double lik = pi[kq];
+        const int je = std::min(i, p1 - 1) - p0;
+        for (int j = kq + 1; j <= je; ++j) pi[j] -= lik * P[size_t(p0 + j) * kPanel + kq];
       }
-      for (int i = n - 1; i >= 0; --i) {
-        const double* Ui = &U[size_t(i) * n];
-        double s = col[size_t(i)];
-        for (int k = i + 1; k < n; ++k) s -= Ui[k] * col[size_t(k)];
-        col[size_t(i)] = s / Ui[i];
-      }
-      for (int i = 0; i < n; ++i) A[size_t(i) * n + c] = col[size_t(i)];
     }
-  };
-  // a few threads (several handles may refresh their coarse spaces at once),
-  // or the caller's count
-  const int nt = threads > 0 ? threads : int(std::max(1u, std::min(4u, std::thread::hardware_concurrency())));
-  const int per = (n + nt - 1) / nt;
-  if (nt == 1 || n < 64) {
-    columns(0, n);
-  } else {
-    std::vector<std::thread> th;
-    for (int t = 0; t < nt; ++t) {
-      const int c0 = t * per, c1 = std::min(n, c0 + per);
-      if (c0 < c1) th.emplace_back(columns, c0, c1);
-    }
-    for (auto& x : th) x.join();
+    for (int q = 0; q < b; ++q)
+      for (int i = p0 + q; i < n; ++i) Lt[size_t(p0 + q) * n + i] = P[size_t(i) * kPanel + q];
+    if (p1 < n)  // the trailing rows and columns: the panel's rank-b update
+      parallel_ranges(nt, p1, n, [p1](int i) { return double(i - p1 + 1); }, [&, p0, p1](int r0, int r1) {
+        for (int i = r0; i < r1; ++i) {
+          double* __restrict__ wi = &W[size_t(i) * n];
+          for (int k = p0; k < p1; ++k) {
+            const double* __restrict__ lk = &Lt[size_t(k) * n];
+            const double lik = lk[i];
+            for (int j = p1; j <= i; ++j) wi[j] -= lik * lk[j];
+          }
+        }
+      });
   }
+  // X = L^-1 by forward substitution, kCols columns at a time (X^T rows of
+  // kCols values: every L column is read once per group of columns).
+  constexpr int kCols = 8;
+  std::vector<double> X(size_t(n) * n, 0.0);  // X[i][c]
+  parallel_ranges(nt, 0, (n + kCols - 1) / kCols,
+                  [n](int g) { const double r = n - g * kCols; return r * r; },
+                  [&](int g0, int g1) {
+    std::vector<double> x(size_t(n) * kCols);
+    for (int g = g0; g < g1; ++g) {
+      const int c0 = g * kCols, w = std::min(kCols, n - c0);
+      std::fill(x.begin(), x.end(), 0.0);
+      for (int q = 0; q < w; ++q) x[size_t(c0 + q) * kCols + q] = 1.0;
+      for (int k = c0; k < n; ++k) {  // row k of x is final once columns < k of L are applied
+        const double* __restrict__ lk = &Lt[size_t(k) * n];
+        double v[kCols];
+        for (int q = 0; q < kCols; ++q) v[q] = x[size_t(k) * kCols + q] / lk[k];
+        for (int q = 0; q < kCols; ++q) x[size_t(k) * kCols + q] = v[q];
+        for (int i = k + 1; i < n; ++i) {
+          const double lik = lk[i];
+          double* __restrict__ xi = &x[size_t(i) * kCols];
+          for (int q = 0; q < kCols; ++q) xi[q] -= lik * v[q];
+        }
+      }
+      for (int i = c0; i < n; ++i)
+        for (int q = 0; q < w; ++q) X[size_t(i) * n + c0 + q] = x[size_t(i) * kCols + q];
+    }
+  });
+  // A^-1 = X^T X: row i = sum over k >= i of X[k][i] X[k][0..k], kRows rows at
+  // a time (each X row is read once per group of rows).
+  constexpr int kRows = 8;
+  parallel_ranges(nt, 0, (n + kRows - 1) / kRows,
+                  [n](int g) { const double r0 = g * kRows; return double(n) * n - r0 * r0; },
+                  [&](int g0, int g1) {
+    for (int g = g0; g < g1; ++g) {
+      const int i0 = g * kRows, h = std::min(kRows, n - i0);
+      for (int r = 0; r < h; ++r) std::fill(A + size_t(i0 + r) * n, A + size_t(i0 + r + 1) * n, 0.0);
+      for (int k = i0; k < n; ++k) {
+        const double* __restrict__ xk = &X[size_t(k) * n];
+        for (int r = 0; r < h && i0 + r <= k; ++r) {
+          const double xki = xk[i0 + r];
+          double* __restrict__ ai = A + size_t(i0 + r) * n;
+          for (int j = 0; j <= k; ++j) ai[j] += xki * xk[j];
+        }
+      }
+    }
+  });
   return true;
 }
 
