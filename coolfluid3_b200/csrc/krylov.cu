@@ -163,8 +163,8 @@ void parallel_ranges(int nt, int n0, int n, C&& cost, F&& fn) {
 // A^-1 = X^T X (the LAPACK potrf / trtri / lauum sequence, n^3 / 2
 // multiply-adds), every inner loop a contiguous multiply-add over rows that
 // stay in cache (the Cholesky in panels of 32 columns, L^-1 in groups of 8
-// columns, the product in groups of 8 rows).  From n = 256 the three phases
-// are split over `threads` host threads (default: up to 4, since several
+// columns, the product in groups of 8 rows).  From n = 256 the last two
+// phases are split over `threads` host threads (default: up to 4, since several
 // handles may refresh their coarse spaces at once), in ranges of equal work;
 // every element's arithmetic is the same whatever the split.  False if a pivot
 // is not positive (a coarse matrix of a system without conditions that fix its
@@ -199,8 +199,9 @@ bool spd_invert(double* A, int n, int threads = 0) {
     }
     for (int q = 0; q < b; ++q)
       for (int i = p0 + q; i < n; ++i) Lt[size_t(p0 + q) * n + i] = P[size_t(i) * kPanel + q];
-    if (p1 < n)  // the trailing rows and columns: the panel's rank-b update
-      parallel_ranges(nt, p1, n, [p1](int i) { return double(i - p1 + 1); }, [&, p0, p1](int r0, int r1) {
+    if (p1 < n)  // the trailing rows and columns: the panel's rank-b update, on this thread (a
+                 // fork per panel costs more than it saves beside a serving loop's threads)
+      parallel_ranges(1, p1, n, [p1](int i) { return double(i - p1 + 1); }, [&, p0, p1](int r0, int r1) {
         for (int i = r0; i < r1; ++i) {
           double* __restrict__ wi = &W[size_t(i) * n];
           for (int k = p0; k < p1; ++k) {
