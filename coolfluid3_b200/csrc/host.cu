@@ -29,21 +29,52 @@ int set_error(int code, const std::string& msg) {
 }
 
 namespace {
+// Helper threads the library's host loops may run at once, over all callers:
+// one less than the machine's hardware threads, shared, so that handles built
+// or coarse spaces inverted concurrently (a serving loop's creator and worker
+// threads) do not each start a thread per core beside the threads that drive
+// the GPU.  -1 until first use.
+std::atomic<int> g_spare_threads{-1};
+}  // namespace
 
+int acquire_spare_threads(int want) {
+  int unset = -1;
+  g_spare_threads.compare_exchange_strong(
+      unset, int(std::max<unsigned>(1u, std::thread::hardware_concurrency())) - 1);
+  int cur = g_spare_threads.load();
+  while (want > 0 && cur > 0) {
+    const int take = std::min(want, cur);
+    if (g_spare_threads.compare_exchange_weak(cur, cur - take)) return take;
+  }
+  return 0;
+}
+
+void release_spare_threads(int n) {
+  if (n > 0) g_spare_threads.fetch_add(n);
+}
+
+namespace {
+
+// f(a, b) over [0, n) in contiguous ranges, on the calling thread and as many
+// spare helper threads as the loop can use (one per 8192 items); every range
+// writes its own outputs, so results do not depend on the split.
 template <typename F>
 void parallel_for(int64_t n, F&& f) {
-  const int64_t hw = std::max<unsigned>(1u, std::thread::hardware_concurrency());
-  const int64_t nt = std::max<int64_t>(1, std::min<int64_t>(hw, (n + 8191) / 8192));
+  const int hw = int(std::max<unsigned>(1u, std::thread::hardware_concurrency()));
+  const int got = acquire_spare_threads(int(std::max<int64_t>(0, std::min<int64_t>(hw, (n + 8191) / 8192) - 1)));
+  const int64_t nt = 1 + got;
   if (nt <= 1) {
     f(int64_t(0), n);
     return;
   }
   std::vector<std::thread> th;
-  for (int64_t t = 0; t < nt; ++t) {
+  for (int64_t t = 1; t < nt; ++t) {
     const int64_t a = n * t / nt, b = n * (t + 1) / nt;
     th.emplace_back([&f, a, b] { f(a, b); });
   }
+  f(int64_t(0), n / nt);  // the first range on the calling thread
   for (auto& x : th) x.join();
+  release_spare_threads(got);
 }
 
 inline uint64_t mix64(uint64_t z) {

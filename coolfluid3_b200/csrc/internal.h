@@ -16,6 +16,11 @@ namespace ufem {
 // Error reporting across the C ABI: a thread-local message plus a code.
 // ---------------------------------------------------------------------------
 int set_error(int code, const std::string& msg);
+// Host helper threads (see host.cu): takes up to `want` of the process-wide
+// spare threads (possibly none) and gives them back; the caller's own thread
+// is never counted.
+int acquire_spare_threads(int want);
+void release_spare_threads(int n);
 
 // Serialises device-lifecycle calls (allocation, free, device-wide
 // synchronisation) with CUDA-graph capture: a capture in one host thread must

@@ -138,7 +138,9 @@ __device__ __forceinline__ double block_sum(double v, double* sm) {
 // the cut.
 template <typename F, typename C>
 void parallel_ranges(int nt, int n0, int n, C&& cost, F&& fn) {
-  if (nt <= 1 || n - n0 < 2) {
+  const int extra = (nt <= 1 || n - n0 < 2) ? 0 : acquire_spare_threads(nt - 1);
+  nt = 1 + extra;
+  if (nt <= 1) {
     fn(n0, n);
     return;
   }
@@ -157,6 +159,7 @@ void parallel_ranges(int nt, int n0, int n, C&& cost, F&& fn) {
     lo = hi;
   }
   for (auto& x : th) x.join();
+  release_spare_threads(extra);
 }
 
 // In-place inverse of an SPD matrix (row-major, n x n): A = L L^T, X = L^-1,
@@ -1968,8 +1971,8 @@ int krylov_coupled_coarse_members(ufem_ns_handle* const* hs, const int32_t* acti
   for (int m = 0; m < n; ++m)
     if (active[m] && hs[m]->kw->nc > 0) todo.push_back(m);
   std::vector<char> spd(size_t(n), 0);
-  const size_t hw = std::max(1u, std::thread::hardware_concurrency());
-  const int nt = int(std::max<size_t>(1, std::min(todo.size(), hw)));
+  const int extra = todo.size() > 1 ? acquire_spare_threads(int(todo.size()) - 1) : 0;
+  const int nt = 1 + extra;
   std::atomic<size_t> next{0};
   auto work = [&]() {
     for (size_t q = next++; q < todo.size(); q = next++) {
@@ -1978,13 +1981,13 @@ int krylov_coupled_coarse_members(ufem_ns_handle* const* hs, const int32_t* acti
       spd[size_t(m)] = spd_invert(kw.h_ac, kw.nc, 1) ? 1 : 0;
     }
   };
-  if (nt <= 1) {
-    work();
-  } else {
+  {
     std::vector<std::thread> th;
-    for (int t = 0; t < nt; ++t) th.emplace_back(work);
+    for (int t = 1; t < nt; ++t) th.emplace_back(work);
+    work();  // the calling thread takes members too
     for (auto& x : th) x.join();
   }
+  release_spare_threads(extra);
   for (int m = 0; m < n; ++m) {
     views[m] = CoarseView{};
     if (!active[m]) continue;
