@@ -109,6 +109,14 @@ namespace {
 constexpr int kBnorm = 0, kBeta = 1, kEst = 2, kHnext = 3, kTrue = 4;
 constexpr int kRho = 5, kRhoOld = 6, kAlpha = 7, kOmega = 8, kRhV = 9, kTS = 10, kTT = 11, kR2 = 12, kScale = 13;
 constexpr int kRedThreads = 256;
+// Blocks of the vector kernels and their reductions for n rows: one per 1024
+// rows, at most 4 a B200 SM (enough loads in flight to stream the vectors).
+// The allocating and the allocation-free solves use the same count, so their
+// reductions add in the same order.
+constexpr int kRedBlocksMax = 4 * 148;
+inline int red_blocks(int64_t n) {
+  return int(std::min<int64_t>(kRedBlocksMax, std::max<int64_t>(1, (n + 1023) / 1024)));
+}
 constexpr int kInnerIterCap = 400;  // iterations of one FP32 inner solve of the mixed path
 constexpr int kMaxRestarts = 10;    // BiCGStab restarts after breakdowns in one solve
 constexpr int kCGMaxBlocks = 8 * 148;  // blocks of the fused CG kernels
@@ -1216,7 +1224,7 @@ int ensure_work(ufem_ns_handle* h, int m, bool need32, bool bicg) {
   }
   kw.m = std::max(kw.m, m);
   kw.n = n;
-  kw.nblk = int(std::min<int64_t>(296, std::max<int64_t>(1, (n + 2047) / 2048)));
+  kw.nblk = red_blocks(n);
   kw.cg_nblk = int(std::min<int64_t>(kCGMaxBlocks, std::max<int64_t>(1, (n + 511) / 512)));
   const int M = kw.m;
   const size_t nd = size_t(n);
@@ -2318,7 +2326,7 @@ void krylov_free(ufem_ns_handle* h) {
 // integer flags.
 // ---------------------------------------------------------------------------
 constexpr int64_t kNoAllocRows = UFEM_NOALLOC_MAX_ROWS;
-constexpr int kMaxPartials = 296;  // the largest block count ensure_work chooses
+constexpr int kMaxPartials = kRedBlocksMax;  // the largest block count red_blocks gives
 constexpr int64_t kNoAllocDoubles = 9 * kNoAllocRows + 2 * kMaxPartials + 16 + 8;
 
 static __device__ __align__(256) double g_noalloc_scratch[kNoAllocDoubles];
@@ -2376,7 +2384,7 @@ extern "C" int ufem_ns_solve_noalloc(ufem_ns_handle* h, const ufem_krylov_opts* 
   KrylovWork kw;  // a view of the fixed scratch; owns nothing
   kw.use_graph = false;  // graph instantiation would allocate
   kw.n = n;
-  kw.nblk = int(std::min<int64_t>(kMaxPartials, std::max<int64_t>(1, (n + 2047) / 2048)));
+  kw.nblk = red_blocks(n);
   double* vec[9];
   for (int k = 0; k < 9; ++k) vec[k] = base + k * kNoAllocRows;
   kw.part = base + 9 * kNoAllocRows;
