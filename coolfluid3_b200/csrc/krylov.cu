@@ -1108,31 +1108,35 @@ __global__ void cg_xr_plain_kernel(int64_t n, const VT* __restrict__ p, const VT
   if (threadIdx.x == 0) part[blockIdx.x] = rr;
 }
 
-// c[I] = sum of r over the rows of aggregate I (ascending), one warp per aggregate.
+// Threads of the restriction and coarse-product blocks.
+constexpr int kCoarseThreads = 128;
+
+// c[I] = sum of r over the rows of aggregate I, one block per aggregate (a fixed
+// thread partition and block tree: deterministic).
 template <typename VT>
-__global__ void restrict_kernel(int nc, const int32_t* __restrict__ agg_ptr, const int32_t* __restrict__ agg_rows,
-                                const VT* __restrict__ r, double* __restrict__ c, const int* __restrict__ done) {
+__global__ void __launch_bounds__(kCoarseThreads)
+    restrict_kernel(int nc, const int32_t* __restrict__ agg_ptr, const int32_t* __restrict__ agg_rows,
+                    const VT* __restrict__ r, double* __restrict__ c, const int* __restrict__ done) {
   if (done && *done) return;
-  const int I = int((int64_t(blockIdx.x) * blockDim.x + threadIdx.x) >> 5);
-  const int lane = threadIdx.x & 31;
-  if (I >= nc) return;  // whole warps: blockDim is a multiple of 32
+  __shared__ double sm[32];
+  const int I = blockIdx.x;
   double s = 0.0;
-  for (int k = agg_ptr[I] + lane; k < agg_ptr[I + 1]; k += 32) s += double(r[agg_rows[k]]);
-  s = warp_sum(s);
-  if (lane == 0) c[I] = s;
+  for (int k = agg_ptr[I] + threadIdx.x; k < agg_ptr[I + 1]; k += blockDim.x) s += double(r[agg_rows[k]]);
+  s = block_sum(s, sm);
+  if (threadIdx.x == 0) c[I] = s;
 }
 
-// y = Ac^-1 c, one warp per row.
-__global__ void coarse_kernel(int nc, const double* __restrict__ ainv, const double* __restrict__ c,
-                              double* __restrict__ y, const int* __restrict__ done) {
+// y = Ac^-1 c, one block per coarse row.
+__global__ void __launch_bounds__(kCoarseThreads)
+    coarse_kernel(int nc, const double* __restrict__ ainv, const double* __restrict__ c, double* __restrict__ y,
+                  const int* __restrict__ done) {
   if (done && *done) return;
-  const int I = int((int64_t(blockIdx.x) * blockDim.x + threadIdx.x) >> 5);
-  const int lane = threadIdx.x & 31;
-  if (I >= nc) return;
+  __shared__ double sm[32];
+  const int I = blockIdx.x;
   double s = 0.0;
-  for (int J = lane; J < nc; J += 32) s += ainv[int64_t(I) * nc + J] * c[J];
-  s = warp_sum(s);
-  if (lane == 0) y[I] = s;
+  for (int J = threadIdx.x; J < nc; J += blockDim.x) s += ainv[int64_t(I) * nc + J] * c[J];
+  s = block_sum(s, sm);
+  if (threadIdx.x == 0) y[I] = s;
 }
 
 // z = D^-1 r + y[agg]
@@ -1304,9 +1308,8 @@ int setup_precond(ufem_ns_handle* h, int kind, const MT* vals, VT* dinv, cudaStr
 template <typename VT>
 int coarse_correct(ufem_ns_handle* h, const VT* v, VT* z, const int* done, cudaStream_t s) {
   KrylovWork& kw = *h->kw;
-  const unsigned gw = unsigned((int64_t(kw.nc) * 32 + 255) / 256);
-  restrict_kernel<VT><<<gw, 256, 0, s>>>(kw.nc, kw.agg_ptr, kw.agg_rows, v, kw.cvec, done);
-  coarse_kernel<<<gw, 256, 0, s>>>(kw.nc, kw.ainv, kw.cvec, kw.yvec, done);
+  restrict_kernel<VT><<<unsigned(kw.nc), kCoarseThreads, 0, s>>>(kw.nc, kw.agg_ptr, kw.agg_rows, v, kw.cvec, done);
+  coarse_kernel<<<unsigned(kw.nc), kCoarseThreads, 0, s>>>(kw.nc, kw.ainv, kw.cvec, kw.yvec, done);
   prolong_add_kernel<VT><<<unsigned(kw.nblk), kRedThreads, 0, s>>>(h->nrows, kw.agg, kw.yvec, z, done);
   UFEM_CUDA_TRY(cudaGetLastError());
   return UFEM_OK;
@@ -1570,13 +1573,13 @@ int cg_iteration(ufem_ns_handle* h, KrylovWork& kw, const MT* vals, VT* x, VT* r
   int rc;
   if (pkind == 3) {
     const unsigned gc = unsigned(kw.cg_nblk);
-    const unsigned gw = unsigned((int64_t(kw.nc) * 32 + 255) / 256);
+    const unsigned gw = unsigned(kw.nc);  // one block per aggregate / coarse row
     cg_p_kernel<VT><<<gc, kRedThreads, 0, st>>>(n, z, p, kw.dctl, kw.ictl);
     if ((rc = spmv<VT, MT>(h, vals, p, q, kw.ictl, st))) return rc;
     cg_pq_fold_kernel<VT><<<gc, kRedThreads, 0, st>>>(n, p, q, kw.part, kw.cg_counter, kw.dctl, kw.ictl);
     cg_xr_plain_kernel<VT><<<gc, kRedThreads, 0, st>>>(n, p, q, x, r, kw.part, kw.dctl, kw.ictl);
-    restrict_kernel<VT><<<gw, 256, 0, st>>>(kw.nc, kw.agg_ptr, kw.agg_rows, r, kw.cvec, kw.ictl);
-    coarse_kernel<<<gw, 256, 0, st>>>(kw.nc, kw.ainv, kw.cvec, kw.yvec, kw.ictl);
+    restrict_kernel<VT><<<gw, kCoarseThreads, 0, st>>>(kw.nc, kw.agg_ptr, kw.agg_rows, r, kw.cvec, kw.ictl);
+    coarse_kernel<<<gw, kCoarseThreads, 0, st>>>(kw.nc, kw.ainv, kw.cvec, kw.yvec, kw.ictl);
     cg_prolong_fold_kernel<VT><<<gc, kRedThreads, 0, st>>>(n, dinv, kw.agg, kw.yvec, r, z, kw.part, kw.cg_counter,
                                                           kw.dctl, kw.ictl, tol, maxit);
     UFEM_CUDA_TRY(cudaGetLastError());
@@ -1628,9 +1631,9 @@ int cg(ufem_ns_handle* h, KrylovWork& kw, const MT* vals, const BT* b, VT* x, VT
   finalize_norm_kernel<<<1, 1, 0, st>>>(nblk, kw.part, kw.dctl, kBeta, 1);
   finalize_norm_kernel<<<1, 1, 0, st>>>(nblk, kw.part + nblk, kw.dctl, kBnorm, 1);
   if (pkind == 3) {
-    const unsigned gw = unsigned((int64_t(kw.nc) * 32 + 255) / 256);
-    restrict_kernel<VT><<<gw, 256, 0, st>>>(kw.nc, kw.agg_ptr, kw.agg_rows, r, kw.cvec, nullptr);
-    coarse_kernel<<<gw, 256, 0, st>>>(kw.nc, kw.ainv, kw.cvec, kw.yvec, nullptr);
+    const unsigned gw = unsigned(kw.nc);  // one block per aggregate / coarse row
+    restrict_kernel<VT><<<gw, kCoarseThreads, 0, st>>>(kw.nc, kw.agg_ptr, kw.agg_rows, r, kw.cvec, nullptr);
+    coarse_kernel<<<gw, kCoarseThreads, 0, st>>>(kw.nc, kw.ainv, kw.cvec, kw.yvec, nullptr);
     prolong_kernel<VT><<<g1, kRedThreads, 0, st>>>(n, dinv, kw.agg, kw.yvec, r, z);
     UFEM_CUDA_TRY(cudaGetLastError());
   } else if ((rc = precond<VT>(h, pkind, dinv, r, z, nullptr, st))) {
