@@ -576,15 +576,19 @@ __global__ void fill_kernel(int64_t n, VT v, VT* __restrict__ x) {
 // dctl[idx] = (sqrt) sum of nblk partials
 __global__ void finalize_norm_kernel(int nblk, const double* __restrict__ part, double* __restrict__ dctl, int idx,
                                      int take_sqrt) {
+  __shared__ double sm[32];
   double s = 0.0;
-  for (int b = 0; b < nblk; ++b) s += part[b];
-  dctl[idx] = take_sqrt ? sqrt(s) : s;
+  for (int b = threadIdx.x; b < nblk; b += blockDim.x) s += part[b];
+  s = block_sum(s, sm);
+  if (threadIdx.x == 0) dctl[idx] = take_sqrt ? sqrt(s) : s;
 }
 
 // ---- BiCGStab kernels ---------------------------------------------------------
 // Scalars in dctl: rho (= rh.r of the current residual), rho_old, alpha, omega.
-// Each single-block "reduce" kernel folds the block partials in a fixed order
-// and computes the next scalar, so an iteration is ten launches.
+// Each reduction's last block folds the block partials in a fixed order and
+// computes the next scalar (the single-block "reduce" kernels do the same where
+// the workspace has no fold counter), so an iteration is seven launches, and
+// thirteen with the two-level preconditioner's coarse correction.
 
 // p = r + beta (p - omega v), beta = (rho/rho_old)(alpha/omega); ph = M^-1 p
 // (point Jacobi or identity inline; block Jacobi applied by precond_kernel).
@@ -1338,7 +1342,7 @@ int true_residual(ufem_ns_handle* h, KrylovWork& kw, const MT* vals, const BT* b
   int rc;
   if ((rc = spmv<VT, MT>(h, vals, x, w, nullptr, s))) return rc;
   residual_kernel<VT, BT><<<unsigned(kw.nblk), kRedThreads, 0, s>>>(h->nrows, b, w, r, kw.part, nullptr);
-  finalize_norm_kernel<<<1, 1, 0, s>>>(kw.nblk, kw.part, kw.dctl, kTrue, 1);
+  finalize_norm_kernel<<<1, kRedThreads, 0, s>>>(kw.nblk, kw.part, kw.dctl, kTrue, 1);
   UFEM_CUDA_TRY(cudaMemcpyAsync(kw.h_dctl, kw.dctl, 16 * sizeof(double), cudaMemcpyDeviceToHost, s));
   UFEM_CUDA_TRY(cudaStreamSynchronize(s));
   // a zero RHS has the zero solution; a non-finite ||b|| never counts as converged
@@ -1439,8 +1443,8 @@ int bicgstab(ufem_ns_handle* h, KrylovWork& kw, const MT* vals, const BT* b, VT*
   res = SolveResult();
   if ((rc = spmv<VT, MT>(h, vals, x, v, nullptr, st))) return rc;
   residual_kernel<VT, BT><<<g1, kRedThreads, 0, st>>>(n, b, v, r, kw.part, kw.part + nblk);
-  finalize_norm_kernel<<<1, 1, 0, st>>>(nblk, kw.part, kw.dctl, kBeta, 1);
-  finalize_norm_kernel<<<1, 1, 0, st>>>(nblk, kw.part + nblk, kw.dctl, kBnorm, 1);
+  finalize_norm_kernel<<<1, kRedThreads, 0, st>>>(nblk, kw.part, kw.dctl, kBeta, 1);
+  finalize_norm_kernel<<<1, kRedThreads, 0, st>>>(nblk, kw.part + nblk, kw.dctl, kBnorm, 1);
   UFEM_CUDA_TRY(cudaMemcpyAsync(rh, r, n * sizeof(VT), cudaMemcpyDeviceToDevice, st));
   fill_kernel<VT><<<g1, kRedThreads, 0, st>>>(n, VT(0), p);
   fill_kernel<VT><<<g1, kRedThreads, 0, st>>>(n, VT(0), v);
@@ -1628,8 +1632,8 @@ int cg(ufem_ns_handle* h, KrylovWork& kw, const MT* vals, const BT* b, VT* x, VT
   res = SolveResult();
   if ((rc = spmv<VT, MT>(h, vals, x, q, nullptr, st))) return rc;
   residual_kernel<VT, BT><<<g1, kRedThreads, 0, st>>>(n, b, q, r, kw.part, kw.part + nblk);
-  finalize_norm_kernel<<<1, 1, 0, st>>>(nblk, kw.part, kw.dctl, kBeta, 1);
-  finalize_norm_kernel<<<1, 1, 0, st>>>(nblk, kw.part + nblk, kw.dctl, kBnorm, 1);
+  finalize_norm_kernel<<<1, kRedThreads, 0, st>>>(nblk, kw.part, kw.dctl, kBeta, 1);
+  finalize_norm_kernel<<<1, kRedThreads, 0, st>>>(nblk, kw.part + nblk, kw.dctl, kBnorm, 1);
   if (pkind == 3) {
     const unsigned gw = unsigned(kw.nc);  // one block per aggregate / coarse row
     restrict_kernel<VT><<<gw, kCoarseThreads, 0, st>>>(kw.nc, kw.agg_ptr, kw.agg_rows, r, kw.cvec, nullptr);
@@ -2124,8 +2128,8 @@ int krylov_solve(ufem_ns_handle* h, const ufem_krylov_opts* ko, ufem_krylov_stat
         residual_kernel<double, double><<<g1, kRedThreads, 0, s>>>(n, h->d_rhs, kw.w, kw.r, kw.part,
                                                                    kw.part + kw.nblk);
       }
-      finalize_norm_kernel<<<1, 1, 0, s>>>(kw.nblk, kw.part, kw.dctl, kScale, 1);
-      finalize_norm_kernel<<<1, 1, 0, s>>>(kw.nblk, kw.part + kw.nblk, kw.dctl, kR2, 1);
+      finalize_norm_kernel<<<1, kRedThreads, 0, s>>>(kw.nblk, kw.part, kw.dctl, kScale, 1);
+      finalize_norm_kernel<<<1, kRedThreads, 0, s>>>(kw.nblk, kw.part + kw.nblk, kw.dctl, kR2, 1);
       UFEM_CUDA_TRY(cudaMemcpyAsync(kw.h_dctl, kw.dctl, 16 * sizeof(double), cudaMemcpyDeviceToHost, s));
       UFEM_CUDA_TRY(cudaStreamSynchronize(s));
       if (bnorm < 0) bnorm = kw.h_dctl[kR2];
