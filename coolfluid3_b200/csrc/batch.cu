@@ -276,7 +276,7 @@ __device__ __forceinline__ double* vec(const BatchMesh& M, double* work) {
 }
 
 // y = A x over the solver chunks (one CTA per chunk of at most kChunkNodes
-// nodes of one member; spmv_node per node, as spmv_kernel, and for triangles
+// nodes of one member; spmv_node per node (one warp each), and for triangles
 // spmv_node3_group with 4 nodes per warp): a finished member's chunks return
 // after one flag read, so an iteration costs what the members still iterating
 // need, not a launch over every node of the batch.
