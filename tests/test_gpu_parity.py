@@ -138,6 +138,35 @@ def test_apply_matches_scipy():
     assert vec_rel_error(y, ref) <= 1e-13
 
 
+@pytest.mark.parametrize("case", ["cube20", "fan30"])
+def test_apply_matches_scipy_on_long_walks_and_wide_rows(case):
+    """The coupled SpMV runs persistent warps that walk several nodes each,
+    with the next node's loads in flight: a 20^3 x 6 mesh (9,261 nodes, more
+    than the resident warps) takes every warp through that walk; a fan of 60
+    tetrahedra around one node gives a row of 33 neighbours, whose column
+    pairs past the first 32 each lane loads while it reduces the row."""
+    if case == "cube20":
+        pb = P.make_problem(3, 20)
+        coords, conn, up, lin, nu = pb.coords, pb.conn, pb.up, pb.lin, pb.nu
+    else:
+        from .test_assembly_kernels import fan_mesh, fan_state
+        coords, conn = fan_mesh(3, 30)
+        up, lin, nu = fan_state(coords)
+    ns = NavierStokes(coords, conn, dt=0.01, use_specializations=False)
+    ns.set_state(up, lin, nu)
+    ns.assemble()
+    rp, ci = ns.csr()
+    v, _ = ns.system()
+    ref_op = csr_matrix(rp, ci, v, ns.nb_rows)
+    rng = np.random.default_rng(5)
+    for _ in range(2):  # the same y twice (deterministic)
+        x = rng.normal(size=ns.nb_rows)
+        y = ns.apply(x)
+        assert vec_rel_error(y, ref_op @ x) <= 1e-13
+        assert np.array_equal(y, ns.apply(x))
+    ns.close()
+
+
 def fp64_residual(ns) -> float:
     """||b - A x|| / ||b|| of the GPU's solution, evaluated on the host in FP64."""
     rp, ci = ns.csr()
