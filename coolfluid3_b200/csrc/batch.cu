@@ -276,8 +276,9 @@ __device__ __forceinline__ double* vec(const BatchMesh& M, double* work) {
 }
 
 // y = A x over the solver chunks (one CTA per chunk of at most kChunkNodes
-// nodes of one member; spmv_node per node (one warp each), and for triangles
-// spmv_node3_group with 4 nodes per warp): a finished member's chunks return
+// nodes of one member; each warp walks its nodes with spmv4_walk, and for
+// triangles 8-lane groups with spmv_group_walk, 4 nodes per warp at a time,
+// each with the next node's loads in flight): a finished member's chunks return
 // after one flag read, so an iteration costs what the members still iterating
 // need, not a launch over every node of the batch.
 template <int NEQ, typename MT, int XL>
@@ -293,11 +294,10 @@ __global__ void __launch_bounds__(256) spmv_chunk_kernel(const Chunk* __restrict
   double* y = ywork + M.row_off;
   const MT* vals;
   if constexpr (std::is_same<MT, float>::value) vals = M.vals32; else vals = M.vals;
-  for (int node = c.lo / NEQ + warp; node < c.hi / NEQ; node += int(blockDim.x >> 5)) {
-    const int64_t s0 = __ldg(M.start + node);
-    const int S = int(__ldg(M.start + node + 1) - s0);
-    spmv_node<NEQ, MT, double, double>(vals + int64_t(NEQ) * NEQ * s0, S, M.adj + s0, x, lane, y + int64_t(node) * NEQ);
-  }
+  static_assert(NEQ == 4, "the tetrahedron chunks; triangles use spmv3_chunk_kernel");
+  // the warp's nodes of the chunk, with the next node's loads in flight
+  spmv4_walk<MT, double, double>(c.lo / NEQ + warp, c.hi / NEQ, int(blockDim.x >> 5), M.start, M.adj, vals, x, y,
+                                 lane);
 }
 
 template <typename MT, int XL>
@@ -311,15 +311,10 @@ __global__ void __launch_bounds__(256) spmv3_chunk_kernel(const Chunk* __restric
   const int grp = threadIdx.x >> 3, sub = threadIdx.x & 7;  // 4 nodes per warp, 8 lanes each
   const MT* vals;
   if constexpr (std::is_same<MT, float>::value) vals = M.vals32; else vals = M.vals;
-  const int n0 = c.lo / 3, n1 = c.hi / 3;
-  for (int base = n0; base < n1; base += int(blockDim.x >> 3)) {  // the same trip count for every lane
-    const int node = base + grp;
-    const bool valid = node < n1;
-    const int64_t s0 = valid ? __ldg(M.start + node) : 0;
-    const int S = valid ? int(__ldg(M.start + node + 1) - s0) : 0;
-    spmv_node3_group<MT, double, double>(vals + 9 * s0, S, M.adj + s0, vec<XL>(M, xwork), sub, valid,
-                                         ywork + M.row_off + int64_t(valid ? node : 0) * 3);
-  }
+  // the chunk's nodes, 32 at a time (the same trip count for every lane), with
+  // each group's next node's loads in flight
+  spmv_group_walk<3, MT, double, double>(c.lo / 3, c.hi / 3, int(blockDim.x >> 3), grp, sub, M.start, M.adj, vals,
+                                         vec<XL>(M, xwork), ywork + M.row_off);
 }
 
 // dinv = 1 / diag (point Jacobi) of the operator the solve uses.

@@ -279,119 +279,31 @@ bool spd_invert(double* A, int n, int threads = 0) {
 // contiguous (row r, neighbour slot s, component c at r*S*NEQ + s*NEQ + c);
 // FP64 accumulation, fixed-order warp reduction.
 //
-// NEQ = 4 (the coupled tetrahedron system): persistent warps that keep the next node's loads in
-// flight: warp w walks the nodes w, w + W, w + 2W, ... (W: warps of the grid).
-// While it reduces one node, the neighbour ids and values of its next node and
-// the row extent of the node after that are already loading, so the chain
-// extent -> values and ids -> x costs one round trip a node instead of three.
-// Lane l owns the column pairs l, l + 32, ... of a node exactly as in
-// spmv_node, summed in the same order: the same y, bitwise.  The prefetched
-// pair is the lane's first; a node with more than 16 neighbours loads its
-// further pairs when it is reduced.
+// NEQ = 4 (the coupled tetrahedron system): persistent warps, warp w walking
+// the nodes w, w + W, w + 2W, ... (W: warps of the grid) with spmv4_walk, the
+// next node's loads in flight while one node is reduced.
 template <typename VT, typename MT>
 __global__ void __launch_bounds__(256, 3) spmv4_stream_kernel(int64_t N, const int64_t* __restrict__ start,
                                                              const int32_t* __restrict__ adj,
                                                              const MT* __restrict__ vals, const VT* __restrict__ x,
                                                              VT* __restrict__ y, const int* __restrict__ done) {
-  using MP = typename Pair<MT>::type;
-  using XP = typename Pair<VT>::type;
-  const int lane = threadIdx.x & 31;
-  const int64_t W = int64_t(gridDim.x) * (blockDim.x >> 5);
-  int64_t node = (int64_t(blockIdx.x) * blockDim.x + threadIdx.x) >> 5;
-  if (node >= N) return;  // whole warp
   if (done && *done) return;
-  // the lane's first column pair of the block row at s0 (S neighbours)
-  auto load_first = [&](int64_t s0, int S, int& col, MP (&v)[4]) {
-    if (lane < 2 * S) {
-      col = __ldg(adj + s0 + (lane >> 1));
-      const MP* __restrict__ rp = reinterpret_cast<const MP*>(vals + 16 * s0);
-#pragma unroll
-      for (int r = 0; r < 4; ++r) v[r] = __ldcs(rp + (r * 2 * S + lane));  // streamed once
-    }
-  };
-  int64_t sA = __ldg(start + node);
-  int SA = int(__ldg(start + node + 1) - sA);
-  int colA = 0;
-  MP vA[4];
-  load_first(sA, SA, colA, vA);
-  int64_t nodeB = node + W, sB = 0;
-  int SB = 0;
-  if (nodeB < N) {
-    sB = __ldg(start + nodeB);
-    SB = int(__ldg(start + nodeB + 1) - sB);
-  }
-  for (;;) {
-    XP xA;
-    if (lane < 2 * SA) xA = __ldg(reinterpret_cast<const XP*>(x + int64_t(colA) * 4 + (lane & 1) * 2));
-    // the next node's first pair and the extent of the node after it
-    int colB = 0;
-    MP vB[4];
-    const int64_t nodeC = nodeB + W;
-    int64_t sC = 0;
-    int SC = 0;
-    if (nodeB < N) {
-      load_first(sB, SB, colB, vB);
-      if (nodeC < N) {
-        sC = __ldg(start + nodeC);
-        SC = int(__ldg(start + nodeC + 1) - sC);
-      }
-    }
-    double acc[4] = {0.0, 0.0, 0.0, 0.0};
-    if (lane < 2 * SA) {
-#pragma unroll
-      for (int r = 0; r < 4; ++r) {
-        acc[r] = fma(double(vA[r].x), double(xA.x), acc[r]);
-        acc[r] = fma(double(vA[r].y), double(xA.y), acc[r]);
-      }
-    }
-    {  // further pairs of a node with more than 16 neighbours
-      const MP* __restrict__ rp = reinterpret_cast<const MP*>(vals + 16 * sA);
-      const int stride = 2 * SA;
-#pragma unroll 1
-      for (int p = lane + 32; p < stride; p += 32) {
-        const int col = __ldg(adj + sA + (p >> 1));
-        const XP xv = __ldg(reinterpret_cast<const XP*>(x + int64_t(col) * 4 + (p & 1) * 2));
-        MP v[4];
-#pragma unroll
-        for (int r = 0; r < 4; ++r) v[r] = __ldcs(rp + (r * stride + p));
-#pragma unroll
-        for (int r = 0; r < 4; ++r) {
-          acc[r] = fma(double(v[r].x), double(xv.x), acc[r]);
-          acc[r] = fma(double(v[r].y), double(xv.y), acc[r]);
-        }
-      }
-    }
-    const double sum = warp_sum4(acc, lane);
-    if ((lane & 7) == 0) y[node * 4 + (lane >> 3)] = VT(sum);
-    if (nodeB >= N) break;
-    node = nodeB;
-    sA = sB;
-    SA = SB;
-    colA = colB;
-#pragma unroll
-    for (int r = 0; r < 4; ++r) vA[r] = vB[r];
-    nodeB = nodeC;
-    sB = sC;
-    SB = SC;
-  }
+  spmv4_walk<MT, VT, VT>((int64_t(blockIdx.x) * blockDim.x + threadIdx.x) >> 5, N,
+                         int64_t(gridDim.x) * (blockDim.x >> 5), start, adj, vals, x, y, threadIdx.x & 31);
 }
 
-// y = A x for block rows of NEQ <= 3 equations: 4 nodes per warp (spmv_node_group).
+// y = A x for block rows of NEQ <= 3 equations: persistent 8-lane groups, 4 a
+// warp, walking the nodes g, g + G, ... (G: groups of the grid) with the next
+// node's loads in flight (spmv_group_walk).
 template <int NEQ, typename VT, typename MT>
 __global__ void __launch_bounds__(256) spmv_small_kernel(int64_t N, const int64_t* __restrict__ start,
                                                          const int32_t* __restrict__ adj, const MT* __restrict__ vals,
                                                          const VT* __restrict__ x, VT* __restrict__ y,
                                                          const int* __restrict__ done) {
+  if (done && *done) return;
   const int64_t t = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
-  if ((t >> 5) * 4 >= N) return;  // whole warp
-  const int stop = done ? *done : 0;
-  if (stop) return;
-  const int64_t node = t >> 3;
-  const int sub = int(t & 7);
-  const bool valid = node < N;
-  const int64_t s0 = valid ? __ldg(start + node) : 0;
-  const int S = valid ? int(__ldg(start + node + 1) - s0) : 0;
-  spmv_node_group<NEQ, MT, VT, VT>(vals + NEQ * NEQ * s0, S, adj + s0, x, sub, valid, y + node * NEQ);
+  spmv_group_walk<NEQ, MT, VT, VT>(0, N, int64_t(gridDim.x) * (blockDim.x >> 3), t >> 3, int(t & 7), start, adj,
+                                   vals, x, y);
 }
 
 template <typename MT, typename VT>
@@ -1379,12 +1291,27 @@ int spmv(ufem_ns_handle* h, const MT* vals, const VT* x, VT* y, const int* done,
     }();
     spmv4_stream_kernel<VT, MT><<<std::min(grid, resident), 256, 0, s>>>(h->N, h->d_start, h->d_adj, vals, x, y,
                                                                           done);
-  } else if (h->neq == 3)
-    spmv_small_kernel<3, VT, MT><<<grid8, 256, 0, s>>>(h->N, h->d_start, h->d_adj, vals, x, y, done);
-  else if (h->neq == 2)
-    spmv_small_kernel<2, VT, MT><<<grid8, 256, 0, s>>>(h->N, h->d_start, h->d_adj, vals, x, y, done);
-  else
-    spmv_small_kernel<1, VT, MT><<<grid8, 256, 0, s>>>(h->N, h->d_start, h->d_adj, vals, x, y, done);
+  } else {
+    // resident grid of the persistent group kernel (queried once per instantiation)
+    auto resident_of = [](auto kernel) {
+      int b = 0, dev = 0, sms = 0;
+      if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, kernel, 256, 0) != cudaSuccess) b = 1;
+      if (cudaGetDevice(&dev) != cudaSuccess ||
+          cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess)
+        sms = 1;
+      return unsigned(std::max(1, b) * std::max(1, sms));
+    };
+    if (h->neq == 3) {
+      static const unsigned r3 = resident_of(spmv_small_kernel<3, VT, MT>);
+      spmv_small_kernel<3, VT, MT><<<std::min(grid8, r3), 256, 0, s>>>(h->N, h->d_start, h->d_adj, vals, x, y, done);
+    } else if (h->neq == 2) {
+      static const unsigned r2 = resident_of(spmv_small_kernel<2, VT, MT>);
+      spmv_small_kernel<2, VT, MT><<<std::min(grid8, r2), 256, 0, s>>>(h->N, h->d_start, h->d_adj, vals, x, y, done);
+    } else {
+      static const unsigned r1 = resident_of(spmv_small_kernel<1, VT, MT>);
+      spmv_small_kernel<1, VT, MT><<<std::min(grid8, r1), 256, 0, s>>>(h->N, h->d_start, h->d_adj, vals, x, y, done);
+    }
+  }
   UFEM_CUDA_TRY(cudaGetLastError());
   return UFEM_OK;
 }
